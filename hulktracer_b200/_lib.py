@@ -1,0 +1,113 @@
+"""ctypes binding of ``libhulkcuda.so`` (the C ABI in include/hulkcuda.h).
+
+There is no fallback: if the library is missing or a call fails, an exception
+is raised.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "libhulkcuda.so")
+
+HK_OK = 0
+STATUS_NAMES = {0: "HK_OK", 1: "HK_E_ALLOC", 2: "HK_E_FILE_OPEN", 3: "HK_E_FILE_CLOSE",
+                4: "HK_E_ILLEGAL_INPUT", 5: "HK_E_NODE_NOT_FOUND", 16: "HK_E_CUDA",
+                17: "HK_E_DEVICE_TIMEOUT", 18: "HK_E_CAPACITY", 19: "HK_E_BOUNDS", 20: "HK_E_STATE"}
+
+FULLSTACK, SHORTSTACK, SMEMSTACK, RESTART, RESTART_EARLY, ROPES, BRUTE = range(7)
+VARIANTS = {"fullstack": FULLSTACK, "shortstack": SHORTSTACK, "smemstack": SMEMSTACK,
+            "restart": RESTART, "restart_early": RESTART_EARLY, "ropes": ROPES, "brute": BRUTE}
+BUILD_BINNED, BUILD_LEARNED = 0, 1
+SHADE_CPU, SHADE_PICTURE = 0, 1
+
+
+class HkError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__("%s: %s" % (STATUS_NAMES.get(status, str(status)), msg))
+        self.status = status
+
+
+class Config(C.Structure):
+    _fields_ = [("device", C.c_int), ("traverse_cost", C.c_float), ("intersect_cost", C.c_float),
+                ("max_depth", C.c_uint32), ("leaf_size", C.c_uint32), ("bins", C.c_uint32),
+                ("short_stack", C.c_uint32), ("block_size", C.c_uint32), ("blocks_per_sm", C.c_uint32),
+                ("max_refs", C.c_uint32), ("topk", C.c_uint32), ("fallback_ratio", C.c_float)]
+
+
+class TreeStats(C.Structure):
+    _fields_ = [("nodes", C.c_uint32), ("leaves", C.c_uint32), ("refs", C.c_uint32), ("depth", C.c_uint32),
+                ("build_ms", C.c_float), ("capacity_hit", C.c_uint32), ("learned_nodes", C.c_uint32),
+                ("fallback_nodes", C.c_uint32)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+HIT_DTYPE = np.dtype([("t", np.float32), ("tri", np.int32)])
+
+_lib = None
+
+
+def load(path: str = LIB_PATH):
+    """Load the CUDA library (raises if it is absent: there is no CPU path)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise FileNotFoundError("libhulkcuda.so not built (%s); run python -m hulktracer_b200.build" % path)
+    L = C.CDLL(path)
+    vp, u32, f32p, u32p = C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p
+    sig = {
+        "hk_config_default": [C.POINTER(Config)],
+        "hk_create": [C.POINTER(C.c_void_p), C.POINTER(Config)],
+        "hk_destroy": [vp],
+        "hk_set_stream": [vp, vp],
+        "hk_synchronize": [vp],
+        "hk_scene_upload": [vp, f32p, u32, u32p, u32],
+        "hk_scene_set_box": [vp, f32p],
+        "hk_scene_get_box": [vp, f32p],
+        "hk_scene_set_parts": [vp, u32p, u32],
+        "hk_scene_transform": [vp, f32p],
+        "hk_scene_get_vertices": [vp, f32p],
+        "hk_precompute": [vp],
+        "hk_cache_import": [vp, f32p, u32],
+        "hk_cache_export": [vp, f32p],
+        "hk_build": [vp, C.c_int, C.POINTER(TreeStats)],
+        "hk_tree_import": [vp, u32p, u32, u32p, u32],
+        "hk_tree_export": [vp, u32p, u32, u32p, u32, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)],
+        "hk_tree_export_compact": [vp, u32p, u32, u32p, u32, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)],
+        "hk_tree_stats_get": [vp, C.POINTER(TreeStats)],
+        "hk_trace": [vp, f32p, u32, C.c_int, vp],
+        "hk_trace_device": [vp, vp, u32, C.c_int, vp],
+        "hk_set_counting": [vp, C.c_int],
+        "hk_get_counters": [vp, vp],
+        "hk_camera_rays": [vp, f32p, u32, u32, f32p],
+        "hk_render": [vp, f32p, f32p, u32, u32, u32, C.c_int, C.c_int, u32p],
+        "hk_render_device": [vp, f32p, f32p, u32, u32, u32, C.c_int, C.c_int, vp],
+        "hk_shade_picture": [vp, f32p, f32p, u32, f32p, u32, u32p],
+        "hk_frame": [vp, f32p, f32p, f32p, u32, u32, u32, C.c_int, C.c_int, C.c_int, vp, C.POINTER(TreeStats)],
+    }
+    for name, args in sig.items():
+        fn = getattr(L, name)
+        fn.argtypes = args
+        fn.restype = C.c_int
+    L.hk_last_error.argtypes = [vp]
+    L.hk_last_error.restype = C.c_char_p
+    _lib = L
+    return L
+
+
+def exported_symbols() -> list[str]:
+    """Names the header declares (used by the load test)."""
+    import re
+    hdr = os.path.join(os.path.dirname(PKG), "include", "hulkcuda.h")
+    txt = open(hdr).read()
+    return sorted(set(re.findall(r"^(?:hk_status|const char \*)\s*(hk_\w+)\s*\(", txt, re.M)))
+
+
+def ptr(a: np.ndarray | None):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)

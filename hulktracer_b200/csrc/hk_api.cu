@@ -1,0 +1,851 @@
+// hk_api.cu -- the extern "C" boundary (include/hulkcuda.h): context,
+// device arena, input validation, tree import/export and the per-call
+// drivers around the kernels.
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "hk_build.h"
+#include "hk_common.cuh"
+#include "hk_internal.h"
+
+using namespace hk;
+
+namespace {
+
+template <class T>
+struct DevBuf {
+    T *p = nullptr;
+    size_t cap = 0;
+    cudaError_t ensure(size_t n) {
+        if (n <= cap && p) return cudaSuccess;
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+        size_t bytes = std::max<size_t>(n, 1) * sizeof(T);
+        cudaError_t e = cudaMalloc((void **)&p, bytes);
+        if (e == cudaSuccess) cap = std::max<size_t>(n, 1);
+        return e;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+    }
+};
+
+}  // namespace
+
+struct hk_ctx {
+    hk_config cfg;
+    int device = 0;
+    int sm_count = 148;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    // scene
+    uint32_t nv = 0, nt = 0, nparts = 0;
+    DevBuf<float4> verts, rest;
+    DevBuf<uint4> tris;
+    DevBuf<uint32_t> part;
+    DevBuf<float> mats;
+    DevBuf<float> box;          // 8 floats
+    DevBuf<uint32_t> box_ord;   // 8 words
+    float hbox[8] = {0};
+    bool box_user = false;
+    // triangle records
+    DevBuf<TriRec> rec;
+    DevBuf<float> cache_tmp;
+    bool rec_valid = false;
+    // tree (compact)
+    DevBuf<uint2> nodes;
+    DevBuf<uint32_t> refs;
+    uint32_t nn = 0, nr = 0;
+    bool tree_valid = false;
+    bool tree_built = false;             // current tree = the GPU builder's output
+    bool tree_on_device_counts = false;  // its sizes still live in device memory
+    hk_tree_stats stats{};
+    BuildState build;
+    // trace scratch
+    DevBuf<uint32_t> fetch;
+    DevBuf<unsigned long long> counters;
+    DevBuf<uint32_t> errw;
+    bool counting = false;
+    DevBuf<float4> rays;
+    DevBuf<hk_hit> hits;
+    DevBuf<float> cam, lights;
+    // shadow rays
+    DevBuf<float4> srays;
+    DevBuf<hk_hit> shits;
+    DevBuf<uint32_t> slot, spix, scount;
+    DevBuf<float4> hit4;
+    DevBuf<uint32_t> rgba;
+    // frame graph
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
+    uint64_t graph_key = 0;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+// current tree arrays (imported or built)
+static const uint2 *tree_nodes(hk_ctx *c) { return c->tree_built ? c->build.out_nodes : c->nodes.p; }
+static const uint32_t *tree_refs(hk_ctx *c) { return c->tree_built ? c->build.out_refs : c->refs.p; }
+
+#define HK_CUDA(ctx, call)                                                       \
+    do {                                                                         \
+        cudaError_t e_ = (call);                                                 \
+        if (e_ != cudaSuccess) {                                                 \
+            (ctx)->err = std::string(#call) + ": " + cudaGetErrorString(e_);     \
+            return HK_E_CUDA;                                                    \
+        }                                                                        \
+    } while (0)
+
+static hk_status fail(hk_ctx *c, hk_status s, const char *msg) {
+    if (c) c->err = msg;
+    return s;
+}
+
+static hk_status check_err_word(hk_ctx *c) {
+    uint32_t w = 0;
+    HK_CUDA(c, cudaMemcpyAsync(&w, c->errw.p, 4, cudaMemcpyDeviceToHost, c->stream));
+    HK_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (w) {
+        HK_CUDA(c, cudaMemsetAsync(c->errw.p, 0, 4, c->stream));
+        if (w & 2u) return fail(c, HK_E_CAPACITY, "device: arena capacity exceeded");
+        return fail(c, HK_E_BOUNDS, "device: traversal step bound exceeded (malformed tree?)");
+    }
+    return HK_OK;
+}
+
+extern "C" {
+
+hk_status hk_config_default(hk_config *cfg) {
+    if (!cfg) return HK_E_ILLEGAL_INPUT;
+    memset(cfg, 0, sizeof(*cfg));
+    cfg->device = 0;
+    cfg->traverse_cost = 1.0f;
+    cfg->intersect_cost = 1.5f;
+    cfg->max_depth = 24;
+    cfg->leaf_size = 4;
+    cfg->bins = 32;
+    cfg->short_stack = 6;
+    cfg->block_size = 128;
+    cfg->blocks_per_sm = 0;
+    cfg->max_refs = 0;
+    cfg->topk = 4;
+    cfg->fallback_ratio = 1.02f;
+    return HK_OK;
+}
+
+static hk_status validate_config(const hk_config *c) {
+    if (c->short_stack < 1 || c->short_stack > 16) return HK_E_ILLEGAL_INPUT;
+    if (c->block_size < 32 || c->block_size > 1024 || (c->block_size % 32)) return HK_E_ILLEGAL_INPUT;
+    if (c->bins != 32) return HK_E_ILLEGAL_INPUT;
+    if (c->max_depth < 1 || c->max_depth > 48) return HK_E_ILLEGAL_INPUT;
+    if (!(c->intersect_cost > 0) || !(c->traverse_cost >= 0)) return HK_E_ILLEGAL_INPUT;
+    return HK_OK;
+}
+
+hk_status hk_create(hk_ctx **out, const hk_config *cfg) {
+    if (!out) return HK_E_ILLEGAL_INPUT;
+    *out = nullptr;
+    hk_config c;
+    if (cfg) c = *cfg;
+    else hk_config_default(&c);
+    if (validate_config(&c) != HK_OK) return HK_E_ILLEGAL_INPUT;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || c.device < 0 || c.device >= ndev) return HK_E_CUDA;
+    hk_ctx *x = new hk_ctx();
+    x->cfg = c;
+    x->device = c.device;
+    if (cudaSetDevice(c.device) != cudaSuccess) {
+        delete x;
+        return HK_E_CUDA;
+    }
+    cudaDeviceGetAttribute(&x->sm_count, cudaDevAttrMultiProcessorCount, c.device);
+    if (cudaStreamCreateWithFlags(&x->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete x;
+        return HK_E_CUDA;
+    }
+    x->stream = x->own_stream;
+    cudaEventCreate(&x->ev0);
+    cudaEventCreate(&x->ev1);
+    if (x->fetch.ensure(4) || x->counters.ensure(3) || x->errw.ensure(1) || x->box.ensure(8) ||
+        x->box_ord.ensure(8) || x->scount.ensure(1)) {
+        hk_destroy(x);
+        return HK_E_ALLOC;
+    }
+    cudaMemset(x->errw.p, 0, 4);
+    cudaMemset(x->counters.p, 0, 24);
+    *out = x;
+    return HK_OK;
+}
+
+hk_status hk_destroy(hk_ctx *c) {
+    if (!c) return HK_E_ILLEGAL_INPUT;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
+    if (c->graph) cudaGraphDestroy(c->graph);
+    c->verts.release(); c->rest.release(); c->tris.release(); c->part.release(); c->mats.release();
+    c->box.release(); c->box_ord.release(); c->rec.release(); c->cache_tmp.release();
+    c->nodes.release(); c->refs.release(); c->fetch.release(); c->counters.release(); c->errw.release();
+    c->rays.release(); c->hits.release(); c->cam.release(); c->lights.release();
+    c->srays.release(); c->shits.release(); c->slot.release(); c->spix.release(); c->scount.release();
+    c->hit4.release(); c->rgba.release();
+    build_release(c->build);
+    if (c->ev0) cudaEventDestroy(c->ev0);
+    if (c->ev1) cudaEventDestroy(c->ev1);
+    if (c->own_stream) cudaStreamDestroy(c->own_stream);
+    delete c;
+    return HK_OK;
+}
+
+const char *hk_last_error(const hk_ctx *c) { return c ? c->err.c_str() : "null context"; }
+
+hk_status hk_set_stream(hk_ctx *c, void *s) {
+    if (!c) return HK_E_ILLEGAL_INPUT;
+    c->stream = s ? (cudaStream_t)s : c->own_stream;
+    return HK_OK;
+}
+
+hk_status hk_synchronize(hk_ctx *c) {
+    if (!c) return HK_E_ILLEGAL_INPUT;
+    cudaSetDevice(c->device);
+    HK_CUDA(c, cudaStreamSynchronize(c->stream));
+    return check_err_word(c);
+}
+
+// ---------------------------------------------------------------------------
+// scene
+// ---------------------------------------------------------------------------
+static void host_box(const float *v, uint32_t nv, float *box) {
+    float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (uint32_t i = 0; i < nv; i++)
+        for (int k = 0; k < 3; k++) {
+            float x = v[4 * (size_t)i + k];
+            lo[k] = std::fmin(lo[k], x);
+            hi[k] = std::fmax(hi[k], x);
+        }
+    for (int k = 0; k < 3; k++) {
+        box[k] = lo[k];
+        box[4 + k] = hi[k];
+    }
+    box[3] = box[7] = 1.0f;
+}
+
+static void invalidate_graph(hk_ctx *c) {
+    if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
+    if (c->graph) cudaGraphDestroy(c->graph);
+    c->graph_exec = nullptr;
+    c->graph = nullptr;
+    c->graph_key = 0;
+}
+
+hk_status hk_scene_upload(hk_ctx *c, const float *verts4, uint32_t nv, const uint32_t *tris4, uint32_t nt) {
+    if (!c || (nv && !verts4) || (nt && !tris4)) return fail(c, HK_E_ILLEGAL_INPUT, "null scene array");
+    if (nt > (1u << 28)) return fail(c, HK_E_ILLEGAL_INPUT, "too many triangles");
+    for (uint32_t i = 0; i < nv; i++) {
+        const float *v = verts4 + 4 * (size_t)i;
+        if (v[3] != 1.0f || !std::isfinite(v[0]) || !std::isfinite(v[1]) || !std::isfinite(v[2]))
+            return fail(c, HK_E_ILLEGAL_INPUT, "vertices must be finite with w == 1");
+    }
+    for (size_t i = 0; i < (size_t)nt * 4; i++)
+        if ((i & 3) != 3 && tris4[i] >= nv) return fail(c, HK_E_ILLEGAL_INPUT, "triangle index out of range");
+    cudaSetDevice(c->device);
+    invalidate_graph(c);
+    HK_CUDA(c, c->verts.ensure(nv));
+    HK_CUDA(c, c->tris.ensure(nt));
+    HK_CUDA(c, c->rec.ensure(nt));
+    HK_CUDA(c, cudaMemcpyAsync(c->verts.p, verts4, (size_t)nv * 16, cudaMemcpyHostToDevice, c->stream));
+    HK_CUDA(c, cudaMemcpyAsync(c->tris.p, tris4, (size_t)nt * 16, cudaMemcpyHostToDevice, c->stream));
+    c->nv = nv;
+    c->nt = nt;
+    c->nparts = 0;
+    c->rec_valid = false;
+    c->tree_valid = false;
+    c->box_user = false;
+    host_box(verts4, nv, c->hbox);
+    HK_CUDA(c, cudaMemcpyAsync(c->box.p, c->hbox, 32, cudaMemcpyHostToDevice, c->stream));
+    HK_CUDA(c, cudaStreamSynchronize(c->stream));
+    return HK_OK;
+}
+
+hk_status hk_scene_set_box(hk_ctx *c, const float *box8) {
+    if (!c || !box8) return HK_E_ILLEGAL_INPUT;
+    for (int k = 0; k < 3; k++)
+        if (!(box8[k] <= box8[4 + k])) return fail(c, HK_E_ILLEGAL_INPUT, "box min > max");
+    cudaSetDevice(c->device);
+    memcpy(c->hbox, box8, 32);
+    c->box_user = true;
+    HK_CUDA(c, cudaMemcpyAsync(c->box.p, c->hbox, 32, cudaMemcpyHostToDevice, c->stream));
+    HK_CUDA(c, cudaStreamSynchronize(c->stream));
+    return HK_OK;
+}
+
+hk_status hk_scene_get_box(hk_ctx *c, float *box8) {
+    if (!c || !box8) return HK_E_ILLEGAL_INPUT;
+    cudaSetDevice(c->device);
+    HK_CUDA(c, cudaMemcpyAsync(box8, c->box.p, 32, cudaMemcpyDeviceToHost, c->stream));
+    HK_CUDA(c, cudaStreamSynchronize(c->stream));
+    return HK_OK;
+}
+
+hk_status hk_scene_set_parts(hk_ctx *c, const uint32_t *part, uint32_t nparts) {
+    if (!c || !part || nparts == 0) return fail(c, HK_E_ILLEGAL_INPUT, "parts");
+    if (c->nv == 0) return fail(c, HK_E_STATE, "upload the scene first");
+    for (uint32_t i = 0; i < c->nv; i++)
+        if (part[i] >= nparts) return fail(c, HK_E_ILLEGAL_INPUT, "part index out of range");
+    cudaSetDevice(c->device);
+    invalidate_graph(c);
+    HK_CUDA(c, c->part.ensure(c->nv));
+    HK_CUDA(c, c->rest.ensure(c->nv));
+    HK_CUDA(c, c->mats.ensure((size_t)nparts * 12));
+    HK_CUDA(c, cudaMemcpyAsync(c->part.p, part, (size_t)c->nv * 4, cudaMemcpyHostToDevice, c->stream));
+    HK_CUDA(c, cudaMemcpyAsync(c->rest.p, c->verts.p, (size_t)c->nv * 16, cudaMemcpyDeviceToDevice, c->stream));
+    c->nparts = nparts;
+    HK_CUDA(c, cudaStreamSynchronize(c->stream));
+    return HK_OK;
+}
+
+// device part of a frame's transform: mats already in c->mats
+static hk_status transform_device(hk_ctx *c) {
+    HK_CUDA(c, launch_transform(c->rest.p, c->part.p, c->nv, c->mats.p, c->verts.p, c->box_ord.p, c->stream));
+    if (!c->box_user) HK_CUDA(c, launch_box_finish(c->box_ord.p, c->box.p, c->stream));
+    HK_CUDA(c, launch_precompute(c->verts.p, c->tris.p, c->nt, c->rec.p, c->stream));
+    c->rec_valid = true;
+    return HK_OK;
+}
+
+hk_status hk_scene_transform(hk_ctx *c, const float *mats12) {
+    if (!c || !mats12) return HK_E_ILLEGAL_INPUT;
+    if (c->nparts == 0) return fail(c, HK_E_STATE, "hk_scene_set_parts first");
+    cudaSetDevice(c->device);
+    HK_CUDA(c, cudaMemcpyAsync(c->mats.p, mats12, (size_t)c->nparts * 48, cudaMemcpyHostToDevice, c->stream));
+    hk_status s = transform_device(c);
+    if (s != HK_OK) return s;
+    c->tree_valid = false;
+    HK_CUDA(c, cudaStreamSynchronize(c->stream));
+    return HK_OK;
+}
+
+hk_status hk_scene_get_vertices(hk_ctx *c, float *verts4) {
+    if (!c || !verts4) return HK_E_ILLEGAL_INPUT;
+    cudaSetDevice(c->device);
+    HK_CUDA(c, cudaMemcpyAsync(verts4, c->verts.p, (size_t)c->nv * 16, cudaMemcpyDeviceToHost, c->stream));
+    HK_CUDA(c, cudaStreamSynchronize(c->stream));
+    return HK_OK;
+}
+
+// ---------------------------------------------------------------------------
+// triangle cache
+// ---------------------------------------------------------------------------
+hk_status hk_precompute(hk_ctx *c) {
+    if (!c) return HK_E_ILLEGAL_INPUT;
+    if (c->nt == 0 && c->nv == 0) return fail(c, HK_E_STATE, "no scene");
+    cudaSetDevice(c->device);
+    HK_CUDA(c, launch_precompute(c->verts.p, c->tris.p, c->nt, c->rec.p, c->stream));
+    HK_CUDA(c, cudaStreamSynchronize(c->stream));
+    c->rec_valid = true;
+    return HK_OK;
+}
+
+hk_status hk_cache_import(hk_ctx *c, const float *cache16, uint32_t nt) {
+    if (!c || (nt && !cache16)) return HK_E_ILLEGAL_INPUT;
+    if (nt != c->nt) return fail(c, HK_E_ILLEGAL_INPUT, "cache size != triangle count");
+    for (uint32_t i = 0; i < nt; i++) {
+        const float *q = cache16 + 16 * (size_t)i;
+        // w lanes of normal / e0 / e1 are 0 for w == 1 vertices (NaN normal of a
+        // zero-area triangle included: it never produces a hit)
+        bool nan_n = std::isnan(q[0]) || std::isnan(q[1]) || std::isnan(q[2]);
+        if (!(q[7] == 0.0f && q[11] == 0.0f && (q[3] == 0.0f || nan_n)))
+            return fail(c, HK_E_ILLEGAL_INPUT, "cache w lanes must be 0");
+    }
+    cudaSetDevice(c->device);
+    HK_CUDA(c, c->cache_tmp.ensure((size_t)nt * 16));
+    HK_CUDA(c, cudaMemcpyAsync(c->cache_tmp.p, cache16, (size_t)nt * 64, cudaMemcpyHostToDevice, c->stream));
+    HK_CUDA(c, launch_cache_to_rec(c->cache_tmp.p, c->verts.p, c->tris.p, nt, c->rec.p, c->stream));
+    HK_CUDA(c, cudaStreamSynchronize(c->stream));
+    c->rec_valid = true;
+    return HK_OK;
+}
+
+hk_status hk_cache_export(hk_ctx *c, float *cache16) {
+    if (!c || !cache16) return HK_E_ILLEGAL_INPUT;
+    if (!c->rec_valid) return fail(c, HK_E_STATE, "no cache");
+    cudaSetDevice(c->device);
+    HK_CUDA(c, c->cache_tmp.ensure((size_t)c->nt * 16));
+    HK_CUDA(c, launch_rec_to_cache(c->rec.p, c->nt, c->cache_tmp.p, c->stream));
+    HK_CUDA(c, cudaMemcpyAsync(cache16, c->cache_tmp.p, (size_t)c->nt * 64, cudaMemcpyDeviceToHost, c->stream));
+    HK_CUDA(c, cudaStreamSynchronize(c->stream));
+    return HK_OK;
+}
+
+// ---------------------------------------------------------------------------
+// tree import / export
+// ---------------------------------------------------------------------------
+hk_status hk_tree_import(hk_ctx *c, const uint32_t *nodes4, uint32_t nn, const uint32_t *refs, uint32_t nr) {
+    if (!c || !nodes4 || nn == 0 || (nr && !refs)) return fail(c, HK_E_ILLEGAL_INPUT, "tree arrays");
+    if (c->nt == 0) return fail(c, HK_E_STATE, "upload the scene first");
+    if (nn >= (1u << 29) || nr >= (1u << 30)) return fail(c, HK_E_ILLEGAL_INPUT, "tree too large");
+    for (uint32_t i = 0; i < nr; i++)
+        if (refs[i] >= c->nt) return fail(c, HK_E_ILLEGAL_INPUT, "leaf reference out of range");
+    // breadth-first relayout into child pairs; reference child 0 -> empty cell
+    std::vector<uint2> out;
+    out.reserve(2 * (size_t)nn + 2);
+    std::vector<uint32_t> src;
+    src.reserve(2 * (size_t)nn + 2);
+    std::vector<uint8_t> seen(nn, 0);
+    const uint32_t kEmpty = 0xffffffffu, kPad = 0xfffffffeu;
+    src.push_back(0);
+    src.push_back(kPad);
+    seen[0] = 1;
+    for (size_t h = 0; h < src.size(); h++) {
+        uint32_t s = src[h];
+        uint2 cn;
+        if (s == kEmpty || s == kPad) {
+            cn = make_uint2(kLeafTag, 0);
+        } else {
+            const uint32_t *n = nodes4 + 4 * (size_t)s;
+            if (n[0] == 4u) {
+                if ((uint64_t)n[1] + n[2] > nr) return fail(c, HK_E_ILLEGAL_INPUT, "leaf range out of bounds");
+                cn = make_uint2((n[1] << 2) | kLeafTag, n[2]);
+            } else if ((n[0] & ~3u) == 8u && (n[0] & 3u) < 3u) {
+                uint32_t above = n[1], below = n[2];
+                if (above >= nn || below >= nn) return fail(c, HK_E_ILLEGAL_INPUT, "child index out of range");
+                for (uint32_t ch : {below, above}) {
+                    if (ch == 0) continue;
+                    if (seen[ch]) return fail(c, HK_E_ILLEGAL_INPUT, "tree is not a tree (shared or cyclic child)");
+                    seen[ch] = 1;
+                }
+                uint32_t pair = (uint32_t)src.size();
+                src.push_back(below ? below : kEmpty);
+                src.push_back(above ? above : kEmpty);
+                cn = make_uint2((pair << 2) | (n[0] & 3u), n[3]);
+            } else {
+                return fail(c, HK_E_ILLEGAL_INPUT, "bad node flags");
+            }
+        }
+        out.push_back(cn);
+    }
+    cudaSetDevice(c->device);
+    invalidate_graph(c);
+    HK_CUDA(c, c->nodes.ensure(out.size()));
+    HK_CUDA(c, c->refs.ensure(std::max<uint32_t>(nr, 1)));
+    HK_CUDA(c, cudaMemcpyAsync(c->nodes.p, out.data(), out.size() * 8, cudaMemcpyHostToDevice, c->stream));
+    if (nr) HK_CUDA(c, cudaMemcpyAsync(c->refs.p, refs, (size_t)nr * 4, cudaMemcpyHostToDevice, c->stream));
+    HK_CUDA(c, cudaStreamSynchronize(c->stream));
+    c->nn = (uint32_t)out.size();
+    c->nr = nr;
+    c->tree_valid = true;
+    c->tree_built = false;
+    c->tree_on_device_counts = false;
+    memset(&c->stats, 0, sizeof(c->stats));
+    c->stats.nodes = c->nn;
+    c->stats.refs = nr;
+    return HK_OK;
+}
+
+static hk_status sync_tree_sizes(hk_ctx *c) {
+    if (c->tree_on_device_counts) {
+        hk_status s = build_read_stats(c->build, c->stream, &c->stats);
+        if (s != HK_OK) return fail(c, s, "build stats");
+        c->nn = c->stats.nodes;
+        c->nr = c->stats.refs;
+        c->tree_on_device_counts = false;
+    }
+    return HK_OK;
+}
+
+hk_status hk_tree_export_compact(hk_ctx *c, uint32_t *cn, uint32_t cap_nodes, uint32_t *refs, uint32_t cap_refs,
+                                 uint32_t *nn, uint32_t *nr) {
+    if (!c) return HK_E_ILLEGAL_INPUT;
+    if (!c->tree_valid) return fail(c, HK_E_STATE, "no tree");
+    cudaSetDevice(c->device);
+    hk_status s = sync_tree_sizes(c);
+    if (s != HK_OK) return s;
+    if (nn) *nn = c->nn;
+    if (nr) *nr = c->nr;
+    if (!cn) return HK_OK;
+    if (cap_nodes < c->nn || cap_refs < c->nr) return fail(c, HK_E_CAPACITY, "export buffers too small");
+    HK_CUDA(c, cudaMemcpyAsync(cn, tree_nodes(c), (size_t)c->nn * 8, cudaMemcpyDeviceToHost, c->stream));
+    if (c->nr && refs) HK_CUDA(c, cudaMemcpyAsync(refs, tree_refs(c), (size_t)c->nr * 4, cudaMemcpyDeviceToHost, c->stream));
+    HK_CUDA(c, cudaStreamSynchronize(c->stream));
+    return HK_OK;
+}
+
+hk_status hk_tree_export(hk_ctx *c, uint32_t *nodes4, uint32_t cap_nodes, uint32_t *refs, uint32_t cap_refs,
+                         uint32_t *nn, uint32_t *nr) {
+    if (!c) return HK_E_ILLEGAL_INPUT;
+    if (!c->tree_valid) return fail(c, HK_E_STATE, "no tree");
+    cudaSetDevice(c->device);
+    hk_status s = sync_tree_sizes(c);
+    if (s != HK_OK) return s;
+    if (nn) *nn = c->nn;
+    if (nr) *nr = c->nr;
+    if (!nodes4) return HK_OK;
+    if (cap_nodes < c->nn || cap_refs < c->nr) return fail(c, HK_E_CAPACITY, "export buffers too small");
+    std::vector<uint2> cn(c->nn);
+    HK_CUDA(c, cudaMemcpyAsync(cn.data(), tree_nodes(c), (size_t)c->nn * 8, cudaMemcpyDeviceToHost, c->stream));
+    if (c->nr && refs) HK_CUDA(c, cudaMemcpyAsync(refs, tree_refs(c), (size_t)c->nr * 4, cudaMemcpyDeviceToHost, c->stream));
+    HK_CUDA(c, cudaStreamSynchronize(c->stream));
+    // same indices; empty cells become the reference's child 0
+    uint32_t leaf = 0;
+    auto empty = [&](uint32_t i) { return (cn[i].x & 3u) == kLeafTag && cn[i].y == 0; };
+    for (uint32_t i = 0; i < c->nn; i++) {
+        uint32_t *n = nodes4 + 4 * (size_t)i;
+        if ((cn[i].x & 3u) == kLeafTag) {
+            n[0] = 4u;
+            n[1] = cn[i].x >> 2;
+            n[2] = cn[i].y;
+            n[3] = leaf++;
+        } else {
+            uint32_t pair = cn[i].x >> 2;
+            n[0] = (cn[i].x & 3u) | 8u;
+            n[2] = empty(pair) ? 0u : pair;
+            n[1] = empty(pair + 1) ? 0u : pair + 1;
+            n[3] = cn[i].y;
+        }
+    }
+    return HK_OK;
+}
+
+hk_status hk_tree_stats_get(hk_ctx *c, hk_tree_stats *st) {
+    if (!c || !st) return HK_E_ILLEGAL_INPUT;
+    cudaSetDevice(c->device);
+    hk_status s = sync_tree_sizes(c);
+    if (s != HK_OK) return s;
+    *st = c->stats;
+    return HK_OK;
+}
+
+// ---------------------------------------------------------------------------
+// build
+// ---------------------------------------------------------------------------
+static BuildParams build_params(hk_ctx *c, hk_build_mode mode) {
+    BuildParams p;
+    p.ct = c->cfg.traverse_cost;
+    p.ci = c->cfg.intersect_cost;
+    p.max_depth = c->cfg.max_depth;
+    p.leaf_size = c->cfg.leaf_size;
+    p.max_refs = c->cfg.max_refs ? c->cfg.max_refs : std::max<uint32_t>(16u * c->nt, 1024u);
+    p.mode = (int)mode;
+    p.topk = c->cfg.topk;
+    p.fallback_ratio = c->cfg.fallback_ratio;
+    return p;
+}
+
+// enqueue a build on c->stream (no host synchronisation)
+static hk_status build_enqueue(hk_ctx *c, hk_build_mode mode) {
+    BuildParams p = build_params(c, mode);
+    hk_status s = build_prepare(c->build, p, c->nt, c->sm_count);
+    if (s != HK_OK) return fail(c, s, "builder arena allocation failed");
+    BuildOutputs o;
+    s = build_ensure_outputs(c->build, &o);
+    if (s != HK_OK) return fail(c, s, "builder output allocation failed");
+    cudaError_t e = build_launch(c->build, c->verts.p, c->tris.p, c->nt, c->box.p, c->stream);
+    if (e != cudaSuccess) {
+        c->err = std::string("build launch: ") + cudaGetErrorString(e);
+        return HK_E_CUDA;
+    }
+    // the device tree lives in the builder's output buffers
+    c->tree_valid = true;
+    c->tree_built = true;
+    c->tree_on_device_counts = true;
+    return HK_OK;
+}
+
+}  // extern "C"
+
+
+extern "C" {
+
+hk_status hk_build(hk_ctx *c, hk_build_mode mode, hk_tree_stats *stats) {
+    if (!c) return HK_E_ILLEGAL_INPUT;
+    if (c->nt == 0) return fail(c, HK_E_STATE, "no scene");
+    if (mode != HK_BUILD_BINNED && mode != HK_BUILD_LEARNED) return fail(c, HK_E_ILLEGAL_INPUT, "mode");
+    cudaSetDevice(c->device);
+    HK_CUDA(c, cudaEventRecord(c->ev0, c->stream));
+    hk_status s = build_enqueue(c, mode);
+    if (s != HK_OK) return s;
+    HK_CUDA(c, cudaEventRecord(c->ev1, c->stream));
+    HK_CUDA(c, cudaStreamSynchronize(c->stream));
+    s = check_err_word(c);
+    if (s != HK_OK) return s;
+    s = sync_tree_sizes(c);
+    if (s != HK_OK) return s;
+    float ms = 0;
+    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+    c->stats.build_ms = ms;
+    if (stats) *stats = c->stats;
+    return HK_OK;
+}
+
+// ---------------------------------------------------------------------------
+// tracing
+// ---------------------------------------------------------------------------
+static hk_status trace_enqueue(hk_ctx *c, const float4 *d_rays, uint32_t n, const uint32_t *n_dev, hk_variant v,
+                               hk_hit *d_hits) {
+    if ((int)v < HK_TRACE_FULLSTACK || (int)v > HK_TRACE_BRUTE) return fail(c, HK_E_ILLEGAL_INPUT, "variant");
+    if (!c->rec_valid) return fail(c, HK_E_STATE, "no triangle cache (hk_precompute or hk_cache_import)");
+    if (v != HK_TRACE_BRUTE && !c->tree_valid) return fail(c, HK_E_STATE, "no tree");
+    if (v == HK_TRACE_ROPES) return fail(c, HK_E_ILLEGAL_INPUT, "ropes variant not available");
+    TraceLaunch L;
+    memset(&L, 0, sizeof(L));
+    L.nodes = tree_nodes(c);
+    L.refs = tree_refs(c);
+    L.tris = c->rec.p;
+    L.rays = d_rays;
+    L.hits = d_hits;
+    L.n = n;
+    L.n_dev = n_dev;
+    L.ntris = c->nt;
+    L.box = c->box.p;
+    L.fetch = c->fetch.p;
+    L.counters = c->counters.p;
+    L.err = c->errw.p;
+    L.stack_depth = c->cfg.short_stack;
+    L.max_steps = 1u << 26;
+    L.variant = (int)v;
+    L.count = c->counting;
+    L.block = (int)c->cfg.block_size;
+    int per_sm = c->cfg.blocks_per_sm ? (int)c->cfg.blocks_per_sm : std::max(1, 2048 / L.block);
+    L.grid = c->sm_count * per_sm;
+    if (c->counting) HK_CUDA(c, cudaMemsetAsync(c->counters.p, 0, 24, c->stream));
+    HK_CUDA(c, launch_trace(L, c->stream));
+    return HK_OK;
+}
+
+hk_status hk_trace_device(hk_ctx *c, const float *d_rays8, uint32_t n, hk_variant v, hk_hit *d_hits) {
+    if (!c || (n && (!d_rays8 || !d_hits))) return HK_E_ILLEGAL_INPUT;
+    if ((reinterpret_cast<uintptr_t>(d_rays8) & 15u) || (reinterpret_cast<uintptr_t>(d_hits) & 7u))
+        return fail(c, HK_E_ILLEGAL_INPUT, "device arrays must be 16-byte (rays) / 8-byte (hits) aligned");
+    cudaSetDevice(c->device);
+    return trace_enqueue(c, reinterpret_cast<const float4 *>(d_rays8), n, nullptr, v, d_hits);
+}
+
+hk_status hk_trace(hk_ctx *c, const float *rays8, uint32_t n, hk_variant v, hk_hit *hits) {
+    if (!c || (n && (!rays8 || !hits))) return HK_E_ILLEGAL_INPUT;
+    for (size_t i = 0; i < n; i++)
+        if (rays8[8 * i + 3] != 0.0f || rays8[8 * i + 7] != 0.0f)
+            return fail(c, HK_E_ILLEGAL_INPUT, "ray w lanes must be 0");
+    cudaSetDevice(c->device);
+    HK_CUDA(c, c->rays.ensure(2 * (size_t)std::max<uint32_t>(n, 1)));
+    HK_CUDA(c, c->hits.ensure(std::max<uint32_t>(n, 1)));
+    HK_CUDA(c, cudaMemcpyAsync(c->rays.p, rays8, (size_t)n * 32, cudaMemcpyHostToDevice, c->stream));
+    hk_status s = trace_enqueue(c, c->rays.p, n, nullptr, v, c->hits.p);
+    if (s != HK_OK) return s;
+    HK_CUDA(c, cudaMemcpyAsync(hits, c->hits.p, (size_t)n * 8, cudaMemcpyDeviceToHost, c->stream));
+    HK_CUDA(c, cudaStreamSynchronize(c->stream));
+    return check_err_word(c);
+}
+
+hk_status hk_set_counting(hk_ctx *c, int enable) {
+    if (!c) return HK_E_ILLEGAL_INPUT;
+    c->counting = enable != 0;
+    return HK_OK;
+}
+
+hk_status hk_get_counters(hk_ctx *c, uint64_t *tot) {
+    if (!c || !tot) return HK_E_ILLEGAL_INPUT;
+    cudaSetDevice(c->device);
+    HK_CUDA(c, cudaMemcpyAsync(tot, c->counters.p, 24, cudaMemcpyDeviceToHost, c->stream));
+    HK_CUDA(c, cudaStreamSynchronize(c->stream));
+    return HK_OK;
+}
+
+hk_status hk_camera_rays(hk_ctx *c, const float *cam16, uint32_t w, uint32_t h, float *rays8) {
+    if (!c || !cam16 || !rays8) return HK_E_ILLEGAL_INPUT;
+    size_t n = (size_t)w * h;
+    if (n == 0 || n > (1u << 30)) return fail(c, HK_E_ILLEGAL_INPUT, "image size");
+    cudaSetDevice(c->device);
+    HK_CUDA(c, c->cam.ensure(16));
+    HK_CUDA(c, c->rays.ensure(2 * n));
+    HK_CUDA(c, cudaMemcpyAsync(c->cam.p, cam16, 64, cudaMemcpyHostToDevice, c->stream));
+    HK_CUDA(c, launch_camera_rays(c->cam.p, w, h, c->rays.p, c->stream));
+    HK_CUDA(c, cudaMemcpyAsync(rays8, c->rays.p, n * 32, cudaMemcpyDeviceToHost, c->stream));
+    HK_CUDA(c, cudaStreamSynchronize(c->stream));
+    return HK_OK;
+}
+
+// ---------------------------------------------------------------------------
+// rendering
+// ---------------------------------------------------------------------------
+static hk_status validate_lights(hk_ctx *c, const float *lights8, uint32_t nl) {
+    if (nl && !lights8) return fail(c, HK_E_ILLEGAL_INPUT, "lights");
+    if (nl > 64) return fail(c, HK_E_ILLEGAL_INPUT, "at most 64 lights");
+    return HK_OK;
+}
+
+static hk_status render_buffers(hk_ctx *c, uint32_t npix, uint32_t nl) {
+    size_t ns = (size_t)npix * std::max<uint32_t>(nl, 1);
+    HK_CUDA(c, c->rays.ensure(2 * (size_t)npix));
+    HK_CUDA(c, c->hits.ensure(npix));
+    HK_CUDA(c, c->srays.ensure(2 * ns));
+    HK_CUDA(c, c->shits.ensure(ns));
+    HK_CUDA(c, c->slot.ensure(ns));
+    HK_CUDA(c, c->spix.ensure(ns));
+    HK_CUDA(c, c->hit4.ensure(npix));
+    HK_CUDA(c, c->rgba.ensure(npix));
+    HK_CUDA(c, c->cam.ensure(16));
+    HK_CUDA(c, c->lights.ensure(8 * (size_t)std::max<uint32_t>(nl, 1)));
+    return HK_OK;
+}
+
+// camera + lights already in c->cam / c->lights
+static hk_status render_enqueue(hk_ctx *c, uint32_t nl, uint32_t w, uint32_t h, hk_variant v, int shade,
+                                uint32_t *d_rgba) {
+    uint32_t npix = w * h;
+    HK_CUDA(c, launch_camera_rays(c->cam.p, w, h, c->rays.p, c->stream));
+    hk_status s = trace_enqueue(c, c->rays.p, npix, nullptr, v, c->hits.p);
+    if (s != HK_OK) return s;
+    if (shade == HK_SHADE_PICTURE) {
+        HK_CUDA(c, launch_hit4(c->hits.p, c->rec.p, npix, c->hit4.p, c->stream));
+        HK_CUDA(c, launch_shade_picture(c->rays.p, c->hit4.p, npix, c->lights.p, nl, d_rgba, c->stream));
+        return HK_OK;
+    }
+    HK_CUDA(c, launch_shadow_rays(c->rays.p, c->hits.p, c->rec.p, npix, c->lights.p, nl, c->srays.p, c->slot.p,
+                                  c->spix.p, c->scount.p, c->stream));
+    s = trace_enqueue(c, c->srays.p, 0, c->scount.p, v, c->shits.p);
+    if (s != HK_OK) return s;
+    HK_CUDA(c, launch_shade_cpu(c->rays.p, c->hits.p, c->rec.p, npix, c->lights.p, nl, c->slot.p, c->shits.p,
+                                d_rgba, c->stream));
+    return HK_OK;
+}
+
+hk_status hk_render_device(hk_ctx *c, const float *cam16, const float *lights8, uint32_t nl, uint32_t w, uint32_t h,
+                           hk_variant v, int shade, uint32_t *d_rgba) {
+    if (!c || !cam16 || !d_rgba) return HK_E_ILLEGAL_INPUT;
+    if ((size_t)w * h == 0 || (size_t)w * h > (1u << 28)) return fail(c, HK_E_ILLEGAL_INPUT, "image size");
+    if (shade != HK_SHADE_CPU && shade != HK_SHADE_PICTURE) return fail(c, HK_E_ILLEGAL_INPUT, "shade mode");
+    hk_status s = validate_lights(c, lights8, nl);
+    if (s != HK_OK) return s;
+    cudaSetDevice(c->device);
+    s = render_buffers(c, w * h, nl);
+    if (s != HK_OK) return s;
+    HK_CUDA(c, cudaMemcpyAsync(c->cam.p, cam16, 64, cudaMemcpyHostToDevice, c->stream));
+    if (nl) HK_CUDA(c, cudaMemcpyAsync(c->lights.p, lights8, (size_t)nl * 32, cudaMemcpyHostToDevice, c->stream));
+    return render_enqueue(c, nl, w, h, v, shade, d_rgba);
+}
+
+hk_status hk_render(hk_ctx *c, const float *cam16, const float *lights8, uint32_t nl, uint32_t w, uint32_t h,
+                    hk_variant v, int shade, uint32_t *rgba) {
+    if (!c || !rgba) return HK_E_ILLEGAL_INPUT;
+    cudaSetDevice(c->device);
+    if ((size_t)w * h == 0 || (size_t)w * h > (1u << 28)) return fail(c, HK_E_ILLEGAL_INPUT, "image size");
+    hk_status s = render_buffers(c, w * h, nl);
+    if (s != HK_OK) return s;
+    s = hk_render_device(c, cam16, lights8, nl, w, h, v, shade, c->rgba.p);
+    if (s != HK_OK) return s;
+    HK_CUDA(c, cudaMemcpyAsync(rgba, c->rgba.p, (size_t)w * h * 4, cudaMemcpyDeviceToHost, c->stream));
+    HK_CUDA(c, cudaStreamSynchronize(c->stream));
+    return check_err_word(c);
+}
+
+hk_status hk_shade_picture(hk_ctx *c, const float *rays8, const float *hit4, uint32_t n, const float *lights8,
+                           uint32_t nl, uint32_t *rgba) {
+    if (!c || (n && (!rays8 || !hit4 || !rgba))) return HK_E_ILLEGAL_INPUT;
+    hk_status s = validate_lights(c, lights8, nl);
+    if (s != HK_OK) return s;
+    cudaSetDevice(c->device);
+    HK_CUDA(c, c->rays.ensure(2 * (size_t)std::max<uint32_t>(n, 1)));
+    HK_CUDA(c, c->hit4.ensure(std::max<uint32_t>(n, 1)));
+    HK_CUDA(c, c->rgba.ensure(std::max<uint32_t>(n, 1)));
+    HK_CUDA(c, c->lights.ensure(8 * (size_t)std::max<uint32_t>(nl, 1)));
+    HK_CUDA(c, cudaMemcpyAsync(c->rays.p, rays8, (size_t)n * 32, cudaMemcpyHostToDevice, c->stream));
+    HK_CUDA(c, cudaMemcpyAsync(c->hit4.p, hit4, (size_t)n * 16, cudaMemcpyHostToDevice, c->stream));
+    if (nl) HK_CUDA(c, cudaMemcpyAsync(c->lights.p, lights8, (size_t)nl * 32, cudaMemcpyHostToDevice, c->stream));
+    HK_CUDA(c, launch_shade_picture(c->rays.p, c->hit4.p, n, c->lights.p, nl, c->rgba.p, c->stream));
+    HK_CUDA(c, cudaMemcpyAsync(rgba, c->rgba.p, (size_t)n * 4, cudaMemcpyDeviceToHost, c->stream));
+    HK_CUDA(c, cudaStreamSynchronize(c->stream));
+    return HK_OK;
+}
+
+// ---------------------------------------------------------------------------
+// frame: transform -> build -> trace -> shade, optionally as a CUDA graph
+// ---------------------------------------------------------------------------
+static hk_status frame_enqueue(hk_ctx *c, bool animated, uint32_t nl, uint32_t w, uint32_t h, hk_build_mode mode,
+                               hk_variant v, uint32_t *d_rgba) {
+    hk_status s;
+    if (animated) {
+        s = transform_device(c);
+        if (s != HK_OK) return s;
+    } else if (!c->rec_valid) {
+        HK_CUDA(c, launch_precompute(c->verts.p, c->tris.p, c->nt, c->rec.p, c->stream));
+        c->rec_valid = true;
+    }
+    s = build_enqueue(c, mode);
+    if (s != HK_OK) return s;
+    return render_enqueue(c, nl, w, h, v, HK_SHADE_CPU, d_rgba);
+}
+
+hk_status hk_frame(hk_ctx *c, const float *mats12, const float *cam16, const float *lights8, uint32_t nl, uint32_t w,
+                   uint32_t h, hk_build_mode mode, hk_variant v, int use_graph, uint32_t *d_rgba,
+                   hk_tree_stats *stats) {
+    if (!c || !cam16 || !d_rgba) return HK_E_ILLEGAL_INPUT;
+    if (c->nt == 0) return fail(c, HK_E_STATE, "no scene");
+    if (mats12 && c->nparts == 0) return fail(c, HK_E_STATE, "hk_scene_set_parts first");
+    if ((size_t)w * h == 0 || (size_t)w * h > (1u << 28)) return fail(c, HK_E_ILLEGAL_INPUT, "image size");
+    hk_status s = validate_lights(c, lights8, nl);
+    if (s != HK_OK) return s;
+    cudaSetDevice(c->device);
+    s = render_buffers(c, w * h, nl);
+    if (s != HK_OK) return s;
+    // size every arena before any capture so that the graph never allocates
+    BuildParams bp = build_params(c, mode);
+    s = build_prepare(c->build, bp, c->nt, c->sm_count);
+    if (s != HK_OK) return fail(c, s, "builder arena allocation failed");
+    BuildOutputs bo;
+    s = build_ensure_outputs(c->build, &bo);
+    if (s != HK_OK) return fail(c, s, "builder output allocation failed");
+    // inputs of this frame
+    if (mats12) HK_CUDA(c, cudaMemcpyAsync(c->mats.p, mats12, (size_t)c->nparts * 48, cudaMemcpyHostToDevice, c->stream));
+    HK_CUDA(c, cudaMemcpyAsync(c->cam.p, cam16, 64, cudaMemcpyHostToDevice, c->stream));
+    if (nl) HK_CUDA(c, cudaMemcpyAsync(c->lights.p, lights8, (size_t)nl * 32, cudaMemcpyHostToDevice, c->stream));
+    bool animated = mats12 != nullptr;
+    if (!use_graph) {
+        s = frame_enqueue(c, animated, nl, w, h, mode, v, d_rgba);
+        if (s != HK_OK) return s;
+    } else {
+        uint64_t key = ((uint64_t)w << 40) ^ ((uint64_t)h << 20) ^ ((uint64_t)nl << 12) ^ ((uint64_t)mode << 8) ^
+                       ((uint64_t)v << 4) ^ (animated ? 1u : 0u) ^ ((uint64_t)(uintptr_t)d_rgba << 1) ^
+                       ((uint64_t)c->nt << 44);
+        if (!c->graph_exec || c->graph_key != key) {
+            invalidate_graph(c);
+            HK_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+            s = frame_enqueue(c, animated, nl, w, h, mode, v, d_rgba);
+            cudaGraph_t g = nullptr;
+            cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+            if (s != HK_OK) {
+                if (g) cudaGraphDestroy(g);
+                return s;
+            }
+            if (e != cudaSuccess) {
+                c->err = std::string("graph capture: ") + cudaGetErrorString(e);
+                return HK_E_CUDA;
+            }
+            c->graph = g;
+            HK_CUDA(c, cudaGraphInstantiate(&c->graph_exec, g, 0));
+            c->graph_key = key;
+        }
+        HK_CUDA(c, cudaGraphLaunch(c->graph_exec, c->stream));
+        c->tree_valid = true;
+        c->tree_built = true;
+        c->tree_on_device_counts = true;
+    }
+    if (stats) {
+        HK_CUDA(c, cudaStreamSynchronize(c->stream));
+        s = check_err_word(c);
+        if (s != HK_OK) return s;
+        s = sync_tree_sizes(c);
+        if (s != HK_OK) return s;
+        *stats = c->stats;
+    }
+    return HK_OK;
+}
+
+}  // extern "C"

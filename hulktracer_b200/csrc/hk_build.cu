@@ -1,0 +1,789 @@
+// hk_build.cu -- GPU KD-tree builder: exact binned SAH (sm_100a).
+//
+// Breadth-first and level-synchronous. Per level:
+//   prep/scan     which nodes are "large" and how many histogram chunks each has
+//   hist_large    one CTA per chunk of a large node: shared-memory histograms
+//                 (3 axes x {lo bin, hi bin, flat-on-plane}) of the clipped
+//                 reference bounds, flushed to global memory with atomics
+//   sah_large     one warp per large node: warp scans over the 32 bins, exact
+//                 SAH at the 31 planes of each axis, warp argmin
+//   small         one warp per small node: histogram in warp-private shared
+//                 memory, then the same SAH evaluation
+//   plan/scan     leaf refs, child pairs, next-level nodes, child refs
+//   guard         capacity check (the whole level stops splitting on overflow)
+//   emit          compact node entries and next-level node records
+//   scan/scatter  stable partition of the references (global exclusive scan of
+//                 below/above flags), leaf references to the output list
+//   advance       level counters
+// Every kernel reads its work size from device memory, so the whole build is
+// a fixed launch sequence (graph-capturable, no host round trips).
+//
+// The algorithm is restated serially in the CPU oracle (hko_build_binned); the
+// two produce identical trees. The plane / bin / cost arithmetic below is
+// written with explicit IEEE round-to-nearest intrinsics for that reason.
+#include <algorithm>
+#include <cstdio>
+
+#include "hk_build.h"
+#include "hk_common.cuh"
+#include "hk_internal.h"
+
+namespace hk {
+
+constexpr uint32_t kBins = 32;
+constexpr uint32_t kSmall = 256;     // nodes with <= kSmall refs: one warp per node
+constexpr uint32_t kChunk = 2048;    // refs per histogram CTA of a large node
+constexpr uint32_t kHist = 3 * 3 * kBins;
+constexpr int kScanThreads = 256;
+constexpr int kScanItems = 4;
+constexpr uint32_t kTile = kScanThreads * kScanItems;
+
+// ---------------------------------------------------------------------------
+// small vector types for the scans
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint2 vadd(uint2 a, uint2 b) { return make_uint2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ uint4 vadd(uint4 a, uint4 b) { return make_uint4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w); }
+template <class T> __device__ __forceinline__ T vzero();
+template <> __device__ __forceinline__ uint2 vzero<uint2>() { return make_uint2(0, 0); }
+template <> __device__ __forceinline__ uint4 vzero<uint4>() { return make_uint4(0, 0, 0, 0); }
+__device__ __forceinline__ uint2 shfl_up(uint2 v, int d) {
+    return make_uint2(__shfl_up_sync(0xffffffffu, v.x, d), __shfl_up_sync(0xffffffffu, v.y, d));
+}
+__device__ __forceinline__ uint4 shfl_up(uint4 v, int d) {
+    return make_uint4(__shfl_up_sync(0xffffffffu, v.x, d), __shfl_up_sync(0xffffffffu, v.y, d),
+                      __shfl_up_sync(0xffffffffu, v.z, d), __shfl_up_sync(0xffffffffu, v.w, d));
+}
+
+// inclusive warp scan
+template <class T>
+__device__ __forceinline__ T warp_incl(T v) {
+    const int lane = threadIdx.x & 31;
+    for (int d = 1; d < 32; d <<= 1) {
+        T u = shfl_up(v, d);
+        if (lane >= d) v = vadd(v, u);
+    }
+    return v;
+}
+
+__device__ __forceinline__ uint2 vsub(uint2 a, uint2 b) { return make_uint2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ uint4 vsub(uint4 a, uint4 b) { return make_uint4(a.x - b.x, a.y - b.y, a.z - b.z, a.w - b.w); }
+
+// exclusive block scan of one value per thread (kScanThreads threads); returns
+// the thread's exclusive prefix and the block total
+template <class T>
+__device__ __forceinline__ T block_excl(T v, T *sh_warp, T &total) {
+    constexpr int NW = kScanThreads / 32;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    T inc = warp_incl(v);
+    if (lane == 31) sh_warp[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+        T w = lane < NW ? sh_warp[lane] : vzero<T>();
+        T wi = warp_incl(w);
+        if (lane < NW) sh_warp[lane] = wi;
+    }
+    __syncthreads();
+    T wbase = warp ? sh_warp[warp - 1] : vzero<T>();
+    total = sh_warp[NW - 1];
+    __syncthreads();
+    return vadd(wbase, vsub(inc, v));
+}
+
+// scan phase 1: per-tile sums
+template <class T, class Load>
+__global__ void __launch_bounds__(kScanThreads) k_scan_reduce(Load ld, T *partials) {
+    __shared__ T sh[kScanThreads / 32 + 1];
+    const uint32_t n = ld.count();
+    const uint32_t ntiles = (n + kTile - 1) / kTile;
+    for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        T s = vzero<T>();
+        uint32_t base = tile * kTile + threadIdx.x * kScanItems;
+        for (int k = 0; k < kScanItems; k++)
+            if (base + k < n) s = vadd(s, ld(base + k));
+        T tot;
+        block_excl(s, sh, tot);
+        if (threadIdx.x == 0) partials[tile] = tot;
+    }
+}
+
+// scan phase 2: one CTA scans the tile sums (exclusive) and writes the total
+template <class T, class Load>
+__global__ void __launch_bounds__(kScanThreads) k_scan_partials(Load ld, T *partials, T *total) {
+    __shared__ T sh[kScanThreads / 32 + 1];
+    const uint32_t n = ld.count();
+    const uint32_t ntiles = (n + kTile - 1) / kTile;
+    T carry = vzero<T>();
+    for (uint32_t b = 0; b < ntiles; b += kScanThreads) {
+        uint32_t i = b + threadIdx.x;
+        T v = i < ntiles ? partials[i] : vzero<T>();
+        T tot;
+        T ex = block_excl(v, sh, tot);
+        if (i < ntiles) partials[i] = vadd(carry, ex);
+        carry = vadd(carry, tot);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *total = carry;
+}
+
+// scan phase 3: exclusive prefix of every element
+template <class T, class Load>
+__global__ void __launch_bounds__(kScanThreads) k_scan_apply(Load ld, const T *partials, T *out) {
+    __shared__ T sh[kScanThreads / 32 + 1];
+    const uint32_t n = ld.count();
+    const uint32_t ntiles = (n + kTile - 1) / kTile;
+    for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        uint32_t base = tile * kTile + threadIdx.x * kScanItems;
+        T v[kScanItems];
+        T s = vzero<T>();
+        for (int k = 0; k < kScanItems; k++) {
+            v[k] = (base + k < n) ? ld(base + k) : vzero<T>();
+            s = vadd(s, v[k]);
+        }
+        T tot;
+        T ex = vadd(partials[tile], block_excl(s, sh, tot));
+        for (int k = 0; k < kScanItems; k++) {
+            if (base + k < n) out[base + k] = ex;
+            ex = vadd(ex, v[k]);
+        }
+    }
+}
+
+template <class T, class Load>
+static cudaError_t scan(const Load &ld, T *partials, T *out, T *total, int grid, cudaStream_t s) {
+    k_scan_reduce<T, Load><<<grid, kScanThreads, 0, s>>>(ld, partials);
+    k_scan_partials<T, Load><<<1, kScanThreads, 0, s>>>(ld, partials, total);
+    k_scan_apply<T, Load><<<grid, kScanThreads, 0, s>>>(ld, partials, out);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// exact-order helpers shared with the oracle restatement
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float mxf(float a, float b) { return a > b ? a : b; }
+__device__ __forceinline__ float mnf(float a, float b) { return a < b ? a : b; }
+__device__ __forceinline__ float c3(float4 v, uint32_t a) { return a == 0 ? v.x : (a == 1 ? v.y : v.z); }
+__device__ __forceinline__ void s3(float4 &v, uint32_t a, float x) {
+    if (a == 0) v.x = x;
+    else if (a == 1) v.y = x;
+    else v.z = x;
+}
+
+// p_k = min + ext * (k / bins)
+__device__ __forceinline__ float plane_k(float blo, float ext, uint32_t k) {
+    return __fadd_rn(blo, __fmul_rn(ext, __fmul_rn((float)k, 0.03125f)));
+}
+
+__device__ __forceinline__ float surf(float4 lo, float4 hi) {
+    float sx = __fsub_rn(hi.x, lo.x), sy = __fsub_rn(hi.y, lo.y), sz = __fsub_rn(hi.z, lo.z);
+    return __fmul_rn(2.0f, __fadd_rn(__fadd_rn(__fmul_rn(sx, sy), __fmul_rn(sz, sy)), __fmul_rn(sx, sz)));
+}
+
+// bins of a clipped interval [lo, hi] on one axis: p_b <= lo < p_{b+1},
+// p_c < hi <= p_{c+1}; on = the interval is flat and lies on plane b
+__device__ __forceinline__ void bin_interval(float lo, float hi, float blo, float ext, float inv, int &b, int &c,
+                                             bool &on) {
+    b = __float2int_rz(__fmul_rn(__fsub_rn(lo, blo), inv));
+    b = b < 0 ? 0 : (b > (int)kBins - 1 ? (int)kBins - 1 : b);
+    while (b > 0 && lo < plane_k(blo, ext, b)) b--;
+    while (b < (int)kBins - 1 && lo >= plane_k(blo, ext, b + 1)) b++;
+    c = __float2int_rz(__fmul_rn(__fsub_rn(hi, blo), inv));
+    c = c < 0 ? 0 : (c > (int)kBins - 1 ? (int)kBins - 1 : c);
+    while (c > 0 && hi <= plane_k(blo, ext, c)) c--;
+    while (c < (int)kBins - 1 && hi > plane_k(blo, ext, c + 1)) c++;
+    on = (lo == hi) && b >= 1 && lo == plane_k(blo, ext, b);
+}
+
+// histogram contribution of one reference (shared-memory counters)
+__device__ __forceinline__ void hist_ref(uint32_t *H, float4 tlo, float4 thi, float4 blo, float4 bhi) {
+#pragma unroll
+    for (uint32_t a = 0; a < 3; a++) {
+        float l = c3(blo, a), h = c3(bhi, a);
+        float ext = __fsub_rn(h, l);
+        if (!(ext > 0.0f)) continue;
+        float inv = __fdiv_rn(32.0f, ext);
+        float lo = mxf(c3(tlo, a), l), hi = mnf(c3(thi, a), h);
+        int b, c;
+        bool on;
+        bin_interval(lo, hi, l, ext, inv, b, c, on);
+        atomicAdd(&H[a * 96 + b], 1u);
+        atomicAdd(&H[a * 96 + 32 + c], 1u);
+        if (on) atomicAdd(&H[a * 96 + 64 + b], 1u);
+    }
+}
+
+struct Decision {
+    int axis;
+    float plane;
+    uint32_t nb, na;
+    float cost;
+};
+
+// Warp-wide SAH over the node's histograms (all 32 lanes call it). The
+// first minimum in (axis, plane) order wins, as in the serial loop.
+template <class HistPtr>
+__device__ Decision sah_warp(HistPtr H, float4 blo, float4 bhi, uint32_t cnt, float ct, float ci) {
+    const uint32_t lane = threadIdx.x & 31u;
+    float A = surf(blo, bhi);
+    Decision best{-1, 0.0f, 0, 0, kInf};
+    for (uint32_t a = 0; a < 3; a++) {
+        float l = c3(blo, a), h = c3(bhi, a);
+        float ext = __fsub_rn(h, l);
+        if (!(ext > 0.0f)) continue;
+        uint32_t hlo = H[a * 96 + lane], hhi = H[a * 96 + 32 + lane];
+        // exclusive prefix over bins < lane
+        uint32_t slo = hlo, shi = hhi;
+        for (int d = 1; d < 32; d <<= 1) {
+            uint32_t u = __shfl_up_sync(0xffffffffu, slo, d), w = __shfl_up_sync(0xffffffffu, shi, d);
+            if ((int)lane >= d) {
+                slo += u;
+                shi += w;
+            }
+        }
+        uint32_t below = slo - hlo;          // sum_{b < k} hlo[b]
+        uint32_t above = cnt - (shi - hhi);  // sum_{c >= k} hhi[c]
+        uint32_t on = H[a * 96 + 64 + lane];
+        float pk = plane_k(l, ext, lane), pk1 = plane_k(l, ext, lane + 1);
+        bool valid = lane >= 1 && pk > l && pk < h && (lane == 31 || pk < pk1);
+        float cost = kInf;
+        uint32_t nb = below + on, na = above + on;
+        if (valid) {
+            float4 bb = bhi, ba = blo;
+            s3(bb, a, pk);
+            s3(ba, a, pk);
+            float sb = surf(blo, bb), sa = surf(ba, bhi);
+            cost = __fadd_rn(ct, __fmul_rn(ci, __fdiv_rn(__fadd_rn(__fmul_rn(sb, (float)nb), __fmul_rn(sa, (float)na)), A)));
+            if (!(cost < kInf)) cost = kInf;  // NaN / inf never win
+        }
+        // argmin with ties to the lower plane index
+        float mc = cost;
+        uint32_t mk = lane;
+        for (int off = 16; off; off >>= 1) {
+            float oc = __shfl_xor_sync(0xffffffffu, mc, off);
+            uint32_t ok = __shfl_xor_sync(0xffffffffu, mk, off);
+            if (oc < mc || (oc == mc && ok < mk)) {
+                mc = oc;
+                mk = ok;
+            }
+        }
+        if (mc < best.cost) {
+            best.cost = mc;
+            best.axis = (int)a;
+            best.plane = __shfl_sync(0xffffffffu, pk, mk);
+            best.nb = __shfl_sync(0xffffffffu, nb, mk);
+            best.na = __shfl_sync(0xffffffffu, na, mk);
+        }
+    }
+    if (best.axis >= 0 && !(best.cost < __fmul_rn(ci, (float)cnt))) best.axis = -1;
+    return best;
+}
+
+// ---------------------------------------------------------------------------
+// kernels
+// ---------------------------------------------------------------------------
+struct LevelArgs {
+    const float4 *tb_lo, *tb_hi;
+    const float4 *n_lo, *n_hi;
+    const uint4 *n_info;
+    float4 *nx_lo, *nx_hi;
+    uint4 *nx_info;
+    int32_t *axis;
+    float *plane;
+    uint2 *cnt;
+    uint4 *plan;
+    const uint4 *plan_tot;
+    uint2 *prep;
+    const uint2 *prep_tot;
+    uint2 *chunks;
+    uint32_t *large_slot;
+    uint32_t *hist;
+    const uint32_t *refs;
+    const uint32_t *ref_node;
+    uint32_t *nx_refs, *nx_ref_node;
+    const uint2 *rscan;
+    uint2 *out_nodes;
+    uint32_t *out_refs;
+    BuildCounters *ctr;
+    uint32_t *err;
+    uint32_t level;
+    float ct, ci;
+    uint32_t max_depth, leaf_size;
+    uint32_t cap_refs, cap_nodes, cap_level, cap_large, cap_chunks;
+};
+
+__global__ void k_tri_bounds(const float4 *__restrict__ V, const uint4 *__restrict__ T, uint32_t nt, float4 *lo,
+                             float4 *hi) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nt) return;
+    uint4 t = T[i];
+    float4 a = V[t.x], b = V[t.y], c = V[t.z];
+    lo[i] = make_float4(mnf(mnf(a.x, b.x), c.x), mnf(mnf(a.y, b.y), c.y), mnf(mnf(a.z, b.z), c.z), 0.0f);
+    hi[i] = make_float4(mxf(mxf(a.x, b.x), c.x), mxf(mxf(a.y, b.y), c.y), mxf(mxf(a.z, b.z), c.z), 0.0f);
+}
+
+__global__ void k_root(LevelArgs A, const float *box, uint32_t nt) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        BuildCounters *c = A.ctr;
+        c->level_nodes = 1;
+        c->level_refs = nt;
+        c->nodes_total = 2;
+        c->leafrefs_total = 0;
+        c->stop = 0;
+        c->depth = 0;
+        c->leaves = 0;
+        c->capacity_hit = 0;
+        c->learned_nodes = 0;
+        c->fallback_nodes = 0;
+        A.nx_lo[0] = make_float4(box[0], box[1], box[2], 0.0f);
+        A.nx_hi[0] = make_float4(box[4], box[5], box[6], 0.0f);
+        A.nx_info[0] = make_uint4(0, nt, 0, 0);
+        A.out_nodes[1] = make_uint2(kLeafTag, 0);
+        A.out_nodes[0] = make_uint2(kLeafTag, 0);
+    }
+}
+
+__global__ void k_iota(uint32_t *refs, uint32_t *ref_node, uint32_t nt) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nt; i += gridDim.x * blockDim.x) {
+        refs[i] = i;
+        ref_node[i] = 0;
+    }
+}
+
+struct LoadPrep {
+    const uint4 *info;
+    const BuildCounters *ctr;
+    uint32_t level, max_depth, leaf_size;
+    __device__ uint32_t count() const { return ctr->level_nodes; }
+    __device__ uint2 operator()(uint32_t s) const {
+        uint32_t cnt = info[s].y;
+        bool dec = cnt > leaf_size && level < max_depth;
+        bool large = dec && cnt > kSmall;
+        return make_uint2(large ? 1u : 0u, large ? (cnt + kChunk - 1) / kChunk : 0u);
+    }
+};
+
+__global__ void k_chunk_fill(LevelArgs A, uint32_t max_depth, uint32_t leaf_size) {
+    const uint32_t n = A.ctr->level_nodes;
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
+        uint32_t cnt = A.n_info[s].y;
+        bool dec = cnt > leaf_size && A.level < max_depth;
+        if (!(dec && cnt > kSmall)) continue;
+        uint2 pr = A.prep[s];
+        uint32_t rank = pr.x, first = pr.y, nch = (cnt + kChunk - 1) / kChunk;
+        if (rank >= A.cap_large || first + nch > A.cap_chunks) {
+            atomicOr(A.err, 2u);
+            continue;
+        }
+        A.large_slot[rank] = s;
+        for (uint32_t k = 0; k < nch; k++) A.chunks[first + k] = make_uint2(s, rank);
+        uint32_t *H = A.hist + (size_t)rank * kHist;
+        for (uint32_t k = 0; k < kHist; k++) H[k] = 0;
+    }
+}
+
+__global__ void __launch_bounds__(256) k_hist_large(LevelArgs A) {
+    __shared__ uint32_t H[kHist];
+    const uint32_t nch = min(A.prep_tot->y, A.cap_chunks);
+    for (uint32_t ch = blockIdx.x; ch < nch; ch += gridDim.x) {
+        uint2 cr = A.chunks[ch];
+        uint32_t s = cr.x;
+        if (s >= A.ctr->level_nodes || cr.y >= A.cap_large) continue;  // uniform per CTA
+        uint4 info = A.n_info[s];
+        uint32_t k = ch - A.prep[s].y;
+        uint32_t r0 = info.x + k * kChunk, r1 = min(info.x + info.y, r0 + kChunk);
+        float4 blo = A.n_lo[s], bhi = A.n_hi[s];
+        for (uint32_t i = threadIdx.x; i < kHist; i += blockDim.x) H[i] = 0;
+        __syncthreads();
+        for (uint32_t r = r0 + threadIdx.x; r < r1; r += blockDim.x) {
+            uint32_t tri = A.refs[r];
+            hist_ref(H, A.tb_lo[tri], A.tb_hi[tri], blo, bhi);
+        }
+        __syncthreads();
+        uint32_t *G = A.hist + (size_t)cr.y * kHist;
+        for (uint32_t i = threadIdx.x; i < kHist; i += blockDim.x)
+            if (H[i]) atomicAdd(&G[i], H[i]);
+        __syncthreads();
+    }
+}
+
+__device__ __forceinline__ void write_decision(const LevelArgs &A, uint32_t s, const Decision &d) {
+    A.axis[s] = d.axis;
+    A.plane[s] = d.plane;
+    A.cnt[s] = make_uint2(d.nb, d.na);
+}
+
+__global__ void __launch_bounds__(256) k_sah_large(LevelArgs A) {
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+    const uint32_t nl = min(A.prep_tot->x, A.cap_large);
+    for (uint32_t r = warp; r < nl; r += nwarps) {
+        uint32_t s = A.large_slot[r];
+        if (s >= A.ctr->level_nodes) continue;
+        uint4 info = A.n_info[s];
+        Decision d = sah_warp(A.hist + (size_t)r * kHist, A.n_lo[s], A.n_hi[s], info.y, A.ct, A.ci);
+        if ((threadIdx.x & 31u) == 0) write_decision(A, s, d);
+    }
+}
+
+__global__ void __launch_bounds__(256) k_small(LevelArgs A) {
+    __shared__ uint32_t HS[8][kHist];
+    const uint32_t wib = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+    uint32_t *H = HS[wib];
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+    const uint32_t n = A.ctr->level_nodes;
+    for (uint32_t s = warp; s < n; s += nwarps) {
+        uint4 info = A.n_info[s];
+        uint32_t cnt = info.y;
+        bool dec = cnt > A.leaf_size && A.level < A.max_depth;
+        if (dec && cnt > kSmall) continue;  // large: k_sah_large
+        if (!dec) {
+            if (lane == 0) write_decision(A, s, Decision{-1, 0.0f, 0, 0, kInf});
+            continue;
+        }
+        for (uint32_t i = lane; i < kHist; i += 32) H[i] = 0;
+        __syncwarp();
+        float4 blo = A.n_lo[s], bhi = A.n_hi[s];
+        for (uint32_t r = info.x + lane; r < info.x + cnt; r += 32) {
+            uint32_t tri = A.refs[r];
+            hist_ref(H, A.tb_lo[tri], A.tb_hi[tri], blo, bhi);
+        }
+        __syncwarp();
+        Decision d = sah_warp(H, blo, bhi, cnt, A.ct, A.ci);
+        if (lane == 0) write_decision(A, s, d);
+        __syncwarp();
+    }
+}
+
+struct LoadPlan {
+    const uint4 *info;
+    const int32_t *axis;
+    const uint2 *cnt;
+    const BuildCounters *ctr;
+    __device__ uint32_t count() const { return ctr->level_nodes; }
+    __device__ uint4 operator()(uint32_t s) const {
+        if (axis[s] < 0) return make_uint4(info[s].y, 0, 0, 0);
+        uint2 c = cnt[s];
+        return make_uint4(0, 1, (c.x > 0) + (c.y > 0), c.x + c.y);
+    }
+};
+
+__global__ void k_guard(LevelArgs A) {
+    if (threadIdx.x || blockIdx.x) return;
+    BuildCounters *c = A.ctr;
+    uint4 t = *A.plan_tot;
+    uint64_t child_refs = t.w, leaf_refs = t.x, splits = t.y;
+    bool over = child_refs > A.cap_refs || (uint64_t)c->leafrefs_total + leaf_refs + child_refs > A.cap_refs ||
+                (uint64_t)c->nodes_total + 2 * splits > A.cap_nodes || t.z > A.cap_level;
+    c->stop = over ? 1u : 0u;
+    if (over) c->capacity_hit = 1;
+}
+
+__global__ void k_emit(LevelArgs A) {
+    const BuildCounters *c = A.ctr;
+    const uint32_t n = c->level_nodes;
+    const bool stop = c->stop != 0;
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
+        uint4 info = A.n_info[s];
+        int ax = stop ? -1 : A.axis[s];
+        uint4 pl = A.plan[s];
+        if (ax < 0) {
+            uint32_t off = c->leafrefs_total + (stop ? info.x : pl.x);
+            A.out_nodes[info.z] = make_uint2((off << 2) | kLeafTag, info.y);
+            if (info.y) atomicAdd(&A.ctr->leaves, 1u);
+            continue;
+        }
+        uint32_t pair = c->nodes_total + 2 * pl.y;
+        float p = A.plane[s];
+        uint2 ct = A.cnt[s];
+        A.out_nodes[info.z] = make_uint2((pair << 2) | (uint32_t)ax, __float_as_uint(p));
+        uint32_t ns = pl.z, co = pl.w;
+        float4 lo = A.n_lo[s], hi = A.n_hi[s];
+        if (ct.x) {
+            float4 h2 = hi;
+            s3(h2, ax, p);
+            A.nx_lo[ns] = lo;
+            A.nx_hi[ns] = h2;
+            A.nx_info[ns] = make_uint4(co, ct.x, pair, 0);
+            ns++;
+        } else {
+            A.out_nodes[pair] = make_uint2(kLeafTag, 0);
+        }
+        if (ct.y) {
+            float4 l2 = lo;
+            s3(l2, ax, p);
+            A.nx_lo[ns] = l2;
+            A.nx_hi[ns] = hi;
+            A.nx_info[ns] = make_uint4(co + ct.x, ct.y, pair + 1, 0);
+        } else {
+            A.out_nodes[pair + 1] = make_uint2(kLeafTag, 0);
+        }
+    }
+}
+
+__device__ __forceinline__ uint2 ref_flags(const LevelArgs &A, uint32_t r, uint32_t s, int ax) {
+    uint32_t tri = A.refs[r];
+    float l = c3(A.n_lo[s], ax), h = c3(A.n_hi[s], ax), p = A.plane[s];
+    float lo = mxf(c3(A.tb_lo[tri], ax), l), hi = mnf(c3(A.tb_hi[tri], ax), h);
+    bool flat_on = (lo == hi) && lo == p;
+    return make_uint2((lo < p || flat_on) ? 1u : 0u, (hi > p || flat_on) ? 1u : 0u);
+}
+
+struct LoadRefFlags {
+    LevelArgs A;
+    __device__ uint32_t count() const { return A.ctr->level_refs; }
+    __device__ uint2 operator()(uint32_t r) const {
+        if (A.ctr->stop) return make_uint2(0, 0);
+        uint32_t s = A.ref_node[r];
+        int ax = A.axis[s];
+        if (ax < 0) return make_uint2(0, 0);
+        return ref_flags(A, r, s, ax);
+    }
+};
+
+__global__ void k_scatter(LevelArgs A) {
+    const BuildCounters *c = A.ctr;
+    const uint32_t n = c->level_refs;
+    const bool stop = c->stop != 0;
+    for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+        uint32_t s = A.ref_node[r];
+        uint4 info = A.n_info[s];
+        int ax = stop ? -1 : A.axis[s];
+        uint32_t tri = A.refs[r];
+        if (ax < 0) {
+            uint32_t off = c->leafrefs_total + (stop ? info.x : A.plan[s].x) + (r - info.x);
+            if (off < A.cap_refs) A.out_refs[off] = tri;
+            else atomicOr(A.err, 2u);
+            continue;
+        }
+        uint2 f = ref_flags(A, r, s, ax);
+        uint2 base = A.rscan[info.x], mine = A.rscan[r];
+        uint4 pl = A.plan[s];
+        uint2 ct = A.cnt[s];
+        if (f.x) {
+            uint32_t pos = pl.w + (mine.x - base.x);
+            if (pos < A.cap_refs && pos < pl.w + ct.x) {
+                A.nx_refs[pos] = tri;
+                A.nx_ref_node[pos] = pl.z;
+            } else {
+                atomicOr(A.err, 2u);
+            }
+        }
+        if (f.y) {
+            uint32_t pos = pl.w + ct.x + (mine.y - base.y);
+            if (pos < A.cap_refs && pos < pl.w + ct.x + ct.y) {
+                A.nx_refs[pos] = tri;
+                A.nx_ref_node[pos] = pl.z + (ct.x ? 1u : 0u);
+            } else {
+                atomicOr(A.err, 2u);
+            }
+        }
+    }
+}
+
+__global__ void k_advance(LevelArgs A) {
+    if (threadIdx.x || blockIdx.x) return;
+    BuildCounters *c = A.ctr;
+    uint4 t = *A.plan_tot;
+    if (c->level_nodes == 0) return;
+    if (c->stop) {
+        c->leafrefs_total += c->level_refs;
+        c->level_nodes = 0;
+        c->level_refs = 0;
+        c->stop = 0;
+        return;
+    }
+    c->leafrefs_total += t.x;
+    c->nodes_total += 2 * t.y;
+    c->level_nodes = t.z;
+    c->level_refs = t.w;
+    if (t.z) c->depth = A.level + 1;
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+template <class T>
+static cudaError_t dalloc(T *&p, size_t n) {
+    if (p) cudaFree(p);
+    p = nullptr;
+    return cudaMalloc((void **)&p, std::max<size_t>(n, 1) * sizeof(T));
+}
+
+void build_release(BuildState &S) {
+    auto f = [](void *p) {
+        if (p) cudaFree(p);
+    };
+    f(S.tb_lo); f(S.tb_hi);
+    for (int k = 0; k < 2; k++) {
+        f(S.n_lo[k]); f(S.n_hi[k]); f(S.n_info[k]); f(S.refs[k]); f(S.ref_node[k]);
+        S.n_lo[k] = S.n_hi[k] = nullptr; S.n_info[k] = nullptr; S.refs[k] = S.ref_node[k] = nullptr;
+    }
+    f(S.d_axis); f(S.d_plane); f(S.d_cnt); f(S.plan); f(S.plan_tot); f(S.prep); f(S.prep_tot);
+    f(S.chunks); f(S.hist); f(S.rscan); f(S.rscan_tot); f(S.scan_partials); f(S.ctr); f(S.err);
+    f(S.out_nodes); f(S.out_refs);
+    S.tb_lo = S.tb_hi = nullptr;
+    S.d_axis = nullptr; S.d_plane = nullptr; S.d_cnt = nullptr; S.plan = nullptr; S.plan_tot = nullptr;
+    S.prep = nullptr; S.prep_tot = nullptr; S.chunks = nullptr; S.hist = nullptr; S.rscan = nullptr;
+    S.rscan_tot = nullptr; S.scan_partials = nullptr; S.ctr = nullptr; S.err = nullptr;
+    S.out_nodes = nullptr; S.out_refs = nullptr;
+    S.nt = S.cap_refs = S.cap_nodes = S.cap_level = 0;
+    S.active = false;
+}
+
+hk_status build_prepare(BuildState &S, const BuildParams &p, uint32_t nt, int sm_count) {
+    // leaf starts and child-pair indices are stored shifted left by 2 bits
+    const uint64_t kMaxIndex = (1ull << 30) - 64;
+    if ((uint64_t)nt > kMaxIndex / 16) return HK_E_CAPACITY;
+    uint32_t cap_refs = (uint32_t)std::min<uint64_t>(std::max<uint64_t>(p.max_refs, nt), kMaxIndex);
+    uint32_t cap_nodes = (uint32_t)std::min<uint64_t>(std::max<uint64_t>(12ull * nt, 1024ull), kMaxIndex);
+    S.p = p;
+    S.sm_count = sm_count;
+    if (S.ctr && S.nt == nt && S.cap_refs == cap_refs && S.cap_nodes == cap_nodes) return HK_OK;
+    build_release(S);
+    S.nt = nt;
+    S.cap_refs = cap_refs;
+    S.cap_nodes = cap_nodes;
+    S.cap_level = std::min(cap_refs, cap_nodes) + 1;
+    S.cap_large = cap_refs / kSmall + 2;
+    S.cap_chunks = cap_refs / kChunk + S.cap_large + 2;
+    uint32_t tiles = (std::max(cap_refs, S.cap_level) + kTile - 1) / kTile + 1;
+    S.cap_partials = tiles;
+    bool bad = false;
+    bad |= dalloc(S.tb_lo, nt) != cudaSuccess;
+    bad |= dalloc(S.tb_hi, nt) != cudaSuccess;
+    for (int k = 0; k < 2; k++) {
+        bad |= dalloc(S.n_lo[k], S.cap_level) != cudaSuccess;
+        bad |= dalloc(S.n_hi[k], S.cap_level) != cudaSuccess;
+        bad |= dalloc(S.n_info[k], S.cap_level) != cudaSuccess;
+        bad |= dalloc(S.refs[k], cap_refs) != cudaSuccess;
+        bad |= dalloc(S.ref_node[k], cap_refs) != cudaSuccess;
+    }
+    bad |= dalloc(S.d_axis, S.cap_level) != cudaSuccess;
+    bad |= dalloc(S.d_plane, S.cap_level) != cudaSuccess;
+    bad |= dalloc(S.d_cnt, S.cap_level) != cudaSuccess;
+    bad |= dalloc(S.plan, S.cap_level) != cudaSuccess;
+    bad |= dalloc(S.plan_tot, 1) != cudaSuccess;
+    bad |= dalloc(S.prep, S.cap_level) != cudaSuccess;
+    bad |= dalloc(S.prep_tot, 1) != cudaSuccess;
+    bad |= dalloc(S.chunks, S.cap_chunks + S.cap_large) != cudaSuccess;  // tail holds large_slot
+    bad |= dalloc(S.hist, (size_t)S.cap_large * kHist) != cudaSuccess;
+    bad |= dalloc(S.rscan, cap_refs) != cudaSuccess;
+    bad |= dalloc(S.rscan_tot, 1) != cudaSuccess;
+    {
+        uint4 *pp = nullptr;
+        bad |= dalloc(pp, tiles) != cudaSuccess;
+        S.scan_partials = pp;
+    }
+    bad |= dalloc(S.ctr, 1) != cudaSuccess;
+    bad |= dalloc(S.err, 1) != cudaSuccess;
+    bad |= dalloc(S.out_nodes, cap_nodes) != cudaSuccess;
+    bad |= dalloc(S.out_refs, cap_refs) != cudaSuccess;
+    if (bad) {
+        build_release(S);
+        return HK_E_ALLOC;
+    }
+    cudaMemset(S.err, 0, 4);
+    cudaMemset(S.ctr, 0, sizeof(BuildCounters));
+    return HK_OK;
+}
+
+hk_status build_ensure_outputs(BuildState &S, BuildOutputs *o) {
+    if (!S.out_nodes || !S.out_refs) return HK_E_ALLOC;
+    if (o) {
+        o->nodes = S.out_nodes;
+        o->refs = S.out_refs;
+    }
+    return HK_OK;
+}
+
+cudaError_t build_launch(BuildState &S, const float4 *verts, const uint4 *tris, uint32_t nt, const float *box,
+                         cudaStream_t st) {
+    const int G = S.sm_count * 4;
+    LevelArgs A;
+    memset(&A, 0, sizeof(A));
+    A.tb_lo = S.tb_lo;
+    A.tb_hi = S.tb_hi;
+    A.axis = S.d_axis;
+    A.plane = S.d_plane;
+    A.cnt = S.d_cnt;
+    A.plan = S.plan;
+    A.plan_tot = S.plan_tot;
+    A.prep = S.prep;
+    A.prep_tot = S.prep_tot;
+    A.chunks = S.chunks;
+    A.large_slot = reinterpret_cast<uint32_t *>(S.chunks + S.cap_chunks);
+    A.hist = S.hist;
+    A.rscan = S.rscan;
+    A.out_nodes = S.out_nodes;
+    A.out_refs = S.out_refs;
+    A.ctr = S.ctr;
+    A.err = S.err;
+    A.ct = S.p.ct;
+    A.ci = S.p.ci;
+    A.max_depth = S.p.max_depth;
+    A.leaf_size = S.p.leaf_size;
+    A.cap_refs = S.cap_refs;
+    A.cap_nodes = S.cap_nodes;
+    A.cap_level = S.cap_level;
+    A.cap_large = S.cap_large;
+    A.cap_chunks = S.cap_chunks;
+    if (nt) k_tri_bounds<<<(nt + 255) / 256, 256, 0, st>>>(verts, tris, nt, S.tb_lo, S.tb_hi);
+    // level 0 lives in slot buffers [0]
+    A.nx_lo = S.n_lo[0];
+    A.nx_hi = S.n_hi[0];
+    A.nx_info = S.n_info[0];
+    k_root<<<1, 32, 0, st>>>(A, box, nt);
+    k_iota<<<G, 256, 0, st>>>(S.refs[0], S.ref_node[0], nt);
+    for (uint32_t L = 0; L <= S.p.max_depth; L++) {
+        int cur = L & 1, nxt = cur ^ 1;
+        A.level = L;
+        A.n_lo = S.n_lo[cur];
+        A.n_hi = S.n_hi[cur];
+        A.n_info = S.n_info[cur];
+        A.nx_lo = S.n_lo[nxt];
+        A.nx_hi = S.n_hi[nxt];
+        A.nx_info = S.n_info[nxt];
+        A.refs = S.refs[cur];
+        A.ref_node = S.ref_node[cur];
+        A.nx_refs = S.refs[nxt];
+        A.nx_ref_node = S.ref_node[nxt];
+        LoadPrep lp{A.n_info, S.ctr, L, S.p.max_depth, S.p.leaf_size};
+        scan<uint2>(lp, reinterpret_cast<uint2 *>(S.scan_partials), S.prep, S.prep_tot, G, st);
+        k_chunk_fill<<<G, 256, 0, st>>>(A, S.p.max_depth, S.p.leaf_size);
+        k_hist_large<<<G, 256, 0, st>>>(A);
+        k_sah_large<<<G, 256, 0, st>>>(A);
+        k_small<<<G * 2, 256, 0, st>>>(A);
+        LoadPlan lpl{A.n_info, S.d_axis, S.d_cnt, S.ctr};
+        scan<uint4>(lpl, reinterpret_cast<uint4 *>(S.scan_partials), S.plan, S.plan_tot, G, st);
+        k_guard<<<1, 32, 0, st>>>(A);
+        k_emit<<<G, 256, 0, st>>>(A);
+        LoadRefFlags lr{A};
+        scan<uint2>(lr, reinterpret_cast<uint2 *>(S.scan_partials), S.rscan, S.rscan_tot, G, st);
+        k_scatter<<<G, 256, 0, st>>>(A);
+        k_advance<<<1, 32, 0, st>>>(A);
+    }
+    S.active = true;
+    return cudaGetLastError();
+}
+
+hk_status build_read_stats(BuildState &S, cudaStream_t st, hk_tree_stats *out) {
+    BuildCounters c;
+    uint32_t err = 0;
+    if (cudaMemcpyAsync(&c, S.ctr, sizeof(c), cudaMemcpyDeviceToHost, st) != cudaSuccess) return HK_E_CUDA;
+    if (cudaMemcpyAsync(&err, S.err, 4, cudaMemcpyDeviceToHost, st) != cudaSuccess) return HK_E_CUDA;
+    if (cudaStreamSynchronize(st) != cudaSuccess) return HK_E_CUDA;
+    if (err) {
+        cudaMemsetAsync(S.err, 0, 4, st);
+        return HK_E_CAPACITY;
+    }
+    out->nodes = c.nodes_total;
+    out->refs = c.leafrefs_total;
+    out->leaves = c.leaves;
+    out->depth = c.depth;
+    out->capacity_hit = c.capacity_hit;
+    out->learned_nodes = c.learned_nodes;
+    out->fallback_nodes = c.fallback_nodes;
+    return HK_OK;
+}
+
+}  // namespace hk

@@ -1,0 +1,87 @@
+// hk_build.h -- GPU KD-tree builder state (binned SAH and the learned
+// split proposer). Every launch reads its work size from device memory, so a
+// whole build is a fixed sequence of kernels that a CUDA graph can capture.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/hulkcuda.h"
+
+namespace hk {
+
+struct BuildParams {
+    float ct = 1.0f, ci = 1.5f;
+    uint32_t max_depth = 24;
+    uint32_t leaf_size = 4;
+    uint32_t max_refs = 0;      // reference arena (also the leaf list) capacity
+    int mode = 0;               // hk_build_mode
+    uint32_t topk = 4;
+    float fallback_ratio = 1.02f;
+};
+
+// device scalars of one build (one struct in device memory)
+struct BuildCounters {
+    uint32_t level_nodes;       // active nodes of the current level
+    uint32_t level_refs;        // their references
+    uint32_t nodes_total;       // compact nodes written so far
+    uint32_t leafrefs_total;    // leaf references written so far
+    uint32_t stop;              // current level stops splitting (capacity)
+    uint32_t depth;             // deepest level reached
+    uint32_t leaves;            // leaves written (empty cells excluded)
+    uint32_t capacity_hit;
+    uint32_t n_large;           // large nodes of the level
+    uint32_t n_chunks;          // histogram chunks of the level
+    uint32_t learned_nodes;
+    uint32_t fallback_nodes;
+    uint32_t pad[4];
+};
+
+struct BuildOutputs {
+    uint2 *nodes;
+    uint32_t *refs;
+};
+
+struct BuildState {
+    BuildParams p{};
+    uint32_t nt = 0, cap_refs = 0, cap_nodes = 0, cap_level = 0, cap_large = 0, cap_chunks = 0;
+    int sm_count = 148;
+    bool active = false;        // a built tree is the current tree
+    // per-triangle bounds
+    float4 *tb_lo = nullptr, *tb_hi = nullptr;
+    // level nodes (ping-pong)
+    float4 *n_lo[2] = {nullptr, nullptr}, *n_hi[2] = {nullptr, nullptr};
+    uint4 *n_info[2] = {nullptr, nullptr};      // start, count, cidx, -
+    // decision per node
+    int32_t *d_axis = nullptr;
+    float *d_plane = nullptr;
+    uint2 *d_cnt = nullptr;                      // below, above
+    uint4 *plan = nullptr;                       // scan of (leafrefs, pairs, nextnodes, childrefs)
+    uint4 *plan_tot = nullptr;
+    uint2 *prep = nullptr;                       // scan of (is_large, chunks)
+    uint2 *prep_tot = nullptr;
+    uint2 *chunks = nullptr;                     // (slot, large rank)
+    uint32_t *hist = nullptr;                    // per large node 3 x 96
+    // references (ping-pong)
+    uint32_t *refs[2] = {nullptr, nullptr};
+    uint32_t *ref_node[2] = {nullptr, nullptr};
+    uint2 *rscan = nullptr;                      // exclusive scan of (below, above) flags
+    uint2 *rscan_tot = nullptr;
+    void *scan_partials = nullptr;               // scan scratch
+    uint32_t cap_partials = 0;
+    BuildCounters *ctr = nullptr;
+    uint32_t *err = nullptr;
+    // output
+    uint2 *out_nodes = nullptr;
+    uint32_t *out_refs = nullptr;
+    // learned proposer (hk_mlp.cu)
+    void *mlp = nullptr;
+};
+
+hk_status build_prepare(BuildState &S, const BuildParams &p, uint32_t nt, int sm_count);
+hk_status build_ensure_outputs(BuildState &S, BuildOutputs *o);
+cudaError_t build_launch(BuildState &S, const float4 *verts, const uint4 *tris, uint32_t nt, const float *box,
+                         cudaStream_t s);
+hk_status build_read_stats(BuildState &S, cudaStream_t s, hk_tree_stats *st);
+void build_release(BuildState &S);
+
+}  // namespace hk

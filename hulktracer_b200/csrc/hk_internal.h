@@ -1,0 +1,59 @@
+// hk_internal.h -- launch descriptors shared between the host API and the
+// kernel translation units.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/hulkcuda.h"
+
+namespace hk {
+
+struct TriRec;
+
+struct TraceLaunch {
+    const uint2 *nodes;
+    const uint32_t *refs;
+    const TriRec *tris;
+    const float4 *rays;
+    hk_hit *hits;
+    uint32_t n;                 // ray count (ignored when n_dev != nullptr)
+    const uint32_t *n_dev;      // device-side ray count, or nullptr
+    uint32_t ntris;
+    const float *box;           // device pointer, 8 floats
+    uint32_t *fetch;            // ray-batch counter
+    unsigned long long *counters;
+    uint32_t *err;
+    uint32_t stack_depth;
+    uint32_t max_steps;
+    int variant;
+    bool count;
+    int grid, block;
+    // ropes
+    const uint32_t *ropes;      // 6 per node
+    const float4 *cbox;         // 2 per node (min, max)
+};
+
+cudaError_t launch_trace(const TraceLaunch &L, cudaStream_t s);
+
+// hk_shade.cu
+cudaError_t launch_precompute(const float4 *verts, const uint4 *tris, uint32_t nt, TriRec *out,
+                              cudaStream_t s);
+cudaError_t launch_cache_to_rec(const float *cache16, const float4 *verts, const uint4 *tris, uint32_t nt,
+                                TriRec *out, cudaStream_t s);
+cudaError_t launch_rec_to_cache(const TriRec *rec, uint32_t nt, float *cache16, cudaStream_t s);
+cudaError_t launch_transform(const float4 *rest, const uint32_t *part, uint32_t nv, const float *mats12,
+                             float4 *out, uint32_t *box_ord, cudaStream_t s);
+cudaError_t launch_box_finish(const uint32_t *box_ord, float *box, cudaStream_t s);
+cudaError_t launch_box(const float4 *verts, uint32_t nv, uint32_t *box_ord, float *box, cudaStream_t s);
+cudaError_t launch_camera_rays(const float *cam16_dev, uint32_t w, uint32_t h, float4 *rays, cudaStream_t s);
+cudaError_t launch_shadow_rays(const float4 *rays, const hk_hit *hits, const TriRec *tris, uint32_t npix,
+                               const float *lights_dev, uint32_t nl, float4 *srays, uint32_t *slot,
+                               uint32_t *spix, uint32_t *scount, cudaStream_t s);
+cudaError_t launch_shade_cpu(const float4 *rays, const hk_hit *hits, const TriRec *tris, uint32_t npix,
+                             const float *lights_dev, uint32_t nl, const uint32_t *slot, const hk_hit *shits,
+                             uint32_t *rgba, cudaStream_t s);
+cudaError_t launch_hit4(const hk_hit *hits, const TriRec *tris, uint32_t n, float4 *hit4, cudaStream_t s);
+cudaError_t launch_shade_picture(const float4 *rays, const float4 *hit4, uint32_t n, const float *lights_dev,
+                                 uint32_t nl, uint32_t *rgba, cudaStream_t s);
+
+}  // namespace hk

@@ -1,0 +1,253 @@
+"""Host-side mirror of HulkEngine's KD-tree and GPU-visitor surface over the C ABI.
+
+* :class:`Context` -- one ``hk_ctx`` (device arena + stream), numpy in/out.
+* :class:`KDTreeCUDA` -- the ``KDTreeCPU`` interface (HulkEngine/src/KDTreeCPU.hpp:
+  53-72): ``buildKDTree``, ``checkCollision`` (batched), ``getNodeArray``,
+  ``getPolygonArray``; the GPU builder fills the empty ``KDTreeGPU`` slot
+  (HulkEngine/src/KDTreeGPU.hpp:12-22).
+* :class:`TraceCUDA` -- a headless ``GLVisitorGPUTrace`` (HulkEngine/src/
+  GLVisitorGPUTrace.hpp:26-72): ``initializeVisitor``, ``buildTree``,
+  ``traceScene`` returning the framebuffer instead of a GL texture.
+
+Every call goes to ``libhulkcuda.so``; failures raise :class:`HkError`.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._lib import HkError, ptr
+
+EHulkResult_ok = 0
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def _u32(a):
+    return np.ascontiguousarray(a, dtype=np.uint32)
+
+
+class Context:
+    def __init__(self, device: int = 0, **cfg):
+        self.L = _lib.load()
+        c = _lib.Config()
+        self._check(self.L.hk_config_default(C.byref(c)))
+        for k, v in cfg.items():
+            if not hasattr(c, k):
+                raise KeyError(k)
+            setattr(c, k, v)
+        c.device = device
+        self.cfg = c
+        h = C.c_void_p()
+        st = self.L.hk_create(C.byref(h), C.byref(c))
+        if st != 0:
+            raise HkError(st, "hk_create failed")
+        self.h = h
+        self.ntris = 0
+        self.nverts = 0
+
+    def _check(self, st):
+        if st != 0:
+            msg = self.L.hk_last_error(self.h).decode() if getattr(self, "h", None) else ""
+            raise HkError(st, msg)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.hk_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- scene --
+    def upload(self, verts, tris):
+        v, t = _f32(verts), _u32(tris)
+        self._check(self.L.hk_scene_upload(self.h, ptr(v), v.shape[0], ptr(t), t.shape[0]))
+        self.ntris, self.nverts = t.shape[0], v.shape[0]
+
+    def set_box(self, box):
+        self._check(self.L.hk_scene_set_box(self.h, ptr(_f32(box))))
+
+    def get_box(self):
+        b = np.zeros(8, np.float32)
+        self._check(self.L.hk_scene_get_box(self.h, ptr(b)))
+        return b
+
+    def set_parts(self, part_of_vertex, nparts):
+        self._part = _u32(part_of_vertex)
+        self._check(self.L.hk_scene_set_parts(self.h, ptr(self._part), int(nparts)))
+
+    def transform(self, mats12):
+        self._check(self.L.hk_scene_transform(self.h, ptr(_f32(mats12))))
+
+    def get_vertices(self):
+        v = np.zeros((self.nverts, 4), np.float32)
+        self._check(self.L.hk_scene_get_vertices(self.h, ptr(v)))
+        return v
+
+    # -- cache --
+    def precompute(self):
+        self._check(self.L.hk_precompute(self.h))
+
+    def import_cache(self, cache16):
+        c = _f32(cache16)
+        self._check(self.L.hk_cache_import(self.h, ptr(c), c.shape[0]))
+
+    def export_cache(self):
+        c = np.zeros((self.ntris, 16), np.float32)
+        self._check(self.L.hk_cache_export(self.h, ptr(c)))
+        return c
+
+    # -- tree --
+    def build(self, mode=_lib.BUILD_BINNED):
+        st = _lib.TreeStats()
+        self._check(self.L.hk_build(self.h, int(mode), C.byref(st)))
+        return st.as_dict()
+
+    def import_tree(self, nodes, refs):
+        n, r = _u32(nodes).reshape(-1, 4), _u32(refs)
+        self._check(self.L.hk_tree_import(self.h, ptr(n), n.shape[0], ptr(r), r.shape[0]))
+
+    def export_tree(self):
+        nn, nr = C.c_uint32(), C.c_uint32()
+        self._check(self.L.hk_tree_export(self.h, None, 0, None, 0, C.byref(nn), C.byref(nr)))
+        nodes = np.zeros((nn.value, 4), np.uint32)
+        refs = np.zeros(max(nr.value, 1), np.uint32)
+        self._check(self.L.hk_tree_export(self.h, ptr(nodes), nn.value, ptr(refs), nr.value, C.byref(nn),
+                                          C.byref(nr)))
+        return nodes, refs[:nr.value]
+
+    def export_compact(self):
+        nn, nr = C.c_uint32(), C.c_uint32()
+        self._check(self.L.hk_tree_export_compact(self.h, None, 0, None, 0, C.byref(nn), C.byref(nr)))
+        nodes = np.zeros((nn.value, 2), np.uint32)
+        refs = np.zeros(max(nr.value, 1), np.uint32)
+        self._check(self.L.hk_tree_export_compact(self.h, ptr(nodes), nn.value, ptr(refs), nr.value,
+                                                  C.byref(nn), C.byref(nr)))
+        return nodes, refs[:nr.value]
+
+    def stats(self):
+        st = _lib.TreeStats()
+        self._check(self.L.hk_tree_stats_get(self.h, C.byref(st)))
+        return st.as_dict()
+
+    # -- trace --
+    def trace(self, rays, variant=_lib.SHORTSTACK):
+        r = _f32(rays).reshape(-1, 8)
+        hits = np.zeros(r.shape[0], _lib.HIT_DTYPE)
+        self._check(self.L.hk_trace(self.h, ptr(r), r.shape[0], int(variant), ptr(hits)))
+        return hits
+
+    def trace_device(self, d_rays: int, n: int, d_hits: int, variant=_lib.SHORTSTACK):
+        self._check(self.L.hk_trace_device(self.h, C.c_void_p(d_rays), n, int(variant), C.c_void_p(d_hits)))
+
+    def set_counting(self, on=True):
+        self._check(self.L.hk_set_counting(self.h, 1 if on else 0))
+
+    def counters(self):
+        c = np.zeros(3, np.uint64)
+        self._check(self.L.hk_get_counters(self.h, ptr(c)))
+        return c
+
+    def synchronize(self):
+        self._check(self.L.hk_synchronize(self.h))
+
+    def set_stream(self, stream_ptr: int | None):
+        self._check(self.L.hk_set_stream(self.h, C.c_void_p(stream_ptr) if stream_ptr else None))
+
+    def camera_rays(self, cam, w, h):
+        out = np.zeros((w * h, 8), np.float32)
+        self._check(self.L.hk_camera_rays(self.h, ptr(_f32(cam).ravel()), w, h, ptr(out)))
+        return out
+
+    def render(self, cam, lights, w, h, variant=_lib.SHORTSTACK, shade=_lib.SHADE_CPU):
+        lights = _f32(lights).reshape(-1, 8)
+        out = np.zeros(w * h, np.uint32)
+        self._check(self.L.hk_render(self.h, ptr(_f32(cam).ravel()), ptr(lights), lights.shape[0], w, h,
+                                     int(variant), int(shade), ptr(out)))
+        return out
+
+    def render_device(self, cam, lights, w, h, d_rgba: int, variant=_lib.SHORTSTACK, shade=_lib.SHADE_CPU):
+        lights = _f32(lights).reshape(-1, 8)
+        self._check(self.L.hk_render_device(self.h, ptr(_f32(cam).ravel()), ptr(lights), lights.shape[0], w, h,
+                                            int(variant), int(shade), C.c_void_p(d_rgba)))
+
+    def shade_picture(self, rays, hit4, lights):
+        r = _f32(rays).reshape(-1, 8)
+        lights = _f32(lights).reshape(-1, 8)
+        out = np.zeros(r.shape[0], np.uint32)
+        self._check(self.L.hk_shade_picture(self.h, ptr(r), ptr(_f32(hit4)), r.shape[0], ptr(lights),
+                                            lights.shape[0], ptr(out)))
+        return out
+
+    def frame(self, mats12, cam, lights, w, h, d_rgba: int, mode=_lib.BUILD_BINNED, variant=_lib.SHORTSTACK,
+              use_graph=True, want_stats=False):
+        lights = _f32(lights).reshape(-1, 8)
+        m = None if mats12 is None else _f32(mats12)
+        st = _lib.TreeStats() if want_stats else None
+        self._check(self.L.hk_frame(self.h, ptr(m), ptr(_f32(cam).ravel()), ptr(lights), lights.shape[0], w, h,
+                                    int(mode), int(variant), 1 if use_graph else 0, C.c_void_p(d_rgba),
+                                    C.byref(st) if st is not None else None))
+        return st.as_dict() if st is not None else None
+
+
+class KDTreeCUDA:
+    """``KDTreeCPU``'s interface on the GPU (HulkEngine/src/KDTreeCPU.hpp:53-72)."""
+
+    def __init__(self, ctx: Context | None = None, mode=_lib.BUILD_BINNED):
+        self.ctx = ctx or Context()
+        self.mode = mode
+        self.scene = None
+
+    def buildKDTree(self, scene) -> int:
+        """Upload the scene arrays, compute the triangle cache and build
+        (KDTreeCPU::buildKDTree, KDTreeCPU.cpp:61-94). Returns e_ok."""
+        self.scene = scene
+        self.ctx.upload(scene.verts, scene.tris)
+        self.ctx.precompute()
+        self.last_stats = self.ctx.build(self.mode)
+        return EHulkResult_ok
+
+    def checkCollision(self, rays, variant=_lib.SHORTSTACK):
+        """Batched KDTreeCPU::checkCollision (KDTreeCPU.cpp:230-253): per ray the
+        closest hit time (inf on a miss) and triangle index (-1 on a miss)."""
+        return self.ctx.trace(rays, variant)
+
+    def getNodeArray(self):
+        return self.ctx.export_tree()[0]
+
+    def getPolygonArray(self):
+        return self.ctx.export_tree()[1]
+
+
+class TraceCUDA:
+    """Headless GLVisitorGPUTrace: build the tree, trace primary + shadow rays
+    and shade into a framebuffer (HulkEngine/src/GLVisitorGPUTrace.cpp:256-410)."""
+
+    def __init__(self, ctx: Context | None = None, variant=_lib.SHORTSTACK, mode=_lib.BUILD_BINNED):
+        self.ctx = ctx or Context()
+        self.variant = variant
+        self.mode = mode
+        self.scene = None
+
+    def initializeVisitor(self, scene):
+        self.scene = scene
+        self.ctx.upload(scene.verts, scene.tris)
+        if scene.part_of_vertex is not None:
+            self.ctx.set_parts(scene.part_of_vertex, scene.part_center.shape[0])
+
+    def buildTree(self):
+        self.ctx.precompute()
+        return self.ctx.build(self.mode)
+
+    def traceScene(self, shade=_lib.SHADE_CPU):
+        sc = self.scene
+        img = self.ctx.render(sc.camera, sc.lights, sc.width, sc.height, self.variant, shade)
+        return img.reshape(sc.height, sc.width)

@@ -1,0 +1,214 @@
+/*
+ * hulkcuda.h -- C ABI of the B200 (sm_100a) ray-tracing hot path.
+ *
+ * Drop-in boundary for HulkEngine's OpenCL render path: the calls below take
+ * the place of KDTreeCPU's build / collision API and of GLVisitorGPUTrace's
+ * per-frame OpenCL driver. Plain pointers and sizes only; host arrays are
+ * copied at call time; the context owns all device memory.
+ *
+ * Layouts are the reference's (HulkEngine/public/SharedStructs.hpp):
+ *   vertex    float[4], w = 1                       (Scene::m_vertices)
+ *   triangle  uint32[4] (3 indices + padding)       (TriangleIndices, :37-41)
+ *   KD node   uint32[4] (KDTreeNode, :113-137)      flags | {above, below, plane}
+ *                                                   or {start, count, leafID}
+ *   cache     float[16] (PolyToRayCache, :80-90)    normal4, e0_4, e1_4,
+ *                                                   e00, e01, e11, det
+ *   ray       float[8]  (Ray, :71-76)               origin4, dir4, w = 0
+ *   camera    float[16] (CameraPos, :99-105)        from, vertical, horizontal,
+ *                                                   lowerLeft
+ *   light     float[8]  (Light, :53-63)             color.xyz + type in .w,
+ *                                                   pos-or-dir
+ *   box       float[8]  (Box, :65-69)               min4, max4
+ *
+ * Every call returns hk_status and never aborts the process.
+ */
+#ifndef HULKCUDA_H
+#define HULKCUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. The first six keep the values of the reference's EHulkResult
+ * (HulkEngine/public/hulk_assert.h:42-50). */
+typedef enum hk_status {
+    HK_OK = 0,
+    HK_E_ALLOC = 1,
+    HK_E_FILE_OPEN = 2,
+    HK_E_FILE_CLOSE = 3,
+    HK_E_ILLEGAL_INPUT = 4,
+    HK_E_NODE_NOT_FOUND = 5,
+    HK_E_CUDA = 16,           /* a CUDA runtime call failed (see hk_last_error) */
+    HK_E_DEVICE_TIMEOUT = 17, /* a bounded device-side wait expired */
+    HK_E_CAPACITY = 18,       /* a fixed-capacity arena is too small */
+    HK_E_BOUNDS = 19,         /* a device-side bound check fired */
+    HK_E_STATE = 20           /* call order violated (e.g. trace before a tree exists) */
+} hk_status;
+
+/* Traversal variants. FULLSTACK follows KDTreeCPU::searchKDTree
+ * (HulkEngine/src/KDTreeCPU.cpp:285-361, GPUTrace.cl:6-90); SHORTSTACK and
+ * SMEMSTACK the ring stack of KDTreeCPU::searchKDTreeStackless
+ * (KDTreeCPU.cpp:363-447; GPUTrace_shortStack.cl, GPUTrace_LDSshortStack.cl)
+ * with the ring in registers or in shared memory; RESTART is kd-restart as in
+ * GPUTrace_stackless.cl:53-117 with every leaf resident (no early exit);
+ * RESTART_EARLY exits once the closest hit lies before the current segment's
+ * end; ROPES follows leaf ropes (no reference counterpart); BRUTE tests every
+ * triangle (GPUTrace_bruteforce.cl:30-42). */
+typedef enum hk_variant {
+    HK_TRACE_FULLSTACK = 0,
+    HK_TRACE_SHORTSTACK = 1,
+    HK_TRACE_SMEMSTACK = 2,
+    HK_TRACE_RESTART = 3,
+    HK_TRACE_RESTART_EARLY = 4,
+    HK_TRACE_ROPES = 5,
+    HK_TRACE_BRUTE = 6
+} hk_variant;
+
+typedef enum hk_build_mode {
+    HK_BUILD_BINNED = 0,   /* exact binned SAH, every (axis, bin) plane costed */
+    HK_BUILD_LEARNED = 1   /* MLP proposes top-k planes; binned fallback */
+} hk_build_mode;
+
+/* Shading semantics for hk_render */
+enum {
+    HK_SHADE_CPU = 0,          /* GLVisitorCPUTrace::traceScene: shadow rays, misses 0 */
+    HK_SHADE_PICTURE = 1       /* ShadePicture (shadePicture.cl:7-55): no shadow rays */
+};
+
+typedef struct hk_config {
+    int device;               /* CUDA device ordinal */
+    float traverse_cost;      /* Ct (KDTreeCPU.cpp:17) */
+    float intersect_cost;     /* Ci (KDTreeCPU.cpp:18) */
+    uint32_t max_depth;       /* c_maxKDTreeDepth (SharedStructs.hpp:16) */
+    uint32_t leaf_size;       /* a node with <= leaf_size refs becomes a leaf */
+    uint32_t bins;            /* SAH bins per axis (32) */
+    uint32_t short_stack;     /* ring depth of SHORTSTACK / SMEMSTACK (4..16) */
+    uint32_t block_size;      /* trace kernel block size (multiple of 32, <= 1024) */
+    uint32_t blocks_per_sm;   /* persistent trace grid = SMs * blocks_per_sm */
+    uint32_t max_refs;        /* builder reference arena capacity (0 = 16 x tris) */
+    uint32_t topk;            /* learned builder: proposals costed per node */
+    float fallback_ratio;     /* learned builder: fall back to full binned SAH when a
+                                 proposal costs more than ratio x the best exactly
+                                 costed candidate (1.02) */
+} hk_config;
+
+typedef struct hk_tree_stats {
+    uint32_t nodes;           /* compact nodes, including padding/empty cells */
+    uint32_t leaves;
+    uint32_t refs;            /* leaf references */
+    uint32_t depth;
+    float build_ms;           /* device time of the last build */
+    uint32_t capacity_hit;    /* 1 if a level stopped splitting for lack of arena */
+    uint32_t learned_nodes;   /* nodes split by a learned proposal */
+    uint32_t fallback_nodes;  /* nodes that fell back to the full binned search */
+} hk_tree_stats;
+
+/* one hit: t (+inf on a miss) and the triangle index (-1 on a miss) */
+typedef struct hk_hit {
+    float t;
+    int32_t tri;
+} hk_hit;
+
+typedef struct hk_ctx hk_ctx;
+
+/* defaults: Ct 1, Ci 1.5, depth 24, leaf 4, 32 bins, stack 6, block 128 */
+hk_status hk_config_default(hk_config *cfg);
+
+/* Create a context on cfg->device. Replaces GLVisitorGPUTrace::initializeVisitor
+ * (HulkEngine/src/GLVisitorGPUTrace.cpp:94-161) minus the GL interop. */
+hk_status hk_create(hk_ctx **ctx, const hk_config *cfg);
+hk_status hk_destroy(hk_ctx *ctx);
+const char *hk_last_error(const hk_ctx *ctx);
+/* run subsequent work on this cudaStream_t (NULL = the context's own stream) */
+hk_status hk_set_stream(hk_ctx *ctx, void *cuda_stream);
+hk_status hk_synchronize(hk_ctx *ctx);
+
+/* ---- scene (Scene::m_vertices / m_vertexIndices / m_sceneBox) ---- */
+/* Copy the triangle soup to the device. Vertices must have w == 1 and every
+ * index must be < nv (HK_E_ILLEGAL_INPUT otherwise). The scene box becomes the
+ * vertices' bounds unless hk_scene_set_box overrides it. */
+hk_status hk_scene_upload(hk_ctx *ctx, const float *verts4, uint32_t nv, const uint32_t *tris4,
+                          uint32_t nt);
+hk_status hk_scene_set_box(hk_ctx *ctx, const float *box8);
+hk_status hk_scene_get_box(hk_ctx *ctx, float *box8);
+/* Rigid animation: one part index per vertex; the uploaded vertices are the
+ * rest pose. hk_scene_transform then writes M[part] * (x, y, z, 1) into the
+ * current vertices on the device, recomputes the scene box and the triangle
+ * cache (the per-frame Intersectable::update of HulkEngine/src/
+ * Intersectable.cpp:116-141). mats12: nparts x 3x4 row-major. */
+hk_status hk_scene_set_parts(hk_ctx *ctx, const uint32_t *part_of_vertex, uint32_t nparts);
+hk_status hk_scene_transform(hk_ctx *ctx, const float *mats12);
+hk_status hk_scene_get_vertices(hk_ctx *ctx, float *verts4);
+
+/* ---- per-triangle cache (KDTreeCPU::buildPolygonCache, KDTreeCPU.cpp:479-507;
+ *      build_cache, GPUTrace_buildCache.cl:5-37) ---- */
+/* Compute the cache on the device (normal normalised with IEEE 1/sqrt). */
+hk_status hk_precompute(hk_ctx *ctx);
+/* Use a cache computed elsewhere (e.g. the reference's, whose normals come
+ * from the CPU's rsqrt). Normal / edge w lanes must be 0. */
+hk_status hk_cache_import(hk_ctx *ctx, const float *cache16, uint32_t nt);
+hk_status hk_cache_export(hk_ctx *ctx, float *cache16);
+
+/* ---- KD tree ---- */
+/* KDTreeCPU::buildKDTree (KDTreeCPU.cpp:61-94) on the GPU: exact binned SAH
+ * or the learned split proposer. stats may be NULL. */
+hk_status hk_build(hk_ctx *ctx, hk_build_mode mode, hk_tree_stats *stats);
+/* Import a tree in the reference layout (KDTreeCPU::getNodeArray /
+ * getPolygonArray, KDTreeCPU.hpp:62-72). */
+hk_status hk_tree_import(hk_ctx *ctx, const uint32_t *nodes4, uint32_t nn, const uint32_t *refs,
+                         uint32_t nr);
+/* Export the current tree in the reference layout. With nodes4 == NULL only
+ * the sizes are returned. */
+hk_status hk_tree_export(hk_ctx *ctx, uint32_t *nodes4, uint32_t cap_nodes, uint32_t *refs,
+                         uint32_t cap_refs, uint32_t *nn, uint32_t *nr);
+/* Export the device's compact layout: 2 x uint32 per node (junction:
+ * (pair << 2) | axis, plane bits; leaf: (start << 2) | 3, count). */
+hk_status hk_tree_export_compact(hk_ctx *ctx, uint32_t *cnodes2, uint32_t cap_nodes,
+                                 uint32_t *refs, uint32_t cap_refs, uint32_t *cnn, uint32_t *nr);
+hk_status hk_tree_stats_get(hk_ctx *ctx, hk_tree_stats *stats);
+
+/* ---- tracing (KDTreeCPU::checkCollision, KDTreeCPU.cpp:230-253; gpu_trace,
+ *      GPUTrace_stackless.cl:122-168) ---- */
+/* Host rays in, host hits out (copies included). Ray w lanes must be 0. */
+hk_status hk_trace(hk_ctx *ctx, const float *rays8, uint32_t n, hk_variant variant, hk_hit *hits);
+/* Device pointers (rays8: n x 8 floats, hits: n x hk_hit), stream-ordered on
+ * the context's stream; no host synchronisation. */
+hk_status hk_trace_device(hk_ctx *ctx, const float *d_rays8, uint32_t n, hk_variant variant,
+                          hk_hit *d_hits);
+/* Per-ray counters (node visits, refs read, triangle tests) of the last
+ * hk_trace / hk_trace_device call when counting is enabled. */
+hk_status hk_set_counting(hk_ctx *ctx, int enable);
+hk_status hk_get_counters(hk_ctx *ctx, uint64_t *totals3);
+
+/* ---- primary rays (castRay, GLVisitorCPUTrace.cpp:201-216) ---- */
+hk_status hk_camera_rays(hk_ctx *ctx, const float *cam16, uint32_t w, uint32_t h, float *rays8);
+
+/* ---- rendering: trace + shade (GLVisitorGPUTrace::traceScene,
+ *      GLVisitorGPUTrace.cpp:296-410, headless) ----
+ * rgba: w*h pixels, index y*w + x. HK_SHADE_CPU packs R | G<<8 | B<<16
+ * (FrameBuffer::replacePixel, HulkEngine/public/FrameBuffer.hpp:196-217);
+ * HK_SHADE_PICTURE writes RGBA8. */
+hk_status hk_render(hk_ctx *ctx, const float *cam16, const float *lights8, uint32_t nl, uint32_t w,
+                    uint32_t h, hk_variant variant, int shade, uint32_t *rgba);
+hk_status hk_render_device(hk_ctx *ctx, const float *cam16, const float *lights8, uint32_t nl,
+                           uint32_t w, uint32_t h, hk_variant variant, int shade, uint32_t *d_rgba);
+/* ShadePicture over caller hits: hit4 = float4(normal.xyz, t) per pixel as the
+ * reference's pHitDataArray, t == FLT_MAX for a miss. */
+hk_status hk_shade_picture(hk_ctx *ctx, const float *rays8, const float *hit4, uint32_t n,
+                           const float *lights8, uint32_t nl, uint32_t *rgba);
+
+/* ---- one animated frame: transform -> build -> trace -> shade ----
+ * mats12 may be NULL for a static scene. With use_graph != 0 the frame's
+ * device work is captured once into a CUDA graph and replayed (the graph is
+ * re-captured when sizes or modes change). d_rgba is a device pointer. */
+hk_status hk_frame(hk_ctx *ctx, const float *mats12, const float *cam16, const float *lights8,
+                   uint32_t nl, uint32_t w, uint32_t h, hk_build_mode mode, hk_variant variant,
+                   int use_graph, uint32_t *d_rgba, hk_tree_stats *stats);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HULKCUDA_H */

@@ -1242,9 +1242,20 @@ int hko_build_binned(const float *verts, const uint32_t *tris, uint32_t nt, cons
             if (axis[s] >= 0 && !(best < p->ci * (float)n->count)) axis[s] = -1;
             if (axis[s] >= 0) child_refs += (uint64_t)bnb + bna;
         }
-        /* capacity guard: a level that would overflow the ref arena stops splitting */
-        if (child_refs > p->max_refs)
-            for (uint32_t s = 0; s < ncur; s++) axis[s] = -1;
+        /* capacity guard: a level whose children would overflow the reference
+         * arena, the leaf-reference array or the node array stops splitting
+         * (every node of the level becomes a leaf) */
+        {
+            uint64_t leaf_refs_level = 0, splits = 0;
+            for (uint32_t s = 0; s < ncur; s++) {
+                if (axis[s] >= 0) splits++;
+                else leaf_refs_level += cur[s].count;
+            }
+            if (child_refs > p->max_refs ||
+                (uint64_t)leafrefs.n + leaf_refs_level + child_refs > p->max_refs ||
+                (uint64_t)(cn.n / 2) + 2 * splits > p->max_nodes)
+                for (uint32_t s = 0; s < ncur; s++) axis[s] = -1;
+        }
         /* 2) emit leaves and partition */
         bnode_t *nxt = (bnode_t *)malloc((size_t)2 * ncur * sizeof(bnode_t) + sizeof(bnode_t));
         uint32_t nnxt = 0;

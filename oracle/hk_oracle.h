@@ -139,7 +139,8 @@ typedef struct {
     uint32_t max_depth;
     uint32_t leaf_size;     /* leaf when refs <= leaf_size */
     uint32_t bins;          /* 32 */
-    uint32_t max_refs;      /* capacity of the reference arena */
+    uint32_t max_refs;      /* capacity of the reference arena (and of the leaf list) */
+    uint32_t max_nodes;     /* capacity of the compact node array */
 } hko_binned_params;
 int hko_build_binned(const float *verts, const uint32_t *tris, uint32_t nt, const float *box,
                      const hko_binned_params *p, uint32_t **nodes_out, uint32_t *nn_out,

@@ -1,0 +1,107 @@
+"""GPU binned-SAH builder, per-frame transform and the frame graph against the
+oracle's serial restatement of the same algorithm, through the C ABI."""
+import os
+
+import numpy as np
+import pytest
+
+from hulktracer_b200 import scenes
+from oracle.oracle import NORM_IEEE, SHORTSTACK as O_SHORT
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def load(name):
+    return dict(np.load(os.path.join(GOLDEN, name)))
+
+
+@pytest.fixture(scope="module")
+def ctx(hk):
+    return hk.Context()
+
+
+def small_animated():
+    return scenes.animated_parts(n_parts=6, width=96, height=64)
+
+
+@pytest.mark.parametrize("which", ["soup3k", "small24k", "animated6"])
+def test_build_identical_to_oracle(ctx, oracle, which):
+    if which == "animated6":
+        sc = small_animated()
+        verts, tris, box = sc.verts, sc.tris, sc.scene_box()
+    else:
+        g = load(which + ".npz")
+        verts, tris, box = g["verts"], g["tris"], g["box"]
+    ctx.upload(verts, tris)
+    ctx.set_box(box)
+    ctx.precompute()
+    st = ctx.build()
+    cn, cr = ctx.export_compact()
+    on, orf = oracle.build_binned(verts, tris, box, ct=1.0, ci=1.5, max_depth=24, leaf_size=4)
+    assert cn.shape == on.shape
+    assert np.array_equal(cn, on)
+    assert np.array_equal(cr, orf)
+    assert st["nodes"] == on.shape[0] and st["refs"] == orf.shape[0]
+
+
+def test_trace_on_built_tree(ctx, hk, oracle):
+    g = load("small24k.npz")
+    ctx.upload(g["verts"], g["tris"])
+    ctx.set_box(g["box"])
+    ctx.precompute()
+    ctx.build()
+    nodes, refs = ctx.export_tree()
+    cache = ctx.export_cache()
+    hits = ctx.trace(g["rays"], hk.SHORTSTACK)
+    tree = oracle.make_tree(g["verts"], g["tris"], cache, nodes, refs, g["box"])
+    oh, oid = oracle.trace(tree, g["rays"], O_SHORT, 6)
+    assert np.array_equal(hits["tri"], oid)
+    m = oid >= 0
+    assert np.array_equal(hits["t"][m], oh[m, 0])
+    # the same closest hits as brute force over all triangles (t exact)
+    bh = ctx.trace(g["rays"], hk.BRUTE)
+    assert np.array_equal(bh["tri"] >= 0, m)
+    assert np.array_equal(bh["t"][m], hits["t"][m])
+
+
+def test_transform_and_box(ctx, oracle):
+    sc = small_animated()
+    ctx.upload(sc.verts, sc.tris)
+    ctx.set_parts(sc.part_of_vertex, sc.part_center.shape[0])
+    mats = scenes.part_matrices(sc, 7)
+    ctx.transform(mats)
+    v = ctx.get_vertices()
+    o = oracle.transform(sc.rest_verts, sc.part_of_vertex, mats)
+    assert np.array_equal(v.view(np.uint32), o.view(np.uint32))
+    box = ctx.get_box()
+    ob = oracle.scene_box(o)
+    assert np.array_equal(box[:3], ob[:3]) and np.array_equal(box[4:7], ob[4:7])
+
+
+def test_frame_graph_matches_oracle_pipeline(ctx, hk, oracle):
+    import torch
+    sc = small_animated()
+    w, h = sc.width, sc.height
+    ctx.upload(sc.verts, sc.tris)
+    ctx.set_parts(sc.part_of_vertex, sc.part_center.shape[0])
+    out = torch.zeros(w * h, dtype=torch.int32, device="cuda")
+    for frame in (0, 3, 11):
+        mats = scenes.part_matrices(sc, frame)
+        ctx.frame(mats, sc.camera, sc.lights, w, h, out.data_ptr(), use_graph=True)
+        ctx.synchronize()
+        img_g = out.cpu().numpy().view(np.uint32).copy()
+        ctx.frame(mats, sc.camera, sc.lights, w, h, out.data_ptr(), use_graph=False)
+        ctx.synchronize()
+        img_n = out.cpu().numpy().view(np.uint32).copy()
+        assert np.array_equal(img_g, img_n)
+        verts = oracle.transform(sc.rest_verts, sc.part_of_vertex, mats)
+        box = oracle.scene_box(verts)
+        cache = oracle.cache(verts, sc.tris, NORM_IEEE)
+        cn, cr = oracle.build_binned(verts, sc.tris, box)
+        nodes = oracle.compact_to_ref(cn)
+        tree = oracle.make_tree(verts, sc.tris, cache, nodes, cr, box)
+        rays = oracle.camera_rays(sc.camera, w, h, NORM_IEEE)
+        oimg = oracle.render_cpu(tree, rays, w, h, sc.lights, O_SHORT, 6, NORM_IEEE)
+        assert np.array_equal(img_g, oimg)
