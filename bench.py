@@ -1,0 +1,380 @@
+#!/usr/bin/env python3
+"""Benchmark: Mrays/s and build+trace+shade ms/frame on one B200 per rank.
+
+Workload (default): the animated 64-part scene (~200k triangles) at 1280x720.
+One step = one animation frame through the engine: rigid transform + scene
+box + triangle records, GPU SAH KD-tree build, primary rays, shadow rays,
+shading -- captured once as a CUDA graph and replayed per frame with that
+frame's matrices. Rays counted = primary + shadow rays traced.
+
+value   : device time (CUDA events on the frame's stream), scene resident in
+          HBM, L2 flushed (256 MB write) between frames.
+e2e     : the same frames through the C ABI with host inputs: per frame the
+          part matrices, camera and lights are copied from pinned host memory
+          and the image is read back to pinned host memory, inside the timed
+          region.
+roofline: the trace kernel (primary rays) on the last frame's tree:
+          algorithmic bytes per ray 32 + 8 + 8 N_node + 4 N_ref + 36 N_tri with
+          the per-ray counts measured by the kernel's counting mode.
+Multi-GPU: frames are sharded across ranks (rank r renders frames r, r+N, ...)
+with no data-path collective; the barrier / max-over-ranks timing uses NCCL.
+
+--impl reference: the reference's own CPU path (KDTreeCPU SAH-NlogN build +
+checkCollision shading loop, compiled from its sources into oracle/_ref) on the
+host cores for the same frames.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="animated", choices=["animated", "static_small", "static_large"])
+    ap.add_argument("--mode", default="binned", choices=["binned", "learned"])
+    ap.add_argument("--variant", default="shortstack")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-frames", type=int, default=2)
+    return ap.parse_args()
+
+
+def make_scene(name):
+    from hulktracer_b200 import scenes
+    if name == "animated":
+        return scenes.animated_parts()
+    if name == "static_small":
+        return scenes.static_small()
+    return scenes.static_large()
+
+
+def workload_name(sc):
+    return "%s %d tris %dx%d primary+shadow" % (sc.name, sc.ntris, sc.width, sc.height)
+
+
+def frame_mats(sc, f):
+    from hulktracer_b200 import scenes
+    if sc.part_center is None:
+        return None
+    return scenes.part_matrices(sc, f)
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.rows.append([x.strip() for x in ln.split(",")])
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = [r for r in self.rows if len(r) >= 9]
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the reference compiled from its sources
+# ---------------------------------------------------------------------------
+def reference_frame(R, O, sc, f, prim, nthreads):
+    """One frame of the reference CPU visitor (GLVisitorCPUTrace::traverseBegin):
+    rigid transform of the vertices, KDTreeCPU::buildKDTree, traceScene.
+    Returns (seconds, rays)."""
+    t0 = time.perf_counter()
+    mats = frame_mats(sc, f)
+    if mats is not None:
+        verts = O.transform(sc.rest_verts, sc.part_of_vertex, mats)
+    else:
+        verts = sc.verts
+    box = O.scene_box(verts)
+    R.set_vertices(verts, box)
+    R.build()
+    img = R.render(prim, sc.width, sc.height, sc.lights, nthreads=nthreads)
+    dt = time.perf_counter() - t0
+    nhit = int((img != 0).sum())
+    npoint = int((sc.lights[:, 3] == 1.0).sum())
+    return dt, sc.width * sc.height + nhit * npoint
+
+
+def cpu_baseline(sc, frames, nthreads):
+    from oracle.oracle import NORM_IEEE, Oracle, Reference
+    O = Oracle()
+    if Reference.available():
+        R = Reference()
+        kind = "reference"
+    else:
+        return None
+    prim = O.camera_rays(sc.camera, sc.width, sc.height, NORM_IEEE)
+    R.load(sc.verts, sc.tris, sc.scene_box())
+    reference_frame(R, O, sc, 0, prim, nthreads)   # warm-up (page-in, OpenMP pool)
+    tot_t, tot_r = 0.0, 0
+    for f in range(frames):
+        dt, r = reference_frame(R, O, sc, f + 1, prim, nthreads)
+        tot_t += dt
+        tot_r += r
+    return {"value": tot_r / tot_t / 1e6, "unit": "Mrays/s", "cores": nthreads, "kind": kind,
+            "sample": "%d full frames (CPU transform + SAH-NlogN build + shaded trace), %d threads" % (frames, nthreads),
+            "ms_per_frame": 1000.0 * tot_t / frames}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    sc = make_scene(args.workload)
+    nthreads = os.cpu_count() or 1
+    from oracle.oracle import NORM_IEEE, Oracle, Reference
+    if not Reference.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref not built (reference sources absent when building)"}))
+        return
+    O = Oracle()
+    R = Reference()
+    prim = O.camera_rays(sc.camera, sc.width, sc.height, NORM_IEEE)
+    R.load(sc.verts, sc.tris, sc.scene_box())
+    for f in range(args.warmup):
+        reference_frame(R, O, sc, f, prim, nthreads)
+    tot_t, tot_r = 0.0, 0
+    for i in range(args.steps):
+        dt, r = reference_frame(R, O, sc, args.warmup + i, prim, nthreads)
+        tot_t += dt
+        tot_r += r
+    v = tot_r / tot_t / 1e6
+    line = {"metric": "Mrays/s (build+trace+shade per frame)", "value": v, "unit": "Mrays/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1000.0 * tot_t / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scene)",
+            "config": {"workload": workload_name(sc), "build": "reference SAH-NlogN (CPU)",
+                       "parallelism": "OpenMP rows, %d threads" % nthreads},
+            "impl": "reference",
+            "cpu_baseline": {"value": v, "unit": "Mrays/s", "cores": nthreads, "kind": "reference",
+                             "sample": "%d full frames per step" % 1},
+            "e2e": {"value": v, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+# ---------------------------------------------------------------------------
+# our engine
+# ---------------------------------------------------------------------------
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    import hulktracer_b200 as hk
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+    sc = make_scene(args.workload)
+    W, H = sc.width, sc.height
+    variant = hk.VARIANTS[args.variant]
+    mode = hk.BUILD_LEARNED if args.mode == "learned" else hk.BUILD_BINNED
+    stream = torch.cuda.Stream()
+    ctx = hk.Context(device=local)
+    ctx.set_stream(stream.cuda_stream)
+    ctx.upload(sc.verts, sc.tris)
+    animated = sc.part_of_vertex is not None
+    if animated:
+        ctx.set_parts(sc.part_of_vertex, sc.part_center.shape[0])
+    rgba = torch.zeros(W * H, dtype=torch.int32, device="cuda")
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    frames = [args.warmup + rank + world * i for i in range(args.steps)]
+    mats_all = {f: frame_mats(sc, f) for f in list(range(args.warmup)) + frames}
+    # pinned host inputs / outputs for the e2e leg
+    pin_mats = {f: (torch.from_numpy(m).pin_memory() if m is not None else None) for f, m in mats_all.items()}
+    pin_img = torch.empty(W * H, dtype=torch.int32).pin_memory()
+
+    def do_frame(f, use_graph=True):
+        m = pin_mats[f]
+        ctx.frame(m.numpy() if m is not None else None, sc.camera, sc.lights, W, H, rgba.data_ptr(), mode, variant,
+                  use_graph)
+
+    with torch.cuda.stream(stream):
+        for f in range(args.warmup):
+            do_frame(f)
+        stream.synchronize()
+        ctx.synchronize()
+        kern_nodes, all_nodes = ctx.graph_info()
+        # ---- device-timed frames ----
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        clocks = ClockSampler(local)
+        clocks.start()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in frames]
+        rays = 0
+        for (e0, e1), f in zip(ev, frames):
+            flush.zero_()
+            e0.record(stream)
+            do_frame(f)
+            e1.record(stream)
+            p, s = ctx.ray_counts()   # synchronises after the end event (outside the timed span)
+            rays += p + s
+        torch.cuda.synchronize()
+        cl = clocks.stop()
+        t_dev = sum(e0.elapsed_time(e1) for e0, e1 in ev) / 1000.0
+        # ---- e2e: host inputs in, image out, through the C ABI ----
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        ev2 = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in frames]
+        for (e0, e1), f in zip(ev2, frames):
+            flush.zero_()
+            e0.record(stream)
+            do_frame(f)
+            pin_img.copy_(rgba, non_blocking=True)
+            e1.record(stream)
+        torch.cuda.synchronize()
+        t_e2e = sum(e0.elapsed_time(e1) for e0, e1 in ev2) / 1000.0
+
+    # ---- max over ranks ----
+    tt = torch.tensor([t_dev, t_e2e, float(rays)], dtype=torch.float64, device="cuda")
+    if world > 1:
+        mx = tt.clone()
+        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+        sm = tt.clone()
+        dist.all_reduce(sm, op=dist.ReduceOp.SUM)
+        t_dev, t_e2e, total_rays = float(mx[0]), float(mx[1]), float(sm[2])
+    else:
+        total_rays = float(rays)
+
+    # ---- roofline of the trace kernel (rank 0) ----
+    roof = None
+    if rank == 0:
+        roof = trace_roofline(ctx, sc, stream, variant)
+
+    base = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        base = cpu_baseline(sc, args.cpu_frames, os.cpu_count() or 1)
+
+    if rank == 0:
+        nl = sc.lights.shape[0]
+        h2d = (0 if not animated else sc.part_center.shape[0] * 48) + 64 + nl * 32
+        line = {
+            "metric": "Mrays/s (build+trace+shade per frame)", "value": total_rays / t_dev / 1e6, "unit": "Mrays/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1000.0 * t_dev / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scene)",
+            "config": {"workload": workload_name(sc), "build": "GPU %s SAH (32 bins/axis), per frame" % args.mode,
+                       "traversal": args.variant, "graph": "one CUDA graph per frame",
+                       "l2": "flushed (256 MB write) between frames", "parallelism": "frames sharded over %d GPU(s)" % world},
+            "e2e": {"value": total_rays / t_e2e / 1e6, "unit": "Mrays/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": W * H * 4, "ms_per_step": 1000.0 * t_e2e / args.steps},
+            "gpu_launches": int(kern_nodes) * args.steps,
+            "clocks": cl,
+            "roofline": roof,
+            "cpu_baseline": base,
+        }
+        print(json.dumps(line))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    ctx.close()
+
+
+def trace_roofline(ctx, sc, stream, variant):
+    import torch
+    W, H = sc.width, sc.height
+    n = W * H
+    rays_h = ctx.camera_rays(sc.camera, W, H)
+    d_rays = torch.from_numpy(rays_h).cuda()
+    d_hits = torch.zeros(2 * n, dtype=torch.int32, device="cuda")
+    ctx.set_counting(True)
+    ctx.trace_device(d_rays.data_ptr(), n, d_hits.data_ptr(), variant)
+    ctx.synchronize()
+    cnt = ctx.counters()
+    ctx.set_counting(False)
+    n_node, n_ref, n_tri = (float(x) / n for x in cnt)
+    b_ray = 32 + 8 + 8 * n_node + 4 * n_ref + 36 * n_tri
+    reps = 20
+    with torch.cuda.stream(stream):
+        for _ in range(3):
+            ctx.trace_device(d_rays.data_ptr(), n, d_hits.data_ptr(), variant)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            ctx.trace_device(d_rays.data_ptr(), n, d_hits.data_ptr(), variant)
+        e1.record(stream)
+    torch.cuda.synchronize()
+    t = e0.elapsed_time(e1) / 1000.0 / reps
+    peak, src = measured_peak()
+    achieved = n * b_ray / t / 1e9
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", "trace_traffic.json")
+    if os.path.exists(prof):
+        with open(prof) as f:
+            traffic = json.load(f).get("bytes_per_launch")
+    return {"kernel": "k_trace primary rays", "bound": "hbm", "achieved": achieved, "peak": peak,
+            "peak_source": src, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+            "launch_ms": t * 1000.0, "rays_per_launch": n, "bytes_per_ray": b_ray,
+            "per_ray": {"nodes": n_node, "refs": n_ref, "tris": n_tri}, "mrays_per_s": n / t / 1e6}
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -90,6 +90,8 @@ def load(path: str = LIB_PATH):
         "hk_render_device": [vp, f32p, f32p, u32, u32, u32, C.c_int, C.c_int, vp],
         "hk_shade_picture": [vp, f32p, f32p, u32, f32p, u32, u32p],
         "hk_frame": [vp, f32p, f32p, f32p, u32, u32, u32, C.c_int, C.c_int, C.c_int, vp, C.POINTER(TreeStats)],
+        "hk_get_ray_counts": [vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)],
+        "hk_frame_graph_info": [vp, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)],
     }
     for name, args in sig.items():
         fn = getattr(L, name)

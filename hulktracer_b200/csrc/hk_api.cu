@@ -89,6 +89,8 @@ struct hk_ctx {
     cudaGraphExec_t graph_exec = nullptr;
     uint64_t graph_key = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    uint64_t last_primary = 0;
+    int last_shade = HK_SHADE_CPU;
 };
 
 // current tree arrays (imported or built)
@@ -700,6 +702,8 @@ static hk_status render_buffers(hk_ctx *c, uint32_t npix, uint32_t nl) {
 static hk_status render_enqueue(hk_ctx *c, uint32_t nl, uint32_t w, uint32_t h, hk_variant v, int shade,
                                 uint32_t *d_rgba) {
     uint32_t npix = w * h;
+    c->last_primary = npix;
+    c->last_shade = shade;
     HK_CUDA(c, launch_camera_rays(c->cam.p, w, h, c->rays.p, c->stream));
     hk_status s = trace_enqueue(c, c->rays.p, npix, nullptr, v, c->hits.p);
     if (s != HK_OK) return s;
@@ -845,6 +849,38 @@ hk_status hk_frame(hk_ctx *c, const float *mats12, const float *cam16, const flo
         if (s != HK_OK) return s;
         *stats = c->stats;
     }
+    return HK_OK;
+}
+
+hk_status hk_get_ray_counts(hk_ctx *c, uint64_t *primary, uint64_t *shadow) {
+    if (!c) return HK_E_ILLEGAL_INPUT;
+    cudaSetDevice(c->device);
+    uint32_t ns = 0;
+    if (c->last_shade == HK_SHADE_CPU && c->last_primary)
+        HK_CUDA(c, cudaMemcpyAsync(&ns, c->scount.p, 4, cudaMemcpyDeviceToHost, c->stream));
+    HK_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (primary) *primary = c->last_primary;
+    if (shadow) *shadow = ns;
+    return HK_OK;
+}
+
+hk_status hk_frame_graph_info(hk_ctx *c, uint32_t *kernel_nodes, uint32_t *all_nodes) {
+    if (!c) return HK_E_ILLEGAL_INPUT;
+    uint32_t k = 0, a = 0;
+    if (c->graph) {
+        size_t n = 0;
+        HK_CUDA(c, cudaGraphGetNodes(c->graph, nullptr, &n));
+        std::vector<cudaGraphNode_t> nodes(n);
+        HK_CUDA(c, cudaGraphGetNodes(c->graph, nodes.data(), &n));
+        for (size_t i = 0; i < n; i++) {
+            cudaGraphNodeType t;
+            HK_CUDA(c, cudaGraphNodeGetType(nodes[i], &t));
+            if (t == cudaGraphNodeTypeKernel) k++;
+        }
+        a = (uint32_t)n;
+    }
+    if (kernel_nodes) *kernel_nodes = k;
+    if (all_nodes) *all_nodes = a;
     return HK_OK;
 }
 

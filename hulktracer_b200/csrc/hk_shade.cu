@@ -92,7 +92,8 @@ __global__ void k_rec_to_cache(const TriRec *__restrict__ R, uint32_t nt, float 
     if (i >= nt) return;
     TriRec r = R[i];
     float *c = C + 16 * (size_t)i;
-    c[0] = r.a.x; c[1] = r.a.y; c[2] = r.a.z; c[3] = 0.0f;
+    // the reference's normal w is 0 * (1/|n|): NaN exactly when the normal is
+    c[0] = r.a.x; c[1] = r.a.y; c[2] = r.a.z; c[3] = isnan(r.a.x) ? r.a.x : 0.0f;
     c[4] = r.c.x; c[5] = r.c.y; c[6] = r.c.z; c[7] = 0.0f;
     c[8] = r.d.x; c[9] = r.d.y; c[10] = r.d.z; c[11] = 0.0f;
     c[12] = r.a.w; c[13] = r.b.w; c[14] = r.c.w; c[15] = r.d.w;

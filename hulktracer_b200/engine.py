@@ -198,6 +198,17 @@ class Context:
         return st.as_dict() if st is not None else None
 
 
+    def ray_counts(self):
+        p, sh = C.c_uint64(), C.c_uint64()
+        self._check(self.L.hk_get_ray_counts(self.h, C.byref(p), C.byref(sh)))
+        return p.value, sh.value
+
+    def graph_info(self):
+        k, a = C.c_uint32(), C.c_uint32()
+        self._check(self.L.hk_frame_graph_info(self.h, C.byref(k), C.byref(a)))
+        return k.value, a.value
+
+
 class KDTreeCUDA:
     """``KDTreeCPU``'s interface on the GPU (HulkEngine/src/KDTreeCPU.hpp:53-72)."""
 

@@ -208,6 +208,12 @@ hk_status hk_frame(hk_ctx *ctx, const float *mats12, const float *cam16, const f
                    uint32_t nl, uint32_t w, uint32_t h, hk_build_mode mode, hk_variant variant,
                    int use_graph, uint32_t *d_rgba, hk_tree_stats *stats);
 
+/* Rays of the last hk_render / hk_render_device / hk_frame: primary rays and
+ * shadow rays actually traced (synchronises the context's stream). */
+hk_status hk_get_ray_counts(hk_ctx *ctx, uint64_t *primary, uint64_t *shadow);
+/* Kernel nodes and all nodes of the captured frame graph (0 before capture). */
+hk_status hk_frame_graph_info(hk_ctx *ctx, uint32_t *kernel_nodes, uint32_t *all_nodes);
+
 #ifdef __cplusplus
 }
 #endif
