@@ -47,6 +47,8 @@ class TreeStats(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+NOALLOC_SCRATCH_BYTES = 24 << 20
+
 HIT_DTYPE = np.dtype([("t", np.float32), ("tri", np.int32)])
 
 _lib = None
@@ -92,6 +94,7 @@ def load(path: str = LIB_PATH):
         "hk_frame": [vp, f32p, f32p, f32p, u32, u32, u32, C.c_int, C.c_int, C.c_int, vp, C.POINTER(TreeStats)],
         "hk_get_ray_counts": [vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)],
         "hk_frame_graph_info": [vp, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)],
+        "hk_render_noalloc": [vp, vp, vp, u32, f32p, f32p, f32p, u32, u32, u32, C.c_int, vp, vp],
     }
     for name, args in sig.items():
         fn = getattr(L, name)

@@ -214,6 +214,34 @@ hk_status hk_get_ray_counts(hk_ctx *ctx, uint64_t *primary, uint64_t *shadow);
 /* Kernel nodes and all nodes of the captured frame graph (0 before capture). */
 hk_status hk_frame_graph_info(hk_ctx *ctx, uint32_t *kernel_nodes, uint32_t *all_nodes);
 
+/* ---- rendering without any device allocation ----
+ * No counterpart in the reference: an addition for callers that cannot let
+ * the library call cudaMalloc (hosts with their own pooled allocator, code
+ * running while a graph capture is open elsewhere, fixed memory budgets).
+ * The caller passes the tree, the triangle records and the image in its own
+ * device memory:
+ *   d_nodes2     compact nodes, 2 x uint32 each (hk_tree_export_compact layout)
+ *   d_refs       leaf references (uint32)
+ *   d_records16  16 floats per triangle: {n.xyz, e00} {p1.xyz, e01}
+ *                {e0.xyz, e11} {e1.xyz, det} (the PolyToRayCache of
+ *                hk_cache_export with vertex p1 in the free lanes)
+ *   d_rgba       w*h pixels, HK_SHADE_CPU packing
+ * and host box8 / cam16 / lights8. Everything else -- rays, hits, shadow rays,
+ * counters -- lives in one static device array of HK_NOALLOC_SCRATCH_BYTES
+ * that every GPU loading the library holds until the process exits. A call
+ * needing more scratch than that (roughly w*h*(40 + 44*point_lights +
+ * 4*lights) bytes; 512x512 with one point light fits) returns HK_E_CAPACITY
+ * before doing anything. The first call on a device looks up the array's
+ * device address; make it before any stream capture starts. Calls share the
+ * array and keep the last call's contents (counters are cleared per call);
+ * calls whose GPU work overlaps race on it. The call synchronises
+ * cuda_stream before returning (to read the device error word). */
+#define HK_NOALLOC_SCRATCH_BYTES (24u << 20)
+hk_status hk_render_noalloc(const uint32_t *d_nodes2, const uint32_t *d_refs, const float *d_records16,
+                            uint32_t ntris, const float *box8, const float *cam16, const float *lights8,
+                            uint32_t nl, uint32_t w, uint32_t h, hk_variant variant, uint32_t *d_rgba,
+                            void *cuda_stream);
+
 #ifdef __cplusplus
 }
 #endif
