@@ -1,0 +1,63 @@
+"""Small, self-contained GPU cases for profiler captures (ncu) of single kernels.
+
+    python -m hulktracer_b200.profile_case --case trace --variant shortstack
+    python -m hulktracer_b200.profile_case --case build
+    python -m hulktracer_b200.profile_case --case frame
+
+Each case sets up the animated 64-part scene (~200k triangles, 1280x720), does
+its warm-up work first and then launches the kernel of interest a few times, so
+an ncu command can select it with -k / -s / -c.
+"""
+from __future__ import annotations
+
+import argparse
+import os
+import sys
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+
+def main():
+    import numpy as np
+    import torch
+
+    import hulktracer_b200 as hk
+    from hulktracer_b200 import scenes
+
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--case", default="trace", choices=["trace", "build", "frame"])
+    ap.add_argument("--variant", default="shortstack")
+    ap.add_argument("--mode", default="binned", choices=["binned", "learned"])
+    ap.add_argument("--reps", type=int, default=3)
+    a = ap.parse_args()
+    sc = scenes.animated_parts()
+    W, H = sc.width, sc.height
+    ctx = hk.Context()
+    ctx.upload(sc.verts, sc.tris)
+    ctx.set_parts(sc.part_of_vertex, sc.part_center.shape[0])
+    ctx.transform(scenes.part_matrices(sc, 1))
+    mode = hk.BUILD_LEARNED if a.mode == "learned" else hk.BUILD_BINNED
+    st = ctx.build(mode)
+    if a.case == "trace":
+        rays = torch.from_numpy(ctx.camera_rays(sc.camera, W, H)).cuda()
+        hits = torch.zeros(2 * W * H, dtype=torch.int32, device="cuda")
+        for _ in range(a.reps):
+            ctx.trace_device(rays.data_ptr(), W * H, hits.data_ptr(), hk.VARIANTS[a.variant])
+        ctx.synchronize()
+    elif a.case == "build":
+        for _ in range(a.reps):
+            st = ctx.build(mode)
+    else:
+        out = torch.zeros(W * H, dtype=torch.int32, device="cuda")
+        for f in range(a.reps):
+            ctx.frame(scenes.part_matrices(sc, f), sc.camera, sc.lights, W, H, out.data_ptr(), mode,
+                      hk.VARIANTS[a.variant], True)
+        ctx.synchronize()
+    print("case %s done: tree %s" % (a.case, {k: st[k] for k in ("nodes", "refs", "depth")}))
+    del np
+
+
+if __name__ == "__main__":
+    main()
