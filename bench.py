@@ -335,6 +335,8 @@ def trace_roofline(ctx, sc, stream, variant):
     W, H = sc.width, sc.height
     n = W * H
     rays_h = ctx.camera_rays(sc.camera, W, H)
+    if W % 8 == 0 and H % 4 == 0:   # the frame traces primary rays in 8x4-pixel tiles
+        rays_h = np.ascontiguousarray(rays_h.reshape(H // 4, 4, W // 8, 8, 8).transpose(0, 2, 1, 3, 4).reshape(-1, 8))
     d_rays = torch.from_numpy(rays_h).cuda()
     d_hits = torch.zeros(2 * n, dtype=torch.int32, device="cuda")
     ctx.set_counting(True)

@@ -704,12 +704,13 @@ static hk_status render_enqueue(hk_ctx *c, uint32_t nl, uint32_t w, uint32_t h, 
     uint32_t npix = w * h;
     c->last_primary = npix;
     c->last_shade = shade;
-    HK_CUDA(c, launch_camera_rays(c->cam.p, w, h, c->rays.p, c->stream));
+    const bool tiled = (w % 8u == 0) && (h % 4u == 0);
+    HK_CUDA(c, launch_camera_rays(c->cam.p, w, h, c->rays.p, c->stream, tiled));
     hk_status s = trace_enqueue(c, c->rays.p, npix, nullptr, v, c->hits.p);
     if (s != HK_OK) return s;
     if (shade == HK_SHADE_PICTURE) {
         HK_CUDA(c, launch_hit4(c->hits.p, c->rec.p, npix, c->hit4.p, c->stream));
-        HK_CUDA(c, launch_shade_picture(c->rays.p, c->hit4.p, npix, c->lights.p, nl, d_rgba, c->stream));
+        HK_CUDA(c, launch_shade_picture(c->rays.p, c->hit4.p, npix, c->lights.p, nl, d_rgba, c->stream, w, tiled));
         return HK_OK;
     }
     HK_CUDA(c, launch_shadow_rays(c->rays.p, c->hits.p, c->rec.p, npix, c->lights.p, nl, c->srays.p, c->slot.p,
@@ -717,7 +718,7 @@ static hk_status render_enqueue(hk_ctx *c, uint32_t nl, uint32_t w, uint32_t h, 
     s = trace_enqueue(c, c->srays.p, 0, c->scount.p, v, c->shits.p);
     if (s != HK_OK) return s;
     HK_CUDA(c, launch_shade_cpu(c->rays.p, c->hits.p, c->rec.p, npix, c->lights.p, nl, c->slot.p, c->shits.p,
-                                d_rgba, c->stream));
+                                d_rgba, c->stream, w, tiled));
     return HK_OK;
 }
 

@@ -122,7 +122,10 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_partials(Load ld, T *part
         carry = vadd(carry, tot);
         __syncthreads();
     }
-    if (threadIdx.x == 0) *total = carry;
+    if (threadIdx.x == 0) {
+        *total = carry;
+        ld.on_total(carry);
+    }
 }
 
 // scan phase 3: exclusive prefix of every element
@@ -142,7 +145,10 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_apply(Load ld, const T *p
         T tot;
         T ex = vadd(partials[tile], block_excl(s, sh, tot));
         for (int k = 0; k < kScanItems; k++) {
-            if (base + k < n) out[base + k] = ex;
+            if (base + k < n) {
+                out[base + k] = ex;
+                ld.on_prefix(base + k, ex);
+            }
             ex = vadd(ex, v[k]);
         }
     }
@@ -290,12 +296,10 @@ struct LevelArgs {
     float *plane;
     uint2 *cnt;
     uint4 *plan;
-    const uint4 *plan_tot;
-    uint2 *prep;
-    const uint2 *prep_tot;
-    uint2 *chunks;
+    uint2 *chunks;          // (large rank, chunk index within the node)
     uint32_t *large_slot;
     uint32_t *hist;
+    uint32_t *done;
     const uint32_t *refs;
     const uint32_t *ref_node;
     uint32_t *nx_refs, *nx_ref_node;
@@ -303,6 +307,7 @@ struct LevelArgs {
     uint2 *out_nodes;
     uint32_t *out_refs;
     BuildCounters *ctr;
+    LevelCounters *lc, *nlc;
     uint32_t *err;
     uint32_t level;
     float ct, ci;
@@ -320,88 +325,49 @@ __global__ void k_tri_bounds(const float4 *__restrict__ V, const uint4 *__restri
     hi[i] = make_float4(mxf(mxf(a.x, b.x), c.x), mxf(mxf(a.y, b.y), c.y), mxf(mxf(a.z, b.z), c.z), 0.0f);
 }
 
+// root node + references of level 0 (the counters were zeroed by a memset)
 __global__ void k_root(LevelArgs A, const float *box, uint32_t nt) {
-    if (threadIdx.x == 0 && blockIdx.x == 0) {
-        BuildCounters *c = A.ctr;
-        c->level_nodes = 1;
-        c->level_refs = nt;
-        c->nodes_total = 2;
-        c->leafrefs_total = 0;
-        c->stop = 0;
-        c->depth = 0;
-        c->leaves = 0;
-        c->capacity_hit = 0;
-        c->learned_nodes = 0;
-        c->fallback_nodes = 0;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        LevelCounters *l0 = &A.ctr->lvl[0];
+        l0->nodes = 1;
+        l0->refs = nt;
+        l0->nodes_total = 2;
+        l0->leafrefs_total = 0;
         A.nx_lo[0] = make_float4(box[0], box[1], box[2], 0.0f);
         A.nx_hi[0] = make_float4(box[4], box[5], box[6], 0.0f);
         A.nx_info[0] = make_uint4(0, nt, 0, 0);
         A.out_nodes[1] = make_uint2(kLeafTag, 0);
         A.out_nodes[0] = make_uint2(kLeafTag, 0);
     }
-}
-
-__global__ void k_iota(uint32_t *refs, uint32_t *ref_node, uint32_t nt) {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nt; i += gridDim.x * blockDim.x) {
-        refs[i] = i;
-        ref_node[i] = 0;
+        const_cast<uint32_t *>(A.refs)[i] = i;
+        const_cast<uint32_t *>(A.ref_node)[i] = 0;
     }
 }
 
-struct LoadPrep {
-    const uint4 *info;
-    const BuildCounters *ctr;
-    uint32_t level, max_depth, leaf_size;
-    __device__ uint32_t count() const { return ctr->level_nodes; }
-    __device__ uint2 operator()(uint32_t s) const {
-        uint32_t cnt = info[s].y;
-        bool dec = cnt > leaf_size && level < max_depth;
-        bool large = dec && cnt > kSmall;
-        return make_uint2(large ? 1u : 0u, large ? (cnt + kChunk - 1) / kChunk : 0u);
-    }
-};
+__device__ __forceinline__ bool decidable(const LevelArgs &A, uint32_t cnt) {
+    return cnt > A.leaf_size && A.level < A.max_depth;
+}
 
-__global__ void k_chunk_fill(LevelArgs A, uint32_t max_depth, uint32_t leaf_size) {
-    const uint32_t n = A.ctr->level_nodes;
+// large nodes take ranks and chunk ranges (atomics: the histogram sums do not
+// depend on their order)
+__global__ void k_prep(LevelArgs A) {
+    const uint32_t n = A.lc->nodes;
     for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
         uint32_t cnt = A.n_info[s].y;
-        bool dec = cnt > leaf_size && A.level < max_depth;
-        if (!(dec && cnt > kSmall)) continue;
-        uint2 pr = A.prep[s];
-        uint32_t rank = pr.x, first = pr.y, nch = (cnt + kChunk - 1) / kChunk;
+        if (!(decidable(A, cnt) && cnt > kSmall)) continue;
+        uint32_t nch = (cnt + kChunk - 1) / kChunk;
+        uint32_t rank = atomicAdd(&A.lc->n_large, 1u);
+        uint32_t first = atomicAdd(&A.lc->n_chunks, nch);
         if (rank >= A.cap_large || first + nch > A.cap_chunks) {
             atomicOr(A.err, 2u);
             continue;
         }
         A.large_slot[rank] = s;
-        for (uint32_t k = 0; k < nch; k++) A.chunks[first + k] = make_uint2(s, rank);
+        for (uint32_t k = 0; k < nch; k++) A.chunks[first + k] = make_uint2(rank, k);
         uint32_t *H = A.hist + (size_t)rank * kHist;
         for (uint32_t k = 0; k < kHist; k++) H[k] = 0;
-    }
-}
-
-__global__ void __launch_bounds__(256) k_hist_large(LevelArgs A) {
-    __shared__ uint32_t H[kHist];
-    const uint32_t nch = min(A.prep_tot->y, A.cap_chunks);
-    for (uint32_t ch = blockIdx.x; ch < nch; ch += gridDim.x) {
-        uint2 cr = A.chunks[ch];
-        uint32_t s = cr.x;
-        if (s >= A.ctr->level_nodes || cr.y >= A.cap_large) continue;  // uniform per CTA
-        uint4 info = A.n_info[s];
-        uint32_t k = ch - A.prep[s].y;
-        uint32_t r0 = info.x + k * kChunk, r1 = min(info.x + info.y, r0 + kChunk);
-        float4 blo = A.n_lo[s], bhi = A.n_hi[s];
-        for (uint32_t i = threadIdx.x; i < kHist; i += blockDim.x) H[i] = 0;
-        __syncthreads();
-        for (uint32_t r = r0 + threadIdx.x; r < r1; r += blockDim.x) {
-            uint32_t tri = A.refs[r];
-            hist_ref(H, A.tb_lo[tri], A.tb_hi[tri], blo, bhi);
-        }
-        __syncthreads();
-        uint32_t *G = A.hist + (size_t)cr.y * kHist;
-        for (uint32_t i = threadIdx.x; i < kHist; i += blockDim.x)
-            if (H[i]) atomicAdd(&G[i], H[i]);
-        __syncthreads();
+        A.done[rank] = 0;
     }
 }
 
@@ -411,88 +377,129 @@ __device__ __forceinline__ void write_decision(const LevelArgs &A, uint32_t s, c
     A.cnt[s] = make_uint2(d.nb, d.na);
 }
 
-__global__ void __launch_bounds__(256) k_sah_large(LevelArgs A) {
-    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-    const uint32_t nl = min(A.prep_tot->x, A.cap_large);
-    for (uint32_t r = warp; r < nl; r += nwarps) {
-        uint32_t s = A.large_slot[r];
-        if (s >= A.ctr->level_nodes) continue;
-        uint4 info = A.n_info[s];
-        Decision d = sah_warp(A.hist + (size_t)r * kHist, A.n_lo[s], A.n_hi[s], info.y, A.ct, A.ci);
-        if ((threadIdx.x & 31u) == 0) write_decision(A, s, d);
-    }
-}
-
-__global__ void __launch_bounds__(256) k_small(LevelArgs A) {
-    __shared__ uint32_t HS[8][kHist];
-    const uint32_t wib = threadIdx.x >> 5, lane = threadIdx.x & 31u;
-    uint32_t *H = HS[wib];
-    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-    const uint32_t n = A.ctr->level_nodes;
-    for (uint32_t s = warp; s < n; s += nwarps) {
-        uint4 info = A.n_info[s];
-        uint32_t cnt = info.y;
-        bool dec = cnt > A.leaf_size && A.level < A.max_depth;
-        if (dec && cnt > kSmall) continue;  // large: k_sah_large
-        if (!dec) {
-            if (lane == 0) write_decision(A, s, Decision{-1, 0.0f, 0, 0, kInf});
-            continue;
-        }
-        for (uint32_t i = lane; i < kHist; i += 32) H[i] = 0;
-        __syncwarp();
-        float4 blo = A.n_lo[s], bhi = A.n_hi[s];
-        for (uint32_t r = info.x + lane; r < info.x + cnt; r += 32) {
-            uint32_t tri = A.refs[r];
-            hist_ref(H, A.tb_lo[tri], A.tb_hi[tri], blo, bhi);
-        }
-        __syncwarp();
-        Decision d = sah_warp(H, blo, bhi, cnt, A.ct, A.ci);
-        if (lane == 0) write_decision(A, s, d);
-        __syncwarp();
-    }
-}
-
-struct LoadPlan {
-    const uint4 *info;
-    const int32_t *axis;
-    const uint2 *cnt;
-    const BuildCounters *ctr;
-    __device__ uint32_t count() const { return ctr->level_nodes; }
-    __device__ uint4 operator()(uint32_t s) const {
-        if (axis[s] < 0) return make_uint4(info[s].y, 0, 0, 0);
-        uint2 c = cnt[s];
-        return make_uint4(0, 1, (c.x > 0) + (c.y > 0), c.x + c.y);
-    }
+// global histogram read past L1 (other CTAs wrote it with atomics)
+struct GHist {
+    const uint32_t *p;
+    __device__ uint32_t operator[](uint32_t i) const { return __ldcg(p + i); }
 };
 
-__global__ void k_guard(LevelArgs A) {
-    if (threadIdx.x || blockIdx.x) return;
-    BuildCounters *c = A.ctr;
-    uint4 t = *A.plan_tot;
-    uint64_t child_refs = t.w, leaf_refs = t.x, splits = t.y;
-    bool over = child_refs > A.cap_refs || (uint64_t)c->leafrefs_total + leaf_refs + child_refs > A.cap_refs ||
-                (uint64_t)c->nodes_total + 2 * splits > A.cap_nodes || t.z > A.cap_level;
-    c->stop = over ? 1u : 0u;
-    if (over) c->capacity_hit = 1;
+// Work items: first the chunks of large nodes (one CTA each; the CTA that
+// finishes a node's last chunk evaluates its SAH), then groups of 8 small
+// nodes (one warp each: warp-private histogram + SAH).
+__global__ void __launch_bounds__(256) k_work(LevelArgs A) {
+    __shared__ uint32_t H[kHist];
+    __shared__ uint32_t HS[8][kHist];
+    __shared__ int s_last;
+    const uint32_t wib = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+    const uint32_t nch = min(A.lc->n_chunks, A.cap_chunks);
+    const uint32_t nodes = A.lc->nodes;
+    const uint32_t ngroups = (nodes + 7) / 8;
+    for (uint32_t item = blockIdx.x; item < nch + ngroups; item += gridDim.x) {
+        if (item < nch) {
+            uint2 ck = A.chunks[item];
+            uint32_t rank = ck.x;
+            if (rank >= A.cap_large) continue;  // uniform per CTA
+            uint32_t s = A.large_slot[rank];
+            if (s >= nodes) continue;
+            uint4 info = A.n_info[s];
+            uint32_t r0 = info.x + ck.y * kChunk, r1 = min(info.x + info.y, r0 + kChunk);
+            float4 blo = A.n_lo[s], bhi = A.n_hi[s];
+            for (uint32_t i = threadIdx.x; i < kHist; i += blockDim.x) H[i] = 0;
+            __syncthreads();
+            for (uint32_t r = r0 + threadIdx.x; r < r1; r += blockDim.x) {
+                uint32_t tri = A.refs[r];
+                hist_ref(H, A.tb_lo[tri], A.tb_hi[tri], blo, bhi);
+            }
+            __syncthreads();
+            uint32_t *G = A.hist + (size_t)rank * kHist;
+            for (uint32_t i = threadIdx.x; i < kHist; i += blockDim.x)
+                if (H[i]) atomicAdd(&G[i], H[i]);
+            __threadfence();
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                uint32_t nchunks = (info.y + kChunk - 1) / kChunk;
+                s_last = (atomicAdd(&A.done[rank], 1u) == nchunks - 1) ? 1 : 0;
+            }
+            __syncthreads();
+            if (s_last && wib == 0) {
+                __threadfence();
+                Decision d = sah_warp(GHist{G}, blo, bhi, info.y, A.ct, A.ci);
+                if (lane == 0) write_decision(A, s, d);
+            }
+            __syncthreads();
+        } else {
+            uint32_t s = (item - nch) * 8 + wib;
+            if (s >= nodes) continue;
+            uint4 info = A.n_info[s];
+            uint32_t cnt = info.y;
+            bool dec = decidable(A, cnt);
+            if (dec && cnt > kSmall) continue;  // large: handled by its chunks
+            if (!dec) {
+                if (lane == 0) write_decision(A, s, Decision{-1, 0.0f, 0, 0, kInf});
+                continue;
+            }
+            uint32_t *Hw = HS[wib];
+            for (uint32_t i = lane; i < kHist; i += 32) Hw[i] = 0;
+            __syncwarp();
+            float4 blo = A.n_lo[s], bhi = A.n_hi[s];
+            for (uint32_t r = info.x + lane; r < info.x + cnt; r += 32) {
+                uint32_t tri = A.refs[r];
+                hist_ref(Hw, A.tb_lo[tri], A.tb_hi[tri], blo, bhi);
+            }
+            __syncwarp();
+            Decision d = sah_warp(Hw, blo, bhi, cnt, A.ct, A.ci);
+            if (lane == 0) write_decision(A, s, d);
+            __syncwarp();
+        }
+    }
 }
 
-__global__ void k_emit(LevelArgs A) {
-    const BuildCounters *c = A.ctr;
-    const uint32_t n = c->level_nodes;
-    const bool stop = c->stop != 0;
-    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
+// plan scan: (leaf refs, child pairs, next-level nodes, child refs) per node.
+// on_total (one thread, after the tile sums) is the capacity guard and writes
+// the next level's counters; on_prefix emits node s's compact entry and its
+// children's next-level records.
+struct LoadPlan {
+    LevelArgs A;
+    __device__ uint32_t count() const { return A.lc->nodes; }
+    __device__ uint4 operator()(uint32_t s) const {
+        if (A.axis[s] < 0) return make_uint4(A.n_info[s].y, 0, 0, 0);
+        uint2 c = A.cnt[s];
+        return make_uint4(0, 1, (c.x > 0) + (c.y > 0), c.x + c.y);
+    }
+    __device__ void on_total(uint4 t) const {
+        LevelCounters *l = A.lc, *nx = A.nlc;
+        nx->n_large = 0;
+        nx->n_chunks = 0;
+        if (l->nodes == 0) {
+            nx->nodes = 0;
+            nx->refs = 0;
+            nx->nodes_total = l->nodes_total;
+            nx->leafrefs_total = l->leafrefs_total;
+            return;
+        }
+        uint64_t child_refs = t.w, leaf_refs = t.x, splits = t.y;
+        bool over = child_refs > A.cap_refs || (uint64_t)l->leafrefs_total + leaf_refs + child_refs > A.cap_refs ||
+                    (uint64_t)l->nodes_total + 2 * splits > A.cap_nodes || t.z > A.cap_level;
+        l->stop = over ? 1u : 0u;
+        if (over) A.ctr->capacity_hit = 1;
+        nx->nodes = over ? 0u : t.z;
+        nx->refs = over ? 0u : t.w;
+        nx->nodes_total = l->nodes_total + (over ? 0u : 2u * t.y);
+        nx->leafrefs_total = l->leafrefs_total + (over ? l->refs : t.x);
+        if (!over && t.z) A.ctr->depth = A.level + 1;
+    }
+    __device__ void on_prefix(uint32_t s, uint4 pl) const {
+        const LevelCounters *l = A.lc;
+        const bool stop = l->stop != 0;
         uint4 info = A.n_info[s];
         int ax = stop ? -1 : A.axis[s];
-        uint4 pl = A.plan[s];
         if (ax < 0) {
-            uint32_t off = c->leafrefs_total + (stop ? info.x : pl.x);
+            uint32_t off = l->leafrefs_total + (stop ? info.x : pl.x);
             A.out_nodes[info.z] = make_uint2((off << 2) | kLeafTag, info.y);
             if (info.y) atomicAdd(&A.ctr->leaves, 1u);
-            continue;
+            return;
         }
-        uint32_t pair = c->nodes_total + 2 * pl.y;
+        uint32_t pair = l->nodes_total + 2 * pl.y;
         float p = A.plane[s];
         uint2 ct = A.cnt[s];
         A.out_nodes[info.z] = make_uint2((pair << 2) | (uint32_t)ax, __float_as_uint(p));
@@ -518,7 +525,7 @@ __global__ void k_emit(LevelArgs A) {
             A.out_nodes[pair + 1] = make_uint2(kLeafTag, 0);
         }
     }
-}
+};
 
 __device__ __forceinline__ uint2 ref_flags(const LevelArgs &A, uint32_t r, uint32_t s, int ax) {
     uint32_t tri = A.refs[r];
@@ -530,27 +537,29 @@ __device__ __forceinline__ uint2 ref_flags(const LevelArgs &A, uint32_t r, uint3
 
 struct LoadRefFlags {
     LevelArgs A;
-    __device__ uint32_t count() const { return A.ctr->level_refs; }
+    __device__ uint32_t count() const { return A.lc->refs; }
     __device__ uint2 operator()(uint32_t r) const {
-        if (A.ctr->stop) return make_uint2(0, 0);
+        if (A.lc->stop) return make_uint2(0, 0);
         uint32_t s = A.ref_node[r];
         int ax = A.axis[s];
         if (ax < 0) return make_uint2(0, 0);
         return ref_flags(A, r, s, ax);
     }
+    __device__ void on_total(uint2) const {}
+    __device__ void on_prefix(uint32_t, uint2) const {}
 };
 
 __global__ void k_scatter(LevelArgs A) {
-    const BuildCounters *c = A.ctr;
-    const uint32_t n = c->level_refs;
-    const bool stop = c->stop != 0;
+    const LevelCounters *l = A.lc;
+    const uint32_t n = l->refs;
+    const bool stop = l->stop != 0;
     for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
         uint32_t s = A.ref_node[r];
         uint4 info = A.n_info[s];
         int ax = stop ? -1 : A.axis[s];
         uint32_t tri = A.refs[r];
         if (ax < 0) {
-            uint32_t off = c->leafrefs_total + (stop ? info.x : A.plan[s].x) + (r - info.x);
+            uint32_t off = l->leafrefs_total + (stop ? info.x : A.plan[s].x) + (r - info.x);
             if (off < A.cap_refs) A.out_refs[off] = tri;
             else atomicOr(A.err, 2u);
             continue;
@@ -580,25 +589,6 @@ __global__ void k_scatter(LevelArgs A) {
     }
 }
 
-__global__ void k_advance(LevelArgs A) {
-    if (threadIdx.x || blockIdx.x) return;
-    BuildCounters *c = A.ctr;
-    uint4 t = *A.plan_tot;
-    if (c->level_nodes == 0) return;
-    if (c->stop) {
-        c->leafrefs_total += c->level_refs;
-        c->level_nodes = 0;
-        c->level_refs = 0;
-        c->stop = 0;
-        return;
-    }
-    c->leafrefs_total += t.x;
-    c->nodes_total += 2 * t.y;
-    c->level_nodes = t.z;
-    c->level_refs = t.w;
-    if (t.z) c->depth = A.level + 1;
-}
-
 // ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
@@ -619,11 +609,11 @@ void build_release(BuildState &S) {
         S.n_lo[k] = S.n_hi[k] = nullptr; S.n_info[k] = nullptr; S.refs[k] = S.ref_node[k] = nullptr;
     }
     f(S.d_axis); f(S.d_plane); f(S.d_cnt); f(S.plan); f(S.plan_tot); f(S.prep); f(S.prep_tot);
-    f(S.chunks); f(S.hist); f(S.rscan); f(S.rscan_tot); f(S.scan_partials); f(S.ctr); f(S.err);
+    f(S.chunks); f(S.hist); f(S.done); f(S.rscan); f(S.rscan_tot); f(S.scan_partials); f(S.ctr); f(S.err);
     f(S.out_nodes); f(S.out_refs);
     S.tb_lo = S.tb_hi = nullptr;
     S.d_axis = nullptr; S.d_plane = nullptr; S.d_cnt = nullptr; S.plan = nullptr; S.plan_tot = nullptr;
-    S.prep = nullptr; S.prep_tot = nullptr; S.chunks = nullptr; S.hist = nullptr; S.rscan = nullptr;
+    S.prep = nullptr; S.prep_tot = nullptr; S.chunks = nullptr; S.hist = nullptr; S.done = nullptr; S.rscan = nullptr;
     S.rscan_tot = nullptr; S.scan_partials = nullptr; S.ctr = nullptr; S.err = nullptr;
     S.out_nodes = nullptr; S.out_refs = nullptr;
     S.nt = S.cap_refs = S.cap_nodes = S.cap_level = 0;
@@ -667,6 +657,7 @@ hk_status build_prepare(BuildState &S, const BuildParams &p, uint32_t nt, int sm
     bad |= dalloc(S.prep_tot, 1) != cudaSuccess;
     bad |= dalloc(S.chunks, S.cap_chunks + S.cap_large) != cudaSuccess;  // tail holds large_slot
     bad |= dalloc(S.hist, (size_t)S.cap_large * kHist) != cudaSuccess;
+    bad |= dalloc(S.done, S.cap_large) != cudaSuccess;
     bad |= dalloc(S.rscan, cap_refs) != cudaSuccess;
     bad |= dalloc(S.rscan_tot, 1) != cudaSuccess;
     {
@@ -707,12 +698,10 @@ cudaError_t build_launch(BuildState &S, const float4 *verts, const uint4 *tris, 
     A.plane = S.d_plane;
     A.cnt = S.d_cnt;
     A.plan = S.plan;
-    A.plan_tot = S.plan_tot;
-    A.prep = S.prep;
-    A.prep_tot = S.prep_tot;
     A.chunks = S.chunks;
     A.large_slot = reinterpret_cast<uint32_t *>(S.chunks + S.cap_chunks);
     A.hist = S.hist;
+    A.done = S.done;
     A.rscan = S.rscan;
     A.out_nodes = S.out_nodes;
     A.out_refs = S.out_refs;
@@ -727,16 +716,19 @@ cudaError_t build_launch(BuildState &S, const float4 *verts, const uint4 *tris, 
     A.cap_level = S.cap_level;
     A.cap_large = S.cap_large;
     A.cap_chunks = S.cap_chunks;
+    cudaMemsetAsync(S.ctr, 0, sizeof(BuildCounters), st);
     if (nt) k_tri_bounds<<<(nt + 255) / 256, 256, 0, st>>>(verts, tris, nt, S.tb_lo, S.tb_hi);
-    // level 0 lives in slot buffers [0]
     A.nx_lo = S.n_lo[0];
     A.nx_hi = S.n_hi[0];
     A.nx_info = S.n_info[0];
-    k_root<<<1, 32, 0, st>>>(A, box, nt);
-    k_iota<<<G, 256, 0, st>>>(S.refs[0], S.ref_node[0], nt);
+    A.refs = S.refs[0];
+    A.ref_node = S.ref_node[0];
+    k_root<<<G, 256, 0, st>>>(A, box, nt);
     for (uint32_t L = 0; L <= S.p.max_depth; L++) {
         int cur = L & 1, nxt = cur ^ 1;
         A.level = L;
+        A.lc = &S.ctr->lvl[L];
+        A.nlc = &S.ctr->lvl[L + 1];
         A.n_lo = S.n_lo[cur];
         A.n_hi = S.n_hi[cur];
         A.n_info = S.n_info[cur];
@@ -747,22 +739,14 @@ cudaError_t build_launch(BuildState &S, const float4 *verts, const uint4 *tris, 
         A.ref_node = S.ref_node[cur];
         A.nx_refs = S.refs[nxt];
         A.nx_ref_node = S.ref_node[nxt];
-        LoadPrep lp{A.n_info, S.ctr, L, S.p.max_depth, S.p.leaf_size};
-        scan<uint2>(lp, reinterpret_cast<uint2 *>(S.scan_partials), S.prep, S.prep_tot, G, st);
-        k_chunk_fill<<<G, 256, 0, st>>>(A, S.p.max_depth, S.p.leaf_size);
-        k_hist_large<<<G, 256, 0, st>>>(A);
-        k_sah_large<<<G, 256, 0, st>>>(A);
-        k_small<<<G * 2, 256, 0, st>>>(A);
-        LoadPlan lpl{A.n_info, S.d_axis, S.d_cnt, S.ctr};
-        scan<uint4>(lpl, reinterpret_cast<uint4 *>(S.scan_partials), S.plan, S.plan_tot, G, st);
-        k_guard<<<1, 32, 0, st>>>(A);
-        k_emit<<<G, 256, 0, st>>>(A);
-        LoadRefFlags lr{A};
-        scan<uint2>(lr, reinterpret_cast<uint2 *>(S.scan_partials), S.rscan, S.rscan_tot, G, st);
+        k_prep<<<G, 256, 0, st>>>(A);
+        k_work<<<G * 2, 256, 0, st>>>(A);
+        scan<uint4>(LoadPlan{A}, reinterpret_cast<uint4 *>(S.scan_partials), S.plan, S.plan_tot, G, st);
+        scan<uint2>(LoadRefFlags{A}, reinterpret_cast<uint2 *>(S.scan_partials), S.rscan, S.rscan_tot, G, st);
         k_scatter<<<G, 256, 0, st>>>(A);
-        k_advance<<<1, 32, 0, st>>>(A);
     }
     S.active = true;
+    S.last_level = S.p.max_depth + 1;
     return cudaGetLastError();
 }
 
@@ -776,8 +760,9 @@ hk_status build_read_stats(BuildState &S, cudaStream_t st, hk_tree_stats *out) {
         cudaMemsetAsync(S.err, 0, 4, st);
         return HK_E_CAPACITY;
     }
-    out->nodes = c.nodes_total;
-    out->refs = c.leafrefs_total;
+    const LevelCounters &fin = c.lvl[S.last_level];
+    out->nodes = fin.nodes_total;
+    out->refs = fin.leafrefs_total;
     out->leaves = c.leaves;
     out->depth = c.depth;
     out->capacity_hit = c.capacity_hit;

@@ -19,21 +19,30 @@ struct BuildParams {
     float fallback_ratio = 1.02f;
 };
 
+constexpr int kMaxLevels = 52;  // max_depth <= 48, plus the level after the last
+
+// counters of one tree level; level L's kernels read lvl[L] and the scan that
+// plans its children writes lvl[L + 1], so no bookkeeping launch is needed
+struct LevelCounters {
+    uint32_t nodes;             // active nodes of the level
+    uint32_t refs;              // their references
+    uint32_t nodes_total;       // compact nodes written before this level
+    uint32_t leafrefs_total;    // leaf references written before this level
+    uint32_t stop;              // the level stops splitting (capacity)
+    uint32_t n_large;           // large nodes (chunked histograms)
+    uint32_t n_chunks;          // histogram chunks
+    uint32_t pad;
+};
+
 // device scalars of one build (one struct in device memory)
 struct BuildCounters {
-    uint32_t level_nodes;       // active nodes of the current level
-    uint32_t level_refs;        // their references
-    uint32_t nodes_total;       // compact nodes written so far
-    uint32_t leafrefs_total;    // leaf references written so far
-    uint32_t stop;              // current level stops splitting (capacity)
     uint32_t depth;             // deepest level reached
     uint32_t leaves;            // leaves written (empty cells excluded)
     uint32_t capacity_hit;
-    uint32_t n_large;           // large nodes of the level
-    uint32_t n_chunks;          // histogram chunks of the level
     uint32_t learned_nodes;
     uint32_t fallback_nodes;
-    uint32_t pad[4];
+    uint32_t pad[3];
+    LevelCounters lvl[kMaxLevels];
 };
 
 struct BuildOutputs {
@@ -46,6 +55,7 @@ struct BuildState {
     uint32_t nt = 0, cap_refs = 0, cap_nodes = 0, cap_level = 0, cap_large = 0, cap_chunks = 0;
     int sm_count = 148;
     bool active = false;        // a built tree is the current tree
+    uint32_t last_level = 0;    // lvl[] index holding the final totals
     // per-triangle bounds
     float4 *tb_lo = nullptr, *tb_hi = nullptr;
     // level nodes (ping-pong)
@@ -61,6 +71,7 @@ struct BuildState {
     uint2 *prep_tot = nullptr;
     uint2 *chunks = nullptr;                     // (slot, large rank)
     uint32_t *hist = nullptr;                    // per large node 3 x 96
+    uint32_t *done = nullptr;                    // per large node: chunks finished
     // references (ping-pong)
     uint32_t *refs[2] = {nullptr, nullptr};
     uint32_t *ref_node[2] = {nullptr, nullptr};

@@ -45,15 +45,16 @@ cudaError_t launch_transform(const float4 *rest, const uint32_t *part, uint32_t 
                              float4 *out, uint32_t *box_ord, cudaStream_t s);
 cudaError_t launch_box_finish(const uint32_t *box_ord, float *box, cudaStream_t s);
 cudaError_t launch_box(const float4 *verts, uint32_t nv, uint32_t *box_ord, float *box, cudaStream_t s);
-cudaError_t launch_camera_rays(const float *cam16_dev, uint32_t w, uint32_t h, float4 *rays, cudaStream_t s);
+cudaError_t launch_camera_rays(const float *cam16_dev, uint32_t w, uint32_t h, float4 *rays, cudaStream_t s,
+                               bool tiled = false);
 cudaError_t launch_shadow_rays(const float4 *rays, const hk_hit *hits, const TriRec *tris, uint32_t npix,
                                const float *lights_dev, uint32_t nl, float4 *srays, uint32_t *slot,
                                uint32_t *spix, uint32_t *scount, cudaStream_t s);
 cudaError_t launch_shade_cpu(const float4 *rays, const hk_hit *hits, const TriRec *tris, uint32_t npix,
                              const float *lights_dev, uint32_t nl, const uint32_t *slot, const hk_hit *shits,
-                             uint32_t *rgba, cudaStream_t s);
+                             uint32_t *rgba, cudaStream_t s, uint32_t w = 0, bool tiled = false);
 cudaError_t launch_hit4(const hk_hit *hits, const TriRec *tris, uint32_t n, float4 *hit4, cudaStream_t s);
 cudaError_t launch_shade_picture(const float4 *rays, const float4 *hit4, uint32_t n, const float *lights_dev,
-                                 uint32_t nl, uint32_t *rgba, cudaStream_t s);
+                                 uint32_t nl, uint32_t *rgba, cudaStream_t s, uint32_t w = 0, bool tiled = false);
 
 }  // namespace hk

@@ -184,10 +184,21 @@ cudaError_t launch_box(const float4 *verts, uint32_t nv, uint32_t *box_ord, floa
 // primary rays: castRay (GLVisitorCPUTrace.cpp:201-216) with IEEE normalise:
 // dir = ((lowerLeft + vertical * x/W) + horizontal * y/H) - from
 // ---------------------------------------------------------------------------
-__global__ void k_camera_rays(const float *__restrict__ cam, uint32_t w, uint32_t h, float4 *__restrict__ rays) {
+// Ray order: row-major, or 8x4-pixel tiles (one warp batch per tile, for
+// coherent traversal) when the image divides into tiles.
+__device__ __forceinline__ uint32_t pixel_of(uint32_t i, uint32_t w, bool tiled) {
+    if (!tiled) return i;
+    uint32_t tile = i >> 5, j = i & 31u, tiles_x = w >> 3;
+    uint32_t x = (tile % tiles_x) * 8u + (j & 7u), y = (tile / tiles_x) * 4u + (j >> 3);
+    return y * w + x;
+}
+
+__global__ void k_camera_rays(const float *__restrict__ cam, uint32_t w, uint32_t h, float4 *__restrict__ rays,
+                              bool tiled) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= w * h) return;
-    uint32_t x = i % w, y = i / w;
+    uint32_t pix = pixel_of(i, w, tiled);
+    uint32_t x = pix % w, y = pix / w;
     float u = __fdiv_rn((float)x, (float)w), v = __fdiv_rn((float)y, (float)h);
     float4 from = make_float4(cam[0], cam[1], cam[2], cam[3]);
     float d[4];
@@ -201,9 +212,10 @@ __global__ void k_camera_rays(const float *__restrict__ cam, uint32_t w, uint32_
     rays[2 * (size_t)i + 1] = dir;
 }
 
-cudaError_t launch_camera_rays(const float *cam16_dev, uint32_t w, uint32_t h, float4 *rays, cudaStream_t s) {
+cudaError_t launch_camera_rays(const float *cam16_dev, uint32_t w, uint32_t h, float4 *rays, cudaStream_t s,
+                               bool tiled) {
     uint32_t n = w * h;
-    if (n) k_camera_rays<<<blocks_for(n, 256), 256, 0, s>>>(cam16_dev, w, h, rays);
+    if (n) k_camera_rays<<<blocks_for(n, 256), 256, 0, s>>>(cam16_dev, w, h, rays, tiled);
     return cudaGetLastError();
 }
 
@@ -290,12 +302,13 @@ __device__ __forceinline__ uint32_t pack_pixel(float4 c) {
 __global__ void k_shade_cpu(const float4 *__restrict__ rays, const hk_hit *__restrict__ hits,
                             const TriRec *__restrict__ tris, uint32_t npix, const float *__restrict__ lights,
                             uint32_t nl, const uint32_t *__restrict__ slot, const hk_hit *__restrict__ shits,
-                            uint32_t *__restrict__ rgba) {
+                            uint32_t *__restrict__ rgba, uint32_t w, bool tiled) {
     uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= npix) return;
     hk_hit h = hits[p];
+    uint32_t pix = pixel_of(p, w, tiled);
     if (h.tri < 0) {
-        rgba[p] = 0u;
+        rgba[pix] = 0u;
         return;
     }
     float4 o = rays[2 * (size_t)p], d = rays[2 * (size_t)p + 1];
@@ -327,13 +340,15 @@ __global__ void k_shade_cpu(const float4 *__restrict__ rays, const hk_hit *__res
             col.w = __fadd_rn(col.w, __fmul_rn(L[3], sc));
         }
     }
-    rgba[p] = pack_pixel(col);
+    rgba[pix] = pack_pixel(col);
 }
 
 cudaError_t launch_shade_cpu(const float4 *rays, const hk_hit *hits, const TriRec *tris, uint32_t npix,
                              const float *lights_dev, uint32_t nl, const uint32_t *slot, const hk_hit *shits,
-                             uint32_t *rgba, cudaStream_t s) {
-    if (npix) k_shade_cpu<<<blocks_for(npix, 256), 256, 0, s>>>(rays, hits, tris, npix, lights_dev, nl, slot, shits, rgba);
+                             uint32_t *rgba, cudaStream_t s, uint32_t w, bool tiled) {
+    if (npix)
+        k_shade_cpu<<<blocks_for(npix, 256), 256, 0, s>>>(rays, hits, tris, npix, lights_dev, nl, slot, shits, rgba,
+                                                         w, tiled);
     return cudaGetLastError();
 }
 
@@ -369,7 +384,8 @@ __device__ __forceinline__ uint32_t unorm8(float x) {
 }
 
 __global__ void k_shade_picture(const float4 *__restrict__ rays, const float4 *__restrict__ hit4, uint32_t n,
-                                const float *__restrict__ lights, uint32_t nl, uint32_t *__restrict__ rgba) {
+                                const float *__restrict__ lights, uint32_t nl, uint32_t *__restrict__ rgba,
+                                uint32_t w, bool tiled) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     float4 col = make_float4(0.1f, 0.1f, 0.1f, 0.0f);
@@ -397,12 +413,12 @@ __global__ void k_shade_picture(const float4 *__restrict__ rays, const float4 *_
             col.w = __fadd_rn(col.w, __fmul_rn(L[3], sc));
         }
     }
-    rgba[i] = unorm8(col.x) | (unorm8(col.y) << 8) | (unorm8(col.z) << 16) | (unorm8(col.w) << 24);
+    rgba[pixel_of(i, w, tiled)] = unorm8(col.x) | (unorm8(col.y) << 8) | (unorm8(col.z) << 16) | (unorm8(col.w) << 24);
 }
 
 cudaError_t launch_shade_picture(const float4 *rays, const float4 *hit4, uint32_t n, const float *lights_dev,
-                                 uint32_t nl, uint32_t *rgba, cudaStream_t s) {
-    if (n) k_shade_picture<<<blocks_for(n, 256), 256, 0, s>>>(rays, hit4, n, lights_dev, nl, rgba);
+                                 uint32_t nl, uint32_t *rgba, cudaStream_t s, uint32_t w, bool tiled) {
+    if (n) k_shade_picture<<<blocks_for(n, 256), 256, 0, s>>>(rays, hit4, n, lights_dev, nl, rgba, w ? w : n, tiled);
     return cudaGetLastError();
 }
 

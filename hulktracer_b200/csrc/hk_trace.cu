@@ -71,249 +71,288 @@ __device__ __forceinline__ uint32_t sentinel_to_root(const uint2 *nodes, uint32_
 }
 
 // ---------------------------------------------------------------------------
-// ring short stack: KDTreeCPU::searchKDTreeStackless (KDTreeCPU.cpp:363-447),
-// GPUTrace_shortStack.cl:6-105 and GPUTrace_LDSshortStack.cl:7-105. The ring
-// lives in local memory (SMEM = false) or in shared memory, one column per
-// thread (SMEM = true).
+// persistent driver with per-lane refill
+//
+// Every lane keeps its ray's traversal state across iterations of the warp
+// loop. One iteration runs one "leg" per active lane: pop (or restart at the
+// root), descend to a leaf, test it. A lane whose ray is finished writes its
+// hit and takes a new ray at the next iteration: the warp counts its idle
+// lanes with __ballot_sync, lane 0 takes that many rays with one atomicAdd
+// and each idle lane picks its own by rank. Rays of different cost therefore
+// no longer hold a warp hostage until the slowest of 32 finishes.
 // ---------------------------------------------------------------------------
-template <bool SMEM, bool COUNT>
-__device__ void trace_shortstack(const TraceArgs &A, float3 o, float3 d, float3 inv, float ts, float te,
-                                 float &best, int32_t &best_id, uint32_t &c_nodes, uint32_t &c_refs,
-                                 float *s_s, float *s_e, uint32_t *s_n) {
-    constexpr int kMaxRing = 16;
-    float l_s[SMEM ? 1 : kMaxRing], l_e[SMEM ? 1 : kMaxRing];
-    uint32_t l_n[SMEM ? 1 : kMaxRing];
-    const uint32_t D = A.stack_depth;
-    const uint32_t stride = blockDim.x;
-    const uint32_t tid = threadIdx.x;
-    int size = 0, idx = 0;
-    float tmin = ts, tmax = ts;
-    const uint2 root = A.nodes[0];
-    uint32_t steps = 0;
-    while (tmax < te) {
-        uint32_t cur;
-        uint2 node;
-        if (size == 0) {
-            cur = 0;
-            node = root;
-            tmin = tmax;
-            tmax = te;
-        } else {
-            --size;
-            --idx;
-            if (idx == -1) idx += (int)D;
-            if (SMEM) {
-                tmin = s_s[idx * stride + tid];
-                tmax = s_e[idx * stride + tid];
-                cur = s_n[idx * stride + tid];
-            } else {
-                tmin = l_s[idx];
-                tmax = l_e[idx];
-                cur = l_n[idx];
-            }
-            node = A.nodes[cur];
-        }
-        while (!is_leaf(node)) {
-            if (COUNT) c_nodes++;
-            if (++steps > A.max_steps) {
-                atomicOr(A.err, 1u);
-                return;
-            }
-            uint32_t axis = node.x & 3u, pair = node.x >> 2;
-            float pl = __int_as_float(node.y);
-            float rs = comp(o, axis), dc = comp(d, axis);
-            float split = __fmul_rn(__fsub_rn(pl, rs), comp(inv, axis));
-            bool below_first = (rs < pl) || (rs == pl && dc <= 0.0f);
-            if (split >= tmax || split <= 0.0f) {
-                pick_child(A.nodes, pair, below_first, cur, node, root);
-            } else if (split <= tmin) {
-                pick_child(A.nodes, pair, !below_first, cur, node, root);
-            } else {
-                uint32_t second = sentinel_to_root(A.nodes, below_first ? pair + 1 : pair);
-                if (SMEM) {
-                    s_s[idx * stride + tid] = split;
-                    s_e[idx * stride + tid] = tmax;
-                    s_n[idx * stride + tid] = second;
-                } else {
-                    l_s[idx] = split;
-                    l_e[idx] = tmax;
-                    l_n[idx] = second;
-                }
-                idx = (idx + 1) % (int)D;
-                size++;
-                size = size > (int)D ? (int)D : size;
-                pick_child(A.nodes, pair, below_first, cur, node, root);
-                tmax = split;
-            }
-            if (cur == 0) break;
-        }
-        if (is_leaf(node)) {
-            if (COUNT) c_nodes++;
-            test_leaf<COUNT>(A, node, o, d, best, best_id, c_refs);
-            if (best < tmax) break;
-        }
-    }
-}
+struct LaneState {
+    float3 o, d, inv;
+    float te, tmin, tmax, best;
+    int32_t best_id;
+    uint32_t cur;
+    uint2 node;
+    int size, idx;     // ring (short stack) / todo count (full stack)
+    uint32_t ray;
+};
 
-// ---------------------------------------------------------------------------
-// full stack: KDTreeCPU::searchKDTree (KDTreeCPU.cpp:285-361) == GPUTrace.cl:
-// 6-90. Far children are pushed only when they exist.
-// ---------------------------------------------------------------------------
-template <bool COUNT>
-__device__ void trace_fullstack(const TraceArgs &A, float3 o, float3 d, float3 inv, float ts, float te,
-                                float &best, int32_t &best_id, uint32_t &c_nodes, uint32_t &c_refs) {
-    constexpr int kMaxStack = 64;
-    float st_s[kMaxStack], st_e[kMaxStack];
-    uint32_t st_n[kMaxStack];
-    int todo = 0;
-    float tmin = ts, tmax = te;
-    const uint2 root = A.nodes[0];
-    uint32_t cur = 0;
-    uint2 node = root;
-    uint32_t steps = 0;
-    do {
-        if (best < tmin) break;
+// one leg of the ring short stack (KDTreeCPU::searchKDTreeStackless,
+// KDTreeCPU.cpp:363-447; GPUTrace_shortStack.cl:6-105; GPUTrace_LDSshortStack.cl:
+// 7-105 with the ring in shared memory, one column per thread); true = finished
+template <bool SMEM, bool COUNT>
+__device__ __forceinline__ bool leg_shortstack(const TraceArgs &A, LaneState &L, uint2 root, float *s_s, float *s_e,
+                                               uint32_t *s_n, float *l_s, float *l_e, uint32_t *l_n,
+                                               uint32_t &c_nodes, uint32_t &c_refs, uint32_t &steps) {
+    const uint32_t D = A.stack_depth, stride = blockDim.x, tid = threadIdx.x;
+    if (!(L.tmax < L.te)) return true;
+    if (L.size == 0) {
+        L.cur = 0;
+        L.node = root;
+        L.tmin = L.tmax;
+        L.tmax = L.te;
+    } else {
+        --L.size;
+        --L.idx;
+        if (L.idx == -1) L.idx += (int)D;
+        if (SMEM) {
+            L.tmin = s_s[L.idx * stride + tid];
+            L.tmax = s_e[L.idx * stride + tid];
+            L.cur = s_n[L.idx * stride + tid];
+        } else {
+            L.tmin = l_s[L.idx];
+            L.tmax = l_e[L.idx];
+            L.cur = l_n[L.idx];
+        }
+        L.node = A.nodes[L.cur];
+    }
+    while (!is_leaf(L.node)) {
         if (COUNT) c_nodes++;
         if (++steps > A.max_steps) {
             atomicOr(A.err, 1u);
-            return;
+            return true;
         }
-        if (is_leaf(node)) {
-            test_leaf<COUNT>(A, node, o, d, best, best_id, c_refs);
-            cur = 0;
+        uint32_t axis = L.node.x & 3u, pair = L.node.x >> 2;
+        float pl = __int_as_float(L.node.y);
+        float rs = comp(L.o, axis), dc = comp(L.d, axis);
+        float split = __fmul_rn(__fsub_rn(pl, rs), comp(L.inv, axis));
+        bool below_first = (rs < pl) || (rs == pl && dc <= 0.0f);
+        if (split >= L.tmax || split <= 0.0f) {
+            pick_child(A.nodes, pair, below_first, L.cur, L.node, root);
+        } else if (split <= L.tmin) {
+            pick_child(A.nodes, pair, !below_first, L.cur, L.node, root);
         } else {
-            uint32_t axis = node.x & 3u, pair = node.x >> 2;
-            float pl = __int_as_float(node.y);
-            float rs = comp(o, axis), dc = comp(d, axis);
-            float split = __fmul_rn(__fsub_rn(pl, rs), comp(inv, axis));
-            bool below_first = (rs < pl) || (rs == pl && dc <= 0.0f);
-            if (split > tmax || split <= 0.0f) {
-                pick_child(A.nodes, pair, below_first, cur, node, root);
-            } else if (split < tmin) {
-                pick_child(A.nodes, pair, !below_first, cur, node, root);
+            uint32_t second = sentinel_to_root(A.nodes, below_first ? pair + 1 : pair);
+            if (SMEM) {
+                s_s[L.idx * stride + tid] = split;
+                s_e[L.idx * stride + tid] = L.tmax;
+                s_n[L.idx * stride + tid] = second;
             } else {
-                uint32_t second = sentinel_to_root(A.nodes, below_first ? pair + 1 : pair);
-                if (second != 0 && todo < kMaxStack) {
-                    st_n[todo] = second;
-                    st_s[todo] = split;
-                    st_e[todo] = tmax;
-                    todo++;
-                }
-                pick_child(A.nodes, pair, below_first, cur, node, root);
-                tmax = split;
+                l_s[L.idx] = split;
+                l_e[L.idx] = L.tmax;
+                l_n[L.idx] = second;
             }
+            L.idx = (L.idx + 1) % (int)D;
+            L.size++;
+            L.size = L.size > (int)D ? (int)D : L.size;
+            pick_child(A.nodes, pair, below_first, L.cur, L.node, root);
+            L.tmax = split;
         }
-        if (cur == 0 && todo > 0) {
-            todo--;
-            tmin = st_s[todo];
-            tmax = st_e[todo];
-            cur = st_n[todo];
-            node = A.nodes[cur];
-        }
-    } while (cur != 0);
+        if (L.cur == 0) break;
+    }
+    if (is_leaf(L.node)) {
+        if (COUNT) c_nodes++;
+        test_leaf<COUNT>(A, L.node, L.o, L.d, L.best, L.best_id, c_refs);
+        if (L.best < L.tmax) return true;
+    }
+    return false;
 }
 
-// ---------------------------------------------------------------------------
-// kd-restart: GPUTrace_stackless.cl:53-117 with every leaf resident. The
-// ThreadContext starts zeroed, so the first descent runs with tmin = tmax = 0;
-// EARLY adds the exit the resume path performs (closest hit before tmax).
-// ---------------------------------------------------------------------------
-template <bool EARLY, bool COUNT>
-__device__ void trace_restart(const TraceArgs &A, float3 o, float3 d, float3 inv, float te, float &best,
-                              int32_t &best_id, uint32_t &c_nodes, uint32_t &c_refs) {
-    float tmax = 0.0f, tmin = 0.0f;
-    const uint2 root = A.nodes[0];
-    uint32_t steps = 0;
-    while (tmax < te) {
-        tmin = tmax;
-        tmax = te;
-        uint32_t cur = 0;
-        uint2 node = root;
-        while (!is_leaf(node)) {
-            if (COUNT) c_nodes++;
-            if (++steps > A.max_steps) {
-                atomicOr(A.err, 1u);
-                return;
-            }
-            uint32_t axis = node.x & 3u, pair = node.x >> 2;
-            float pl = __int_as_float(node.y);
-            float rs = comp(o, axis), dc = comp(d, axis);
-            float split = __fmul_rn(__fsub_rn(pl, rs), comp(inv, axis));
+// one leg of the full stack (KDTreeCPU::searchKDTree, KDTreeCPU.cpp:285-361 ==
+// GPUTrace.cl:6-90; far children pushed only when they exist), run until a leaf
+// has been tested; true = finished
+template <bool COUNT>
+__device__ __forceinline__ bool leg_fullstack(const TraceArgs &A, LaneState &L, uint2 root, float *st_s, float *st_e,
+                                              uint32_t *st_n, int max_stack, uint32_t &c_nodes, uint32_t &c_refs,
+                                              uint32_t &steps) {
+    while (true) {
+        if (L.best < L.tmin) return true;
+        if (COUNT) c_nodes++;
+        if (++steps > A.max_steps) {
+            atomicOr(A.err, 1u);
+            return true;
+        }
+        bool tested = false;
+        if (is_leaf(L.node)) {
+            test_leaf<COUNT>(A, L.node, L.o, L.d, L.best, L.best_id, c_refs);
+            L.cur = 0;
+            tested = true;
+        } else {
+            uint32_t axis = L.node.x & 3u, pair = L.node.x >> 2;
+            float pl = __int_as_float(L.node.y);
+            float rs = comp(L.o, axis), dc = comp(L.d, axis);
+            float split = __fmul_rn(__fsub_rn(pl, rs), comp(L.inv, axis));
             bool below_first = (rs < pl) || (rs == pl && dc <= 0.0f);
-            if (split >= tmax || split <= 0.0f) {
-                pick_child(A.nodes, pair, below_first, cur, node, root);
-            } else if (split <= tmin) {
-                pick_child(A.nodes, pair, !below_first, cur, node, root);
+            if (split > L.tmax || split <= 0.0f) {
+                pick_child(A.nodes, pair, below_first, L.cur, L.node, root);
+            } else if (split < L.tmin) {
+                pick_child(A.nodes, pair, !below_first, L.cur, L.node, root);
             } else {
-                pick_child(A.nodes, pair, below_first, cur, node, root);
-                tmax = split;
+                uint32_t second = sentinel_to_root(A.nodes, below_first ? pair + 1 : pair);
+                if (second != 0 && L.size < max_stack) {
+                    st_n[L.size] = second;
+                    st_s[L.size] = split;
+                    st_e[L.size] = L.tmax;
+                    L.size++;
+                }
+                pick_child(A.nodes, pair, below_first, L.cur, L.node, root);
+                L.tmax = split;
             }
-            if (cur == 0) break;
         }
-        if (is_leaf(node)) {
-            if (COUNT) c_nodes++;
-            test_leaf<COUNT>(A, node, o, d, best, best_id, c_refs);
-            if (EARLY && best < tmax) break;
+        if (L.cur == 0 && L.size > 0) {
+            L.size--;
+            L.tmin = st_s[L.size];
+            L.tmax = st_e[L.size];
+            L.cur = st_n[L.size];
+            L.node = A.nodes[L.cur];
         }
+        if (L.cur == 0) return true;
+        if (tested) return false;
     }
 }
 
-// ---------------------------------------------------------------------------
-// persistent driver
-// ---------------------------------------------------------------------------
+// one leg of kd-restart (GPUTrace_stackless.cl:53-117 with every leaf resident;
+// EARLY adds the resume path's exit once the closest hit precedes tmax); true = finished
+template <bool EARLY, bool COUNT>
+__device__ __forceinline__ bool leg_restart(const TraceArgs &A, LaneState &L, uint2 root, uint32_t &c_nodes,
+                                            uint32_t &c_refs, uint32_t &steps) {
+    if (!(L.tmax < L.te)) return true;
+    L.tmin = L.tmax;
+    L.tmax = L.te;
+    L.cur = 0;
+    L.node = root;
+    while (!is_leaf(L.node)) {
+        if (COUNT) c_nodes++;
+        if (++steps > A.max_steps) {
+            atomicOr(A.err, 1u);
+            return true;
+        }
+        uint32_t axis = L.node.x & 3u, pair = L.node.x >> 2;
+        float pl = __int_as_float(L.node.y);
+        float rs = comp(L.o, axis), dc = comp(L.d, axis);
+        float split = __fmul_rn(__fsub_rn(pl, rs), comp(L.inv, axis));
+        bool below_first = (rs < pl) || (rs == pl && dc <= 0.0f);
+        if (split >= L.tmax || split <= 0.0f) {
+            pick_child(A.nodes, pair, below_first, L.cur, L.node, root);
+        } else if (split <= L.tmin) {
+            pick_child(A.nodes, pair, !below_first, L.cur, L.node, root);
+        } else {
+            pick_child(A.nodes, pair, below_first, L.cur, L.node, root);
+            L.tmax = split;
+        }
+        if (L.cur == 0) break;
+    }
+    if (is_leaf(L.node)) {
+        if (COUNT) c_nodes++;
+        test_leaf<COUNT>(A, L.node, L.o, L.d, L.best, L.best_id, c_refs);
+        if (EARLY && L.best < L.tmax) return true;
+    }
+    return false;
+}
+
 template <int VARIANT, bool COUNT>
-__global__ void __launch_bounds__(1024) k_trace(TraceArgs A) {
+__global__ void __launch_bounds__(128, 10) k_trace(TraceArgs A) {
     extern __shared__ float smem[];
+    const bool smem_ring = (VARIANT == HK_TRACE_SMEMSTACK);
     float *s_s = smem;
     float *s_e = smem + A.stack_depth * blockDim.x;
     uint32_t *s_n = reinterpret_cast<uint32_t *>(smem + 2 * A.stack_depth * blockDim.x);
+    constexpr int kLocal = (VARIANT == HK_TRACE_FULLSTACK) ? 64 : ((VARIANT == HK_TRACE_SHORTSTACK) ? 16 : 1);
+    float l_s[kLocal], l_e[kLocal];
+    uint32_t l_n[kLocal];
     const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t lt_mask = (1u << lane) - 1u;
     uint32_t c_nodes = 0, c_refs = 0;
     const uint32_t n = A.n_dev ? *A.n_dev : A.n;
     const float bmin[3] = {A.box[0], A.box[1], A.box[2]};
     const float bmax[3] = {A.box[4], A.box[5], A.box[6]};
+    const uint2 root = A.nodes[0];
+    LaneState L;
+    bool active = false, drained = false;
+    uint32_t steps = 0;
     while (true) {
-        uint32_t base = 0;
-        if (lane == 0) base = atomicAdd(A.fetch, 32u);
-        base = __shfl_sync(0xffffffffu, base, 0);
-        if (base >= n) break;
-        uint32_t i = base + lane;
-        if (i >= n) continue;
-        float4 ro = A.rays[2 * (size_t)i], rd = A.rays[2 * (size_t)i + 1];
-        float3 o = make_float3(ro.x, ro.y, ro.z), d = make_float3(rd.x, rd.y, rd.z);
-        float best = kInf;
-        int32_t best_id = -1;
+        // refill idle lanes
+        uint32_t idle = __ballot_sync(0xffffffffu, !active);
+        if (idle && !drained) {
+            uint32_t want = __popc(idle);
+            uint32_t base = 0;
+            if (lane == 0) base = atomicAdd(A.fetch, want);
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if (base + want >= n) drained = true;
+            if (!active) {
+                uint32_t rid = base + __popc(idle & lt_mask);
+                if (rid < n) {
+                    float4 ro = A.rays[2 * (size_t)rid], rd = A.rays[2 * (size_t)rid + 1];
+                    L.o = make_float3(ro.x, ro.y, ro.z);
+                    L.d = make_float3(rd.x, rd.y, rd.z);
+                    L.ray = rid;
+                    L.best = kInf;
+                    L.best_id = -1;
+                    steps = 0;
+                    if (VARIANT == HK_TRACE_BRUTE) {
+                        active = true;
+                    } else {
+                        float ts = 0.0f, te = kInf;
+                        if (ray_box(bmin, bmax, L.o, L.d, ts, te)) {
+                            // invDir = 1 / rayDir (KDTreeCPU.cpp:293): correctly rounded reciprocal
+                            L.inv = make_float3(__frcp_rn(L.d.x), __frcp_rn(L.d.y), __frcp_rn(L.d.z));
+                            L.te = te;
+                            L.size = 0;
+                            L.idx = 0;
+                            if (VARIANT == HK_TRACE_FULLSTACK) {
+                                L.tmin = ts;
+                                L.tmax = te;
+                                L.cur = 0;
+                                L.node = root;
+                            } else if (VARIANT == HK_TRACE_RESTART || VARIANT == HK_TRACE_RESTART_EARLY) {
+                                L.tmin = 0.0f;   // ThreadContext starts zeroed (GPUTrace_stackless.cl:98-100)
+                                L.tmax = 0.0f;
+                            } else {
+                                L.tmin = ts;
+                                L.tmax = ts;
+                            }
+                            active = true;
+                        } else {
+                            A.hits[rid] = hk_hit{kInf, -1};
+                        }
+                    }
+                }
+            }
+        }
+        if (__ballot_sync(0xffffffffu, active) == 0) {
+            if (drained) break;
+            continue;
+        }
+        if (!active) continue;
+        bool done;
         if (VARIANT == HK_TRACE_BRUTE) {
             // GPUTrace_bruteforce.cl:30-42: every triangle in index order
             for (uint32_t t = 0; t < A.ntris; t++) {
-                float h = isect_tri(&A.tris[t], o, d, best);
-                if (h < best) {
-                    best = h;
-                    best_id = (int32_t)t;
+                float h = isect_tri(&A.tris[t], L.o, L.d, L.best);
+                if (h < L.best) {
+                    L.best = h;
+                    L.best_id = (int32_t)t;
                 }
             }
             if (COUNT) c_refs += A.ntris;
+            done = true;
+        } else if (VARIANT == HK_TRACE_FULLSTACK) {
+            done = leg_fullstack<COUNT>(A, L, root, l_s, l_e, l_n, kLocal, c_nodes, c_refs, steps);
+        } else if (VARIANT == HK_TRACE_RESTART) {
+            done = leg_restart<false, COUNT>(A, L, root, c_nodes, c_refs, steps);
+        } else if (VARIANT == HK_TRACE_RESTART_EARLY) {
+            done = leg_restart<true, COUNT>(A, L, root, c_nodes, c_refs, steps);
         } else {
-            float ts = 0.0f, te = kInf;
-            if (ray_box(bmin, bmax, o, d, ts, te)) {
-                // invDir = 1 / rayDir (KDTreeCPU.cpp:293)
-                float3 inv = make_float3(__fdiv_rn(1.0f, d.x), __fdiv_rn(1.0f, d.y), __fdiv_rn(1.0f, d.z));
-                if (VARIANT == HK_TRACE_SHORTSTACK)
-                    trace_shortstack<false, COUNT>(A, o, d, inv, ts, te, best, best_id, c_nodes, c_refs, s_s, s_e, s_n);
-                else if (VARIANT == HK_TRACE_SMEMSTACK)
-                    trace_shortstack<true, COUNT>(A, o, d, inv, ts, te, best, best_id, c_nodes, c_refs, s_s, s_e, s_n);
-                else if (VARIANT == HK_TRACE_FULLSTACK)
-                    trace_fullstack<COUNT>(A, o, d, inv, ts, te, best, best_id, c_nodes, c_refs);
-                else if (VARIANT == HK_TRACE_RESTART)
-                    trace_restart<false, COUNT>(A, o, d, inv, te, best, best_id, c_nodes, c_refs);
-                else if (VARIANT == HK_TRACE_RESTART_EARLY)
-                    trace_restart<true, COUNT>(A, o, d, inv, te, best, best_id, c_nodes, c_refs);
-            }
+            done = leg_shortstack<smem_ring, COUNT>(A, L, root, s_s, s_e, s_n, l_s, l_e, l_n, c_nodes, c_refs, steps);
         }
-        hk_hit h;
-        h.t = best;
-        h.tri = best_id;
-        A.hits[i] = h;
+        if (done) {
+            A.hits[L.ray] = hk_hit{L.best, L.best_id};
+            active = false;
+        }
     }
     if (COUNT) {
         atomicAdd(&A.counters[0], (unsigned long long)c_nodes);

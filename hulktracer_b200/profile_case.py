@@ -27,7 +27,7 @@ def main():
     from hulktracer_b200 import scenes
 
     ap = argparse.ArgumentParser()
-    ap.add_argument("--case", default="trace", choices=["trace", "build", "frame"])
+    ap.add_argument("--case", default="trace", choices=["trace", "build", "frame", "breakdown"])
     ap.add_argument("--variant", default="shortstack")
     ap.add_argument("--mode", default="binned", choices=["binned", "learned"])
     ap.add_argument("--reps", type=int, default=3)
@@ -49,6 +49,41 @@ def main():
     elif a.case == "build":
         for _ in range(a.reps):
             st = ctx.build(mode)
+    elif a.case == "breakdown":
+        # device time per stage (CUDA events, no graph), median of reps
+        import json
+        out = torch.zeros(W * H, dtype=torch.int32, device="cuda")
+        stream = torch.cuda.Stream()
+        ctx.set_stream(stream.cuda_stream)
+        rays = torch.from_numpy(ctx.camera_rays(sc.camera, W, H)).cuda()
+        rays = rays.reshape(H // 4, 4, W // 8, 8, 8).permute(0, 2, 1, 3, 4).reshape(-1, 8).contiguous()
+        hits = torch.zeros(2 * W * H, dtype=torch.int32, device="cuda")
+        v = hk.VARIANTS[a.variant]
+        res = {}
+
+        def timed(name, fn, reps=10):
+            ts = []
+            for _ in range(reps):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                fn()
+                e1.record(stream)
+                stream.synchronize()
+                ts.append(e0.elapsed_time(e1))
+            res[name] = sorted(ts)[len(ts) // 2]
+
+        mats = scenes.part_matrices(sc, 2)
+        with torch.cuda.stream(stream):
+            timed("transform+precompute", lambda: ctx.transform(mats))
+            timed("build", lambda: ctx.L.hk_build(ctx.h, mode, None))
+            timed("trace_primary", lambda: ctx.trace_device(rays.data_ptr(), W * H, hits.data_ptr(), v))
+            timed("render(primary+shadow+shade)", lambda: ctx.render_device(sc.camera, sc.lights, W, H, out.data_ptr(), v))
+            timed("frame_graph", lambda: ctx.frame(mats, sc.camera, sc.lights, W, H, out.data_ptr(), mode, v, True))
+            timed("frame_nograph", lambda: ctx.frame(mats, sc.camera, sc.lights, W, H, out.data_ptr(), mode, v, False))
+        p_, s_ = ctx.ray_counts()
+        res["rays"] = {"primary": p_, "shadow": s_}
+        res["tree"] = ctx.stats()
+        print(json.dumps(res))
     else:
         out = torch.zeros(W * H, dtype=torch.int32, device="cuda")
         for f in range(a.reps):
