@@ -317,8 +317,8 @@ def animated_parts(seed: int = 3, width: int = 1280, height: int = 720, n_parts:
     vs, ts, parts, centers = [], [], [], []
     for p in range(n_parts):
         v, t = prims[p % 3]
-        size = rng.uniform(1.0, 2.5) * scale
-        c = rng.uniform([-18, -8, -18], [18, 8, 18]) * scale
+        size = rng.uniform(2.5, 4.0) * scale
+        c = rng.uniform([-12, -6, -12], [12, 6, 12]) * scale
         vs.append(v * size + c)
         ts.append(t)
         parts.append(np.full(v.shape[0], p, dtype=np.uint32))
@@ -328,9 +328,9 @@ def animated_parts(seed: int = 3, width: int = 1280, height: int = 720, n_parts:
     axis /= np.linalg.norm(axis, axis=1, keepdims=True)
     omega = rng.uniform(0.1, 1.0, size=n_parts)
     drift = rng.uniform(-0.05, 0.05, size=(n_parts, 3))
-    cam = look_at_camera((0.0, 14.0, 48.0) if scale == 1.0 else (0.0, 14.0 * scale, 48.0 * scale),
-                         (0.0, 0.0, 0.0), 60.0, width, height)
-    lights = np.stack([point_light((25.0 * scale, 40.0 * scale, 30.0 * scale))])
+    # parts fill about three quarters of the view
+    cam = look_at_camera((0.0, 7.0 * scale, 20.0 * scale), (0.0, 0.0, 0.0), 60.0, width, height)
+    lights = np.stack([point_light((20.0 * scale, 30.0 * scale, 25.0 * scale))])
     sc = Scene(V, T, lights, cam, width, height, name="animated_parts_200k",
                part_of_vertex=np.concatenate(parts), rest_verts=V.copy(),
                part_center=np.asarray(centers), part_axis=axis, part_omega=omega, part_drift=drift)
