@@ -47,7 +47,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="animated", choices=["animated", "static_small", "static_large"])
     ap.add_argument("--mode", default="binned", choices=["binned", "learned"])
-    ap.add_argument("--variant", default="shortstack")
+    ap.add_argument("--variant", default="ropes")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-frames", type=int, default=2)
     return ap.parse_args()

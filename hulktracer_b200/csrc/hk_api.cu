@@ -70,6 +70,11 @@ struct hk_ctx {
     bool tree_on_device_counts = false;  // its sizes still live in device memory
     hk_tree_stats stats{};
     BuildState build;
+    // ropes of an imported tree (computed on the host when first needed)
+    std::vector<uint2> host_nodes;
+    DevBuf<uint32_t> imp_ropes;
+    DevBuf<float4> imp_cbox;
+    bool imp_ropes_valid = false;
     // trace scratch
     DevBuf<uint32_t> fetch;
     DevBuf<unsigned long long> counters;
@@ -195,7 +200,7 @@ hk_status hk_destroy(hk_ctx *c) {
     if (c->graph) cudaGraphDestroy(c->graph);
     c->verts.release(); c->rest.release(); c->tris.release(); c->part.release(); c->mats.release();
     c->box.release(); c->box_ord.release(); c->rec.release(); c->cache_tmp.release();
-    c->nodes.release(); c->refs.release(); c->fetch.release(); c->counters.release(); c->errw.release();
+    c->nodes.release(); c->refs.release(); c->imp_ropes.release(); c->imp_cbox.release(); c->fetch.release(); c->counters.release(); c->errw.release();
     c->rays.release(); c->hits.release(); c->cam.release(); c->lights.release();
     c->srays.release(); c->shits.release(); c->slot.release(); c->spix.release(); c->scount.release();
     c->hit4.release(); c->rgba.release();
@@ -284,6 +289,7 @@ hk_status hk_scene_set_box(hk_ctx *c, const float *box8) {
     cudaSetDevice(c->device);
     memcpy(c->hbox, box8, 32);
     c->box_user = true;
+    c->imp_ropes_valid = false;
     HK_CUDA(c, cudaMemcpyAsync(c->box.p, c->hbox, 32, cudaMemcpyHostToDevice, c->stream));
     HK_CUDA(c, cudaStreamSynchronize(c->stream));
     return HK_OK;
@@ -445,6 +451,8 @@ hk_status hk_tree_import(hk_ctx *c, const uint32_t *nodes4, uint32_t nn, const u
     c->nr = nr;
     c->tree_valid = true;
     c->tree_built = false;
+    c->host_nodes.swap(out);
+    c->imp_ropes_valid = false;
     c->tree_on_device_counts = false;
     memset(&c->stats, 0, sizeof(c->stats));
     c->stats.nodes = c->nn;
@@ -590,14 +598,71 @@ hk_status hk_build(hk_ctx *c, hk_build_mode mode, hk_tree_stats *stats) {
 // ---------------------------------------------------------------------------
 // tracing
 // ---------------------------------------------------------------------------
+// Ropes and cells of an imported tree: each face of a node's cell points to
+// the node across it (the sibling across the parent's split plane, the
+// parent's rope otherwise); children always follow their parent in the
+// compact order, so one forward pass suffices.
+static hk_status ensure_imported_ropes(hk_ctx *c) {
+    if (c->imp_ropes_valid) return HK_OK;
+    const std::vector<uint2> &N = c->host_nodes;
+    size_t nn = N.size();
+    std::vector<uint32_t> ropes(6 * nn, 0xffffffffu);
+    std::vector<float4> cbox(2 * nn, make_float4(0, 0, 0, 0));
+    cbox[0] = make_float4(c->hbox[0], c->hbox[1], c->hbox[2], 0.0f);
+    cbox[1] = make_float4(c->hbox[4], c->hbox[5], c->hbox[6], 0.0f);
+    auto set = [](float4 &v, uint32_t a, float x) {
+        if (a == 0) v.x = x;
+        else if (a == 1) v.y = x;
+        else v.z = x;
+    };
+    for (size_t i = 0; i < nn; i++) {
+        if (i == 1 || (N[i].x & 3u) == kLeafTag) continue;
+        uint32_t axis = N[i].x & 3u, pair = N[i].x >> 2;
+        float plane;
+        memcpy(&plane, &N[i].y, 4);
+        for (uint32_t ch = 0; ch < 2; ch++) {
+            size_t k = pair + ch;
+            cbox[2 * k] = cbox[2 * i];
+            cbox[2 * k + 1] = cbox[2 * i + 1];
+            for (int f = 0; f < 6; f++) ropes[6 * k + f] = ropes[6 * i + f];
+            if (ch == 0) {
+                set(cbox[2 * k + 1], axis, plane);
+                ropes[6 * k + 2 * axis + 1] = pair + 1;
+            } else {
+                set(cbox[2 * k], axis, plane);
+                ropes[6 * k + 2 * axis] = pair;
+            }
+        }
+    }
+    HK_CUDA(c, c->imp_ropes.ensure(ropes.size()));
+    HK_CUDA(c, c->imp_cbox.ensure(cbox.size()));
+    HK_CUDA(c, cudaMemcpyAsync(c->imp_ropes.p, ropes.data(), ropes.size() * 4, cudaMemcpyHostToDevice, c->stream));
+    HK_CUDA(c, cudaMemcpyAsync(c->imp_cbox.p, cbox.data(), cbox.size() * 16, cudaMemcpyHostToDevice, c->stream));
+    HK_CUDA(c, cudaStreamSynchronize(c->stream));
+    c->imp_ropes_valid = true;
+    return HK_OK;
+}
+
 static hk_status trace_enqueue(hk_ctx *c, const float4 *d_rays, uint32_t n, const uint32_t *n_dev, hk_variant v,
                                hk_hit *d_hits) {
     if ((int)v < HK_TRACE_FULLSTACK || (int)v > HK_TRACE_BRUTE) return fail(c, HK_E_ILLEGAL_INPUT, "variant");
     if (!c->rec_valid) return fail(c, HK_E_STATE, "no triangle cache (hk_precompute or hk_cache_import)");
     if (v != HK_TRACE_BRUTE && !c->tree_valid) return fail(c, HK_E_STATE, "no tree");
-    if (v == HK_TRACE_ROPES) return fail(c, HK_E_ILLEGAL_INPUT, "ropes variant not available");
     TraceLaunch L;
     memset(&L, 0, sizeof(L));
+    if (v == HK_TRACE_ROPES) {
+        if (c->tree_built) {
+            L.ropes = c->build.out_ropes;
+            L.cbox = c->build.out_cbox;
+            L.rope_nn_dev = build_nodes_total_ptr(c->build);
+        } else {
+            hk_status s = ensure_imported_ropes(c);
+            if (s != HK_OK) return s;
+            L.ropes = c->imp_ropes.p;
+            L.cbox = c->imp_cbox.p;
+            L.rope_nn = c->nn;
+        }
+    }
     L.nodes = tree_nodes(c);
     L.refs = tree_refs(c);
     L.tris = c->rec.p;

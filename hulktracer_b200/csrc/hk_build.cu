@@ -306,6 +306,8 @@ struct LevelArgs {
     const uint2 *rscan;
     uint2 *out_nodes;
     uint32_t *out_refs;
+    uint32_t *out_ropes;
+    float4 *out_cbox;
     BuildCounters *ctr;
     LevelCounters *lc, *nlc;
     uint32_t *err;
@@ -338,6 +340,10 @@ __global__ void k_root(LevelArgs A, const float *box, uint32_t nt) {
         A.nx_info[0] = make_uint4(0, nt, 0, 0);
         A.out_nodes[1] = make_uint2(kLeafTag, 0);
         A.out_nodes[0] = make_uint2(kLeafTag, 0);
+        // root cell = scene box, no ropes (every face is the scene boundary)
+        A.out_cbox[0] = A.nx_lo[0];
+        A.out_cbox[1] = A.nx_hi[0];
+        for (int f = 0; f < 6; f++) A.out_ropes[f] = 0xffffffffu;
     }
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nt; i += gridDim.x * blockDim.x) {
         const_cast<uint32_t *>(A.refs)[i] = i;
@@ -505,6 +511,26 @@ struct LoadPlan {
         A.out_nodes[info.z] = make_uint2((pair << 2) | (uint32_t)ax, __float_as_uint(p));
         uint32_t ns = pl.z, co = pl.w;
         float4 lo = A.n_lo[s], hi = A.n_hi[s];
+        {
+            // cells and ropes of both children: the parent's ropes, with the
+            // face on the split plane pointing at the sibling
+            float4 bh = hi, al = lo;
+            s3(bh, ax, p);
+            s3(al, ax, p);
+            A.out_cbox[2 * (size_t)pair] = lo;
+            A.out_cbox[2 * (size_t)pair + 1] = bh;
+            A.out_cbox[2 * (size_t)pair + 2] = al;
+            A.out_cbox[2 * (size_t)pair + 3] = hi;
+            const uint32_t *pr = A.out_ropes + 6 * (size_t)info.z;
+            uint32_t *rb = A.out_ropes + 6 * (size_t)pair, *ra = rb + 6;
+            for (int f = 0; f < 6; f++) {
+                uint32_t r = pr[f];
+                rb[f] = r;
+                ra[f] = r;
+            }
+            rb[2 * ax + 1] = pair + 1;
+            ra[2 * ax] = pair;
+        }
         if (ct.x) {
             float4 h2 = hi;
             s3(h2, ax, p);
@@ -610,12 +636,12 @@ void build_release(BuildState &S) {
     }
     f(S.d_axis); f(S.d_plane); f(S.d_cnt); f(S.plan); f(S.plan_tot); f(S.prep); f(S.prep_tot);
     f(S.chunks); f(S.hist); f(S.done); f(S.rscan); f(S.rscan_tot); f(S.scan_partials); f(S.ctr); f(S.err);
-    f(S.out_nodes); f(S.out_refs);
+    f(S.out_nodes); f(S.out_refs); f(S.out_ropes); f(S.out_cbox);
     S.tb_lo = S.tb_hi = nullptr;
     S.d_axis = nullptr; S.d_plane = nullptr; S.d_cnt = nullptr; S.plan = nullptr; S.plan_tot = nullptr;
     S.prep = nullptr; S.prep_tot = nullptr; S.chunks = nullptr; S.hist = nullptr; S.done = nullptr; S.rscan = nullptr;
     S.rscan_tot = nullptr; S.scan_partials = nullptr; S.ctr = nullptr; S.err = nullptr;
-    S.out_nodes = nullptr; S.out_refs = nullptr;
+    S.out_nodes = nullptr; S.out_refs = nullptr; S.out_ropes = nullptr; S.out_cbox = nullptr;
     S.nt = S.cap_refs = S.cap_nodes = S.cap_level = 0;
     S.active = false;
 }
@@ -669,6 +695,8 @@ hk_status build_prepare(BuildState &S, const BuildParams &p, uint32_t nt, int sm
     bad |= dalloc(S.err, 1) != cudaSuccess;
     bad |= dalloc(S.out_nodes, cap_nodes) != cudaSuccess;
     bad |= dalloc(S.out_refs, cap_refs) != cudaSuccess;
+    bad |= dalloc(S.out_ropes, (size_t)cap_nodes * 6) != cudaSuccess;
+    bad |= dalloc(S.out_cbox, (size_t)cap_nodes * 2) != cudaSuccess;
     if (bad) {
         build_release(S);
         return HK_E_ALLOC;
@@ -705,6 +733,8 @@ cudaError_t build_launch(BuildState &S, const float4 *verts, const uint4 *tris, 
     A.rscan = S.rscan;
     A.out_nodes = S.out_nodes;
     A.out_refs = S.out_refs;
+    A.out_ropes = S.out_ropes;
+    A.out_cbox = S.out_cbox;
     A.ctr = S.ctr;
     A.err = S.err;
     A.ct = S.p.ct;
@@ -748,6 +778,10 @@ cudaError_t build_launch(BuildState &S, const float4 *verts, const uint4 *tris, 
     S.active = true;
     S.last_level = S.p.max_depth + 1;
     return cudaGetLastError();
+}
+
+const uint32_t *build_nodes_total_ptr(const BuildState &S) {
+    return &S.ctr->lvl[S.p.max_depth + 1].nodes_total;
 }
 
 hk_status build_read_stats(BuildState &S, cudaStream_t st, hk_tree_stats *out) {

@@ -84,6 +84,8 @@ struct BuildState {
     // output
     uint2 *out_nodes = nullptr;
     uint32_t *out_refs = nullptr;
+    uint32_t *out_ropes = nullptr;               // 6 per node: -x,+x,-y,+y,-z,+z (0xffffffff = none)
+    float4 *out_cbox = nullptr;                  // 2 per node: cell min, max
     // learned proposer (hk_mlp.cu)
     void *mlp = nullptr;
 };
@@ -93,6 +95,8 @@ hk_status build_ensure_outputs(BuildState &S, BuildOutputs *o);
 cudaError_t build_launch(BuildState &S, const float4 *verts, const uint4 *tris, uint32_t nt, const float *box,
                          cudaStream_t s);
 hk_status build_read_stats(BuildState &S, cudaStream_t s, hk_tree_stats *st);
+// device address of the built tree's node count (valid once build_launch ran)
+const uint32_t *build_nodes_total_ptr(const BuildState &S);
 void build_release(BuildState &S);
 
 }  // namespace hk

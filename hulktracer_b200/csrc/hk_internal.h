@@ -31,6 +31,8 @@ struct TraceLaunch {
     // ropes
     const uint32_t *ropes;      // 6 per node
     const float4 *cbox;         // 2 per node (min, max)
+    uint32_t rope_nn;           // compact node count
+    const uint32_t *rope_nn_dev;
 };
 
 cudaError_t launch_trace(const TraceLaunch &L, cudaStream_t s);

@@ -27,6 +27,10 @@ struct TraceArgs {
     uint32_t *err;            // error word (bounded loops)
     uint32_t stack_depth;     // ring depth for the short-stack variants
     uint32_t max_steps;       // per-ray iteration bound
+    const uint32_t *ropes;    // ropes variant: 6 per node
+    const float4 *cbox;       // ropes variant: cell min, max per node
+    uint32_t rope_nn;         // compact node count (legs bound 4 n + 8) ...
+    const uint32_t *rope_nn_dev;  // ... or its device copy
 };
 
 // ---------------------------------------------------------------------------
@@ -254,6 +258,61 @@ __device__ __forceinline__ bool leg_restart(const TraceArgs &A, LaneState &L, ui
     return false;
 }
 
+// one leg of the ropes traversal (no reference counterpart; restated in the
+// oracle's search_ropes): locate the leaf cell holding o + d*tentry from the
+// current node (ties on a plane go to the side the ray moves into), test it,
+// stop when the closest hit precedes the cell's exit, else follow the rope of
+// the exit face. Legs are bounded by 4 * nodes + 8.
+template <bool COUNT>
+__device__ __forceinline__ bool leg_ropes(const TraceArgs &A, LaneState &L, uint32_t legs_max, uint32_t &c_nodes,
+                                          uint32_t &c_refs) {
+    if (++L.size > (int)legs_max) return true;
+    float p[3] = {__fadd_rn(L.o.x, __fmul_rn(L.d.x, L.tmin)), __fadd_rn(L.o.y, __fmul_rn(L.d.y, L.tmin)),
+                  __fadd_rn(L.o.z, __fmul_rn(L.d.z, L.tmin))};
+    uint2 node = A.nodes[L.cur];
+    while (!is_leaf(node)) {
+        if (COUNT) c_nodes++;
+        uint32_t axis = node.x & 3u, pair = node.x >> 2;
+        float pl = __int_as_float(node.y);
+        float pc = axis == 0 ? p[0] : (axis == 1 ? p[1] : p[2]);
+        bool below = (pc < pl) || (pc == pl && comp(L.d, axis) <= 0.0f);
+        L.cur = below ? pair : pair + 1;
+        node = A.nodes[L.cur];
+    }
+    const float4 blo = A.cbox[2 * (size_t)L.cur], bhi = A.cbox[2 * (size_t)L.cur + 1];
+    float texit = L.te;
+    int face = -1;
+    const float o3[3] = {L.o.x, L.o.y, L.o.z}, d3[3] = {L.d.x, L.d.y, L.d.z}, i3[3] = {L.inv.x, L.inv.y, L.inv.z};
+    const float lo3[3] = {blo.x, blo.y, blo.z}, hi3[3] = {bhi.x, bhi.y, bhi.z};
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        if (d3[k] > 0.0f) {
+            float tt = __fmul_rn(__fsub_rn(hi3[k], o3[k]), i3[k]);
+            if (tt < texit) {
+                texit = tt;
+                face = 2 * k + 1;
+            }
+        } else if (d3[k] < 0.0f) {
+            float tt = __fmul_rn(__fsub_rn(lo3[k], o3[k]), i3[k]);
+            if (tt < texit) {
+                texit = tt;
+                face = 2 * k;
+            }
+        }
+    }
+    if (COUNT) c_nodes++;
+    if (node.y) {
+        test_leaf<COUNT>(A, node, L.o, L.d, L.best, L.best_id, c_refs);
+        if (L.best < texit) return true;
+    }
+    if (face < 0) return true;
+    uint32_t r = A.ropes[6 * (size_t)L.cur + face];
+    if (r == 0xffffffffu) return true;
+    L.tmin = texit > L.tmin ? texit : L.tmin;
+    L.cur = r;
+    return false;
+}
+
 template <int VARIANT, bool COUNT>
 __global__ void __launch_bounds__(128, 10) k_trace(TraceArgs A) {
     extern __shared__ float smem[];
@@ -271,6 +330,7 @@ __global__ void __launch_bounds__(128, 10) k_trace(TraceArgs A) {
     const float bmin[3] = {A.box[0], A.box[1], A.box[2]};
     const float bmax[3] = {A.box[4], A.box[5], A.box[6]};
     const uint2 root = A.nodes[0];
+    const uint32_t legs_max = VARIANT == HK_TRACE_ROPES ? 4u * (A.rope_nn_dev ? *A.rope_nn_dev : A.rope_nn) + 8u : 0u;
     LaneState L;
     bool active = false, drained = false;
     uint32_t steps = 0;
@@ -308,6 +368,9 @@ __global__ void __launch_bounds__(128, 10) k_trace(TraceArgs A) {
                                 L.tmax = te;
                                 L.cur = 0;
                                 L.node = root;
+                            } else if (VARIANT == HK_TRACE_ROPES) {
+                                L.tmin = ts;  // entry distance
+                                L.cur = 0;
                             } else if (VARIANT == HK_TRACE_RESTART || VARIANT == HK_TRACE_RESTART_EARLY) {
                                 L.tmin = 0.0f;   // ThreadContext starts zeroed (GPUTrace_stackless.cl:98-100)
                                 L.tmax = 0.0f;
@@ -342,6 +405,8 @@ __global__ void __launch_bounds__(128, 10) k_trace(TraceArgs A) {
             done = true;
         } else if (VARIANT == HK_TRACE_FULLSTACK) {
             done = leg_fullstack<COUNT>(A, L, root, l_s, l_e, l_n, kLocal, c_nodes, c_refs, steps);
+        } else if (VARIANT == HK_TRACE_ROPES) {
+            done = leg_ropes<COUNT>(A, L, legs_max, c_nodes, c_refs);
         } else if (VARIANT == HK_TRACE_RESTART) {
             done = leg_restart<false, COUNT>(A, L, root, c_nodes, c_refs, steps);
         } else if (VARIANT == HK_TRACE_RESTART_EARLY) {
@@ -386,6 +451,10 @@ cudaError_t launch_trace(const TraceLaunch &L, cudaStream_t s) {
     a.err = L.err;
     a.stack_depth = L.stack_depth;
     a.max_steps = L.max_steps;
+    a.ropes = L.ropes;
+    a.cbox = L.cbox;
+    a.rope_nn = L.rope_nn;
+    a.rope_nn_dev = L.rope_nn_dev;
     cudaError_t e = cudaMemsetAsync(L.fetch, 0, sizeof(uint32_t), s);
     if (e != cudaSuccess) return e;
     if (L.n == 0 && L.n_dev == nullptr) return cudaSuccess;
@@ -399,6 +468,9 @@ cudaError_t launch_trace(const TraceLaunch &L, cudaStream_t s) {
     case HK_TRACE_SMEMSTACK: return launch_v<HK_TRACE_SMEMSTACK>(a, L.count, grid, block, smem, s);
     case HK_TRACE_RESTART: return launch_v<HK_TRACE_RESTART>(a, L.count, grid, block, smem, s);
     case HK_TRACE_RESTART_EARLY: return launch_v<HK_TRACE_RESTART_EARLY>(a, L.count, grid, block, smem, s);
+    case HK_TRACE_ROPES:
+        if (!L.ropes || !L.cbox) return cudaErrorInvalidValue;
+        return launch_v<HK_TRACE_ROPES>(a, L.count, grid, block, smem, s);
     case HK_TRACE_BRUTE: return launch_v<HK_TRACE_BRUTE>(a, L.count, grid, block, smem, s);
     default: return cudaErrorInvalidValue;
     }

@@ -6,7 +6,7 @@ import numpy as np
 import pytest
 
 from hulktracer_b200 import scenes
-from oracle.oracle import NORM_IEEE, SHORTSTACK as O_SHORT
+from oracle.oracle import NORM_IEEE, ROPES as O_ROPES, SHORTSTACK as O_SHORT
 
 pytestmark = pytest.mark.gpu
 
@@ -64,6 +64,31 @@ def test_trace_on_built_tree(ctx, hk, oracle):
     bh = ctx.trace(g["rays"], hk.BRUTE)
     assert np.array_equal(bh["tri"] >= 0, m)
     assert np.array_equal(bh["t"][m], hits["t"][m])
+
+
+def test_ropes_on_built_tree(ctx, hk, oracle):
+    """Ropes written by the GPU builder: the ropes traversal equals the
+    oracle's ropes traversal on the same (identical) tree, and finds the same
+    closest hits as the stack traversal."""
+    g = load("small24k.npz")
+    ctx.upload(g["verts"], g["tris"])
+    ctx.set_box(g["box"])
+    ctx.precompute()
+    ctx.build()
+    cn, cr = ctx.export_compact()
+    cache = ctx.export_cache()
+    hits = ctx.trace(g["rays"], hk.ROPES)
+    nodes = oracle.compact_to_ref(cn)
+    tree = oracle.make_tree(g["verts"], g["tris"], cache, nodes, cr, g["box"])
+    tree.cnodes = np.ascontiguousarray(cn, np.uint32)
+    r, b = oracle.ropes(cn, g["box"])
+    tree.ropes, tree.cbox = r, b
+    oh, oid = oracle.trace(tree, g["rays"], O_ROPES, 6)
+    assert np.array_equal(hits["tri"], oid)
+    m = oid >= 0
+    assert np.array_equal(hits["t"][m], oh[m, 0])
+    sh = ctx.trace(g["rays"], hk.SHORTSTACK)
+    assert np.array_equal(sh["t"], hits["t"])
 
 
 def test_transform_and_box(ctx, oracle):

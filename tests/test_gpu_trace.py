@@ -10,7 +10,7 @@ import numpy as np
 import pytest
 
 from oracle.oracle import (BRUTE as O_BRUTE, FULLSTACK as O_FULL, NORM_IEEE, RESTART as O_RESTART,
-                           RESTART_EARLY as O_RESTART_EARLY, SHORTSTACK as O_SHORT)
+                           RESTART_EARLY as O_RESTART_EARLY, ROPES as O_ROPES, SHORTSTACK as O_SHORT)
 
 pytestmark = pytest.mark.gpu
 
@@ -62,12 +62,14 @@ def test_shortstack5_equals_reference_checkcollision(ctx5, hk, name):
 @pytest.mark.parametrize("name", CASES)
 @pytest.mark.parametrize("variant,ovariant", [("fullstack", O_FULL), ("shortstack", O_SHORT),
                                               ("smemstack", O_SHORT), ("restart", O_RESTART),
-                                              ("restart_early", O_RESTART_EARLY), ("brute", O_BRUTE)])
+                                              ("restart_early", O_RESTART_EARLY), ("brute", O_BRUTE),
+                                              ("ropes", O_ROPES)])
 def test_variant_bit_exact_vs_oracle(ctx6, hk, oracle, name, variant, ovariant):
     g = load(name)
     setup_ref_tree(ctx6, g)
     hits = ctx6.trace(g["rays"], hk.VARIANTS[variant])
-    tree = oracle.make_tree(g["verts"], g["tris"], g["ref_cache"], g["ref_nodes"], g["ref_refs"], g["box"])
+    tree = oracle.make_tree(g["verts"], g["tris"], g["ref_cache"], g["ref_nodes"], g["ref_refs"], g["box"],
+                            with_ropes=(ovariant == O_ROPES))
     oh, oid = oracle.trace(tree, g["rays"], ovariant, 6)
     check_hits(hits, oid, oh[:, 0])
 
@@ -108,7 +110,7 @@ def test_camera_rays_bit_exact(ctx6, oracle):
 
 
 @pytest.mark.parametrize("name", CASES)
-@pytest.mark.parametrize("variant", ["shortstack", "fullstack", "restart_early"])
+@pytest.mark.parametrize("variant", ["shortstack", "fullstack", "restart_early", "ropes"])
 def test_render_cpu_semantics(ctx6, hk, oracle, name, variant):
     """GLVisitorCPUTrace::traceScene semantics (shadow rays, replacePixel):
     equal to the oracle with IEEE normalisation, and within 1/255 of the
@@ -117,8 +119,9 @@ def test_render_cpu_semantics(ctx6, hk, oracle, name, variant):
     setup_ref_tree(ctx6, g)
     w, h = (int(x) for x in g["render_wh"])
     img = ctx6.render(g["camera"], g["lights"], w, h, hk.VARIANTS[variant])
-    ovar = {"shortstack": O_SHORT, "fullstack": O_FULL, "restart_early": O_RESTART_EARLY}[variant]
-    tree = oracle.make_tree(g["verts"], g["tris"], g["ref_cache"], g["ref_nodes"], g["ref_refs"], g["box"])
+    ovar = {"shortstack": O_SHORT, "fullstack": O_FULL, "restart_early": O_RESTART_EARLY, "ropes": O_ROPES}[variant]
+    tree = oracle.make_tree(g["verts"], g["tris"], g["ref_cache"], g["ref_nodes"], g["ref_refs"], g["box"],
+                            with_ropes=(ovar == O_ROPES))
     oimg = oracle.render_cpu(tree, g["render_rays"], w, h, g["lights"], ovar, 6, NORM_IEEE)
     assert np.array_equal(img, oimg)
     a = img.view(np.uint8).reshape(-1, 4)[:, :3].astype(int)
