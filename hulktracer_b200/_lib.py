@@ -95,6 +95,10 @@ def load(path: str = LIB_PATH):
         "hk_get_ray_counts": [vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)],
         "hk_frame_graph_info": [vp, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)],
         "hk_render_noalloc": [vp, vp, vp, u32, f32p, f32p, f32p, u32, u32, u32, C.c_int, vp, vp],
+        "hk_batch_create": [vp, C.POINTER(C.c_void_p)],
+        "hk_batch_destroy": [vp],
+        "hk_batch_add_scene": [vp, f32p, u32, u32p, u32, C.POINTER(C.c_uint32)],
+        "hk_batch_trace_device": [vp, vp, u32p, u32, C.c_int, vp, f32p],
     }
     for name, args in sig.items():
         fn = getattr(L, name)

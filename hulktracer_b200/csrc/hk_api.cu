@@ -950,4 +950,154 @@ hk_status hk_frame_graph_info(hk_ctx *c, uint32_t *kernel_nodes, uint32_t *all_n
     return HK_OK;
 }
 
+// ---------------------------------------------------------------------------
+// batches
+// ---------------------------------------------------------------------------
+}  // extern "C"
+
+struct hk_batch {
+    hk_ctx *ctx;
+    struct Scene {
+        DevBuf<TriRec> rec;
+        DevBuf<uint2> nodes;
+        DevBuf<uint32_t> refs, ropes;
+        DevBuf<float4> cbox;
+        float box[8];
+        uint32_t nn, nr, nt;
+    };
+    std::vector<Scene *> scenes;
+    DevBuf<SceneDesc> table;
+    DevBuf<uint32_t> offsets, remaining;
+    DevBuf<unsigned long long> times;   // [0] start, [1..] per-scene done
+};
+
+extern "C" {
+
+hk_status hk_batch_create(hk_ctx *c, hk_batch **out) {
+    if (!c || !out) return HK_E_ILLEGAL_INPUT;
+    hk_batch *b = new hk_batch();
+    b->ctx = c;
+    *out = b;
+    return HK_OK;
+}
+
+hk_status hk_batch_destroy(hk_batch *b) {
+    if (!b) return HK_E_ILLEGAL_INPUT;
+    cudaSetDevice(b->ctx->device);
+    cudaStreamSynchronize(b->ctx->stream);
+    for (auto *s : b->scenes) {
+        s->rec.release(); s->nodes.release(); s->refs.release(); s->ropes.release(); s->cbox.release();
+        delete s;
+    }
+    b->table.release(); b->offsets.release(); b->remaining.release(); b->times.release();
+    delete b;
+    return HK_OK;
+}
+
+hk_status hk_batch_add_scene(hk_batch *b, const float *verts4, uint32_t nv, const uint32_t *tris4, uint32_t nt,
+                             uint32_t *scene_id) {
+    if (!b || nt == 0) return HK_E_ILLEGAL_INPUT;
+    hk_ctx *c = b->ctx;
+    hk_status st = hk_scene_upload(c, verts4, nv, tris4, nt);
+    if (st != HK_OK) return st;
+    st = hk_precompute(c);
+    if (st != HK_OK) return st;
+    hk_tree_stats ts;
+    st = hk_build(c, HK_BUILD_BINNED, &ts);
+    if (st != HK_OK) return st;
+    auto *s = new hk_batch::Scene();
+    s->nn = ts.nodes;
+    s->nr = ts.refs;
+    s->nt = nt;
+    memcpy(s->box, c->hbox, 32);
+    HK_CUDA(c, s->rec.ensure(nt));
+    HK_CUDA(c, s->nodes.ensure(s->nn));
+    HK_CUDA(c, s->refs.ensure(std::max<uint32_t>(s->nr, 1)));
+    HK_CUDA(c, s->ropes.ensure((size_t)s->nn * 6));
+    HK_CUDA(c, s->cbox.ensure((size_t)s->nn * 2));
+    HK_CUDA(c, cudaMemcpyAsync(s->rec.p, c->rec.p, (size_t)nt * sizeof(TriRec), cudaMemcpyDeviceToDevice, c->stream));
+    HK_CUDA(c, cudaMemcpyAsync(s->nodes.p, c->build.out_nodes, (size_t)s->nn * 8, cudaMemcpyDeviceToDevice, c->stream));
+    if (s->nr)
+        HK_CUDA(c, cudaMemcpyAsync(s->refs.p, c->build.out_refs, (size_t)s->nr * 4, cudaMemcpyDeviceToDevice, c->stream));
+    HK_CUDA(c, cudaMemcpyAsync(s->ropes.p, c->build.out_ropes, (size_t)s->nn * 24, cudaMemcpyDeviceToDevice, c->stream));
+    HK_CUDA(c, cudaMemcpyAsync(s->cbox.p, c->build.out_cbox, (size_t)s->nn * 32, cudaMemcpyDeviceToDevice, c->stream));
+    HK_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (scene_id) *scene_id = (uint32_t)b->scenes.size();
+    b->scenes.push_back(s);
+    return HK_OK;
+}
+
+hk_status hk_batch_trace_device(hk_batch *b, const float *d_rays8, const uint32_t *ray_offsets, uint32_t nscenes,
+                                hk_variant v, hk_hit *d_hits, float *scene_ms) {
+    if (!b || !ray_offsets || !d_rays8 || !d_hits) return HK_E_ILLEGAL_INPUT;
+    hk_ctx *c = b->ctx;
+    if (nscenes == 0 || nscenes != b->scenes.size()) return fail(c, HK_E_ILLEGAL_INPUT, "nscenes != scenes in batch");
+    if ((int)v < HK_TRACE_FULLSTACK || (int)v > HK_TRACE_BRUTE) return fail(c, HK_E_ILLEGAL_INPUT, "variant");
+    if (v == HK_TRACE_SMEMSTACK && c->cfg.short_stack * c->cfg.block_size * 12 > 48 * 1024)
+        return fail(c, HK_E_ILLEGAL_INPUT, "shared ring too large");
+    if (ray_offsets[0] != 0) return fail(c, HK_E_ILLEGAL_INPUT, "ray_offsets[0] must be 0");
+    std::vector<uint32_t> rem(nscenes);
+    for (uint32_t i = 0; i < nscenes; i++) {
+        if (ray_offsets[i + 1] < ray_offsets[i]) return fail(c, HK_E_ILLEGAL_INPUT, "ray_offsets must ascend");
+        rem[i] = ray_offsets[i + 1] - ray_offsets[i];
+    }
+    uint32_t n = ray_offsets[nscenes];
+    cudaSetDevice(c->device);
+    std::vector<SceneDesc> table(nscenes);
+    for (uint32_t i = 0; i < nscenes; i++) {
+        auto *s = b->scenes[i];
+        SceneDesc &d = table[i];
+        memset(&d, 0, sizeof(d));
+        d.nodes = s->nodes.p;
+        d.refs = s->refs.p;
+        d.tris = s->rec.p;
+        d.ropes = s->ropes.p;
+        d.cbox = s->cbox.p;
+        memcpy(d.box, s->box, 32);
+        d.nn = s->nn;
+        d.ntris = s->nt;
+    }
+    HK_CUDA(c, b->table.ensure(nscenes));
+    HK_CUDA(c, b->offsets.ensure(nscenes + 1));
+    HK_CUDA(c, b->remaining.ensure(nscenes));
+    HK_CUDA(c, b->times.ensure(nscenes + 1));
+    HK_CUDA(c, cudaMemcpyAsync(b->table.p, table.data(), nscenes * sizeof(SceneDesc), cudaMemcpyHostToDevice, c->stream));
+    HK_CUDA(c, cudaMemcpyAsync(b->offsets.p, ray_offsets, (nscenes + 1) * 4, cudaMemcpyHostToDevice, c->stream));
+    HK_CUDA(c, cudaMemcpyAsync(b->remaining.p, rem.data(), nscenes * 4, cudaMemcpyHostToDevice, c->stream));
+    HK_CUDA(c, cudaMemsetAsync(b->times.p, 0xff, 8, c->stream));
+    HK_CUDA(c, cudaMemsetAsync(b->times.p + 1, 0, nscenes * 8, c->stream));
+    TraceLaunch L;
+    memset(&L, 0, sizeof(L));
+    L.rays = reinterpret_cast<const float4 *>(d_rays8);
+    L.hits = d_hits;
+    L.n = n;
+    L.fetch = c->fetch.p;
+    L.counters = c->counters.p;
+    L.err = c->errw.p;
+    L.stack_depth = c->cfg.short_stack;
+    L.max_steps = 1u << 26;
+    L.variant = (int)v;
+    L.count = c->counting;
+    L.block = (int)c->cfg.block_size;
+    int per_sm = c->cfg.blocks_per_sm ? (int)c->cfg.blocks_per_sm : std::max(1, 2048 / L.block);
+    L.grid = c->sm_count * per_sm;
+    L.scenes = b->table.p;
+    L.ray_offsets = b->offsets.p;
+    L.nscenes = nscenes;
+    L.remaining = b->remaining.p;
+    L.start_ns = b->times.p;
+    L.done_ns = b->times.p + 1;
+    if (c->counting) HK_CUDA(c, cudaMemsetAsync(c->counters.p, 0, 24, c->stream));
+    HK_CUDA(c, launch_trace(L, c->stream));
+    if (scene_ms) {
+        std::vector<unsigned long long> t(nscenes + 1);
+        HK_CUDA(c, cudaMemcpyAsync(t.data(), b->times.p, (nscenes + 1) * 8, cudaMemcpyDeviceToHost, c->stream));
+        HK_CUDA(c, cudaStreamSynchronize(c->stream));
+        for (uint32_t i = 0; i < nscenes; i++)
+            scene_ms[i] = (t[i + 1] >= t[0]) ? (float)((double)(t[i + 1] - t[0]) * 1e-6) : 0.0f;
+        return check_err_word(c);
+    }
+    return HK_OK;
+}
+
 }  // extern "C"

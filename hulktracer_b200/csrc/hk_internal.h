@@ -10,6 +10,19 @@ namespace hk {
 
 struct TriRec;
 
+// one scene of a batched launch (device table entry)
+struct SceneDesc {
+    const uint2 *nodes;
+    const uint32_t *refs;
+    const TriRec *tris;
+    const uint32_t *ropes;
+    const float4 *cbox;
+    float box[8];
+    uint32_t nn;        // compact nodes (ropes legs bound)
+    uint32_t ntris;
+    uint32_t pad[2];
+};
+
 struct TraceLaunch {
     const uint2 *nodes;
     const uint32_t *refs;
@@ -33,6 +46,13 @@ struct TraceLaunch {
     const float4 *cbox;         // 2 per node (min, max)
     uint32_t rope_nn;           // compact node count
     const uint32_t *rope_nn_dev;
+    // batch mode (scenes != nullptr)
+    const SceneDesc *scenes;
+    const uint32_t *ray_offsets;
+    uint32_t nscenes;
+    uint32_t *remaining;
+    unsigned long long *done_ns;
+    unsigned long long *start_ns;
 };
 
 cudaError_t launch_trace(const TraceLaunch &L, cudaStream_t s);

@@ -31,6 +31,22 @@ struct TraceArgs {
     const float4 *cbox;       // ropes variant: cell min, max per node
     uint32_t rope_nn;         // compact node count (legs bound 4 n + 8) ...
     const uint32_t *rope_nn_dev;  // ... or its device copy
+    // batch mode: many scenes in one launch
+    const SceneDesc *scenes;
+    const uint32_t *ray_offsets;   // nscenes + 1, ascending
+    uint32_t nscenes;
+    uint32_t *remaining;           // rays left per scene
+    unsigned long long *done_ns;   // globaltimer when a scene's last ray finished
+    unsigned long long *start_ns;  // globaltimer at launch start (min over CTAs)
+};
+
+// per-scene arrays a traversal reads
+struct SceneView {
+    const uint2 *nodes;
+    const uint32_t *refs;
+    const TriRec *tris;
+    const uint32_t *ropes;
+    const float4 *cbox;
 };
 
 // ---------------------------------------------------------------------------
@@ -38,7 +54,7 @@ struct TraceArgs {
 // in leaf order, a hit replaces the best only when strictly closer.
 // ---------------------------------------------------------------------------
 template <bool COUNT>
-__device__ __forceinline__ void test_leaf(const TraceArgs &A, uint2 leaf, float3 o, float3 d,
+__device__ __forceinline__ void test_leaf(const SceneView &A, uint2 leaf, float3 o, float3 d,
                                           float &best, int32_t &best_id, uint32_t &c_refs) {
     uint32_t start = leaf.x >> 2, cnt = leaf.y;
     for (uint32_t i = 0; i < cnt; i++) {
@@ -99,7 +115,7 @@ struct LaneState {
 // KDTreeCPU.cpp:363-447; GPUTrace_shortStack.cl:6-105; GPUTrace_LDSshortStack.cl:
 // 7-105 with the ring in shared memory, one column per thread); true = finished
 template <bool SMEM, bool COUNT>
-__device__ __forceinline__ bool leg_shortstack(const TraceArgs &A, LaneState &L, uint2 root, float *s_s, float *s_e,
+__device__ __forceinline__ bool leg_shortstack(const TraceArgs &A, const SceneView &V, LaneState &L, uint2 root, float *s_s, float *s_e,
                                                uint32_t *s_n, float *l_s, float *l_e, uint32_t *l_n,
                                                uint32_t &c_nodes, uint32_t &c_refs, uint32_t &steps) {
     const uint32_t D = A.stack_depth, stride = blockDim.x, tid = threadIdx.x;
@@ -122,7 +138,7 @@ __device__ __forceinline__ bool leg_shortstack(const TraceArgs &A, LaneState &L,
             L.tmax = l_e[L.idx];
             L.cur = l_n[L.idx];
         }
-        L.node = A.nodes[L.cur];
+        L.node = V.nodes[L.cur];
     }
     while (!is_leaf(L.node)) {
         if (COUNT) c_nodes++;
@@ -136,11 +152,11 @@ __device__ __forceinline__ bool leg_shortstack(const TraceArgs &A, LaneState &L,
         float split = __fmul_rn(__fsub_rn(pl, rs), comp(L.inv, axis));
         bool below_first = (rs < pl) || (rs == pl && dc <= 0.0f);
         if (split >= L.tmax || split <= 0.0f) {
-            pick_child(A.nodes, pair, below_first, L.cur, L.node, root);
+            pick_child(V.nodes, pair, below_first, L.cur, L.node, root);
         } else if (split <= L.tmin) {
-            pick_child(A.nodes, pair, !below_first, L.cur, L.node, root);
+            pick_child(V.nodes, pair, !below_first, L.cur, L.node, root);
         } else {
-            uint32_t second = sentinel_to_root(A.nodes, below_first ? pair + 1 : pair);
+            uint32_t second = sentinel_to_root(V.nodes, below_first ? pair + 1 : pair);
             if (SMEM) {
                 s_s[L.idx * stride + tid] = split;
                 s_e[L.idx * stride + tid] = L.tmax;
@@ -153,14 +169,14 @@ __device__ __forceinline__ bool leg_shortstack(const TraceArgs &A, LaneState &L,
             L.idx = (L.idx + 1) % (int)D;
             L.size++;
             L.size = L.size > (int)D ? (int)D : L.size;
-            pick_child(A.nodes, pair, below_first, L.cur, L.node, root);
+            pick_child(V.nodes, pair, below_first, L.cur, L.node, root);
             L.tmax = split;
         }
         if (L.cur == 0) break;
     }
     if (is_leaf(L.node)) {
         if (COUNT) c_nodes++;
-        test_leaf<COUNT>(A, L.node, L.o, L.d, L.best, L.best_id, c_refs);
+        test_leaf<COUNT>(V, L.node, L.o, L.d, L.best, L.best_id, c_refs);
         if (L.best < L.tmax) return true;
     }
     return false;
@@ -170,7 +186,7 @@ __device__ __forceinline__ bool leg_shortstack(const TraceArgs &A, LaneState &L,
 // GPUTrace.cl:6-90; far children pushed only when they exist), run until a leaf
 // has been tested; true = finished
 template <bool COUNT>
-__device__ __forceinline__ bool leg_fullstack(const TraceArgs &A, LaneState &L, uint2 root, float *st_s, float *st_e,
+__device__ __forceinline__ bool leg_fullstack(const TraceArgs &A, const SceneView &V, LaneState &L, uint2 root, float *st_s, float *st_e,
                                               uint32_t *st_n, int max_stack, uint32_t &c_nodes, uint32_t &c_refs,
                                               uint32_t &steps) {
     while (true) {
@@ -182,7 +198,7 @@ __device__ __forceinline__ bool leg_fullstack(const TraceArgs &A, LaneState &L, 
         }
         bool tested = false;
         if (is_leaf(L.node)) {
-            test_leaf<COUNT>(A, L.node, L.o, L.d, L.best, L.best_id, c_refs);
+            test_leaf<COUNT>(V, L.node, L.o, L.d, L.best, L.best_id, c_refs);
             L.cur = 0;
             tested = true;
         } else {
@@ -192,18 +208,18 @@ __device__ __forceinline__ bool leg_fullstack(const TraceArgs &A, LaneState &L, 
             float split = __fmul_rn(__fsub_rn(pl, rs), comp(L.inv, axis));
             bool below_first = (rs < pl) || (rs == pl && dc <= 0.0f);
             if (split > L.tmax || split <= 0.0f) {
-                pick_child(A.nodes, pair, below_first, L.cur, L.node, root);
+                pick_child(V.nodes, pair, below_first, L.cur, L.node, root);
             } else if (split < L.tmin) {
-                pick_child(A.nodes, pair, !below_first, L.cur, L.node, root);
+                pick_child(V.nodes, pair, !below_first, L.cur, L.node, root);
             } else {
-                uint32_t second = sentinel_to_root(A.nodes, below_first ? pair + 1 : pair);
+                uint32_t second = sentinel_to_root(V.nodes, below_first ? pair + 1 : pair);
                 if (second != 0 && L.size < max_stack) {
                     st_n[L.size] = second;
                     st_s[L.size] = split;
                     st_e[L.size] = L.tmax;
                     L.size++;
                 }
-                pick_child(A.nodes, pair, below_first, L.cur, L.node, root);
+                pick_child(V.nodes, pair, below_first, L.cur, L.node, root);
                 L.tmax = split;
             }
         }
@@ -212,7 +228,7 @@ __device__ __forceinline__ bool leg_fullstack(const TraceArgs &A, LaneState &L, 
             L.tmin = st_s[L.size];
             L.tmax = st_e[L.size];
             L.cur = st_n[L.size];
-            L.node = A.nodes[L.cur];
+            L.node = V.nodes[L.cur];
         }
         if (L.cur == 0) return true;
         if (tested) return false;
@@ -222,7 +238,7 @@ __device__ __forceinline__ bool leg_fullstack(const TraceArgs &A, LaneState &L, 
 // one leg of kd-restart (GPUTrace_stackless.cl:53-117 with every leaf resident;
 // EARLY adds the resume path's exit once the closest hit precedes tmax); true = finished
 template <bool EARLY, bool COUNT>
-__device__ __forceinline__ bool leg_restart(const TraceArgs &A, LaneState &L, uint2 root, uint32_t &c_nodes,
+__device__ __forceinline__ bool leg_restart(const TraceArgs &A, const SceneView &V, LaneState &L, uint2 root, uint32_t &c_nodes,
                                             uint32_t &c_refs, uint32_t &steps) {
     if (!(L.tmax < L.te)) return true;
     L.tmin = L.tmax;
@@ -241,18 +257,18 @@ __device__ __forceinline__ bool leg_restart(const TraceArgs &A, LaneState &L, ui
         float split = __fmul_rn(__fsub_rn(pl, rs), comp(L.inv, axis));
         bool below_first = (rs < pl) || (rs == pl && dc <= 0.0f);
         if (split >= L.tmax || split <= 0.0f) {
-            pick_child(A.nodes, pair, below_first, L.cur, L.node, root);
+            pick_child(V.nodes, pair, below_first, L.cur, L.node, root);
         } else if (split <= L.tmin) {
-            pick_child(A.nodes, pair, !below_first, L.cur, L.node, root);
+            pick_child(V.nodes, pair, !below_first, L.cur, L.node, root);
         } else {
-            pick_child(A.nodes, pair, below_first, L.cur, L.node, root);
+            pick_child(V.nodes, pair, below_first, L.cur, L.node, root);
             L.tmax = split;
         }
         if (L.cur == 0) break;
     }
     if (is_leaf(L.node)) {
         if (COUNT) c_nodes++;
-        test_leaf<COUNT>(A, L.node, L.o, L.d, L.best, L.best_id, c_refs);
+        test_leaf<COUNT>(V, L.node, L.o, L.d, L.best, L.best_id, c_refs);
         if (EARLY && L.best < L.tmax) return true;
     }
     return false;
@@ -264,7 +280,7 @@ __device__ __forceinline__ bool leg_restart(const TraceArgs &A, LaneState &L, ui
 // stop when the closest hit precedes the cell's exit, else follow the rope of
 // the exit face. Legs are bounded by 4 * nodes + 8.
 template <bool COUNT>
-__device__ __forceinline__ bool leg_ropes(const TraceArgs &A, LaneState &L, uint32_t legs_max, uint32_t &c_nodes,
+__device__ __forceinline__ bool leg_ropes(const SceneView &A, LaneState &L, uint32_t legs_max, uint32_t &c_nodes,
                                           uint32_t &c_refs) {
     if (++L.size > (int)legs_max) return true;
     float p[3] = {__fadd_rn(L.o.x, __fmul_rn(L.d.x, L.tmin)), __fadd_rn(L.o.y, __fmul_rn(L.d.y, L.tmin)),
@@ -313,7 +329,24 @@ __device__ __forceinline__ bool leg_ropes(const TraceArgs &A, LaneState &L, uint
     return false;
 }
 
-template <int VARIANT, bool COUNT>
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// scene of a ray in a batch: the last s with ray_offsets[s] <= rid
+__device__ __forceinline__ uint32_t scene_of(const uint32_t *off, uint32_t nscenes, uint32_t rid) {
+    uint32_t lo = 0, hi = nscenes;  // invariant off[lo] <= rid < off[hi]
+    while (hi - lo > 1) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (__ldg(&off[mid]) <= rid) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+template <int VARIANT, bool COUNT, bool BATCH>
 __global__ void __launch_bounds__(128, 10) k_trace(TraceArgs A) {
     extern __shared__ float smem[];
     const bool smem_ring = (VARIANT == HK_TRACE_SMEMSTACK);
@@ -327,10 +360,20 @@ __global__ void __launch_bounds__(128, 10) k_trace(TraceArgs A) {
     const uint32_t lt_mask = (1u << lane) - 1u;
     uint32_t c_nodes = 0, c_refs = 0;
     const uint32_t n = A.n_dev ? *A.n_dev : A.n;
-    const float bmin[3] = {A.box[0], A.box[1], A.box[2]};
-    const float bmax[3] = {A.box[4], A.box[5], A.box[6]};
-    const uint2 root = A.nodes[0];
-    const uint32_t legs_max = VARIANT == HK_TRACE_ROPES ? 4u * (A.rope_nn_dev ? *A.rope_nn_dev : A.rope_nn) + 8u : 0u;
+    if (BATCH && threadIdx.x == 0) atomicMin(A.start_ns, global_ns());
+    // scene arrays: launch-uniform for one scene, per lane in a batch
+    SceneView V{A.nodes, A.refs, A.tris, A.ropes, A.cbox};
+    float bmin[3], bmax[3];
+    uint2 root = make_uint2(kLeafTag, 0);
+    uint32_t legs_max = 0, ntris = A.ntris, scene = 0;
+    if (!BATCH) {
+        for (int k = 0; k < 3; k++) {
+            bmin[k] = A.box[k];
+            bmax[k] = A.box[4 + k];
+        }
+        root = A.nodes[0];
+        legs_max = VARIANT == HK_TRACE_ROPES ? 4u * (A.rope_nn_dev ? *A.rope_nn_dev : A.rope_nn) + 8u : 0u;
+    }
     LaneState L;
     bool active = false, drained = false;
     uint32_t steps = 0;
@@ -346,6 +389,18 @@ __global__ void __launch_bounds__(128, 10) k_trace(TraceArgs A) {
             if (!active) {
                 uint32_t rid = base + __popc(idle & lt_mask);
                 if (rid < n) {
+                    if (BATCH) {
+                        scene = scene_of(A.ray_offsets, A.nscenes, rid);
+                        const SceneDesc &D = A.scenes[scene];
+                        V = SceneView{D.nodes, D.refs, D.tris, D.ropes, D.cbox};
+                        for (int k = 0; k < 3; k++) {
+                            bmin[k] = D.box[k];
+                            bmax[k] = D.box[4 + k];
+                        }
+                        root = V.nodes[0];
+                        legs_max = 4u * D.nn + 8u;
+                        ntris = D.ntris;
+                    }
                     float4 ro = A.rays[2 * (size_t)rid], rd = A.rays[2 * (size_t)rid + 1];
                     L.o = make_float3(ro.x, ro.y, ro.z);
                     L.d = make_float3(rd.x, rd.y, rd.z);
@@ -381,6 +436,7 @@ __global__ void __launch_bounds__(128, 10) k_trace(TraceArgs A) {
                             active = true;
                         } else {
                             A.hits[rid] = hk_hit{kInf, -1};
+                            if (BATCH && atomicSub(&A.remaining[scene], 1u) == 1u) A.done_ns[scene] = global_ns();
                         }
                     }
                 }
@@ -394,29 +450,31 @@ __global__ void __launch_bounds__(128, 10) k_trace(TraceArgs A) {
         bool done;
         if (VARIANT == HK_TRACE_BRUTE) {
             // GPUTrace_bruteforce.cl:30-42: every triangle in index order
-            for (uint32_t t = 0; t < A.ntris; t++) {
-                float h = isect_tri(&A.tris[t], L.o, L.d, L.best);
+            for (uint32_t t = 0; t < ntris; t++) {
+                float h = isect_tri(&V.tris[t], L.o, L.d, L.best);
                 if (h < L.best) {
                     L.best = h;
                     L.best_id = (int32_t)t;
                 }
             }
-            if (COUNT) c_refs += A.ntris;
+            if (COUNT) c_refs += ntris;
             done = true;
         } else if (VARIANT == HK_TRACE_FULLSTACK) {
-            done = leg_fullstack<COUNT>(A, L, root, l_s, l_e, l_n, kLocal, c_nodes, c_refs, steps);
+            done = leg_fullstack<COUNT>(A, V, L, root, l_s, l_e, l_n, kLocal, c_nodes, c_refs, steps);
         } else if (VARIANT == HK_TRACE_ROPES) {
-            done = leg_ropes<COUNT>(A, L, legs_max, c_nodes, c_refs);
+            done = leg_ropes<COUNT>(V, L, legs_max, c_nodes, c_refs);
         } else if (VARIANT == HK_TRACE_RESTART) {
-            done = leg_restart<false, COUNT>(A, L, root, c_nodes, c_refs, steps);
+            done = leg_restart<false, COUNT>(A, V, L, root, c_nodes, c_refs, steps);
         } else if (VARIANT == HK_TRACE_RESTART_EARLY) {
-            done = leg_restart<true, COUNT>(A, L, root, c_nodes, c_refs, steps);
+            done = leg_restart<true, COUNT>(A, V, L, root, c_nodes, c_refs, steps);
         } else {
-            done = leg_shortstack<smem_ring, COUNT>(A, L, root, s_s, s_e, s_n, l_s, l_e, l_n, c_nodes, c_refs, steps);
+            done = leg_shortstack<smem_ring, COUNT>(A, V, L, root, s_s, s_e, s_n, l_s, l_e, l_n, c_nodes, c_refs,
+                                                    steps);
         }
         if (done) {
             A.hits[L.ray] = hk_hit{L.best, L.best_id};
             active = false;
+            if (BATCH && atomicSub(&A.remaining[scene], 1u) == 1u) A.done_ns[scene] = global_ns();
         }
     }
     if (COUNT) {
@@ -428,10 +486,16 @@ __global__ void __launch_bounds__(128, 10) k_trace(TraceArgs A) {
 
 template <int V>
 static cudaError_t launch_v(const TraceArgs &a, bool count, int grid, int block, size_t smem, cudaStream_t s) {
-    if (count)
-        k_trace<V, true><<<grid, block, smem, s>>>(a);
-    else
-        k_trace<V, false><<<grid, block, smem, s>>>(a);
+    if (a.scenes) {
+        if (count)
+            k_trace<V, true, true><<<grid, block, smem, s>>>(a);
+        else
+            k_trace<V, false, true><<<grid, block, smem, s>>>(a);
+    } else if (count) {
+        k_trace<V, true, false><<<grid, block, smem, s>>>(a);
+    } else {
+        k_trace<V, false, false><<<grid, block, smem, s>>>(a);
+    }
     return cudaGetLastError();
 }
 
@@ -455,6 +519,12 @@ cudaError_t launch_trace(const TraceLaunch &L, cudaStream_t s) {
     a.cbox = L.cbox;
     a.rope_nn = L.rope_nn;
     a.rope_nn_dev = L.rope_nn_dev;
+    a.scenes = L.scenes;
+    a.ray_offsets = L.ray_offsets;
+    a.nscenes = L.nscenes;
+    a.remaining = L.remaining;
+    a.done_ns = L.done_ns;
+    a.start_ns = L.start_ns;
     cudaError_t e = cudaMemsetAsync(L.fetch, 0, sizeof(uint32_t), s);
     if (e != cudaSuccess) return e;
     if (L.n == 0 && L.n_dev == nullptr) return cudaSuccess;
@@ -469,7 +539,7 @@ cudaError_t launch_trace(const TraceLaunch &L, cudaStream_t s) {
     case HK_TRACE_RESTART: return launch_v<HK_TRACE_RESTART>(a, L.count, grid, block, smem, s);
     case HK_TRACE_RESTART_EARLY: return launch_v<HK_TRACE_RESTART_EARLY>(a, L.count, grid, block, smem, s);
     case HK_TRACE_ROPES:
-        if (!L.ropes || !L.cbox) return cudaErrorInvalidValue;
+        if (!L.scenes && (!L.ropes || !L.cbox)) return cudaErrorInvalidValue;
         return launch_v<HK_TRACE_ROPES>(a, L.count, grid, block, smem, s);
     case HK_TRACE_BRUTE: return launch_v<HK_TRACE_BRUTE>(a, L.count, grid, block, smem, s);
     default: return cudaErrorInvalidValue;

@@ -209,6 +209,42 @@ class Context:
         return k.value, a.value
 
 
+class Batch:
+    """Many scenes traced in one persistent launch (include/hulkcuda.h, hk_batch_*)."""
+
+    def __init__(self, ctx: Context):
+        self.ctx = ctx
+        h = C.c_void_p()
+        ctx._check(ctx.L.hk_batch_create(ctx.h, C.byref(h)))
+        self.h = h
+        self.nscenes = 0
+
+    def add_scene(self, verts, tris) -> int:
+        v, t = _f32(verts), _u32(tris)
+        sid = C.c_uint32()
+        self.ctx._check(self.ctx.L.hk_batch_add_scene(self.h, ptr(v), v.shape[0], ptr(t), t.shape[0], C.byref(sid)))
+        self.nscenes += 1
+        return sid.value
+
+    def trace_device(self, d_rays: int, offsets, d_hits: int, variant=_lib.ROPES, want_times=True):
+        off = _u32(offsets)
+        ms = np.zeros(self.nscenes, np.float32) if want_times else None
+        self.ctx._check(self.ctx.L.hk_batch_trace_device(self.h, C.c_void_p(d_rays), ptr(off), self.nscenes,
+                                                         int(variant), C.c_void_p(d_hits), ptr(ms)))
+        return ms
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.ctx.L.hk_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class KDTreeCUDA:
     """``KDTreeCPU``'s interface on the GPU (HulkEngine/src/KDTreeCPU.hpp:53-72)."""
 

@@ -368,3 +368,68 @@ def random_soup(n: int, seed: int = 0, extent: float = 10.0, size: float = 1.0) 
     cam = look_at_camera((0.0, 0.5 * extent, 2.2 * extent), (0.0, 0.0, 0.0), 60.0, 64, 64)
     lights = np.stack([point_light((extent, 2 * extent, extent))])
     return Scene(V, T, lights, cam, 64, 64, name="soup%d" % n)
+
+
+# ----------------------------------------------------------------------------
+# batched scenes and incoherent rays
+# ----------------------------------------------------------------------------
+
+def cluster_soup(n_tris: int, seed: int, n_clusters: int = 64, extent: float = 50.0) -> Scene:
+    """Clustered small random triangles (the large static generator at any size)."""
+    rng = np.random.default_rng(seed)
+    centers = rng.uniform(-extent, extent, size=(n_clusters, 3))
+    sigmas = rng.uniform(0.05, 0.4, size=n_clusters) * extent
+    cluster_of = rng.integers(0, n_clusters, size=n_tris)
+    v, t = _random_small_tris(rng, n_tris, centers, sigmas, cluster_of)
+    V, T = _pack([v], [t])
+    cam = look_at_camera((0.0, 0.3 * extent, 2.2 * extent), (0.0, 0.0, 0.0), 60.0, 256, 256)
+    lights = np.stack([point_light((0.6 * extent, 1.6 * extent, 1.2 * extent))])
+    return Scene(V, T, lights, cam, 256, 256, name="soup%d" % n_tris)
+
+
+def incoherent_rays(sc: Scene, n: int, seed: int) -> np.ndarray:
+    """A quarter primary rays through random pixels; the rest leave random
+    points of random triangles in cosine-weighted directions about the face
+    normal (stand-ins for shadow rays and two diffuse bounces). float32
+    [n, 8], directions normalised, w = 0."""
+    rng = np.random.default_rng(seed)
+    n_prim = n // 4
+    out = np.zeros((n, 8), np.float32)
+    cam = sc.camera.astype(np.float64)
+    u = rng.random(n_prim)
+    v = rng.random(n_prim)
+    d = cam[3, :3] + cam[1, :3] * u[:, None] + cam[2, :3] * v[:, None] - cam[0, :3]
+    out[:n_prim, :3] = cam[0, :3]
+    out[:n_prim, 4:7] = d / np.linalg.norm(d, axis=1, keepdims=True)
+    m = n - n_prim
+    tri = rng.integers(0, sc.ntris, size=m)
+    p = sc.verts[sc.tris[tri, :3], :3].astype(np.float64)           # [m, 3, 3]
+    a, b = rng.random(m), rng.random(m)
+    flip = a + b > 1.0
+    a[flip], b[flip] = 1.0 - a[flip], 1.0 - b[flip]
+    pos = p[:, 0] + (p[:, 1] - p[:, 0]) * a[:, None] + (p[:, 2] - p[:, 0]) * b[:, None]
+    nrm = np.cross(p[:, 1] - p[:, 0], p[:, 2] - p[:, 0])
+    ln = np.linalg.norm(nrm, axis=1, keepdims=True)
+    nrm = np.where(ln > 0, nrm / np.maximum(ln, 1e-30), np.array([0.0, 1.0, 0.0]))
+    # cosine-weighted hemisphere sample in the normal's frame
+    r1, r2 = rng.random(m), rng.random(m)
+    phi = 2.0 * math.pi * r1
+    sx, sy, sz = np.cos(phi) * np.sqrt(r2), np.sin(phi) * np.sqrt(r2), np.sqrt(1.0 - r2)
+    helper = np.where(np.abs(nrm[:, :1]) > 0.9, np.array([0.0, 1.0, 0.0]), np.array([1.0, 0.0, 0.0]))
+    t1 = np.cross(nrm, helper)
+    t1 /= np.linalg.norm(t1, axis=1, keepdims=True)
+    t2 = np.cross(nrm, t1)
+    side = np.where(rng.random(m) < 0.5, 1.0, -1.0)[:, None]     # either face
+    dirs = t1 * sx[:, None] + t2 * sy[:, None] + nrm * (sz[:, None] * side)
+    dirs /= np.linalg.norm(dirs, axis=1, keepdims=True)
+    out[n_prim:, :3] = pos + dirs * 1e-3
+    out[n_prim:, 4:7] = dirs
+    return out
+
+
+def batch_scenes(n_scenes: int = 64, seed: int = 5, tris=(10_000, 2_000_000), rays=(65_536, 4_194_304)):
+    """Scenes with log-uniform triangle counts and log-uniform ray counts."""
+    rng = np.random.default_rng(seed)
+    nt = np.exp(rng.uniform(math.log(tris[0]), math.log(tris[1]), n_scenes)).astype(np.int64)
+    nr = np.exp(rng.uniform(math.log(rays[0]), math.log(rays[1]), n_scenes)).astype(np.int64)
+    return [(cluster_soup(int(nt[i]), seed * 1000 + i), int(nr[i])) for i in range(n_scenes)]

@@ -214,6 +214,25 @@ hk_status hk_get_ray_counts(hk_ctx *ctx, uint64_t *primary, uint64_t *shadow);
 /* Kernel nodes and all nodes of the captured frame graph (0 before capture). */
 hk_status hk_frame_graph_info(hk_ctx *ctx, uint32_t *kernel_nodes, uint32_t *all_nodes);
 
+/* ---- batching: many scenes, uneven ray batches, one persistent launch ----
+ * No reference counterpart (the reference renders one scene per frame). A
+ * batch keeps its own copy of each scene's triangle records and GPU-built tree
+ * (ropes included). hk_batch_trace_device traces the rays of every scene in a
+ * single launch of the persistent traversal kernel: rays of scene s are
+ * d_rays8[ray_offsets[s] .. ray_offsets[s+1]) and warps take 32 rays at a time
+ * from one counter across all scenes. scene_ms (optional, host, nscenes)
+ * receives the time from the launch's start until each scene's last ray
+ * finished (device %globaltimer). */
+typedef struct hk_batch hk_batch;
+hk_status hk_batch_create(hk_ctx *ctx, hk_batch **batch);
+hk_status hk_batch_destroy(hk_batch *batch);
+/* upload + triangle records + GPU build (the context's settings), then keep a
+ * copy; uses the context's scene slot as working space */
+hk_status hk_batch_add_scene(hk_batch *batch, const float *verts4, uint32_t nv, const uint32_t *tris4,
+                             uint32_t nt, uint32_t *scene_id);
+hk_status hk_batch_trace_device(hk_batch *batch, const float *d_rays8, const uint32_t *ray_offsets,
+                                uint32_t nscenes, hk_variant variant, hk_hit *d_hits, float *scene_ms);
+
 /* ---- rendering without any device allocation ----
  * No counterpart in the reference: an addition for callers that cannot let
  * the library call cudaMalloc (hosts with their own pooled allocator, code
