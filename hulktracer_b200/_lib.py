@@ -38,6 +38,14 @@ class Config(C.Structure):
                 ("max_refs", C.c_uint32), ("topk", C.c_uint32), ("fallback_ratio", C.c_float)]
 
 
+class TuneResult(C.Structure):
+    _fields_ = [("variant", C.c_int), ("block_size", C.c_uint32), ("short_stack", C.c_uint32),
+                ("best_ms", C.c_float), ("default_ms", C.c_float), ("tried", C.c_uint32)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class TreeStats(C.Structure):
     _fields_ = [("nodes", C.c_uint32), ("leaves", C.c_uint32), ("refs", C.c_uint32), ("depth", C.c_uint32),
                 ("build_ms", C.c_float), ("capacity_hit", C.c_uint32), ("learned_nodes", C.c_uint32),
@@ -95,6 +103,7 @@ def load(path: str = LIB_PATH):
         "hk_get_ray_counts": [vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)],
         "hk_frame_graph_info": [vp, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)],
         "hk_render_noalloc": [vp, vp, vp, u32, f32p, f32p, f32p, u32, u32, u32, C.c_int, vp, vp],
+        "hk_autotune": [vp, vp, u32, C.c_char_p, C.POINTER(TuneResult)],
         "hk_batch_create": [vp, C.POINTER(C.c_void_p)],
         "hk_batch_destroy": [vp],
         "hk_batch_add_scene": [vp, f32p, u32, u32p, u32, C.POINTER(C.c_uint32)],

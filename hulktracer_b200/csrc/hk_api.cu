@@ -1100,4 +1100,112 @@ hk_status hk_batch_trace_device(hk_batch *b, const float *d_rays8, const uint32_
     return HK_OK;
 }
 
+// ---------------------------------------------------------------------------
+// autotuner
+// ---------------------------------------------------------------------------
+static float time_trace(hk_ctx *c, const float4 *d_rays, uint32_t n, hk_variant v, hk_hit *d_hits, int reps) {
+    std::vector<float> ts;
+    for (int r = 0; r < reps + 2; r++) {
+        cudaEventRecord(c->ev0, c->stream);
+        if (trace_enqueue(c, d_rays, n, nullptr, v, d_hits) != HK_OK) return -1.0f;
+        cudaEventRecord(c->ev1, c->stream);
+        if (cudaEventSynchronize(c->ev1) != cudaSuccess) return -1.0f;
+        float ms = 0;
+        cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+        if (r >= 2) ts.push_back(ms);
+    }
+    std::sort(ts.begin(), ts.end());
+    return ts[ts.size() / 2];
+}
+
+static std::string tune_key(hk_ctx *c) {
+    cudaDeviceProp prop;
+    cudaGetDeviceProperties(&prop, c->device);
+    uint32_t cls = 0;
+    while ((1u << (cls + 1)) <= std::max<uint32_t>(c->nt, 1)) cls++;
+    char buf[256];
+    snprintf(buf, sizeof buf, "%s|sm%d|tris2^%u", prop.name, c->sm_count, cls);
+    return buf;
+}
+
+hk_status hk_autotune(hk_ctx *c, const float *d_rays8, uint32_t n, const char *cache_path, hk_tune_result *res) {
+    if (!c || !d_rays8 || n == 0) return HK_E_ILLEGAL_INPUT;
+    if (!c->tree_valid || !c->rec_valid) return fail(c, HK_E_STATE, "autotune needs a scene and a tree");
+    cudaSetDevice(c->device);
+    hk_tune_result r;
+    memset(&r, 0, sizeof r);
+    std::string key = tune_key(c);
+    if (cache_path) {
+        FILE *f = fopen(cache_path, "r");
+        if (f) {
+            char line[512];
+            while (fgets(line, sizeof line, f)) {
+                char k[300];
+                int var;
+                unsigned bs, ss;
+                float ms;
+                if (sscanf(line, "%299[^,],%d,%u,%u,%f", k, &var, &bs, &ss, &ms) == 5 && key == k) {
+                    r.variant = var;
+                    r.block_size = bs;
+                    r.short_stack = ss;
+                    r.best_ms = ms;
+                }
+            }
+            fclose(f);
+            if (r.block_size) {
+                c->cfg.block_size = r.block_size;
+                c->cfg.short_stack = r.short_stack;
+                if (res) *res = r;
+                return HK_OK;
+            }
+        }
+    }
+    hk_config saved = c->cfg;
+    DevBuf<hk_hit> hits;
+    HK_CUDA(c, hits.ensure(n));
+    const float4 *rays = reinterpret_cast<const float4 *>(d_rays8);
+    c->cfg.block_size = 128;
+    c->cfg.short_stack = 6;
+    c->cfg.blocks_per_sm = 0;
+    r.default_ms = time_trace(c, rays, n, HK_TRACE_ROPES, hits.p, 3);
+    float best = 1e30f;
+    const hk_variant vs[] = {HK_TRACE_ROPES, HK_TRACE_SHORTSTACK, HK_TRACE_SMEMSTACK, HK_TRACE_FULLSTACK,
+                             HK_TRACE_RESTART_EARLY};
+    const uint32_t blocks[] = {64, 128, 256};
+    const uint32_t stacks[] = {4, 6, 8, 12, 16};
+    for (hk_variant v : vs) {
+        bool uses_stack = (v == HK_TRACE_SHORTSTACK || v == HK_TRACE_SMEMSTACK);
+        for (uint32_t bs : blocks) {
+            for (uint32_t ss : stacks) {
+                if (!uses_stack && ss != 6) continue;
+                if (v == HK_TRACE_SMEMSTACK && (size_t)ss * bs * 12 > 48 * 1024) continue;
+                c->cfg.block_size = bs;
+                c->cfg.short_stack = ss;
+                float ms = time_trace(c, rays, n, v, hits.p, 3);
+                r.tried++;
+                if (ms > 0 && ms < best) {
+                    best = ms;
+                    r.variant = (int)v;
+                    r.block_size = bs;
+                    r.short_stack = ss;
+                }
+            }
+        }
+    }
+    hits.release();
+    c->cfg = saved;
+    if (r.tried == 0 || best >= 1e30f) return fail(c, HK_E_CUDA, "autotune: no candidate ran");
+    r.best_ms = best;
+    c->cfg.block_size = r.block_size;
+    c->cfg.short_stack = r.short_stack;
+    if (cache_path) {
+        FILE *f = fopen(cache_path, "a");
+        if (!f) return fail(c, HK_E_FILE_OPEN, "autotune cache not writable");
+        fprintf(f, "%s,%d,%u,%u,%.6f\n", key.c_str(), r.variant, r.block_size, r.short_stack, r.best_ms);
+        if (fclose(f) != 0) return fail(c, HK_E_FILE_CLOSE, "autotune cache close failed");
+    }
+    if (res) *res = r;
+    return check_err_word(c);
+}
+
 }  // extern "C"

@@ -198,6 +198,12 @@ class Context:
         return st.as_dict() if st is not None else None
 
 
+    def autotune(self, d_rays: int, n: int, cache_path: str | None = None):
+        r = _lib.TuneResult()
+        self._check(self.L.hk_autotune(self.h, C.c_void_p(d_rays), n,
+                                       cache_path.encode() if cache_path else None, C.byref(r)))
+        return r.as_dict()
+
     def ray_counts(self):
         p, sh = C.c_uint64(), C.c_uint64()
         self._check(self.L.hk_get_ray_counts(self.h, C.byref(p), C.byref(sh)))

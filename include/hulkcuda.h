@@ -214,6 +214,25 @@ hk_status hk_get_ray_counts(hk_ctx *ctx, uint64_t *primary, uint64_t *shadow);
 /* Kernel nodes and all nodes of the captured frame graph (0 before capture). */
 hk_status hk_frame_graph_info(hk_ctx *ctx, uint32_t *kernel_nodes, uint32_t *all_nodes);
 
+/* ---- autotuner (no reference counterpart) ----
+ * Times the persistent traversal on n device rays of the current scene for
+ * every candidate: traversal layout (ropes: compact nodes + per-node cells and
+ * ropes; stack / restart variants: compact nodes only), block size
+ * (64, 128, 256) and short-stack depth (4, 6, 8, 12, 16), picks the fastest
+ * and writes it into the context's configuration. With cache_path non-NULL
+ * the choice is stored per device and scene-size class in that text file and
+ * reused on later calls (no timing then). */
+typedef struct hk_tune_result {
+    int variant;
+    uint32_t block_size;
+    uint32_t short_stack;
+    float best_ms;          /* median launch time of the winner */
+    float default_ms;       /* the default configuration (ropes, 128, stack 6) */
+    uint32_t tried;         /* candidates timed (0 = taken from the cache) */
+} hk_tune_result;
+hk_status hk_autotune(hk_ctx *ctx, const float *d_rays8, uint32_t n, const char *cache_path,
+                      hk_tune_result *result);
+
 /* ---- batching: many scenes, uneven ray batches, one persistent launch ----
  * No reference counterpart (the reference renders one scene per frame). A
  * batch keeps its own copy of each scene's triangle records and GPU-built tree
