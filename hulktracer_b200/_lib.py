@@ -22,7 +22,7 @@ FULLSTACK, SHORTSTACK, SMEMSTACK, RESTART, RESTART_EARLY, ROPES, BRUTE = range(7
 VARIANTS = {"fullstack": FULLSTACK, "shortstack": SHORTSTACK, "smemstack": SMEMSTACK,
             "restart": RESTART, "restart_early": RESTART_EARLY, "ropes": ROPES, "brute": BRUTE}
 BUILD_BINNED, BUILD_LEARNED = 0, 1
-SHADE_CPU, SHADE_PICTURE = 0, 1
+SHADE_CPU, SHADE_PICTURE, SHADE_MIRROR = 0, 1, 2
 
 
 class HkError(RuntimeError):
@@ -83,6 +83,7 @@ def load(path: str = LIB_PATH):
         "hk_scene_set_parts": [vp, u32p, u32],
         "hk_scene_transform": [vp, f32p],
         "hk_scene_get_vertices": [vp, f32p],
+        "hk_scene_set_mirrors": [vp, vp, u32],
         "hk_precompute": [vp],
         "hk_cache_import": [vp, f32p, u32],
         "hk_cache_export": [vp, f32p],

@@ -89,6 +89,12 @@ struct hk_ctx {
     DevBuf<uint32_t> slot, spix, scount;
     DevBuf<float4> hit4;
     DevBuf<uint32_t> rgba;
+    // mirror bounce
+    DevBuf<uint8_t> mirror;
+    bool has_mirrors = false;
+    DevBuf<float4> mrays, prays;
+    DevBuf<hk_hit> mhits, phits;
+    DevBuf<uint32_t> mslot, mcount;
     // frame graph
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
@@ -204,6 +210,8 @@ hk_status hk_destroy(hk_ctx *c) {
     c->rays.release(); c->hits.release(); c->cam.release(); c->lights.release();
     c->srays.release(); c->shits.release(); c->slot.release(); c->spix.release(); c->scount.release();
     c->hit4.release(); c->rgba.release();
+    c->mirror.release(); c->mrays.release(); c->prays.release(); c->mhits.release(); c->phits.release();
+    c->mslot.release(); c->mcount.release();
     build_release(c->build);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
@@ -338,6 +346,18 @@ hk_status hk_scene_transform(hk_ctx *c, const float *mats12) {
     if (s != HK_OK) return s;
     c->tree_valid = false;
     HK_CUDA(c, cudaStreamSynchronize(c->stream));
+    return HK_OK;
+}
+
+hk_status hk_scene_set_mirrors(hk_ctx *c, const uint8_t *mirror, uint32_t nt) {
+    if (!c || (nt && !mirror)) return HK_E_ILLEGAL_INPUT;
+    if (nt != c->nt) return fail(c, HK_E_ILLEGAL_INPUT, "mirror flags size != triangle count");
+    cudaSetDevice(c->device);
+    invalidate_graph(c);
+    HK_CUDA(c, c->mirror.ensure(std::max<uint32_t>(nt, 1)));
+    HK_CUDA(c, cudaMemcpyAsync(c->mirror.p, mirror, nt, cudaMemcpyHostToDevice, c->stream));
+    HK_CUDA(c, cudaStreamSynchronize(c->stream));
+    c->has_mirrors = true;
     return HK_OK;
 }
 
@@ -760,6 +780,14 @@ static hk_status render_buffers(hk_ctx *c, uint32_t npix, uint32_t nl) {
     HK_CUDA(c, c->rgba.ensure(npix));
     HK_CUDA(c, c->cam.ensure(16));
     HK_CUDA(c, c->lights.ensure(8 * (size_t)std::max<uint32_t>(nl, 1)));
+    if (c->has_mirrors) {
+        HK_CUDA(c, c->mrays.ensure(2 * (size_t)npix));
+        HK_CUDA(c, c->prays.ensure(2 * (size_t)npix));
+        HK_CUDA(c, c->mhits.ensure(npix));
+        HK_CUDA(c, c->phits.ensure(npix));
+        HK_CUDA(c, c->mslot.ensure(npix));
+        HK_CUDA(c, c->mcount.ensure(1));
+    }
     return HK_OK;
 }
 
@@ -778,11 +806,24 @@ static hk_status render_enqueue(hk_ctx *c, uint32_t nl, uint32_t w, uint32_t h, 
         HK_CUDA(c, launch_shade_picture(c->rays.p, c->hit4.p, npix, c->lights.p, nl, d_rgba, c->stream, w, tiled));
         return HK_OK;
     }
-    HK_CUDA(c, launch_shadow_rays(c->rays.p, c->hits.p, c->rec.p, npix, c->lights.p, nl, c->srays.p, c->slot.p,
+    const float4 *shade_rays = c->rays.p;
+    const hk_hit *shade_hits = c->hits.p;
+    if (shade == HK_SHADE_MIRROR) {
+        // one mirror bounce: reflected rays, traced, merged into the shading rays
+        HK_CUDA(c, launch_mirror_rays(c->rays.p, c->hits.p, c->rec.p, c->mirror.p, npix, c->mrays.p, c->mslot.p,
+                                      c->mcount.p, c->stream));
+        s = trace_enqueue(c, c->mrays.p, 0, c->mcount.p, v, c->mhits.p);
+        if (s != HK_OK) return s;
+        HK_CUDA(c, launch_mirror_merge(c->rays.p, c->hits.p, c->mslot.p, c->mrays.p, c->mhits.p, npix, c->prays.p,
+                                       c->phits.p, c->stream));
+        shade_rays = c->prays.p;
+        shade_hits = c->phits.p;
+    }
+    HK_CUDA(c, launch_shadow_rays(shade_rays, shade_hits, c->rec.p, npix, c->lights.p, nl, c->srays.p, c->slot.p,
                                   c->spix.p, c->scount.p, c->stream));
     s = trace_enqueue(c, c->srays.p, 0, c->scount.p, v, c->shits.p);
     if (s != HK_OK) return s;
-    HK_CUDA(c, launch_shade_cpu(c->rays.p, c->hits.p, c->rec.p, npix, c->lights.p, nl, c->slot.p, c->shits.p,
+    HK_CUDA(c, launch_shade_cpu(shade_rays, shade_hits, c->rec.p, npix, c->lights.p, nl, c->slot.p, c->shits.p,
                                 d_rgba, c->stream, w, tiled));
     return HK_OK;
 }
@@ -791,7 +832,9 @@ hk_status hk_render_device(hk_ctx *c, const float *cam16, const float *lights8, 
                            hk_variant v, int shade, uint32_t *d_rgba) {
     if (!c || !cam16 || !d_rgba) return HK_E_ILLEGAL_INPUT;
     if ((size_t)w * h == 0 || (size_t)w * h > (1u << 28)) return fail(c, HK_E_ILLEGAL_INPUT, "image size");
-    if (shade != HK_SHADE_CPU && shade != HK_SHADE_PICTURE) return fail(c, HK_E_ILLEGAL_INPUT, "shade mode");
+    if (shade != HK_SHADE_CPU && shade != HK_SHADE_PICTURE && shade != HK_SHADE_MIRROR)
+        return fail(c, HK_E_ILLEGAL_INPUT, "shade mode");
+    if (shade == HK_SHADE_MIRROR && !c->has_mirrors) return fail(c, HK_E_STATE, "hk_scene_set_mirrors first");
     hk_status s = validate_lights(c, lights8, nl);
     if (s != HK_OK) return s;
     cudaSetDevice(c->device);
@@ -921,12 +964,14 @@ hk_status hk_frame(hk_ctx *c, const float *mats12, const float *cam16, const flo
 hk_status hk_get_ray_counts(hk_ctx *c, uint64_t *primary, uint64_t *shadow) {
     if (!c) return HK_E_ILLEGAL_INPUT;
     cudaSetDevice(c->device);
-    uint32_t ns = 0;
-    if (c->last_shade == HK_SHADE_CPU && c->last_primary)
+    uint32_t ns = 0, nm = 0;
+    if (c->last_shade != HK_SHADE_PICTURE && c->last_primary)
         HK_CUDA(c, cudaMemcpyAsync(&ns, c->scount.p, 4, cudaMemcpyDeviceToHost, c->stream));
+    if (c->last_shade == HK_SHADE_MIRROR && c->last_primary)
+        HK_CUDA(c, cudaMemcpyAsync(&nm, c->mcount.p, 4, cudaMemcpyDeviceToHost, c->stream));
     HK_CUDA(c, cudaStreamSynchronize(c->stream));
     if (primary) *primary = c->last_primary;
-    if (shadow) *shadow = ns;
+    if (shadow) *shadow = (uint64_t)ns + nm;   /* secondary rays: shadow + mirror */
     return HK_OK;
 }
 

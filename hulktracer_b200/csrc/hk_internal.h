@@ -79,4 +79,9 @@ cudaError_t launch_hit4(const hk_hit *hits, const TriRec *tris, uint32_t n, floa
 cudaError_t launch_shade_picture(const float4 *rays, const float4 *hit4, uint32_t n, const float *lights_dev,
                                  uint32_t nl, uint32_t *rgba, cudaStream_t s, uint32_t w = 0, bool tiled = false);
 
+cudaError_t launch_mirror_rays(const float4 *rays, const hk_hit *hits, const TriRec *tris, const uint8_t *mirror,
+                               uint32_t npix, float4 *mrays, uint32_t *mslot, uint32_t *mcount, cudaStream_t s);
+cudaError_t launch_mirror_merge(const float4 *rays, const hk_hit *hits, const uint32_t *mslot, const float4 *mrays,
+                                const hk_hit *mhits, uint32_t npix, float4 *srays, hk_hit *shits, cudaStream_t s);
+
 }  // namespace hk

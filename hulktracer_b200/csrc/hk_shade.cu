@@ -422,4 +422,73 @@ cudaError_t launch_shade_picture(const float4 *rays, const float4 *hit4, uint32_
     return cudaGetLastError();
 }
 
+// ---------------------------------------------------------------------------
+// one mirror bounce (no reference counterpart): reflected rays of primary
+// hits on mirror triangles, then the per-pixel shading ray / hit
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void reflect_ray(float4 o, float4 d, float t, float4 na, float4 &ro, float4 &rd) {
+    float4 pos = hit_pos(o, d, t);
+    pos.w = 0.0f;
+    float dn = dot4(d.x, d.y, d.z, d.w, na.x, na.y, na.z, 0.0f);
+    float k = __fmul_rn(2.0f, dn);
+    rd = make_float4(__fsub_rn(d.x, __fmul_rn(na.x, k)), __fsub_rn(d.y, __fmul_rn(na.y, k)),
+                     __fsub_rn(d.z, __fmul_rn(na.z, k)), 0.0f);
+    ro = make_float4(__fadd_rn(pos.x, __fmul_rn(rd.x, 0.001f)), __fadd_rn(pos.y, __fmul_rn(rd.y, 0.001f)),
+                     __fadd_rn(pos.z, __fmul_rn(rd.z, 0.001f)), 0.0f);
+}
+
+__global__ void k_mirror_rays(const float4 *__restrict__ rays, const hk_hit *__restrict__ hits,
+                              const TriRec *__restrict__ tris, const uint8_t *__restrict__ mirror, uint32_t npix,
+                              float4 *__restrict__ mrays, uint32_t *__restrict__ mslot, uint32_t *mcount) {
+    uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    hk_hit h = p < npix ? hits[p] : hk_hit{kInf, -1};
+    bool want = p < npix && h.tri >= 0 && mirror[h.tri];
+    uint32_t m = __ballot_sync(0xffffffffu, want);
+    uint32_t base = 0;
+    if ((threadIdx.x & 31u) == 0 && m) base = atomicAdd(mcount, (uint32_t)__popc(m));
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (p >= npix) return;
+    mslot[p] = 0xffffffffu;
+    if (!want) return;
+    uint32_t k = base + __popc(m & ((1u << (threadIdx.x & 31u)) - 1u));
+    float4 ro, rd;
+    reflect_ray(rays[2 * (size_t)p], rays[2 * (size_t)p + 1], h.t, tris[h.tri].a, ro, rd);
+    mrays[2 * (size_t)k] = ro;
+    mrays[2 * (size_t)k + 1] = rd;
+    mslot[p] = k;
+}
+
+// shading ray / hit per pixel: the reflected one on mirrors, else the primary
+__global__ void k_mirror_merge(const float4 *__restrict__ rays, const hk_hit *__restrict__ hits,
+                               const uint32_t *__restrict__ mslot, const float4 *__restrict__ mrays,
+                               const hk_hit *__restrict__ mhits, uint32_t npix, float4 *__restrict__ srays,
+                               hk_hit *__restrict__ shits) {
+    uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= npix) return;
+    uint32_t k = mslot[p];
+    if (k == 0xffffffffu) {
+        srays[2 * (size_t)p] = rays[2 * (size_t)p];
+        srays[2 * (size_t)p + 1] = rays[2 * (size_t)p + 1];
+        shits[p] = hits[p];
+    } else {
+        srays[2 * (size_t)p] = mrays[2 * (size_t)k];
+        srays[2 * (size_t)p + 1] = mrays[2 * (size_t)k + 1];
+        shits[p] = mhits[k];
+    }
+}
+
+cudaError_t launch_mirror_rays(const float4 *rays, const hk_hit *hits, const TriRec *tris, const uint8_t *mirror,
+                               uint32_t npix, float4 *mrays, uint32_t *mslot, uint32_t *mcount, cudaStream_t s) {
+    cudaError_t e = cudaMemsetAsync(mcount, 0, sizeof(uint32_t), s);
+    if (e != cudaSuccess) return e;
+    if (npix) k_mirror_rays<<<blocks_for(npix, 256), 256, 0, s>>>(rays, hits, tris, mirror, npix, mrays, mslot, mcount);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_mirror_merge(const float4 *rays, const hk_hit *hits, const uint32_t *mslot, const float4 *mrays,
+                                const hk_hit *mhits, uint32_t npix, float4 *srays, hk_hit *shits, cudaStream_t s) {
+    if (npix) k_mirror_merge<<<blocks_for(npix, 256), 256, 0, s>>>(rays, hits, mslot, mrays, mhits, npix, srays, shits);
+    return cudaGetLastError();
+}
+
 }  // namespace hk

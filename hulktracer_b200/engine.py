@@ -84,6 +84,10 @@ class Context:
         self._part = _u32(part_of_vertex)
         self._check(self.L.hk_scene_set_parts(self.h, ptr(self._part), int(nparts)))
 
+    def set_mirrors(self, mirror):
+        m = np.ascontiguousarray(mirror, dtype=np.uint8)
+        self._check(self.L.hk_scene_set_mirrors(self.h, ptr(m), m.shape[0]))
+
     def transform(self, mats12):
         self._check(self.L.hk_scene_transform(self.h, ptr(_f32(mats12))))
 

@@ -75,7 +75,13 @@ typedef enum hk_build_mode {
 /* Shading semantics for hk_render */
 enum {
     HK_SHADE_CPU = 0,          /* GLVisitorCPUTrace::traceScene: shadow rays, misses 0 */
-    HK_SHADE_PICTURE = 1       /* ShadePicture (shadePicture.cl:7-55): no shadow rays */
+    HK_SHADE_PICTURE = 1,      /* ShadePicture (shadePicture.cl:7-55): no shadow rays */
+    HK_SHADE_MIRROR = 2        /* HK_SHADE_CPU plus one mirror bounce (no reference
+                                  counterpart): a primary hit on a mirror triangle
+                                  (hk_scene_set_mirrors) is replaced by the hit of the
+                                  reflected ray r = d - n*(2 d.n) leaving pos + r*0.001,
+                                  which is then shaded (shadow rays included); a
+                                  reflected ray that misses gives 0 */
 };
 
 typedef struct hk_config {
@@ -142,6 +148,8 @@ hk_status hk_scene_get_box(hk_ctx *ctx, float *box8);
 hk_status hk_scene_set_parts(hk_ctx *ctx, const uint32_t *part_of_vertex, uint32_t nparts);
 hk_status hk_scene_transform(hk_ctx *ctx, const float *mats12);
 hk_status hk_scene_get_vertices(hk_ctx *ctx, float *verts4);
+/* Per-triangle material flag (1 = mirror) for HK_SHADE_MIRROR. */
+hk_status hk_scene_set_mirrors(hk_ctx *ctx, const uint8_t *mirror, uint32_t nt);
 
 /* ---- per-triangle cache (KDTreeCPU::buildPolygonCache, KDTreeCPU.cpp:479-507;
  *      build_cache, GPUTrace_buildCache.cl:5-37) ---- */

@@ -936,6 +936,46 @@ void hko_render_cpu(const hko_tree *t, int variant, int D, const float *rays, ui
     }
 }
 
+/* One mirror bounce (no reference counterpart; the CUDA path's HK_SHADE_MIRROR):
+ * a primary hit on a mirror triangle is replaced by the hit of the reflected ray
+ * r = d - n*(2 d.n) leaving pos + r*0.001, which is shaded like a primary hit
+ * (GLVisitorCPUTrace.cpp:165-194 semantics, shadow rays included); a reflected
+ * ray that misses gives 0. */
+void hko_render_mirror(const hko_tree *t, int variant, int D, const float *rays, uint32_t w, uint32_t h,
+                       const float *lights, uint32_t nl, const uint8_t *mirror, int mode, uint32_t *rgba,
+                       int nthreads) {
+    size_t n = (size_t)w * h;
+    float *srays = (float *)malloc(n * 8 * sizeof(float));
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel for schedule(dynamic, 256)
+#endif
+    for (long i = 0; i < (long)n; i++) {
+        const float *ray = rays + 8 * (size_t)i;
+        float *out = srays + 8 * (size_t)i;
+        memcpy(out, ray, 32);
+        float hit[8];
+        hko_counters c = {0, 0, 0};
+        int id = hko_trace_one(t, variant, D, ray, hit, &c);
+        if (id < 0 || !mirror[id]) continue;
+        const float *o = ray, *d = ray + 4;
+        const float *nrm = t->cache + 16 * (size_t)id;
+        float n4[4] = {nrm[0], nrm[1], nrm[2], 0.0f};
+        float pos[4];
+        for (int k = 0; k < 4; k++) pos[k] = o[k] + d[k] * hit[0];
+        pos[3] = 0.0f;
+        float k2 = 2.0f * hko_dot4(d, n4);
+        float r[4];
+        for (int q = 0; q < 3; q++) r[q] = d[q] - n4[q] * k2;
+        r[3] = 0.0f;
+        for (int q = 0; q < 3; q++) out[q] = pos[q] + r[q] * 0.001f;
+        out[3] = 0.0f;
+        memcpy(out + 4, r, 16);
+    }
+    hko_render_cpu(t, variant, D, srays, w, h, lights, nl, mode, rgba, nthreads);
+    free(srays);
+}
+
 /* ShadePicture, shadePicture.cl:7-55 (float3 dot as (x*x + y*y) + z*z) */
 static float dot3(const float *a, const float *b) { return (a[0] * b[0] + a[1] * b[1]) + a[2] * b[2]; }
 

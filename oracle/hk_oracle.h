@@ -127,6 +127,10 @@ void hko_trace(const hko_tree *t, int variant, int stack_depth, const float *ray
 void hko_render_cpu(const hko_tree *t, int variant, int stack_depth, const float *rays,
                     uint32_t w, uint32_t h, const float *lights, uint32_t nl, int norm_mode,
                     uint32_t *rgba_out, int nthreads);
+/* one mirror bounce before shading (mirror: per-triangle flags) */
+void hko_render_mirror(const hko_tree *t, int variant, int stack_depth, const float *rays, uint32_t w,
+                       uint32_t h, const float *lights, uint32_t nl, const uint8_t *mirror, int norm_mode,
+                       uint32_t *rgba_out, int nthreads);
 /* ShadePicture semantics (shadePicture.cl:7-55) from float4(normal, t) hits:
  * colour starts at 0.1 for every pixel, point lights /2, no shadow rays.
  * Output RGBA8 (alpha from colour.w). */

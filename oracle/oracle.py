@@ -113,6 +113,9 @@ class Oracle:
         L.hko_render_cpu.argtypes = [C.POINTER(_Tree), C.c_int, C.c_int, _f32p, C.c_uint32, C.c_uint32,
                                      _f32p, C.c_uint32, C.c_int, _u32p, C.c_int]
         L.hko_shade_picture.argtypes = [_f32p, _f32p, C.c_uint32, _f32p, C.c_uint32, _u32p]
+        L.hko_render_mirror.argtypes = [C.POINTER(_Tree), C.c_int, C.c_int, _f32p, C.c_uint32, C.c_uint32,
+                                        _f32p, C.c_uint32, np.ctypeslib.ndpointer(dtype=np.uint8, flags="C_CONTIGUOUS"),
+                                        C.c_int, _u32p, C.c_int]
 
     # -- helpers --
     def dot4(self, a, b):
@@ -233,6 +236,15 @@ class Oracle:
         ts = tree.cstruct()
         self.lib.hko_render_cpu(C.byref(ts), variant, stack_depth, _c(rays, np.float32).reshape(-1),
                                 w, h, lights.ravel(), lights.shape[0], mode, out, nthreads)
+        return out
+
+    def render_mirror(self, tree: Tree, rays, w, h, lights, mirror, variant=SHORTSTACK, stack_depth=5,
+                      mode=NORM_IEEE, nthreads=0):
+        out = np.zeros(w * h, np.uint32)
+        lights = _c(lights, np.float32).reshape(-1, 8)
+        ts = tree.cstruct()
+        self.lib.hko_render_mirror(C.byref(ts), variant, stack_depth, _c(rays, np.float32).reshape(-1), w, h,
+                                   lights.ravel(), lights.shape[0], _c(mirror, np.uint8), mode, out, nthreads)
         return out
 
     def shade_picture(self, rays, hit4, lights):

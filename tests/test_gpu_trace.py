@@ -170,3 +170,23 @@ def test_rejects_bad_inputs(ctx6, hk):
     ctx6.import_tree(g["ref_nodes"], g["ref_refs"])
     with pytest.raises(hk.HkError):
         ctx6.trace(rays)
+
+
+@pytest.mark.parametrize("variant", ["ropes", "shortstack"])
+def test_render_mirror_bounce(ctx6, hk, oracle, variant):
+    """HK_SHADE_MIRROR (no reference counterpart) equals the oracle's
+    restatement: reflected rays on 30% of triangles, then the usual shading."""
+    g = load("small24k.npz")
+    setup_ref_tree(ctx6, g)
+    nt = g["tris"].shape[0]
+    h32 = (np.arange(nt, dtype=np.uint64) * np.uint64(2654435761)) & np.uint64(0xFFFFFFFF)
+    mirror = (h32.astype(np.float64) / 4294967296.0 < 0.3).astype(np.uint8)
+    ctx6.set_mirrors(mirror)
+    w, h = (int(x) for x in g["render_wh"])
+    img = ctx6.render(g["camera"], g["lights"], w, h, hk.VARIANTS[variant], hk.SHADE_MIRROR)
+    ovar = O_ROPES if variant == "ropes" else O_SHORT
+    tree = oracle.make_tree(g["verts"], g["tris"], g["ref_cache"], g["ref_nodes"], g["ref_refs"], g["box"],
+                            with_ropes=(ovar == O_ROPES))
+    oimg = oracle.render_mirror(tree, g["render_rays"], w, h, g["lights"], mirror, ovar, 6, NORM_IEEE)
+    assert np.array_equal(img, oimg)
+    assert (img != ctx6.render(g["camera"], g["lights"], w, h, hk.VARIANTS[variant])).any()
