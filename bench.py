@@ -48,6 +48,9 @@ def parse():
     ap.add_argument("--workload", default="animated", choices=["animated", "static_small", "static_large"])
     ap.add_argument("--mode", default="binned", choices=["binned", "learned"])
     ap.add_argument("--variant", default="ropes")
+    ap.add_argument("--weights", default=os.path.join(os.path.dirname(os.path.abspath(__file__)), "hulktracer_b200",
+                                                      "weights", "proposer.bin"),
+                    help="trained proposer weights (learned mode)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-frames", type=int, default=2)
     return ap.parse_args()
@@ -230,6 +233,8 @@ def run_ours(args):
     stream = torch.cuda.Stream()
     ctx = hk.Context(device=local)
     ctx.set_stream(stream.cuda_stream)
+    if mode == hk.BUILD_LEARNED:
+        ctx.mlp_load(args.weights)
     ctx.upload(sc.verts, sc.tris)
     animated = sc.part_of_vertex is not None
     if animated:

@@ -56,6 +56,8 @@ class TreeStats(C.Structure):
 
 
 NOALLOC_SCRATCH_BYTES = 24 << 20
+MLP_IN, MLP_HID, MLP_OUT = 200, 256, 96
+MLP_PARAMS = 200 * 256 + 256 + 2 * (256 * 256 + 256) + 256 * 96 + 96
 
 HIT_DTYPE = np.dtype([("t", np.float32), ("tri", np.int32)])
 
@@ -105,6 +107,16 @@ def load(path: str = LIB_PATH):
         "hk_frame_graph_info": [vp, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)],
         "hk_render_noalloc": [vp, vp, vp, u32, f32p, f32p, f32p, u32, u32, u32, C.c_int, vp, vp],
         "hk_autotune": [vp, vp, u32, C.c_char_p, C.POINTER(TuneResult)],
+        "hk_mlp_init": [vp, C.c_uint64],
+        "hk_mlp_save": [vp, C.c_char_p],
+        "hk_mlp_load": [vp, C.c_char_p],
+        "hk_mlp_get_params": [vp, f32p, u32],
+        "hk_mlp_set_params": [vp, f32p, u32],
+        "hk_mlp_forward": [vp, f32p, u32, f32p],
+        "hk_mlp_grad": [vp, f32p, vp, u32, f32p, vp],
+        "hk_mlp_record": [vp, u32],
+        "hk_mlp_dataset": [vp, f32p, vp, u32, C.POINTER(C.c_uint32)],
+        "hk_mlp_train": [vp, u32, u32, C.c_float, C.c_uint64, f32p],
         "hk_batch_create": [vp, C.POINTER(C.c_void_p)],
         "hk_batch_destroy": [vp],
         "hk_batch_add_scene": [vp, f32p, u32, u32p, u32, C.POINTER(C.c_uint32)],

@@ -12,6 +12,8 @@
 #include "hk_build.h"
 #include "hk_common.cuh"
 #include "hk_internal.h"
+#include "hk_mlp.h"
+#include <random>
 
 using namespace hk;
 
@@ -102,6 +104,16 @@ struct hk_ctx {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     uint64_t last_primary = 0;
     int last_shade = HK_SHADE_CPU;
+    // learned split proposer
+    LearnBuffers learn;
+    DevBuf<float> mlp_params, mlp_grads, mlp_m, mlp_v;
+    DevBuf<uint32_t> mlp_w1p, mlp_w2p, mlp_w3p, mlp_w4p;
+    int mlp_step = 0;
+    DevBuf<float> rec_X;
+    DevBuf<int32_t> rec_y;
+    DevBuf<uint32_t> rec_rows;
+    uint32_t rec_cap = 0;
+    bool recording = false;
 };
 
 // current tree arrays (imported or built)
@@ -160,6 +172,7 @@ static hk_status validate_config(const hk_config *c) {
     if (c->bins != 32) return HK_E_ILLEGAL_INPUT;
     if (c->max_depth < 1 || c->max_depth > 48) return HK_E_ILLEGAL_INPUT;
     if (!(c->intersect_cost > 0) || !(c->traverse_cost >= 0)) return HK_E_ILLEGAL_INPUT;
+    if (c->topk < 1 || c->topk > 8 || !(c->fallback_ratio >= 0)) return HK_E_ILLEGAL_INPUT;
     return HK_OK;
 }
 
@@ -213,6 +226,9 @@ hk_status hk_destroy(hk_ctx *c) {
     c->mirror.release(); c->mrays.release(); c->prays.release(); c->mhits.release(); c->phits.release();
     c->mslot.release(); c->mcount.release();
     build_release(c->build);
+    c->mlp_params.release(); c->mlp_grads.release(); c->mlp_m.release(); c->mlp_v.release();
+    c->mlp_w1p.release(); c->mlp_w2p.release(); c->mlp_w3p.release(); c->mlp_w4p.release();
+    c->rec_X.release(); c->rec_y.release(); c->rec_rows.release();
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
@@ -566,6 +582,8 @@ static BuildParams build_params(hk_ctx *c, hk_build_mode mode) {
     p.mode = (int)mode;
     p.topk = c->cfg.topk;
     p.fallback_ratio = c->cfg.fallback_ratio;
+    p.record = c->recording ? 1 : 0;
+    c->build.learn = &c->learn;
     return p;
 }
 
@@ -1251,6 +1269,307 @@ hk_status hk_autotune(hk_ctx *c, const float *d_rays8, uint32_t n, const char *c
     }
     if (res) *res = r;
     return check_err_word(c);
+}
+
+// ---------------------------------------------------------------------------
+// learned split proposer: parameters, inference, training
+// ---------------------------------------------------------------------------
+static hk_status mlp_alloc(hk_ctx *c) {
+    HK_CUDA(c, c->mlp_params.ensure(kMlpParams));
+    HK_CUDA(c, c->mlp_grads.ensure(kMlpParams));
+    HK_CUDA(c, c->mlp_m.ensure(kMlpParams));
+    HK_CUDA(c, c->mlp_v.ensure(kMlpParams));
+    HK_CUDA(c, c->mlp_w1p.ensure(packed_words(kMlpIn, kMlpHid)));
+    HK_CUDA(c, c->mlp_w2p.ensure(packed_words(kMlpHid, kMlpHid)));
+    HK_CUDA(c, c->mlp_w3p.ensure(packed_words(kMlpHid, kMlpHid)));
+    HK_CUDA(c, c->mlp_w4p.ensure(packed_words(kMlpHid, kMlpOut)));
+    return HK_OK;
+}
+
+// BF16 fragment copies of the current FP32 weights
+static hk_status mlp_pack(hk_ctx *c) {
+    const float *P = c->mlp_params.p;
+    HK_CUDA(c, mlp_setup());
+    HK_CUDA(c, pack_b(P + kOffW1, kMlpIn, kMlpHid, c->mlp_w1p.p, c->stream));
+    HK_CUDA(c, pack_b(P + kOffW2, kMlpHid, kMlpHid, c->mlp_w2p.p, c->stream));
+    HK_CUDA(c, pack_b(P + kOffW3, kMlpHid, kMlpHid, c->mlp_w3p.p, c->stream));
+    HK_CUDA(c, pack_b(P + kOffW4, kMlpHid, kMlpOut, c->mlp_w4p.p, c->stream));
+    MlpDevice &M = c->learn.mlp;
+    M.w1p = c->mlp_w1p.p;
+    M.w2p = c->mlp_w2p.p;
+    M.w3p = c->mlp_w3p.p;
+    M.w4p = c->mlp_w4p.p;
+    M.b1 = P + kOffB1;
+    M.b2 = P + kOffB2;
+    M.b3 = P + kOffB3;
+    M.b4 = P + kOffB4;
+    c->learn.have_mlp = true;
+    invalidate_graph(c);
+    HK_CUDA(c, cudaStreamSynchronize(c->stream));
+    return HK_OK;
+}
+
+static hk_status mlp_upload(hk_ctx *c, const float *params) {
+    hk_status s = mlp_alloc(c);
+    if (s != HK_OK) return s;
+    HK_CUDA(c, cudaMemcpyAsync(c->mlp_params.p, params, kMlpParams * 4, cudaMemcpyHostToDevice, c->stream));
+    HK_CUDA(c, cudaMemsetAsync(c->mlp_m.p, 0, kMlpParams * 4, c->stream));
+    HK_CUDA(c, cudaMemsetAsync(c->mlp_v.p, 0, kMlpParams * 4, c->stream));
+    c->mlp_step = 0;
+    return mlp_pack(c);
+}
+
+hk_status hk_mlp_init(hk_ctx *c, uint64_t seed) {
+    if (!c) return HK_E_ILLEGAL_INPUT;
+    cudaSetDevice(c->device);
+    std::vector<float> P(kMlpParams, 0.0f);
+    std::mt19937_64 rng(seed);
+    auto he = [&](size_t off, int fan_in, size_t n) {
+        std::normal_distribution<float> nd(0.0f, std::sqrt(2.0f / (float)fan_in));
+        for (size_t i = 0; i < n; i++) P[off + i] = nd(rng);
+    };
+    he(kOffW1, kMlpIn, (size_t)kMlpIn * kMlpHid);
+    he(kOffW2, kMlpHid, (size_t)kMlpHid * kMlpHid);
+    he(kOffW3, kMlpHid, (size_t)kMlpHid * kMlpHid);
+    he(kOffW4, kMlpHid, (size_t)kMlpHid * kMlpOut);
+    return mlp_upload(c, P.data());
+}
+
+static const char kMlpMagic[8] = {'H', 'K', 'M', 'L', 'P', '1', 0, 0};
+
+hk_status hk_mlp_save(hk_ctx *c, const char *path) {
+    if (!c || !path) return HK_E_ILLEGAL_INPUT;
+    if (!c->learn.have_mlp) return fail(c, HK_E_STATE, "no network");
+    cudaSetDevice(c->device);
+    std::vector<float> P(kMlpParams);
+    HK_CUDA(c, cudaMemcpyAsync(P.data(), c->mlp_params.p, kMlpParams * 4, cudaMemcpyDeviceToHost, c->stream));
+    HK_CUDA(c, cudaStreamSynchronize(c->stream));
+    FILE *f = fopen(path, "wb");
+    if (!f) return fail(c, HK_E_FILE_OPEN, "cannot open weights file for writing");
+    uint32_t hdr[4] = {1u, (uint32_t)kMlpIn, (uint32_t)kMlpHid, (uint32_t)kMlpOut};
+    uint32_t n = (uint32_t)kMlpParams;
+    bool ok = fwrite(kMlpMagic, 1, 8, f) == 8 && fwrite(hdr, 4, 4, f) == 4 && fwrite(&n, 4, 1, f) == 1 &&
+              fwrite(P.data(), 4, kMlpParams, f) == kMlpParams;
+    if (fclose(f) != 0 || !ok) return fail(c, HK_E_FILE_CLOSE, "weights file write failed");
+    return HK_OK;
+}
+
+hk_status hk_mlp_load(hk_ctx *c, const char *path) {
+    if (!c || !path) return HK_E_ILLEGAL_INPUT;
+    cudaSetDevice(c->device);
+    FILE *f = fopen(path, "rb");
+    if (!f) return fail(c, HK_E_FILE_OPEN, "cannot open weights file");
+    char magic[8];
+    uint32_t hdr[4], n = 0;
+    std::vector<float> P(kMlpParams);
+    bool ok = fread(magic, 1, 8, f) == 8 && memcmp(magic, kMlpMagic, 8) == 0 && fread(hdr, 4, 4, f) == 4 &&
+              hdr[0] == 1u && hdr[1] == (uint32_t)kMlpIn && hdr[2] == (uint32_t)kMlpHid &&
+              hdr[3] == (uint32_t)kMlpOut && fread(&n, 4, 1, f) == 1 && n == kMlpParams &&
+              fread(P.data(), 4, kMlpParams, f) == kMlpParams;
+    fclose(f);
+    if (!ok) return fail(c, HK_E_ILLEGAL_INPUT, "not a proposer weights file of this network");
+    return mlp_upload(c, P.data());
+}
+
+hk_status hk_mlp_get_params(hk_ctx *c, float *params, uint32_t n) {
+    if (!c || !params || n != kMlpParams) return HK_E_ILLEGAL_INPUT;
+    if (!c->learn.have_mlp) return fail(c, HK_E_STATE, "no network");
+    cudaSetDevice(c->device);
+    HK_CUDA(c, cudaMemcpyAsync(params, c->mlp_params.p, kMlpParams * 4, cudaMemcpyDeviceToHost, c->stream));
+    HK_CUDA(c, cudaStreamSynchronize(c->stream));
+    return HK_OK;
+}
+
+hk_status hk_mlp_set_params(hk_ctx *c, const float *params, uint32_t n) {
+    if (!c || !params || n != kMlpParams) return HK_E_ILLEGAL_INPUT;
+    cudaSetDevice(c->device);
+    return mlp_upload(c, params);
+}
+
+hk_status hk_mlp_forward(hk_ctx *c, const float *X, uint32_t n, float *logits) {
+    if (!c || (n && (!X || !logits))) return HK_E_ILLEGAL_INPUT;
+    if (!c->learn.have_mlp) return fail(c, HK_E_STATE, "no network");
+    cudaSetDevice(c->device);
+    DevBuf<float> dx, dl;
+    HK_CUDA(c, dx.ensure((size_t)n * kMlpIn));
+    HK_CUDA(c, dl.ensure((size_t)n * kMlpOut));
+    HK_CUDA(c, cudaMemcpyAsync(dx.p, X, (size_t)n * kMlpIn * 4, cudaMemcpyHostToDevice, c->stream));
+    HK_CUDA(c, mlp_infer(c->learn.mlp, dx.p, nullptr, n, dl.p, c->sm_count, c->stream));
+    HK_CUDA(c, cudaMemcpyAsync(logits, dl.p, (size_t)n * kMlpOut * 4, cudaMemcpyDeviceToHost, c->stream));
+    HK_CUDA(c, cudaStreamSynchronize(c->stream));
+    dx.release();
+    dl.release();
+    return HK_OK;
+}
+
+// FP32 forward + backward of rows Xb (device) with labels yb; gradients into
+// c->mlp_grads, summed loss into *dloss (device)
+struct MlpWork {
+    DevBuf<float> H1, H2, H3, Z4, d1, d2, d3, d4, loss;
+    cudaError_t ensure(uint32_t B) {
+        cudaError_t e;
+        if ((e = H1.ensure((size_t)B * kMlpHid)) || (e = H2.ensure((size_t)B * kMlpHid)) ||
+            (e = H3.ensure((size_t)B * kMlpHid)) || (e = Z4.ensure((size_t)B * kMlpOut)) ||
+            (e = d1.ensure((size_t)B * kMlpHid)) || (e = d2.ensure((size_t)B * kMlpHid)) ||
+            (e = d3.ensure((size_t)B * kMlpHid)) || (e = d4.ensure((size_t)B * kMlpOut)) || (e = loss.ensure(1)))
+            return e;
+        return cudaSuccess;
+    }
+    void release() {
+        H1.release(); H2.release(); H3.release(); Z4.release();
+        d1.release(); d2.release(); d3.release(); d4.release(); loss.release();
+    }
+};
+
+static hk_status mlp_fwd_bwd(hk_ctx *c, MlpWork &W, const float *Xb, const int32_t *yb, int B) {
+    const float *P = c->mlp_params.p;
+    float *G = c->mlp_grads.p;
+    cudaStream_t s = c->stream;
+    const int I = kMlpIn, Hd = kMlpHid, O = kMlpOut;
+    HK_CUDA(c, sgemm(false, false, Xb, P + kOffW1, W.H1.p, P + kOffB1, B, Hd, I, I, Hd, Hd, true, false, s));
+    HK_CUDA(c, sgemm(false, false, W.H1.p, P + kOffW2, W.H2.p, P + kOffB2, B, Hd, Hd, Hd, Hd, Hd, true, false, s));
+    HK_CUDA(c, sgemm(false, false, W.H2.p, P + kOffW3, W.H3.p, P + kOffB3, B, Hd, Hd, Hd, Hd, Hd, true, false, s));
+    HK_CUDA(c, sgemm(false, false, W.H3.p, P + kOffW4, W.Z4.p, P + kOffB4, B, O, Hd, Hd, O, O, false, false, s));
+    HK_CUDA(c, softmax_xent(W.Z4.p, yb, B, W.d4.p, W.loss.p, s));
+    // layer 4
+    HK_CUDA(c, sgemm(true, false, W.H3.p, W.d4.p, G + kOffW4, nullptr, Hd, O, B, Hd, O, O, false, false, s));
+    HK_CUDA(c, colsum(W.d4.p, B, O, G + kOffB4, s));
+    HK_CUDA(c, sgemm(false, true, W.d4.p, P + kOffW4, W.d3.p, nullptr, B, Hd, O, O, O, Hd, false, false, s));
+    HK_CUDA(c, relu_back(W.d3.p, W.H3.p, (size_t)B * Hd, s));
+    // layer 3
+    HK_CUDA(c, sgemm(true, false, W.H2.p, W.d3.p, G + kOffW3, nullptr, Hd, Hd, B, Hd, Hd, Hd, false, false, s));
+    HK_CUDA(c, colsum(W.d3.p, B, Hd, G + kOffB3, s));
+    HK_CUDA(c, sgemm(false, true, W.d3.p, P + kOffW3, W.d2.p, nullptr, B, Hd, Hd, Hd, Hd, Hd, false, false, s));
+    HK_CUDA(c, relu_back(W.d2.p, W.H2.p, (size_t)B * Hd, s));
+    // layer 2
+    HK_CUDA(c, sgemm(true, false, W.H1.p, W.d2.p, G + kOffW2, nullptr, Hd, Hd, B, Hd, Hd, Hd, false, false, s));
+    HK_CUDA(c, colsum(W.d2.p, B, Hd, G + kOffB2, s));
+    HK_CUDA(c, sgemm(false, true, W.d2.p, P + kOffW2, W.d1.p, nullptr, B, Hd, Hd, Hd, Hd, Hd, false, false, s));
+    HK_CUDA(c, relu_back(W.d1.p, W.H1.p, (size_t)B * Hd, s));
+    // layer 1
+    HK_CUDA(c, sgemm(true, false, Xb, W.d1.p, G + kOffW1, nullptr, I, Hd, B, I, Hd, Hd, false, false, s));
+    HK_CUDA(c, colsum(W.d1.p, B, Hd, G + kOffB1, s));
+    return HK_OK;
+}
+
+hk_status hk_mlp_grad(hk_ctx *c, const float *X, const int32_t *y, uint32_t n, float *grads, float *loss) {
+    if (!c || !X || !y || n == 0 || !grads) return HK_E_ILLEGAL_INPUT;
+    if (!c->learn.have_mlp) return fail(c, HK_E_STATE, "no network");
+    for (uint32_t i = 0; i < n; i++)
+        if (y[i] < 0 || y[i] >= kMlpOut) return fail(c, HK_E_ILLEGAL_INPUT, "label out of range");
+    cudaSetDevice(c->device);
+    DevBuf<float> dx;
+    DevBuf<int32_t> dy;
+    MlpWork W;
+    HK_CUDA(c, dx.ensure((size_t)n * kMlpIn));
+    HK_CUDA(c, dy.ensure(n));
+    HK_CUDA(c, W.ensure(n));
+    HK_CUDA(c, cudaMemcpyAsync(dx.p, X, (size_t)n * kMlpIn * 4, cudaMemcpyHostToDevice, c->stream));
+    HK_CUDA(c, cudaMemcpyAsync(dy.p, y, (size_t)n * 4, cudaMemcpyHostToDevice, c->stream));
+    HK_CUDA(c, cudaMemsetAsync(W.loss.p, 0, 4, c->stream));
+    hk_status st = mlp_fwd_bwd(c, W, dx.p, dy.p, (int)n);
+    if (st != HK_OK) return st;
+    float ls = 0;
+    HK_CUDA(c, cudaMemcpyAsync(grads, c->mlp_grads.p, kMlpParams * 4, cudaMemcpyDeviceToHost, c->stream));
+    HK_CUDA(c, cudaMemcpyAsync(&ls, W.loss.p, 4, cudaMemcpyDeviceToHost, c->stream));
+    HK_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (loss) *loss = ls / (float)n;
+    dx.release();
+    dy.release();
+    W.release();
+    return HK_OK;
+}
+
+hk_status hk_mlp_record(hk_ctx *c, uint32_t cap) {
+    if (!c) return HK_E_ILLEGAL_INPUT;
+    cudaSetDevice(c->device);
+    invalidate_graph(c);
+    if (cap == 0) {
+        c->recording = false;
+        return HK_OK;
+    }
+    HK_CUDA(c, c->rec_X.ensure((size_t)cap * kMlpIn));
+    HK_CUDA(c, c->rec_y.ensure(cap));
+    HK_CUDA(c, c->rec_rows.ensure(1));
+    HK_CUDA(c, cudaMemsetAsync(c->rec_rows.p, 0, 4, c->stream));
+    HK_CUDA(c, cudaStreamSynchronize(c->stream));
+    c->rec_cap = cap;
+    c->learn.rec_X = c->rec_X.p;
+    c->learn.rec_y = c->rec_y.p;
+    c->learn.rec_rows = c->rec_rows.p;
+    c->learn.rec_cap = cap;
+    c->recording = true;
+    return HK_OK;
+}
+
+static hk_status dataset_rows(hk_ctx *c, uint32_t *rows) {
+    uint32_t r = 0;
+    if (c->rec_rows.p) {
+        HK_CUDA(c, cudaMemcpyAsync(&r, c->rec_rows.p, 4, cudaMemcpyDeviceToHost, c->stream));
+        HK_CUDA(c, cudaStreamSynchronize(c->stream));
+    }
+    *rows = std::min(r, c->rec_cap);
+    return HK_OK;
+}
+
+hk_status hk_mlp_dataset(hk_ctx *c, float *X, int32_t *y, uint32_t cap, uint32_t *rows) {
+    if (!c || !rows) return HK_E_ILLEGAL_INPUT;
+    cudaSetDevice(c->device);
+    uint32_t r;
+    hk_status st = dataset_rows(c, &r);
+    if (st != HK_OK) return st;
+    *rows = r;
+    if (!X && !y) return HK_OK;
+    if (cap < r) return fail(c, HK_E_CAPACITY, "dataset buffers too small");
+    if (X && r) HK_CUDA(c, cudaMemcpyAsync(X, c->rec_X.p, (size_t)r * kMlpIn * 4, cudaMemcpyDeviceToHost, c->stream));
+    if (y && r) HK_CUDA(c, cudaMemcpyAsync(y, c->rec_y.p, (size_t)r * 4, cudaMemcpyDeviceToHost, c->stream));
+    HK_CUDA(c, cudaStreamSynchronize(c->stream));
+    return HK_OK;
+}
+
+hk_status hk_mlp_train(hk_ctx *c, uint32_t epochs, uint32_t batch, float lr, uint64_t seed, float *epoch_loss) {
+    if (!c || epochs == 0 || batch == 0 || batch > 65536 || !(lr > 0)) return HK_E_ILLEGAL_INPUT;
+    if (!c->learn.have_mlp) return fail(c, HK_E_STATE, "hk_mlp_init or hk_mlp_load first");
+    cudaSetDevice(c->device);
+    uint32_t rows;
+    hk_status st = dataset_rows(c, &rows);
+    if (st != HK_OK) return st;
+    if (rows < batch) return fail(c, HK_E_STATE, "fewer recorded rows than one batch");
+    DevBuf<uint32_t> perm;
+    DevBuf<float> Xb;
+    DevBuf<int32_t> yb;
+    MlpWork W;
+    HK_CUDA(c, perm.ensure(rows));
+    HK_CUDA(c, Xb.ensure((size_t)batch * kMlpIn));
+    HK_CUDA(c, yb.ensure(batch));
+    HK_CUDA(c, W.ensure(batch));
+    std::vector<uint32_t> idx(rows);
+    std::mt19937_64 rng(seed);
+    for (uint32_t e = 0; e < epochs; e++) {
+        for (uint32_t i = 0; i < rows; i++) idx[i] = i;
+        std::shuffle(idx.begin(), idx.end(), rng);
+        HK_CUDA(c, cudaMemcpyAsync(perm.p, idx.data(), (size_t)rows * 4, cudaMemcpyHostToDevice, c->stream));
+        HK_CUDA(c, cudaMemsetAsync(W.loss.p, 0, 4, c->stream));
+        uint32_t nb = rows / batch;
+        for (uint32_t b = 0; b < nb; b++) {
+            HK_CUDA(c, gather_rows(c->rec_X.p, c->rec_y.p, perm.p + (size_t)b * batch, (int)batch, Xb.p, yb.p,
+                                   c->stream));
+            st = mlp_fwd_bwd(c, W, Xb.p, yb.p, (int)batch);
+            if (st != HK_OK) return st;
+            c->mlp_step++;
+            HK_CUDA(c, adam(c->mlp_params.p, c->mlp_grads.p, c->mlp_m.p, c->mlp_v.p, kMlpParams, lr, c->mlp_step,
+                            c->stream));
+        }
+        float ls = 0;
+        HK_CUDA(c, cudaMemcpyAsync(&ls, W.loss.p, 4, cudaMemcpyDeviceToHost, c->stream));
+        HK_CUDA(c, cudaStreamSynchronize(c->stream));
+        if (epoch_loss) epoch_loss[e] = ls / (float)(nb * batch);
+    }
+    perm.release();
+    Xb.release();
+    yb.release();
+    W.release();
+    return mlp_pack(c);
 }
 
 }  // extern "C"

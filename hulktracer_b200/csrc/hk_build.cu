@@ -222,6 +222,7 @@ struct Decision {
     float plane;
     uint32_t nb, na;
     float cost;
+    int bin;      // plane index k of the chosen plane
 };
 
 // Warp-wide SAH over the node's histograms (all 32 lanes call it). The
@@ -230,7 +231,7 @@ template <class HistPtr>
 __device__ Decision sah_warp(HistPtr H, float4 blo, float4 bhi, uint32_t cnt, float ct, float ci) {
     const uint32_t lane = threadIdx.x & 31u;
     float A = surf(blo, bhi);
-    Decision best{-1, 0.0f, 0, 0, kInf};
+    Decision best{-1, 0.0f, 0, 0, kInf, 0};
     for (uint32_t a = 0; a < 3; a++) {
         float l = c3(blo, a), h = c3(bhi, a);
         float ext = __fsub_rn(h, l);
@@ -277,6 +278,7 @@ __device__ Decision sah_warp(HistPtr H, float4 blo, float4 bhi, uint32_t cnt, fl
             best.plane = __shfl_sync(0xffffffffu, pk, mk);
             best.nb = __shfl_sync(0xffffffffu, nb, mk);
             best.na = __shfl_sync(0xffffffffu, na, mk);
+            best.bin = (int)mk;
         }
     }
     if (best.axis >= 0 && !(best.cost < __fmul_rn(ci, (float)cnt))) best.axis = -1;
@@ -315,6 +317,15 @@ struct LevelArgs {
     float ct, ci;
     uint32_t max_depth, leaf_size;
     uint32_t cap_refs, cap_nodes, cap_level, cap_large, cap_chunks;
+    // learned proposer
+    int learned, record;
+    uint32_t *lrank;        // node slot -> proposer row (0xffffffff: none)
+    float *feat, *logits;
+    float *rec_X;
+    int32_t *rec_y;
+    uint32_t *rec_rows, rec_cap;
+    float fallback_ratio;
+    uint32_t topk;
 };
 
 __global__ void k_tri_bounds(const float4 *__restrict__ V, const uint4 *__restrict__ T, uint32_t nt, float4 *lo,
@@ -361,6 +372,7 @@ __global__ void k_prep(LevelArgs A) {
     const uint32_t n = A.lc->nodes;
     for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
         uint32_t cnt = A.n_info[s].y;
+        if (A.learned) A.lrank[s] = 0xffffffffu;
         if (!(decidable(A, cnt) && cnt > kSmall)) continue;
         uint32_t nch = (cnt + kChunk - 1) / kChunk;
         uint32_t rank = atomicAdd(&A.lc->n_large, 1u);
@@ -370,6 +382,7 @@ __global__ void k_prep(LevelArgs A) {
             continue;
         }
         A.large_slot[rank] = s;
+        if (A.learned) A.lrank[s] = rank;   // the proposer row of the node
         for (uint32_t k = 0; k < nch; k++) A.chunks[first + k] = make_uint2(rank, k);
         uint32_t *H = A.hist + (size_t)rank * kHist;
         for (uint32_t k = 0; k < kHist; k++) H[k] = 0;
@@ -389,6 +402,69 @@ struct GHist {
     __device__ uint32_t operator[](uint32_t i) const { return __ldcg(p + i); }
 };
 
+// ---------------------------------------------------------------------------
+// proposer features of one node (one warp): from at most 64 references taken
+// at a fixed stride, per axis a 32-bin histogram of clipped centroids and
+// 16-bin histograms of clipped lower / upper bounds (fractions of the sample),
+// the extents over the largest extent, depth / max_depth, 4 zeros = 200.
+// Counts are exact small integers, so the order of the shared atomics does
+// not matter.
+// ---------------------------------------------------------------------------
+constexpr uint32_t kFeatSample = 64;
+
+__device__ void node_features(const LevelArgs &A, uint4 info, float4 blo, float4 bhi, float *sh, float *out) {
+    const uint32_t lane = threadIdx.x & 31u;
+    for (uint32_t i = lane; i < 200; i += 32) sh[i] = 0.0f;
+    __syncwarp();
+    const uint32_t cnt = info.y;
+    const uint32_t S = cnt < kFeatSample ? cnt : kFeatSample;
+    for (uint32_t i = lane; i < S; i += 32) {
+        uint32_t r = info.x + (uint32_t)(((uint64_t)i * cnt) / S);
+        uint32_t tri = A.refs[r];
+        float4 tlo = A.tb_lo[tri], thi = A.tb_hi[tri];
+        for (uint32_t a = 0; a < 3; a++) {
+            float l = c3(blo, a), h = c3(bhi, a), ext = h - l;
+            if (!(ext > 0.0f)) continue;
+            float lo = mxf(c3(tlo, a), l), hi = mnf(c3(thi, a), h);
+            float c = (lo + hi) * 0.5f;
+            int b32 = (int)((c - l) * (32.0f / ext));
+            int blo16 = (int)((lo - l) * (16.0f / ext));
+            int bhi16 = (int)((hi - l) * (16.0f / ext));
+            b32 = b32 < 0 ? 0 : (b32 > 31 ? 31 : b32);
+            blo16 = blo16 < 0 ? 0 : (blo16 > 15 ? 15 : blo16);
+            bhi16 = bhi16 < 0 ? 0 : (bhi16 > 15 ? 15 : bhi16);
+            atomicAdd(&sh[a * 32 + b32], 1.0f);
+            atomicAdd(&sh[96 + a * 32 + blo16], 1.0f);
+            atomicAdd(&sh[96 + a * 32 + 16 + bhi16], 1.0f);
+        }
+    }
+    __syncwarp();
+    const float inv = S ? 1.0f / (float)S : 0.0f;
+    for (uint32_t i = lane; i < 192; i += 32) out[i] = sh[i] * inv;
+    if (lane == 0) {
+        float ex = bhi.x - blo.x, ey = bhi.y - blo.y, ez = bhi.z - blo.z;
+        float m = fmaxf(ex, fmaxf(ey, ez));
+        float im = m > 0.0f ? 1.0f / m : 0.0f;
+        out[192] = ex * im;
+        out[193] = ey * im;
+        out[194] = ez * im;
+        out[195] = (float)A.level / (float)A.max_depth;
+        out[196] = out[197] = out[198] = out[199] = 0.0f;
+    }
+    __syncwarp();
+}
+
+// binned mode, recording: (features, label) of a node the exact SAH split
+__device__ void record_node(const LevelArgs &A, uint4 info, float4 blo, float4 bhi, const Decision &d, float *sh) {
+    if (!A.record || d.axis < 0 || info.y <= kSmall) return;
+    uint32_t row = 0;
+    if ((threadIdx.x & 31u) == 0) row = atomicAdd(A.rec_rows, 1u);
+    row = __shfl_sync(0xffffffffu, row, 0);
+    if (row >= A.rec_cap) return;
+    node_features(A, info, blo, bhi, sh, A.rec_X + (size_t)row * 200);
+    if ((threadIdx.x & 31u) == 0) A.rec_y[row] = d.axis * 32 + d.bin;
+}
+
 // Work items: first the chunks of large nodes (one CTA each; the CTA that
 // finishes a node's last chunk evaluates its SAH), then groups of 8 small
 // nodes (one warp each: warp-private histogram + SAH).
@@ -402,6 +478,7 @@ __global__ void __launch_bounds__(256) k_work(LevelArgs A) {
     const uint32_t ngroups = (nodes + 7) / 8;
     for (uint32_t item = blockIdx.x; item < nch + ngroups; item += gridDim.x) {
         if (item < nch) {
+            if (A.learned) continue;  // learned mode: chunks are costed by k_propose
             uint2 ck = A.chunks[item];
             uint32_t rank = ck.x;
             if (rank >= A.cap_large) continue;  // uniform per CTA
@@ -431,6 +508,7 @@ __global__ void __launch_bounds__(256) k_work(LevelArgs A) {
                 __threadfence();
                 Decision d = sah_warp(GHist{G}, blo, bhi, info.y, A.ct, A.ci);
                 if (lane == 0) write_decision(A, s, d);
+                record_node(A, info, blo, bhi, d, reinterpret_cast<float *>(HS[0]));
             }
             __syncthreads();
         } else {
@@ -439,9 +517,18 @@ __global__ void __launch_bounds__(256) k_work(LevelArgs A) {
             uint4 info = A.n_info[s];
             uint32_t cnt = info.y;
             bool dec = decidable(A, cnt);
-            if (dec && cnt > kSmall) continue;  // large: handled by its chunks
+            if (dec && cnt > kSmall) {
+                // learned mode: the proposer's features instead of histograms
+                if (A.learned) {
+                    uint32_t row = A.lrank[s];
+                    if (row < A.cap_large)
+                        node_features(A, info, A.n_lo[s], A.n_hi[s], reinterpret_cast<float *>(HS[wib]),
+                                      A.feat + (size_t)row * 200);
+                }
+                continue;  // binned mode: handled by its chunks
+            }
             if (!dec) {
-                if (lane == 0) write_decision(A, s, Decision{-1, 0.0f, 0, 0, kInf});
+                if (lane == 0) write_decision(A, s, Decision{-1, 0.0f, 0, 0, kInf, 0});
                 continue;
             }
             uint32_t *Hw = HS[wib];
@@ -460,6 +547,208 @@ __global__ void __launch_bounds__(256) k_work(LevelArgs A) {
     }
 }
 
+// ---------------------------------------------------------------------------
+// learned proposals. Per proposer row (a large node), the valid planes (those
+// the binned search would cost) with the top-k logits, plus a reference plane
+// -- the middle plane of the node's longest axis -- are costed exactly with
+// the partition's own classification. The references are counted in the
+// node's chunks (one CTA each, counts summed with global atomics); the CTA
+// that finishes the node's last chunk costs the candidates. The cheapest
+// proposal wins unless it costs more than fallback_ratio x the reference
+// plane, in which case that CTA runs the full binned SAH on the node.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ bool plane_valid(float l, float ext, float h, uint32_t k, float &pk) {
+    if (!(ext > 0.0f) || k < 1 || k > 31) return false;
+    pk = plane_k(l, ext, k);
+    float pk1 = plane_k(l, ext, k + 1);
+    return pk > l && pk < h && (k == 31 || pk < pk1);
+}
+
+constexpr int kMaxCand = 9;   // top-k (k <= 8) + the reference plane
+
+struct Candidates {
+    int n;          // proposals
+    int has_ref;    // candidate n is the reference plane
+    int axis[kMaxCand];
+    int bin[kMaxCand];
+    float plane[kMaxCand];
+};
+
+// warp 0: the top-k valid planes by logit (ties: lowest index) + reference
+__device__ void select_candidates(const LevelArgs &A, const float *__restrict__ L, float4 blo, float4 bhi,
+                                  Candidates &C) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t K = A.topk < 8 ? A.topk : 8;
+    float v[3];
+    float pk[3];
+    for (int j = 0; j < 3; j++) {
+        uint32_t c = lane + 32u * j, a = c / 32u, k = c % 32u;
+        float l = c3(blo, a), h = c3(bhi, a);
+        float x = L[c];
+        v[j] = plane_valid(l, __fsub_rn(h, l), h, k, pk[j]) ? (x == x ? x : -INFINITY) : NAN;
+    }
+    int n = 0;
+    for (uint32_t r = 0; r < K; r++) {
+        // lane-local best (NaN = invalid or taken)
+        float bv = NAN;
+        int bc = 1 << 30;
+        for (int j = 0; j < 3; j++)
+            if (v[j] == v[j] && (bv != bv || v[j] > bv)) {
+                bv = v[j];
+                bc = (int)lane + 32 * j;
+            }
+        for (int o = 16; o; o >>= 1) {
+            float ov = __shfl_xor_sync(0xffffffffu, bv, o);
+            int oc = __shfl_xor_sync(0xffffffffu, bc, o);
+            bool take = (ov == ov) && (bv != bv || ov > bv || (ov == bv && oc < bc));
+            if (take) {
+                bv = ov;
+                bc = oc;
+            }
+        }
+        if (bv != bv) break;  // no valid plane left (uniform across the warp)
+        if ((uint32_t)(bc & 31) == lane) {
+            int j = bc >> 5;
+            C.axis[n] = bc / 32;
+            C.bin[n] = bc % 32;
+            C.plane[n] = pk[j];
+            v[j] = NAN;
+        }
+        n++;
+    }
+    if (lane == 0) {
+        float ex = __fsub_rn(bhi.x, blo.x), ey = __fsub_rn(bhi.y, blo.y), ez = __fsub_rn(bhi.z, blo.z);
+        uint32_t la = (ex >= ey && ex >= ez) ? 0 : (ey >= ez ? 1 : 2);
+        float p;
+        C.has_ref = plane_valid(c3(blo, la), __fsub_rn(c3(bhi, la), c3(blo, la)), c3(bhi, la), 16, p) ? 1 : 0;
+        if (C.has_ref) {
+            C.axis[n] = (int)la;
+            C.plane[n] = p;
+            C.bin[n] = 16;
+        }
+        C.n = n;
+    }
+    __syncwarp();
+}
+
+__global__ void __launch_bounds__(256) k_propose(LevelArgs A) {
+    __shared__ uint32_t H[kHist];
+    __shared__ Candidates C;
+    __shared__ uint32_t s_cnt[2 * kMaxCand];
+    __shared__ int s_last, s_fallback;
+    const uint32_t nch = min(A.lc->n_chunks, A.cap_chunks);
+    const uint32_t nodes = A.lc->nodes;
+    for (uint32_t item = blockIdx.x; item < nch; item += gridDim.x) {
+        const uint2 ck = A.chunks[item];
+        const uint32_t rank = ck.x;
+        if (rank >= A.cap_large) continue;  // uniform per CTA
+        const uint32_t s = A.large_slot[rank];
+        if (s >= nodes) continue;
+        const uint4 info = A.n_info[s];
+        const float4 blo = A.n_lo[s], bhi = A.n_hi[s];
+        if (threadIdx.x < 32) select_candidates(A, A.logits + (size_t)rank * kMlpOut, blo, bhi, C);
+        if (threadIdx.x < 2 * kMaxCand) s_cnt[threadIdx.x] = 0;
+        __syncthreads();
+        const int nc = C.n + C.has_ref;
+        // exact below / above counts of every candidate over this chunk
+        const uint32_t r0 = info.x + ck.y * kChunk, r1 = min(info.x + info.y, r0 + kChunk);
+        uint32_t nb[kMaxCand], na[kMaxCand];
+#pragma unroll
+        for (int i = 0; i < kMaxCand; i++) nb[i] = na[i] = 0;
+        for (uint32_t r = r0 + threadIdx.x; r < r1; r += blockDim.x) {
+            const uint32_t tri = A.refs[r];
+            const float4 tlo = A.tb_lo[tri], thi = A.tb_hi[tri];
+#pragma unroll
+            for (int i = 0; i < kMaxCand; i++) {
+                if (i >= nc) break;
+                const uint32_t a = (uint32_t)C.axis[i];
+                const float l = c3(blo, a), h = c3(bhi, a), p = C.plane[i];
+                const float lo = mxf(c3(tlo, a), l), hi = mnf(c3(thi, a), h);
+                const bool flat_on = (lo == hi) && lo == p;
+                nb[i] += (lo < p || flat_on) ? 1u : 0u;
+                na[i] += (hi > p || flat_on) ? 1u : 0u;
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < kMaxCand; i++) {
+            if (i >= nc) break;
+            uint32_t b = nb[i], a = na[i];
+            for (int o = 16; o; o >>= 1) {
+                b += __shfl_xor_sync(0xffffffffu, b, o);
+                a += __shfl_xor_sync(0xffffffffu, a, o);
+            }
+            if ((threadIdx.x & 31u) == 0) {
+                atomicAdd(&s_cnt[2 * i], b);
+                atomicAdd(&s_cnt[2 * i + 1], a);
+            }
+        }
+        __syncthreads();
+        uint32_t *G = A.hist + (size_t)rank * kHist;   // 2 x 9 counters of the row
+        if (threadIdx.x < 2 * (uint32_t)nc && s_cnt[threadIdx.x]) atomicAdd(&G[threadIdx.x], s_cnt[threadIdx.x]);
+        __threadfence();
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            const uint32_t nchunks = (info.y + kChunk - 1) / kChunk;
+            s_last = (atomicAdd(&A.done[rank], 1u) == nchunks - 1) ? 1 : 0;
+        }
+        __syncthreads();
+        if (!s_last) continue;
+        __threadfence();
+        if (threadIdx.x == 0) {
+            uint32_t cb[kMaxCand], ca[kMaxCand];
+            for (int i = 0; i < nc; i++) {
+                cb[i] = __ldcg(G + 2 * i);
+                ca[i] = __ldcg(G + 2 * i + 1);
+            }
+            const float Anode = surf(blo, bhi);
+            auto cost = [&](int i) {
+                float4 bb = bhi, ba = blo;
+                s3(bb, (uint32_t)C.axis[i], C.plane[i]);
+                s3(ba, (uint32_t)C.axis[i], C.plane[i]);
+                float sb = surf(blo, bb), sa = surf(ba, bhi);
+                return __fadd_rn(A.ct, __fmul_rn(A.ci, __fdiv_rn(__fadd_rn(__fmul_rn(sb, (float)cb[i]),
+                                                                            __fmul_rn(sa, (float)ca[i])), Anode)));
+            };
+            int bi = -1;
+            float bc = INFINITY;
+            for (int i = 0; i < C.n; i++) {
+                float ci = cost(i);
+                if (ci < bc) {
+                    bc = ci;
+                    bi = i;
+                }
+            }
+            bool fb = bi < 0 || (C.has_ref && bc > A.fallback_ratio * cost(C.n));
+            s_fallback = fb ? 1 : 0;
+            if (!fb) {
+                Decision d{C.axis[bi], C.plane[bi], cb[bi], ca[bi], bc, C.bin[bi]};
+                if (!(bc < __fmul_rn(A.ci, (float)info.y))) d.axis = -1;
+                write_decision(A, s, d);
+                atomicAdd(&A.ctr->learned_nodes, 1u);
+            } else {
+                atomicAdd(&A.ctr->fallback_nodes, 1u);
+            }
+        }
+        __syncthreads();
+        if (s_fallback) {
+            // the full binned SAH on this node
+            for (uint32_t i = threadIdx.x; i < kHist; i += blockDim.x) H[i] = 0;
+            __syncthreads();
+            for (uint32_t r = info.x + threadIdx.x; r < info.x + info.y; r += blockDim.x) {
+                uint32_t tri = A.refs[r];
+                hist_ref(H, A.tb_lo[tri], A.tb_hi[tri], blo, bhi);
+            }
+            __syncthreads();
+            if (threadIdx.x < 32) {
+                Decision d = sah_warp(H, blo, bhi, info.y, A.ct, A.ci);
+                if (threadIdx.x == 0) write_decision(A, s, d);
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
 // plan scan: (leaf refs, child pairs, next-level nodes, child refs) per node.
 // on_total (one thread, after the tile sums) is the capacity guard and writes
 // the next level's counters; on_prefix emits node s's compact entry and its
@@ -635,7 +924,8 @@ void build_release(BuildState &S) {
         S.n_lo[k] = S.n_hi[k] = nullptr; S.n_info[k] = nullptr; S.refs[k] = S.ref_node[k] = nullptr;
     }
     f(S.d_axis); f(S.d_plane); f(S.d_cnt); f(S.plan); f(S.plan_tot); f(S.prep); f(S.prep_tot);
-    f(S.chunks); f(S.hist); f(S.done); f(S.rscan); f(S.rscan_tot); f(S.scan_partials); f(S.ctr); f(S.err);
+    f(S.chunks); f(S.hist); f(S.done); f(S.lrank); f(S.feat); f(S.logits);
+    S.lrank = nullptr; S.feat = nullptr; S.logits = nullptr; f(S.rscan); f(S.rscan_tot); f(S.scan_partials); f(S.ctr); f(S.err);
     f(S.out_nodes); f(S.out_refs); f(S.out_ropes); f(S.out_cbox);
     S.tb_lo = S.tb_hi = nullptr;
     S.d_axis = nullptr; S.d_plane = nullptr; S.d_cnt = nullptr; S.plan = nullptr; S.plan_tot = nullptr;
@@ -684,6 +974,9 @@ hk_status build_prepare(BuildState &S, const BuildParams &p, uint32_t nt, int sm
     bad |= dalloc(S.chunks, S.cap_chunks + S.cap_large) != cudaSuccess;  // tail holds large_slot
     bad |= dalloc(S.hist, (size_t)S.cap_large * kHist) != cudaSuccess;
     bad |= dalloc(S.done, S.cap_large) != cudaSuccess;
+    bad |= dalloc(S.lrank, S.cap_level) != cudaSuccess;
+    bad |= dalloc(S.feat, (size_t)S.cap_large * 200) != cudaSuccess;
+    bad |= dalloc(S.logits, (size_t)S.cap_large * kMlpOut) != cudaSuccess;
     bad |= dalloc(S.rscan, cap_refs) != cudaSuccess;
     bad |= dalloc(S.rscan_tot, 1) != cudaSuccess;
     {
@@ -746,6 +1039,20 @@ cudaError_t build_launch(BuildState &S, const float4 *verts, const uint4 *tris, 
     A.cap_level = S.cap_level;
     A.cap_large = S.cap_large;
     A.cap_chunks = S.cap_chunks;
+    A.learned = (S.p.mode == HK_BUILD_LEARNED) ? 1 : 0;
+    A.record = (S.p.mode == HK_BUILD_BINNED && S.p.record && S.learn && S.learn->rec_X) ? 1 : 0;
+    A.lrank = S.lrank;
+    A.feat = S.feat;
+    A.logits = S.logits;
+    A.fallback_ratio = S.p.fallback_ratio;
+    A.topk = S.p.topk;
+    if (S.learn) {
+        A.rec_X = S.learn->rec_X;
+        A.rec_y = S.learn->rec_y;
+        A.rec_rows = S.learn->rec_rows;
+        A.rec_cap = S.learn->rec_cap;
+    }
+    if (A.learned && !(S.learn && S.learn->have_mlp)) return cudaErrorInvalidValue;
     cudaMemsetAsync(S.ctr, 0, sizeof(BuildCounters), st);
     if (nt) k_tri_bounds<<<(nt + 255) / 256, 256, 0, st>>>(verts, tris, nt, S.tb_lo, S.tb_hi);
     A.nx_lo = S.n_lo[0];
@@ -771,6 +1078,10 @@ cudaError_t build_launch(BuildState &S, const float4 *verts, const uint4 *tris, 
         A.nx_ref_node = S.ref_node[nxt];
         k_prep<<<G, 256, 0, st>>>(A);
         k_work<<<G * 2, 256, 0, st>>>(A);
+        if (A.learned) {
+            mlp_infer(S.learn->mlp, S.feat, &A.lc->n_large, S.cap_large, S.logits, G, st);
+            k_propose<<<G * 2, 256, 0, st>>>(A);
+        }
         scan<uint4>(LoadPlan{A}, reinterpret_cast<uint4 *>(S.scan_partials), S.plan, S.plan_tot, G, st);
         scan<uint2>(LoadRefFlags{A}, reinterpret_cast<uint2 *>(S.scan_partials), S.rscan, S.rscan_tot, G, st);
         k_scatter<<<G, 256, 0, st>>>(A);

@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include "../../include/hulkcuda.h"
+#include "hk_mlp.h"
 
 namespace hk {
 
@@ -17,6 +18,17 @@ struct BuildParams {
     int mode = 0;               // hk_build_mode
     uint32_t topk = 4;
     float fallback_ratio = 1.02f;
+    int record = 0;             // binned mode: append (features, label) rows
+};
+
+// learned-proposer buffers owned by the context (device pointers)
+struct LearnBuffers {
+    MlpDevice mlp{};
+    bool have_mlp = false;
+    float *rec_X = nullptr;      // recorded features [cap][200]
+    int32_t *rec_y = nullptr;    // recorded labels (axis * 32 + plane index)
+    uint32_t *rec_rows = nullptr;
+    uint32_t rec_cap = 0;
 };
 
 constexpr int kMaxLevels = 52;  // max_depth <= 48, plus the level after the last
@@ -31,7 +43,6 @@ struct LevelCounters {
     uint32_t stop;              // the level stops splitting (capacity)
     uint32_t n_large;           // large nodes (chunked histograms)
     uint32_t n_chunks;          // histogram chunks
-    uint32_t pad;
 };
 
 // device scalars of one build (one struct in device memory)
@@ -86,8 +97,11 @@ struct BuildState {
     uint32_t *out_refs = nullptr;
     uint32_t *out_ropes = nullptr;               // 6 per node: -x,+x,-y,+y,-z,+z (0xffffffff = none)
     float4 *out_cbox = nullptr;                  // 2 per node: cell min, max
-    // learned proposer (hk_mlp.cu)
-    void *mlp = nullptr;
+    // learned proposer: per-level rows (large nodes), their features and logits
+    uint32_t *lrank = nullptr;                   // node slot -> row (0xffffffff: none)
+    float *feat = nullptr;                       // [cap_large][200]
+    float *logits = nullptr;                     // [cap_large][96]
+    LearnBuffers *learn = nullptr;               // context-owned (weights, recording)
 };
 
 hk_status build_prepare(BuildState &S, const BuildParams &p, uint32_t nt, int sm_count);

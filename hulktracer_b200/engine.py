@@ -202,6 +202,57 @@ class Context:
         return st.as_dict() if st is not None else None
 
 
+    # -- learned split proposer --
+    def mlp_init(self, seed=0):
+        self._check(self.L.hk_mlp_init(self.h, seed))
+
+    def mlp_save(self, path):
+        self._check(self.L.hk_mlp_save(self.h, path.encode()))
+
+    def mlp_load(self, path):
+        self._check(self.L.hk_mlp_load(self.h, path.encode()))
+
+    def mlp_params(self):
+        p = np.zeros(_lib.MLP_PARAMS, np.float32)
+        self._check(self.L.hk_mlp_get_params(self.h, ptr(p), p.size))
+        return p
+
+    def mlp_set_params(self, p):
+        p = _f32(p)
+        self._check(self.L.hk_mlp_set_params(self.h, ptr(p), p.size))
+
+    def mlp_forward(self, X):
+        X = _f32(X).reshape(-1, _lib.MLP_IN)
+        out = np.zeros((X.shape[0], _lib.MLP_OUT), np.float32)
+        self._check(self.L.hk_mlp_forward(self.h, ptr(X), X.shape[0], ptr(out)))
+        return out
+
+    def mlp_grad(self, X, y):
+        X = _f32(X).reshape(-1, _lib.MLP_IN)
+        y = np.ascontiguousarray(y, np.int32)
+        g = np.zeros(_lib.MLP_PARAMS, np.float32)
+        loss = np.zeros(1, np.float32)
+        self._check(self.L.hk_mlp_grad(self.h, ptr(X), ptr(y), X.shape[0], ptr(g), ptr(loss)))
+        return g, float(loss[0])
+
+    def mlp_record(self, capacity_rows):
+        self._check(self.L.hk_mlp_record(self.h, int(capacity_rows)))
+
+    def mlp_dataset(self, fetch=True):
+        rows = C.c_uint32()
+        self._check(self.L.hk_mlp_dataset(self.h, None, None, 0, C.byref(rows)))
+        if not fetch:
+            return rows.value
+        X = np.zeros((rows.value, _lib.MLP_IN), np.float32)
+        y = np.zeros(rows.value, np.int32)
+        self._check(self.L.hk_mlp_dataset(self.h, ptr(X), ptr(y), rows.value, C.byref(rows)))
+        return X, y
+
+    def mlp_train(self, epochs=1, batch=1024, lr=1e-3, seed=0):
+        losses = np.zeros(epochs, np.float32)
+        self._check(self.L.hk_mlp_train(self.h, epochs, batch, lr, seed, ptr(losses)))
+        return losses
+
     def autotune(self, d_rays: int, n: int, cache_path: str | None = None):
         r = _lib.TuneResult()
         self._check(self.L.hk_autotune(self.h, C.c_void_p(d_rays), n,

@@ -31,10 +31,13 @@ def main():
     ap.add_argument("--variant", default="shortstack")
     ap.add_argument("--mode", default="binned", choices=["binned", "learned"])
     ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--weights", default=os.path.join(ROOT, "hulktracer_b200", "weights", "proposer.bin"))
     a = ap.parse_args()
     sc = scenes.animated_parts()
     W, H = sc.width, sc.height
     ctx = hk.Context()
+    if a.mode == "learned":
+        ctx.mlp_load(a.weights)
     ctx.upload(sc.verts, sc.tris)
     ctx.set_parts(sc.part_of_vertex, sc.part_center.shape[0])
     ctx.transform(scenes.part_matrices(sc, 1))

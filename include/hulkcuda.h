@@ -95,10 +95,10 @@ typedef struct hk_config {
     uint32_t block_size;      /* trace kernel block size (multiple of 32, <= 1024) */
     uint32_t blocks_per_sm;   /* persistent trace grid = SMs * blocks_per_sm */
     uint32_t max_refs;        /* builder reference arena capacity (0 = 16 x tris) */
-    uint32_t topk;            /* learned builder: proposals costed per node */
-    float fallback_ratio;     /* learned builder: fall back to full binned SAH when a
-                                 proposal costs more than ratio x the best exactly
-                                 costed candidate (1.02) */
+    uint32_t topk;            /* learned builder: proposals costed per node (1..8, 4) */
+    float fallback_ratio;     /* learned builder: fall back to the full binned SAH
+                                 when the best proposal costs more than ratio x the
+                                 exactly costed reference plane (1.02; 0 = always) */
 } hk_config;
 
 typedef struct hk_tree_stats {
@@ -221,6 +221,39 @@ hk_status hk_frame(hk_ctx *ctx, const float *mats12, const float *cam16, const f
 hk_status hk_get_ray_counts(hk_ctx *ctx, uint64_t *primary, uint64_t *shadow);
 /* Kernel nodes and all nodes of the captured frame graph (0 before capture). */
 hk_status hk_frame_graph_info(hk_ctx *ctx, uint32_t *kernel_nodes, uint32_t *all_nodes);
+
+/* ---- learned split proposer (no reference counterpart) ----
+ * A 200 -> 256 -> 256 -> 256 -> 96 MLP (ReLU). Features of a node (sampled
+ * from at most 64 of its references): per axis a 32-bin histogram of clipped
+ * centroids and 16-bin histograms of clipped lower / upper bounds (fractions),
+ * extents over the largest extent, depth / max_depth, 4 zeros. Output: one
+ * logit per (axis, plane index 0..31). In HK_BUILD_LEARNED, nodes with more
+ * than 256 references are handed to the proposer: the top-k valid planes
+ * (hk_config.topk) and the middle plane of the longest axis are costed
+ * exactly; the cheapest proposal is taken unless it costs more than
+ * hk_config.fallback_ratio x the middle plane, in which case that node gets
+ * the full binned SAH. Inference runs on the tensor cores in BF16 with FP32
+ * accumulation; training uses FP32 master weights and Adam. */
+hk_status hk_mlp_init(hk_ctx *ctx, uint64_t seed);
+hk_status hk_mlp_save(hk_ctx *ctx, const char *path);
+hk_status hk_mlp_load(hk_ctx *ctx, const char *path);
+/* flat FP32 parameters: W1 (200x256) b1 W2 (256x256) b2 W3 b3 W4 (256x96) b4,
+ * W stored in x out row-major; n = 207712 */
+hk_status hk_mlp_get_params(hk_ctx *ctx, float *params, uint32_t n);
+hk_status hk_mlp_set_params(hk_ctx *ctx, const float *params, uint32_t n);
+/* tensor-core inference: logits[n][96] of X[n][200] (host arrays) */
+hk_status hk_mlp_forward(hk_ctx *ctx, const float *X, uint32_t n, float *logits);
+/* FP32 training kernels: mean softmax cross-entropy of labels y and its
+ * gradient with respect to every parameter (flat layout above) */
+hk_status hk_mlp_grad(hk_ctx *ctx, const float *X, const int32_t *y, uint32_t n, float *grads, float *loss);
+/* record (features, label) rows during HK_BUILD_BINNED builds: label = axis *
+ * 32 + plane index chosen by the exact binned SAH; capacity 0 stops recording.
+ * Restarting recording empties the dataset. */
+hk_status hk_mlp_record(hk_ctx *ctx, uint32_t capacity_rows);
+hk_status hk_mlp_dataset(hk_ctx *ctx, float *X, int32_t *y, uint32_t cap_rows, uint32_t *rows);
+/* train on the recorded rows (shuffled per epoch from seed); epoch_loss
+ * (optional, host, epochs) receives the mean loss of every epoch */
+hk_status hk_mlp_train(hk_ctx *ctx, uint32_t epochs, uint32_t batch, float lr, uint64_t seed, float *epoch_loss);
 
 /* ---- autotuner (no reference counterpart) ----
  * Times the persistent traversal on n device rays of the current scene for

@@ -1,0 +1,227 @@
+"""The learned split proposer on the GPU: the network's tensor-core inference
+and FP32 training kernels against the CPU oracle (oracle/mlp.py), the
+recorded training rows against the oracle's features of the same (identical)
+binned tree, and learned builds (validity, the fallback's exactness, the
+trained network's cost and what it gains over an untrained one)."""
+import os
+
+import numpy as np
+import pytest
+
+from hulktracer_b200 import scenes
+from oracle import mlp
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+WEIGHTS = os.path.join(os.path.dirname(os.path.dirname(__file__)), "hulktracer_b200", "weights", "proposer.bin")
+KSMALL = 256            # nodes with more references than this go to the proposer
+CT, CI = 1.0, 1.5
+
+
+def load(name):
+    return dict(np.load(os.path.join(GOLDEN, name)))
+
+
+@pytest.fixture(scope="module")
+def ctx(hk):
+    return hk.Context()
+
+
+def features_like(n, seed):
+    rng = np.random.default_rng(seed)
+    X = rng.random((n, mlp.IN), dtype=np.float32)
+    X[:, :192] /= 8.0
+    return X
+
+
+def test_forward_bf16_matches_oracle(ctx):
+    ctx.mlp_init(7)
+    p = ctx.mlp_params()
+    X = features_like(300, 1)                      # 3 CTAs, the last one partial
+    Z = ctx.mlp_forward(X)
+    Zb = mlp.forward_bf16(p, X)
+    Zf, _ = mlp.forward_fp32(p, X)
+    scale = float(np.abs(Zb).max())
+    err = np.abs(Z - Zb)
+    assert err.max() <= 1e-2 * scale and err.mean() <= 1e-3 * scale
+    # BF16 against the FP32 network: close, and the same top plane on most rows
+    assert np.abs(Z - Zf).max() <= 5e-2 * scale
+    assert (Z.argmax(1) == Zf.argmax(1)).mean() >= 0.9
+
+
+def test_grad_matches_oracle(ctx):
+    ctx.mlp_init(11)
+    p = ctx.mlp_params()
+    X = features_like(200, 2)
+    y = np.random.default_rng(3).integers(0, mlp.OUT, 200).astype(np.int32)
+    g, loss = ctx.mlp_grad(X, y)
+    og, oloss = mlp.grad_fp32(p, X, y)
+    assert abs(loss - oloss) <= 1e-5 * max(1.0, abs(oloss))
+    o = 0
+    for name, shp in mlp.SHAPES:
+        n = int(np.prod(shp))
+        a, b = g[o:o + n], og[o:o + n]
+        assert np.linalg.norm(a - b) <= 1e-4 * np.linalg.norm(b) + 1e-12, name
+        o += n
+
+
+def test_params_save_load_roundtrip(ctx, hk, tmp_path):
+    ctx.mlp_init(5)
+    p = ctx.mlp_params()
+    f = str(tmp_path / "w.bin")
+    ctx.mlp_save(f)
+    other = hk.Context()
+    other.mlp_load(f)
+    assert np.array_equal(other.mlp_params(), p)
+    X = features_like(64, 4)
+    assert np.array_equal(other.mlp_forward(X), ctx.mlp_forward(X))
+    with open(f, "r+b") as fh:
+        fh.write(b"XXXX")
+    with pytest.raises(hk.HkError):
+        other.mlp_load(f)
+
+
+def oracle_rows(oracle, verts, tris, box, max_depth=24):
+    """(features, axis) of every node of the oracle's binned tree that has
+    more than KSMALL references and is split, from its references in
+    ascending triangle order (the builder's stable partition keeps that
+    order), sampled as the builder samples them."""
+    cn, cr = oracle.build_binned(verts, tris, box, ct=CT, ci=CI, max_depth=max_depth, leaf_size=4)
+    v = verts[:, :3]
+    t = tris[:, :3]
+    tlo = np.minimum(np.minimum(v[t[:, 0]], v[t[:, 1]]), v[t[:, 2]]).astype(np.float32)
+    thi = np.maximum(np.maximum(v[t[:, 0]], v[t[:, 1]]), v[t[:, 2]]).astype(np.float32)
+    rows = []
+
+    def walk(i, lo, hi, level):
+        w0, w1 = int(cn[i, 0]), int(cn[i, 1])
+        if (w0 & 3) == 3:
+            return np.unique(cr[w0 >> 2:(w0 >> 2) + w1])
+        axis, pair = w0 & 3, w0 >> 2
+        plane = np.uint32(w1).view(np.float32)
+        lhi, rlo = hi.copy(), lo.copy()
+        lhi[axis] = plane
+        rlo[axis] = plane
+        refs = np.union1d(walk(pair, lo, lhi, level + 1), walk(pair + 1, rlo, hi, level + 1))
+        cnt = refs.shape[0]
+        if cnt > KSMALL:
+            S = min(cnt, 64)
+            pick = refs[(np.arange(S, dtype=np.int64) * cnt) // S]
+            rows.append((mlp.features(lo, hi, tlo[pick], thi[pick], level, max_depth), axis))
+        return refs
+
+    walk(0, np.asarray(box[:4], np.float32).copy(), np.asarray(box[4:], np.float32).copy(), 0)
+    return rows
+
+
+def test_recorded_rows_match_oracle(ctx, oracle):
+    g = load("small24k.npz")
+    ctx.upload(g["verts"], g["tris"])
+    ctx.set_box(g["box"])
+    ctx.precompute()
+    ctx.mlp_record(100000)
+    try:
+        ctx.build()
+        X, y = ctx.mlp_dataset()
+    finally:
+        ctx.mlp_record(0)
+    rows = oracle_rows(oracle, g["verts"], g["tris"], g["box"])
+    assert X.shape[0] == len(rows) > 0
+    assert np.all((y >= 0) & (y < 96))
+    got = sorted((X[i].tobytes(), int(y[i]) // 32) for i in range(X.shape[0]))
+    want = sorted((f.tobytes(), a) for f, a in rows)
+    assert got == want
+
+
+def trace_equals_brute(ctx, hk, rays):
+    b = ctx.trace(rays, hk.BRUTE)
+    for v in (hk.SHORTSTACK, hk.ROPES):
+        h = ctx.trace(rays, v)
+        m = b["tri"] >= 0
+        assert np.array_equal(h["tri"] >= 0, m)
+        assert np.array_equal(h["t"][m], b["t"][m])
+
+
+def test_learned_build_valid_with_untrained_network(ctx, hk):
+    g = load("small24k.npz")
+    ctx.upload(g["verts"], g["tris"])
+    ctx.set_box(g["box"])
+    ctx.precompute()
+    ctx.mlp_init(3)
+    st = ctx.build(hk.BUILD_LEARNED)
+    assert st["learned_nodes"] + st["fallback_nodes"] > 0
+    trace_equals_brute(ctx, hk, g["rays"])
+
+
+def test_learned_fallback_zero_equals_binned(hk):
+    """fallback_ratio 0: every proposer node takes the full binned SAH, so
+    the learned build must equal the binned build bit for bit."""
+    c = hk.Context(fallback_ratio=0.0)
+    sc = scenes.animated_parts(n_parts=6, width=96, height=64)
+    c.upload(sc.verts, sc.tris)
+    c.set_box(sc.scene_box())
+    c.precompute()
+    c.mlp_init(1)
+    c.build(hk.BUILD_BINNED)
+    bn, br = c.export_compact()
+    st = c.build(hk.BUILD_LEARNED)
+    ln, lr = c.export_compact()
+    assert st["learned_nodes"] == 0 and st["fallback_nodes"] > 0
+    assert np.array_equal(bn, ln) and np.array_equal(br, lr)
+
+
+def test_train_reduces_loss(hk):
+    c = hk.Context()
+    c.mlp_init(0)
+    c.mlp_record(200000)
+    for seed in range(4):
+        sc = scenes.animated_parts(seed=100 + seed, n_parts=12, width=64, height=64)
+        c.upload(sc.verts, sc.tris)
+        c.set_parts(sc.part_of_vertex, sc.part_center.shape[0])
+        for f in range(3):
+            c.transform(scenes.part_matrices(sc, 5 * f))
+            c.build()
+    rows = c.mlp_dataset(fetch=False)
+    c.mlp_record(0)
+    assert rows > 256
+    losses = c.mlp_train(epochs=8, batch=128, lr=1e-3, seed=1)
+    assert np.all(np.isfinite(losses))
+    assert losses[-1] < 0.8 * losses[0]
+
+
+@pytest.mark.skipif(not os.path.exists(WEIGHTS), reason="no trained proposer weights")
+def test_trained_proposer_cost_and_gain(hk, oracle):
+    """On held-out frames of the animated 200k scene: the trained proposer's
+    tree costs within 2% of the exact binned tree (the fallback judges every
+    proposal), and it beats the untrained network on both the cost and the
+    share of proposer nodes that needed the fallback."""
+    sc = scenes.animated_parts()
+    res = {}
+    for name in ("trained", "untrained"):
+        c = hk.Context()
+        if name == "trained":
+            c.mlp_load(WEIGHTS)
+        else:
+            c.mlp_init(12345)
+        c.upload(sc.verts, sc.tris)
+        c.set_parts(sc.part_of_vertex, sc.part_center.shape[0])
+        costs, fb, n = [], 0, 0
+        for frame in (0, 17, 42):
+            c.transform(scenes.part_matrices(sc, frame))
+            box = c.get_box()
+            c.build(hk.BUILD_BINNED)
+            bn, _ = c.export_compact()
+            st = c.build(hk.BUILD_LEARNED)
+            ln, _ = c.export_compact()
+            cb = oracle.tree_cost(oracle.compact_to_ref(bn), box, CT, CI)
+            cl = oracle.tree_cost(oracle.compact_to_ref(ln), box, CT, CI)
+            costs.append(cl / cb)
+            fb += st["fallback_nodes"]
+            n += st["fallback_nodes"] + st["learned_nodes"]
+        res[name] = (max(costs), fb / max(n, 1))
+        c.close()
+    print("proposer ablation (max cost ratio, fallback share):", res)
+    assert res["trained"][0] <= 1.02
+    assert res["trained"][1] < res["untrained"][1]
+    assert res["trained"][0] <= res["untrained"][0]
