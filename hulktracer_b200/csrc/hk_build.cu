@@ -1,22 +1,31 @@
 // hk_build.cu -- GPU KD-tree builder: exact binned SAH (sm_100a).
 //
-// Breadth-first and level-synchronous. Per level:
-//   prep/scan     which nodes are "large" and how many histogram chunks each has
-//   hist_large    one CTA per chunk of a large node: shared-memory histograms
-//                 (3 axes x {lo bin, hi bin, flat-on-plane}) of the clipped
-//                 reference bounds, flushed to global memory with atomics
-//   sah_large     one warp per large node: warp scans over the 32 bins, exact
-//                 SAH at the 31 planes of each axis, warp argmin
-//   small         one warp per small node: histogram in warp-private shared
-//                 memory, then the same SAH evaluation
-//   plan/scan     leaf refs, child pairs, next-level nodes, child refs
-//   guard         capacity check (the whole level stops splitting on overflow)
-//   emit          compact node entries and next-level node records
-//   scan/scatter  stable partition of the references (global exclusive scan of
-//                 below/above flags), leaf references to the output list
-//   advance       level counters
+// Breadth-first and level-synchronous; three launches per level (five with
+// the learned proposer):
+//   work      large nodes (> 256 references): one CTA per chunk of 2048
+//             references builds shared-memory histograms (3 axes x {lo bin,
+//             hi bin, flat-on-plane}) of the clipped reference bounds and
+//             flushes them with atomics; the CTA that finishes a node's last
+//             chunk runs the SAH (one warp: scans over the 32 bins, exact cost
+//             at the 31 planes per axis, argmin). Small nodes: one warp per
+//             node, warp-private histogram, same SAH. Every decision is also
+//             tallied into the level totals (leaf refs, splits, next-level
+//             nodes, child refs) that the capacity guard needs.
+//   [infer, propose]  learned mode: tensor-core MLP on the large nodes'
+//             features, exact costing of the top-k proposals (chunked)
+//   plan      single-pass scan over nodes (decoupled look-back): leaf
+//             reference offsets, child pairs, next-level slots, child
+//             reference offsets; emits compact node entries, cells and ropes,
+//             next-level node records and the next level's large-node
+//             chunks. The guard (the whole level stops splitting on overflow)
+//             is decided from the tallies before anything is emitted.
+//   refs      single-pass scan of the below/above flags of every reference,
+//             fused with the stable partition into the next level and the
+//             leaf reference list.
 // Every kernel reads its work size from device memory, so the whole build is
-// a fixed launch sequence (graph-capturable, no host round trips).
+// a fixed launch sequence (graph-capturable, no host round trips). Look-back
+// waits are bounded: a wait that runs out sets an error bit and the build
+// reports failure instead of hanging.
 //
 // The algorithm is restated serially in the CPU oracle (hko_build_binned); the
 // two produce identical trees. The plane / bin / cost arithmetic below is
@@ -32,26 +41,47 @@ namespace hk {
 
 constexpr uint32_t kBins = 32;
 constexpr uint32_t kSmall = 256;     // nodes with <= kSmall refs: one warp per node
-constexpr uint32_t kChunk = 2048;    // refs per histogram CTA of a large node
+constexpr uint32_t kChunk = 1024;    // refs per histogram CTA of a large node (4 per thread)
 constexpr uint32_t kHist = 3 * 3 * kBins;
 constexpr int kScanThreads = 256;
 constexpr int kScanItems = 4;
 constexpr uint32_t kTile = kScanThreads * kScanItems;
 
 // ---------------------------------------------------------------------------
-// small vector types for the scans
+// scan value types: uint2 (reference below/above flags) and U5 (node plan:
+// leaf refs, splits, next-level nodes, child refs, below child refs)
 // ---------------------------------------------------------------------------
+struct U5 {
+    uint32_t x, y, z, w, v;
+};
 __device__ __forceinline__ uint2 vadd(uint2 a, uint2 b) { return make_uint2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ uint4 vadd(uint4 a, uint4 b) { return make_uint4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w); }
+__device__ __forceinline__ U5 vadd(U5 a, U5 b) { return U5{a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w, a.v + b.v}; }
+__device__ __forceinline__ uint2 vsub(uint2 a, uint2 b) { return make_uint2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ U5 vsub(U5 a, U5 b) { return U5{a.x - b.x, a.y - b.y, a.z - b.z, a.w - b.w, a.v - b.v}; }
 template <class T> __device__ __forceinline__ T vzero();
 template <> __device__ __forceinline__ uint2 vzero<uint2>() { return make_uint2(0, 0); }
-template <> __device__ __forceinline__ uint4 vzero<uint4>() { return make_uint4(0, 0, 0, 0); }
+template <> __device__ __forceinline__ U5 vzero<U5>() { return U5{0, 0, 0, 0, 0}; }
 __device__ __forceinline__ uint2 shfl_up(uint2 v, int d) {
     return make_uint2(__shfl_up_sync(0xffffffffu, v.x, d), __shfl_up_sync(0xffffffffu, v.y, d));
 }
-__device__ __forceinline__ uint4 shfl_up(uint4 v, int d) {
-    return make_uint4(__shfl_up_sync(0xffffffffu, v.x, d), __shfl_up_sync(0xffffffffu, v.y, d),
-                      __shfl_up_sync(0xffffffffu, v.z, d), __shfl_up_sync(0xffffffffu, v.w, d));
+__device__ __forceinline__ U5 shfl_up(U5 v, int d) {
+    return U5{__shfl_up_sync(0xffffffffu, v.x, d), __shfl_up_sync(0xffffffffu, v.y, d),
+              __shfl_up_sync(0xffffffffu, v.z, d), __shfl_up_sync(0xffffffffu, v.w, d),
+              __shfl_up_sync(0xffffffffu, v.v, d)};
+}
+__device__ __forceinline__ uint2 shfl_xor(uint2 v, int d) {
+    return make_uint2(__shfl_xor_sync(0xffffffffu, v.x, d), __shfl_xor_sync(0xffffffffu, v.y, d));
+}
+__device__ __forceinline__ U5 shfl_xor(U5 v, int d) {
+    return U5{__shfl_xor_sync(0xffffffffu, v.x, d), __shfl_xor_sync(0xffffffffu, v.y, d),
+              __shfl_xor_sync(0xffffffffu, v.z, d), __shfl_xor_sync(0xffffffffu, v.w, d),
+              __shfl_xor_sync(0xffffffffu, v.v, d)};
+}
+// loads past L1 (values other CTAs of the same kernel published)
+__device__ __forceinline__ uint2 ldcg(const uint2 *p) { return __ldcg(p); }
+__device__ __forceinline__ U5 ldcg(const U5 *p) {
+    const uint32_t *q = reinterpret_cast<const uint32_t *>(p);
+    return U5{__ldcg(q), __ldcg(q + 1), __ldcg(q + 2), __ldcg(q + 3), __ldcg(q + 4)};
 }
 
 // inclusive warp scan
@@ -64,9 +94,6 @@ __device__ __forceinline__ T warp_incl(T v) {
     }
     return v;
 }
-
-__device__ __forceinline__ uint2 vsub(uint2 a, uint2 b) { return make_uint2(a.x - b.x, a.y - b.y); }
-__device__ __forceinline__ uint4 vsub(uint4 a, uint4 b) { return make_uint4(a.x - b.x, a.y - b.y, a.z - b.z, a.w - b.w); }
 
 // exclusive block scan of one value per thread (kScanThreads threads); returns
 // the thread's exclusive prefix and the block total
@@ -89,77 +116,116 @@ __device__ __forceinline__ T block_excl(T v, T *sh_warp, T &total) {
     return vadd(wbase, vsub(inc, v));
 }
 
-// scan phase 1: per-tile sums
-template <class T, class Load>
-__global__ void __launch_bounds__(kScanThreads) k_scan_reduce(Load ld, T *partials) {
-    __shared__ T sh[kScanThreads / 32 + 1];
-    const uint32_t n = ld.count();
-    const uint32_t ntiles = (n + kTile - 1) / kTile;
-    for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        T s = vzero<T>();
-        uint32_t base = tile * kTile + threadIdx.x * kScanItems;
-        for (int k = 0; k < kScanItems; k++)
-            if (base + k < n) s = vadd(s, ld(base + k));
-        T tot;
-        block_excl(s, sh, tot);
-        if (threadIdx.x == 0) partials[tile] = tot;
+// ---------------------------------------------------------------------------
+// single-pass scan with decoupled look-back. Tiles are taken in order from an
+// atomic ticket, so every tile a CTA waits for belongs to a CTA that is
+// already running and publishes its aggregate without waiting. A tile's flag
+// is (tag << 2) | status, status 1 = aggregate, 2 = inclusive prefix; the tag
+// (build epoch x 64 + level) makes flags of earlier levels and builds stale,
+// so the flag arrays are never cleared. Waits are bounded (kSpinLimit polls):
+// one that runs out sets error bit 4 and counts the tile as zero.
+// ---------------------------------------------------------------------------
+constexpr uint32_t kSpinLimit = 1u << 22;
+
+template <class T>
+__device__ T lookback(const uint32_t *flags, const T *aggs, const T *incls, uint32_t tile, uint32_t tag,
+                      uint32_t *err) {
+    const int lane = threadIdx.x & 31;
+    T excl = vzero<T>();
+    int32_t p = (int32_t)tile - 1;
+    for (;;) {
+        const int32_t q = p - lane;
+        uint32_t st = 2;    // before tile 0: an inclusive prefix of zero
+        bool have = false;
+        if (q >= 0) {
+            have = true;
+            for (uint32_t spins = 0;; spins++) {
+                const uint32_t f = __ldcv(flags + q);
+                if ((f >> 2) == tag && (f & 3u)) {
+                    st = f & 3u;
+                    break;
+                }
+                if (spins >= kSpinLimit) {
+                    atomicOr(err, 4u);
+                    have = false;
+                    st = 2;
+                    break;
+                }
+                __nanosleep(32);
+            }
+        }
+        __threadfence();
+        const uint32_t m2 = __ballot_sync(0xffffffffu, st == 2);
+        const int stop = m2 ? __ffs(m2) - 1 : 32;
+        T v = vzero<T>();
+        if (have && lane <= stop) v = lane == stop ? ldcg(incls + q) : ldcg(aggs + q);
+        for (int o = 16; o; o >>= 1) v = vadd(v, shfl_xor(v, o));
+        excl = vadd(excl, v);
+        if (m2) break;
+        p -= 32;
     }
+    return excl;
 }
 
-// scan phase 2: one CTA scans the tile sums (exclusive) and writes the total
-template <class T, class Load>
-__global__ void __launch_bounds__(kScanThreads) k_scan_partials(Load ld, T *partials, T *total) {
+// Op: T (scan value), Item (what load caches for apply), Ctx (per-CTA
+// constants), kItems (consecutive elements per thread); count(), tag(),
+// err(), ctx() (all threads; block 0 may also publish level state), load(i)
+// -> Item, value(Item) -> T, apply(i, exclusive prefix, Item, Ctx) -- apply
+// sees every element once, with its global prefix
+template <class Op>
+__global__ void __launch_bounds__(kScanThreads) k_onepass(Op op, uint32_t *flags, typename Op::T *aggs,
+                                                          typename Op::T *incls, uint32_t *ticket) {
+    using T = typename Op::T;
+    constexpr int kItems = Op::kItems;
+    constexpr uint32_t kTileN = kScanThreads * kItems;
     __shared__ T sh[kScanThreads / 32 + 1];
-    const uint32_t n = ld.count();
-    const uint32_t ntiles = (n + kTile - 1) / kTile;
-    T carry = vzero<T>();
-    for (uint32_t b = 0; b < ntiles; b += kScanThreads) {
-        uint32_t i = b + threadIdx.x;
-        T v = i < ntiles ? partials[i] : vzero<T>();
+    __shared__ T s_excl;
+    __shared__ uint32_t s_tile;
+    const uint32_t n = op.count();
+    const uint32_t ntiles = (n + kTileN - 1) / kTileN;
+    const uint32_t tag = op.tag();
+    const typename Op::Ctx cx = op.ctx();
+    for (;;) {
+        if (threadIdx.x == 0) s_tile = atomicAdd(ticket, 1u);
+        __syncthreads();
+        const uint32_t tile = s_tile;
+        if (tile >= ntiles) break;
+        const uint32_t base = tile * kTileN + threadIdx.x * kItems;
+        typename Op::Item it[kItems];
+        T s = vzero<T>();
+#pragma unroll
+        for (int k = 0; k < kItems; k++) {
+            it[k] = op.load(base + k < n ? base + k : 0xffffffffu, cx);
+            s = vadd(s, op.value(it[k]));
+        }
         T tot;
-        T ex = block_excl(v, sh, tot);
-        if (i < ntiles) partials[i] = vadd(carry, ex);
-        carry = vadd(carry, tot);
+        const T ex = block_excl(s, sh, tot);
+        if (threadIdx.x == 0) {
+            if (tile == 0) incls[0] = tot;
+            else aggs[tile] = tot;
+            __threadfence();
+            *reinterpret_cast<volatile uint32_t *>(flags + tile) = (tag << 2) | (tile == 0 ? 2u : 1u);
+        }
+        if (threadIdx.x < 32) {
+            const T e = tile ? lookback(flags, aggs, incls, tile, tag, op.err()) : vzero<T>();
+            if (threadIdx.x == 0) {
+                if (tile) {
+                    incls[tile] = vadd(e, tot);
+                    __threadfence();
+                    *reinterpret_cast<volatile uint32_t *>(flags + tile) = (tag << 2) | 2u;
+                }
+                s_excl = e;
+            }
+        }
+        __syncthreads();
+        T pre = vadd(s_excl, ex);
+#pragma unroll
+        for (int k = 0; k < kItems; k++) {
+            if (base + k < n) op.apply(base + k, pre, it[k], cx);
+            pre = vadd(pre, op.value(it[k]));
+        }
         __syncthreads();
     }
-    if (threadIdx.x == 0) {
-        *total = carry;
-        ld.on_total(carry);
-    }
-}
-
-// scan phase 3: exclusive prefix of every element
-template <class T, class Load>
-__global__ void __launch_bounds__(kScanThreads) k_scan_apply(Load ld, const T *partials, T *out) {
-    __shared__ T sh[kScanThreads / 32 + 1];
-    const uint32_t n = ld.count();
-    const uint32_t ntiles = (n + kTile - 1) / kTile;
-    for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        uint32_t base = tile * kTile + threadIdx.x * kScanItems;
-        T v[kScanItems];
-        T s = vzero<T>();
-        for (int k = 0; k < kScanItems; k++) {
-            v[k] = (base + k < n) ? ld(base + k) : vzero<T>();
-            s = vadd(s, v[k]);
-        }
-        T tot;
-        T ex = vadd(partials[tile], block_excl(s, sh, tot));
-        for (int k = 0; k < kScanItems; k++) {
-            if (base + k < n) {
-                out[base + k] = ex;
-                ld.on_prefix(base + k, ex);
-            }
-            ex = vadd(ex, v[k]);
-        }
-    }
-}
-
-template <class T, class Load>
-static cudaError_t scan(const Load &ld, T *partials, T *out, T *total, int grid, cudaStream_t s) {
-    k_scan_reduce<T, Load><<<grid, kScanThreads, 0, s>>>(ld, partials);
-    k_scan_partials<T, Load><<<1, kScanThreads, 0, s>>>(ld, partials, total);
-    k_scan_apply<T, Load><<<grid, kScanThreads, 0, s>>>(ld, partials, out);
-    return cudaGetLastError();
 }
 
 // ---------------------------------------------------------------------------
@@ -199,14 +265,25 @@ __device__ __forceinline__ void bin_interval(float lo, float hi, float blo, floa
     on = (lo == hi) && b >= 1 && lo == plane_k(blo, ext, b);
 }
 
-// histogram contribution of one reference (shared-memory counters)
-__device__ __forceinline__ void hist_ref(uint32_t *H, float4 tlo, float4 thi, float4 blo, float4 bhi) {
+// bins per unit length of the node on each axis (32 / extent)
+__device__ __forceinline__ float4 bin_scale(float4 blo, float4 bhi) {
+    float4 r;
+    r.x = __fdiv_rn(32.0f, __fsub_rn(bhi.x, blo.x));
+    r.y = __fdiv_rn(32.0f, __fsub_rn(bhi.y, blo.y));
+    r.z = __fdiv_rn(32.0f, __fsub_rn(bhi.z, blo.z));
+    r.w = 0.0f;
+    return r;
+}
+
+// histogram contribution of one reference (shared-memory counters); inv3 =
+// bin_scale(blo, bhi)
+__device__ __forceinline__ void hist_ref(uint32_t *H, float4 tlo, float4 thi, float4 blo, float4 bhi, float4 inv3) {
 #pragma unroll
     for (uint32_t a = 0; a < 3; a++) {
         float l = c3(blo, a), h = c3(bhi, a);
         float ext = __fsub_rn(h, l);
         if (!(ext > 0.0f)) continue;
-        float inv = __fdiv_rn(32.0f, ext);
+        float inv = c3(inv3, a);
         float lo = mxf(c3(tlo, a), l), hi = mnf(c3(thi, a), h);
         int b, c;
         bool on;
@@ -297,7 +374,7 @@ struct LevelArgs {
     int32_t *axis;
     float *plane;
     uint2 *cnt;
-    uint4 *plan;
+    uint4 *plan;            // per node: leaf-ref offset, next slot, child-ref offset, below-ref offset
     uint2 *chunks;          // (large rank, chunk index within the node)
     uint32_t *large_slot;
     uint32_t *hist;
@@ -305,7 +382,6 @@ struct LevelArgs {
     const uint32_t *refs;
     const uint32_t *ref_node;
     uint32_t *nx_refs, *nx_ref_node;
-    const uint2 *rscan;
     uint2 *out_nodes;
     uint32_t *out_refs;
     uint32_t *out_ropes;
@@ -313,6 +389,7 @@ struct LevelArgs {
     BuildCounters *ctr;
     LevelCounters *lc, *nlc;
     uint32_t *err;
+    uint32_t *epoch;        // build counter (k_root increments it)
     uint32_t level;
     float ct, ci;
     uint32_t max_depth, leaf_size;
@@ -338,14 +415,22 @@ __global__ void k_tri_bounds(const float4 *__restrict__ V, const uint4 *__restri
     hi[i] = make_float4(mxf(mxf(a.x, b.x), c.x), mxf(mxf(a.y, b.y), c.y), mxf(mxf(a.z, b.z), c.z), 0.0f);
 }
 
-// root node + references of level 0 (the counters were zeroed by a memset)
+// root node + references of level 0 (the counters were zeroed by a memset);
+// a root with more than 256 references is the first large node
 __global__ void k_root(LevelArgs A, const float *box, uint32_t nt) {
+    const bool large = nt > kSmall && nt > A.leaf_size && A.max_depth > 0;
+    const uint32_t nch = large ? (nt + kChunk - 1) / kChunk : 0u;
     if (blockIdx.x == 0 && threadIdx.x == 0) {
+        *A.epoch += 1u;
         LevelCounters *l0 = &A.ctr->lvl[0];
         l0->nodes = 1;
         l0->refs = nt;
         l0->nodes_total = 2;
         l0->leafrefs_total = 0;
+        l0->n_large = large ? 1u : 0u;
+        l0->n_chunks = nch;
+        if (large) A.large_slot[0] = 0;
+        if (A.learned) A.lrank[0] = large ? 0u : 0xffffffffu;
         A.nx_lo[0] = make_float4(box[0], box[1], box[2], 0.0f);
         A.nx_hi[0] = make_float4(box[4], box[5], box[6], 0.0f);
         A.nx_info[0] = make_uint4(0, nt, 0, 0);
@@ -360,34 +445,42 @@ __global__ void k_root(LevelArgs A, const float *box, uint32_t nt) {
         const_cast<uint32_t *>(A.refs)[i] = i;
         const_cast<uint32_t *>(A.ref_node)[i] = 0;
     }
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < nch; k += gridDim.x * blockDim.x)
+        A.chunks[k] = make_uint2(0, k);
 }
 
 __device__ __forceinline__ bool decidable(const LevelArgs &A, uint32_t cnt) {
     return cnt > A.leaf_size && A.level < A.max_depth;
 }
 
-// large nodes take ranks and chunk ranges (atomics: the histogram sums do not
-// depend on their order)
-__global__ void k_prep(LevelArgs A) {
-    const uint32_t n = A.lc->nodes;
-    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
-        uint32_t cnt = A.n_info[s].y;
-        if (A.learned) A.lrank[s] = 0xffffffffu;
-        if (!(decidable(A, cnt) && cnt > kSmall)) continue;
-        uint32_t nch = (cnt + kChunk - 1) / kChunk;
-        uint32_t rank = atomicAdd(&A.lc->n_large, 1u);
-        uint32_t first = atomicAdd(&A.lc->n_chunks, nch);
-        if (rank >= A.cap_large || first + nch > A.cap_chunks) {
-            atomicOr(A.err, 2u);
-            continue;
+// level totals of the decisions (what the capacity guard needs), kept per
+// thread and flushed once per CTA
+struct Tally {
+    uint32_t leafrefs = 0, leafnodes = 0, splits = 0, next = 0, childrefs = 0;
+    __device__ void add(const Decision &d, uint32_t cnt) {
+        if (d.axis < 0) {
+            leafrefs += cnt;
+            leafnodes += cnt ? 1u : 0u;
+        } else {
+            splits += 1;
+            next += (d.nb > 0 ? 1u : 0u) + (d.na > 0 ? 1u : 0u);
+            childrefs += d.nb + d.na;
         }
-        A.large_slot[rank] = s;
-        if (A.learned) A.lrank[s] = rank;   // the proposer row of the node
-        for (uint32_t k = 0; k < nch; k++) A.chunks[first + k] = make_uint2(rank, k);
-        uint32_t *H = A.hist + (size_t)rank * kHist;
-        for (uint32_t k = 0; k < kHist; k++) H[k] = 0;
-        A.done[rank] = 0;
     }
+};
+
+// all threads of the CTA call it once, at the end of the kernel
+__device__ void tally_flush(const LevelArgs &A, const Tally &t, uint32_t *sh5) {
+    if (threadIdx.x < 5) sh5[threadIdx.x] = 0;
+    __syncthreads();
+    if (t.leafrefs) atomicAdd(&sh5[0], t.leafrefs);
+    if (t.leafnodes) atomicAdd(&sh5[1], t.leafnodes);
+    if (t.splits) atomicAdd(&sh5[2], t.splits);
+    if (t.next) atomicAdd(&sh5[3], t.next);
+    if (t.childrefs) atomicAdd(&sh5[4], t.childrefs);
+    __syncthreads();
+    // t_leafrefs .. t_childrefs are consecutive fields of LevelCounters
+    if (threadIdx.x < 5 && sh5[threadIdx.x]) atomicAdd(&A.lc->t_leafrefs + threadIdx.x, sh5[threadIdx.x]);
 }
 
 __device__ __forceinline__ void write_decision(const LevelArgs &A, uint32_t s, const Decision &d) {
@@ -468,10 +561,12 @@ __device__ void record_node(const LevelArgs &A, uint4 info, float4 blo, float4 b
 // Work items: first the chunks of large nodes (one CTA each; the CTA that
 // finishes a node's last chunk evaluates its SAH), then groups of 8 small
 // nodes (one warp each: warp-private histogram + SAH).
-__global__ void __launch_bounds__(256) k_work(LevelArgs A) {
+__global__ void __launch_bounds__(256, 5) k_work(LevelArgs A) {
     __shared__ uint32_t H[kHist];
     __shared__ uint32_t HS[8][kHist];
     __shared__ int s_last;
+    __shared__ uint32_t s_tally[5];
+    Tally tally;
     const uint32_t wib = threadIdx.x >> 5, lane = threadIdx.x & 31u;
     const uint32_t nch = min(A.lc->n_chunks, A.cap_chunks);
     const uint32_t nodes = A.lc->nodes;
@@ -489,9 +584,31 @@ __global__ void __launch_bounds__(256) k_work(LevelArgs A) {
             float4 blo = A.n_lo[s], bhi = A.n_hi[s];
             for (uint32_t i = threadIdx.x; i < kHist; i += blockDim.x) H[i] = 0;
             __syncthreads();
-            for (uint32_t r = r0 + threadIdx.x; r < r1; r += blockDim.x) {
-                uint32_t tri = A.refs[r];
-                hist_ref(H, A.tb_lo[tri], A.tb_hi[tri], blo, bhi);
+            {
+                // the thread's references loaded together, their bounds two
+                // at a time (few dependent load latencies, no spills)
+                constexpr int kPer = kChunk / 256;
+                const float4 inv3 = bin_scale(blo, bhi);
+                uint32_t tri[kPer];
+#pragma unroll
+                for (int k = 0; k < kPer; k++) {
+                    const uint32_t r = r0 + threadIdx.x + 256u * k;
+                    tri[k] = r < r1 ? A.refs[r] : 0xffffffffu;
+                }
+#pragma unroll
+                for (int k = 0; k < kPer; k += 2) {
+                    float4 lo0, hi0, lo1, hi1;
+                    if (tri[k] != 0xffffffffu) {
+                        lo0 = A.tb_lo[tri[k]];
+                        hi0 = A.tb_hi[tri[k]];
+                    }
+                    if (tri[k + 1] != 0xffffffffu) {
+                        lo1 = A.tb_lo[tri[k + 1]];
+                        hi1 = A.tb_hi[tri[k + 1]];
+                    }
+                    if (tri[k] != 0xffffffffu) hist_ref(H, lo0, hi0, blo, bhi, inv3);
+                    if (tri[k + 1] != 0xffffffffu) hist_ref(H, lo1, hi1, blo, bhi, inv3);
+                }
             }
             __syncthreads();
             uint32_t *G = A.hist + (size_t)rank * kHist;
@@ -507,7 +624,14 @@ __global__ void __launch_bounds__(256) k_work(LevelArgs A) {
             if (s_last && wib == 0) {
                 __threadfence();
                 Decision d = sah_warp(GHist{G}, blo, bhi, info.y, A.ct, A.ci);
-                if (lane == 0) write_decision(A, s, d);
+                if (lane == 0) {
+                    write_decision(A, s, d);
+                    tally.add(d, info.y);
+                }
+                // clean the histogram and the done counter for the next level
+                __syncwarp();
+                for (uint32_t i = lane; i < kHist; i += 32) G[i] = 0;
+                if (lane == 0) A.done[rank] = 0;
                 record_node(A, info, blo, bhi, d, reinterpret_cast<float *>(HS[0]));
             }
             __syncthreads();
@@ -528,23 +652,32 @@ __global__ void __launch_bounds__(256) k_work(LevelArgs A) {
                 continue;  // binned mode: handled by its chunks
             }
             if (!dec) {
-                if (lane == 0) write_decision(A, s, Decision{-1, 0.0f, 0, 0, kInf, 0});
+                if (lane == 0) {
+                    const Decision leaf{-1, 0.0f, 0, 0, kInf, 0};
+                    write_decision(A, s, leaf);
+                    tally.add(leaf, cnt);
+                }
                 continue;
             }
             uint32_t *Hw = HS[wib];
             for (uint32_t i = lane; i < kHist; i += 32) Hw[i] = 0;
             __syncwarp();
             float4 blo = A.n_lo[s], bhi = A.n_hi[s];
+            const float4 inv3 = bin_scale(blo, bhi);
             for (uint32_t r = info.x + lane; r < info.x + cnt; r += 32) {
                 uint32_t tri = A.refs[r];
-                hist_ref(Hw, A.tb_lo[tri], A.tb_hi[tri], blo, bhi);
+                hist_ref(Hw, A.tb_lo[tri], A.tb_hi[tri], blo, bhi, inv3);
             }
             __syncwarp();
             Decision d = sah_warp(Hw, blo, bhi, cnt, A.ct, A.ci);
-            if (lane == 0) write_decision(A, s, d);
+            if (lane == 0) {
+                write_decision(A, s, d);
+                tally.add(d, cnt);
+            }
             __syncwarp();
         }
     }
+    tally_flush(A, tally, s_tally);
 }
 
 // ---------------------------------------------------------------------------
@@ -636,6 +769,8 @@ __global__ void __launch_bounds__(256) k_propose(LevelArgs A) {
     __shared__ Candidates C;
     __shared__ uint32_t s_cnt[2 * kMaxCand];
     __shared__ int s_last, s_fallback;
+    __shared__ uint32_t s_tally[5];
+    Tally tally;
     const uint32_t nch = min(A.lc->n_chunks, A.cap_chunks);
     const uint32_t nodes = A.lc->nodes;
     for (uint32_t item = blockIdx.x; item < nch; item += gridDim.x) {
@@ -655,9 +790,24 @@ __global__ void __launch_bounds__(256) k_propose(LevelArgs A) {
         uint32_t nb[kMaxCand], na[kMaxCand];
 #pragma unroll
         for (int i = 0; i < kMaxCand; i++) nb[i] = na[i] = 0;
-        for (uint32_t r = r0 + threadIdx.x; r < r1; r += blockDim.x) {
-            const uint32_t tri = A.refs[r];
-            const float4 tlo = A.tb_lo[tri], thi = A.tb_hi[tri];
+        constexpr int kPer = kChunk / 256;
+        uint32_t tris[kPer];
+        float4 tlos[kPer], this_[kPer];
+#pragma unroll
+        for (int k = 0; k < kPer; k++) {
+            const uint32_t r = r0 + threadIdx.x + 256u * k;
+            tris[k] = r < r1 ? A.refs[r] : 0xffffffffu;
+        }
+#pragma unroll
+        for (int k = 0; k < kPer; k++)
+            if (tris[k] != 0xffffffffu) {
+                tlos[k] = A.tb_lo[tris[k]];
+                this_[k] = A.tb_hi[tris[k]];
+            }
+#pragma unroll
+        for (int k = 0; k < kPer; k++) {
+            if (tris[k] == 0xffffffffu) continue;
+            const float4 tlo = tlos[k], thi = this_[k];
 #pragma unroll
             for (int i = 0; i < kMaxCand; i++) {
                 if (i >= nc) break;
@@ -699,7 +849,9 @@ __global__ void __launch_bounds__(256) k_propose(LevelArgs A) {
             for (int i = 0; i < nc; i++) {
                 cb[i] = __ldcg(G + 2 * i);
                 ca[i] = __ldcg(G + 2 * i + 1);
+                G[2 * i] = G[2 * i + 1] = 0;   // clean for the next level
             }
+            A.done[rank] = 0;
             const float Anode = surf(blo, bhi);
             auto cost = [&](int i) {
                 float4 bb = bhi, ba = blo;
@@ -724,6 +876,7 @@ __global__ void __launch_bounds__(256) k_propose(LevelArgs A) {
                 Decision d{C.axis[bi], C.plane[bi], cb[bi], ca[bi], bc, C.bin[bi]};
                 if (!(bc < __fmul_rn(A.ci, (float)info.y))) d.axis = -1;
                 write_decision(A, s, d);
+                tally.add(d, info.y);
                 atomicAdd(&A.ctr->learned_nodes, 1u);
             } else {
                 atomicAdd(&A.ctr->fallback_nodes, 1u);
@@ -734,72 +887,139 @@ __global__ void __launch_bounds__(256) k_propose(LevelArgs A) {
             // the full binned SAH on this node
             for (uint32_t i = threadIdx.x; i < kHist; i += blockDim.x) H[i] = 0;
             __syncthreads();
+            const float4 inv3 = bin_scale(blo, bhi);
             for (uint32_t r = info.x + threadIdx.x; r < info.x + info.y; r += blockDim.x) {
                 uint32_t tri = A.refs[r];
-                hist_ref(H, A.tb_lo[tri], A.tb_hi[tri], blo, bhi);
+                hist_ref(H, A.tb_lo[tri], A.tb_hi[tri], blo, bhi, inv3);
             }
             __syncthreads();
             if (threadIdx.x < 32) {
                 Decision d = sah_warp(H, blo, bhi, info.y, A.ct, A.ci);
-                if (threadIdx.x == 0) write_decision(A, s, d);
+                if (threadIdx.x == 0) {
+                    write_decision(A, s, d);
+                    tally.add(d, info.y);
+                }
             }
         }
         __syncthreads();
     }
+    tally_flush(A, tally, s_tally);
 }
 
 // ---------------------------------------------------------------------------
-// plan scan: (leaf refs, child pairs, next-level nodes, child refs) per node.
-// on_total (one thread, after the tile sums) is the capacity guard and writes
-// the next level's counters; on_prefix emits node s's compact entry and its
-// children's next-level records.
-struct LoadPlan {
+// plan: single-pass scan over the level's nodes of (leaf refs, splits,
+// next-level nodes, child refs, below child refs); the guard is decided from
+// the decision tallies, block 0 writes the next level's counters, and every
+// node emits its compact entry, its children's cells / ropes / next-level
+// records and the next level's large-node chunks.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t level_tag(const LevelArgs &A) {
+    return (*A.epoch * 64u + A.level) & 0x3fffffffu;
+}
+
+// the capacity guard: true when splitting this level would overflow
+__device__ __forceinline__ bool level_over(const LevelArgs &A) {
+    const LevelCounters *l = A.lc;
+    const uint64_t child_refs = l->t_childrefs, leaf_refs = l->t_leafrefs, splits = l->t_splits;
+    return child_refs > A.cap_refs || (uint64_t)l->leafrefs_total + leaf_refs + child_refs > A.cap_refs ||
+           (uint64_t)l->nodes_total + 2 * splits > A.cap_nodes || l->t_next > A.cap_level;
+}
+
+// a child of count c in next-level slot ns: large nodes take a rank and
+// their chunks (few per level, so plain atomics)
+__device__ void child_setup(const LevelArgs &A, uint32_t ns, uint32_t c) {
+    const bool large = c > kSmall && c > A.leaf_size && A.level + 1 < A.max_depth;
+    if (A.learned) A.lrank[ns] = 0xffffffffu;
+    if (!large) return;
+    const uint32_t nch = (c + kChunk - 1) / kChunk;
+    const uint32_t rank = atomicAdd(&A.nlc->n_large, 1u);
+    const uint32_t first = atomicAdd(&A.nlc->n_chunks, nch);
+    if (rank >= A.cap_large || first + nch > A.cap_chunks) {
+        atomicOr(A.err, 2u);
+        return;
+    }
+    A.large_slot[rank] = ns;
+    if (A.learned) A.lrank[ns] = rank;
+    for (uint32_t k = 0; k < nch; k++) A.chunks[first + k] = make_uint2(rank, k);
+}
+
+struct PlanCtx {
+    uint32_t stop, nodes_total, leafrefs_total;
+};
+
+struct PlanItem {
+    uint4 info;     // start, count, compact index
+    uint2 cnt;      // below, above
+    int axis;
+};
+
+struct PlanOp {
+    using T = U5;
+    using Item = PlanItem;
+    using Ctx = PlanCtx;
+    static constexpr int kItems = 1;
     LevelArgs A;
     __device__ uint32_t count() const { return A.lc->nodes; }
-    __device__ uint4 operator()(uint32_t s) const {
-        if (A.axis[s] < 0) return make_uint4(A.n_info[s].y, 0, 0, 0);
-        uint2 c = A.cnt[s];
-        return make_uint4(0, 1, (c.x > 0) + (c.y > 0), c.x + c.y);
-    }
-    __device__ void on_total(uint4 t) const {
+    __device__ uint32_t tag() const { return level_tag(A); }
+    __device__ uint32_t *err() const { return A.err; }
+    __device__ Ctx ctx() const {
         LevelCounters *l = A.lc, *nx = A.nlc;
-        nx->n_large = 0;
-        nx->n_chunks = 0;
-        if (l->nodes == 0) {
-            nx->nodes = 0;
-            nx->refs = 0;
-            nx->nodes_total = l->nodes_total;
-            nx->leafrefs_total = l->leafrefs_total;
-            return;
+        const bool over = level_over(A);
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            l->stop = over ? 1u : 0u;
+            if (over) A.ctr->capacity_hit = 1;
+            nx->nodes = over ? 0u : l->t_next;
+            nx->refs = over ? 0u : l->t_childrefs;
+            nx->nodes_total = l->nodes_total + (over ? 0u : 2u * l->t_splits);
+            nx->leafrefs_total = l->leafrefs_total + (over ? l->refs : l->t_leafrefs);
+            A.ctr->leaves += over ? l->nodes : l->t_leafnodes;
+            if (!over && l->t_next) A.ctr->depth = A.level + 1;
         }
-        uint64_t child_refs = t.w, leaf_refs = t.x, splits = t.y;
-        bool over = child_refs > A.cap_refs || (uint64_t)l->leafrefs_total + leaf_refs + child_refs > A.cap_refs ||
-                    (uint64_t)l->nodes_total + 2 * splits > A.cap_nodes || t.z > A.cap_level;
-        l->stop = over ? 1u : 0u;
-        if (over) A.ctr->capacity_hit = 1;
-        nx->nodes = over ? 0u : t.z;
-        nx->refs = over ? 0u : t.w;
-        nx->nodes_total = l->nodes_total + (over ? 0u : 2u * t.y);
-        nx->leafrefs_total = l->leafrefs_total + (over ? l->refs : t.x);
-        if (!over && t.z) A.ctr->depth = A.level + 1;
+        return Ctx{over ? 1u : 0u, l->nodes_total, l->leafrefs_total};
     }
-    __device__ void on_prefix(uint32_t s, uint4 pl) const {
-        const LevelCounters *l = A.lc;
-        const bool stop = l->stop != 0;
-        uint4 info = A.n_info[s];
-        int ax = stop ? -1 : A.axis[s];
-        if (ax < 0) {
-            uint32_t off = l->leafrefs_total + (stop ? info.x : pl.x);
-            A.out_nodes[info.z] = make_uint2((off << 2) | kLeafTag, info.y);
-            if (info.y) atomicAdd(&A.ctr->leaves, 1u);
+    __device__ Item load(uint32_t s, const Ctx &) const {
+        if (s == 0xffffffffu) return Item{make_uint4(0, 0, 0, 0), make_uint2(0, 0), -1};
+        return Item{A.n_info[s], A.cnt[s], A.axis[s]};
+    }
+    __device__ T value(const Item &it) const {
+        if (it.axis < 0) return U5{it.info.y, 0, 0, 0, 0};
+        const uint2 c = it.cnt;
+        return U5{0, 1, (c.x > 0 ? 1u : 0u) + (c.y > 0 ? 1u : 0u), c.x + c.y, c.x};
+    }
+    __device__ void apply(uint32_t s, U5 pl, const Item &it, const Ctx &cx) const {
+        const uint4 info = it.info;
+        const int ax = cx.stop ? -1 : it.axis;
+        A.plan[s] = make_uint4(pl.x, pl.z, pl.w, pl.v);
+        if (info.z >= A.cap_nodes) {
+            atomicOr(A.err, 2u);
             return;
         }
-        uint32_t pair = l->nodes_total + 2 * pl.y;
-        float p = A.plane[s];
-        uint2 ct = A.cnt[s];
+        if (ax < 0) {
+            const uint32_t off = cx.leafrefs_total + (cx.stop ? info.x : pl.x);
+            A.out_nodes[info.z] = make_uint2((off << 2) | kLeafTag, info.y);
+            return;
+        }
+        const uint32_t pair = cx.nodes_total + 2 * pl.y;
+        const uint2 ct = it.cnt;
+        // the tallies that passed the guard and this scan sum the same
+        // decisions; these checks only keep an inconsistent level in bounds
+        if ((uint64_t)pair + 1 >= A.cap_nodes ||
+            (uint64_t)pl.z + (ct.x ? 1u : 0u) + (ct.y ? 1u : 0u) > A.cap_level) {
+            atomicOr(A.err, 2u);
+            return;
+        }
+        const float p = A.plane[s];
+        const float4 lo = A.n_lo[s], hi = A.n_hi[s];
+        uint32_t r[6];
+        {
+            // the parent's ropes: 6 words at a 24-byte stride (8-byte aligned)
+            const uint2 *pr2 = reinterpret_cast<const uint2 *>(A.out_ropes + 6 * (size_t)info.z);
+            const uint2 a0 = pr2[0], a1 = pr2[1], a2 = pr2[2];
+            r[0] = a0.x; r[1] = a0.y; r[2] = a1.x; r[3] = a1.y; r[4] = a2.x; r[5] = a2.y;
+        }
         A.out_nodes[info.z] = make_uint2((pair << 2) | (uint32_t)ax, __float_as_uint(p));
-        uint32_t ns = pl.z, co = pl.w;
-        float4 lo = A.n_lo[s], hi = A.n_hi[s];
+        uint32_t ns = pl.z;
+        const uint32_t co = pl.w;
         {
             // cells and ropes of both children: the parent's ropes, with the
             // face on the split plane pointing at the sibling
@@ -810,15 +1030,18 @@ struct LoadPlan {
             A.out_cbox[2 * (size_t)pair + 1] = bh;
             A.out_cbox[2 * (size_t)pair + 2] = al;
             A.out_cbox[2 * (size_t)pair + 3] = hi;
-            const uint32_t *pr = A.out_ropes + 6 * (size_t)info.z;
-            uint32_t *rb = A.out_ropes + 6 * (size_t)pair, *ra = rb + 6;
+            uint32_t rb[6], ra[6];
+#pragma unroll
             for (int f = 0; f < 6; f++) {
-                uint32_t r = pr[f];
-                rb[f] = r;
-                ra[f] = r;
+                rb[f] = f == 2 * ax + 1 ? pair + 1 : r[f];
+                ra[f] = f == 2 * ax ? pair : r[f];
             }
-            rb[2 * ax + 1] = pair + 1;
-            ra[2 * ax] = pair;
+            // the pair's 12 rope words start at 24 * pair bytes, pair even
+            // (nodes_total starts at 2 and grows by pairs): 16-byte aligned
+            uint4 *dst = reinterpret_cast<uint4 *>(A.out_ropes + 6 * (size_t)pair);
+            dst[0] = make_uint4(rb[0], rb[1], rb[2], rb[3]);
+            dst[1] = make_uint4(rb[4], rb[5], ra[0], ra[1]);
+            dst[2] = make_uint4(ra[2], ra[3], ra[4], ra[5]);
         }
         if (ct.x) {
             float4 h2 = hi;
@@ -826,6 +1049,7 @@ struct LoadPlan {
             A.nx_lo[ns] = lo;
             A.nx_hi[ns] = h2;
             A.nx_info[ns] = make_uint4(co, ct.x, pair, 0);
+            child_setup(A, ns, ct.x);
             ns++;
         } else {
             A.out_nodes[pair] = make_uint2(kLeafTag, 0);
@@ -836,73 +1060,79 @@ struct LoadPlan {
             A.nx_lo[ns] = l2;
             A.nx_hi[ns] = hi;
             A.nx_info[ns] = make_uint4(co + ct.x, ct.y, pair + 1, 0);
+            child_setup(A, ns, ct.y);
         } else {
             A.out_nodes[pair + 1] = make_uint2(kLeafTag, 0);
         }
     }
 };
 
-__device__ __forceinline__ uint2 ref_flags(const LevelArgs &A, uint32_t r, uint32_t s, int ax) {
-    uint32_t tri = A.refs[r];
-    float l = c3(A.n_lo[s], ax), h = c3(A.n_hi[s], ax), p = A.plane[s];
-    float lo = mxf(c3(A.tb_lo[tri], ax), l), hi = mnf(c3(A.tb_hi[tri], ax), h);
-    bool flat_on = (lo == hi) && lo == p;
-    return make_uint2((lo < p || flat_on) ? 1u : 0u, (hi > p || flat_on) ? 1u : 0u);
-}
-
-struct LoadRefFlags {
-    LevelArgs A;
-    __device__ uint32_t count() const { return A.lc->refs; }
-    __device__ uint2 operator()(uint32_t r) const {
-        if (A.lc->stop) return make_uint2(0, 0);
-        uint32_t s = A.ref_node[r];
-        int ax = A.axis[s];
-        if (ax < 0) return make_uint2(0, 0);
-        return ref_flags(A, r, s, ax);
-    }
-    __device__ void on_total(uint2) const {}
-    __device__ void on_prefix(uint32_t, uint2) const {}
+// refs: single-pass scan of the below / above flags fused with the stable
+// partition. The global prefix of a node's first reference is the sum of the
+// earlier split nodes' below (above) counts, which the plan scan provides, so
+// a reference's rank within its node's below list is prefix - that sum.
+struct RefItem {
+    uint2 f;        // below / above flags
+    uint32_t s;     // node slot
+    uint32_t tri;
 };
 
-__global__ void k_scatter(LevelArgs A) {
-    const LevelCounters *l = A.lc;
-    const uint32_t n = l->refs;
-    const bool stop = l->stop != 0;
-    for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
-        uint32_t s = A.ref_node[r];
-        uint4 info = A.n_info[s];
-        int ax = stop ? -1 : A.axis[s];
-        uint32_t tri = A.refs[r];
+struct RefOp {
+    using T = uint2;
+    using Item = RefItem;
+    using Ctx = uint32_t;   // the level stopped splitting
+    static constexpr int kItems = 4;
+    LevelArgs A;
+    __device__ uint32_t count() const { return A.lc->refs; }
+    __device__ uint32_t tag() const { return level_tag(A); }
+    __device__ uint32_t *err() const { return A.err; }
+    __device__ Ctx ctx() const { return A.lc->stop; }
+    __device__ Item load(uint32_t r, const Ctx &stop) const {
+        if (r == 0xffffffffu) return Item{make_uint2(0, 0), 0, 0};
+        const uint32_t s = A.ref_node[r];
+        const uint32_t tri = A.refs[r];
+        const int ax = stop ? -1 : A.axis[s];
+        if (ax < 0) return Item{make_uint2(0, 0), s, tri};
+        const float l = c3(A.n_lo[s], ax), h = c3(A.n_hi[s], ax), p = A.plane[s];
+        const float lo = mxf(c3(A.tb_lo[tri], ax), l), hi = mnf(c3(A.tb_hi[tri], ax), h);
+        const bool flat_on = (lo == hi) && lo == p;
+        return Item{make_uint2((lo < p || flat_on) ? 1u : 0u, (hi > p || flat_on) ? 1u : 0u), s, tri};
+    }
+    __device__ T value(const Item &it) const { return it.f; }
+    __device__ void apply(uint32_t r, uint2 P, const Item &it, const Ctx &stop) const {
+        const LevelCounters *l = A.lc;
+        const uint32_t s = it.s;
+        const uint4 info = A.n_info[s];
+        const int ax = stop ? -1 : A.axis[s];
         if (ax < 0) {
-            uint32_t off = l->leafrefs_total + (stop ? info.x : A.plan[s].x) + (r - info.x);
-            if (off < A.cap_refs) A.out_refs[off] = tri;
+            const uint32_t off = l->leafrefs_total + (stop ? info.x : A.plan[s].x) + (r - info.x);
+            if (off < A.cap_refs) A.out_refs[off] = it.tri;
             else atomicOr(A.err, 2u);
-            continue;
+            return;
         }
-        uint2 f = ref_flags(A, r, s, ax);
-        uint2 base = A.rscan[info.x], mine = A.rscan[r];
-        uint4 pl = A.plan[s];
-        uint2 ct = A.cnt[s];
-        if (f.x) {
-            uint32_t pos = pl.w + (mine.x - base.x);
-            if (pos < A.cap_refs && pos < pl.w + ct.x) {
-                A.nx_refs[pos] = tri;
-                A.nx_ref_node[pos] = pl.z;
+        const uint4 pl = A.plan[s];   // y: next slot, z: child-ref offset, w: below refs before s
+        const uint2 ct = A.cnt[s];
+        if (it.f.x) {
+            const uint32_t pos = pl.z + (P.x - pl.w);
+            if (pos < A.cap_refs && pos < pl.z + ct.x) {
+                A.nx_refs[pos] = it.tri;
+                A.nx_ref_node[pos] = pl.y;
             } else {
                 atomicOr(A.err, 2u);
             }
         }
-        if (f.y) {
-            uint32_t pos = pl.w + ct.x + (mine.y - base.y);
-            if (pos < A.cap_refs && pos < pl.w + ct.x + ct.y) {
-                A.nx_refs[pos] = tri;
-                A.nx_ref_node[pos] = pl.z + (ct.x ? 1u : 0u);
+        if (it.f.y) {
+            const uint32_t above_before = pl.z - pl.w;
+            const uint32_t pos = pl.z + ct.x + (P.y - above_before);
+            if (pos < A.cap_refs && pos < pl.z + ct.x + ct.y) {
+                A.nx_refs[pos] = it.tri;
+                A.nx_ref_node[pos] = pl.y + (ct.x ? 1u : 0u);
             } else {
                 atomicOr(A.err, 2u);
             }
         }
     }
-}
+};
 
 // ---------------------------------------------------------------------------
 // host side
@@ -915,24 +1145,21 @@ static cudaError_t dalloc(T *&p, size_t n) {
 }
 
 void build_release(BuildState &S) {
-    auto f = [](void *p) {
-        if (p) cudaFree(p);
+    auto f = [](auto *&p) {
+        if (p) cudaFree((void *)p);
+        p = nullptr;
     };
     f(S.tb_lo); f(S.tb_hi);
     for (int k = 0; k < 2; k++) {
         f(S.n_lo[k]); f(S.n_hi[k]); f(S.n_info[k]); f(S.refs[k]); f(S.ref_node[k]);
-        S.n_lo[k] = S.n_hi[k] = nullptr; S.n_info[k] = nullptr; S.refs[k] = S.ref_node[k] = nullptr;
     }
-    f(S.d_axis); f(S.d_plane); f(S.d_cnt); f(S.plan); f(S.plan_tot); f(S.prep); f(S.prep_tot);
+    f(S.d_axis); f(S.d_plane); f(S.d_cnt); f(S.plan);
     f(S.chunks); f(S.hist); f(S.done); f(S.lrank); f(S.feat); f(S.logits);
-    S.lrank = nullptr; S.feat = nullptr; S.logits = nullptr; f(S.rscan); f(S.rscan_tot); f(S.scan_partials); f(S.ctr); f(S.err);
+    f(S.plan_flags); f(S.ref_flags); f(S.plan_agg); f(S.plan_incl); f(S.ref_agg); f(S.ref_incl); f(S.epoch);
+    f(S.ctr); f(S.err);
     f(S.out_nodes); f(S.out_refs); f(S.out_ropes); f(S.out_cbox);
-    S.tb_lo = S.tb_hi = nullptr;
-    S.d_axis = nullptr; S.d_plane = nullptr; S.d_cnt = nullptr; S.plan = nullptr; S.plan_tot = nullptr;
-    S.prep = nullptr; S.prep_tot = nullptr; S.chunks = nullptr; S.hist = nullptr; S.done = nullptr; S.rscan = nullptr;
-    S.rscan_tot = nullptr; S.scan_partials = nullptr; S.ctr = nullptr; S.err = nullptr;
-    S.out_nodes = nullptr; S.out_refs = nullptr; S.out_ropes = nullptr; S.out_cbox = nullptr;
     S.nt = S.cap_refs = S.cap_nodes = S.cap_level = 0;
+    S.plan_tiles = S.ref_tiles = 0;
     S.active = false;
 }
 
@@ -952,8 +1179,8 @@ hk_status build_prepare(BuildState &S, const BuildParams &p, uint32_t nt, int sm
     S.cap_level = std::min(cap_refs, cap_nodes) + 1;
     S.cap_large = cap_refs / kSmall + 2;
     S.cap_chunks = cap_refs / kChunk + S.cap_large + 2;
-    uint32_t tiles = (std::max(cap_refs, S.cap_level) + kTile - 1) / kTile + 1;
-    S.cap_partials = tiles;
+    S.plan_tiles = S.cap_level / kScanThreads + 2;   // one node per thread
+    S.ref_tiles = cap_refs / kTile + 2;
     bool bad = false;
     bad |= dalloc(S.tb_lo, nt) != cudaSuccess;
     bad |= dalloc(S.tb_hi, nt) != cudaSuccess;
@@ -968,22 +1195,24 @@ hk_status build_prepare(BuildState &S, const BuildParams &p, uint32_t nt, int sm
     bad |= dalloc(S.d_plane, S.cap_level) != cudaSuccess;
     bad |= dalloc(S.d_cnt, S.cap_level) != cudaSuccess;
     bad |= dalloc(S.plan, S.cap_level) != cudaSuccess;
-    bad |= dalloc(S.plan_tot, 1) != cudaSuccess;
-    bad |= dalloc(S.prep, S.cap_level) != cudaSuccess;
-    bad |= dalloc(S.prep_tot, 1) != cudaSuccess;
     bad |= dalloc(S.chunks, S.cap_chunks + S.cap_large) != cudaSuccess;  // tail holds large_slot
     bad |= dalloc(S.hist, (size_t)S.cap_large * kHist) != cudaSuccess;
     bad |= dalloc(S.done, S.cap_large) != cudaSuccess;
     bad |= dalloc(S.lrank, S.cap_level) != cudaSuccess;
     bad |= dalloc(S.feat, (size_t)S.cap_large * 200) != cudaSuccess;
     bad |= dalloc(S.logits, (size_t)S.cap_large * kMlpOut) != cudaSuccess;
-    bad |= dalloc(S.rscan, cap_refs) != cudaSuccess;
-    bad |= dalloc(S.rscan_tot, 1) != cudaSuccess;
+    bad |= dalloc(S.plan_flags, S.plan_tiles) != cudaSuccess;
+    bad |= dalloc(S.ref_flags, S.ref_tiles) != cudaSuccess;
     {
-        uint4 *pp = nullptr;
-        bad |= dalloc(pp, tiles) != cudaSuccess;
-        S.scan_partials = pp;
+        U5 *pa = nullptr, *pi = nullptr;
+        bad |= dalloc(pa, S.plan_tiles) != cudaSuccess;
+        bad |= dalloc(pi, S.plan_tiles) != cudaSuccess;
+        S.plan_agg = pa;
+        S.plan_incl = pi;
     }
+    bad |= dalloc(S.ref_agg, S.ref_tiles) != cudaSuccess;
+    bad |= dalloc(S.ref_incl, S.ref_tiles) != cudaSuccess;
+    bad |= dalloc(S.epoch, 1) != cudaSuccess;
     bad |= dalloc(S.ctr, 1) != cudaSuccess;
     bad |= dalloc(S.err, 1) != cudaSuccess;
     bad |= dalloc(S.out_nodes, cap_nodes) != cudaSuccess;
@@ -995,6 +1224,9 @@ hk_status build_prepare(BuildState &S, const BuildParams &p, uint32_t nt, int sm
         return HK_E_ALLOC;
     }
     cudaMemset(S.err, 0, 4);
+    cudaMemset(S.epoch, 0, 4);
+    cudaMemset(S.plan_flags, 0, (size_t)S.plan_tiles * 4);
+    cudaMemset(S.ref_flags, 0, (size_t)S.ref_tiles * 4);
     cudaMemset(S.ctr, 0, sizeof(BuildCounters));
     return HK_OK;
 }
@@ -1023,13 +1255,13 @@ cudaError_t build_launch(BuildState &S, const float4 *verts, const uint4 *tris, 
     A.large_slot = reinterpret_cast<uint32_t *>(S.chunks + S.cap_chunks);
     A.hist = S.hist;
     A.done = S.done;
-    A.rscan = S.rscan;
     A.out_nodes = S.out_nodes;
     A.out_refs = S.out_refs;
     A.out_ropes = S.out_ropes;
     A.out_cbox = S.out_cbox;
     A.ctr = S.ctr;
     A.err = S.err;
+    A.epoch = S.epoch;
     A.ct = S.p.ct;
     A.ci = S.p.ci;
     A.max_depth = S.p.max_depth;
@@ -1054,6 +1286,10 @@ cudaError_t build_launch(BuildState &S, const float4 *verts, const uint4 *tris, 
     }
     if (A.learned && !(S.learn && S.learn->have_mlp)) return cudaErrorInvalidValue;
     cudaMemsetAsync(S.ctr, 0, sizeof(BuildCounters), st);
+    // per-rank histograms / done counters start at zero (the kernels clean
+    // what they use; this also clears what an aborted build left)
+    cudaMemsetAsync(S.hist, 0, (size_t)S.cap_large * kHist * sizeof(uint32_t), st);
+    cudaMemsetAsync(S.done, 0, (size_t)S.cap_large * sizeof(uint32_t), st);
     if (nt) k_tri_bounds<<<(nt + 255) / 256, 256, 0, st>>>(verts, tris, nt, S.tb_lo, S.tb_hi);
     A.nx_lo = S.n_lo[0];
     A.nx_hi = S.n_hi[0];
@@ -1076,15 +1312,15 @@ cudaError_t build_launch(BuildState &S, const float4 *verts, const uint4 *tris, 
         A.ref_node = S.ref_node[cur];
         A.nx_refs = S.refs[nxt];
         A.nx_ref_node = S.ref_node[nxt];
-        k_prep<<<G, 256, 0, st>>>(A);
         k_work<<<G * 2, 256, 0, st>>>(A);
         if (A.learned) {
             mlp_infer(S.learn->mlp, S.feat, &A.lc->n_large, S.cap_large, S.logits, G, st);
             k_propose<<<G * 2, 256, 0, st>>>(A);
         }
-        scan<uint4>(LoadPlan{A}, reinterpret_cast<uint4 *>(S.scan_partials), S.plan, S.plan_tot, G, st);
-        scan<uint2>(LoadRefFlags{A}, reinterpret_cast<uint2 *>(S.scan_partials), S.rscan, S.rscan_tot, G, st);
-        k_scatter<<<G, 256, 0, st>>>(A);
+        k_onepass<PlanOp><<<G, kScanThreads, 0, st>>>(PlanOp{A}, S.plan_flags, static_cast<U5 *>(S.plan_agg),
+                                                      static_cast<U5 *>(S.plan_incl), &A.lc->plan_ticket);
+        k_onepass<RefOp><<<G, kScanThreads, 0, st>>>(RefOp{A}, S.ref_flags, S.ref_agg, S.ref_incl,
+                                                     &A.lc->ref_ticket);
     }
     S.active = true;
     S.last_level = S.p.max_depth + 1;

@@ -33,8 +33,9 @@ struct LearnBuffers {
 
 constexpr int kMaxLevels = 52;  // max_depth <= 48, plus the level after the last
 
-// counters of one tree level; level L's kernels read lvl[L] and the scan that
-// plans its children writes lvl[L + 1], so no bookkeeping launch is needed
+// counters of one tree level; level L's kernels read lvl[L] and the plan
+// scan that emits its children writes lvl[L + 1], so no bookkeeping launch
+// is needed
 struct LevelCounters {
     uint32_t nodes;             // active nodes of the level
     uint32_t refs;              // their references
@@ -43,6 +44,10 @@ struct LevelCounters {
     uint32_t stop;              // the level stops splitting (capacity)
     uint32_t n_large;           // large nodes (chunked histograms)
     uint32_t n_chunks;          // histogram chunks
+    // tallies of the level's decisions (the capacity guard's inputs)
+    uint32_t t_leafrefs, t_leafnodes, t_splits, t_next, t_childrefs;
+    // tile tickets of the single-pass scans
+    uint32_t plan_ticket, ref_ticket;
 };
 
 // device scalars of one build (one struct in device memory)
@@ -76,20 +81,19 @@ struct BuildState {
     int32_t *d_axis = nullptr;
     float *d_plane = nullptr;
     uint2 *d_cnt = nullptr;                      // below, above
-    uint4 *plan = nullptr;                       // scan of (leafrefs, pairs, nextnodes, childrefs)
-    uint4 *plan_tot = nullptr;
-    uint2 *prep = nullptr;                       // scan of (is_large, chunks)
-    uint2 *prep_tot = nullptr;
-    uint2 *chunks = nullptr;                     // (slot, large rank)
+    uint4 *plan = nullptr;                       // per node: leaf-ref / child-ref / below-ref offsets, next slot
+    uint2 *chunks = nullptr;                     // (large rank, chunk index); tail: large_slot
     uint32_t *hist = nullptr;                    // per large node 3 x 96
     uint32_t *done = nullptr;                    // per large node: chunks finished
     // references (ping-pong)
     uint32_t *refs[2] = {nullptr, nullptr};
     uint32_t *ref_node[2] = {nullptr, nullptr};
-    uint2 *rscan = nullptr;                      // exclusive scan of (below, above) flags
-    uint2 *rscan_tot = nullptr;
-    void *scan_partials = nullptr;               // scan scratch
-    uint32_t cap_partials = 0;
+    // single-pass scan tile states (flags, aggregates, inclusive prefixes)
+    uint32_t *plan_flags = nullptr, *ref_flags = nullptr;
+    void *plan_agg = nullptr, *plan_incl = nullptr;
+    uint2 *ref_agg = nullptr, *ref_incl = nullptr;
+    uint32_t plan_tiles = 0, ref_tiles = 0;
+    uint32_t *epoch = nullptr;                   // build counter (scan flag tags)
     BuildCounters *ctr = nullptr;
     uint32_t *err = nullptr;
     // output

@@ -196,22 +196,44 @@ __device__ __forceinline__ void mma_bf16(float *c, const uint32_t *a, const uint
         : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
 }
 
-constexpr int kRowsCta = 128;
+constexpr int kRowsCta = 64;      // 4 row groups of 16 x 2 column halves = 8 warps
 constexpr int kActStride = 264;   // bf16 elements per activation row (256 + 8: conflict-free fragment loads)
+constexpr size_t kWBufBytes = (size_t)(kMlpHid / 16) * (kMlpHid / 8) * 32 * 8;   // largest packed layer
+constexpr size_t kInferSmem = 2 * (size_t)kRowsCta * kActStride * 2 + kWBufBytes;
 
-// one layer for the warp's 16 rows: out = act(in[16 x K] W[K x N] + b)
+// packed layer weights -> shared memory (16-byte cp.async; every size is a
+// multiple of 256 bytes)
+__device__ __forceinline__ void stage_weights(uint32_t *wbuf, const uint32_t *__restrict__ Wp, int K, int N) {
+    const int n16 = (K / 16) * (N / 8) * 32 * 8 / 16;
+    const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(wbuf);
+    for (int i = threadIdx.x; i < n16; i += blockDim.x)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sbase + 16u * i), "l"(Wp + 4 * (size_t)i)
+                     : "memory");
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+
+__device__ __forceinline__ void wait_weights() {
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    __syncthreads();
+}
+
+// one layer: warp (row group rg, column half ch) computes its 16 rows x N/2
+// columns of act(in[16 x K] W[K x N] + b); W fragments from shared memory
 template <bool LAST>
-__device__ __forceinline__ void mlp_layer(const __nv_bfloat16 *in, int K, const uint32_t *__restrict__ Wp, int N,
+__device__ __forceinline__ void mlp_layer(const __nv_bfloat16 *in, int K, const uint32_t *Ws, int N,
                                           const float *__restrict__ bias, __nv_bfloat16 *out, float *__restrict__ logits,
                                           int row0, int rows) {
     const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
-    const int wrow = (threadIdx.x >> 5) * 16;
+    const int warp = threadIdx.x >> 5;
+    const int wrow = (warp & 3) * 16;
     const int KT = K / 16, NT = N / 8;
-    for (int nc = 0; nc < NT; nc += 8) {
+    const int nt0 = (warp >> 2) * (NT / 2), nt1 = nt0 + NT / 2;
+    const uint2 *Wf = reinterpret_cast<const uint2 *>(Ws);
+    for (int nc = nt0; nc < nt1; nc += 8) {
         float acc[8][4];
 #pragma unroll
         for (int j = 0; j < 8; j++) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.0f;
-        const int nj = NT - nc < 8 ? NT - nc : 8;
+        const int nj = nt1 - nc < 8 ? nt1 - nc : 8;
         for (int kt = 0; kt < KT; kt++) {
             const int c = kt * 16 + 2 * t;
             uint32_t a[4];
@@ -222,7 +244,7 @@ __device__ __forceinline__ void mlp_layer(const __nv_bfloat16 *in, int K, const 
 #pragma unroll
             for (int j = 0; j < 8; j++) {
                 if (j >= nj) break;
-                const uint2 bf = __ldg(reinterpret_cast<const uint2 *>(Wp) + ((size_t)(kt * NT + nc + j) * 32 + lane));
+                const uint2 bf = Wf[(size_t)(kt * NT + nc + j) * 32 + lane];
                 uint32_t b[2] = {bf.x, bf.y};
                 mma_bf16(acc[j], a, b);
             }
@@ -261,24 +283,32 @@ __global__ void __launch_bounds__(256) k_mlp_infer(MlpDevice M, const float *__r
     extern __shared__ __align__(16) unsigned char sm_raw[];
     __nv_bfloat16 *act0 = reinterpret_cast<__nv_bfloat16 *>(sm_raw);
     __nv_bfloat16 *act1 = act0 + kRowsCta * kActStride;
+    uint32_t *wbuf = reinterpret_cast<uint32_t *>(act1 + kRowsCta * kActStride);
     // rows_dev (device count, e.g. written by the builder) is clamped to
     // rows_host, the capacity of X and logits
     const int rows = (int)(rows_dev ? min(*rows_dev, rows_host) : rows_host);
     for (int row0 = blockIdx.x * kRowsCta; row0 < rows; row0 += gridDim.x * kRowsCta) {
-        // stage the CTA's rows as BF16 (features 200 -> padded 208 with zeros)
+        stage_weights(wbuf, M.w1p, kMlpInPad, kMlpHid);
+        // the tile's rows as BF16 (features 200 -> padded 208 with zeros)
         for (int i = threadIdx.x; i < kRowsCta * kMlpInPad; i += blockDim.x) {
             int r = i / kMlpInPad, c = i % kMlpInPad;
             float v = (row0 + r < rows && c < kMlpIn) ? X[(size_t)(row0 + r) * kMlpIn + c] : 0.0f;
             act0[r * kActStride + c] = __float2bfloat16_rn(v);
         }
+        wait_weights();
+        mlp_layer<false>(act0, kMlpInPad, wbuf, kMlpHid, M.b1, act1, nullptr, row0, rows);
         __syncthreads();
-        mlp_layer<false>(act0, kMlpInPad, M.w1p, kMlpHid, M.b1, act1, nullptr, row0, rows);
-        __syncwarp();
-        mlp_layer<false>(act1, kMlpHid, M.w2p, kMlpHid, M.b2, act0, nullptr, row0, rows);
-        __syncwarp();
-        mlp_layer<false>(act0, kMlpHid, M.w3p, kMlpHid, M.b3, act1, nullptr, row0, rows);
-        __syncwarp();
-        mlp_layer<true>(act1, kMlpHid, M.w4p, kMlpOut, M.b4, nullptr, logits, row0, rows);
+        stage_weights(wbuf, M.w2p, kMlpHid, kMlpHid);
+        wait_weights();
+        mlp_layer<false>(act1, kMlpHid, wbuf, kMlpHid, M.b2, act0, nullptr, row0, rows);
+        __syncthreads();
+        stage_weights(wbuf, M.w3p, kMlpHid, kMlpHid);
+        wait_weights();
+        mlp_layer<false>(act0, kMlpHid, wbuf, kMlpHid, M.b3, act1, nullptr, row0, rows);
+        __syncthreads();
+        stage_weights(wbuf, M.w4p, kMlpHid, kMlpOut);
+        wait_weights();
+        mlp_layer<true>(act1, kMlpHid, wbuf, kMlpOut, M.b4, nullptr, logits, row0, rows);
         __syncthreads();
     }
 }
@@ -286,7 +316,7 @@ __global__ void __launch_bounds__(256) k_mlp_infer(MlpDevice M, const float *__r
 cudaError_t mlp_setup() {
     // the attribute is per device; set it once for each
     static uint64_t attr_set = 0;
-    const size_t smem = 2 * (size_t)kRowsCta * kActStride * sizeof(__nv_bfloat16);
+    const size_t smem = kInferSmem;
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
@@ -302,7 +332,7 @@ cudaError_t mlp_infer(const MlpDevice &M, const float *X, const uint32_t *rows_d
                       int grid, cudaStream_t s) {
     cudaError_t e = mlp_setup();
     if (e != cudaSuccess) return e;
-    const size_t smem = 2 * (size_t)kRowsCta * kActStride * sizeof(__nv_bfloat16);
+    const size_t smem = kInferSmem;
     k_mlp_infer<<<grid, 256, smem, s>>>(M, X, rows_dev, rows_host, logits);
     return cudaGetLastError();
 }
