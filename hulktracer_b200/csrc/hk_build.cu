@@ -302,61 +302,88 @@ struct Decision {
     int bin;      // plane index k of the chosen plane
 };
 
-// Warp-wide SAH over the node's histograms (all 32 lanes call it). The
-// first minimum in (axis, plane) order wins, as in the serial loop.
+// Warp-wide SAH over the node's histograms (all 32 lanes call it): lane k
+// costs plane k of every axis, keeps its cheapest, and one warp argmin over
+// (cost, axis, plane) picks the first minimum in (axis, plane) order, as the
+// serial loop does. Below / above counts come from exclusive scans over the
+// bins (packed 16 + 16 bits when the node has fewer than 65536 references).
 template <class HistPtr>
 __device__ Decision sah_warp(HistPtr H, float4 blo, float4 bhi, uint32_t cnt, float ct, float ci) {
     const uint32_t lane = threadIdx.x & 31u;
-    float A = surf(blo, bhi);
-    Decision best{-1, 0.0f, 0, 0, kInf, 0};
+    const float A = surf(blo, bhi);
+    const bool packed = cnt < 65536u;
+    float mc = kInf;
+    uint32_t mkey = 0xffffffffu, m_nb = 0, m_na = 0;
+    float m_pk = 0.0f;
+#pragma unroll 1
     for (uint32_t a = 0; a < 3; a++) {
-        float l = c3(blo, a), h = c3(bhi, a);
-        float ext = __fsub_rn(h, l);
+        const float l = c3(blo, a), h = c3(bhi, a);
+        const float ext = __fsub_rn(h, l);
         if (!(ext > 0.0f)) continue;
-        uint32_t hlo = H[a * 96 + lane], hhi = H[a * 96 + 32 + lane];
-        // exclusive prefix over bins < lane
-        uint32_t slo = hlo, shi = hhi;
-        for (int d = 1; d < 32; d <<= 1) {
-            uint32_t u = __shfl_up_sync(0xffffffffu, slo, d), w = __shfl_up_sync(0xffffffffu, shi, d);
-            if ((int)lane >= d) {
-                slo += u;
-                shi += w;
+        const uint32_t hlo = H[a * 96 + lane], hhi = H[a * 96 + 32 + lane];
+        uint32_t slo, shi;
+        if (packed) {
+            uint32_t v = hlo | (hhi << 16);
+            for (int d = 1; d < 32; d <<= 1) {
+                const uint32_t u = __shfl_up_sync(0xffffffffu, v, d);
+                if ((int)lane >= d) v += u;
+            }
+            slo = v & 0xffffu;
+            shi = v >> 16;
+        } else {
+            slo = hlo;
+            shi = hhi;
+            for (int d = 1; d < 32; d <<= 1) {
+                const uint32_t u = __shfl_up_sync(0xffffffffu, slo, d), w = __shfl_up_sync(0xffffffffu, shi, d);
+                if ((int)lane >= d) {
+                    slo += u;
+                    shi += w;
+                }
             }
         }
-        uint32_t below = slo - hlo;          // sum_{b < k} hlo[b]
-        uint32_t above = cnt - (shi - hhi);  // sum_{c >= k} hhi[c]
-        uint32_t on = H[a * 96 + 64 + lane];
-        float pk = plane_k(l, ext, lane), pk1 = plane_k(l, ext, lane + 1);
-        bool valid = lane >= 1 && pk > l && pk < h && (lane == 31 || pk < pk1);
-        float cost = kInf;
-        uint32_t nb = below + on, na = above + on;
-        if (valid) {
-            float4 bb = bhi, ba = blo;
-            s3(bb, a, pk);
-            s3(ba, a, pk);
-            float sb = surf(blo, bb), sa = surf(ba, bhi);
-            cost = __fadd_rn(ct, __fmul_rn(ci, __fdiv_rn(__fadd_rn(__fmul_rn(sb, (float)nb), __fmul_rn(sa, (float)na)), A)));
-            if (!(cost < kInf)) cost = kInf;  // NaN / inf never win
+        const uint32_t below = slo - hlo;          // sum_{b < k} hlo[b]
+        const uint32_t above = cnt - (shi - hhi);  // sum_{c >= k} hhi[c]
+        const uint32_t on = H[a * 96 + 64 + lane];
+        const float pk = plane_k(l, ext, lane), pk1 = plane_k(l, ext, lane + 1);
+        const bool valid = lane >= 1 && pk > l && pk < h && (lane == 31 || pk < pk1);
+        if (!valid) continue;
+        const uint32_t nb = below + on, na = above + on;
+        float4 bb = bhi, ba = blo;
+        s3(bb, a, pk);
+        s3(ba, a, pk);
+        const float sb = surf(blo, bb), sa = surf(ba, bhi);
+        const float cost =
+            __fadd_rn(ct, __fmul_rn(ci, __fdiv_rn(__fadd_rn(__fmul_rn(sb, (float)nb), __fmul_rn(sa, (float)na)), A)));
+        if (cost < mc) {   // NaN / inf never win; an earlier axis keeps ties
+            mc = cost;
+            mkey = a * 32u + lane;
+            m_nb = nb;
+            m_na = na;
+            m_pk = pk;
         }
-        // argmin with ties to the lower plane index
-        float mc = cost;
-        uint32_t mk = lane;
-        for (int off = 16; off; off >>= 1) {
-            float oc = __shfl_xor_sync(0xffffffffu, mc, off);
-            uint32_t ok = __shfl_xor_sync(0xffffffffu, mk, off);
-            if (oc < mc || (oc == mc && ok < mk)) {
-                mc = oc;
-                mk = ok;
-            }
+    }
+    // argmin over (cost, axis, plane)
+    float bc = mc;
+    uint32_t bk = mkey;
+    for (int off = 16; off; off >>= 1) {
+        const float oc = __shfl_xor_sync(0xffffffffu, bc, off);
+        const uint32_t ok = __shfl_xor_sync(0xffffffffu, bk, off);
+        if (oc < bc || (oc == bc && ok < bk)) {
+            bc = oc;
+            bk = ok;
         }
-        if (mc < best.cost) {
-            best.cost = mc;
-            best.axis = (int)a;
-            best.plane = __shfl_sync(0xffffffffu, pk, mk);
-            best.nb = __shfl_sync(0xffffffffu, nb, mk);
-            best.na = __shfl_sync(0xffffffffu, na, mk);
-            best.bin = (int)mk;
-        }
+    }
+    Decision best{-1, 0.0f, 0, 0, kInf, 0};
+    const uint32_t src = bk & 31u;
+    const float pk = __shfl_sync(0xffffffffu, m_pk, src);
+    const uint32_t nb = __shfl_sync(0xffffffffu, m_nb, src), na = __shfl_sync(0xffffffffu, m_na, src);
+    if (bc < kInf) {
+        best.axis = (int)(bk >> 5);
+        best.plane = pk;
+        best.nb = nb;
+        best.na = na;
+        best.cost = bc;
+        best.bin = (int)src;
     }
     if (best.axis >= 0 && !(best.cost < __fmul_rn(ci, (float)cnt))) best.axis = -1;
     return best;
@@ -558,124 +585,128 @@ __device__ void record_node(const LevelArgs &A, uint4 info, float4 blo, float4 b
     if ((threadIdx.x & 31u) == 0) A.rec_y[row] = d.axis * 32 + d.bin;
 }
 
-// Work items: first the chunks of large nodes (one CTA each; the CTA that
-// finishes a node's last chunk evaluates its SAH), then groups of 8 small
-// nodes (one warp each: warp-private histogram + SAH).
-__global__ void __launch_bounds__(256, 5) k_work(LevelArgs A) {
+// Large nodes, binned mode: one CTA per chunk of 1024 references builds the
+// chunk's histograms in shared memory and adds them to the node's global
+// histogram; the CTA that finishes the node's last chunk evaluates the SAH.
+__global__ void __launch_bounds__(256) k_hist(LevelArgs A) {
     __shared__ uint32_t H[kHist];
-    __shared__ uint32_t HS[8][kHist];
+    __shared__ float feat_scratch[200];
     __shared__ int s_last;
     __shared__ uint32_t s_tally[5];
     Tally tally;
     const uint32_t wib = threadIdx.x >> 5, lane = threadIdx.x & 31u;
     const uint32_t nch = min(A.lc->n_chunks, A.cap_chunks);
     const uint32_t nodes = A.lc->nodes;
-    const uint32_t ngroups = (nodes + 7) / 8;
-    for (uint32_t item = blockIdx.x; item < nch + ngroups; item += gridDim.x) {
-        if (item < nch) {
-            if (A.learned) continue;  // learned mode: chunks are costed by k_propose
-            uint2 ck = A.chunks[item];
-            uint32_t rank = ck.x;
-            if (rank >= A.cap_large) continue;  // uniform per CTA
-            uint32_t s = A.large_slot[rank];
-            if (s >= nodes) continue;
-            uint4 info = A.n_info[s];
-            uint32_t r0 = info.x + ck.y * kChunk, r1 = min(info.x + info.y, r0 + kChunk);
-            float4 blo = A.n_lo[s], bhi = A.n_hi[s];
-            for (uint32_t i = threadIdx.x; i < kHist; i += blockDim.x) H[i] = 0;
-            __syncthreads();
-            {
-                // the thread's references loaded together, their bounds two
-                // at a time (few dependent load latencies, no spills)
-                constexpr int kPer = kChunk / 256;
-                const float4 inv3 = bin_scale(blo, bhi);
-                uint32_t tri[kPer];
-#pragma unroll
-                for (int k = 0; k < kPer; k++) {
-                    const uint32_t r = r0 + threadIdx.x + 256u * k;
-                    tri[k] = r < r1 ? A.refs[r] : 0xffffffffu;
-                }
-#pragma unroll
-                for (int k = 0; k < kPer; k += 2) {
-                    float4 lo0, hi0, lo1, hi1;
-                    if (tri[k] != 0xffffffffu) {
-                        lo0 = A.tb_lo[tri[k]];
-                        hi0 = A.tb_hi[tri[k]];
-                    }
-                    if (tri[k + 1] != 0xffffffffu) {
-                        lo1 = A.tb_lo[tri[k + 1]];
-                        hi1 = A.tb_hi[tri[k + 1]];
-                    }
-                    if (tri[k] != 0xffffffffu) hist_ref(H, lo0, hi0, blo, bhi, inv3);
-                    if (tri[k + 1] != 0xffffffffu) hist_ref(H, lo1, hi1, blo, bhi, inv3);
-                }
-            }
-            __syncthreads();
-            uint32_t *G = A.hist + (size_t)rank * kHist;
-            for (uint32_t i = threadIdx.x; i < kHist; i += blockDim.x)
-                if (H[i]) atomicAdd(&G[i], H[i]);
-            __threadfence();
-            __syncthreads();
-            if (threadIdx.x == 0) {
-                uint32_t nchunks = (info.y + kChunk - 1) / kChunk;
-                s_last = (atomicAdd(&A.done[rank], 1u) == nchunks - 1) ? 1 : 0;
-            }
-            __syncthreads();
-            if (s_last && wib == 0) {
-                __threadfence();
-                Decision d = sah_warp(GHist{G}, blo, bhi, info.y, A.ct, A.ci);
-                if (lane == 0) {
-                    write_decision(A, s, d);
-                    tally.add(d, info.y);
-                }
-                // clean the histogram and the done counter for the next level
-                __syncwarp();
-                for (uint32_t i = lane; i < kHist; i += 32) G[i] = 0;
-                if (lane == 0) A.done[rank] = 0;
-                record_node(A, info, blo, bhi, d, reinterpret_cast<float *>(HS[0]));
-            }
-            __syncthreads();
-        } else {
-            uint32_t s = (item - nch) * 8 + wib;
-            if (s >= nodes) continue;
-            uint4 info = A.n_info[s];
-            uint32_t cnt = info.y;
-            bool dec = decidable(A, cnt);
-            if (dec && cnt > kSmall) {
-                // learned mode: the proposer's features instead of histograms
-                if (A.learned) {
-                    uint32_t row = A.lrank[s];
-                    if (row < A.cap_large)
-                        node_features(A, info, A.n_lo[s], A.n_hi[s], reinterpret_cast<float *>(HS[wib]),
-                                      A.feat + (size_t)row * 200);
-                }
-                continue;  // binned mode: handled by its chunks
-            }
-            if (!dec) {
-                if (lane == 0) {
-                    const Decision leaf{-1, 0.0f, 0, 0, kInf, 0};
-                    write_decision(A, s, leaf);
-                    tally.add(leaf, cnt);
-                }
-                continue;
-            }
-            uint32_t *Hw = HS[wib];
-            for (uint32_t i = lane; i < kHist; i += 32) Hw[i] = 0;
-            __syncwarp();
-            float4 blo = A.n_lo[s], bhi = A.n_hi[s];
+    for (uint32_t item = blockIdx.x; item < nch; item += gridDim.x) {
+        const uint2 ck = A.chunks[item];
+        const uint32_t rank = ck.x;
+        if (rank >= A.cap_large) continue;  // uniform per CTA
+        const uint32_t s = A.large_slot[rank];
+        if (s >= nodes) continue;
+        const uint4 info = A.n_info[s];
+        const uint32_t r0 = info.x + ck.y * kChunk, r1 = min(info.x + info.y, r0 + kChunk);
+        const float4 blo = A.n_lo[s], bhi = A.n_hi[s];
+        for (uint32_t i = threadIdx.x; i < kHist; i += blockDim.x) H[i] = 0;
+        __syncthreads();
+        {
+            // all of the thread's references and bounds loaded first
+            constexpr int kPer = kChunk / 256;
             const float4 inv3 = bin_scale(blo, bhi);
-            for (uint32_t r = info.x + lane; r < info.x + cnt; r += 32) {
-                uint32_t tri = A.refs[r];
-                hist_ref(Hw, A.tb_lo[tri], A.tb_hi[tri], blo, bhi, inv3);
+            uint32_t tri[kPer];
+            float4 tlo[kPer], thi[kPer];
+#pragma unroll
+            for (int k = 0; k < kPer; k++) {
+                const uint32_t r = r0 + threadIdx.x + 256u * k;
+                tri[k] = r < r1 ? A.refs[r] : 0xffffffffu;
             }
-            __syncwarp();
-            Decision d = sah_warp(Hw, blo, bhi, cnt, A.ct, A.ci);
+#pragma unroll
+            for (int k = 0; k < kPer; k++)
+                if (tri[k] != 0xffffffffu) {
+                    tlo[k] = A.tb_lo[tri[k]];
+                    thi[k] = A.tb_hi[tri[k]];
+                }
+#pragma unroll
+            for (int k = 0; k < kPer; k++)
+                if (tri[k] != 0xffffffffu) hist_ref(H, tlo[k], thi[k], blo, bhi, inv3);
+        }
+        __syncthreads();
+        uint32_t *G = A.hist + (size_t)rank * kHist;
+        for (uint32_t i = threadIdx.x; i < kHist; i += blockDim.x)
+            if (H[i]) atomicAdd(&G[i], H[i]);
+        __threadfence();
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            const uint32_t nchunks = (info.y + kChunk - 1) / kChunk;
+            s_last = (atomicAdd(&A.done[rank], 1u) == nchunks - 1) ? 1 : 0;
+        }
+        __syncthreads();
+        if (s_last && wib == 0) {
+            __threadfence();
+            const Decision d = sah_warp(GHist{G}, blo, bhi, info.y, A.ct, A.ci);
             if (lane == 0) {
                 write_decision(A, s, d);
-                tally.add(d, cnt);
+                tally.add(d, info.y);
             }
+            // clean the histogram and the done counter for the next level
             __syncwarp();
+            for (uint32_t i = lane; i < kHist; i += 32) G[i] = 0;
+            if (lane == 0) A.done[rank] = 0;
+            record_node(A, info, blo, bhi, d, feat_scratch);
         }
+        __syncthreads();
+    }
+    tally_flush(A, tally, s_tally);
+}
+
+// Small nodes (<= 256 references, or not splittable): one warp per node,
+// warp-private histogram + SAH. Learned mode: the warp of a large node
+// computes the proposer's features instead.
+__global__ void __launch_bounds__(256, 6) k_small(LevelArgs A) {
+    __shared__ uint32_t HS[8][kHist];
+    __shared__ uint32_t s_tally[5];
+    Tally tally;
+    const uint32_t wib = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+    const uint32_t nodes = A.lc->nodes;
+    const uint32_t ngroups = (nodes + 7) / 8;
+    for (uint32_t g = blockIdx.x; g < ngroups; g += gridDim.x) {
+        const uint32_t s = g * 8 + wib;
+        if (s >= nodes) continue;
+        const uint4 info = A.n_info[s];
+        const uint32_t cnt = info.y;
+        const bool dec = decidable(A, cnt);
+        if (dec && cnt > kSmall) {
+            if (A.learned) {
+                const uint32_t row = A.lrank[s];
+                if (row < A.cap_large)
+                    node_features(A, info, A.n_lo[s], A.n_hi[s], reinterpret_cast<float *>(HS[wib]),
+                                  A.feat + (size_t)row * 200);
+            }
+            continue;  // binned mode: k_hist
+        }
+        if (!dec) {
+            if (lane == 0) {
+                const Decision leaf{-1, 0.0f, 0, 0, kInf, 0};
+                write_decision(A, s, leaf);
+                tally.add(leaf, cnt);
+            }
+            continue;
+        }
+        uint32_t *Hw = HS[wib];
+        for (uint32_t i = lane; i < kHist; i += 32) Hw[i] = 0;
+        __syncwarp();
+        const float4 blo = A.n_lo[s], bhi = A.n_hi[s];
+        const float4 inv3 = bin_scale(blo, bhi);
+        for (uint32_t r = info.x + lane; r < info.x + cnt; r += 32) {
+            const uint32_t tri = A.refs[r];
+            hist_ref(Hw, A.tb_lo[tri], A.tb_hi[tri], blo, bhi, inv3);
+        }
+        __syncwarp();
+        const Decision d = sah_warp(Hw, blo, bhi, cnt, A.ct, A.ci);
+        if (lane == 0) {
+            write_decision(A, s, d);
+            tally.add(d, cnt);
+        }
+        __syncwarp();
     }
     tally_flush(A, tally, s_tally);
 }
@@ -1158,6 +1189,11 @@ void build_release(BuildState &S) {
     f(S.plan_flags); f(S.ref_flags); f(S.plan_agg); f(S.plan_incl); f(S.ref_agg); f(S.ref_incl); f(S.epoch);
     f(S.ctr); f(S.err);
     f(S.out_nodes); f(S.out_refs); f(S.out_ropes); f(S.out_cbox);
+    if (S.ev_fork) cudaEventDestroy(S.ev_fork);
+    if (S.ev_join) cudaEventDestroy(S.ev_join);
+    if (S.aux) cudaStreamDestroy(S.aux);
+    S.ev_fork = S.ev_join = nullptr;
+    S.aux = nullptr;
     S.nt = S.cap_refs = S.cap_nodes = S.cap_level = 0;
     S.plan_tiles = S.ref_tiles = 0;
     S.active = false;
@@ -1219,6 +1255,9 @@ hk_status build_prepare(BuildState &S, const BuildParams &p, uint32_t nt, int sm
     bad |= dalloc(S.out_refs, cap_refs) != cudaSuccess;
     bad |= dalloc(S.out_ropes, (size_t)cap_nodes * 6) != cudaSuccess;
     bad |= dalloc(S.out_cbox, (size_t)cap_nodes * 2) != cudaSuccess;
+    bad |= cudaStreamCreateWithFlags(&S.aux, cudaStreamNonBlocking) != cudaSuccess;
+    bad |= cudaEventCreateWithFlags(&S.ev_fork, cudaEventDisableTiming) != cudaSuccess;
+    bad |= cudaEventCreateWithFlags(&S.ev_join, cudaEventDisableTiming) != cudaSuccess;
     if (bad) {
         build_release(S);
         return HK_E_ALLOC;
@@ -1312,7 +1351,18 @@ cudaError_t build_launch(BuildState &S, const float4 *verts, const uint4 *tris, 
         A.ref_node = S.ref_node[cur];
         A.nx_refs = S.refs[nxt];
         A.nx_ref_node = S.ref_node[nxt];
-        k_work<<<G * 2, 256, 0, st>>>(A);
+        if (!A.learned) {
+            // large-node histograms on the second stream, beside the small
+            // nodes (independent nodes; both only add to the level tallies)
+            cudaEventRecord(S.ev_fork, st);
+            cudaStreamWaitEvent(S.aux, S.ev_fork, 0);
+            k_hist<<<G, 256, 0, S.aux>>>(A);
+            cudaEventRecord(S.ev_join, S.aux);
+            k_small<<<G * 2, 256, 0, st>>>(A);
+            cudaStreamWaitEvent(st, S.ev_join, 0);
+        } else {
+            k_small<<<G * 2, 256, 0, st>>>(A);
+        }
         if (A.learned) {
             mlp_infer(S.learn->mlp, S.feat, &A.lc->n_large, S.cap_large, S.logits, G, st);
             k_propose<<<G * 2, 256, 0, st>>>(A);
