@@ -218,6 +218,7 @@ def run_ours(args):
     import torch
     import torch.distributed as dist
     import hulktracer_b200 as hk
+    from hulktracer_b200.shard import frames_for_rank, reduce_job
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -241,7 +242,7 @@ def run_ours(args):
         ctx.set_parts(sc.part_of_vertex, sc.part_center.shape[0])
     rgba = torch.zeros(W * H, dtype=torch.int32, device="cuda")
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
-    frames = [args.warmup + rank + world * i for i in range(args.steps)]
+    frames = frames_for_rank(args.warmup, args.steps, rank, world)
     mats_all = {f: frame_mats(sc, f) for f in list(range(args.warmup)) + frames}
     # pinned host inputs / outputs for the e2e leg
     pin_mats = {f: (torch.from_numpy(m).pin_memory() if m is not None else None) for f, m in mats_all.items()}
@@ -291,15 +292,7 @@ def run_ours(args):
         t_e2e = sum(e0.elapsed_time(e1) for e0, e1 in ev2) / 1000.0
 
     # ---- max over ranks ----
-    tt = torch.tensor([t_dev, t_e2e, float(rays)], dtype=torch.float64, device="cuda")
-    if world > 1:
-        mx = tt.clone()
-        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
-        sm = tt.clone()
-        dist.all_reduce(sm, op=dist.ReduceOp.SUM)
-        t_dev, t_e2e, total_rays = float(mx[0]), float(mx[1]), float(sm[2])
-    else:
-        total_rays = float(rays)
+    (t_dev, t_e2e), total_rays = reduce_job([t_dev, t_e2e], rays, world, device="cuda")
 
     # ---- roofline of the trace kernel (rank 0) ----
     roof = None

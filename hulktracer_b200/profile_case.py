@@ -44,7 +44,10 @@ def main():
     mode = hk.BUILD_LEARNED if a.mode == "learned" else hk.BUILD_BINNED
     st = ctx.build(mode)
     if a.case == "trace":
-        rays = torch.from_numpy(ctx.camera_rays(sc.camera, W, H)).cuda()
+        # primary rays in the frame's 8x4-pixel tile order
+        rays_h = ctx.camera_rays(sc.camera, W, H)
+        rays_h = np.ascontiguousarray(rays_h.reshape(H // 4, 4, W // 8, 8, 8).transpose(0, 2, 1, 3, 4).reshape(-1, 8))
+        rays = torch.from_numpy(rays_h).cuda()
         hits = torch.zeros(2 * W * H, dtype=torch.int32, device="cuda")
         for _ in range(a.reps):
             ctx.trace_device(rays.data_ptr(), W * H, hits.data_ptr(), hk.VARIANTS[a.variant])
@@ -94,7 +97,6 @@ def main():
                       hk.VARIANTS[a.variant], True)
         ctx.synchronize()
     print("case %s done: tree %s" % (a.case, {k: st[k] for k in ("nodes", "refs", "depth")}))
-    del np
 
 
 if __name__ == "__main__":
