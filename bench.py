@@ -66,7 +66,8 @@ def make_scene(name):
 
 
 def workload_name(sc):
-    return "%s %d tris %dx%d primary+shadow" % (sc.name, sc.ntris, sc.width, sc.height)
+    rays = "primary+mirror+shadow" if "mirror" in sc.extra else "primary+shadow"
+    return "%s %d tris %dx%d %s" % (sc.name, sc.ntris, sc.width, sc.height, rays)
 
 
 def frame_mats(sc, f):
@@ -240,6 +241,10 @@ def run_ours(args):
     animated = sc.part_of_vertex is not None
     if animated:
         ctx.set_parts(sc.part_of_vertex, sc.part_center.shape[0])
+    if "mirror" in sc.extra:
+        # the large static scene: one mirror bounce on 30% of the triangles
+        ctx.set_mirrors(sc.extra["mirror"])
+        ctx.set_frame_shading(hk.SHADE_MIRROR)
     rgba = torch.zeros(W * H, dtype=torch.int32, device="cuda")
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     frames = frames_for_rank(args.warmup, args.steps, rank, world)

@@ -85,6 +85,10 @@ def load(path: str = LIB_PATH):
         "hk_scene_set_parts": [vp, u32p, u32],
         "hk_scene_transform": [vp, f32p],
         "hk_scene_get_vertices": [vp, f32p],
+        "hk_scene_get_counts": [vp, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)],
+        "hk_tree_save_file": [vp, C.c_char_p],
+        "hk_set_frame_shading": [vp, C.c_int],
+        "hk_tree_load_file": [vp, C.c_char_p, C.c_int],
         "hk_scene_set_mirrors": [vp, vp, u32],
         "hk_precompute": [vp],
         "hk_cache_import": [vp, f32p, u32],

@@ -14,6 +14,7 @@
 #include "hk_internal.h"
 #include "hk_mlp.h"
 #include <random>
+#include <unordered_map>
 
 using namespace hk;
 
@@ -104,6 +105,7 @@ struct hk_ctx {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     uint64_t last_primary = 0;
     int last_shade = HK_SHADE_CPU;
+    int frame_shade = HK_SHADE_CPU;   // shading of hk_frame
     // learned split proposer
     LearnBuffers learn;
     DevBuf<float> mlp_params, mlp_grads, mlp_m, mlp_v;
@@ -374,6 +376,13 @@ hk_status hk_scene_set_mirrors(hk_ctx *c, const uint8_t *mirror, uint32_t nt) {
     HK_CUDA(c, cudaMemcpyAsync(c->mirror.p, mirror, nt, cudaMemcpyHostToDevice, c->stream));
     HK_CUDA(c, cudaStreamSynchronize(c->stream));
     c->has_mirrors = true;
+    return HK_OK;
+}
+
+hk_status hk_scene_get_counts(hk_ctx *c, uint32_t *nv, uint32_t *nt) {
+    if (!c) return HK_E_ILLEGAL_INPUT;
+    if (nv) *nv = c->nv;
+    if (nt) *nt = c->nt;
     return HK_OK;
 }
 
@@ -911,7 +920,17 @@ static hk_status frame_enqueue(hk_ctx *c, bool animated, uint32_t nl, uint32_t w
     }
     s = build_enqueue(c, mode);
     if (s != HK_OK) return s;
-    return render_enqueue(c, nl, w, h, v, HK_SHADE_CPU, d_rgba);
+    return render_enqueue(c, nl, w, h, v, c->frame_shade, d_rgba);
+}
+
+hk_status hk_set_frame_shading(hk_ctx *c, int shade) {
+    if (!c) return HK_E_ILLEGAL_INPUT;
+    if (shade != HK_SHADE_CPU && shade != HK_SHADE_PICTURE && shade != HK_SHADE_MIRROR)
+        return fail(c, HK_E_ILLEGAL_INPUT, "shade mode");
+    if (shade == HK_SHADE_MIRROR && !c->has_mirrors) return fail(c, HK_E_STATE, "hk_scene_set_mirrors first");
+    if (shade != c->frame_shade) invalidate_graph(c);
+    c->frame_shade = shade;
+    return HK_OK;
 }
 
 hk_status hk_frame(hk_ctx *c, const float *mats12, const float *cam16, const float *lights8, uint32_t nl, uint32_t w,
@@ -944,7 +963,7 @@ hk_status hk_frame(hk_ctx *c, const float *mats12, const float *cam16, const flo
     } else {
         uint64_t key = ((uint64_t)w << 40) ^ ((uint64_t)h << 20) ^ ((uint64_t)nl << 12) ^ ((uint64_t)mode << 8) ^
                        ((uint64_t)v << 4) ^ (animated ? 1u : 0u) ^ ((uint64_t)(uintptr_t)d_rgba << 1) ^
-                       ((uint64_t)c->nt << 44);
+                       ((uint64_t)c->nt << 44) ^ ((uint64_t)c->frame_shade << 2);
         if (!c->graph_exec || c->graph_key != key) {
             invalidate_graph(c);
             HK_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
@@ -1570,6 +1589,202 @@ hk_status hk_mlp_train(hk_ctx *c, uint32_t epochs, uint32_t batch, float lr, uin
     yb.release();
     W.release();
     return mlp_pack(c);
+}
+
+// ---------------------------------------------------------------------------
+// tree interchange file (the reference's KdFileHeader dataset layout)
+// ---------------------------------------------------------------------------
+struct KdFileHeader {
+    uint64_t headerSize, KDTreeSize, KDTreeOffset, leafExtDataSize, leafExtDataOffset, indexPerLeafSize,
+        indexPerLeafOffset, vertexPerLeafSize, vertexPerLeafOffset;
+};
+struct LeafExtData {
+    uint32_t indexOffset, vertexOffset, vertxSize, indexSize;
+};
+static const char kLeafTrailer[8] = {'H', 'K', 'L', 'E', 'A', 'F', 'P', 'L'};
+constexpr uint32_t kObjectPerLeafMult = 32;   // per-leaf blocks padded to 32 entries
+constexpr uint32_t kRefLeaf = 4u;             // KDTreeNode::m_flags of a leaf
+
+hk_status hk_tree_save_file(hk_ctx *c, const char *path) {
+    if (!c || !path) return HK_E_ILLEGAL_INPUT;
+    uint32_t nn = 0, nr = 0;
+    hk_status st = hk_tree_export(c, nullptr, 0, nullptr, 0, &nn, &nr);
+    if (st != HK_OK) return st;
+    std::vector<uint32_t> nodes((size_t)nn * 4), refs(std::max<uint32_t>(nr, 1));
+    st = hk_tree_export(c, nodes.data(), nn, refs.data(), nr, &nn, &nr);
+    if (st != HK_OK) return st;
+    std::vector<float> verts((size_t)c->nv * 4);
+    std::vector<uint32_t> tris((size_t)c->nt * 4);
+    HK_CUDA(c, cudaMemcpyAsync(verts.data(), c->verts.p, verts.size() * 4, cudaMemcpyDeviceToHost, c->stream));
+    HK_CUDA(c, cudaMemcpyAsync(tris.data(), c->tris.p, tris.size() * 4, cudaMemcpyDeviceToHost, c->stream));
+    HK_CUDA(c, cudaStreamSynchronize(c->stream));
+    float box[8];
+    if ((st = hk_scene_get_box(c, box)) != HK_OK) return st;
+    // per-leaf data: leaf-local vertex numbering in first-use order
+    std::vector<LeafExtData> ext;
+    std::vector<uint32_t> idx;      // 4 per entry
+    std::vector<float> lverts;      // 4 per entry
+    std::unordered_map<uint32_t, uint32_t> vmap;
+    for (uint32_t i = 0; i < nn; i++) {
+        const uint32_t *n = &nodes[4 * (size_t)i];
+        if (n[0] != kRefLeaf) continue;
+        vmap.clear();
+        LeafExtData e{(uint32_t)(idx.size() / 4), (uint32_t)(lverts.size() / 4), 0, 0};
+        uint32_t nloc = 0;
+        for (uint32_t k = 0; k < n[2]; k++) {
+            const uint32_t t = refs[n[1] + k];
+            uint32_t loc[4] = {0, 0, 0, 0};
+            for (int v = 0; v < 3; v++) {
+                const uint32_t g = tris[4 * (size_t)t + v];
+                auto it = vmap.find(g);
+                if (it != vmap.end()) {
+                    loc[v] = it->second;
+                } else {
+                    loc[v] = nloc;
+                    vmap.emplace(g, nloc++);
+                    lverts.insert(lverts.end(), &verts[4 * (size_t)g], &verts[4 * (size_t)g] + 4);
+                }
+            }
+            idx.insert(idx.end(), loc, loc + 4);
+        }
+        uint32_t ni = (uint32_t)(idx.size() / 4) - e.indexOffset, nv = (uint32_t)(lverts.size() / 4) - e.vertexOffset;
+        const uint32_t ri = (ni + kObjectPerLeafMult - 1) & ~(kObjectPerLeafMult - 1);
+        const uint32_t rv = (nv + kObjectPerLeafMult - 1) & ~(kObjectPerLeafMult - 1);
+        idx.resize(idx.size() + 4 * (size_t)(ri - ni), 0u);
+        lverts.resize(lverts.size() + 4 * (size_t)(rv - nv), 0.0f);
+        e.indexSize = ri;
+        e.vertxSize = rv;
+        ext.push_back(e);
+    }
+    KdFileHeader h{};
+    h.headerSize = sizeof(KdFileHeader);
+    h.KDTreeOffset = h.headerSize;
+    h.KDTreeSize = (uint64_t)nn * 16;
+    h.leafExtDataOffset = h.KDTreeOffset + h.KDTreeSize;
+    h.leafExtDataSize = ext.size() * sizeof(LeafExtData);
+    h.indexPerLeafOffset = (h.leafExtDataOffset + h.leafExtDataSize + 511) & ~(uint64_t)511;
+    h.indexPerLeafSize = idx.size() * 4;
+    h.vertexPerLeafOffset = h.indexPerLeafOffset + h.indexPerLeafSize;
+    h.vertexPerLeafSize = lverts.size() * 4;
+    FILE *f = fopen(path, "wb");
+    if (!f) return fail(c, HK_E_FILE_OPEN, "cannot open tree file for writing");
+    const uint64_t gap = h.indexPerLeafOffset - (h.leafExtDataOffset + h.leafExtDataSize);
+    std::vector<char> zeros(gap, 0);
+    const uint64_t counts[2] = {c->nt, nr};
+    bool ok = fwrite(&h, sizeof(h), 1, f) == 1 && fwrite(nodes.data(), 16, nn, f) == nn &&
+              (ext.empty() || fwrite(ext.data(), sizeof(LeafExtData), ext.size(), f) == ext.size()) &&
+              (gap == 0 || fwrite(zeros.data(), 1, gap, f) == gap) &&
+              (idx.empty() || fwrite(idx.data(), 4, idx.size(), f) == idx.size()) &&
+              (lverts.empty() || fwrite(lverts.data(), 4, lverts.size(), f) == lverts.size()) &&
+              fwrite(kLeafTrailer, 1, 8, f) == 8 && fwrite(counts, 8, 2, f) == 2 && fwrite(box, 4, 8, f) == 8 &&
+              (nr == 0 || fwrite(refs.data(), 4, nr, f) == nr);
+    if (fclose(f) != 0 || !ok) return fail(c, HK_E_FILE_CLOSE, "tree file write failed");
+    return HK_OK;
+}
+
+hk_status hk_tree_load_file(hk_ctx *c, const char *path, int load_scene) {
+    if (!c || !path) return HK_E_ILLEGAL_INPUT;
+    FILE *f = fopen(path, "rb");
+    if (!f) return fail(c, HK_E_FILE_OPEN, "cannot open tree file");
+    fseek(f, 0, SEEK_END);
+    const uint64_t fsize = (uint64_t)ftell(f);
+    fseek(f, 0, SEEK_SET);
+    KdFileHeader h{};
+    auto bad = [&](const char *m) {
+        fclose(f);
+        return fail(c, HK_E_ILLEGAL_INPUT, m);
+    };
+    if (fread(&h, sizeof(h), 1, f) != 1 || h.headerSize != sizeof(KdFileHeader)) return bad("not a tree file");
+    auto in_file = [&](uint64_t off, uint64_t size) { return off <= fsize && size <= fsize - off; };
+    if (h.KDTreeSize % 16 || h.leafExtDataSize % sizeof(LeafExtData) || h.indexPerLeafSize % 16 ||
+        h.vertexPerLeafSize % 16 || !in_file(h.KDTreeOffset, h.KDTreeSize) ||
+        !in_file(h.leafExtDataOffset, h.leafExtDataSize) || !in_file(h.indexPerLeafOffset, h.indexPerLeafSize) ||
+        !in_file(h.vertexPerLeafOffset, h.vertexPerLeafSize) || h.KDTreeSize / 16 >= (1u << 29))
+        return bad("tree file sizes or offsets out of range");
+    const uint32_t nn = (uint32_t)(h.KDTreeSize / 16);
+    const size_t nleaf = h.leafExtDataSize / sizeof(LeafExtData);
+    std::vector<uint32_t> nodes((size_t)nn * 4);
+    std::vector<LeafExtData> ext(nleaf);
+    std::vector<uint32_t> idx(h.indexPerLeafSize / 4);
+    std::vector<float> lverts(h.vertexPerLeafSize / 4);
+    bool ok = fseek(f, (long)h.KDTreeOffset, SEEK_SET) == 0 && fread(nodes.data(), 16, nn, f) == nn &&
+              fseek(f, (long)h.leafExtDataOffset, SEEK_SET) == 0 &&
+              (nleaf == 0 || fread(ext.data(), sizeof(LeafExtData), nleaf, f) == nleaf) &&
+              fseek(f, (long)h.indexPerLeafOffset, SEEK_SET) == 0 &&
+              (idx.empty() || fread(idx.data(), 4, idx.size(), f) == idx.size()) &&
+              fseek(f, (long)h.vertexPerLeafOffset, SEEK_SET) == 0 &&
+              (lverts.empty() || fread(lverts.data(), 4, lverts.size(), f) == lverts.size());
+    if (!ok) return bad("tree file truncated");
+    // the trailer (written by this library)
+    std::vector<uint32_t> refs;
+    uint64_t counts[2] = {0, 0};
+    float box[8];
+    bool have_trailer = false;
+    {
+        char m[8];
+        const uint64_t toff = h.vertexPerLeafOffset + h.vertexPerLeafSize;
+        if (toff + 56 <= fsize && fseek(f, (long)toff, SEEK_SET) == 0 && fread(m, 1, 8, f) == 8 &&
+            memcmp(m, kLeafTrailer, 8) == 0 && fread(counts, 8, 2, f) == 2 && fread(box, 4, 8, f) == 8 &&
+            counts[1] < (1ull << 30) && toff + 56 + counts[1] * 4 <= fsize) {
+            refs.resize(counts[1]);
+            have_trailer = counts[1] == 0 || fread(refs.data(), 4, counts[1], f) == counts[1];
+        }
+    }
+    fclose(f);
+    if (!load_scene) {
+        if (!have_trailer) return fail(c, HK_E_ILLEGAL_INPUT, "no leaf polygon list in the file (load_scene = 1)");
+        if (counts[0] != c->nt) return fail(c, HK_E_STATE, "the uploaded scene does not match the file");
+        return hk_tree_import(c, nodes.data(), nn, refs.data(), (uint32_t)refs.size());
+    }
+    // the per-leaf triangles become the scene; leaves take consecutive ids
+    std::vector<float> verts;
+    std::vector<uint32_t> tris, lrefs;
+    size_t leaf = 0;
+    for (uint32_t i = 0; i < nn; i++) {
+        uint32_t *n = &nodes[4 * (size_t)i];
+        if (n[0] != kRefLeaf) continue;
+        if (leaf >= nleaf) return fail(c, HK_E_ILLEGAL_INPUT, "fewer leaf records than leaves");
+        const LeafExtData &e = ext[leaf++];
+        const uint32_t cnt = n[2];
+        if (cnt > e.indexSize || (uint64_t)e.indexOffset + e.indexSize > idx.size() / 4 ||
+            (uint64_t)e.vertexOffset + e.vertxSize > lverts.size() / 4)
+            return fail(c, HK_E_ILLEGAL_INPUT, "leaf record out of range");
+        const uint32_t vbase = (uint32_t)(verts.size() / 4);
+        for (uint32_t k = 0; k < e.vertxSize; k++) {
+            const float *v = &lverts[4 * ((size_t)e.vertexOffset + k)];
+            verts.insert(verts.end(), {v[0], v[1], v[2], 1.0f});
+        }
+        n[1] = (uint32_t)lrefs.size();
+        for (uint32_t k = 0; k < cnt; k++) {
+            const uint32_t *t = &idx[4 * ((size_t)e.indexOffset + k)];
+            if (t[0] >= e.vertxSize || t[1] >= e.vertxSize || t[2] >= e.vertxSize)
+                return fail(c, HK_E_ILLEGAL_INPUT, "leaf vertex index out of range");
+            lrefs.push_back((uint32_t)(tris.size() / 4));
+            tris.insert(tris.end(), {vbase + t[0], vbase + t[1], vbase + t[2], 0u});
+        }
+    }
+    if (tris.empty()) return fail(c, HK_E_ILLEGAL_INPUT, "the file holds no triangles");
+    hk_status st = hk_scene_upload(c, verts.data(), (uint32_t)(verts.size() / 4), tris.data(), (uint32_t)(tris.size() / 4));
+    if (st != HK_OK) return st;
+    if (!have_trailer) {
+        // bounds of the vertices the triangles use (the padding entries are not)
+        for (int k = 0; k < 3; k++) {
+            box[k] = INFINITY;
+            box[4 + k] = -INFINITY;
+        }
+        box[3] = box[7] = 0.0f;
+        for (size_t i = 0; i < tris.size(); i++) {
+            if ((i & 3) == 3) continue;
+            const float *v = &verts[4 * (size_t)tris[i]];
+            for (int k = 0; k < 3; k++) {
+                box[k] = std::min(box[k], v[k]);
+                box[4 + k] = std::max(box[4 + k], v[k]);
+            }
+        }
+    }
+    if ((st = hk_scene_set_box(c, box)) != HK_OK) return st;
+    if ((st = hk_precompute(c)) != HK_OK) return st;
+    return hk_tree_import(c, nodes.data(), nn, lrefs.data(), (uint32_t)lrefs.size());
 }
 
 }  // extern "C"

@@ -137,6 +137,18 @@ class Context:
                                                   C.byref(nn), C.byref(nr)))
         return nodes, refs[:nr.value]
 
+    def save_tree_file(self, path):
+        """The current tree + vertices in the reference's dataset file layout."""
+        self._check(self.L.hk_tree_save_file(self.h, path.encode()))
+
+    def load_tree_file(self, path, load_scene=False):
+        """Import a tree file onto the uploaded scene, or (load_scene) upload
+        the file's per-leaf triangles as the scene with the tree over them."""
+        self._check(self.L.hk_tree_load_file(self.h, path.encode(), 1 if load_scene else 0))
+        nv, nt = C.c_uint32(), C.c_uint32()
+        self._check(self.L.hk_scene_get_counts(self.h, C.byref(nv), C.byref(nt)))
+        self.nverts, self.ntris = nv.value, nt.value
+
     def stats(self):
         st = _lib.TreeStats()
         self._check(self.L.hk_tree_stats_get(self.h, C.byref(st)))
@@ -190,6 +202,9 @@ class Context:
         self._check(self.L.hk_shade_picture(self.h, ptr(r), ptr(_f32(hit4)), r.shape[0], ptr(lights),
                                             lights.shape[0], ptr(out)))
         return out
+
+    def set_frame_shading(self, shade):
+        self._check(self.L.hk_set_frame_shading(self.h, int(shade)))
 
     def frame(self, mats12, cam, lights, w, h, d_rgba: int, mode=_lib.BUILD_BINNED, variant=_lib.SHORTSTACK,
               use_graph=True, want_stats=False):

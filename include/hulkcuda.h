@@ -148,6 +148,8 @@ hk_status hk_scene_get_box(hk_ctx *ctx, float *box8);
 hk_status hk_scene_set_parts(hk_ctx *ctx, const uint32_t *part_of_vertex, uint32_t nparts);
 hk_status hk_scene_transform(hk_ctx *ctx, const float *mats12);
 hk_status hk_scene_get_vertices(hk_ctx *ctx, float *verts4);
+/* vertex and triangle counts of the current scene */
+hk_status hk_scene_get_counts(hk_ctx *ctx, uint32_t *nv, uint32_t *nt);
 /* Per-triangle material flag (1 = mirror) for HK_SHADE_MIRROR. */
 hk_status hk_scene_set_mirrors(hk_ctx *ctx, const uint8_t *mirror, uint32_t nt);
 
@@ -215,12 +217,39 @@ hk_status hk_shade_picture(hk_ctx *ctx, const float *rays8, const float *hit4, u
 hk_status hk_frame(hk_ctx *ctx, const float *mats12, const float *cam16, const float *lights8,
                    uint32_t nl, uint32_t w, uint32_t h, hk_build_mode mode, hk_variant variant,
                    int use_graph, uint32_t *d_rgba, hk_tree_stats *stats);
+/* shading of hk_frame (HK_SHADE_CPU by default; HK_SHADE_MIRROR needs
+ * hk_scene_set_mirrors first) */
+hk_status hk_set_frame_shading(hk_ctx *ctx, int shade);
 
 /* Rays of the last hk_render / hk_render_device / hk_frame: primary rays and
  * shadow rays actually traced (synchronises the context's stream). */
 hk_status hk_get_ray_counts(hk_ctx *ctx, uint64_t *primary, uint64_t *shadow);
 /* Kernel nodes and all nodes of the captured frame graph (0 before capture). */
 hk_status hk_frame_graph_info(hk_ctx *ctx, uint32_t *kernel_nodes, uint32_t *all_nodes);
+
+/* ---- tree interchange file ----
+ * The reference's dataset dump (GLVisitorGPUTrace::saveDataSetToFile,
+ * HulkEngine/src/GLVisitorGPUTrace.cpp:638-674, read back by
+ * GLVisitorGPUTraceSSD::buildTree, GLVisitorGPUTraceSSD.cpp:43-107): a
+ * KdFileHeader (9 x uint64 sizes / offsets, GLVisitorGPUTrace.hpp:52-63), the
+ * KDTreeNode array, one LeafExtData {indexOffset, vertexOffset, vertxSize,
+ * indexSize} per leaf node in node order, then at a 512-byte boundary the
+ * per-leaf TriangleIndices (leaf-local vertex indices) and the per-leaf
+ * vertices, each leaf's blocks padded to a multiple of 32 entries
+ * (buildPerLeafData, GLVisitorGPUTrace.cpp:163-228). After the vertex block
+ * this library appends a trailer the reference does not read: "HKLEAFPL",
+ * uint64 triangle count, uint64 reference count, the scene box (8 floats),
+ * then the leaf polygon list (global triangle ids), so a file written here
+ * reloads onto its own scene.
+ *
+ * hk_tree_save_file writes the current tree and the current vertices.
+ * hk_tree_load_file with load_scene = 0 needs the trailer and an uploaded
+ * scene of the same triangle count and imports the tree as it was; with
+ * load_scene = 1 it uploads the per-leaf triangles as the scene (triangle id =
+ * position in the per-leaf lists, leaf by leaf) with a tree over them, as the
+ * reference's SSD path renders such a file. */
+hk_status hk_tree_save_file(hk_ctx *ctx, const char *path);
+hk_status hk_tree_load_file(hk_ctx *ctx, const char *path, int load_scene);
 
 /* ---- learned split proposer (no reference counterpart) ----
  * A 200 -> 256 -> 256 -> 256 -> 96 MLP (ReLU). Features of a node (sampled

@@ -130,3 +130,67 @@ def test_frame_graph_matches_oracle_pipeline(ctx, hk, oracle):
         rays = oracle.camera_rays(sc.camera, w, h, NORM_IEEE)
         oimg = oracle.render_cpu(tree, rays, w, h, sc.lights, O_SHORT, 6, NORM_IEEE)
         assert np.array_equal(img_g, oimg)
+
+
+def test_tree_file_layout_and_reload(ctx, hk, tmp_path):
+    """hk_tree_save_file writes the reference's dataset layout (compared with
+    the oracle's restatement of saveDataSetToFile); the file reloads onto its
+    scene as the same tree, and on its own (per-leaf triangles as the scene)
+    traces to the same hit distances."""
+    from oracle import treefile
+    g = load("small24k.npz")
+    ctx.upload(g["verts"], g["tris"])
+    ctx.set_box(g["box"])
+    ctx.import_cache(g["ref_cache"])
+    ctx.import_tree(g["ref_nodes"], g["ref_refs"])
+    nodes, refs = ctx.export_tree()
+    f = str(tmp_path / "tree.bin")
+    ctx.save_tree_file(f)
+    data = open(f, "rb").read()
+    want = treefile.dataset_bytes(nodes, refs, g["verts"], g["tris"])
+    assert data[:len(want)] == want
+    assert data[len(want):len(want) + 8] == b"HKLEAFPL"
+    hits = ctx.trace(g["rays"], hk.SHORTSTACK)
+    # reload onto the same scene: the same tree
+    c2 = hk.Context(short_stack=6)
+    c2.upload(g["verts"], g["tris"])
+    c2.import_cache(g["ref_cache"])
+    c2.load_tree_file(f)
+    n2, r2 = c2.export_tree()
+    assert np.array_equal(n2, nodes) and np.array_equal(r2, refs)
+    assert np.array_equal(c2.trace(g["rays"], hk.SHORTSTACK)["tri"], hits["tri"])
+    # on its own: triangle k of the new scene is leaf polygon k of the file
+    c3 = hk.Context()
+    c3.load_tree_file(f, load_scene=True)
+    assert c3.ntris == refs.shape[0]
+    h3 = c3.trace(g["rays"], hk.BRUTE)
+    ctx.precompute()   # the same (IEEE) triangle records as c3's
+    b = ctx.trace(g["rays"], hk.BRUTE)
+    m = b["tri"] >= 0
+    assert np.array_equal(h3["tri"] >= 0, m)
+    assert np.array_equal(h3["t"][m], b["t"][m])
+    h4 = c3.trace(g["rays"], hk.SHORTSTACK)
+    assert np.array_equal(h4["t"][m], b["t"][m])
+
+
+def test_frame_mirror_shading_equals_render(ctx, hk):
+    """hk_frame with HK_SHADE_MIRROR (graph) equals hk_render with the same
+    shading on the tree the frame built."""
+    import torch
+    sc = scenes.static_small(width=64, height=64)
+    nt = sc.ntris
+    h32 = (np.arange(nt, dtype=np.uint64) * np.uint64(2654435761)) & np.uint64(0xFFFFFFFF)
+    mirror = (h32.astype(np.float64) / 4294967296.0 < 0.3).astype(np.uint8)
+    ctx.upload(sc.verts, sc.tris)
+    ctx.set_mirrors(mirror)
+    ctx.set_frame_shading(hk.SHADE_MIRROR)
+    try:
+        out = torch.zeros(64 * 64, dtype=torch.int32, device="cuda")
+        ctx.frame(None, sc.camera, sc.lights, 64, 64, out.data_ptr(), use_graph=True)
+        ctx.synchronize()
+        img_f = out.cpu().numpy().view(np.uint32).copy()
+        img_r = ctx.render(sc.camera, sc.lights, 64, 64, hk.SHORTSTACK, hk.SHADE_MIRROR)
+        assert np.array_equal(img_f, img_r)
+        assert (img_r != ctx.render(sc.camera, sc.lights, 64, 64, hk.SHORTSTACK)).any()
+    finally:
+        ctx.set_frame_shading(hk.SHADE_CPU)
