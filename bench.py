@@ -70,6 +70,10 @@ def workload_name(sc):
     return "%s %d tris %dx%d %s" % (sc.name, sc.ntris, sc.width, sc.height, rays)
 
 
+def traffic_tag(sc):
+    return {"animated_parts_200k": "animated200k"}.get(sc.name, sc.name)
+
+
 def frame_mats(sc, f):
     from hulktracer_b200 import scenes
     if sc.part_center is None:
@@ -335,6 +339,8 @@ def run_ours(args):
 
 def trace_roofline(ctx, sc, stream, variant):
     import torch
+
+    import hulktracer_b200 as hk
     W, H = sc.width, sc.height
     n = W * H
     rays_h = ctx.camera_rays(sc.camera, W, H)
@@ -362,11 +368,16 @@ def trace_roofline(ctx, sc, stream, variant):
     t = e0.elapsed_time(e1) / 1000.0 / reps
     peak, src = measured_peak()
     achieved = n * b_ray / t / 1e9
+    # DRAM bytes of one launch from the committed ncu summary of the same
+    # kernel, workload and tree (dram__bytes_read.sum + dram__bytes_write.sum)
     traffic = None
-    prof = os.path.join(ROOT, "profiles", "trace_traffic.json")
+    vname = {v: k for k, v in hk.VARIANTS.items()}.get(variant, "")
+    prof = os.path.join(ROOT, "profiles", "k_trace_%s_%s_primary.md" % (vname, traffic_tag(sc)))
     if os.path.exists(prof):
         with open(prof) as f:
-            traffic = json.load(f).get("bytes_per_launch")
+            for line in f:
+                if line.startswith("| traffic_bytes_per_launch |"):
+                    traffic = int(line.split("|")[2])
     return {"kernel": "k_trace primary rays", "bound": "hbm", "achieved": achieved, "peak": peak,
             "peak_source": src, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
             "launch_ms": t * 1000.0, "rays_per_launch": n, "bytes_per_ray": b_ray,
