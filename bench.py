@@ -48,6 +48,8 @@ def parse():
     ap.add_argument("--workload", default="animated", choices=["animated", "static_small", "static_large"])
     ap.add_argument("--mode", default="binned", choices=["binned", "learned"])
     ap.add_argument("--variant", default="ropes")
+    ap.add_argument("--exact-max", type=int, default=0,
+                    help="exact SAH on nodes of at most this many references (0: 32-bin binned SAH everywhere)")
     ap.add_argument("--weights", default=os.path.join(os.path.dirname(os.path.abspath(__file__)), "hulktracer_b200",
                                                       "weights", "proposer.bin"),
                     help="trained proposer weights (learned mode)")
@@ -237,7 +239,7 @@ def run_ours(args):
     variant = hk.VARIANTS[args.variant]
     mode = hk.BUILD_LEARNED if args.mode == "learned" else hk.BUILD_BINNED
     stream = torch.cuda.Stream()
-    ctx = hk.Context(device=local)
+    ctx = hk.Context(device=local, exact_max=args.exact_max)
     ctx.set_stream(stream.cuda_stream)
     if mode == hk.BUILD_LEARNED:
         ctx.mlp_load(args.weights)
@@ -320,7 +322,8 @@ def run_ours(args):
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1000.0 * t_dev / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scene)",
-            "config": {"workload": workload_name(sc), "build": "GPU %s SAH (32 bins/axis), per frame" % args.mode,
+            "config": {"workload": workload_name(sc), "build": "GPU %s SAH (32 bins/axis%s), per frame" % (
+                           args.mode, ", exact on nodes <= %d refs" % args.exact_max if args.exact_max else ""),
                        "traversal": args.variant, "graph": "one CUDA graph per frame",
                        "l2": "flushed (256 MB write) between frames", "parallelism": "frames sharded over %d GPU(s)" % world},
             "e2e": {"value": total_rays / t_e2e / 1e6, "unit": "Mrays/s", "h2d_bytes_per_step": h2d,

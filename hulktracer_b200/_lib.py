@@ -35,7 +35,8 @@ class Config(C.Structure):
     _fields_ = [("device", C.c_int), ("traverse_cost", C.c_float), ("intersect_cost", C.c_float),
                 ("max_depth", C.c_uint32), ("leaf_size", C.c_uint32), ("bins", C.c_uint32),
                 ("short_stack", C.c_uint32), ("block_size", C.c_uint32), ("blocks_per_sm", C.c_uint32),
-                ("max_refs", C.c_uint32), ("topk", C.c_uint32), ("fallback_ratio", C.c_float)]
+                ("max_refs", C.c_uint32), ("topk", C.c_uint32), ("fallback_ratio", C.c_float),
+                ("exact_max", C.c_uint32)]
 
 
 class TuneResult(C.Structure):

@@ -165,6 +165,7 @@ hk_status hk_config_default(hk_config *cfg) {
     cfg->max_refs = 0;
     cfg->topk = 4;
     cfg->fallback_ratio = 1.02f;
+    cfg->exact_max = 0;
     return HK_OK;
 }
 
@@ -175,6 +176,7 @@ static hk_status validate_config(const hk_config *c) {
     if (c->max_depth < 1 || c->max_depth > 48) return HK_E_ILLEGAL_INPUT;
     if (!(c->intersect_cost > 0) || !(c->traverse_cost >= 0)) return HK_E_ILLEGAL_INPUT;
     if (c->topk < 1 || c->topk > 8 || !(c->fallback_ratio >= 0)) return HK_E_ILLEGAL_INPUT;
+    if (c->exact_max != 0 && (c->exact_max < 32 || c->exact_max > 1024)) return HK_E_ILLEGAL_INPUT;
     return HK_OK;
 }
 
@@ -508,7 +510,11 @@ hk_status hk_tree_import(hk_ctx *c, const uint32_t *nodes4, uint32_t nn, const u
 static hk_status sync_tree_sizes(hk_ctx *c) {
     if (c->tree_on_device_counts) {
         hk_status s = build_read_stats(c->build, c->stream, &c->stats);
-        if (s != HK_OK) return fail(c, s, "build stats");
+        if (s != HK_OK) {
+            char msg[96];
+            snprintf(msg, sizeof msg, "build failed (error bits 0x%x)", c->build.last_err);
+            return fail(c, s, msg);
+        }
         c->nn = c->stats.nodes;
         c->nr = c->stats.refs;
         c->tree_on_device_counts = false;
@@ -591,6 +597,7 @@ static BuildParams build_params(hk_ctx *c, hk_build_mode mode) {
     p.mode = (int)mode;
     p.topk = c->cfg.topk;
     p.fallback_ratio = c->cfg.fallback_ratio;
+    p.exact_max = c->cfg.exact_max;
     p.record = c->recording ? 1 : 0;
     c->build.learn = &c->learn;
     return p;

@@ -42,6 +42,7 @@ namespace hk {
 constexpr uint32_t kBins = 32;
 constexpr uint32_t kSmall = 256;     // nodes with <= kSmall refs: one warp per node
 constexpr uint32_t kChunk = 1024;    // refs per histogram CTA of a large node (4 per thread)
+constexpr uint32_t kWarpExact = 32;  // exact-SAH nodes up to this size: one warp, in registers
 constexpr uint32_t kHist = 3 * 3 * kBins;
 constexpr int kScanThreads = 256;
 constexpr int kScanItems = 4;
@@ -404,6 +405,7 @@ struct LevelArgs {
     uint4 *plan;            // per node: leaf-ref offset, next slot, child-ref offset, below-ref offset
     uint2 *chunks;          // (large rank, chunk index within the node)
     uint32_t *large_slot;
+    uint32_t *medium_slot;
     uint32_t *hist;
     uint32_t *done;
     const uint32_t *refs;
@@ -420,7 +422,8 @@ struct LevelArgs {
     uint32_t level;
     float ct, ci;
     uint32_t max_depth, leaf_size;
-    uint32_t cap_refs, cap_nodes, cap_level, cap_large, cap_chunks;
+    uint32_t cap_refs, cap_nodes, cap_level, cap_large, cap_chunks, cap_medium;
+    uint32_t exact_max;     // 0: binned everywhere; else nodes <= exact_max refs take the exact SAH
     // learned proposer
     int learned, record;
     uint32_t *lrank;        // node slot -> proposer row (0xffffffff: none)
@@ -442,10 +445,24 @@ __global__ void k_tri_bounds(const float4 *__restrict__ V, const uint4 *__restri
     hi[i] = make_float4(mxf(mxf(a.x, b.x), c.x), mxf(mxf(a.y, b.y), c.y), mxf(mxf(a.z, b.z), c.z), 0.0f);
 }
 
+__device__ __forceinline__ bool decidable(const LevelArgs &A, uint32_t cnt) {
+    return cnt > A.leaf_size && A.level < A.max_depth;
+}
+
+// classes of a splittable node by its reference count: small (one warp,
+// k_small), medium (exact SAH, one CTA, when exact_max reaches it) and large
+// (chunked binned histograms, or the proposer)
+__device__ __forceinline__ bool is_medium(const LevelArgs &A, uint32_t c) {
+    return A.exact_max >= kWarpExact && c > kWarpExact && c <= A.exact_max;
+}
+__device__ __forceinline__ bool is_large(const LevelArgs &A, uint32_t c) { return c > kSmall && !is_medium(A, c); }
+
 // root node + references of level 0 (the counters were zeroed by a memset);
 // a root with more than 256 references is the first large node
 __global__ void k_root(LevelArgs A, const float *box, uint32_t nt) {
-    const bool large = nt > kSmall && nt > A.leaf_size && A.max_depth > 0;
+    const bool dec = nt > A.leaf_size && A.max_depth > 0;
+    const bool medium = dec && is_medium(A, nt);
+    const bool large = dec && is_large(A, nt);
     const uint32_t nch = large ? (nt + kChunk - 1) / kChunk : 0u;
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         *A.epoch += 1u;
@@ -456,8 +473,10 @@ __global__ void k_root(LevelArgs A, const float *box, uint32_t nt) {
         l0->leafrefs_total = 0;
         l0->n_large = large ? 1u : 0u;
         l0->n_chunks = nch;
+        l0->n_medium = medium ? 1u : 0u;
         if (large) A.large_slot[0] = 0;
-        if (A.learned) A.lrank[0] = large ? 0u : 0xffffffffu;
+        if (medium) A.medium_slot[0] = 0;
+        if (A.learned) A.lrank[0] = (large && nt > kChunk) ? 0u : 0xffffffffu;
         A.nx_lo[0] = make_float4(box[0], box[1], box[2], 0.0f);
         A.nx_hi[0] = make_float4(box[4], box[5], box[6], 0.0f);
         A.nx_info[0] = make_uint4(0, nt, 0, 0);
@@ -476,9 +495,7 @@ __global__ void k_root(LevelArgs A, const float *box, uint32_t nt) {
         A.chunks[k] = make_uint2(0, k);
 }
 
-__device__ __forceinline__ bool decidable(const LevelArgs &A, uint32_t cnt) {
-    return cnt > A.leaf_size && A.level < A.max_depth;
-}
+
 
 // level totals of the decisions (what the capacity guard needs), kept per
 // thread and flushed once per CTA
@@ -576,7 +593,7 @@ __device__ void node_features(const LevelArgs &A, uint4 info, float4 blo, float4
 
 // binned mode, recording: (features, label) of a node the exact SAH split
 __device__ void record_node(const LevelArgs &A, uint4 info, float4 blo, float4 bhi, const Decision &d, float *sh) {
-    if (!A.record || d.axis < 0 || info.y <= kSmall) return;
+    if (!A.record || d.axis < 0 || info.y <= kChunk) return;
     uint32_t row = 0;
     if ((threadIdx.x & 31u) == 0) row = atomicAdd(A.rec_rows, 1u);
     row = __shfl_sync(0xffffffffu, row, 0);
@@ -585,27 +602,313 @@ __device__ void record_node(const LevelArgs &A, uint4 info, float4 blo, float4 b
     if ((threadIdx.x & 31u) == 0) A.rec_y[row] = d.axis * 32 + d.bin;
 }
 
+// ---------------------------------------------------------------------------
+// exact SAH (no reference counterpart; the oracle restates it): every clipped
+// reference bound on every axis with a positive extent is a candidate plane p
+// (+0.0f turns a -0 bound into +0), with
+//   below = #(lo < p) + #(flat at p),  above = #(hi > p) + #(flat at p)
+// -- the partition's own classification -- from sorted copies of the lower
+// bounds, upper bounds and flat references' bounds; the lowest cost wins,
+// ties to the lower axis, then the lower plane, as in the oracle's loop.
+// ---------------------------------------------------------------------------
+// sorted ascending across the warp, one value per lane
+__device__ __forceinline__ float warp_sort32(float v) {
+    const uint32_t lane = threadIdx.x & 31u;
+#pragma unroll
+    for (uint32_t k = 2; k <= 32; k <<= 1)
+#pragma unroll
+        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+            const float o = __shfl_xor_sync(0xffffffffu, v, j);
+            const bool keep_min = ((lane & j) == 0) == ((lane & k) == 0);
+            v = keep_min ? (o < v ? o : v) : (o > v ? o : v);
+        }
+    return v;
+}
+
+// #(sorted lane values < p) (LT) or <= p, over the warp's 32 sorted values
+template <bool LE>
+__device__ __forceinline__ uint32_t warp_rank32(float sorted, float p) {
+    uint32_t pos = 0;
+#pragma unroll
+    for (uint32_t step = 16; step; step >>= 1) {
+        const float v = __shfl_sync(0xffffffffu, sorted, (int)(pos + step - 1));
+        if (LE ? v <= p : v < p) pos += step;
+    }
+    // [0, pos) pass; lane pos is untested only when pos == 31
+    const float v = __shfl_sync(0xffffffffu, sorted, (int)pos);
+    if (LE ? v <= p : v < p) pos += 1;
+    return pos;
+}
+
+// a node of at most 32 references, one warp, registers only
+__device__ Decision sah_exact_warp32(const LevelArgs &A, uint4 info, float4 blo, float4 bhi, float ct, float ci) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t cnt = info.y;
+    const bool have = lane < cnt;
+    float4 tlo = make_float4(0, 0, 0, 0), thi = tlo;
+    if (have) {
+        const uint32_t tri = A.refs[info.x + lane];
+        tlo = A.tb_lo[tri];
+        thi = A.tb_hi[tri];
+    }
+    const float Anode = surf(blo, bhi);
+    float mc = kInf, m_pk = 0.0f;
+    uint32_t m_ax = 3, m_nb = 0, m_na = 0;
+#pragma unroll 1
+    for (uint32_t a = 0; a < 3; a++) {
+        const float l = c3(blo, a), h = c3(bhi, a);
+        if (!(__fsub_rn(h, l) > 0.0f)) continue;
+        const float lo = have ? mxf(c3(tlo, a), l) : kInf, hi = have ? mnf(c3(thi, a), h) : kInf;
+        const float slo = warp_sort32(lo), shi = warp_sort32(hi);
+        // references flat on this axis (often none: then no sort, no search)
+        const bool any_flat = __ballot_sync(0xffffffffu, have && lo == hi) != 0u;
+        const float sfl = any_flat ? warp_sort32(lo == hi ? lo : kInf) : kInf;
+#pragma unroll
+        for (int side = 0; side < 2; side++) {
+            const float pk = __fadd_rn(side ? hi : lo, 0.0f);
+            const uint32_t fon = any_flat ? warp_rank32<true>(sfl, pk) - warp_rank32<false>(sfl, pk) : 0u;
+            const uint32_t nb = warp_rank32<false>(slo, pk) + fon;
+            const uint32_t na = (cnt - warp_rank32<true>(shi, pk)) + fon;
+            if (!(have && pk > l && pk < h)) continue;
+            float4 bb = bhi, ba = blo;
+            s3(bb, a, pk);
+            s3(ba, a, pk);
+            const float sb = surf(blo, bb), sa = surf(ba, bhi);
+            const float cost = __fadd_rn(
+                ct, __fmul_rn(ci, __fdiv_rn(__fadd_rn(__fmul_rn(sb, (float)nb), __fmul_rn(sa, (float)na)), Anode)));
+            if (cost < mc || (cost == mc && a == m_ax && pk < m_pk)) {
+                mc = cost;
+                m_ax = a;
+                m_pk = pk;
+                m_nb = nb;
+                m_na = na;
+            }
+        }
+    }
+    float bc = mc, bp = m_pk;
+    uint32_t bax = m_ax, blane = lane;
+    for (int off = 16; off; off >>= 1) {
+        const float oc = __shfl_xor_sync(0xffffffffu, bc, off), op = __shfl_xor_sync(0xffffffffu, bp, off);
+        const uint32_t oax = __shfl_xor_sync(0xffffffffu, bax, off), ol = __shfl_xor_sync(0xffffffffu, blane, off);
+        if (oc < bc || (oc == bc && (oax < bax || (oax == bax && (op < bp || (op == bp && ol < blane)))))) {
+            bc = oc;
+            bp = op;
+            bax = oax;
+            blane = ol;
+        }
+    }
+    Decision best{-1, 0.0f, 0, 0, kInf, 0};
+    const uint32_t nb = __shfl_sync(0xffffffffu, m_nb, blane), na = __shfl_sync(0xffffffffu, m_na, blane);
+    if (bc < kInf) {
+        best.axis = (int)bax;
+        best.plane = bp;
+        best.nb = nb;
+        best.na = na;
+        best.cost = bc;
+    }
+    if (best.axis >= 0 && !(best.cost < __fmul_rn(ci, (float)cnt))) best.axis = -1;
+    return best;
+}
+
+// first index in sorted v[0, n) with v[i] >= p (lower) or v[i] > p (upper)
+__device__ __forceinline__ uint32_t lower_bound_f(const float *v, uint32_t n, float p) {
+    uint32_t lo = 0, hi = n;
+    while (lo < hi) {
+        const uint32_t m = (lo + hi) >> 1;
+        if (v[m] < p) lo = m + 1;
+        else hi = m;
+    }
+    return lo;
+}
+__device__ __forceinline__ uint32_t upper_bound_f(const float *v, uint32_t n, float p) {
+    uint32_t lo = 0, hi = n;
+    while (lo < hi) {
+        const uint32_t m = (lo + hi) >> 1;
+        if (v[m] <= p) lo = m + 1;
+        else hi = m;
+    }
+    return lo;
+}
+
+// Exact SAH of a medium node (33..1024 references), one CTA: the same
+// algorithm with the three sorts (bitonic, shared memory) and the candidates
+// spread over the CTA, then a CTA argmin over (cost, axis, plane).
+struct ExactCtaSmem {
+    float lo[kChunk], hi[kChunk], fl[kChunk];
+    uint32_t nflat;
+    float w_cost[8], w_pk[8];
+    uint32_t w_ax[8], w_nb[8], w_na[8], w_key[8];
+};
+
+__device__ Decision sah_exact_cta(const LevelArgs &A, uint4 info, float4 blo, float4 bhi, float ct, float ci,
+                                  ExactCtaSmem &S) {
+    const uint32_t tid = threadIdx.x, lane = tid & 31u, wid = tid >> 5;
+    const uint32_t cnt = info.y;
+    uint32_t n2 = 1;
+    while (n2 < cnt) n2 <<= 1;
+    const float Anode = surf(blo, bhi);
+    float mc = kInf, m_pk = 0.0f;
+    uint32_t m_ax = 3, m_nb = 0, m_na = 0;
+    for (uint32_t a = 0; a < 3; a++) {
+        const float l = c3(blo, a), h = c3(bhi, a);
+        if (!(__fsub_rn(h, l) > 0.0f)) continue;
+        if (tid == 0) S.nflat = 0;
+        __syncthreads();
+        for (uint32_t i = tid; i < n2; i += blockDim.x) {
+            float lo = kInf, hi = kInf;
+            if (i < cnt) {
+                const uint32_t tri = A.refs[info.x + i];
+                lo = mxf(c3(A.tb_lo[tri], a), l);
+                hi = mnf(c3(A.tb_hi[tri], a), h);
+                if (lo == hi) S.fl[atomicAdd(&S.nflat, 1u)] = lo;   // flat references, any order
+            }
+            S.lo[i] = lo;
+            S.hi[i] = hi;
+        }
+        __syncthreads();
+        const uint32_t nfl = S.nflat;
+        uint32_t nf2 = nfl ? 1u : 0u;
+        while (nf2 < nfl) nf2 <<= 1;
+        for (uint32_t i = nfl + tid; i < nf2; i += blockDim.x) S.fl[i] = kInf;
+        __syncthreads();
+        for (uint32_t k = 2; k <= n2; k <<= 1)
+            for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+                for (uint32_t i = tid; i < n2; i += blockDim.x) {
+                    const uint32_t ixj = i ^ j;
+                    if (ixj > i) {
+                        const bool up = (i & k) == 0;
+                        float x = S.lo[i], y = S.lo[ixj];
+                        if ((x > y) == up) {
+                            S.lo[i] = y;
+                            S.lo[ixj] = x;
+                        }
+                        x = S.hi[i];
+                        y = S.hi[ixj];
+                        if ((x > y) == up) {
+                            S.hi[i] = y;
+                            S.hi[ixj] = x;
+                        }
+                        if (i < nf2 && ixj < nf2 && k <= nf2) {
+                            x = S.fl[i];
+                            y = S.fl[ixj];
+                            if ((x > y) == up) {
+                                S.fl[i] = y;
+                                S.fl[ixj] = x;
+                            }
+                        }
+                    }
+                }
+                __syncthreads();
+            }
+        for (uint32_t q = tid; q < 2 * cnt; q += blockDim.x) {
+            const float pk = __fadd_rn(q < cnt ? S.lo[q] : S.hi[q - cnt], 0.0f);
+            if (!(pk > l && pk < h)) continue;
+            const uint32_t fon = nfl ? upper_bound_f(S.fl, nfl, pk) - lower_bound_f(S.fl, nfl, pk) : 0u;
+            const uint32_t nb = lower_bound_f(S.lo, cnt, pk) + fon;
+            const uint32_t na = (cnt - upper_bound_f(S.hi, cnt, pk)) + fon;
+            float4 bb = bhi, ba = blo;
+            s3(bb, a, pk);
+            s3(ba, a, pk);
+            const float sb = surf(blo, bb), sa = surf(ba, bhi);
+            const float cost = __fadd_rn(
+                ct, __fmul_rn(ci, __fdiv_rn(__fadd_rn(__fmul_rn(sb, (float)nb), __fmul_rn(sa, (float)na)), Anode)));
+            if (cost < mc || (cost == mc && a == m_ax && pk < m_pk)) {
+                mc = cost;
+                m_ax = a;
+                m_pk = pk;
+                m_nb = nb;
+                m_na = na;
+            }
+        }
+        __syncthreads();
+    }
+    // argmin over (cost, axis, plane): warps, then warp 0 over the warps
+    float bc = mc, bp = m_pk;
+    uint32_t bax = m_ax, bkey = tid;
+    for (int off = 16; off; off >>= 1) {
+        const float oc = __shfl_xor_sync(0xffffffffu, bc, off), op = __shfl_xor_sync(0xffffffffu, bp, off);
+        const uint32_t oax = __shfl_xor_sync(0xffffffffu, bax, off), ok = __shfl_xor_sync(0xffffffffu, bkey, off);
+        if (oc < bc || (oc == bc && (oax < bax || (oax == bax && (op < bp || (op == bp && ok < bkey)))))) {
+            bc = oc;
+            bp = op;
+            bax = oax;
+            bkey = ok;
+        }
+    }
+    if (lane == 0) {
+        S.w_cost[wid] = bc;
+        S.w_pk[wid] = bp;
+        S.w_ax[wid] = bax;
+        S.w_key[wid] = bkey;
+    }
+    // the winning thread of each warp publishes its counts
+    if (tid == bkey) {
+        S.w_nb[wid] = m_nb;
+        S.w_na[wid] = m_na;
+    }
+    __syncthreads();
+    const uint32_t nw = blockDim.x >> 5;
+    float fc = S.w_cost[0], fp = S.w_pk[0];
+    uint32_t fax = S.w_ax[0], fw = 0;
+    for (uint32_t w = 1; w < nw; w++) {
+        const float oc = S.w_cost[w], op = S.w_pk[w];
+        const uint32_t oax = S.w_ax[w];
+        if (oc < fc || (oc == fc && (oax < fax || (oax == fax && op < fp)))) {
+            fc = oc;
+            fp = op;
+            fax = oax;
+            fw = w;
+        }
+    }
+    Decision best{-1, 0.0f, 0, 0, kInf, 0};
+    if (fc < kInf) {
+        best.axis = (int)fax;
+        best.plane = fp;
+        best.nb = S.w_nb[fw];
+        best.na = S.w_na[fw];
+        best.cost = fc;
+        best.bin = 0;
+    }
+    if (best.axis >= 0 && !(best.cost < __fmul_rn(ci, (float)cnt))) best.axis = -1;
+    __syncthreads();
+    return best;
+}
+
 // Large nodes, binned mode: one CTA per chunk of 1024 references builds the
 // chunk's histograms in shared memory and adds them to the node's global
 // histogram; the CTA that finishes the node's last chunk evaluates the SAH.
-__global__ void __launch_bounds__(256) k_hist(LevelArgs A) {
+__global__ void __launch_bounds__(256, 3) k_hist(LevelArgs A) {
     __shared__ uint32_t H[kHist];
     __shared__ float feat_scratch[200];
+    __shared__ ExactCtaSmem XS;
     __shared__ int s_last;
     __shared__ uint32_t s_tally[5];
     Tally tally;
     const uint32_t wib = threadIdx.x >> 5, lane = threadIdx.x & 31u;
     const uint32_t nch = min(A.lc->n_chunks, A.cap_chunks);
+    const uint32_t nmed = min(A.lc->n_medium, A.cap_medium);
     const uint32_t nodes = A.lc->nodes;
-    for (uint32_t item = blockIdx.x; item < nch; item += gridDim.x) {
+    for (uint32_t item = blockIdx.x; item < nch + nmed; item += gridDim.x) {
+        if (item >= nch) {
+            // a medium node: the exact SAH in this CTA
+            const uint32_t s = A.medium_slot[item - nch];
+            if (s >= nodes) continue;
+            const uint4 info = A.n_info[s];
+            const Decision d = sah_exact_cta(A, info, A.n_lo[s], A.n_hi[s], A.ct, A.ci, XS);
+            if (threadIdx.x == 0) {
+                write_decision(A, s, d);
+                tally.add(d, info.y);
+            }
+            continue;
+        }
         const uint2 ck = A.chunks[item];
         const uint32_t rank = ck.x;
         if (rank >= A.cap_large) continue;  // uniform per CTA
         const uint32_t s = A.large_slot[rank];
         if (s >= nodes) continue;
         const uint4 info = A.n_info[s];
-        const uint32_t r0 = info.x + ck.y * kChunk, r1 = min(info.x + info.y, r0 + kChunk);
         const float4 blo = A.n_lo[s], bhi = A.n_hi[s];
+        const uint32_t r0 = info.x + ck.y * kChunk, r1 = min(info.x + info.y, r0 + kChunk);
         for (uint32_t i = threadIdx.x; i < kHist; i += blockDim.x) H[i] = 0;
         __syncthreads();
         {
@@ -658,10 +961,11 @@ __global__ void __launch_bounds__(256) k_hist(LevelArgs A) {
     tally_flush(A, tally, s_tally);
 }
 
-// Small nodes (<= 256 references, or not splittable): one warp per node,
-// warp-private histogram + SAH. Learned mode: the warp of a large node
-// computes the proposer's features instead.
-__global__ void __launch_bounds__(256, 6) k_small(LevelArgs A) {
+// Small nodes (not splittable, or splittable and neither medium nor large):
+// one warp per node; the exact SAH in registers for nodes of at most 32
+// references when exact_max >= 32, else a warp-private histogram + the binned
+// SAH. Learned mode: the warp of a proposer row computes its features.
+__global__ void __launch_bounds__(256, 5) k_small(LevelArgs A) {
     __shared__ uint32_t HS[8][kHist];
     __shared__ uint32_t s_tally[5];
     Tally tally;
@@ -674,14 +978,14 @@ __global__ void __launch_bounds__(256, 6) k_small(LevelArgs A) {
         const uint4 info = A.n_info[s];
         const uint32_t cnt = info.y;
         const bool dec = decidable(A, cnt);
-        if (dec && cnt > kSmall) {
+        if (dec && (is_large(A, cnt) || is_medium(A, cnt))) {
             if (A.learned) {
                 const uint32_t row = A.lrank[s];
                 if (row < A.cap_large)
                     node_features(A, info, A.n_lo[s], A.n_hi[s], reinterpret_cast<float *>(HS[wib]),
                                   A.feat + (size_t)row * 200);
             }
-            continue;  // binned mode: k_hist
+            continue;  // k_hist / k_propose
         }
         if (!dec) {
             if (lane == 0) {
@@ -691,17 +995,22 @@ __global__ void __launch_bounds__(256, 6) k_small(LevelArgs A) {
             }
             continue;
         }
-        uint32_t *Hw = HS[wib];
-        for (uint32_t i = lane; i < kHist; i += 32) Hw[i] = 0;
-        __syncwarp();
         const float4 blo = A.n_lo[s], bhi = A.n_hi[s];
-        const float4 inv3 = bin_scale(blo, bhi);
-        for (uint32_t r = info.x + lane; r < info.x + cnt; r += 32) {
-            const uint32_t tri = A.refs[r];
-            hist_ref(Hw, A.tb_lo[tri], A.tb_hi[tri], blo, bhi, inv3);
+        Decision d;
+        if (A.exact_max >= kWarpExact && cnt <= kWarpExact) {
+            d = sah_exact_warp32(A, info, blo, bhi, A.ct, A.ci);
+        } else {
+            uint32_t *Hw = HS[wib];
+            for (uint32_t i = lane; i < kHist; i += 32) Hw[i] = 0;
+            __syncwarp();
+            const float4 inv3 = bin_scale(blo, bhi);
+            for (uint32_t r = info.x + lane; r < info.x + cnt; r += 32) {
+                const uint32_t tri = A.refs[r];
+                hist_ref(Hw, A.tb_lo[tri], A.tb_hi[tri], blo, bhi, inv3);
+            }
+            __syncwarp();
+            d = sah_warp(Hw, blo, bhi, cnt, A.ct, A.ci);
         }
-        __syncwarp();
-        const Decision d = sah_warp(Hw, blo, bhi, cnt, A.ct, A.ci);
         if (lane == 0) {
             write_decision(A, s, d);
             tally.add(d, cnt);
@@ -795,16 +1104,30 @@ __device__ void select_candidates(const LevelArgs &A, const float *__restrict__ 
     __syncwarp();
 }
 
-__global__ void __launch_bounds__(256) k_propose(LevelArgs A) {
+__global__ void __launch_bounds__(256, 3) k_propose(LevelArgs A) {
     __shared__ uint32_t H[kHist];
+    __shared__ ExactCtaSmem XS;
     __shared__ Candidates C;
     __shared__ uint32_t s_cnt[2 * kMaxCand];
     __shared__ int s_last, s_fallback;
     __shared__ uint32_t s_tally[5];
     Tally tally;
     const uint32_t nch = min(A.lc->n_chunks, A.cap_chunks);
+    const uint32_t nmed = min(A.lc->n_medium, A.cap_medium);
     const uint32_t nodes = A.lc->nodes;
-    for (uint32_t item = blockIdx.x; item < nch; item += gridDim.x) {
+    for (uint32_t item = blockIdx.x; item < nch + nmed; item += gridDim.x) {
+        if (item >= nch) {
+            // a medium node: the exact SAH, as in the binned build
+            const uint32_t s = A.medium_slot[item - nch];
+            if (s >= nodes) continue;
+            const uint4 info = A.n_info[s];
+            const Decision d = sah_exact_cta(A, info, A.n_lo[s], A.n_hi[s], A.ct, A.ci, XS);
+            if (threadIdx.x == 0) {
+                write_decision(A, s, d);
+                tally.add(d, info.y);
+            }
+            continue;
+        }
         const uint2 ck = A.chunks[item];
         const uint32_t rank = ck.x;
         if (rank >= A.cap_large) continue;  // uniform per CTA
@@ -812,6 +1135,26 @@ __global__ void __launch_bounds__(256) k_propose(LevelArgs A) {
         if (s >= nodes) continue;
         const uint4 info = A.n_info[s];
         const float4 blo = A.n_lo[s], bhi = A.n_hi[s];
+        if (info.y <= kChunk) {
+            // a one-chunk large node (no proposer row): the full binned SAH
+            for (uint32_t i = threadIdx.x; i < kHist; i += blockDim.x) H[i] = 0;
+            __syncthreads();
+            const float4 inv3 = bin_scale(blo, bhi);
+            for (uint32_t r = info.x + threadIdx.x; r < info.x + info.y; r += blockDim.x) {
+                const uint32_t tri = A.refs[r];
+                hist_ref(H, A.tb_lo[tri], A.tb_hi[tri], blo, bhi, inv3);
+            }
+            __syncthreads();
+            if (threadIdx.x < 32) {
+                const Decision d = sah_warp(H, blo, bhi, info.y, A.ct, A.ci);
+                if (threadIdx.x == 0) {
+                    write_decision(A, s, d);
+                    tally.add(d, info.y);
+                }
+            }
+            __syncthreads();
+            continue;
+        }
         if (threadIdx.x < 32) select_candidates(A, A.logits + (size_t)rank * kMlpOut, blo, bhi, C);
         if (threadIdx.x < 2 * kMaxCand) s_cnt[threadIdx.x] = 0;
         __syncthreads();
@@ -959,9 +1302,15 @@ __device__ __forceinline__ bool level_over(const LevelArgs &A) {
 // a child of count c in next-level slot ns: large nodes take a rank and
 // their chunks (few per level, so plain atomics)
 __device__ void child_setup(const LevelArgs &A, uint32_t ns, uint32_t c) {
-    const bool large = c > kSmall && c > A.leaf_size && A.level + 1 < A.max_depth;
+    const bool dec = c > A.leaf_size && A.level + 1 < A.max_depth;
     if (A.learned) A.lrank[ns] = 0xffffffffu;
-    if (!large) return;
+    if (dec && is_medium(A, c)) {
+        const uint32_t m = atomicAdd(&A.nlc->n_medium, 1u);
+        if (m < A.cap_medium) A.medium_slot[m] = ns;
+        else atomicOr(A.err, 2u);
+        return;
+    }
+    if (!(dec && is_large(A, c))) return;
     const uint32_t nch = (c + kChunk - 1) / kChunk;
     const uint32_t rank = atomicAdd(&A.nlc->n_large, 1u);
     const uint32_t first = atomicAdd(&A.nlc->n_chunks, nch);
@@ -970,7 +1319,7 @@ __device__ void child_setup(const LevelArgs &A, uint32_t ns, uint32_t c) {
         return;
     }
     A.large_slot[rank] = ns;
-    if (A.learned) A.lrank[ns] = rank;
+    if (A.learned && c > kChunk) A.lrank[ns] = rank;   // a proposer row (medium nodes: exact SAH)
     for (uint32_t k = 0; k < nch; k++) A.chunks[first + k] = make_uint2(rank, k);
 }
 
@@ -1022,7 +1371,7 @@ struct PlanOp {
         const int ax = cx.stop ? -1 : it.axis;
         A.plan[s] = make_uint4(pl.x, pl.z, pl.w, pl.v);
         if (info.z >= A.cap_nodes) {
-            atomicOr(A.err, 2u);
+            atomicOr(A.err, 16u);
             return;
         }
         if (ax < 0) {
@@ -1036,7 +1385,7 @@ struct PlanOp {
         // decisions; these checks only keep an inconsistent level in bounds
         if ((uint64_t)pair + 1 >= A.cap_nodes ||
             (uint64_t)pl.z + (ct.x ? 1u : 0u) + (ct.y ? 1u : 0u) > A.cap_level) {
-            atomicOr(A.err, 2u);
+            atomicOr(A.err, 16u);
             return;
         }
         const float p = A.plane[s];
@@ -1149,7 +1498,7 @@ struct RefOp {
                 A.nx_refs[pos] = it.tri;
                 A.nx_ref_node[pos] = pl.y;
             } else {
-                atomicOr(A.err, 2u);
+                atomicOr(A.err, 8u);   // the partition disagrees with the decision's counts
             }
         }
         if (it.f.y) {
@@ -1159,7 +1508,7 @@ struct RefOp {
                 A.nx_refs[pos] = it.tri;
                 A.nx_ref_node[pos] = pl.y + (ct.x ? 1u : 0u);
             } else {
-                atomicOr(A.err, 2u);
+                atomicOr(A.err, 8u);
             }
         }
     }
@@ -1185,7 +1534,7 @@ void build_release(BuildState &S) {
         f(S.n_lo[k]); f(S.n_hi[k]); f(S.n_info[k]); f(S.refs[k]); f(S.ref_node[k]);
     }
     f(S.d_axis); f(S.d_plane); f(S.d_cnt); f(S.plan);
-    f(S.chunks); f(S.hist); f(S.done); f(S.lrank); f(S.feat); f(S.logits);
+    f(S.chunks); f(S.hist); f(S.done); f(S.medium_slot); f(S.lrank); f(S.feat); f(S.logits);
     f(S.plan_flags); f(S.ref_flags); f(S.plan_agg); f(S.plan_incl); f(S.ref_agg); f(S.ref_incl); f(S.epoch);
     f(S.ctr); f(S.err);
     f(S.out_nodes); f(S.out_refs); f(S.out_ropes); f(S.out_cbox);
@@ -1215,6 +1564,7 @@ hk_status build_prepare(BuildState &S, const BuildParams &p, uint32_t nt, int sm
     S.cap_level = std::min(cap_refs, cap_nodes) + 1;
     S.cap_large = cap_refs / kSmall + 2;
     S.cap_chunks = cap_refs / kChunk + S.cap_large + 2;
+    S.cap_medium = cap_refs / (kWarpExact + 1) + 2;
     S.plan_tiles = S.cap_level / kScanThreads + 2;   // one node per thread
     S.ref_tiles = cap_refs / kTile + 2;
     bool bad = false;
@@ -1234,6 +1584,7 @@ hk_status build_prepare(BuildState &S, const BuildParams &p, uint32_t nt, int sm
     bad |= dalloc(S.chunks, S.cap_chunks + S.cap_large) != cudaSuccess;  // tail holds large_slot
     bad |= dalloc(S.hist, (size_t)S.cap_large * kHist) != cudaSuccess;
     bad |= dalloc(S.done, S.cap_large) != cudaSuccess;
+    bad |= dalloc(S.medium_slot, S.cap_medium) != cudaSuccess;
     bad |= dalloc(S.lrank, S.cap_level) != cudaSuccess;
     bad |= dalloc(S.feat, (size_t)S.cap_large * 200) != cudaSuccess;
     bad |= dalloc(S.logits, (size_t)S.cap_large * kMlpOut) != cudaSuccess;
@@ -1310,6 +1661,9 @@ cudaError_t build_launch(BuildState &S, const float4 *verts, const uint4 *tris, 
     A.cap_level = S.cap_level;
     A.cap_large = S.cap_large;
     A.cap_chunks = S.cap_chunks;
+    A.cap_medium = S.cap_medium;
+    A.medium_slot = S.medium_slot;
+    A.exact_max = S.p.exact_max;
     A.learned = (S.p.mode == HK_BUILD_LEARNED) ? 1 : 0;
     A.record = (S.p.mode == HK_BUILD_BINNED && S.p.record && S.learn && S.learn->rec_X) ? 1 : 0;
     A.lrank = S.lrank;
@@ -1387,6 +1741,7 @@ hk_status build_read_stats(BuildState &S, cudaStream_t st, hk_tree_stats *out) {
     if (cudaMemcpyAsync(&c, S.ctr, sizeof(c), cudaMemcpyDeviceToHost, st) != cudaSuccess) return HK_E_CUDA;
     if (cudaMemcpyAsync(&err, S.err, 4, cudaMemcpyDeviceToHost, st) != cudaSuccess) return HK_E_CUDA;
     if (cudaStreamSynchronize(st) != cudaSuccess) return HK_E_CUDA;
+    S.last_err = err;
     if (err) {
         cudaMemsetAsync(S.err, 0, 4, st);
         return HK_E_CAPACITY;

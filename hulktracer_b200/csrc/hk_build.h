@@ -19,6 +19,7 @@ struct BuildParams {
     uint32_t topk = 4;
     float fallback_ratio = 1.02f;
     int record = 0;             // binned mode: append (features, label) rows
+    uint32_t exact_max = 0;     // nodes with at most this many refs (0, or 32..1024) take the exact SAH
 };
 
 // learned-proposer buffers owned by the context (device pointers)
@@ -44,6 +45,7 @@ struct LevelCounters {
     uint32_t stop;              // the level stops splitting (capacity)
     uint32_t n_large;           // large nodes (chunked histograms)
     uint32_t n_chunks;          // histogram chunks
+    uint32_t n_medium;          // exact-SAH nodes of 33..exact_max refs (one CTA each)
     // tallies of the level's decisions (the capacity guard's inputs)
     uint32_t t_leafrefs, t_leafnodes, t_splits, t_next, t_childrefs;
     // tile tickets of the single-pass scans
@@ -68,10 +70,12 @@ struct BuildOutputs {
 
 struct BuildState {
     BuildParams p{};
-    uint32_t nt = 0, cap_refs = 0, cap_nodes = 0, cap_level = 0, cap_large = 0, cap_chunks = 0;
+    uint32_t nt = 0, cap_refs = 0, cap_nodes = 0, cap_level = 0, cap_large = 0, cap_chunks = 0, cap_medium = 0;
     int sm_count = 148;
     bool active = false;        // a built tree is the current tree
     uint32_t last_level = 0;    // lvl[] index holding the final totals
+    uint32_t last_err = 0;      // error bits of the last build: 2 arena capacity, 4 scan wait ran
+                                // out, 8 partition / decision count mismatch, 16 plan bounds
     // per-triangle bounds
     float4 *tb_lo = nullptr, *tb_hi = nullptr;
     // level nodes (ping-pong)
@@ -85,6 +89,7 @@ struct BuildState {
     uint2 *chunks = nullptr;                     // (large rank, chunk index); tail: large_slot
     uint32_t *hist = nullptr;                    // per large node 3 x 96
     uint32_t *done = nullptr;                    // per large node: chunks finished
+    uint32_t *medium_slot = nullptr;             // exact-SAH medium nodes of the level
     // references (ping-pong)
     uint32_t *refs[2] = {nullptr, nullptr};
     uint32_t *ref_node[2] = {nullptr, nullptr};

@@ -32,10 +32,11 @@ def main():
     ap.add_argument("--mode", default="binned", choices=["binned", "learned"])
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--weights", default=os.path.join(ROOT, "hulktracer_b200", "weights", "proposer.bin"))
+    ap.add_argument("--exact-max", type=int, default=0, help="exact SAH on nodes of at most this many refs")
     a = ap.parse_args()
     sc = scenes.animated_parts()
     W, H = sc.width, sc.height
-    ctx = hk.Context()
+    ctx = hk.Context(exact_max=a.exact_max)
     if a.mode == "learned":
         ctx.mlp_load(a.weights)
     ctx.upload(sc.verts, sc.tris)

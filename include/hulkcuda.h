@@ -99,6 +99,10 @@ typedef struct hk_config {
     float fallback_ratio;     /* learned builder: fall back to the full binned SAH
                                  when the best proposal costs more than ratio x the
                                  exactly costed reference plane (1.02; 0 = always) */
+    uint32_t exact_max;       /* builder: nodes with at most this many references take
+                                 the exact SAH over their references' bounds (the
+                                 reference's candidate set) instead of 32 bins; 0 =
+                                 binned everywhere (default), else 32..1024 */
 } hk_config;
 
 typedef struct hk_tree_stats {

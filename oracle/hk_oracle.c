@@ -1162,6 +1162,9 @@ static int search_ropes(const hko_tree *t, const float *o, const float *d, float
 /* (no reference counterpart; the reference builds with the exact event      */
 /* sweep above). Breadth-first, level by level:                              */
 /*  - a node is a leaf when refs <= leaf_size or depth >= max_depth;         */
+/*  - a node with at most exact_max refs costs every clipped bound of its     */
+/*    refs on every axis with a positive extent (the exact SAH candidates),   */
+/*    ties going to the lower axis, then the lower plane;                     */
 /*  - otherwise every axis with a positive extent gets bins planes            */
 /*    p_k = min + ext*(k/bins), k = 1..bins-1, and exact counts of the refs   */
 /*    below / above each plane from two histograms of the refs' clipped       */
@@ -1232,6 +1235,41 @@ int hko_build_binned(const float *verts, const uint32_t *tris, uint32_t nt, cons
             float A = surf(n->box);
             float best = INFINITY;
             uint32_t bnb = 0, bna = 0;
+            if (n->count <= p->exact_max) {
+                /* small node: every clipped reference bound is a candidate
+                 * (+0.0f makes a -0 bound the plane +0) */
+                for (uint32_t a = 0; a < 3; a++) {
+                    float lo_b = n->box[a], hi_b = n->box[4 + a];
+                    if (!(hi_b - lo_b > 0)) continue;
+                    for (uint32_t q = 0; q < 2 * n->count; q++) {
+                        const float *tq = tb + 6 * (size_t)refs[n->start + q / 2];
+                        float pk = ((q & 1) ? mn(tq[3 + a], hi_b) : mx(tq[a], lo_b)) + 0.0f;
+                        if (!(pk > lo_b && pk < hi_b)) continue;
+                        uint32_t nb = 0, na = 0;
+                        for (uint32_t r = 0; r < n->count; r++) {
+                            const float *t6 = tb + 6 * (size_t)refs[n->start + r];
+                            float lo = mx(t6[a], lo_b), hi = mn(t6[3 + a], hi_b);
+                            int on = lo == hi && lo == pk;
+                            nb += (lo < pk || on) ? 1u : 0u;
+                            na += (hi > pk || on) ? 1u : 0u;
+                        }
+                        float bb[8], ba[8];
+                        memcpy(bb, n->box, 32);
+                        memcpy(ba, n->box, 32);
+                        bb[4 + a] = pk;
+                        ba[a] = pk;
+                        float cost = p->ct + p->ci * ((surf(bb) * (float)nb + surf(ba) * (float)na) / A);
+                        /* first minimum in (axis, plane) order */
+                        if (cost < best || (cost == best && (int32_t)a == axis[s] && pk < plane[s])) {
+                            best = cost;
+                            axis[s] = (int32_t)a;
+                            plane[s] = pk;
+                            bnb = nb;
+                            bna = na;
+                        }
+                    }
+                }
+            } else
             for (uint32_t a = 0; a < 3; a++) {
                 float lo_b = n->box[a], hi_b = n->box[4 + a];
                 float ext = hi_b - lo_b;

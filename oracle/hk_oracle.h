@@ -145,6 +145,7 @@ typedef struct {
     uint32_t bins;          /* 32 */
     uint32_t max_refs;      /* capacity of the reference arena (and of the leaf list) */
     uint32_t max_nodes;     /* capacity of the compact node array */
+    uint32_t exact_max;     /* nodes with at most this many refs cost the event planes */
 } hko_binned_params;
 int hko_build_binned(const float *verts, const uint32_t *tris, uint32_t nt, const float *box,
                      const hko_binned_params *p, uint32_t **nodes_out, uint32_t *nn_out,

@@ -42,7 +42,7 @@ class _SahParams(C.Structure):
 class _BinnedParams(C.Structure):
     _fields_ = [("ct", C.c_float), ("ci", C.c_float), ("max_depth", C.c_uint32),
                 ("leaf_size", C.c_uint32), ("bins", C.c_uint32), ("max_refs", C.c_uint32),
-                ("max_nodes", C.c_uint32)]
+                ("max_nodes", C.c_uint32), ("exact_max", C.c_uint32)]
 
 
 # reference constants (KDTreeCPU.cpp:17-18, SharedStructs.hpp:16, KDTreeSAH.cpp:317,
@@ -174,13 +174,13 @@ class Oracle:
         return self._take(pn, nn.value, pr, nr.value, 4)
 
     def build_binned(self, verts, tris, box, ct=1.0, ci=1.5, max_depth=24, leaf_size=4, bins=32,
-                     max_refs=None, max_nodes=None):
+                     max_refs=None, max_nodes=None, exact_max=0):
         nt = int(np.asarray(tris).shape[0])
         if max_refs is None:
             max_refs = max(16 * nt, 1024)
         if max_nodes is None:
             max_nodes = max(12 * nt, 1024)
-        prm = _BinnedParams(ct, ci, max_depth, leaf_size, bins, max_refs, max_nodes)
+        prm = _BinnedParams(ct, ci, max_depth, leaf_size, bins, max_refs, max_nodes, exact_max)
         pn, pr = C.POINTER(C.c_uint32)(), C.POINTER(C.c_uint32)()
         nn, nr = C.c_uint32(), C.c_uint32()
         tris = _c(tris, np.uint32)

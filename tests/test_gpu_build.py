@@ -26,8 +26,13 @@ def small_animated():
     return scenes.animated_parts(n_parts=6, width=96, height=64)
 
 
+@pytest.mark.parametrize("exact_max", [0, 256, 1024])
 @pytest.mark.parametrize("which", ["soup3k", "small24k", "animated6"])
-def test_build_identical_to_oracle(ctx, oracle, which):
+def test_build_identical_to_oracle(hk, oracle, which, exact_max):
+    """Binned everywhere (exact_max 0), and with the exact SAH on nodes of
+    at most 256 / 1024 references (warp in registers up to 32, one CTA per
+    medium node above): the GPU tree equals the oracle's, array for array."""
+    ctx = hk.Context(exact_max=exact_max)
     if which == "animated6":
         sc = small_animated()
         verts, tris, box = sc.verts, sc.tris, sc.scene_box()
@@ -39,7 +44,7 @@ def test_build_identical_to_oracle(ctx, oracle, which):
     ctx.precompute()
     st = ctx.build()
     cn, cr = ctx.export_compact()
-    on, orf = oracle.build_binned(verts, tris, box, ct=1.0, ci=1.5, max_depth=24, leaf_size=4)
+    on, orf = oracle.build_binned(verts, tris, box, ct=1.0, ci=1.5, max_depth=24, leaf_size=4, exact_max=exact_max)
     assert cn.shape == on.shape
     assert np.array_equal(cn, on)
     assert np.array_equal(cr, orf)

@@ -15,7 +15,7 @@ pytestmark = pytest.mark.gpu
 
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
 WEIGHTS = os.path.join(os.path.dirname(os.path.dirname(__file__)), "hulktracer_b200", "weights", "proposer.bin")
-KSMALL = 256            # nodes with more references than this go to the proposer
+KPROPOSE = 1024         # nodes with more references than this go to the proposer
 CT, CI = 1.0, 1.5
 
 
@@ -84,7 +84,7 @@ def test_params_save_load_roundtrip(ctx, hk, tmp_path):
 
 def oracle_rows(oracle, verts, tris, box, max_depth=24):
     """(features, axis) of every node of the oracle's binned tree that has
-    more than KSMALL references and is split, from its references in
+    more than KPROPOSE references and is split, from its references in
     ascending triangle order (the builder's stable partition keeps that
     order), sampled as the builder samples them."""
     cn, cr = oracle.build_binned(verts, tris, box, ct=CT, ci=CI, max_depth=max_depth, leaf_size=4)
@@ -105,7 +105,7 @@ def oracle_rows(oracle, verts, tris, box, max_depth=24):
         rlo[axis] = plane
         refs = np.union1d(walk(pair, lo, lhi, level + 1), walk(pair + 1, rlo, hi, level + 1))
         cnt = refs.shape[0]
-        if cnt > KSMALL:
+        if cnt > KPROPOSE:
             S = min(cnt, 64)
             pick = refs[(np.arange(S, dtype=np.int64) * cnt) // S]
             rows.append((mlp.features(lo, hi, tlo[pick], thi[pick], level, max_depth), axis))
@@ -135,8 +135,12 @@ def test_recorded_rows_match_oracle(ctx, oracle):
 
 
 def trace_equals_brute(ctx, hk, rays):
+    """Full stack and ropes find every closest hit. (The reference's short
+    stack and kd-restart can lose a hit lying exactly on a split plane of some
+    trees -- on grid seams at x = 0 here -- and the GPU reproduces them bit for
+    bit, tests/test_gpu_trace.py, so they are not compared with brute force.)"""
     b = ctx.trace(rays, hk.BRUTE)
-    for v in (hk.SHORTSTACK, hk.ROPES):
+    for v in (hk.FULLSTACK, hk.ROPES):
         h = ctx.trace(rays, v)
         m = b["tri"] >= 0
         assert np.array_equal(h["tri"] >= 0, m)
