@@ -1,7 +1,9 @@
 // hk_build.cu -- GPU KD-tree builder: exact binned SAH (sm_100a).
 //
 // Breadth-first and level-synchronous; three launches per level (five with
-// the learned proposer):
+// the learned proposer). Splits are searched over 32 bins per axis, or, with
+// exact_max (32..1024), over every clipped reference bound for nodes of at
+// most exact_max references (one warp in registers up to 32, one CTA above):
 //   work      large nodes (> 256 references): one CTA per chunk of 2048
 //             references builds shared-memory histograms (3 axes x {lo bin,
 //             hi bin, flat-on-plane}) of the clipped reference bounds and
@@ -403,6 +405,8 @@ struct LevelArgs {
     float *plane;
     uint2 *cnt;
     uint4 *plan;            // per node: leaf-ref offset, next slot, child-ref offset, below-ref offset
+    float4 *split;          // per node: axis (int bits, -1 = leaf), plane, node min / max on the axis
+    uint4 *scat;            // per node: where its references go (written by the plan scan)
     uint2 *chunks;          // (large rank, chunk index within the node)
     uint32_t *large_slot;
     uint32_t *medium_slot;
@@ -531,6 +535,13 @@ __device__ __forceinline__ void write_decision(const LevelArgs &A, uint32_t s, c
     A.axis[s] = d.axis;
     A.plane[s] = d.plane;
     A.cnt[s] = make_uint2(d.nb, d.na);
+    // the partition's view of the decision in one 16-byte record
+    float l = 0.0f, h = 0.0f;
+    if (d.axis >= 0) {
+        l = c3(A.n_lo[s], (uint32_t)d.axis);
+        h = c3(A.n_hi[s], (uint32_t)d.axis);
+    }
+    A.split[s] = make_float4(__int_as_float(d.axis), d.plane, l, h);
 }
 
 // global histogram read past L1 (other CTAs wrote it with atomics)
@@ -1377,7 +1388,17 @@ struct PlanOp {
         if (ax < 0) {
             const uint32_t off = cx.leafrefs_total + (cx.stop ? info.x : pl.x);
             A.out_nodes[info.z] = make_uint2((off << 2) | kLeafTag, info.y);
+            // reference r of this leaf goes to out_refs[off - start + r]
+            A.scat[s] = make_uint4(off - info.x, 0, 0, 0);
             return;
+        }
+        {
+            // reference r goes below to nx_refs[child refs - below refs before s +
+            // P.x(r)] and above to nx_refs[below refs before s + cnt.x + P.y(r)]
+            // (P: the global prefix of the flags), into next-level slots pl.z and
+            // pl.z + (cnt.x > 0)
+            const uint2 c2 = it.cnt;
+            A.scat[s] = make_uint4(pl.w - pl.v, pl.v + c2.x, pl.z, 1u | (c2.x ? 2u : 0u));
         }
         const uint32_t pair = cx.nodes_total + 2 * pl.y;
         const uint2 ct = it.cnt;
@@ -1471,42 +1492,37 @@ struct RefOp {
         if (r == 0xffffffffu) return Item{make_uint2(0, 0), 0, 0};
         const uint32_t s = A.ref_node[r];
         const uint32_t tri = A.refs[r];
-        const int ax = stop ? -1 : A.axis[s];
+        const float4 sp = A.split[s];
+        const int ax = stop ? -1 : __float_as_int(sp.x);
         if (ax < 0) return Item{make_uint2(0, 0), s, tri};
-        const float l = c3(A.n_lo[s], ax), h = c3(A.n_hi[s], ax), p = A.plane[s];
+        const float p = sp.y, l = sp.z, h = sp.w;
         const float lo = mxf(c3(A.tb_lo[tri], ax), l), hi = mnf(c3(A.tb_hi[tri], ax), h);
         const bool flat_on = (lo == hi) && lo == p;
         return Item{make_uint2((lo < p || flat_on) ? 1u : 0u, (hi > p || flat_on) ? 1u : 0u), s, tri};
     }
     __device__ T value(const Item &it) const { return it.f; }
-    __device__ void apply(uint32_t r, uint2 P, const Item &it, const Ctx &stop) const {
-        const LevelCounters *l = A.lc;
-        const uint32_t s = it.s;
-        const uint4 info = A.n_info[s];
-        const int ax = stop ? -1 : A.axis[s];
-        if (ax < 0) {
-            const uint32_t off = l->leafrefs_total + (stop ? info.x : A.plan[s].x) + (r - info.x);
+    __device__ void apply(uint32_t r, uint2 P, const Item &it, const Ctx &) const {
+        const uint4 sc = A.scat[it.s];
+        if (!(sc.w & 1u)) {
+            const uint32_t off = sc.x + r;   // leaf
             if (off < A.cap_refs) A.out_refs[off] = it.tri;
             else atomicOr(A.err, 2u);
             return;
         }
-        const uint4 pl = A.plan[s];   // y: next slot, z: child-ref offset, w: below refs before s
-        const uint2 ct = A.cnt[s];
         if (it.f.x) {
-            const uint32_t pos = pl.z + (P.x - pl.w);
-            if (pos < A.cap_refs && pos < pl.z + ct.x) {
+            const uint32_t pos = sc.x + P.x;
+            if (pos < A.cap_refs) {
                 A.nx_refs[pos] = it.tri;
-                A.nx_ref_node[pos] = pl.y;
+                A.nx_ref_node[pos] = sc.z;
             } else {
-                atomicOr(A.err, 8u);   // the partition disagrees with the decision's counts
+                atomicOr(A.err, 8u);
             }
         }
         if (it.f.y) {
-            const uint32_t above_before = pl.z - pl.w;
-            const uint32_t pos = pl.z + ct.x + (P.y - above_before);
-            if (pos < A.cap_refs && pos < pl.z + ct.x + ct.y) {
+            const uint32_t pos = sc.y + P.y;
+            if (pos < A.cap_refs) {
                 A.nx_refs[pos] = it.tri;
-                A.nx_ref_node[pos] = pl.y + (ct.x ? 1u : 0u);
+                A.nx_ref_node[pos] = sc.z + ((sc.w & 2u) ? 1u : 0u);
             } else {
                 atomicOr(A.err, 8u);
             }
@@ -1533,7 +1549,7 @@ void build_release(BuildState &S) {
     for (int k = 0; k < 2; k++) {
         f(S.n_lo[k]); f(S.n_hi[k]); f(S.n_info[k]); f(S.refs[k]); f(S.ref_node[k]);
     }
-    f(S.d_axis); f(S.d_plane); f(S.d_cnt); f(S.plan);
+    f(S.d_axis); f(S.d_plane); f(S.d_cnt); f(S.plan); f(S.d_split); f(S.d_scat);
     f(S.chunks); f(S.hist); f(S.done); f(S.medium_slot); f(S.lrank); f(S.feat); f(S.logits);
     f(S.plan_flags); f(S.ref_flags); f(S.plan_agg); f(S.plan_incl); f(S.ref_agg); f(S.ref_incl); f(S.epoch);
     f(S.ctr); f(S.err);
@@ -1580,6 +1596,8 @@ hk_status build_prepare(BuildState &S, const BuildParams &p, uint32_t nt, int sm
     bad |= dalloc(S.d_axis, S.cap_level) != cudaSuccess;
     bad |= dalloc(S.d_plane, S.cap_level) != cudaSuccess;
     bad |= dalloc(S.d_cnt, S.cap_level) != cudaSuccess;
+    bad |= dalloc(S.d_split, S.cap_level) != cudaSuccess;
+    bad |= dalloc(S.d_scat, S.cap_level) != cudaSuccess;
     bad |= dalloc(S.plan, S.cap_level) != cudaSuccess;
     bad |= dalloc(S.chunks, S.cap_chunks + S.cap_large) != cudaSuccess;  // tail holds large_slot
     bad |= dalloc(S.hist, (size_t)S.cap_large * kHist) != cudaSuccess;
@@ -1640,6 +1658,8 @@ cudaError_t build_launch(BuildState &S, const float4 *verts, const uint4 *tris, 
     A.axis = S.d_axis;
     A.plane = S.d_plane;
     A.cnt = S.d_cnt;
+    A.split = S.d_split;
+    A.scat = S.d_scat;
     A.plan = S.plan;
     A.chunks = S.chunks;
     A.large_slot = reinterpret_cast<uint32_t *>(S.chunks + S.cap_chunks);
