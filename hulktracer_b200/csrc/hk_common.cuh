@@ -108,12 +108,13 @@ __device__ __forceinline__ bool ray_box(const float *bmin, const float *bmax, fl
 //   fails or t cannot beat `best` (the reference would discard that hit).
 __device__ __forceinline__ float isect_tri(const TriRec *__restrict__ tri, float3 o, float3 d,
                                            float best) {
+    // a and b share one 32-byte sector: load both before the first test
     const float4 a = __ldg(&tri->a);
+    const float4 b = __ldg(&tri->b);
     float den = __fadd_rn(__fadd_rn(__fmul_rn(a.y, d.y), 0.0f),
                           __fadd_rn(__fmul_rn(a.z, d.z), __fmul_rn(a.x, d.x)));
     if (fabsf(den) < 1.192092896e-07f) return __int_as_float(0x7f800000);
     den = __frcp_rn(den);  // == 1.0f / den, correctly rounded
-    const float4 b = __ldg(&tri->b);
     float vx = __fsub_rn(b.x, o.x), vy = __fsub_rn(b.y, o.y), vz = __fsub_rn(b.z, o.z);
     float num = __fadd_rn(__fadd_rn(__fmul_rn(a.y, vy), 0.0f),
                           __fadd_rn(__fmul_rn(a.z, vz), __fmul_rn(a.x, vx)));

@@ -57,13 +57,16 @@ template <bool COUNT>
 __device__ __forceinline__ void test_leaf(const SceneView &A, uint2 leaf, float3 o, float3 d,
                                           float &best, int32_t &best_id, uint32_t &c_refs) {
     uint32_t start = leaf.x >> 2, cnt = leaf.y;
+    // the next reference index is loaded while the current triangle is tested
+    uint32_t tri = cnt ? __ldg(&A.refs[start]) : 0u;
     for (uint32_t i = 0; i < cnt; i++) {
-        uint32_t tri = __ldg(&A.refs[start + i]);
+        const uint32_t next = i + 1 < cnt ? __ldg(&A.refs[start + i + 1]) : 0u;
         float t = isect_tri(&A.tris[tri], o, d, best);
         if (t < best) {
             best = t;
             best_id = (int32_t)tri;
         }
+        tri = next;
     }
     if (COUNT) c_refs += cnt;
 }
