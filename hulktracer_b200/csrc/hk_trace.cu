@@ -393,16 +393,16 @@ __global__ void __launch_bounds__(256, 5) k_trace(TraceArgs A) {
                 uint32_t rid = base + __popc(idle & lt_mask);
                 if (rid < n) {
                     if (BATCH) {
+                        // only the scene index stays with the lane; the scene's
+                        // arrays are looked up again at every leg (L1-resident)
                         scene = scene_of(A.ray_offsets, A.nscenes, rid);
                         const SceneDesc &D = A.scenes[scene];
-                        V = SceneView{D.nodes, D.refs, D.tris, D.ropes, D.cbox};
                         for (int k = 0; k < 3; k++) {
                             bmin[k] = D.box[k];
                             bmax[k] = D.box[4 + k];
                         }
-                        root = V.nodes[0];
-                        legs_max = 4u * D.nn + 8u;
-                        ntris = D.ntris;
+                        // the full stack starts its ray at this scene's root
+                        if (VARIANT == HK_TRACE_FULLSTACK) root = D.nodes[0];
                     }
                     float4 ro = A.rays[2 * (size_t)rid], rd = A.rays[2 * (size_t)rid + 1];
                     L.o = make_float3(ro.x, ro.y, ro.z);
@@ -450,6 +450,13 @@ __global__ void __launch_bounds__(256, 5) k_trace(TraceArgs A) {
             continue;
         }
         if (!active) continue;
+        if (BATCH) {
+            const SceneDesc &D = A.scenes[scene];
+            V = SceneView{D.nodes, D.refs, D.tris, D.ropes, D.cbox};
+            legs_max = 4u * D.nn + 8u;
+            ntris = D.ntris;
+            if (VARIANT != HK_TRACE_ROPES && VARIANT != HK_TRACE_BRUTE) root = V.nodes[0];
+        }
         bool done;
         if (VARIANT == HK_TRACE_BRUTE) {
             // GPUTrace_bruteforce.cl:30-42: every triangle in index order

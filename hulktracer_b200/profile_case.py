@@ -27,13 +27,19 @@ def main():
     from hulktracer_b200 import scenes
 
     ap = argparse.ArgumentParser()
-    ap.add_argument("--case", default="trace", choices=["trace", "build", "frame", "breakdown"])
+    ap.add_argument("--case", default="trace", choices=["trace", "build", "frame", "breakdown", "batch"])
+    ap.add_argument("--scenes", type=int, default=64, help="batch case: number of scenes")
+    ap.add_argument("--rays", type=int, nargs=2, default=[65_536, 4_194_304], help="batch case: ray batch range")
+    ap.add_argument("--tris", type=int, nargs=2, default=[10_000, 2_000_000], help="batch case: triangle range")
     ap.add_argument("--variant", default="shortstack")
     ap.add_argument("--mode", default="binned", choices=["binned", "learned"])
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--weights", default=os.path.join(ROOT, "hulktracer_b200", "weights", "proposer.bin"))
     ap.add_argument("--exact-max", type=int, default=0, help="exact SAH on nodes of at most this many refs")
     a = ap.parse_args()
+    if a.case == "batch":
+        batch_case(a)
+        return
     sc = scenes.animated_parts()
     W, H = sc.width, sc.height
     ctx = hk.Context(exact_max=a.exact_max)
@@ -98,6 +104,79 @@ def main():
                       hk.VARIANTS[a.variant], True)
         ctx.synchronize()
     print("case %s done: tree %s" % (a.case, {k: st[k] for k in ("nodes", "refs", "depth")}))
+
+
+def batch_case(a):
+    """Many scenes, one persistent launch: 64 clustered-soup scenes with
+    log-uniform triangle counts in [10k, 2M] and log-uniform ray batches in
+    [64k, 4M] (a quarter primary rays, the rest cosine-weighted rays leaving
+    random surface points: shadow / diffuse-bounce stand-ins). Prints the
+    aggregate Mrays/s of the batched launch, the per-scene completion times
+    (p50 / p99) and, for comparison, one launch per scene."""
+    import json
+    import time
+
+    import numpy as np
+    import torch
+
+    import hulktracer_b200 as hk
+    from hulktracer_b200 import scenes
+    t0 = time.time()
+    sets = scenes.batch_scenes(n_scenes=a.scenes, tris=tuple(a.tris), rays=tuple(a.rays))
+    ctx = hk.Context()
+    batch = hk.engine.Batch(ctx)
+    rays, offsets = [], [0]
+    for i, (sc, nr) in enumerate(sets):
+        batch.add_scene(sc.verts, sc.tris)
+        rays.append(scenes.incoherent_rays(sc, nr, seed=1000 + i))
+        offsets.append(offsets[-1] + nr)
+    allr = np.concatenate(rays)
+    n = allr.shape[0]
+    d_rays = torch.from_numpy(allr).cuda()
+    d_hits = torch.zeros(2 * n, dtype=torch.int32, device="cuda")
+    setup_s = time.time() - t0
+    v = hk.VARIANTS[a.variant]
+    for _ in range(2):
+        batch.trace_device(d_rays.data_ptr(), offsets, d_hits.data_ptr(), v)
+    torch.cuda.synchronize()
+    reps, ms_all, per = 5, [], []
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        ms = batch.trace_device(d_rays.data_ptr(), offsets, d_hits.data_ptr(), v)
+        e1.record()
+        torch.cuda.synchronize()
+        ms_all.append(e0.elapsed_time(e1))
+        per.append(ms)
+    t = float(np.median(ms_all))
+    per = np.median(np.stack(per), axis=0)
+    # one launch per scene, same rays (each scene's own context and tree)
+    single = []
+    for i, (sc, nr) in enumerate(sets):
+        c = hk.Context()
+        c.upload(sc.verts, sc.tris)
+        c.precompute()
+        c.build()
+        single.append(c)
+    def run_single():
+        for i, c in enumerate(single):
+            c.trace_device(d_rays.data_ptr() + 32 * offsets[i], offsets[i + 1] - offsets[i],
+                           d_hits.data_ptr() + 8 * offsets[i], v)
+        for c in single:
+            c.synchronize()
+    run_single()
+    ts = []
+    for _ in range(3):
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        run_single()
+        ts.append((time.perf_counter() - t1) * 1000.0)
+    out = {"scenes": len(sets), "tris_total": int(sum(sc.ntris for sc, _ in sets)), "rays": int(n),
+           "variant": a.variant, "batched_ms": t, "batched_mrays_s": n / t / 1e3,
+           "scene_done_ms_p50": float(np.percentile(per, 50)), "scene_done_ms_p99": float(np.percentile(per, 99)),
+           "per_scene_launches_ms": float(np.median(ts)), "per_scene_mrays_s": n / float(np.median(ts)) / 1e3,
+           "setup_s": round(setup_s, 1)}
+    print(json.dumps(out))
 
 
 if __name__ == "__main__":
