@@ -88,6 +88,8 @@ def load(path: str = LIB_PATH):
         "hk_scene_get_vertices": [vp, f32p],
         "hk_scene_get_counts": [vp, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)],
         "hk_tree_save_file": [vp, C.c_char_p],
+        "hk_obj_parse": [C.c_char_p, f32p, u32, vp, u32, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)],
+        "hk_scene_load_obj": [vp, C.c_char_p, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)],
         "hk_set_frame_shading": [vp, C.c_int],
         "hk_tree_load_file": [vp, C.c_char_p, C.c_int],
         "hk_scene_set_mirrors": [vp, vp, u32],

@@ -31,6 +31,22 @@ def _u32(a):
     return np.ascontiguousarray(a, dtype=np.uint32)
 
 
+def obj_parse(path: str):
+    """Vertices float32[V, 4] (w = 1) and triangles uint32[T, 4] of an OBJ file,
+    parsed by the library as the reference's OBJ loader reads it."""
+    L = _lib.load()
+    nv, nt = C.c_uint32(), C.c_uint32()
+    st = L.hk_obj_parse(path.encode(), None, 0, None, 0, C.byref(nv), C.byref(nt))
+    if st != 0:
+        raise HkError(st, "hk_obj_parse(%s)" % path)
+    v = np.zeros((nv.value, 4), np.float32)
+    t = np.zeros((nt.value, 4), np.uint32)
+    st = L.hk_obj_parse(path.encode(), ptr(v), nv.value, ptr(t), nt.value, C.byref(nv), C.byref(nt))
+    if st != 0:
+        raise HkError(st, "hk_obj_parse(%s)" % path)
+    return v, t
+
+
 class Context:
     def __init__(self, device: int = 0, **cfg):
         self.L = _lib.load()
@@ -71,6 +87,12 @@ class Context:
         v, t = _f32(verts), _u32(tris)
         self._check(self.L.hk_scene_upload(self.h, ptr(v), v.shape[0], ptr(t), t.shape[0]))
         self.ntris, self.nverts = t.shape[0], v.shape[0]
+
+    def load_obj(self, path):
+        """Parse an OBJ file and upload it as the scene."""
+        nv, nt = C.c_uint32(), C.c_uint32()
+        self._check(self.L.hk_scene_load_obj(self.h, path.encode(), C.byref(nv), C.byref(nt)))
+        self.nverts, self.ntris = nv.value, nt.value
 
     def set_box(self, box):
         self._check(self.L.hk_scene_set_box(self.h, ptr(_f32(box))))

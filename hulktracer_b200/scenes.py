@@ -19,6 +19,7 @@ the shapes and sizes of the benchmark scenes:
 from __future__ import annotations
 
 import math
+import os
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -433,3 +434,19 @@ def batch_scenes(n_scenes: int = 64, seed: int = 5, tris=(10_000, 2_000_000), ra
     nt = np.exp(rng.uniform(math.log(tris[0]), math.log(tris[1]), n_scenes)).astype(np.int64)
     nr = np.exp(rng.uniform(math.log(rays[0]), math.log(rays[1]), n_scenes)).astype(np.int64)
     return [(cluster_soup(int(nt[i]), seed * 1000 + i), int(nr[i])) for i in range(n_scenes)]
+
+
+def from_obj(path: str, width: int = 800, height: int = 600) -> Scene:
+    """A scene from a Wavefront OBJ file (parsed by the library), with the
+    reference OBJ loader's frame size and light (OBJLoader/OBJLoader.cpp:
+    119-135: 800x600, one directional light along normalize(-1, 1, 1), colour
+    0.9) and a camera that looks at the mesh's bounding box from its +z side."""
+    from .engine import obj_parse
+    V, T = obj_parse(path)
+    lo, hi = V[:, :3].min(axis=0).astype(np.float64), V[:, :3].max(axis=0).astype(np.float64)
+    c, r = (lo + hi) / 2.0, float(np.linalg.norm(hi - lo)) / 2.0
+    cam = look_at_camera(tuple(c + np.array([0.25 * r, 0.35 * r, 2.2 * r])), tuple(c), 60.0, width, height)
+    d = np.array([-1.0, 1.0, 1.0]) / math.sqrt(3.0)
+    lights = np.stack([directional_light(tuple(d), (0.9, 0.9, 0.9))])
+    return Scene(V, T, lights, cam, width, height, name=os.path.basename(path))
+

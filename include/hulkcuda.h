@@ -231,6 +231,17 @@ hk_status hk_get_ray_counts(hk_ctx *ctx, uint64_t *primary, uint64_t *shadow);
 /* Kernel nodes and all nodes of the captured frame graph (0 before capture). */
 hk_status hk_frame_graph_info(hk_ctx *ctx, uint32_t *kernel_nodes, uint32_t *all_nodes);
 
+/* ---- OBJ ingest ----
+ * The reference's Wavefront OBJ loader (OBJLoader::viParseFile,
+ * OBJLoader/OBJLoader.cpp:15-136): vertices "v x y z" (w = 1), triangles "f a b c"
+ * (1-based vertex index before the first '/' of each token; only the first
+ * three tokens of a face are read), comments, groups and normals skipped.
+ * hk_obj_parse fills host arrays (pass null arrays first to get the counts);
+ * hk_scene_load_obj parses and uploads the scene (hk_scene_upload). */
+hk_status hk_obj_parse(const char *path, float *verts4, uint32_t cap_verts, uint32_t *tris4, uint32_t cap_tris,
+                       uint32_t *nv, uint32_t *nt);
+hk_status hk_scene_load_obj(hk_ctx *ctx, const char *path, uint32_t *nv, uint32_t *nt);
+
 /* ---- tree interchange file ----
  * The reference's dataset dump (GLVisitorGPUTrace::saveDataSetToFile,
  * HulkEngine/src/GLVisitorGPUTrace.cpp:638-674, read back by
