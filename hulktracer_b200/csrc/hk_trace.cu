@@ -350,7 +350,7 @@ __device__ __forceinline__ uint32_t scene_of(const uint32_t *off, uint32_t nscen
 }
 
 template <int VARIANT, bool COUNT, bool BATCH>
-__global__ void __launch_bounds__(256, 5) k_trace(TraceArgs A) {
+__global__ void __launch_bounds__(256, 6) k_trace(TraceArgs A) {
     extern __shared__ float smem[];
     const bool smem_ring = (VARIANT == HK_TRACE_SMEMSTACK);
     float *s_s = smem;
