@@ -972,10 +972,24 @@ __global__ void __launch_bounds__(256, 3) k_hist(LevelArgs A) {
     tally_flush(A, tally, s_tally);
 }
 
+// Learned mode: the proposer's features of every proposer row (a large node
+// of more than one chunk), one warp per row.
+__global__ void __launch_bounds__(256) k_feat(LevelArgs A) {
+    __shared__ float FS[8][200];
+    const uint32_t wib = threadIdx.x >> 5;
+    const uint32_t nlarge = min(A.lc->n_large, A.cap_large);
+    const uint32_t nodes = A.lc->nodes;
+    for (uint32_t row = blockIdx.x * 8 + wib; row < nlarge; row += gridDim.x * 8) {
+        const uint32_t s = A.large_slot[row];
+        if (s >= nodes || A.lrank[s] != row) continue;   // not a proposer row
+        node_features(A, A.n_info[s], A.n_lo[s], A.n_hi[s], FS[wib], A.feat + (size_t)row * 200);
+    }
+}
+
 // Small nodes (not splittable, or splittable and neither medium nor large):
 // one warp per node; the exact SAH in registers for nodes of at most 32
 // references when exact_max >= 32, else a warp-private histogram + the binned
-// SAH. Learned mode: the warp of a proposer row computes its features.
+// SAH.
 __global__ void __launch_bounds__(256, 5) k_small(LevelArgs A) {
     __shared__ uint32_t HS[8][kHist];
     __shared__ uint32_t s_tally[5];
@@ -989,15 +1003,7 @@ __global__ void __launch_bounds__(256, 5) k_small(LevelArgs A) {
         const uint4 info = A.n_info[s];
         const uint32_t cnt = info.y;
         const bool dec = decidable(A, cnt);
-        if (dec && (is_large(A, cnt) || is_medium(A, cnt))) {
-            if (A.learned) {
-                const uint32_t row = A.lrank[s];
-                if (row < A.cap_large)
-                    node_features(A, info, A.n_lo[s], A.n_hi[s], reinterpret_cast<float *>(HS[wib]),
-                                  A.feat + (size_t)row * 200);
-            }
-            continue;  // k_hist / k_propose
-        }
+        if (dec && (is_large(A, cnt) || is_medium(A, cnt))) continue;   // k_hist / k_feat + k_propose
         if (!dec) {
             if (lane == 0) {
                 const Decision leaf{-1, 0.0f, 0, 0, kInf, 0};
@@ -1725,22 +1731,21 @@ cudaError_t build_launch(BuildState &S, const float4 *verts, const uint4 *tris, 
         A.ref_node = S.ref_node[cur];
         A.nx_refs = S.refs[nxt];
         A.nx_ref_node = S.ref_node[nxt];
+        // large (and medium) nodes on the second stream, beside the small
+        // nodes (independent nodes; both only add to the level tallies):
+        // binned histograms, or the proposer's features, inference and costing
+        cudaEventRecord(S.ev_fork, st);
+        cudaStreamWaitEvent(S.aux, S.ev_fork, 0);
         if (!A.learned) {
-            // large-node histograms on the second stream, beside the small
-            // nodes (independent nodes; both only add to the level tallies)
-            cudaEventRecord(S.ev_fork, st);
-            cudaStreamWaitEvent(S.aux, S.ev_fork, 0);
             k_hist<<<G, 256, 0, S.aux>>>(A);
-            cudaEventRecord(S.ev_join, S.aux);
-            k_small<<<G * 2, 256, 0, st>>>(A);
-            cudaStreamWaitEvent(st, S.ev_join, 0);
         } else {
-            k_small<<<G * 2, 256, 0, st>>>(A);
+            k_feat<<<G, 256, 0, S.aux>>>(A);
+            mlp_infer(S.learn->mlp, S.feat, &A.lc->n_large, S.cap_large, S.logits, S.sm_count, S.aux);
+            k_propose<<<G * 2, 256, 0, S.aux>>>(A);
         }
-        if (A.learned) {
-            mlp_infer(S.learn->mlp, S.feat, &A.lc->n_large, S.cap_large, S.logits, G, st);
-            k_propose<<<G * 2, 256, 0, st>>>(A);
-        }
+        cudaEventRecord(S.ev_join, S.aux);
+        k_small<<<G * 2, 256, 0, st>>>(A);
+        cudaStreamWaitEvent(st, S.ev_join, 0);
         k_onepass<PlanOp><<<G, kScanThreads, 0, st>>>(PlanOp{A}, S.plan_flags, static_cast<U5 *>(S.plan_agg),
                                                       static_cast<U5 *>(S.plan_incl), &A.lc->plan_ticket);
         k_onepass<RefOp><<<G, kScanThreads, 0, st>>>(RefOp{A}, S.ref_flags, S.ref_agg, S.ref_incl,
