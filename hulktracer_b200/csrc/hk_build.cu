@@ -171,64 +171,55 @@ __device__ T lookback(const uint32_t *flags, const T *aggs, const T *incls, uint
 }
 
 // Op: T (scan value), Item (what load caches for apply), Ctx (per-CTA
-// constants), kItems (consecutive elements per thread); count(), tag(),
-// err(), ctx() (all threads; block 0 may also publish level state), load(i)
-// -> Item, value(Item) -> T, apply(i, exclusive prefix, Item, Ctx) -- apply
-// sees every element once, with its global prefix
-template <class Op>
-__global__ void __launch_bounds__(kScanThreads) k_onepass(Op op, uint32_t *flags, typename Op::T *aggs,
-                                                          typename Op::T *incls, uint32_t *ticket) {
+// constants), kItems (consecutive elements per thread); load(i) -> Item,
+// value(Item) -> T, apply(i, exclusive prefix, Item, Ctx), err(). One tile of
+// a single-pass scan: load, block scan, publish the aggregate, look back for
+// the tile's exclusive prefix, then -- after before_apply() (all threads) --
+// apply every element with its global prefix.
+template <class Op, class Before>
+__device__ __forceinline__ void scan_tile(const Op &op, uint32_t tile, uint32_t n, uint32_t tag,
+                                          const typename Op::Ctx &cx, uint32_t *flags, typename Op::T *aggs,
+                                          typename Op::T *incls, typename Op::T *sh, typename Op::T &s_excl,
+                                          const Before &before_apply) {
     using T = typename Op::T;
     constexpr int kItems = Op::kItems;
     constexpr uint32_t kTileN = kScanThreads * kItems;
-    __shared__ T sh[kScanThreads / 32 + 1];
-    __shared__ T s_excl;
-    __shared__ uint32_t s_tile;
-    const uint32_t n = op.count();
-    const uint32_t ntiles = (n + kTileN - 1) / kTileN;
-    const uint32_t tag = op.tag();
-    const typename Op::Ctx cx = op.ctx();
-    for (;;) {
-        if (threadIdx.x == 0) s_tile = atomicAdd(ticket, 1u);
-        __syncthreads();
-        const uint32_t tile = s_tile;
-        if (tile >= ntiles) break;
-        const uint32_t base = tile * kTileN + threadIdx.x * kItems;
-        typename Op::Item it[kItems];
-        T s = vzero<T>();
+    const uint32_t base = tile * kTileN + threadIdx.x * kItems;
+    typename Op::Item it[kItems];
+    T s = vzero<T>();
 #pragma unroll
-        for (int k = 0; k < kItems; k++) {
-            it[k] = op.load(base + k < n ? base + k : 0xffffffffu, cx);
-            s = vadd(s, op.value(it[k]));
-        }
-        T tot;
-        const T ex = block_excl(s, sh, tot);
-        if (threadIdx.x == 0) {
-            if (tile == 0) incls[0] = tot;
-            else aggs[tile] = tot;
-            __threadfence();
-            *reinterpret_cast<volatile uint32_t *>(flags + tile) = (tag << 2) | (tile == 0 ? 2u : 1u);
-        }
-        if (threadIdx.x < 32) {
-            const T e = tile ? lookback(flags, aggs, incls, tile, tag, op.err()) : vzero<T>();
-            if (threadIdx.x == 0) {
-                if (tile) {
-                    incls[tile] = vadd(e, tot);
-                    __threadfence();
-                    *reinterpret_cast<volatile uint32_t *>(flags + tile) = (tag << 2) | 2u;
-                }
-                s_excl = e;
-            }
-        }
-        __syncthreads();
-        T pre = vadd(s_excl, ex);
-#pragma unroll
-        for (int k = 0; k < kItems; k++) {
-            if (base + k < n) op.apply(base + k, pre, it[k], cx);
-            pre = vadd(pre, op.value(it[k]));
-        }
-        __syncthreads();
+    for (int k = 0; k < kItems; k++) {
+        it[k] = op.load(base + k < n ? base + k : 0xffffffffu, cx);
+        s = vadd(s, op.value(it[k]));
     }
+    T tot;
+    const T ex = block_excl(s, sh, tot);
+    if (threadIdx.x == 0) {
+        if (tile == 0) incls[0] = tot;
+        else aggs[tile] = tot;
+        __threadfence();
+        *reinterpret_cast<volatile uint32_t *>(flags + tile) = (tag << 2) | (tile == 0 ? 2u : 1u);
+    }
+    if (threadIdx.x < 32) {
+        const T e = tile ? lookback(flags, aggs, incls, tile, tag, op.err()) : vzero<T>();
+        if (threadIdx.x == 0) {
+            if (tile) {
+                incls[tile] = vadd(e, tot);
+                __threadfence();
+                *reinterpret_cast<volatile uint32_t *>(flags + tile) = (tag << 2) | 2u;
+            }
+            s_excl = e;
+        }
+    }
+    __syncthreads();
+    before_apply();
+    T pre = vadd(s_excl, ex);
+#pragma unroll
+    for (int k = 0; k < kItems; k++) {
+        if (base + k < n) op.apply(base + k, pre, it[k], cx);
+        pre = vadd(pre, op.value(it[k]));
+    }
+    __syncthreads();
 }
 
 // ---------------------------------------------------------------------------
@@ -1508,7 +1499,7 @@ struct RefOp {
     }
     __device__ T value(const Item &it) const { return it.f; }
     __device__ void apply(uint32_t r, uint2 P, const Item &it, const Ctx &) const {
-        const uint4 sc = A.scat[it.s];
+        const uint4 sc = __ldcg(A.scat + it.s);   // written by a plan tile of this launch
         if (!(sc.w & 1u)) {
             const uint32_t off = sc.x + r;   // leaf
             if (off < A.cap_refs) A.out_refs[off] = it.tri;
@@ -1537,6 +1528,67 @@ struct RefOp {
 };
 
 // ---------------------------------------------------------------------------
+// plan + refs of one level in one launch. Tickets 0 .. node tiles - 1 are plan
+// tiles (256 nodes), the rest reference tiles (1024 refs). A plan tile, once
+// applied, publishes a done flag; a reference tile computes its flags, scans
+// and looks back, then waits (bounded) for the plan tiles of its nodes (its
+// references belong to a contiguous run of nodes) before it scatters. Plan
+// tiles take their tickets before any reference tile and wait for nothing but
+// earlier plan tiles, so every wait ends.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kScanThreads) k_plan_refs(LevelArgs A, uint32_t *pflags, U5 *paggs, U5 *pincls,
+                                                            uint32_t *rflags, uint2 *raggs, uint2 *rincls,
+                                                            uint32_t *pdone, uint32_t *ticket) {
+    __shared__ U5 shp[kScanThreads / 32 + 1];
+    __shared__ uint2 shr[kScanThreads / 32 + 1];
+    __shared__ U5 sxp;
+    __shared__ uint2 sxr;
+    __shared__ uint32_t s_tile;
+    const PlanOp P{A};
+    const RefOp R{A};
+    const uint32_t tag = level_tag(A);
+    const PlanCtx pc = P.ctx();                 // block 0 also writes the next level's counters
+    const uint32_t stop = pc.stop;              // the guard, decided from the tallies by every CTA
+    const uint32_t nn = A.lc->nodes, nr = A.lc->refs;
+    const uint32_t ntn = (nn + kScanThreads - 1) / kScanThreads;
+    const uint32_t ntr = (nr + kTile - 1) / kTile;
+    for (;;) {
+        if (threadIdx.x == 0) s_tile = atomicAdd(ticket, 1u);
+        __syncthreads();
+        const uint32_t t = s_tile;
+        if (t < ntn) {
+            scan_tile(P, t, nn, tag, pc, pflags, paggs, pincls, shp, sxp, [] {});
+            // every thread's emission is visible before the done flag
+            __threadfence();
+            __syncthreads();
+            if (threadIdx.x == 0) *reinterpret_cast<volatile uint32_t *>(pdone + t) = tag;
+        } else if (t < ntn + ntr) {
+            const uint32_t rt = t - ntn;
+            auto wait_plan = [&] {
+                if (threadIdx.x == 0) {
+                    const uint32_t r0 = rt * kTile, r1 = min(nr, r0 + kTile) - 1;
+                    const uint32_t k0 = A.ref_node[r0] / kScanThreads, k1 = A.ref_node[r1] / kScanThreads;
+                    for (uint32_t k = k0; k <= k1 && k < ntn; k++) {
+                        for (uint32_t spins = 0; __ldcv(pdone + k) != tag; spins++) {
+                            if (spins >= kSpinLimit) {
+                                atomicOr(A.err, 4u);
+                                break;
+                            }
+                            __nanosleep(32);
+                        }
+                    }
+                    __threadfence();
+                }
+                __syncthreads();
+            };
+            scan_tile(R, rt, nr, tag, stop, rflags, raggs, rincls, shr, sxr, wait_plan);
+        } else {
+            break;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
 template <class T>
@@ -1557,7 +1609,7 @@ void build_release(BuildState &S) {
     }
     f(S.d_axis); f(S.d_plane); f(S.d_cnt); f(S.plan); f(S.d_split); f(S.d_scat);
     f(S.chunks); f(S.hist); f(S.done); f(S.medium_slot); f(S.lrank); f(S.feat); f(S.logits);
-    f(S.plan_flags); f(S.ref_flags); f(S.plan_agg); f(S.plan_incl); f(S.ref_agg); f(S.ref_incl); f(S.epoch);
+    f(S.plan_flags); f(S.ref_flags); f(S.plan_done); f(S.plan_agg); f(S.plan_incl); f(S.ref_agg); f(S.ref_incl); f(S.epoch);
     f(S.ctr); f(S.err);
     f(S.out_nodes); f(S.out_refs); f(S.out_ropes); f(S.out_cbox);
     if (S.ev_fork) cudaEventDestroy(S.ev_fork);
@@ -1614,6 +1666,7 @@ hk_status build_prepare(BuildState &S, const BuildParams &p, uint32_t nt, int sm
     bad |= dalloc(S.logits, (size_t)S.cap_large * kMlpOut) != cudaSuccess;
     bad |= dalloc(S.plan_flags, S.plan_tiles) != cudaSuccess;
     bad |= dalloc(S.ref_flags, S.ref_tiles) != cudaSuccess;
+    bad |= dalloc(S.plan_done, S.plan_tiles) != cudaSuccess;
     {
         U5 *pa = nullptr, *pi = nullptr;
         bad |= dalloc(pa, S.plan_tiles) != cudaSuccess;
@@ -1641,6 +1694,7 @@ hk_status build_prepare(BuildState &S, const BuildParams &p, uint32_t nt, int sm
     cudaMemset(S.epoch, 0, 4);
     cudaMemset(S.plan_flags, 0, (size_t)S.plan_tiles * 4);
     cudaMemset(S.ref_flags, 0, (size_t)S.ref_tiles * 4);
+    cudaMemset(S.plan_done, 0, (size_t)S.plan_tiles * 4);
     cudaMemset(S.ctr, 0, sizeof(BuildCounters));
     return HK_OK;
 }
@@ -1746,10 +1800,9 @@ cudaError_t build_launch(BuildState &S, const float4 *verts, const uint4 *tris, 
         cudaEventRecord(S.ev_join, S.aux);
         k_small<<<G * 2, 256, 0, st>>>(A);
         cudaStreamWaitEvent(st, S.ev_join, 0);
-        k_onepass<PlanOp><<<G, kScanThreads, 0, st>>>(PlanOp{A}, S.plan_flags, static_cast<U5 *>(S.plan_agg),
-                                                      static_cast<U5 *>(S.plan_incl), &A.lc->plan_ticket);
-        k_onepass<RefOp><<<G, kScanThreads, 0, st>>>(RefOp{A}, S.ref_flags, S.ref_agg, S.ref_incl,
-                                                     &A.lc->ref_ticket);
+        k_plan_refs<<<G, kScanThreads, 0, st>>>(A, S.plan_flags, static_cast<U5 *>(S.plan_agg),
+                                                 static_cast<U5 *>(S.plan_incl), S.ref_flags, S.ref_agg, S.ref_incl,
+                                                 S.plan_done, &A.lc->plan_ticket);
     }
     S.active = true;
     S.last_level = S.p.max_depth + 1;

@@ -97,6 +97,7 @@ struct BuildState {
     uint32_t *ref_node[2] = {nullptr, nullptr};
     // single-pass scan tile states (flags, aggregates, inclusive prefixes)
     uint32_t *plan_flags = nullptr, *ref_flags = nullptr;
+    uint32_t *plan_done = nullptr;               // per plan tile: emitted (tag of the level)
     void *plan_agg = nullptr, *plan_incl = nullptr;
     uint2 *ref_agg = nullptr, *ref_incl = nullptr;
     uint32_t plan_tiles = 0, ref_tiles = 0;
