@@ -1536,7 +1536,7 @@ struct RefOp {
 // tiles take their tickets before any reference tile and wait for nothing but
 // earlier plan tiles, so every wait ends.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kScanThreads) k_plan_refs(LevelArgs A, uint32_t *pflags, U5 *paggs, U5 *pincls,
+__global__ void __launch_bounds__(kScanThreads, 6) k_plan_refs(LevelArgs A, uint32_t *pflags, U5 *paggs, U5 *pincls,
                                                             uint32_t *rflags, uint2 *raggs, uint2 *rincls,
                                                             uint32_t *pdone, uint32_t *ticket) {
     __shared__ U5 shp[kScanThreads / 32 + 1];
@@ -1800,7 +1800,7 @@ cudaError_t build_launch(BuildState &S, const float4 *verts, const uint4 *tris, 
         cudaEventRecord(S.ev_join, S.aux);
         k_small<<<G * 2, 256, 0, st>>>(A);
         cudaStreamWaitEvent(st, S.ev_join, 0);
-        k_plan_refs<<<G, kScanThreads, 0, st>>>(A, S.plan_flags, static_cast<U5 *>(S.plan_agg),
+        k_plan_refs<<<S.sm_count * 6, kScanThreads, 0, st>>>(A, S.plan_flags, static_cast<U5 *>(S.plan_agg),
                                                  static_cast<U5 *>(S.plan_incl), S.ref_flags, S.ref_agg, S.ref_incl,
                                                  S.plan_done, &A.lc->plan_ticket);
     }
