@@ -698,7 +698,7 @@ static hk_status ensure_imported_ropes(hk_ctx *c) {
 }
 
 static hk_status trace_enqueue(hk_ctx *c, const float4 *d_rays, uint32_t n, const uint32_t *n_dev, hk_variant v,
-                               hk_hit *d_hits) {
+                               hk_hit *d_hits, bool occlusion = false) {
     if ((int)v < HK_TRACE_FULLSTACK || (int)v > HK_TRACE_BRUTE) return fail(c, HK_E_ILLEGAL_INPUT, "variant");
     if (!c->rec_valid) return fail(c, HK_E_STATE, "no triangle cache (hk_precompute or hk_cache_import)");
     if (v != HK_TRACE_BRUTE && !c->tree_valid) return fail(c, HK_E_STATE, "no tree");
@@ -733,6 +733,7 @@ static hk_status trace_enqueue(hk_ctx *c, const float4 *d_rays, uint32_t n, cons
     L.max_steps = 1u << 26;
     L.variant = (int)v;
     L.count = c->counting;
+    L.occlusion = occlusion;
     L.block = (int)c->cfg.block_size;
     int per_sm = c->cfg.blocks_per_sm ? (int)c->cfg.blocks_per_sm : std::max(1, 2048 / L.block);
     L.grid = c->sm_count * per_sm;
@@ -855,7 +856,7 @@ static hk_status render_enqueue(hk_ctx *c, uint32_t nl, uint32_t w, uint32_t h, 
     }
     HK_CUDA(c, launch_shadow_rays(shade_rays, shade_hits, c->rec.p, npix, c->lights.p, nl, c->srays.p, c->slot.p,
                                   c->spix.p, c->scount.p, c->stream));
-    s = trace_enqueue(c, c->srays.p, 0, c->scount.p, v, c->shits.p);
+    s = trace_enqueue(c, c->srays.p, 0, c->scount.p, v, c->shits.p, true);
     if (s != HK_OK) return s;
     HK_CUDA(c, launch_shade_cpu(shade_rays, shade_hits, c->rec.p, npix, c->lights.p, nl, c->slot.p, c->shits.p,
                                 d_rgba, c->stream, w, tiled));

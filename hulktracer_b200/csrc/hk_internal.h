@@ -40,6 +40,7 @@ struct TraceLaunch {
     uint32_t max_steps;
     int variant;
     bool count;
+    bool occlusion;             // shadow rays: origin w = light distance, stop at the first hit closer than it
     int grid, block;
     // ropes
     const uint32_t *ropes;      // 6 per node

@@ -156,6 +156,7 @@ extern "C" hk_status hk_render_noalloc(const uint32_t *d_nodes2, const uint32_t 
     L.hits = shits;
     L.n = 0;
     L.n_dev = control + 2;
+    L.occlusion = true;
     HK_TRY(launch_trace(L, s));
     HK_TRY(launch_shade_cpu(rays, hits, L.tris, (uint32_t)npix, lights, nl, slot, shits, d_rgba, s));
     uint32_t err = 0;

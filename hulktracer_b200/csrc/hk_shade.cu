@@ -270,7 +270,11 @@ __global__ void k_shadow_rays(const float4 *__restrict__ rays, const hk_hit *__r
         if (want) {
             uint32_t k = base + __popc(m & ((1u << (threadIdx.x & 31u)) - 1u));
             PointLightSetup s = point_light(L, pos);
-            srays[2 * (size_t)k] = s.org;
+            // the origin's w lane (0 here) carries the light distance to the
+            // occlusion trace, which stops at the first hit closer than it
+            float4 org = s.org;
+            org.w = s.dist;
+            srays[2 * (size_t)k] = org;
             srays[2 * (size_t)k + 1] = s.tl;
             spix[k] = p;
             slot[(size_t)l * npix + p] = k;

@@ -51,11 +51,12 @@ struct SceneView {
 
 // ---------------------------------------------------------------------------
 // leaf test: KDTreeCPU::testNodePolygons (KDTreeCPU.cpp:255-283): triangles
-// in leaf order, a hit replaces the best only when strictly closer.
+// in leaf order, a hit replaces the best only when strictly closer. ANY
+// (occlusion rays) returns at the first hit closer than lim.
 // ---------------------------------------------------------------------------
-template <bool COUNT>
+template <bool COUNT, bool ANY = false>
 __device__ __forceinline__ void test_leaf(const SceneView &A, uint2 leaf, float3 o, float3 d,
-                                          float &best, int32_t &best_id, uint32_t &c_refs) {
+                                          float &best, int32_t &best_id, uint32_t &c_refs, float lim = 0.0f) {
     uint32_t start = leaf.x >> 2, cnt = leaf.y;
     // the next reference index is loaded while the current triangle is tested
     uint32_t tri = cnt ? __ldg(&A.refs[start]) : 0u;
@@ -65,6 +66,10 @@ __device__ __forceinline__ void test_leaf(const SceneView &A, uint2 leaf, float3
         if (t < best) {
             best = t;
             best_id = (int32_t)tri;
+            if (ANY && best < lim) {
+                if (COUNT) c_refs += i + 1;
+                return;
+            }
         }
         tri = next;
     }
@@ -107,6 +112,7 @@ __device__ __forceinline__ uint32_t sentinel_to_root(const uint2 *nodes, uint32_
 struct LaneState {
     float3 o, d, inv;
     float te, tmin, tmax, best;
+    float lim;         // occlusion rays: the light distance
     int32_t best_id;
     uint32_t cur;
     uint2 node;
@@ -117,7 +123,7 @@ struct LaneState {
 // one leg of the ring short stack (KDTreeCPU::searchKDTreeStackless,
 // KDTreeCPU.cpp:363-447; GPUTrace_shortStack.cl:6-105; GPUTrace_LDSshortStack.cl:
 // 7-105 with the ring in shared memory, one column per thread); true = finished
-template <bool SMEM, bool COUNT>
+template <bool SMEM, bool COUNT, bool ANY>
 __device__ __forceinline__ bool leg_shortstack(const TraceArgs &A, const SceneView &V, LaneState &L, uint2 root, float *s_s, float *s_e,
                                                uint32_t *s_n, float *l_s, float *l_e, uint32_t *l_n,
                                                uint32_t &c_nodes, uint32_t &c_refs, uint32_t &steps) {
@@ -179,8 +185,8 @@ __device__ __forceinline__ bool leg_shortstack(const TraceArgs &A, const SceneVi
     }
     if (is_leaf(L.node)) {
         if (COUNT) c_nodes++;
-        test_leaf<COUNT>(V, L.node, L.o, L.d, L.best, L.best_id, c_refs);
-        if (L.best < L.tmax) return true;
+        test_leaf<COUNT, ANY>(V, L.node, L.o, L.d, L.best, L.best_id, c_refs, L.lim);
+        if (L.best < L.tmax || (ANY && L.best < L.lim)) return true;
     }
     return false;
 }
@@ -188,7 +194,7 @@ __device__ __forceinline__ bool leg_shortstack(const TraceArgs &A, const SceneVi
 // one leg of the full stack (KDTreeCPU::searchKDTree, KDTreeCPU.cpp:285-361 ==
 // GPUTrace.cl:6-90; far children pushed only when they exist), run until a leaf
 // has been tested; true = finished
-template <bool COUNT>
+template <bool COUNT, bool ANY>
 __device__ __forceinline__ bool leg_fullstack(const TraceArgs &A, const SceneView &V, LaneState &L, uint2 root, float *st_s, float *st_e,
                                               uint32_t *st_n, int max_stack, uint32_t &c_nodes, uint32_t &c_refs,
                                               uint32_t &steps) {
@@ -201,7 +207,8 @@ __device__ __forceinline__ bool leg_fullstack(const TraceArgs &A, const SceneVie
         }
         bool tested = false;
         if (is_leaf(L.node)) {
-            test_leaf<COUNT>(V, L.node, L.o, L.d, L.best, L.best_id, c_refs);
+            test_leaf<COUNT, ANY>(V, L.node, L.o, L.d, L.best, L.best_id, c_refs, L.lim);
+            if (ANY && L.best < L.lim) return true;
             L.cur = 0;
             tested = true;
         } else {
@@ -240,7 +247,7 @@ __device__ __forceinline__ bool leg_fullstack(const TraceArgs &A, const SceneVie
 
 // one leg of kd-restart (GPUTrace_stackless.cl:53-117 with every leaf resident;
 // EARLY adds the resume path's exit once the closest hit precedes tmax); true = finished
-template <bool EARLY, bool COUNT>
+template <bool EARLY, bool COUNT, bool ANY>
 __device__ __forceinline__ bool leg_restart(const TraceArgs &A, const SceneView &V, LaneState &L, uint2 root, uint32_t &c_nodes,
                                             uint32_t &c_refs, uint32_t &steps) {
     if (!(L.tmax < L.te)) return true;
@@ -271,8 +278,8 @@ __device__ __forceinline__ bool leg_restart(const TraceArgs &A, const SceneView 
     }
     if (is_leaf(L.node)) {
         if (COUNT) c_nodes++;
-        test_leaf<COUNT>(V, L.node, L.o, L.d, L.best, L.best_id, c_refs);
-        if (EARLY && L.best < L.tmax) return true;
+        test_leaf<COUNT, ANY>(V, L.node, L.o, L.d, L.best, L.best_id, c_refs, L.lim);
+        if ((EARLY && L.best < L.tmax) || (ANY && L.best < L.lim)) return true;
     }
     return false;
 }
@@ -282,7 +289,7 @@ __device__ __forceinline__ bool leg_restart(const TraceArgs &A, const SceneView 
 // current node (ties on a plane go to the side the ray moves into), test it,
 // stop when the closest hit precedes the cell's exit, else follow the rope of
 // the exit face. Legs are bounded by 4 * nodes + 8.
-template <bool COUNT>
+template <bool COUNT, bool ANY>
 __device__ __forceinline__ bool leg_ropes(const SceneView &A, LaneState &L, uint32_t legs_max, uint32_t &c_nodes,
                                           uint32_t &c_refs) {
     if (++L.size > (int)legs_max) return true;
@@ -321,8 +328,8 @@ __device__ __forceinline__ bool leg_ropes(const SceneView &A, LaneState &L, uint
     }
     if (COUNT) c_nodes++;
     if (node.y) {
-        test_leaf<COUNT>(A, node, L.o, L.d, L.best, L.best_id, c_refs);
-        if (L.best < texit) return true;
+        test_leaf<COUNT, ANY>(A, node, L.o, L.d, L.best, L.best_id, c_refs, L.lim);
+        if (L.best < texit || (ANY && L.best < L.lim)) return true;
     }
     if (face < 0) return true;
     uint32_t r = A.ropes[6 * (size_t)L.cur + face];
@@ -349,7 +356,11 @@ __device__ __forceinline__ uint32_t scene_of(const uint32_t *off, uint32_t nscen
     return lo;
 }
 
-template <int VARIANT, bool COUNT, bool BATCH>
+// ANY: occlusion rays (origin w = distance to the light). A ray stops at the
+// first hit closer than that distance; until then its state is the closest-hit
+// traversal's, so "some hit closer than the light" is found exactly when the
+// closest-hit traversal's answer is closer than the light, in every variant.
+template <int VARIANT, bool COUNT, bool BATCH, bool ANY>
 __global__ void __launch_bounds__(256, 6) k_trace(TraceArgs A) {
     extern __shared__ float smem[];
     const bool smem_ring = (VARIANT == HK_TRACE_SMEMSTACK);
@@ -410,6 +421,7 @@ __global__ void __launch_bounds__(256, 6) k_trace(TraceArgs A) {
                     L.ray = rid;
                     L.best = kInf;
                     L.best_id = -1;
+                    L.lim = ANY ? ro.w : 0.0f;
                     steps = 0;
                     if (VARIANT == HK_TRACE_BRUTE) {
                         active = true;
@@ -465,20 +477,21 @@ __global__ void __launch_bounds__(256, 6) k_trace(TraceArgs A) {
                 if (h < L.best) {
                     L.best = h;
                     L.best_id = (int32_t)t;
+                    if (ANY && L.best < L.lim) break;
                 }
             }
             if (COUNT) c_refs += ntris;
             done = true;
         } else if (VARIANT == HK_TRACE_FULLSTACK) {
-            done = leg_fullstack<COUNT>(A, V, L, root, l_s, l_e, l_n, kLocal, c_nodes, c_refs, steps);
+            done = leg_fullstack<COUNT, ANY>(A, V, L, root, l_s, l_e, l_n, kLocal, c_nodes, c_refs, steps);
         } else if (VARIANT == HK_TRACE_ROPES) {
-            done = leg_ropes<COUNT>(V, L, legs_max, c_nodes, c_refs);
+            done = leg_ropes<COUNT, ANY>(V, L, legs_max, c_nodes, c_refs);
         } else if (VARIANT == HK_TRACE_RESTART) {
-            done = leg_restart<false, COUNT>(A, V, L, root, c_nodes, c_refs, steps);
+            done = leg_restart<false, COUNT, ANY>(A, V, L, root, c_nodes, c_refs, steps);
         } else if (VARIANT == HK_TRACE_RESTART_EARLY) {
-            done = leg_restart<true, COUNT>(A, V, L, root, c_nodes, c_refs, steps);
+            done = leg_restart<true, COUNT, ANY>(A, V, L, root, c_nodes, c_refs, steps);
         } else {
-            done = leg_shortstack<smem_ring, COUNT>(A, V, L, root, s_s, s_e, s_n, l_s, l_e, l_n, c_nodes, c_refs,
+            done = leg_shortstack<smem_ring, COUNT, ANY>(A, V, L, root, s_s, s_e, s_n, l_s, l_e, l_n, c_nodes, c_refs,
                                                     steps);
         }
         if (done) {
@@ -494,17 +507,22 @@ __global__ void __launch_bounds__(256, 6) k_trace(TraceArgs A) {
     }
 }
 
+// occlusion launches take the any-hit instantiation unless they count (the
+// counting one is the closest-hit kernel, which gives the same shading)
 template <int V>
-static cudaError_t launch_v(const TraceArgs &a, bool count, int grid, int block, size_t smem, cudaStream_t s) {
+static cudaError_t launch_v(const TraceArgs &a, bool count, bool occlusion, int grid, int block, size_t smem,
+                            cudaStream_t s) {
     if (a.scenes) {
         if (count)
-            k_trace<V, true, true><<<grid, block, smem, s>>>(a);
+            k_trace<V, true, true, false><<<grid, block, smem, s>>>(a);
         else
-            k_trace<V, false, true><<<grid, block, smem, s>>>(a);
+            k_trace<V, false, true, false><<<grid, block, smem, s>>>(a);
     } else if (count) {
-        k_trace<V, true, false><<<grid, block, smem, s>>>(a);
+        k_trace<V, true, false, false><<<grid, block, smem, s>>>(a);
+    } else if (occlusion) {
+        k_trace<V, false, false, true><<<grid, block, smem, s>>>(a);
     } else {
-        k_trace<V, false, false><<<grid, block, smem, s>>>(a);
+        k_trace<V, false, false, false><<<grid, block, smem, s>>>(a);
     }
     return cudaGetLastError();
 }
@@ -543,15 +561,15 @@ cudaError_t launch_trace(const TraceLaunch &L, cudaStream_t s) {
     size_t smem = 0;
     if (L.variant == HK_TRACE_SMEMSTACK) smem = (size_t)L.stack_depth * block * 12;
     switch (L.variant) {
-    case HK_TRACE_FULLSTACK: return launch_v<HK_TRACE_FULLSTACK>(a, L.count, grid, block, smem, s);
-    case HK_TRACE_SHORTSTACK: return launch_v<HK_TRACE_SHORTSTACK>(a, L.count, grid, block, smem, s);
-    case HK_TRACE_SMEMSTACK: return launch_v<HK_TRACE_SMEMSTACK>(a, L.count, grid, block, smem, s);
-    case HK_TRACE_RESTART: return launch_v<HK_TRACE_RESTART>(a, L.count, grid, block, smem, s);
-    case HK_TRACE_RESTART_EARLY: return launch_v<HK_TRACE_RESTART_EARLY>(a, L.count, grid, block, smem, s);
+    case HK_TRACE_FULLSTACK: return launch_v<HK_TRACE_FULLSTACK>(a, L.count, L.occlusion, grid, block, smem, s);
+    case HK_TRACE_SHORTSTACK: return launch_v<HK_TRACE_SHORTSTACK>(a, L.count, L.occlusion, grid, block, smem, s);
+    case HK_TRACE_SMEMSTACK: return launch_v<HK_TRACE_SMEMSTACK>(a, L.count, L.occlusion, grid, block, smem, s);
+    case HK_TRACE_RESTART: return launch_v<HK_TRACE_RESTART>(a, L.count, L.occlusion, grid, block, smem, s);
+    case HK_TRACE_RESTART_EARLY: return launch_v<HK_TRACE_RESTART_EARLY>(a, L.count, L.occlusion, grid, block, smem, s);
     case HK_TRACE_ROPES:
         if (!L.scenes && (!L.ropes || !L.cbox)) return cudaErrorInvalidValue;
-        return launch_v<HK_TRACE_ROPES>(a, L.count, grid, block, smem, s);
-    case HK_TRACE_BRUTE: return launch_v<HK_TRACE_BRUTE>(a, L.count, grid, block, smem, s);
+        return launch_v<HK_TRACE_ROPES>(a, L.count, L.occlusion, grid, block, smem, s);
+    case HK_TRACE_BRUTE: return launch_v<HK_TRACE_BRUTE>(a, L.count, L.occlusion, grid, block, smem, s);
     default: return cudaErrorInvalidValue;
     }
 }
