@@ -309,7 +309,7 @@ __device__ Decision sah_warp(HistPtr H, float4 blo, float4 bhi, uint32_t cnt, fl
     float mc = kInf;
     uint32_t mkey = 0xffffffffu, m_nb = 0, m_na = 0;
     float m_pk = 0.0f;
-#pragma unroll 1
+#pragma unroll
     for (uint32_t a = 0; a < 3; a++) {
         const float l = c3(blo, a), h = c3(bhi, a);
         const float ext = __fsub_rn(h, l);
@@ -522,17 +522,24 @@ __device__ void tally_flush(const LevelArgs &A, const Tally &t, uint32_t *sh5) {
     if (threadIdx.x < 5 && sh5[threadIdx.x]) atomicAdd(&A.lc->t_leafrefs + threadIdx.x, sh5[threadIdx.x]);
 }
 
-__device__ __forceinline__ void write_decision(const LevelArgs &A, uint32_t s, const Decision &d) {
+// the node's bounds blo / bhi, when the caller has them
+__device__ __forceinline__ void write_decision(const LevelArgs &A, uint32_t s, const Decision &d, float4 blo,
+                                              float4 bhi) {
     A.axis[s] = d.axis;
     A.plane[s] = d.plane;
     A.cnt[s] = make_uint2(d.nb, d.na);
     // the partition's view of the decision in one 16-byte record
     float l = 0.0f, h = 0.0f;
     if (d.axis >= 0) {
-        l = c3(A.n_lo[s], (uint32_t)d.axis);
-        h = c3(A.n_hi[s], (uint32_t)d.axis);
+        l = c3(blo, (uint32_t)d.axis);
+        h = c3(bhi, (uint32_t)d.axis);
     }
     A.split[s] = make_float4(__int_as_float(d.axis), d.plane, l, h);
+}
+
+__device__ __forceinline__ void write_decision(const LevelArgs &A, uint32_t s, const Decision &d) {
+    if (d.axis >= 0) write_decision(A, s, d, A.n_lo[s], A.n_hi[s]);
+    else write_decision(A, s, d, make_float4(0, 0, 0, 0), make_float4(0, 0, 0, 0));
 }
 
 // global histogram read past L1 (other CTAs wrote it with atomics)
@@ -979,8 +986,9 @@ __global__ void __launch_bounds__(256) k_feat(LevelArgs A) {
 
 // Small nodes (not splittable, or splittable and neither medium nor large):
 // one warp per node; the exact SAH in registers for nodes of at most 32
-// references when exact_max >= 32, else a warp-private histogram + the binned
-// SAH.
+// references when exact_max >= 32 (the WARP_EXACT instantiation), else a
+// warp-private histogram + the binned SAH.
+template <bool WARP_EXACT>
 __global__ void __launch_bounds__(256, 5) k_small(LevelArgs A) {
     __shared__ uint32_t HS[8][kHist];
     __shared__ uint32_t s_tally[5];
@@ -1005,7 +1013,7 @@ __global__ void __launch_bounds__(256, 5) k_small(LevelArgs A) {
         }
         const float4 blo = A.n_lo[s], bhi = A.n_hi[s];
         Decision d;
-        if (A.exact_max >= kWarpExact && cnt <= kWarpExact) {
+        if (WARP_EXACT && cnt <= kWarpExact) {
             d = sah_exact_warp32(A, info, blo, bhi, A.ct, A.ci);
         } else {
             uint32_t *Hw = HS[wib];
@@ -1020,7 +1028,7 @@ __global__ void __launch_bounds__(256, 5) k_small(LevelArgs A) {
             d = sah_warp(Hw, blo, bhi, cnt, A.ct, A.ci);
         }
         if (lane == 0) {
-            write_decision(A, s, d);
+            write_decision(A, s, d, blo, bhi);
             tally.add(d, cnt);
         }
         __syncwarp();
@@ -1798,7 +1806,8 @@ cudaError_t build_launch(BuildState &S, const float4 *verts, const uint4 *tris, 
             k_propose<<<G * 2, 256, 0, S.aux>>>(A);
         }
         cudaEventRecord(S.ev_join, S.aux);
-        k_small<<<G * 2, 256, 0, st>>>(A);
+        if (A.exact_max >= kWarpExact) k_small<true><<<G * 2, 256, 0, st>>>(A);
+        else k_small<false><<<G * 2, 256, 0, st>>>(A);
         cudaStreamWaitEvent(st, S.ev_join, 0);
         k_plan_refs<<<S.sm_count * 6, kScanThreads, 0, st>>>(A, S.plan_flags, static_cast<U5 *>(S.plan_agg),
                                                  static_cast<U5 *>(S.plan_incl), S.ref_flags, S.ref_agg, S.ref_incl,
