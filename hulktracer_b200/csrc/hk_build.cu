@@ -46,6 +46,7 @@ constexpr uint32_t kSmall = 256;     // nodes with <= kSmall refs: one warp per 
 constexpr uint32_t kChunk = 1024;    // refs per histogram CTA of a large node (4 per thread)
 constexpr uint32_t kWarpExact = 32;  // exact-SAH nodes up to this size: one warp, in registers
 constexpr uint32_t kHist = 3 * 3 * kBins;
+static_assert(kHist % 4 == 0 && kHist / 4 > 64 && kHist / 4 <= 96, "k_small clears its histogram with 16-byte stores");
 constexpr int kScanThreads = 256;
 constexpr int kScanItems = 4;
 constexpr uint32_t kTile = kScanThreads * kScanItems;
@@ -990,7 +991,7 @@ __global__ void __launch_bounds__(256) k_feat(LevelArgs A) {
 // warp-private histogram + the binned SAH.
 template <bool WARP_EXACT>
 __global__ void __launch_bounds__(256, 5) k_small(LevelArgs A) {
-    __shared__ uint32_t HS[8][kHist];
+    __shared__ __align__(16) uint32_t HS[8][kHist];
     __shared__ uint32_t s_tally[5];
     Tally tally;
     const uint32_t wib = threadIdx.x >> 5, lane = threadIdx.x & 31u;
@@ -1017,7 +1018,13 @@ __global__ void __launch_bounds__(256, 5) k_small(LevelArgs A) {
             d = sah_exact_warp32(A, info, blo, bhi, A.ct, A.ci);
         } else {
             uint32_t *Hw = HS[wib];
-            for (uint32_t i = lane; i < kHist; i += 32) Hw[i] = 0;
+            {
+                // 288 counters = 72 16-byte stores
+                uint4 *H4 = reinterpret_cast<uint4 *>(Hw);
+                H4[lane] = make_uint4(0, 0, 0, 0);
+                H4[lane + 32] = make_uint4(0, 0, 0, 0);
+                if (lane < kHist / 4 - 64) H4[lane + 64] = make_uint4(0, 0, 0, 0);
+            }
             __syncwarp();
             const float4 inv3 = bin_scale(blo, bhi);
             for (uint32_t r = info.x + lane; r < info.x + cnt; r += 32) {
@@ -1398,12 +1405,12 @@ struct PlanOp {
             return;
         }
         {
-            // reference r goes below to nx_refs[child refs - below refs before s +
-            // P.x(r)] and above to nx_refs[below refs before s + cnt.x + P.y(r)]
-            // (P: the global prefix of the flags), into next-level slots pl.z and
-            // pl.z + (cnt.x > 0)
+            // the node's below references go to nx_refs[pl.w ..), its above ones
+            // right after them, each in its order within the node (its rank among
+            // the node's flagged references), as next-level slots pl.z and pl.z +
+            // (cnt.x > 0); w = above count << 2 | has-below << 1 | split
             const uint2 c2 = it.cnt;
-            A.scat[s] = make_uint4(pl.w - pl.v, pl.v + c2.x, pl.z, 1u | (c2.x ? 2u : 0u));
+            A.scat[s] = make_uint4(pl.w, pl.w + c2.x, pl.z, (c2.y << 2) | 1u | (c2.x ? 2u : 0u));
         }
         const uint32_t pair = cx.nodes_total + 2 * pl.y;
         const uint2 ct = it.cnt;
@@ -1473,10 +1480,10 @@ struct PlanOp {
     }
 };
 
-// refs: single-pass scan of the below / above flags fused with the stable
-// partition. The global prefix of a node's first reference is the sum of the
-// earlier split nodes' below (above) counts, which the plan scan provides, so
-// a reference's rank within its node's below list is prefix - that sum.
+// refs: single-pass scan of the below / above flags, segmented by node, fused
+// with the stable partition: a reference's rank among its node's below (above)
+// references, added to where the plan scan put the node's children, is its
+// place in the next level.
 struct RefItem {
     uint2 f;        // below / above flags
     uint32_t s;     // node slot
@@ -1506,7 +1513,8 @@ struct RefOp {
         return Item{make_uint2((lo < p || flat_on) ? 1u : 0u, (hi > p || flat_on) ? 1u : 0u), s, tri};
     }
     __device__ T value(const Item &it) const { return it.f; }
-    __device__ void apply(uint32_t r, uint2 P, const Item &it, const Ctx &) const {
+    // R: the reference's rank among its node's below / above references
+    __device__ void apply(uint32_t r, uint2 R, const Item &it, const Ctx &) const {
         const uint4 sc = __ldcg(A.scat + it.s);   // written by a plan tile of this launch
         if (!(sc.w & 1u)) {
             const uint32_t off = sc.x + r;   // leaf
@@ -1515,8 +1523,8 @@ struct RefOp {
             return;
         }
         if (it.f.x) {
-            const uint32_t pos = sc.x + P.x;
-            if (pos < A.cap_refs) {
+            const uint32_t pos = sc.x + R.x;
+            if (pos < A.cap_refs && R.x < sc.y - sc.x) {
                 A.nx_refs[pos] = it.tri;
                 A.nx_ref_node[pos] = sc.z;
             } else {
@@ -1524,8 +1532,8 @@ struct RefOp {
             }
         }
         if (it.f.y) {
-            const uint32_t pos = sc.y + P.y;
-            if (pos < A.cap_refs) {
+            const uint32_t pos = sc.y + R.y;
+            if (pos < A.cap_refs && R.y < (sc.w >> 2)) {
                 A.nx_refs[pos] = it.tri;
                 A.nx_ref_node[pos] = sc.z + ((sc.w & 2u) ? 1u : 0u);
             } else {
@@ -1534,6 +1542,106 @@ struct RefOp {
         }
     }
 };
+
+// segmented scan values: the flag counts since the last node start, and
+// whether a node starts in the span
+struct SegV {
+    uint2 v;
+    uint32_t h;
+};
+__device__ __forceinline__ SegV seg_join(SegV a, SegV b) {   // a before b
+    return SegV{b.h ? b.v : vadd(a.v, b.v), a.h | b.h};
+}
+__device__ __forceinline__ SegV seg_shfl_up(SegV x, int d) {
+    return SegV{make_uint2(__shfl_up_sync(0xffffffffu, x.v.x, d), __shfl_up_sync(0xffffffffu, x.v.y, d)),
+                __shfl_up_sync(0xffffffffu, x.h, d)};
+}
+
+struct RefTileSmem {
+    SegV w_tot[kScanThreads / 32];
+    uint32_t w_last[kScanThreads / 32];   // node of each warp's last reference
+    uint2 carry;                          // the tile's first segment: flags in earlier tiles
+};
+
+// One reference tile (kTile references, kScanItems per thread). The scan is
+// segmented by node: a tile in which a node starts publishes its last
+// segment's counts as complete (status 2) at once; only its first segment,
+// when it continues a node of earlier tiles, needs the look-back, which ends at
+// the tile where that node starts. wait_plan() runs (all threads) before the
+// scatter.
+template <class Wait>
+__device__ void ref_tile(const RefOp &R, uint32_t rt, uint32_t nr, uint32_t tag, uint32_t stop, uint32_t *flags,
+                         uint2 *aggs, uint2 *incls, RefTileSmem &sh, const Wait &wait_plan) {
+    const LevelArgs &A = R.A;
+    const uint32_t lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
+    const uint32_t r0 = rt * kTile;
+    const uint32_t base = r0 + threadIdx.x * kScanItems;
+    RefItem it[kScanItems];
+    bool hd[kScanItems];
+#pragma unroll
+    for (int k = 0; k < kScanItems; k++) it[k] = R.load(base + k < nr ? base + k : 0xffffffffu, stop);
+    // node of the reference before this thread's first one
+    uint32_t prev = __shfl_up_sync(0xffffffffu, it[kScanItems - 1].s, 1);
+    if (lane == 31) sh.w_last[wid] = it[kScanItems - 1].s;
+    const uint32_t first_prev = (threadIdx.x == 0 && r0 > 0) ? A.ref_node[r0 - 1] : 0xffffffffu;
+    __syncthreads();
+    if (lane == 0) prev = wid ? sh.w_last[wid - 1] : first_prev;
+    SegV t{make_uint2(0, 0), 0u};
+#pragma unroll
+    for (int k = 0; k < kScanItems; k++) {
+        const bool valid = base + k < nr;
+        hd[k] = !valid || it[k].s != (k ? it[k - 1].s : prev);
+        t = seg_join(t, SegV{it[k].f, hd[k] ? 1u : 0u});
+    }
+    // warp and block segmented scans
+    SegV inc = t;
+    for (int d = 1; d < 32; d <<= 1) {
+        const SegV o = seg_shfl_up(inc, d);
+        if ((int)lane >= d) inc = seg_join(o, inc);
+    }
+    SegV ex = seg_shfl_up(inc, 1);
+    if (lane == 0) ex = SegV{make_uint2(0, 0), 0u};
+    if (lane == 31) sh.w_tot[wid] = inc;
+    __syncthreads();
+    SegV wp{make_uint2(0, 0), 0u}, tot{make_uint2(0, 0), 0u};
+    for (uint32_t w = 0; w < kScanThreads / 32; w++) {
+        if (w < wid) wp = seg_join(wp, sh.w_tot[w]);
+        tot = seg_join(tot, sh.w_tot[w]);
+    }
+    ex = seg_join(wp, ex);
+    // the tile's first reference starts a node: no earlier tile matters
+    const bool starts = r0 == 0 || first_prev != it[0].s;
+    if (threadIdx.x == 0) {
+        if (tot.h) incls[rt] = tot.v;
+        else aggs[rt] = tot.v;
+        __threadfence();
+        *reinterpret_cast<volatile uint32_t *>(flags + rt) = (tag << 2) | (tot.h ? 2u : 1u);
+    }
+    if (threadIdx.x < 32) {
+        // the tile-0 rule is kept for the look-back: before tile 0 is zero
+        const uint2 c = (rt && !__shfl_sync(0xffffffffu, starts ? 1u : 0u, 0))
+                            ? lookback(flags, aggs, incls, rt, tag, A.err)
+                            : make_uint2(0, 0);
+        if (threadIdx.x == 0) {
+            if (!tot.h) {
+                incls[rt] = vadd(c, tot.v);
+                __threadfence();
+                *reinterpret_cast<volatile uint32_t *>(flags + rt) = (tag << 2) | 2u;
+            }
+            sh.carry = c;
+        }
+    }
+    __syncthreads();
+    wait_plan();
+    uint2 run = ex.h ? ex.v : vadd(ex.v, sh.carry);
+#pragma unroll
+    for (int k = 0; k < kScanItems; k++) {
+        if (hd[k]) run = make_uint2(0, 0);
+        if (base + k < nr) R.apply(base + k, run, it[k], stop);
+        run = vadd(run, it[k].f);
+    }
+    __syncthreads();
+}
 
 // ---------------------------------------------------------------------------
 // plan + refs of one level in one launch. Tickets 0 .. node tiles - 1 are plan
@@ -1548,9 +1656,8 @@ __global__ void __launch_bounds__(kScanThreads, 6) k_plan_refs(LevelArgs A, uint
                                                             uint32_t *rflags, uint2 *raggs, uint2 *rincls,
                                                             uint32_t *pdone, uint32_t *ticket) {
     __shared__ U5 shp[kScanThreads / 32 + 1];
-    __shared__ uint2 shr[kScanThreads / 32 + 1];
     __shared__ U5 sxp;
-    __shared__ uint2 sxr;
+    __shared__ RefTileSmem shr_seg;
     __shared__ uint32_t s_tile;
     const PlanOp P{A};
     const RefOp R{A};
@@ -1589,7 +1696,7 @@ __global__ void __launch_bounds__(kScanThreads, 6) k_plan_refs(LevelArgs A, uint
                 }
                 __syncthreads();
             };
-            scan_tile(R, rt, nr, tag, stop, rflags, raggs, rincls, shr, sxr, wait_plan);
+            ref_tile(R, rt, nr, tag, stop, rflags, raggs, rincls, shr_seg, wait_plan);
         } else {
             break;
         }
