@@ -50,6 +50,8 @@ static_assert(kHist % 4 == 0 && kHist / 4 > 64 && kHist / 4 <= 96, "k_small clea
 constexpr int kScanThreads = 256;
 constexpr int kScanItems = 4;
 constexpr uint32_t kTile = kScanThreads * kScanItems;
+constexpr int kPlanItems = 1;                                 // nodes per thread of a plan tile
+constexpr uint32_t kPlanTile = kScanThreads * kPlanItems;
 
 // ---------------------------------------------------------------------------
 // scan value types: uint2 (reference below/above flags) and U5 (node plan:
@@ -173,15 +175,16 @@ __device__ T lookback(const uint32_t *flags, const T *aggs, const T *incls, uint
 
 // Op: T (scan value), Item (what load caches for apply), Ctx (per-CTA
 // constants), kItems (consecutive elements per thread); load(i) -> Item,
-// value(Item) -> T, apply(i, exclusive prefix, Item, Ctx), err(). One tile of
-// a single-pass scan: load, block scan, publish the aggregate, look back for
-// the tile's exclusive prefix, then -- after before_apply() (all threads) --
-// apply every element with its global prefix.
-template <class Op, class Before>
+// value(Item) -> T, apply_first / apply(i, exclusive prefix, Item, Ctx),
+// err(). One tile of a single-pass scan: load, block scan, publish the
+// aggregate, look back for the tile's exclusive prefix, then apply_first every
+// element with its global prefix, run between() (all threads), and apply every
+// element.
+template <class Op, class Between>
 __device__ __forceinline__ void scan_tile(const Op &op, uint32_t tile, uint32_t n, uint32_t tag,
                                           const typename Op::Ctx &cx, uint32_t *flags, typename Op::T *aggs,
                                           typename Op::T *incls, typename Op::T *sh, typename Op::T &s_excl,
-                                          const Before &before_apply) {
+                                          const Between &between) {
     using T = typename Op::T;
     constexpr int kItems = Op::kItems;
     constexpr uint32_t kTileN = kScanThreads * kItems;
@@ -213,8 +216,15 @@ __device__ __forceinline__ void scan_tile(const Op &op, uint32_t tile, uint32_t 
         }
     }
     __syncthreads();
-    before_apply();
-    T pre = vadd(s_excl, ex);
+    const T pre0 = vadd(s_excl, ex);
+    T pre = pre0;
+#pragma unroll
+    for (int k = 0; k < kItems; k++) {
+        if (base + k < n) op.apply_first(base + k, pre, it[k], cx);
+        pre = vadd(pre, op.value(it[k]));
+    }
+    between();
+    pre = pre0;
 #pragma unroll
     for (int k = 0; k < kItems; k++) {
         if (base + k < n) op.apply(base + k, pre, it[k], cx);
@@ -396,7 +406,6 @@ struct LevelArgs {
     int32_t *axis;
     float *plane;
     uint2 *cnt;
-    uint4 *plan;            // per node: leaf-ref offset, next slot, child-ref offset, below-ref offset
     float4 *split;          // per node: axis (int bits, -1 = leaf), plane, node min / max on the axis
     uint4 *scat;            // per node: where its references go (written by the plan scan)
     uint2 *chunks;          // (large rank, chunk index within the node)
@@ -1360,7 +1369,7 @@ struct PlanOp {
     using T = U5;
     using Item = PlanItem;
     using Ctx = PlanCtx;
-    static constexpr int kItems = 1;
+    static constexpr int kItems = kPlanItems;
     LevelArgs A;
     __device__ uint32_t count() const { return A.lc->nodes; }
     __device__ uint32_t tag() const { return level_tag(A); }
@@ -1389,10 +1398,27 @@ struct PlanOp {
         const uint2 c = it.cnt;
         return U5{0, 1, (c.x > 0 ? 1u : 0u) + (c.y > 0 ? 1u : 0u), c.x + c.y, c.x};
     }
+    // where the node's references go (what the reference tiles wait for)
+    __device__ void apply_first(uint32_t s, U5 pl, const Item &it, const Ctx &cx) const {
+        const uint4 info = it.info;
+        if (info.z >= A.cap_nodes) return;   // apply flags it
+        if (cx.stop || it.axis < 0) {
+            // reference r of this leaf goes to out_refs[off - start + r]
+            const uint32_t off = cx.leafrefs_total + (cx.stop ? info.x : pl.x);
+            A.scat[s] = make_uint4(off - info.x, 0, 0, 0);
+        } else {
+            // the node's below references go to nx_refs[pl.w ..), its above ones
+            // right after them, each in its order within the node (its rank among
+            // the node's flagged references), as next-level slots pl.z and pl.z +
+            // (cnt.x > 0); w = above count << 2 | has-below << 1 | split
+            const uint2 c2 = it.cnt;
+            A.scat[s] = make_uint4(pl.w, pl.w + c2.x, pl.z, (c2.y << 2) | 1u | (c2.x ? 2u : 0u));
+        }
+    }
+    // the node's compact entry, its children's cells / ropes / records
     __device__ void apply(uint32_t s, U5 pl, const Item &it, const Ctx &cx) const {
         const uint4 info = it.info;
         const int ax = cx.stop ? -1 : it.axis;
-        A.plan[s] = make_uint4(pl.x, pl.z, pl.w, pl.v);
         if (info.z >= A.cap_nodes) {
             atomicOr(A.err, 16u);
             return;
@@ -1400,17 +1426,7 @@ struct PlanOp {
         if (ax < 0) {
             const uint32_t off = cx.leafrefs_total + (cx.stop ? info.x : pl.x);
             A.out_nodes[info.z] = make_uint2((off << 2) | kLeafTag, info.y);
-            // reference r of this leaf goes to out_refs[off - start + r]
-            A.scat[s] = make_uint4(off - info.x, 0, 0, 0);
             return;
-        }
-        {
-            // the node's below references go to nx_refs[pl.w ..), its above ones
-            // right after them, each in its order within the node (its rank among
-            // the node's flagged references), as next-level slots pl.z and pl.z +
-            // (cnt.x > 0); w = above count << 2 | has-below << 1 | split
-            const uint2 c2 = it.cnt;
-            A.scat[s] = make_uint4(pl.w, pl.w + c2.x, pl.z, (c2.y << 2) | 1u | (c2.x ? 2u : 0u));
         }
         const uint32_t pair = cx.nodes_total + 2 * pl.y;
         const uint2 ct = it.cnt;
@@ -1645,12 +1661,13 @@ __device__ void ref_tile(const RefOp &R, uint32_t rt, uint32_t nr, uint32_t tag,
 
 // ---------------------------------------------------------------------------
 // plan + refs of one level in one launch. Tickets 0 .. node tiles - 1 are plan
-// tiles (256 nodes), the rest reference tiles (1024 refs). A plan tile, once
-// applied, publishes a done flag; a reference tile computes its flags, scans
-// and looks back, then waits (bounded) for the plan tiles of its nodes (its
-// references belong to a contiguous run of nodes) before it scatters. Plan
-// tiles take their tickets before any reference tile and wait for nothing but
-// earlier plan tiles, so every wait ends.
+// tiles (kPlanTile nodes), the rest reference tiles (kTile refs). A plan tile
+// publishes a done flag once its nodes' reference destinations are written,
+// then emits the rest; a reference tile computes its flags, scans and looks
+// back, then waits (bounded) for the plan tiles of its nodes (its references
+// belong to a contiguous run of nodes) before it scatters. Plan tiles take
+// their tickets before any reference tile and wait for nothing but earlier
+// plan tiles, so every wait ends.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(kScanThreads, 6) k_plan_refs(LevelArgs A, uint32_t *pflags, U5 *paggs, U5 *pincls,
                                                             uint32_t *rflags, uint2 *raggs, uint2 *rincls,
@@ -1665,24 +1682,26 @@ __global__ void __launch_bounds__(kScanThreads, 6) k_plan_refs(LevelArgs A, uint
     const PlanCtx pc = P.ctx();                 // block 0 also writes the next level's counters
     const uint32_t stop = pc.stop;              // the guard, decided from the tallies by every CTA
     const uint32_t nn = A.lc->nodes, nr = A.lc->refs;
-    const uint32_t ntn = (nn + kScanThreads - 1) / kScanThreads;
+    const uint32_t ntn = (nn + kPlanTile - 1) / kPlanTile;
     const uint32_t ntr = (nr + kTile - 1) / kTile;
     for (;;) {
         if (threadIdx.x == 0) s_tile = atomicAdd(ticket, 1u);
         __syncthreads();
         const uint32_t t = s_tile;
         if (t < ntn) {
-            scan_tile(P, t, nn, tag, pc, pflags, paggs, pincls, shp, sxp, [] {});
-            // every thread's emission is visible before the done flag
-            __threadfence();
-            __syncthreads();
-            if (threadIdx.x == 0) *reinterpret_cast<volatile uint32_t *>(pdone + t) = tag;
+            // the done flag follows the tile's reference destinations; the
+            // rest of its emission overlaps the reference tiles' scatter
+            scan_tile(P, t, nn, tag, pc, pflags, paggs, pincls, shp, sxp, [&] {
+                __threadfence();
+                __syncthreads();
+                if (threadIdx.x == 0) *reinterpret_cast<volatile uint32_t *>(pdone + t) = tag;
+            });
         } else if (t < ntn + ntr) {
             const uint32_t rt = t - ntn;
             auto wait_plan = [&] {
                 if (threadIdx.x == 0) {
                     const uint32_t r0 = rt * kTile, r1 = min(nr, r0 + kTile) - 1;
-                    const uint32_t k0 = A.ref_node[r0] / kScanThreads, k1 = A.ref_node[r1] / kScanThreads;
+                    const uint32_t k0 = A.ref_node[r0] / kPlanTile, k1 = A.ref_node[r1] / kPlanTile;
                     for (uint32_t k = k0; k <= k1 && k < ntn; k++) {
                         for (uint32_t spins = 0; __ldcv(pdone + k) != tag; spins++) {
                             if (spins >= kSpinLimit) {
@@ -1722,7 +1741,7 @@ void build_release(BuildState &S) {
     for (int k = 0; k < 2; k++) {
         f(S.n_lo[k]); f(S.n_hi[k]); f(S.n_info[k]); f(S.refs[k]); f(S.ref_node[k]);
     }
-    f(S.d_axis); f(S.d_plane); f(S.d_cnt); f(S.plan); f(S.d_split); f(S.d_scat);
+    f(S.d_axis); f(S.d_plane); f(S.d_cnt); f(S.d_split); f(S.d_scat);
     f(S.chunks); f(S.hist); f(S.done); f(S.medium_slot); f(S.lrank); f(S.feat); f(S.logits);
     f(S.plan_flags); f(S.ref_flags); f(S.plan_done); f(S.plan_agg); f(S.plan_incl); f(S.ref_agg); f(S.ref_incl); f(S.epoch);
     f(S.ctr); f(S.err);
@@ -1754,7 +1773,7 @@ hk_status build_prepare(BuildState &S, const BuildParams &p, uint32_t nt, int sm
     S.cap_large = cap_refs / kSmall + 2;
     S.cap_chunks = cap_refs / kChunk + S.cap_large + 2;
     S.cap_medium = cap_refs / (kWarpExact + 1) + 2;
-    S.plan_tiles = S.cap_level / kScanThreads + 2;   // one node per thread
+    S.plan_tiles = S.cap_level / kPlanTile + 2;
     S.ref_tiles = cap_refs / kTile + 2;
     bool bad = false;
     bad |= dalloc(S.tb_lo, nt) != cudaSuccess;
@@ -1771,7 +1790,6 @@ hk_status build_prepare(BuildState &S, const BuildParams &p, uint32_t nt, int sm
     bad |= dalloc(S.d_cnt, S.cap_level) != cudaSuccess;
     bad |= dalloc(S.d_split, S.cap_level) != cudaSuccess;
     bad |= dalloc(S.d_scat, S.cap_level) != cudaSuccess;
-    bad |= dalloc(S.plan, S.cap_level) != cudaSuccess;
     bad |= dalloc(S.chunks, S.cap_chunks + S.cap_large) != cudaSuccess;  // tail holds large_slot
     bad |= dalloc(S.hist, (size_t)S.cap_large * kHist) != cudaSuccess;
     bad |= dalloc(S.done, S.cap_large) != cudaSuccess;
@@ -1835,7 +1853,6 @@ cudaError_t build_launch(BuildState &S, const float4 *verts, const uint4 *tris, 
     A.cnt = S.d_cnt;
     A.split = S.d_split;
     A.scat = S.d_scat;
-    A.plan = S.plan;
     A.chunks = S.chunks;
     A.large_slot = reinterpret_cast<uint32_t *>(S.chunks + S.cap_chunks);
     A.hist = S.hist;

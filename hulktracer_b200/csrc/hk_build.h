@@ -87,7 +87,6 @@ struct BuildState {
     uint2 *d_cnt = nullptr;                      // below, above
     float4 *d_split = nullptr;                   // axis bits, plane, node min / max on the axis
     uint4 *d_scat = nullptr;                     // reference destinations (plan scan)
-    uint4 *plan = nullptr;                       // per node: leaf-ref / child-ref / below-ref offsets, next slot
     uint2 *chunks = nullptr;                     // (large rank, chunk index); tail: large_slot
     uint32_t *hist = nullptr;                    // per large node 3 x 96
     uint32_t *done = nullptr;                    // per large node: chunks finished
