@@ -270,12 +270,14 @@ __device__ __forceinline__ void bin_interval(float lo, float hi, float blo, floa
     on = (lo == hi) && b >= 1 && lo == plane_k(blo, ext, b);
 }
 
-// bins per unit length of the node on each axis (32 / extent)
+// bins per unit length of the node on each axis (32 / extent). It only seeds
+// bin_interval's first guess, whose corrections end on the one bin b with
+// p_b <= lo < p_{b+1} from any start in [0, 31], so a fast division serves.
 __device__ __forceinline__ float4 bin_scale(float4 blo, float4 bhi) {
     float4 r;
-    r.x = __fdiv_rn(32.0f, __fsub_rn(bhi.x, blo.x));
-    r.y = __fdiv_rn(32.0f, __fsub_rn(bhi.y, blo.y));
-    r.z = __fdiv_rn(32.0f, __fsub_rn(bhi.z, blo.z));
+    r.x = __fdividef(32.0f, __fsub_rn(bhi.x, blo.x));
+    r.y = __fdividef(32.0f, __fsub_rn(bhi.y, blo.y));
+    r.z = __fdividef(32.0f, __fsub_rn(bhi.z, blo.z));
     r.w = 0.0f;
     return r;
 }
@@ -349,7 +351,8 @@ __device__ Decision sah_warp(HistPtr H, float4 blo, float4 bhi, uint32_t cnt, fl
         const uint32_t below = slo - hlo;          // sum_{b < k} hlo[b]
         const uint32_t above = cnt - (shi - hhi);  // sum_{c >= k} hhi[c]
         const uint32_t on = H[a * 96 + 64 + lane];
-        const float pk = plane_k(l, ext, lane), pk1 = plane_k(l, ext, lane + 1);
+        const float pk = plane_k(l, ext, lane);
+        const float pk1 = __shfl_down_sync(0xffffffffu, pk, 1);   // plane k + 1 (lane 31: unused)
         const bool valid = lane >= 1 && pk > l && pk < h && (lane == 31 || pk < pk1);
         if (!valid) continue;
         const uint32_t nb = below + on, na = above + on;
