@@ -90,6 +90,7 @@ struct hk_ctx {
     DevBuf<float4> srays;
     DevBuf<hk_hit> shits;
     DevBuf<uint32_t> slot, spix, scount;
+    DevBuf<uint32_t> hleaf;     // per pixel: the leaf its primary ropes traversal ended in
     DevBuf<float4> hit4;
     DevBuf<uint32_t> rgba;
     // mirror bounce
@@ -226,6 +227,7 @@ hk_status hk_destroy(hk_ctx *c) {
     c->nodes.release(); c->refs.release(); c->imp_ropes.release(); c->imp_cbox.release(); c->fetch.release(); c->counters.release(); c->errw.release();
     c->rays.release(); c->hits.release(); c->cam.release(); c->lights.release();
     c->srays.release(); c->shits.release(); c->slot.release(); c->spix.release(); c->scount.release();
+    c->hleaf.release();
     c->hit4.release(); c->rgba.release();
     c->mirror.release(); c->mrays.release(); c->prays.release(); c->mhits.release(); c->phits.release();
     c->mslot.release(); c->mcount.release();
@@ -698,7 +700,7 @@ static hk_status ensure_imported_ropes(hk_ctx *c) {
 }
 
 static hk_status trace_enqueue(hk_ctx *c, const float4 *d_rays, uint32_t n, const uint32_t *n_dev, hk_variant v,
-                               hk_hit *d_hits, bool occlusion = false) {
+                               hk_hit *d_hits, bool occlusion = false, uint32_t *leaf_out = nullptr) {
     if ((int)v < HK_TRACE_FULLSTACK || (int)v > HK_TRACE_BRUTE) return fail(c, HK_E_ILLEGAL_INPUT, "variant");
     if (!c->rec_valid) return fail(c, HK_E_STATE, "no triangle cache (hk_precompute or hk_cache_import)");
     if (v != HK_TRACE_BRUTE && !c->tree_valid) return fail(c, HK_E_STATE, "no tree");
@@ -734,6 +736,7 @@ static hk_status trace_enqueue(hk_ctx *c, const float4 *d_rays, uint32_t n, cons
     L.variant = (int)v;
     L.count = c->counting;
     L.occlusion = occlusion;
+    L.leaf_out = v == HK_TRACE_ROPES ? leaf_out : nullptr;
     L.block = (int)c->cfg.block_size;
     int per_sm = c->cfg.blocks_per_sm ? (int)c->cfg.blocks_per_sm : std::max(1, 2048 / L.block);
     L.grid = c->sm_count * per_sm;
@@ -811,6 +814,7 @@ static hk_status render_buffers(hk_ctx *c, uint32_t npix, uint32_t nl) {
     HK_CUDA(c, c->shits.ensure(ns));
     HK_CUDA(c, c->slot.ensure(ns));
     HK_CUDA(c, c->spix.ensure(ns));
+    HK_CUDA(c, c->hleaf.ensure(npix));
     HK_CUDA(c, c->hit4.ensure(npix));
     HK_CUDA(c, c->rgba.ensure(npix));
     HK_CUDA(c, c->cam.ensure(16));
@@ -834,7 +838,9 @@ static hk_status render_enqueue(hk_ctx *c, uint32_t nl, uint32_t w, uint32_t h, 
     c->last_shade = shade;
     const bool tiled = (w % 8u == 0) && (h % 4u == 0);
     HK_CUDA(c, launch_camera_rays(c->cam.p, w, h, c->rays.p, c->stream, tiled));
-    hk_status s = trace_enqueue(c, c->rays.p, npix, nullptr, v, c->hits.p);
+    // ropes: each pixel's last leaf, where its shadow rays may start
+    const bool hint = v == HK_TRACE_ROPES && shade != HK_SHADE_PICTURE;
+    hk_status s = trace_enqueue(c, c->rays.p, npix, nullptr, v, c->hits.p, false, hint ? c->hleaf.p : nullptr);
     if (s != HK_OK) return s;
     if (shade == HK_SHADE_PICTURE) {
         HK_CUDA(c, launch_hit4(c->hits.p, c->rec.p, npix, c->hit4.p, c->stream));
@@ -854,8 +860,9 @@ static hk_status render_enqueue(hk_ctx *c, uint32_t nl, uint32_t w, uint32_t h, 
         shade_rays = c->prays.p;
         shade_hits = c->phits.p;
     }
-    HK_CUDA(c, launch_shadow_rays(shade_rays, shade_hits, c->rec.p, npix, c->lights.p, nl, c->srays.p, c->slot.p,
-                                  c->spix.p, c->scount.p, c->stream));
+    HK_CUDA(c, launch_shadow_rays(shade_rays, shade_hits, c->rec.p, npix, c->lights.p, nl,
+                                  hint ? c->hleaf.p : nullptr, c->srays.p, c->slot.p, c->spix.p, c->scount.p,
+                                  c->stream));
     s = trace_enqueue(c, c->srays.p, 0, c->scount.p, v, c->shits.p, true);
     if (s != HK_OK) return s;
     HK_CUDA(c, launch_shade_cpu(shade_rays, shade_hits, c->rec.p, npix, c->lights.p, nl, c->slot.p, c->shits.p,

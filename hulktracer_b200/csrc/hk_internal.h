@@ -41,6 +41,7 @@ struct TraceLaunch {
     int variant;
     bool count;
     bool occlusion;             // shadow rays: origin w = light distance, stop at the first hit closer than it
+    uint32_t *leaf_out;         // ropes: per ray, the leaf its traversal ended in (a start hint), or nullptr
     int grid, block;
     // ropes
     const uint32_t *ropes;      // 6 per node
@@ -71,8 +72,8 @@ cudaError_t launch_box(const float4 *verts, uint32_t nv, uint32_t *box_ord, floa
 cudaError_t launch_camera_rays(const float *cam16_dev, uint32_t w, uint32_t h, float4 *rays, cudaStream_t s,
                                bool tiled = false);
 cudaError_t launch_shadow_rays(const float4 *rays, const hk_hit *hits, const TriRec *tris, uint32_t npix,
-                               const float *lights_dev, uint32_t nl, float4 *srays, uint32_t *slot,
-                               uint32_t *spix, uint32_t *scount, cudaStream_t s);
+                               const float *lights_dev, uint32_t nl, const uint32_t *leaf_hint, float4 *srays,
+                               uint32_t *slot, uint32_t *spix, uint32_t *scount, cudaStream_t s);
 cudaError_t launch_shade_cpu(const float4 *rays, const hk_hit *hits, const TriRec *tris, uint32_t npix,
                              const float *lights_dev, uint32_t nl, const uint32_t *slot, const hk_hit *shits,
                              uint32_t *rgba, cudaStream_t s, uint32_t w = 0, bool tiled = false);

@@ -151,7 +151,8 @@ extern "C" hk_status hk_render_noalloc(const uint32_t *d_nodes2, const uint32_t 
     L.n = (uint32_t)npix;
     L.n_dev = nullptr;
     HK_TRY(launch_trace(L, s));
-    HK_TRY(launch_shadow_rays(rays, hits, L.tris, (uint32_t)npix, lights, nl, srays, slot, spix, control + 2, s));
+    HK_TRY(launch_shadow_rays(rays, hits, L.tris, (uint32_t)npix, lights, nl, nullptr, srays, slot, spix, control + 2,
+                              s));
     L.rays = srays;
     L.hits = shits;
     L.n = 0;

@@ -246,10 +246,12 @@ __device__ __forceinline__ float4 hit_pos(float4 o, float4 d, float t) {
 
 // Writes one shadow ray per (hit pixel, point light) into a compacted list
 // (warp-aggregated atomics); slot[l * npix + p] = list index or 0xffffffff.
+// leaf_hint (optional): per pixel, the leaf the pixel's ropes traversal ended
+// in, passed in the direction's w lane as where the shadow ray may start.
 __global__ void k_shadow_rays(const float4 *__restrict__ rays, const hk_hit *__restrict__ hits,
                               uint32_t npix, const float *__restrict__ lights, uint32_t nl,
-                              float4 *__restrict__ srays, uint32_t *__restrict__ slot,
-                              uint32_t *__restrict__ spix, uint32_t *scount) {
+                              const uint32_t *__restrict__ leaf_hint, float4 *__restrict__ srays,
+                              uint32_t *__restrict__ slot, uint32_t *__restrict__ spix, uint32_t *scount) {
     uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
     hk_hit h = p < npix ? hits[p] : hk_hit{kInf, -1};
     float4 o = make_float4(0, 0, 0, 0), d = o;
@@ -259,6 +261,7 @@ __global__ void k_shadow_rays(const float4 *__restrict__ rays, const hk_hit *__r
     }
     float4 pos = hit_pos(o, d, h.t);
     pos.w = 0.0f;
+    const float hint = (leaf_hint && p < npix) ? __uint_as_float(leaf_hint[p]) : 0.0f;
     for (uint32_t l = 0; l < nl; l++) {
         const float *L = lights + 8 * l;
         bool want = (p < npix) && h.tri >= 0 && L[3] == 1.0f;
@@ -275,7 +278,9 @@ __global__ void k_shadow_rays(const float4 *__restrict__ rays, const hk_hit *__r
             float4 org = s.org;
             org.w = s.dist;
             srays[2 * (size_t)k] = org;
-            srays[2 * (size_t)k + 1] = s.tl;
+            float4 dir = s.tl;
+            dir.w = hint;
+            srays[2 * (size_t)k + 1] = dir;
             spix[k] = p;
             slot[(size_t)l * npix + p] = k;
         }
@@ -283,11 +288,13 @@ __global__ void k_shadow_rays(const float4 *__restrict__ rays, const hk_hit *__r
 }
 
 cudaError_t launch_shadow_rays(const float4 *rays, const hk_hit *hits, const TriRec *, uint32_t npix,
-                               const float *lights_dev, uint32_t nl, float4 *srays, uint32_t *slot,
-                               uint32_t *spix, uint32_t *scount, cudaStream_t s) {
+                               const float *lights_dev, uint32_t nl, const uint32_t *leaf_hint, float4 *srays,
+                               uint32_t *slot, uint32_t *spix, uint32_t *scount, cudaStream_t s) {
     cudaError_t e = cudaMemsetAsync(scount, 0, sizeof(uint32_t), s);
     if (e != cudaSuccess) return e;
-    if (npix) k_shadow_rays<<<blocks_for(npix, 256), 256, 0, s>>>(rays, hits, npix, lights_dev, nl, srays, slot, spix, scount);
+    if (npix)
+        k_shadow_rays<<<blocks_for(npix, 256), 256, 0, s>>>(rays, hits, npix, lights_dev, nl, leaf_hint, srays, slot,
+                                                            spix, scount);
     return cudaGetLastError();
 }
 

@@ -32,6 +32,7 @@ struct TraceArgs {
     uint32_t rope_nn;         // compact node count (legs bound 4 n + 8) ...
     const uint32_t *rope_nn_dev;  // ... or its device copy
     // batch mode: many scenes in one launch
+    uint32_t *leaf_out;            // ropes: per ray, the leaf its traversal ended in (or nullptr)
     const SceneDesc *scenes;
     const uint32_t *ray_offsets;   // nscenes + 1, ascending
     uint32_t nscenes;
@@ -441,6 +442,19 @@ __global__ void __launch_bounds__(256, 6) k_trace(TraceArgs A) {
                             } else if (VARIANT == HK_TRACE_ROPES) {
                                 L.tmin = ts;  // entry distance
                                 L.cur = 0;
+                                // an occlusion ray may name in its direction's w lane a
+                                // leaf to start from: taken when the start point lies
+                                // strictly inside the leaf's cell, where the descent
+                                // from the root would end as well
+                                const uint32_t hint = __float_as_uint(rd.w);
+                                if (ANY && hint != 0u && hint < (legs_max - 8u) / 4u && is_leaf(V.nodes[hint])) {
+                                    const float4 c0 = V.cbox[2 * (size_t)hint], c1 = V.cbox[2 * (size_t)hint + 1];
+                                    const float px = __fadd_rn(L.o.x, __fmul_rn(L.d.x, ts));
+                                    const float py = __fadd_rn(L.o.y, __fmul_rn(L.d.y, ts));
+                                    const float pz = __fadd_rn(L.o.z, __fmul_rn(L.d.z, ts));
+                                    if (c0.x < px && px < c1.x && c0.y < py && py < c1.y && c0.z < pz && pz < c1.z)
+                                        L.cur = hint;
+                                }
                             } else if (VARIANT == HK_TRACE_RESTART || VARIANT == HK_TRACE_RESTART_EARLY) {
                                 L.tmin = 0.0f;   // ThreadContext starts zeroed (GPUTrace_stackless.cl:98-100)
                                 L.tmax = 0.0f;
@@ -496,6 +510,7 @@ __global__ void __launch_bounds__(256, 6) k_trace(TraceArgs A) {
         }
         if (done) {
             A.hits[L.ray] = hk_hit{L.best, L.best_id};
+            if (VARIANT == HK_TRACE_ROPES && !BATCH && A.leaf_out) A.leaf_out[L.ray] = L.cur;
             active = false;
             if (BATCH && atomicSub(&A.remaining[scene], 1u) == 1u) A.done_ns[scene] = global_ns();
         }
@@ -547,6 +562,7 @@ cudaError_t launch_trace(const TraceLaunch &L, cudaStream_t s) {
     a.cbox = L.cbox;
     a.rope_nn = L.rope_nn;
     a.rope_nn_dev = L.rope_nn_dev;
+    a.leaf_out = L.leaf_out;
     a.scenes = L.scenes;
     a.ray_offsets = L.ray_offsets;
     a.nscenes = L.nscenes;
