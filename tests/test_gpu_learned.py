@@ -229,3 +229,37 @@ def test_trained_proposer_cost_and_gain(hk, oracle):
     assert res["trained"][0] <= 1.02
     assert res["trained"][1] < res["untrained"][1]
     assert res["trained"][0] <= res["untrained"][0]
+
+
+@pytest.mark.skipif(not os.path.exists(WEIGHTS), reason="no trained proposer weights")
+def test_trained_proposer_heldout_2m(hk, oracle):
+    """The held-out 2M-triangle animated sequence (seed 9001, 640 parts, a
+    density like the 200k scene's; neither it nor its seed was trained on):
+    over frames 0, 30 and 59 the learned tree costs within 2% of the binned
+    tree, and the device times of both builds are reported."""
+    sc = scenes.animated_parts(seed=9001, n_parts=640, scale=2.15, width=64, height=64)
+    assert sc.tris.shape[0] > 1_900_000
+    c = hk.Context()
+    c.mlp_load(WEIGHTS)
+    c.upload(sc.verts, sc.tris)
+    c.set_parts(sc.part_of_vertex, sc.part_center.shape[0])
+    ratios, fb, n, t_b, t_l = [], 0, 0, [], []
+    for frame in (0, 30, 59):
+        c.transform(scenes.part_matrices(sc, frame))
+        box = c.get_box()
+        c.build(hk.BUILD_BINNED)       # first build of a frame warms the arenas
+        sb = c.build(hk.BUILD_BINNED)
+        bn, _ = c.export_compact()
+        sl = c.build(hk.BUILD_LEARNED)
+        ln, _ = c.export_compact()
+        ratios.append(oracle.tree_cost(oracle.compact_to_ref(ln), box, CT, CI) /
+                      oracle.tree_cost(oracle.compact_to_ref(bn), box, CT, CI))
+        fb += sl["fallback_nodes"]
+        n += sl["fallback_nodes"] + sl["learned_nodes"]
+        t_b.append(sb["build_ms"])
+        t_l.append(sl["build_ms"])
+    c.close()
+    print("held-out 2M: learned/binned cost", [round(r, 4) for r in ratios], "fallback share %.3f" % (fb / max(n, 1)),
+          "build ms binned", [round(t, 3) for t in t_b], "learned", [round(t, 3) for t in t_l])
+    assert n > 0
+    assert max(ratios) <= 1.02
