@@ -133,6 +133,11 @@ __device__ __forceinline__ T block_excl(T v, T *sh_warp, T &total) {
 // ---------------------------------------------------------------------------
 constexpr uint32_t kSpinLimit = 1u << 22;
 
+// Kernels launched as programmatic dependents (launch_pdl) start before their
+// predecessor in the stream has finished; this waits until it has, with its
+// writes visible. Without the launch attribute it returns at once.
+__device__ __forceinline__ void wait_prior_grid() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 template <class T>
 __device__ T lookback(const uint32_t *flags, const T *aggs, const T *incls, uint32_t tile, uint32_t tag,
                       uint32_t *err) {
@@ -1005,6 +1010,7 @@ template <bool WARP_EXACT>
 __global__ void __launch_bounds__(256, 5) k_small(LevelArgs A) {
     __shared__ __align__(16) uint32_t HS[8][kHist];
     __shared__ uint32_t s_tally[5];
+    wait_prior_grid();
     Tally tally;
     const uint32_t wib = threadIdx.x >> 5, lane = threadIdx.x & 31u;
     const uint32_t nodes = A.lc->nodes;
@@ -1679,6 +1685,7 @@ __global__ void __launch_bounds__(kScanThreads, 6) k_plan_refs(LevelArgs A, uint
     __shared__ U5 sxp;
     __shared__ RefTileSmem shr_seg;
     __shared__ uint32_t s_tile;
+    wait_prior_grid();
     const PlanOp P{A};
     const RefOp R{A};
     const uint32_t tag = level_tag(A);
@@ -1728,6 +1735,24 @@ __global__ void __launch_bounds__(kScanThreads, 6) k_plan_refs(LevelArgs A, uint
 // ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
+// a launch that may start while the stream's previous kernel finishes
+// (programmatic stream serialization); the kernel calls wait_prior_grid()
+// before it reads anything that kernel wrote
+template <class... KArgs, class... Args>
+static cudaError_t launch_pdl(void (*k)(KArgs...), unsigned grid, unsigned block, cudaStream_t st, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, k, static_cast<KArgs>(args)...);
+}
+
 template <class T>
 static cudaError_t dalloc(T *&p, size_t n) {
     if (p) cudaFree(p);
@@ -1933,12 +1958,12 @@ cudaError_t build_launch(BuildState &S, const float4 *verts, const uint4 *tris, 
             k_propose<<<G * 2, 256, 0, S.aux>>>(A);
         }
         cudaEventRecord(S.ev_join, S.aux);
-        if (A.exact_max >= kWarpExact) k_small<true><<<G * 2, 256, 0, st>>>(A);
-        else k_small<false><<<G * 2, 256, 0, st>>>(A);
+        if (A.exact_max >= kWarpExact) launch_pdl(k_small<true>, G * 2, 256, st, A);
+        else launch_pdl(k_small<false>, G * 2, 256, st, A);
         cudaStreamWaitEvent(st, S.ev_join, 0);
-        k_plan_refs<<<S.sm_count * 6, kScanThreads, 0, st>>>(A, S.plan_flags, static_cast<U5 *>(S.plan_agg),
-                                                 static_cast<U5 *>(S.plan_incl), S.ref_flags, S.ref_agg, S.ref_incl,
-                                                 S.plan_done, &A.lc->plan_ticket);
+        launch_pdl(k_plan_refs, S.sm_count * 6, kScanThreads, st, A, S.plan_flags, static_cast<U5 *>(S.plan_agg),
+                   static_cast<U5 *>(S.plan_incl), S.ref_flags, S.ref_agg, S.ref_incl, S.plan_done,
+                   &A.lc->plan_ticket);
     }
     S.active = true;
     S.last_level = S.p.max_depth + 1;
