@@ -1983,7 +1983,9 @@ hk_status build_read_stats(BuildState &S, cudaStream_t st, hk_tree_stats *out) {
     S.last_err = err;
     if (err) {
         cudaMemsetAsync(S.err, 0, 4, st);
-        return HK_E_CAPACITY;
+        if (err & 4u) return HK_E_DEVICE_TIMEOUT;      // a bounded wait ran out
+        if (err & (8u | 16u)) return HK_E_BOUNDS;       // a partition / plan check fired
+        return HK_E_CAPACITY;                           // an arena or list was too small
     }
     const LevelCounters &fin = c.lvl[S.last_level];
     out->nodes = fin.nodes_total;

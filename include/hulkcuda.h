@@ -74,7 +74,10 @@ typedef enum hk_build_mode {
 
 /* Shading semantics for hk_render */
 enum {
-    HK_SHADE_CPU = 0,          /* GLVisitorCPUTrace::traceScene: shadow rays, misses 0 */
+    HK_SHADE_CPU = 0,          /* GLVisitorCPUTrace::traceScene: shadow rays, misses 0
+                                  (shadow rays are traced as occlusion queries that stop
+                                  at the first hit closer than the light: the same
+                                  shading as the reference's closest-hit test) */
     HK_SHADE_PICTURE = 1,      /* ShadePicture (shadePicture.cl:7-55): no shadow rays */
     HK_SHADE_MIRROR = 2        /* HK_SHADE_CPU plus one mirror bounce (no reference
                                   counterpart): a primary hit on a mirror triangle

@@ -199,3 +199,26 @@ def test_frame_mirror_shading_equals_render(ctx, hk):
         assert (img_r != ctx.render(sc.camera, sc.lights, 64, 64, hk.SHORTSTACK)).any()
     finally:
         ctx.set_frame_shading(hk.SHADE_CPU)
+
+
+def test_capacity_guard_stops_splitting(hk):
+    """A reference arena of twice the triangles: the level whose children would
+    not fit stops splitting (its nodes become leaves, capacity_hit = 1) and the
+    build succeeds; the tree stays within the arena and traces like brute force
+    (full stack, ropes)."""
+    g = load("small24k.npz")
+    nt = g["tris"].shape[0]
+    c = hk.Context(max_refs=2 * nt)
+    c.upload(g["verts"], g["tris"])
+    c.set_box(g["box"])
+    c.precompute()
+    st = c.build()
+    assert st["capacity_hit"] == 1
+    assert st["refs"] <= 2 * nt
+    b = c.trace(g["rays"], hk.BRUTE)
+    m = b["tri"] >= 0
+    for v in (hk.FULLSTACK, hk.ROPES):
+        h = c.trace(g["rays"], v)
+        assert np.array_equal(h["tri"] >= 0, m)
+        assert np.array_equal(h["t"][m], b["t"][m])
+    c.close()
