@@ -197,7 +197,7 @@ def test_train_reduces_loss(hk):
 @pytest.mark.skipif(not os.path.exists(WEIGHTS), reason="no trained proposer weights")
 def test_trained_proposer_cost_and_gain(hk, oracle):
     """On held-out frames of the animated 200k scene: the trained proposer's
-    tree costs within 2% of the exact binned tree (the fallback judges every
+    tree costs within 2% of the exact binned tree (the fallback checks every
     proposal), and it beats the untrained network on both the cost and the
     share of proposer nodes that needed the fallback."""
     sc = scenes.animated_parts()

@@ -2,7 +2,7 @@
 GPU trees equal the restatement, tests/test_gpu_build.py) against the
 reference's own SAH-NlogN tree built with the same constants (compiled
 reference, Ct 1, Ci 1.5, depth 24, leaves below 5, no reduction). One cost
-function (full surface areas) judges both. With the exact SAH on nodes of at
+function (full surface areas) costs both. With the exact SAH on nodes of at
 most 1024 references (hk_config.exact_max = 1024) the GPU tree must cost at
 most 1.01x the reference's on the benchmark scenes (at the rest pose the reference loses polygons coplanar
 with its candidate planes, KDTreeSAH.cpp:462-485, and the GPU tree is far
