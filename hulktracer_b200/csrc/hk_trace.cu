@@ -289,7 +289,64 @@ __device__ __forceinline__ bool leg_restart(const TraceArgs &A, const SceneView 
 // oracle's search_ropes): locate the leaf cell holding o + d*tentry from the
 // current node (ties on a plane go to the side the ray moves into), test it,
 // stop when the closest hit precedes the cell's exit, else follow the rope of
-// the exit face. Legs are bounded by 4 * nodes + 8.
+// the exit face. Legs are bounded by 4 * nodes + 8. ropes_locate does the
+// descent and the exit face (true = the leg bound ran out), the leaf test
+// follows, ropes_advance decides and follows the rope (true = finished).
+template <bool COUNT>
+__device__ __forceinline__ bool ropes_locate(const SceneView &A, LaneState &L, uint32_t legs_max, uint32_t &c_nodes,
+                                             uint32_t &lstart, uint32_t &lcnt, float &texit, int &face) {
+    if (++L.size > (int)legs_max) return true;
+    float p[3] = {__fadd_rn(L.o.x, __fmul_rn(L.d.x, L.tmin)), __fadd_rn(L.o.y, __fmul_rn(L.d.y, L.tmin)),
+                  __fadd_rn(L.o.z, __fmul_rn(L.d.z, L.tmin))};
+    uint2 node = A.nodes[L.cur];
+    while (!is_leaf(node)) {
+        if (COUNT) c_nodes++;
+        uint32_t axis = node.x & 3u, pair = node.x >> 2;
+        float pl = __int_as_float(node.y);
+        float pc = axis == 0 ? p[0] : (axis == 1 ? p[1] : p[2]);
+        bool below = (pc < pl) || (pc == pl && comp(L.d, axis) <= 0.0f);
+        L.cur = below ? pair : pair + 1;
+        node = A.nodes[L.cur];
+    }
+    const float4 blo = A.cbox[2 * (size_t)L.cur], bhi = A.cbox[2 * (size_t)L.cur + 1];
+    texit = L.te;
+    face = -1;
+    const float o3[3] = {L.o.x, L.o.y, L.o.z}, d3[3] = {L.d.x, L.d.y, L.d.z}, i3[3] = {L.inv.x, L.inv.y, L.inv.z};
+    const float lo3[3] = {blo.x, blo.y, blo.z}, hi3[3] = {bhi.x, bhi.y, bhi.z};
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        if (d3[k] > 0.0f) {
+            float tt = __fmul_rn(__fsub_rn(hi3[k], o3[k]), i3[k]);
+            if (tt < texit) {
+                texit = tt;
+                face = 2 * k + 1;
+            }
+        } else if (d3[k] < 0.0f) {
+            float tt = __fmul_rn(__fsub_rn(lo3[k], o3[k]), i3[k]);
+            if (tt < texit) {
+                texit = tt;
+                face = 2 * k;
+            }
+        }
+    }
+    if (COUNT) c_nodes++;
+    lstart = node.x >> 2;
+    lcnt = node.y;
+    return false;
+}
+
+template <bool ANY>
+__device__ __forceinline__ bool ropes_advance(const SceneView &A, LaneState &L, uint32_t lcnt, float texit, int face) {
+    if (lcnt && (L.best < texit || (ANY && L.best < L.lim))) return true;
+    if (face < 0) return true;
+    uint32_t r = A.ropes[6 * (size_t)L.cur + face];
+    if (r == 0xffffffffu) return true;
+    L.tmin = texit > L.tmin ? texit : L.tmin;
+    L.cur = r;
+    return false;
+}
+
+// the whole leg with the in-order leaf test (occlusion rays, batches)
 template <bool COUNT, bool ANY>
 __device__ __forceinline__ bool leg_ropes(const SceneView &A, LaneState &L, uint32_t legs_max, uint32_t &c_nodes,
                                           uint32_t &c_refs) {
@@ -340,6 +397,66 @@ __device__ __forceinline__ bool leg_ropes(const SceneView &A, LaneState &L, uint
     return false;
 }
 
+// The leaf tests of a whole warp shared out over its 32 lanes (all lanes call
+// it; lane k brings its leaf's reference run start, cnt, with cnt = 0 when it
+// has nothing to test). The warp's (ray, triangle) pairs are numbered in lane
+// order, then leaf order; lane l takes pairs l, l + 32, ... and tests each
+// against its ray's closest hit so far. Each ray keeps the least key
+// (t without its sign bit, position in the leaf, sign bit) in a shared slot:
+// t does not depend on the best hit it is tested against (that only culls),
+// so this is the hit the in-order loop keeps -- the closest, the first in
+// leaf order among equal t -- bit for bit.
+__device__ __forceinline__ void coop_leaf(const SceneView &V, LaneState &L, uint32_t start, uint32_t cnt,
+                                          unsigned long long *slot) {
+    const uint32_t lane = threadIdx.x & 31u;
+    uint32_t P = cnt;   // inclusive prefix of the counts over the lanes
+#pragma unroll
+    for (int dd = 1; dd < 32; dd <<= 1) {
+        const uint32_t u = __shfl_up_sync(0xffffffffu, P, dd);
+        if ((int)lane >= dd) P += u;
+    }
+    const uint32_t W = __shfl_sync(0xffffffffu, P, 31);
+    if (W == 0) return;   // the same on every lane
+    const uint32_t E = P - cnt;
+    for (uint32_t base = 0; base < W; base += 32) {
+        const uint32_t w = base + lane;
+        // owner: the number of lanes whose inclusive prefix is <= w (P rises
+        // and lane 31's exceeds every valid w, so this stays below 32)
+        uint32_t owner = 0;
+#pragma unroll
+        for (uint32_t step = 16; step; step >>= 1) {
+            const uint32_t pv = __shfl_sync(0xffffffffu, P, owner + step - 1);
+            if (pv <= w) owner += step;
+        }
+        const uint32_t j = w - __shfl_sync(0xffffffffu, E, owner);
+        const uint32_t st = __shfl_sync(0xffffffffu, start, owner);
+        const float3 o = make_float3(__shfl_sync(0xffffffffu, L.o.x, owner), __shfl_sync(0xffffffffu, L.o.y, owner),
+                                     __shfl_sync(0xffffffffu, L.o.z, owner));
+        const float3 d = make_float3(__shfl_sync(0xffffffffu, L.d.x, owner), __shfl_sync(0xffffffffu, L.d.y, owner),
+                                     __shfl_sync(0xffffffffu, L.d.z, owner));
+        const float best = __shfl_sync(0xffffffffu, L.best, owner);
+        if (w < W) {
+            const uint32_t tri = __ldg(&V.refs[st + j]);
+            const float t = isect_tri(&V.tris[tri], o, d, best);
+            if (t < best) {
+                const uint32_t tb = __float_as_uint(t);
+                const unsigned long long key =
+                    ((unsigned long long)(tb & 0x7fffffffu) << 32) | ((unsigned long long)j << 1) | (tb >> 31);
+                atomicMin(&slot[owner], key);
+            }
+        }
+    }
+    __syncwarp();
+    const unsigned long long k = slot[lane];
+    if (k != ~0ull) {
+        slot[lane] = ~0ull;
+        const uint32_t j = (uint32_t)(k >> 1) & 0x7fffffffu;
+        L.best = __uint_as_float((uint32_t)(k >> 32) | ((uint32_t)(k & 1u) << 31));
+        L.best_id = (int32_t)__ldg(&V.refs[start + j]);
+    }
+    __syncwarp();
+}
+
 __device__ __forceinline__ unsigned long long global_ns() {
     unsigned long long t;
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
@@ -362,7 +479,7 @@ __device__ __forceinline__ uint32_t scene_of(const uint32_t *off, uint32_t nscen
 // traversal's, so "some hit closer than the light" is found exactly when the
 // closest-hit traversal's answer is closer than the light, in every variant.
 template <int VARIANT, bool COUNT, bool BATCH, bool ANY>
-__global__ void __launch_bounds__(256, 6) k_trace(TraceArgs A) {
+__global__ void __launch_bounds__(256, (VARIANT == HK_TRACE_ROPES && !BATCH && !ANY) ? 5 : 6) k_trace(TraceArgs A) {
     extern __shared__ float smem[];
     const bool smem_ring = (VARIANT == HK_TRACE_SMEMSTACK);
     float *s_s = smem;
@@ -374,6 +491,16 @@ __global__ void __launch_bounds__(256, 6) k_trace(TraceArgs A) {
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t lt_mask = (1u << lane) - 1u;
     uint32_t c_nodes = 0, c_refs = 0;
+    // single-scene closest-hit ropes: leaf tests shared out over the warp
+    // (coop_leaf), one 8-byte slot per lane in dynamic shared memory. Occlusion
+    // rays keep the in-order test, which stops at the first hit closer than
+    // the light.
+    constexpr bool COOP = VARIANT == HK_TRACE_ROPES && !BATCH && !ANY;
+    unsigned long long *slot = reinterpret_cast<unsigned long long *>(smem) + (threadIdx.x & ~31u);
+    if (COOP) {
+        slot[lane] = ~0ull;
+        __syncwarp();
+    }
     const uint32_t n = A.n_dev ? *A.n_dev : A.n;
     if (BATCH && threadIdx.x == 0) atomicMin(A.start_ns, global_ns());
     // scene arrays: launch-uniform for one scene, per lane in a batch
@@ -390,6 +517,11 @@ __global__ void __launch_bounds__(256, 6) k_trace(TraceArgs A) {
         legs_max = VARIANT == HK_TRACE_ROPES ? 4u * (A.rope_nn_dev ? *A.rope_nn_dev : A.rope_nn) + 8u : 0u;
     }
     LaneState L;
+    if (COOP) {
+        // an idle lane's ray fields are shuffled (and ignored) in coop_leaf
+        L.o = L.d = make_float3(0.0f, 0.0f, 0.0f);
+        L.best = kInf;
+    }
     bool active = false, drained = false;
     uint32_t steps = 0;
     while (true) {
@@ -475,7 +607,25 @@ __global__ void __launch_bounds__(256, 6) k_trace(TraceArgs A) {
             if (drained) break;
             continue;
         }
-        if (!active) continue;
+        if (!COOP && !active) continue;
+        if (COOP) {
+            // every lane takes part in the warp's leaf tests
+            uint32_t lstart = 0, lcnt = 0;
+            float texit = 0.0f;
+            int face = -1;
+            bool fin = false;
+            if (active) fin = ropes_locate<COUNT>(V, L, legs_max, c_nodes, lstart, lcnt, texit, face);
+            const uint32_t work = (active && !fin) ? lcnt : 0u;
+            coop_leaf(V, L, lstart, work, slot);
+            if (COUNT) c_refs += work;
+            if (!active) continue;
+            if (fin || ropes_advance<ANY>(V, L, lcnt, texit, face)) {
+                A.hits[L.ray] = hk_hit{L.best, L.best_id};
+                if (A.leaf_out) A.leaf_out[L.ray] = L.cur;
+                active = false;
+            }
+            continue;
+        }
         if (BATCH) {
             const SceneDesc &D = A.scenes[scene];
             V = SceneView{D.nodes, D.refs, D.tris, D.ropes, D.cbox};
@@ -576,6 +726,8 @@ cudaError_t launch_trace(const TraceLaunch &L, cudaStream_t s) {
     int grid = L.grid;
     size_t smem = 0;
     if (L.variant == HK_TRACE_SMEMSTACK) smem = (size_t)L.stack_depth * block * 12;
+    if (L.variant == HK_TRACE_ROPES && !L.scenes && !(L.occlusion && !L.count))
+        smem = (size_t)block * 8;   // coop_leaf slots (the closest-hit ropes kernel)
     switch (L.variant) {
     case HK_TRACE_FULLSTACK: return launch_v<HK_TRACE_FULLSTACK>(a, L.count, L.occlusion, grid, block, smem, s);
     case HK_TRACE_SHORTSTACK: return launch_v<HK_TRACE_SHORTSTACK>(a, L.count, L.occlusion, grid, block, smem, s);
