@@ -190,3 +190,53 @@ def test_render_mirror_bounce(ctx6, hk, oracle, variant):
     oimg = oracle.render_mirror(tree, g["render_rays"], w, h, g["lights"], mirror, ovar, 6, NORM_IEEE)
     assert np.array_equal(img, oimg)
     assert (img != ctx6.render(g["camera"], g["lights"], w, h, hk.VARIANTS[variant])).any()
+
+
+def test_ropes_ties_and_signed_zero(hk):
+    """Closest-hit ropes shares a warp's leaf tests out over its lanes and
+    keeps each ray's hit by (t, position in the leaf): on a floor whose
+    triangles are each listed three times (every hit is a three-way tie), and
+    for rays that start on the floor heading up, away from its -y normal
+    (t = -0.0 on a hit), the ids and the bits of t equal brute force and the
+    in-order full stack."""
+    rng = np.random.default_rng(21)
+    n = 16
+    xs = np.linspace(-4.0, 4.0, n + 1, dtype=np.float32)
+    floor = np.array([[x, 0.0, z, 1.0] for z in xs for x in xs], np.float32)
+    roof = floor.copy()
+    roof[:, 1] = 2.0
+    verts = np.concatenate([floor, roof])
+    quads = []
+    for j in range(n):
+        for i in range(n):
+            a = j * (n + 1) + i
+            quads += [[a, a + 1, a + n + 2, 0], [a, a + n + 2, a + n + 1, 0]]
+    quads = np.array(quads, np.uint32)
+    roof_tris = quads.copy()
+    roof_tris[:, :3] += floor.shape[0]
+    tris = np.concatenate([quads, quads, quads, roof_tris]).astype(np.uint32)   # the floor three times
+    ctx = hk.Context()
+    ctx.upload(verts, tris)
+    ctx.set_box(np.float32([-4, 0, -4, 1, 4, 2, 4, 1]))
+    ctx.precompute()
+    ctx.build()
+    m = 20000
+    rays = np.zeros((2 * m, 8), np.float32)
+    # from between floor and roof, downwards with a tilt (every one lands on the floor)
+    rays[:m, 0] = rng.uniform(-3.0, 3.0, m)
+    rays[:m, 1] = rng.uniform(0.2, 1.8, m)
+    rays[:m, 2] = rng.uniform(-3.0, 3.0, m)
+    d = np.stack([rng.uniform(-0.5, 0.5, m), -np.ones(m), rng.uniform(-0.5, 0.5, m)], 1)
+    rays[:m, 4:7] = d / np.linalg.norm(d, axis=1, keepdims=True)
+    # starting on the floor, heading up: the floor's hit has t = -0.0
+    rays[m:, 0] = rng.uniform(-3.9, 3.9, m)
+    rays[m:, 2] = rng.uniform(-3.9, 3.9, m)
+    rays[m:, 4:7] = rays[:m, 4:7] * np.float32([1, -1, 1])
+    b = ctx.trace(rays, hk.BRUTE)
+    assert (b["tri"][:m] >= 0).all() and (b["tri"][:m] < quads.shape[0]).all()   # the first copy wins
+    assert (np.signbit(b["t"][m:]) & (b["tri"][m:] >= 0)).sum() > m // 2
+    for v in (hk.ROPES, hk.FULLSTACK):
+        h = ctx.trace(rays, v)
+        assert np.array_equal(h["tri"], b["tri"])
+        assert np.array_equal(h["t"].view(np.uint32), b["t"].view(np.uint32))
+    ctx.close()
