@@ -1275,7 +1275,8 @@ hk_status hk_autotune(hk_ctx *c, const float *d_rays8, uint32_t n, const char *c
         for (uint32_t bs : blocks) {
             for (uint32_t ss : stacks) {
                 if (!uses_stack && ss != 6) continue;
-                if (v == HK_TRACE_SMEMSTACK && (size_t)ss * bs * 12 > 48 * 1024) continue;
+                // the shared ring (12 B per level and thread) plus the leaf-test slots (8 B per thread)
+                if (v == HK_TRACE_SMEMSTACK && (size_t)ss * bs * 12 + (size_t)bs * 8 > 48 * 1024) continue;
                 c->cfg.block_size = bs;
                 c->cfg.short_stack = ss;
                 float ms = time_trace(c, rays, n, v, hits.p, 3);

@@ -121,13 +121,23 @@ struct LaneState {
     uint32_t ray;
 };
 
+// A leg run with DEFER leaves its leaf test to the warp (coop_leaf): it
+// records the leaf's reference run and what follows the test -- kDoneIfCloser:
+// finished when the closest hit precedes tmax; kGoOn: not finished; kDone:
+// finished.
+enum : int { kNoTest = 0, kDoneIfCloser = 2, kGoOn = 3, kDone = 4 };
+struct Defer {
+    uint32_t start, cnt;
+    int after;
+};
+
 // one leg of the ring short stack (KDTreeCPU::searchKDTreeStackless,
 // KDTreeCPU.cpp:363-447; GPUTrace_shortStack.cl:6-105; GPUTrace_LDSshortStack.cl:
 // 7-105 with the ring in shared memory, one column per thread); true = finished
-template <bool SMEM, bool COUNT, bool ANY>
+template <bool SMEM, bool COUNT, bool ANY, bool DEFER = false>
 __device__ __forceinline__ bool leg_shortstack(const TraceArgs &A, const SceneView &V, LaneState &L, uint2 root, float *s_s, float *s_e,
                                                uint32_t *s_n, float *l_s, float *l_e, uint32_t *l_n,
-                                               uint32_t &c_nodes, uint32_t &c_refs, uint32_t &steps) {
+                                               uint32_t &c_nodes, uint32_t &c_refs, uint32_t &steps, Defer *df = nullptr) {
     const uint32_t D = A.stack_depth, stride = blockDim.x, tid = threadIdx.x;
     if (!(L.tmax < L.te)) return true;
     if (L.size == 0) {
@@ -186,6 +196,10 @@ __device__ __forceinline__ bool leg_shortstack(const TraceArgs &A, const SceneVi
     }
     if (is_leaf(L.node)) {
         if (COUNT) c_nodes++;
+        if constexpr (DEFER) {
+            *df = Defer{L.node.x >> 2, L.node.y, kDoneIfCloser};
+            return false;
+        }
         test_leaf<COUNT, ANY>(V, L.node, L.o, L.d, L.best, L.best_id, c_refs, L.lim);
         if (L.best < L.tmax || (ANY && L.best < L.lim)) return true;
     }
@@ -195,10 +209,10 @@ __device__ __forceinline__ bool leg_shortstack(const TraceArgs &A, const SceneVi
 // one leg of the full stack (KDTreeCPU::searchKDTree, KDTreeCPU.cpp:285-361 ==
 // GPUTrace.cl:6-90; far children pushed only when they exist), run until a leaf
 // has been tested; true = finished
-template <bool COUNT, bool ANY>
+template <bool COUNT, bool ANY, bool DEFER = false>
 __device__ __forceinline__ bool leg_fullstack(const TraceArgs &A, const SceneView &V, LaneState &L, uint2 root, float *st_s, float *st_e,
                                               uint32_t *st_n, int max_stack, uint32_t &c_nodes, uint32_t &c_refs,
-                                              uint32_t &steps) {
+                                              uint32_t &steps, Defer *df = nullptr) {
     while (true) {
         if (L.best < L.tmin) return true;
         if (COUNT) c_nodes++;
@@ -208,8 +222,13 @@ __device__ __forceinline__ bool leg_fullstack(const TraceArgs &A, const SceneVie
         }
         bool tested = false;
         if (is_leaf(L.node)) {
-            test_leaf<COUNT, ANY>(V, L.node, L.o, L.d, L.best, L.best_id, c_refs, L.lim);
-            if (ANY && L.best < L.lim) return true;
+            if constexpr (DEFER) {
+                // the stack pop below does not depend on the test's outcome
+                *df = Defer{L.node.x >> 2, L.node.y, kGoOn};
+            } else {
+                test_leaf<COUNT, ANY>(V, L.node, L.o, L.d, L.best, L.best_id, c_refs, L.lim);
+                if (ANY && L.best < L.lim) return true;
+            }
             L.cur = 0;
             tested = true;
         } else {
@@ -241,16 +260,19 @@ __device__ __forceinline__ bool leg_fullstack(const TraceArgs &A, const SceneVie
             L.cur = st_n[L.size];
             L.node = V.nodes[L.cur];
         }
-        if (L.cur == 0) return true;
+        if (L.cur == 0) {
+            if (DEFER && tested) df->after = kDone;
+            return true;
+        }
         if (tested) return false;
     }
 }
 
 // one leg of kd-restart (GPUTrace_stackless.cl:53-117 with every leaf resident;
 // EARLY adds the resume path's exit once the closest hit precedes tmax); true = finished
-template <bool EARLY, bool COUNT, bool ANY>
+template <bool EARLY, bool COUNT, bool ANY, bool DEFER = false>
 __device__ __forceinline__ bool leg_restart(const TraceArgs &A, const SceneView &V, LaneState &L, uint2 root, uint32_t &c_nodes,
-                                            uint32_t &c_refs, uint32_t &steps) {
+                                            uint32_t &c_refs, uint32_t &steps, Defer *df = nullptr) {
     if (!(L.tmax < L.te)) return true;
     L.tmin = L.tmax;
     L.tmax = L.te;
@@ -279,6 +301,10 @@ __device__ __forceinline__ bool leg_restart(const TraceArgs &A, const SceneView 
     }
     if (is_leaf(L.node)) {
         if (COUNT) c_nodes++;
+        if constexpr (DEFER) {
+            *df = Defer{L.node.x >> 2, L.node.y, EARLY ? kDoneIfCloser : kGoOn};
+            return false;
+        }
         test_leaf<COUNT, ANY>(V, L.node, L.o, L.d, L.best, L.best_id, c_refs, L.lim);
         if ((EARLY && L.best < L.tmax) || (ANY && L.best < L.lim)) return true;
     }
@@ -479,7 +505,7 @@ __device__ __forceinline__ uint32_t scene_of(const uint32_t *off, uint32_t nscen
 // traversal's, so "some hit closer than the light" is found exactly when the
 // closest-hit traversal's answer is closer than the light, in every variant.
 template <int VARIANT, bool COUNT, bool BATCH, bool ANY>
-__global__ void __launch_bounds__(256, (VARIANT == HK_TRACE_ROPES && !BATCH && !ANY) ? 5 : 6) k_trace(TraceArgs A) {
+__global__ void __launch_bounds__(256, (VARIANT != HK_TRACE_BRUTE && !BATCH && !ANY) ? 5 : 6) k_trace(TraceArgs A) {
     extern __shared__ float smem[];
     const bool smem_ring = (VARIANT == HK_TRACE_SMEMSTACK);
     float *s_s = smem;
@@ -496,8 +522,12 @@ __global__ void __launch_bounds__(256, (VARIANT == HK_TRACE_ROPES && !BATCH && !
     // rays keep the in-order test, which stops at the first hit closer than
     // the light.
     constexpr bool COOP = VARIANT == HK_TRACE_ROPES && !BATCH && !ANY;
-    unsigned long long *slot = reinterpret_cast<unsigned long long *>(smem) + (threadIdx.x & ~31u);
-    if (COOP) {
+    // the stack variants defer their leaf test to the same warp-wide pass
+    constexpr bool COOP_LEG = VARIANT != HK_TRACE_ROPES && VARIANT != HK_TRACE_BRUTE && !BATCH && !ANY;
+    unsigned long long *slot = reinterpret_cast<unsigned long long *>(
+                                   smem + (smem_ring ? 3 * A.stack_depth * blockDim.x : 0u)) +
+                               (threadIdx.x & ~31u);
+    if (COOP || COOP_LEG) {
         slot[lane] = ~0ull;
         __syncwarp();
     }
@@ -517,7 +547,7 @@ __global__ void __launch_bounds__(256, (VARIANT == HK_TRACE_ROPES && !BATCH && !
         legs_max = VARIANT == HK_TRACE_ROPES ? 4u * (A.rope_nn_dev ? *A.rope_nn_dev : A.rope_nn) + 8u : 0u;
     }
     LaneState L;
-    if (COOP) {
+    if (COOP || COOP_LEG) {
         // an idle lane's ray fields are shuffled (and ignored) in coop_leaf
         L.o = L.d = make_float3(0.0f, 0.0f, 0.0f);
         L.best = kInf;
@@ -607,7 +637,7 @@ __global__ void __launch_bounds__(256, (VARIANT == HK_TRACE_ROPES && !BATCH && !
             if (drained) break;
             continue;
         }
-        if (!COOP && !active) continue;
+        if (!COOP && !COOP_LEG && !active) continue;
         if (COOP) {
             // every lane takes part in the warp's leaf tests
             uint32_t lstart = 0, lcnt = 0;
@@ -622,6 +652,33 @@ __global__ void __launch_bounds__(256, (VARIANT == HK_TRACE_ROPES && !BATCH && !
             if (fin || ropes_advance<ANY>(V, L, lcnt, texit, face)) {
                 A.hits[L.ray] = hk_hit{L.best, L.best_id};
                 if (A.leaf_out) A.leaf_out[L.ray] = L.cur;
+                active = false;
+            }
+            continue;
+        }
+        if (COOP_LEG) {
+            // the leg runs up to its leaf, the warp tests every lane's leaf,
+            // then each lane applies what its leg said follows the test
+            Defer df{0u, 0u, kNoTest};
+            bool fin = false;
+            if (active) {
+                if (VARIANT == HK_TRACE_FULLSTACK)
+                    fin = leg_fullstack<COUNT, ANY, true>(A, V, L, root, l_s, l_e, l_n, kLocal, c_nodes, c_refs,
+                                                          steps, &df);
+                else if (VARIANT == HK_TRACE_RESTART)
+                    fin = leg_restart<false, COUNT, ANY, true>(A, V, L, root, c_nodes, c_refs, steps, &df);
+                else if (VARIANT == HK_TRACE_RESTART_EARLY)
+                    fin = leg_restart<true, COUNT, ANY, true>(A, V, L, root, c_nodes, c_refs, steps, &df);
+                else
+                    fin = leg_shortstack<smem_ring, COUNT, ANY, true>(A, V, L, root, s_s, s_e, s_n, l_s, l_e, l_n,
+                                                                      c_nodes, c_refs, steps, &df);
+            }
+            const uint32_t work = (active && df.after != kNoTest) ? df.cnt : 0u;
+            coop_leaf(V, L, df.start, work, slot);
+            if (COUNT) c_refs += work;
+            if (!active) continue;
+            if (fin || df.after == kDone || (df.after == kDoneIfCloser && L.best < L.tmax)) {
+                A.hits[L.ray] = hk_hit{L.best, L.best_id};
                 active = false;
             }
             continue;
@@ -726,8 +783,8 @@ cudaError_t launch_trace(const TraceLaunch &L, cudaStream_t s) {
     int grid = L.grid;
     size_t smem = 0;
     if (L.variant == HK_TRACE_SMEMSTACK) smem = (size_t)L.stack_depth * block * 12;
-    if (L.variant == HK_TRACE_ROPES && !L.scenes && !(L.occlusion && !L.count))
-        smem = (size_t)block * 8;   // coop_leaf slots (the closest-hit ropes kernel)
+    if (L.variant != HK_TRACE_BRUTE && !L.scenes && !(L.occlusion && !L.count))
+        smem += (size_t)block * 8;   // coop_leaf slots (the closest-hit single-scene kernels)
     switch (L.variant) {
     case HK_TRACE_FULLSTACK: return launch_v<HK_TRACE_FULLSTACK>(a, L.count, L.occlusion, grid, block, smem, s);
     case HK_TRACE_SHORTSTACK: return launch_v<HK_TRACE_SHORTSTACK>(a, L.count, L.occlusion, grid, block, smem, s);
