@@ -505,7 +505,7 @@ __device__ __forceinline__ uint32_t scene_of(const uint32_t *off, uint32_t nscen
 // traversal's, so "some hit closer than the light" is found exactly when the
 // closest-hit traversal's answer is closer than the light, in every variant.
 template <int VARIANT, bool COUNT, bool BATCH, bool ANY>
-__global__ void __launch_bounds__(256, (VARIANT != HK_TRACE_BRUTE && !BATCH && !ANY) ? 5 : 6) k_trace(TraceArgs A) {
+__global__ void __launch_bounds__(256, BATCH ? 4 : ((VARIANT != HK_TRACE_BRUTE && !ANY) ? 5 : 6)) k_trace(TraceArgs A) {
     extern __shared__ float smem[];
     const bool smem_ring = (VARIANT == HK_TRACE_SMEMSTACK);
     float *s_s = smem;
