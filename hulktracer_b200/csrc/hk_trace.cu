@@ -6,7 +6,8 @@
 // count and uneven ray batches balance themselves. Traversal semantics follow
 // the reference kernels exactly (comparison operators, near/far rule, the
 // "child 0" sentinel, strict < between hits in leaf order); see the comments
-// at each variant.
+// at each variant. Closest-hit single-scene launches test the leaves of a
+// whole warp together (coop_leaf), which keeps the same hits bit for bit.
 #include "hk_common.cuh"
 #include "hk_internal.h"
 
