@@ -9,10 +9,19 @@ frame's matrices. Rays counted = primary + shadow rays traced.
 
 value   : device time (CUDA events on the frame's stream), scene resident in
           HBM, L2 flushed (256 MB write) between frames.
-e2e     : the same frames through the C ABI with host inputs: per frame the
-          part matrices, camera and lights are copied from pinned host memory
-          and the image is read back to pinned host memory, inside the timed
-          region.
+e2e     : the same frames through the C ABI with host inputs, timed by the
+          host clock: per frame a synchronise, then the call (part matrices,
+          camera and lights copied from pinned host memory), the image read
+          back to pinned host memory and a final synchronise, all inside the
+          timed span; the L2 flush stays outside it.
+compare : the metric's comparison, on rank 0 over the same frames: the GPU
+          engine with the 32-bin binned SAH (the headline), with the learned
+          split proposer, and with the exact SAH on nodes of up to 1024
+          references ("exact"), each with build ms, trace + shade ms, ms per
+          frame and the SAH cost of one frame's tree (hk_tree_cost), against
+          the cost of the reference's own SAH-NlogN tree of that frame (the
+          compiled reference with the same constants, from the CPU-baseline
+          leg), plus learned_speedup_vs_exact and learned_cost_vs_exact.
 roofline: the trace kernel (primary rays) on the last frame's tree:
           algorithmic bytes per ray 32 + 8 + 8 N_node + 4 N_ref + 36 N_tri with
           the per-ray counts measured by the kernel's counting mode.
@@ -54,6 +63,8 @@ def parse():
                                                       "weights", "proposer.bin"),
                     help="trained proposer weights (learned mode)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-compare", action="store_true", help="skip the learned / exact comparison arms")
+    ap.add_argument("--cost-frame", type=int, default=17, help="frame whose trees are costed in the comparison")
     ap.add_argument("--cpu-frames", type=int, default=2)
     return ap.parse_args()
 
@@ -151,6 +162,23 @@ def reference_frame(R, O, sc, f, prim, nthreads):
     nhit = int((img != 0).sum())
     npoint = int((sc.lights[:, 3] == 1.0).sum())
     return dt, sc.width * sc.height + nhit * npoint
+
+
+def reference_tree(sc, frame):
+    """The reference's own SAH-NlogN tree of one frame, built by the compiled
+    reference with the benchmark constants (Ct 1, Ci 1.5, depth 24, leaves of
+    at most 4, no subsampling): (nodes4, refs, verts, box), or None."""
+    from oracle.oracle import Oracle, Reference
+    if not Reference.available(cfg=True):
+        return None
+    O = Oracle()
+    mats = frame_mats(sc, frame)
+    verts = O.transform(sc.rest_verts, sc.part_of_vertex, mats) if mats is not None else sc.verts
+    box = O.scene_box(verts)
+    R = Reference(cfg=True)
+    R.load(verts, sc.tris, box)
+    nodes, refs, _ = R.build()
+    return nodes, refs, verts, box
 
 
 def cpu_baseline(sc, frames, nthreads):
@@ -288,19 +316,19 @@ def run_ours(args):
         torch.cuda.synchronize()
         cl = clocks.stop()
         t_dev = sum(e0.elapsed_time(e1) for e0, e1 in ev) / 1000.0
-        # ---- e2e: host inputs in, image out, through the C ABI ----
+        # ---- e2e: host inputs in, image out, through the C ABI, host clock ----
         if world > 1:
             dist.barrier()
         torch.cuda.synchronize()
-        ev2 = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in frames]
-        for (e0, e1), f in zip(ev2, frames):
+        t_e2e = 0.0
+        for f in frames:
             flush.zero_()
-            e0.record(stream)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
             do_frame(f)
             pin_img.copy_(rgba, non_blocking=True)
-            e1.record(stream)
-        torch.cuda.synchronize()
-        t_e2e = sum(e0.elapsed_time(e1) for e0, e1 in ev2) / 1000.0
+            stream.synchronize()
+            t_e2e += time.perf_counter() - t0
 
     # ---- max over ranks ----
     (t_dev, t_e2e), total_rays = reduce_job([t_dev, t_e2e], rays, world, device="cuda")
@@ -311,8 +339,17 @@ def run_ours(args):
         roof = trace_roofline(ctx, sc, stream, variant)
 
     base = None
+    ref_cost = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         base = cpu_baseline(sc, args.cpu_frames, os.cpu_count() or 1)
+        if animated and not args.no_compare:
+            rt = reference_tree(sc, args.cost_frame)
+            if rt is not None:
+                ref_cost = reference_tree_cost(hk, rt, local)
+
+    compare = None
+    if rank == 0 and not args.no_compare and animated:
+        compare = compare_arms(args, sc, local, ref_cost)
 
     if rank == 0:
         nl = sc.lights.shape[0]
@@ -327,17 +364,118 @@ def run_ours(args):
                        "traversal": args.variant, "graph": "one CUDA graph per frame",
                        "l2": "flushed (256 MB write) between frames", "parallelism": "frames sharded over %d GPU(s)" % world},
             "e2e": {"value": total_rays / t_e2e / 1e6, "unit": "Mrays/s", "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": W * H * 4, "ms_per_step": 1000.0 * t_e2e / args.steps},
+                    "d2h_bytes_per_step": W * H * 4, "ms_per_step": 1000.0 * t_e2e / args.steps,
+                    "timing": "host clock per frame (synchronise, call, image read-back, synchronise)"},
             "gpu_launches": int(kern_nodes) * args.steps,
             "clocks": cl,
             "roofline": roof,
             "cpu_baseline": base,
+            "compare": compare,
         }
         print(json.dumps(line))
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
     ctx.close()
+
+
+def reference_tree_cost(hk, rt, device):
+    """SAH cost (hk_tree_cost, benchmark constants) of the reference's tree,
+    imported onto its own frame's scene."""
+    nodes, refs, verts, box = rt
+    from hulktracer_b200 import scenes
+    sc = scenes.animated_parts()
+    c = hk.Context(device=device)
+    c.upload(verts, sc.tris)
+    c.set_box(box)
+    c.import_tree(nodes, refs)
+    cost = c.tree_cost(1.0, 1.5)
+    c.close()
+    return cost
+
+
+ARMS = (("binned", "binned", 0), ("learned", "learned", 0), ("exact", "binned", 1024))
+
+
+def compare_arms(args, sc, device, ref_cost):
+    """The metric's comparison on this GPU: the same frames through the same
+    engine with each build (binned 32-bin SAH, learned proposer, exact SAH on
+    nodes of up to 1024 references). Per arm: ms per frame (one CUDA graph per
+    frame, device time, L2 flushed between frames), build ms and trace + shade
+    ms (the stages timed apart, no graph, medians), rays, and the SAH cost of
+    the tree of frame --cost-frame."""
+    import torch
+
+    import hulktracer_b200 as hk
+    W, H = sc.width, sc.height
+    variant = hk.VARIANTS[args.variant]
+    out = {}
+    frames = list(range(args.warmup, args.warmup + args.steps))
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    for name, mode_s, exact_max in ARMS:
+        mode = hk.BUILD_LEARNED if mode_s == "learned" else hk.BUILD_BINNED
+        stream = torch.cuda.Stream()
+        ctx = hk.Context(device=device, exact_max=exact_max)
+        ctx.set_stream(stream.cuda_stream)
+        if mode == hk.BUILD_LEARNED:
+            if not os.path.exists(args.weights):
+                out[name] = {"unavailable": "no trained proposer weights"}
+                ctx.close()
+                continue
+            ctx.mlp_load(args.weights)
+        ctx.upload(sc.verts, sc.tris)
+        ctx.set_parts(sc.part_of_vertex, sc.part_center.shape[0])
+        rgba = torch.zeros(W * H, dtype=torch.int32, device="cuda")
+        with torch.cuda.stream(stream):
+            for f in range(args.warmup):
+                ctx.frame(frame_mats(sc, f), sc.camera, sc.lights, W, H, rgba.data_ptr(), mode, variant, True)
+            stream.synchronize()
+            t_frame, rays = 0.0, 0
+            for f in frames:
+                m = frame_mats(sc, f)
+                flush.zero_()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                ctx.frame(m, sc.camera, sc.lights, W, H, rgba.data_ptr(), mode, variant, True)
+                e1.record(stream)
+                stream.synchronize()
+                t_frame += e0.elapsed_time(e1)
+                p, s_ = ctx.ray_counts()
+                rays += p + s_
+            # stages apart (no graph): build, then trace + shade
+            t_build, t_trace = [], []
+            for f in frames[: min(len(frames), 10)]:
+                ctx.transform(frame_mats(sc, f))
+                flush.zero_()
+                e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+                e0.record(stream)
+                ctx.L.hk_build(ctx.h, mode, None)
+                e1.record(stream)
+                ctx.render_device(sc.camera, sc.lights, W, H, rgba.data_ptr(), variant)
+                e2.record(stream)
+                stream.synchronize()
+                t_build.append(e0.elapsed_time(e1))
+                t_trace.append(e1.elapsed_time(e2))
+            ctx.transform(frame_mats(sc, args.cost_frame))
+            st = ctx.build(mode)
+            cost = ctx.tree_cost(1.0, 1.5)
+            learned_nodes, fallback_nodes = st["learned_nodes"], st["fallback_nodes"]
+        ms = t_frame / len(frames)
+        out[name] = {"build": "%s%s" % (mode_s, ", exact SAH on nodes <= %d refs" % exact_max if exact_max else ""),
+                     "ms_per_frame": ms, "mrays_s": rays / (t_frame / 1000.0) / 1e6,
+                     "build_ms": float(np.median(t_build)), "trace_shade_ms": float(np.median(t_trace)),
+                     "sah_cost": cost, "sah_cost_vs_reference": (cost / ref_cost) if ref_cost else None}
+        if mode == hk.BUILD_LEARNED:
+            out[name].update({"learned_nodes": learned_nodes, "fallback_nodes": fallback_nodes})
+        ctx.close()
+    if "ms_per_frame" in out.get("learned", {}) and "ms_per_frame" in out.get("exact", {}):
+        out["learned_speedup_vs_exact"] = out["exact"]["ms_per_frame"] / out["learned"]["ms_per_frame"]
+        out["learned_cost_vs_exact"] = out["learned"]["sah_cost"] / out["exact"]["sah_cost"]
+        out["learned_speedup_vs_binned"] = out["binned"]["ms_per_frame"] / out["learned"]["ms_per_frame"]
+    out["cost_frame"] = args.cost_frame
+    out["reference_sah_cost"] = ref_cost
+    out["frames"] = [frames[0], frames[-1]]
+    return out
 
 
 def trace_roofline(ctx, sc, stream, variant):

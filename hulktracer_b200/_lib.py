@@ -101,6 +101,7 @@ def load(path: str = LIB_PATH):
         "hk_tree_export": [vp, u32p, u32, u32p, u32, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)],
         "hk_tree_export_compact": [vp, u32p, u32, u32p, u32, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)],
         "hk_tree_stats_get": [vp, C.POINTER(TreeStats)],
+        "hk_tree_cost": [vp, C.c_double, C.c_double, C.POINTER(C.c_double)],
         "hk_trace": [vp, f32p, u32, C.c_int, vp],
         "hk_trace_device": [vp, vp, u32, C.c_int, vp],
         "hk_set_counting": [vp, C.c_int],
@@ -124,6 +125,8 @@ def load(path: str = LIB_PATH):
         "hk_mlp_record": [vp, u32],
         "hk_mlp_dataset": [vp, f32p, vp, u32, C.POINTER(C.c_uint32)],
         "hk_mlp_train": [vp, u32, u32, C.c_float, C.c_uint64, f32p],
+        "hk_set_proposal_log": [vp, C.c_int],
+        "hk_get_proposal_log": [vp, vp, u32, C.POINTER(C.c_uint32)],
         "hk_batch_create": [vp, C.POINTER(C.c_void_p)],
         "hk_batch_destroy": [vp],
         "hk_batch_add_scene": [vp, f32p, u32, u32p, u32, C.POINTER(C.c_uint32)],

@@ -23,8 +23,10 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 # every operation in source order to reproduce the reference bit for bit.
 NVFLAGS = ["-O3", "-lineinfo", "-std=c++17", "-fmad=false", "-Xcompiler", "-fPIC",
            "-Xptxas", "-warn-spills", "-I" + os.path.join(ROOT, "include")]
-# files whose arithmetic has no parity constraint (tensor-core MLP) may contract
-FMAD_OK = {"hk_mlp.cu"}
+# files whose arithmetic has no parity constraint may contract (none: the
+# network's tile code is shared by the builder and hk_mlp_forward, which must
+# agree bit for bit)
+FMAD_OK: set = set()
 
 
 def nvcc() -> str:

@@ -117,6 +117,7 @@ struct hk_ctx {
     DevBuf<uint32_t> rec_rows;
     uint32_t rec_cap = 0;
     bool recording = false;
+    bool prop_log = false;
 };
 
 // current tree arrays (imported or built)
@@ -165,14 +166,14 @@ hk_status hk_config_default(hk_config *cfg) {
     cfg->blocks_per_sm = 0;
     cfg->max_refs = 0;
     cfg->topk = 4;
-    cfg->fallback_ratio = 1.02f;
+    cfg->fallback_ratio = 1.0f;
     cfg->exact_max = 0;
     return HK_OK;
 }
 
 static hk_status validate_config(const hk_config *c) {
     if (c->short_stack < 1 || c->short_stack > 16) return HK_E_ILLEGAL_INPUT;
-    if (c->block_size < 32 || c->block_size > 1024 || (c->block_size % 32)) return HK_E_ILLEGAL_INPUT;
+    if (c->block_size < 32 || c->block_size > kTraceMaxBlock || (c->block_size % 32)) return HK_E_ILLEGAL_INPUT;
     if (c->bins != 32) return HK_E_ILLEGAL_INPUT;
     if (c->max_depth < 1 || c->max_depth > 48) return HK_E_ILLEGAL_INPUT;
     if (!(c->intersect_cost > 0) || !(c->traverse_cost >= 0)) return HK_E_ILLEGAL_INPUT;
@@ -586,6 +587,84 @@ hk_status hk_tree_stats_get(hk_ctx *c, hk_tree_stats *st) {
     return HK_OK;
 }
 
+hk_status hk_set_proposal_log(hk_ctx *c, int enable) {
+    if (!c) return HK_E_ILLEGAL_INPUT;
+    c->prop_log = enable != 0;
+    invalidate_graph(c);
+    return HK_OK;
+}
+
+hk_status hk_get_proposal_log(hk_ctx *c, int32_t *bins8, uint32_t cap_nodes, uint32_t *nn) {
+    if (!c) return HK_E_ILLEGAL_INPUT;
+    if (!c->tree_valid || !c->tree_built || !c->build.prop_log || !c->prop_log)
+        return fail(c, HK_E_STATE, "no logged learned build");
+    cudaSetDevice(c->device);
+    hk_status s = sync_tree_sizes(c);
+    if (s != HK_OK) return s;
+    if (nn) *nn = c->nn;
+    if (!bins8) return HK_OK;
+    if (cap_nodes < c->nn) return fail(c, HK_E_CAPACITY, "log buffer too small");
+    HK_CUDA(c, cudaMemcpyAsync(bins8, c->build.prop_log, (size_t)c->nn * 8 * sizeof(int32_t), cudaMemcpyDeviceToHost,
+                               c->stream));
+    HK_CUDA(c, cudaStreamSynchronize(c->stream));
+    return HK_OK;
+}
+
+// SAH cost of the current tree: sum over reachable junctions of ct A(n) / A(root)
+// plus over leaves of ci |refs(n)| A(n) / A(root), A the full surface area of
+// the node's cell (the scene box split by the planes above it), in double
+// precision. Cells follow the compact layout: pair = below child, pair + 1 =
+// above child; an empty cell (count 0) adds nothing.
+hk_status hk_tree_cost(hk_ctx *c, double ct, double ci, double *cost) {
+    if (!c || !cost) return HK_E_ILLEGAL_INPUT;
+    if (!c->tree_valid) return fail(c, HK_E_STATE, "no tree");
+    cudaSetDevice(c->device);
+    hk_status s = sync_tree_sizes(c);
+    if (s != HK_OK) return s;
+    std::vector<uint2> cn(c->nn);
+    float box[8];
+    HK_CUDA(c, cudaMemcpyAsync(cn.data(), tree_nodes(c), (size_t)c->nn * 8, cudaMemcpyDeviceToHost, c->stream));
+    HK_CUDA(c, cudaMemcpyAsync(box, c->box.p, 32, cudaMemcpyDeviceToHost, c->stream));
+    HK_CUDA(c, cudaStreamSynchronize(c->stream));
+    auto area = [](const float *lo, const float *hi) {
+        const double sx = (double)hi[0] - lo[0], sy = (double)hi[1] - lo[1], sz = (double)hi[2] - lo[2];
+        return 2.0 * (sx * sy + sy * sz + sx * sz);
+    };
+    const double aroot = area(box, box + 4);
+    struct Item {
+        uint32_t i;
+        float lo[3], hi[3];
+    };
+    std::vector<Item> todo;
+    todo.push_back(Item{0, {box[0], box[1], box[2]}, {box[4], box[5], box[6]}});
+    double sum = 0.0;
+    size_t visited = 0;
+    while (!todo.empty()) {
+        const Item it = todo.back();
+        todo.pop_back();
+        if (it.i >= c->nn || ++visited > c->nn) return fail(c, HK_E_BOUNDS, "tree cost: malformed tree");
+        const uint2 n = cn[it.i];
+        const double a = area(it.lo, it.hi);
+        if ((n.x & 3u) == kLeafTag) {
+            sum += ci * (double)n.y * a / aroot;
+            continue;
+        }
+        sum += ct * a / aroot;
+        const uint32_t ax = n.x & 3u, pair = n.x >> 2;
+        float p;
+        memcpy(&p, &n.y, 4);
+        Item b = it, u = it;
+        b.i = pair;
+        b.hi[ax] = p;
+        u.i = pair + 1;
+        u.lo[ax] = p;
+        todo.push_back(u);
+        todo.push_back(b);
+    }
+    *cost = sum;
+    return HK_OK;
+}
+
 // ---------------------------------------------------------------------------
 // build
 // ---------------------------------------------------------------------------
@@ -601,6 +680,7 @@ static BuildParams build_params(hk_ctx *c, hk_build_mode mode) {
     p.fallback_ratio = c->cfg.fallback_ratio;
     p.exact_max = c->cfg.exact_max;
     p.record = c->recording ? 1 : 0;
+    p.prop_log = c->prop_log ? 1 : 0;
     c->build.learn = &c->learn;
     return p;
 }
@@ -738,6 +818,9 @@ static hk_status trace_enqueue(hk_ctx *c, const float4 *d_rays, uint32_t n, cons
     L.occlusion = occlusion;
     L.leaf_out = v == HK_TRACE_ROPES ? leaf_out : nullptr;
     L.block = (int)c->cfg.block_size;
+    if (trace_smem_bytes(L.variant, c->cfg.block_size, L.stack_depth, false, occlusion, L.count) > kTraceMaxSmem)
+        return fail(c, HK_E_ILLEGAL_INPUT,
+                    "shared memory of this traversal exceeds 48 KB (short_stack x block_size x 12 + block_size x 8)");
     int per_sm = c->cfg.blocks_per_sm ? (int)c->cfg.blocks_per_sm : std::max(1, 2048 / L.block);
     L.grid = c->sm_count * per_sm;
     if (c->counting) HK_CUDA(c, cudaMemsetAsync(c->counters.p, 0, 24, c->stream));
@@ -1130,8 +1213,8 @@ hk_status hk_batch_trace_device(hk_batch *b, const float *d_rays8, const uint32_
     hk_ctx *c = b->ctx;
     if (nscenes == 0 || nscenes != b->scenes.size()) return fail(c, HK_E_ILLEGAL_INPUT, "nscenes != scenes in batch");
     if ((int)v < HK_TRACE_FULLSTACK || (int)v > HK_TRACE_BRUTE) return fail(c, HK_E_ILLEGAL_INPUT, "variant");
-    if (v == HK_TRACE_SMEMSTACK && c->cfg.short_stack * c->cfg.block_size * 12 > 48 * 1024)
-        return fail(c, HK_E_ILLEGAL_INPUT, "shared ring too large");
+    if (trace_smem_bytes(v, c->cfg.block_size, c->cfg.short_stack, true, false, c->counting) > kTraceMaxSmem)
+        return fail(c, HK_E_ILLEGAL_INPUT, "shared ring too large (short_stack x block_size x 12 > 48 KB)");
     if (ray_offsets[0] != 0) return fail(c, HK_E_ILLEGAL_INPUT, "ray_offsets[0] must be 0");
     std::vector<uint32_t> rem(nscenes);
     for (uint32_t i = 0; i < nscenes; i++) {
@@ -1276,7 +1359,7 @@ hk_status hk_autotune(hk_ctx *c, const float *d_rays8, uint32_t n, const char *c
             for (uint32_t ss : stacks) {
                 if (!uses_stack && ss != 6) continue;
                 // the shared ring (12 B per level and thread) plus the leaf-test slots (8 B per thread)
-                if (v == HK_TRACE_SMEMSTACK && (size_t)ss * bs * 12 + (size_t)bs * 8 > 48 * 1024) continue;
+                if (trace_smem_bytes(v, bs, ss, false, false, false) > kTraceMaxSmem) continue;
                 c->cfg.block_size = bs;
                 c->cfg.short_stack = ss;
                 float ms = time_trace(c, rays, n, v, hits.p, 3);
@@ -1325,6 +1408,7 @@ static hk_status mlp_alloc(hk_ctx *c) {
 static hk_status mlp_pack(hk_ctx *c) {
     const float *P = c->mlp_params.p;
     HK_CUDA(c, mlp_setup());
+    HK_CUDA(c, build_learn_setup());
     HK_CUDA(c, pack_b(P + kOffW1, kMlpIn, kMlpHid, c->mlp_w1p.p, c->stream));
     HK_CUDA(c, pack_b(P + kOffW2, kMlpHid, kMlpHid, c->mlp_w2p.p, c->stream));
     HK_CUDA(c, pack_b(P + kOffW3, kMlpHid, kMlpHid, c->mlp_w3p.p, c->stream));

@@ -1,10 +1,10 @@
 // hk_build.cu -- GPU KD-tree builder: exact binned SAH (sm_100a).
 //
-// Breadth-first and level-synchronous; three launches per level (five with
+// Breadth-first and level-synchronous; three launches per level (four with
 // the learned proposer). Splits are searched over 32 bins per axis, or, with
 // exact_max (32..1024), over every clipped reference bound for nodes of at
 // most exact_max references (one warp in registers up to 32, one CTA above):
-//   work      large nodes (> 256 references): one CTA per chunk of 2048
+//   work      large nodes (> 256 references): one CTA per chunk of 1024
 //             references builds shared-memory histograms (3 axes x {lo bin,
 //             hi bin, flat-on-plane}) of the clipped reference bounds and
 //             flushes them with atomics; the CTA that finishes a node's last
@@ -13,8 +13,13 @@
 //             node, warp-private histogram, same SAH. Every decision is also
 //             tallied into the level totals (leaf refs, splits, next-level
 //             nodes, child refs) that the capacity guard needs.
-//   [infer, propose]  learned mode: tensor-core MLP on the large nodes'
-//             features, exact costing of the top-k proposals (chunked)
+//   [learn]   learned mode: nodes of 33..1024 references get the binned SAH
+//             and their histogram features in the small-node kernel; then
+//             k_learn runs the tensor-core MLP on them (64-node tiles), takes
+//             the top-k (axis, bin) proposals and costs every clipped
+//             reference bound inside the proposed bins exactly (the exact
+//             SAH restricted to those bins); the cheaper of that and the
+//             binned optimum splits the node
 //   plan      single-pass scan over nodes (decoupled look-back): leaf
 //             reference offsets, child pairs, next-level slots, child
 //             reference offsets; emits compact node entries, cells and ropes,
@@ -38,6 +43,7 @@
 #include "hk_build.h"
 #include "hk_common.cuh"
 #include "hk_internal.h"
+#include "hk_mlp_tile.cuh"
 
 namespace hk {
 
@@ -45,6 +51,7 @@ constexpr uint32_t kBins = 32;
 constexpr uint32_t kSmall = 256;     // nodes with <= kSmall refs: one warp per node
 constexpr uint32_t kChunk = 1024;    // refs per histogram CTA of a large node (4 per thread)
 constexpr uint32_t kWarpExact = 32;  // exact-SAH nodes up to this size: one warp, in registers
+constexpr uint32_t kLearnMax = 1024; // learned mode: nodes of kWarpExact + 1 .. kLearnMax refs are proposer rows
 constexpr uint32_t kHist = 3 * 3 * kBins;
 static_assert(kHist % 4 == 0 && kHist / 4 > 64 && kHist / 4 <= 96, "k_small clears its histogram with 16-byte stores");
 constexpr int kScanThreads = 256;
@@ -439,8 +446,12 @@ struct LevelArgs {
     uint32_t exact_max;     // 0: binned everywhere; else nodes <= exact_max refs take the exact SAH
     // learned proposer
     int learned, record;
-    uint32_t *lrank;        // node slot -> proposer row (0xffffffff: none)
-    float *feat, *logits;
+    uint32_t *learn_slot;   // proposer row -> node slot
+    LearnBin *learn_bin;    // proposer row -> binned decision
+    float *feat;            // proposer row -> features
+    int32_t *prop_log;      // optional: compact node -> its 8 proposed bins
+    uint32_t cap_learn;
+    MlpDevice mlp;
     float *rec_X;
     int32_t *rec_y;
     uint32_t *rec_rows, rec_cap;
@@ -468,7 +479,13 @@ __device__ __forceinline__ bool decidable(const LevelArgs &A, uint32_t cnt) {
 __device__ __forceinline__ bool is_medium(const LevelArgs &A, uint32_t c) {
     return A.exact_max >= kWarpExact && c > kWarpExact && c <= A.exact_max;
 }
-__device__ __forceinline__ bool is_large(const LevelArgs &A, uint32_t c) { return c > kSmall && !is_medium(A, c); }
+__device__ __forceinline__ bool is_large(const LevelArgs &A, uint32_t c) {
+    return c > (A.learned ? kLearnMax : kSmall) && !is_medium(A, c);
+}
+// learned mode: a proposer row (one warp each in k_small, then k_learn)
+__device__ __forceinline__ bool is_learn(const LevelArgs &A, uint32_t c) {
+    return A.learned && c > kWarpExact && c <= kLearnMax;
+}
 
 // root node + references of level 0 (the counters were zeroed by a memset);
 // a root with more than 256 references is the first large node
@@ -489,7 +506,6 @@ __global__ void k_root(LevelArgs A, const float *box, uint32_t nt) {
         l0->n_medium = medium ? 1u : 0u;
         if (large) A.large_slot[0] = 0;
         if (medium) A.medium_slot[0] = 0;
-        if (A.learned) A.lrank[0] = (large && nt > kChunk) ? 0u : 0xffffffffu;
         A.nx_lo[0] = make_float4(box[0], box[1], box[2], 0.0f);
         A.nx_hi[0] = make_float4(box[4], box[5], box[6], 0.0f);
         A.nx_info[0] = make_uint4(0, nt, 0, 0);
@@ -567,66 +583,47 @@ struct GHist {
 };
 
 // ---------------------------------------------------------------------------
-// proposer features of one node (one warp): from at most 64 references taken
-// at a fixed stride, per axis a 32-bin histogram of clipped centroids and
-// 16-bin histograms of clipped lower / upper bounds (fractions of the sample),
-// the extents over the largest extent, depth / max_depth, 4 zeros = 200.
-// Counts are exact small integers, so the order of the shared atomics does
-// not matter.
+// proposer features of one node (one warp), from the node's binned histogram
+// (the counts the binned SAH itself uses, exact integers, so every kernel that
+// builds the histogram gives the same features): per axis the 32 lower-bound
+// bin counts and the 32 upper-bound bin counts as fractions of the node's
+// references (192), the extents over the largest extent (3), depth /
+// max_depth, references / 1024, 3 zeros = 200.
 // ---------------------------------------------------------------------------
-constexpr uint32_t kFeatSample = 64;
-
-__device__ void node_features(const LevelArgs &A, uint4 info, float4 blo, float4 bhi, float *sh, float *out) {
+template <class HistPtr>
+__device__ void hist_features(HistPtr H, uint32_t cnt, float4 blo, float4 bhi, uint32_t level, uint32_t max_depth,
+                              float *out) {
     const uint32_t lane = threadIdx.x & 31u;
-    for (uint32_t i = lane; i < 200; i += 32) sh[i] = 0.0f;
-    __syncwarp();
-    const uint32_t cnt = info.y;
-    const uint32_t S = cnt < kFeatSample ? cnt : kFeatSample;
-    for (uint32_t i = lane; i < S; i += 32) {
-        uint32_t r = info.x + (uint32_t)(((uint64_t)i * cnt) / S);
-        uint32_t tri = A.refs[r];
-        float4 tlo = A.tb_lo[tri], thi = A.tb_hi[tri];
-        for (uint32_t a = 0; a < 3; a++) {
-            float l = c3(blo, a), h = c3(bhi, a), ext = h - l;
-            if (!(ext > 0.0f)) continue;
-            float lo = mxf(c3(tlo, a), l), hi = mnf(c3(thi, a), h);
-            float c = (lo + hi) * 0.5f;
-            int b32 = (int)((c - l) * (32.0f / ext));
-            int blo16 = (int)((lo - l) * (16.0f / ext));
-            int bhi16 = (int)((hi - l) * (16.0f / ext));
-            b32 = b32 < 0 ? 0 : (b32 > 31 ? 31 : b32);
-            blo16 = blo16 < 0 ? 0 : (blo16 > 15 ? 15 : blo16);
-            bhi16 = bhi16 < 0 ? 0 : (bhi16 > 15 ? 15 : bhi16);
-            atomicAdd(&sh[a * 32 + b32], 1.0f);
-            atomicAdd(&sh[96 + a * 32 + blo16], 1.0f);
-            atomicAdd(&sh[96 + a * 32 + 16 + bhi16], 1.0f);
-        }
+    const float inv = cnt ? 1.0f / (float)cnt : 0.0f;
+#pragma unroll
+    for (uint32_t k = 0; k < 6; k++) {
+        const uint32_t i = lane + 32u * k;                 // 0..191
+        const uint32_t a = i >> 6, j = i & 63u;
+        out[i] = (float)H[a * 96 + j] * inv;               // j < 32: lower-bound bins, else upper-bound bins
     }
-    __syncwarp();
-    const float inv = S ? 1.0f / (float)S : 0.0f;
-    for (uint32_t i = lane; i < 192; i += 32) out[i] = sh[i] * inv;
     if (lane == 0) {
-        float ex = bhi.x - blo.x, ey = bhi.y - blo.y, ez = bhi.z - blo.z;
-        float m = fmaxf(ex, fmaxf(ey, ez));
-        float im = m > 0.0f ? 1.0f / m : 0.0f;
+        const float ex = bhi.x - blo.x, ey = bhi.y - blo.y, ez = bhi.z - blo.z;
+        const float m = fmaxf(ex, fmaxf(ey, ez));
+        const float im = m > 0.0f ? 1.0f / m : 0.0f;
         out[192] = ex * im;
         out[193] = ey * im;
         out[194] = ez * im;
-        out[195] = (float)A.level / (float)A.max_depth;
-        out[196] = out[197] = out[198] = out[199] = 0.0f;
+        out[195] = (float)level / (float)max_depth;
+        out[196] = (float)cnt * (1.0f / 1024.0f);
+        out[197] = out[198] = out[199] = 0.0f;
     }
     __syncwarp();
 }
 
-// binned mode, recording: (features, label) of a node the exact SAH split
-__device__ void record_node(const LevelArgs &A, uint4 info, float4 blo, float4 bhi, const Decision &d, float *sh) {
-    if (!A.record || d.axis < 0 || info.y <= kChunk) return;
-    uint32_t row = 0;
-    if ((threadIdx.x & 31u) == 0) row = atomicAdd(A.rec_rows, 1u);
-    row = __shfl_sync(0xffffffffu, row, 0);
-    if (row >= A.rec_cap) return;
-    node_features(A, info, blo, bhi, sh, A.rec_X + (size_t)row * 200);
-    if ((threadIdx.x & 31u) == 0) A.rec_y[row] = d.axis * 32 + d.bin;
+// training label of an exactly searched node: axis * 32 + the bin b of the
+// chosen plane p on its axis (p_b <= p < p_{b+1}, p_k = min + ext * k / 32)
+__device__ __forceinline__ int32_t exact_label(int axis, float p, float4 blo, float4 bhi) {
+    const float l = c3(blo, (uint32_t)axis), h = c3(bhi, (uint32_t)axis), ext = __fsub_rn(h, l);
+    int b = __float2int_rz(__fmul_rn(__fsub_rn(p, l), __fdividef(32.0f, ext)));
+    b = b < 0 ? 0 : (b > (int)kBins - 1 ? (int)kBins - 1 : b);
+    while (b > 0 && p < plane_k(l, ext, (uint32_t)b)) b--;
+    while (b < (int)kBins - 1 && p >= plane_k(l, ext, (uint32_t)b + 1)) b++;
+    return axis * 32 + b;
 }
 
 // ---------------------------------------------------------------------------
@@ -906,7 +903,6 @@ __device__ Decision sah_exact_cta(const LevelArgs &A, uint4 info, float4 blo, fl
 // histogram; the CTA that finishes the node's last chunk evaluates the SAH.
 __global__ void __launch_bounds__(256, 3) k_hist(LevelArgs A) {
     __shared__ uint32_t H[kHist];
-    __shared__ float feat_scratch[200];
     __shared__ ExactCtaSmem XS;
     __shared__ int s_last;
     __shared__ uint32_t s_tally[5];
@@ -921,10 +917,33 @@ __global__ void __launch_bounds__(256, 3) k_hist(LevelArgs A) {
             const uint32_t s = A.medium_slot[item - nch];
             if (s >= nodes) continue;
             const uint4 info = A.n_info[s];
-            const Decision d = sah_exact_cta(A, info, A.n_lo[s], A.n_hi[s], A.ct, A.ci, XS);
+            const float4 blo = A.n_lo[s], bhi = A.n_hi[s];
+            const Decision d = sah_exact_cta(A, info, blo, bhi, A.ct, A.ci, XS);
             if (threadIdx.x == 0) {
                 write_decision(A, s, d);
                 tally.add(d, info.y);
+            }
+            if (A.record && d.axis >= 0 && info.y <= kLearnMax) {
+                // a training row: the node's binned histogram as features, the
+                // bin of the exact plane as label (every thread holds d)
+                for (uint32_t i = threadIdx.x; i < kHist; i += blockDim.x) H[i] = 0;
+                __syncthreads();
+                const float4 inv3 = bin_scale(blo, bhi);
+                for (uint32_t r = info.x + threadIdx.x; r < info.x + info.y; r += blockDim.x) {
+                    const uint32_t tri = A.refs[r];
+                    hist_ref(H, A.tb_lo[tri], A.tb_hi[tri], blo, bhi, inv3);
+                }
+                __syncthreads();
+                if (wib == 0) {
+                    uint32_t row = 0;
+                    if (lane == 0) row = atomicAdd(A.rec_rows, 1u);
+                    row = __shfl_sync(0xffffffffu, row, 0);
+                    if (row < A.rec_cap) {
+                        hist_features(H, info.y, blo, bhi, A.level, A.max_depth, A.rec_X + (size_t)row * 200);
+                        if (lane == 0) A.rec_y[row] = exact_label(d.axis, d.plane, blo, bhi);
+                    }
+                }
+                __syncthreads();
             }
             continue;
         }
@@ -981,32 +1000,20 @@ __global__ void __launch_bounds__(256, 3) k_hist(LevelArgs A) {
             __syncwarp();
             for (uint32_t i = lane; i < kHist; i += 32) G[i] = 0;
             if (lane == 0) A.done[rank] = 0;
-            record_node(A, info, blo, bhi, d, feat_scratch);
         }
         __syncthreads();
     }
     tally_flush(A, tally, s_tally);
 }
 
-// Learned mode: the proposer's features of every proposer row (a large node
-// of more than one chunk), one warp per row.
-__global__ void __launch_bounds__(256) k_feat(LevelArgs A) {
-    __shared__ float FS[8][200];
-    const uint32_t wib = threadIdx.x >> 5;
-    const uint32_t nlarge = min(A.lc->n_large, A.cap_large);
-    const uint32_t nodes = A.lc->nodes;
-    for (uint32_t row = blockIdx.x * 8 + wib; row < nlarge; row += gridDim.x * 8) {
-        const uint32_t s = A.large_slot[row];
-        if (s >= nodes || A.lrank[s] != row) continue;   // not a proposer row
-        node_features(A, A.n_info[s], A.n_lo[s], A.n_hi[s], FS[wib], A.feat + (size_t)row * 200);
-    }
-}
-
 // Small nodes (not splittable, or splittable and neither medium nor large):
 // one warp per node; the exact SAH in registers for nodes of at most 32
-// references when exact_max >= 32 (the WARP_EXACT instantiation), else a
-// warp-private histogram + the binned SAH.
-template <bool WARP_EXACT>
+// references when exact_max >= 32 or in learned mode (the WARP_EXACT
+// instantiations), else a warp-private histogram + the binned SAH. In learned
+// mode (LEARNED) a node of 33..1024 references becomes a proposer row: its
+// binned decision and histogram features are stored for k_learn, which
+// decides it (a node past the row capacity keeps the binned decision).
+template <bool WARP_EXACT, bool LEARNED>
 __global__ void __launch_bounds__(256, 5) k_small(LevelArgs A) {
     __shared__ __align__(16) uint32_t HS[8][kHist];
     __shared__ uint32_t s_tally[5];
@@ -1021,7 +1028,7 @@ __global__ void __launch_bounds__(256, 5) k_small(LevelArgs A) {
         const uint4 info = A.n_info[s];
         const uint32_t cnt = info.y;
         const bool dec = decidable(A, cnt);
-        if (dec && (is_large(A, cnt) || is_medium(A, cnt))) continue;   // k_hist / k_feat + k_propose
+        if (dec && (is_large(A, cnt) || is_medium(A, cnt))) continue;   // k_hist
         if (!dec) {
             if (lane == 0) {
                 const Decision leaf{-1, 0.0f, 0, 0, kInf, 0};
@@ -1051,6 +1058,19 @@ __global__ void __launch_bounds__(256, 5) k_small(LevelArgs A) {
             }
             __syncwarp();
             d = sah_warp(Hw, blo, bhi, cnt, A.ct, A.ci);
+            if (LEARNED && is_learn(A, cnt)) {
+                uint32_t row = 0;
+                if (lane == 0) row = atomicAdd(&A.lc->n_learn, 1u);
+                row = __shfl_sync(0xffffffffu, row, 0);
+                if (row < A.cap_learn) {
+                    if (lane == 0) {
+                        A.learn_slot[row] = s;
+                        A.learn_bin[row] = LearnBin{d.cost, d.plane, d.axis, d.nb, d.na, {0, 0, 0}};
+                    }
+                    hist_features(Hw, cnt, blo, bhi, A.level, A.max_depth, A.feat + (size_t)row * 200);
+                    continue;   // decided and tallied by k_learn
+                }
+            }
         }
         if (lane == 0) {
             write_decision(A, s, d, blo, bhi);
@@ -1062,262 +1082,216 @@ __global__ void __launch_bounds__(256, 5) k_small(LevelArgs A) {
 }
 
 // ---------------------------------------------------------------------------
-// learned proposals. Per proposer row (a large node), the valid planes (those
-// the binned search would cost) with the top-k logits, plus a reference plane
-// -- the middle plane of the node's longest axis -- are costed exactly with
-// the partition's own classification. The references are counted in the
-// node's chunks (one CTA each, counts summed with global atomics); the CTA
-// that finishes the node's last chunk costs the candidates. The cheapest
-// proposal wins unless it costs more than fallback_ratio x the reference
-// plane, in which case that CTA runs the full binned SAH on the node.
+// learned split search (no reference counterpart). For a tile of 64 proposer
+// rows the network (tile_forward) gives 96 logits per row, one per (axis,
+// bin); warp w then takes rows w, w + 8, ... and per row
+//   1. the top-k bins by logit (ties to the lower index; an axis of zero
+//      extent has no valid bin);
+//   2. one pass over the node's references: per proposal (axis a, bin b, the
+//      closed interval [P0, P1] = [p_b, p_{b+1}] with p_0 the node's minimum
+//      and p_32 its maximum) the references whose clipped lower bound lies
+//      below P0 and those whose clipped upper bound lies above P1 are
+//      counted, and the lower bounds, upper bounds and flat references inside
+//      [P0, P1] are listed in shared memory;
+//   3. every listed bound p strictly inside the node is a candidate -- the
+//      exact SAH's candidates that fall in the bin -- with
+//        below = #(lo < P0) + #(listed lo < p) + #(listed flat at p),
+//        above = #(hi > P1) + #(listed hi > p) + #(listed flat at p),
+//      the exact SAH's own counts; the cheapest by (cost, axis, plane) wins;
+//   4. that plane is taken unless it costs more than fallback_ratio x the
+//      binned optimum that k_small found for the node (then the binned
+//      plane); the usual leaf test follows.
+// A proposal whose lists overflow their share of shared memory is not costed.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ bool plane_valid(float l, float ext, float h, uint32_t k, float &pk) {
-    if (!(ext > 0.0f) || k < 1 || k > 31) return false;
-    pk = plane_k(l, ext, k);
-    float pk1 = plane_k(l, ext, k + 1);
-    return pk > l && pk < h && (k == 31 || pk < pk1);
-}
+constexpr int kLearnMaxK = 8;
+constexpr uint32_t kLearnScratch = 2048;   // floats of list space per warp (8 warps: the two stage buffers)
+static_assert(8 * kLearnScratch * 4 <= 2 * kStageWords * 4, "list space overlays the weight stage buffers");
 
-constexpr int kMaxCand = 9;   // top-k (k <= 8) + the reference plane
-
-struct Candidates {
-    int n;          // proposals
-    int has_ref;    // candidate n is the reference plane
-    int axis[kMaxCand];
-    int bin[kMaxCand];
-    float plane[kMaxCand];
-};
-
-// warp 0: the top-k valid planes by logit (ties: lowest index) + reference
-__device__ void select_candidates(const LevelArgs &A, const float *__restrict__ L, float4 blo, float4 bhi,
-                                  Candidates &C) {
+// warp-aggregated append of val (where pred) to list[n ..); n counts past cap
+__device__ __forceinline__ void list_append(float *list, uint32_t cap, uint32_t &n, bool pred, float val) {
     const uint32_t lane = threadIdx.x & 31u;
-    const uint32_t K = A.topk < 8 ? A.topk : 8;
-    float v[3];
-    float pk[3];
-    for (int j = 0; j < 3; j++) {
-        uint32_t c = lane + 32u * j, a = c / 32u, k = c % 32u;
-        float l = c3(blo, a), h = c3(bhi, a);
-        float x = L[c];
-        v[j] = plane_valid(l, __fsub_rn(h, l), h, k, pk[j]) ? (x == x ? x : -INFINITY) : NAN;
+    const uint32_t m = __ballot_sync(0xffffffffu, pred);
+    if (pred) {
+        const uint32_t pos = n + __popc(m & ((1u << lane) - 1u));
+        if (pos < cap) list[pos] = val;
     }
-    int n = 0;
-    for (uint32_t r = 0; r < K; r++) {
-        // lane-local best (NaN = invalid or taken)
-        float bv = NAN;
-        int bc = 1 << 30;
-        for (int j = 0; j < 3; j++)
-            if (v[j] == v[j] && (bv != bv || v[j] > bv)) {
-                bv = v[j];
-                bc = (int)lane + 32 * j;
-            }
-        for (int o = 16; o; o >>= 1) {
-            float ov = __shfl_xor_sync(0xffffffffu, bv, o);
-            int oc = __shfl_xor_sync(0xffffffffu, bc, o);
-            bool take = (ov == ov) && (bv != bv || ov > bv || (ov == bv && oc < bc));
-            if (take) {
-                bv = ov;
-                bc = oc;
-            }
-        }
-        if (bv != bv) break;  // no valid plane left (uniform across the warp)
-        if ((uint32_t)(bc & 31) == lane) {
-            int j = bc >> 5;
-            C.axis[n] = bc / 32;
-            C.bin[n] = bc % 32;
-            C.plane[n] = pk[j];
-            v[j] = NAN;
-        }
-        n++;
-    }
-    if (lane == 0) {
-        float ex = __fsub_rn(bhi.x, blo.x), ey = __fsub_rn(bhi.y, blo.y), ez = __fsub_rn(bhi.z, blo.z);
-        uint32_t la = (ex >= ey && ex >= ez) ? 0 : (ey >= ez ? 1 : 2);
-        float p;
-        C.has_ref = plane_valid(c3(blo, la), __fsub_rn(c3(bhi, la), c3(blo, la)), c3(bhi, la), 16, p) ? 1 : 0;
-        if (C.has_ref) {
-            C.axis[n] = (int)la;
-            C.plane[n] = p;
-            C.bin[n] = 16;
-        }
-        C.n = n;
-    }
-    __syncwarp();
+    n += __popc(m);
 }
 
-__global__ void __launch_bounds__(256, 3) k_propose(LevelArgs A) {
-    __shared__ uint32_t H[kHist];
-    __shared__ ExactCtaSmem XS;
-    __shared__ Candidates C;
-    __shared__ uint32_t s_cnt[2 * kMaxCand];
-    __shared__ int s_last, s_fallback;
+__global__ void __launch_bounds__(256, 1) k_learn(LevelArgs A) {
+    extern __shared__ __align__(16) unsigned char learn_smem[];
     __shared__ uint32_t s_tally[5];
+    __shared__ uint32_t s_stat[2];
+    wait_prior_grid();
     Tally tally;
-    const uint32_t nch = min(A.lc->n_chunks, A.cap_chunks);
-    const uint32_t nmed = min(A.lc->n_medium, A.cap_medium);
-    const uint32_t nodes = A.lc->nodes;
-    for (uint32_t item = blockIdx.x; item < nch + nmed; item += gridDim.x) {
-        if (item >= nch) {
-            // a medium node: the exact SAH, as in the binned build
-            const uint32_t s = A.medium_slot[item - nch];
-            if (s >= nodes) continue;
+    uint32_t n_learned = 0, n_fallback = 0;
+    const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
+    const uint32_t rows = min(A.lc->n_learn, A.cap_learn);
+    const TileSmem S = tile_smem(learn_smem);
+    const uint32_t K = A.topk < (uint32_t)kLearnMaxK ? (A.topk ? A.topk : 1u) : (uint32_t)kLearnMaxK;
+    const uint32_t cap = (kLearnScratch / (3u * K)) & ~7u;
+    float *scratch = reinterpret_cast<float *>(S.stage[0]) + (size_t)wib * kLearnScratch;
+    for (uint32_t row0 = blockIdx.x * kTileRows; row0 < rows; row0 += gridDim.x * kTileRows) {
+        tile_forward(A.mlp, A.feat, row0, rows, S);
+        for (uint32_t rr = wib; rr < (uint32_t)kTileRows && row0 + rr < rows; rr += 8) {
+            const uint32_t row = row0 + rr;
+            const uint32_t s = A.learn_slot[row];
             const uint4 info = A.n_info[s];
-            const Decision d = sah_exact_cta(A, info, A.n_lo[s], A.n_hi[s], A.ct, A.ci, XS);
-            if (threadIdx.x == 0) {
-                write_decision(A, s, d);
-                tally.add(d, info.y);
+            const float4 blo = A.n_lo[s], bhi = A.n_hi[s];
+            const uint32_t cnt = info.y;
+            const LearnBin lb = A.learn_bin[row];
+            const float *Lg = S.logits + rr * kMlpOut;
+            // 1. top-k valid bins
+            float v[3];
+#pragma unroll
+            for (int j = 0; j < 3; j++) {
+                const float x = Lg[32 * j + lane];
+                v[j] = __fsub_rn(c3(bhi, j), c3(blo, j)) > 0.0f ? (x == x ? x : -INFINITY) : NAN;
             }
-            continue;
-        }
-        const uint2 ck = A.chunks[item];
-        const uint32_t rank = ck.x;
-        if (rank >= A.cap_large) continue;  // uniform per CTA
-        const uint32_t s = A.large_slot[rank];
-        if (s >= nodes) continue;
-        const uint4 info = A.n_info[s];
-        const float4 blo = A.n_lo[s], bhi = A.n_hi[s];
-        if (info.y <= kChunk) {
-            // a one-chunk large node (no proposer row): the full binned SAH
-            for (uint32_t i = threadIdx.x; i < kHist; i += blockDim.x) H[i] = 0;
-            __syncthreads();
-            const float4 inv3 = bin_scale(blo, bhi);
-            for (uint32_t r = info.x + threadIdx.x; r < info.x + info.y; r += blockDim.x) {
-                const uint32_t tri = A.refs[r];
-                hist_ref(H, A.tb_lo[tri], A.tb_hi[tri], blo, bhi, inv3);
+            uint32_t pax[kLearnMaxK];
+            float p0[kLearnMaxK], p1[kLearnMaxK];
+            uint32_t np = 0;
+#pragma unroll
+            for (int r = 0; r < kLearnMaxK; r++) {
+                if ((uint32_t)r >= K) break;
+                float bv = NAN;
+                int bc = 1 << 30;
+#pragma unroll
+                for (int j = 0; j < 3; j++)
+                    if (v[j] == v[j] && (bv != bv || v[j] > bv)) {
+                        bv = v[j];
+                        bc = (int)lane + 32 * j;
+                    }
+                for (int o = 16; o; o >>= 1) {
+                    const float ov = __shfl_xor_sync(0xffffffffu, bv, o);
+                    const int oc = __shfl_xor_sync(0xffffffffu, bc, o);
+                    if ((ov == ov) && (bv != bv || ov > bv || (ov == bv && oc < bc))) {
+                        bv = ov;
+                        bc = oc;
+                    }
+                }
+                if (bv != bv) break;   // no valid bin left (uniform across the warp)
+#pragma unroll
+                for (int j = 0; j < 3; j++)
+                    if (bc == (int)lane + 32 * j) v[j] = NAN;
+                const uint32_t a = (uint32_t)bc >> 5, b = (uint32_t)bc & 31u;
+                const float l = c3(blo, a), h = c3(bhi, a), ext = __fsub_rn(h, l);
+                pax[r] = a;
+                p0[r] = b == 0 ? l : plane_k(l, ext, b);
+                p1[r] = b == kBins - 1 ? h : plane_k(l, ext, b + 1);
+                if (A.prop_log && lane == 0 && info.z < A.cap_nodes) A.prop_log[(size_t)info.z * 8 + r] = bc;
+                np++;
             }
-            __syncthreads();
-            if (threadIdx.x < 32) {
-                const Decision d = sah_warp(H, blo, bhi, info.y, A.ct, A.ci);
-                if (threadIdx.x == 0) {
-                    write_decision(A, s, d);
-                    tally.add(d, info.y);
+            // 2. counts and lists over the node's references
+            uint32_t bl[kLearnMaxK], ab[kLearnMaxK], nL[kLearnMaxK], nH[kLearnMaxK], nF[kLearnMaxK];
+#pragma unroll
+            for (int i = 0; i < kLearnMaxK; i++) bl[i] = ab[i] = nL[i] = nH[i] = nF[i] = 0;
+            for (uint32_t base = 0; base < cnt; base += 32) {
+                const bool have = base + lane < cnt;
+                float4 tlo = make_float4(0, 0, 0, 0), thi = tlo;
+                if (have) {
+                    const uint32_t tri = A.refs[info.x + base + lane];
+                    tlo = A.tb_lo[tri];
+                    thi = A.tb_hi[tri];
+                }
+#pragma unroll
+                for (int i = 0; i < kLearnMaxK; i++) {
+                    if ((uint32_t)i >= np) break;
+                    const uint32_t a = pax[i];
+                    const float l = c3(blo, a), h = c3(bhi, a);
+                    const float lo = mxf(c3(tlo, a), l), hi = mnf(c3(thi, a), h);
+                    bl[i] += (have && lo < p0[i]) ? 1u : 0u;
+                    ab[i] += (have && hi > p1[i]) ? 1u : 0u;
+                    const bool inL = have && p0[i] <= lo && lo <= p1[i];
+                    const bool inH = have && p0[i] <= hi && hi <= p1[i];
+                    float *Ls = scratch + (size_t)i * 3 * cap;
+                    list_append(Ls, cap, nL[i], inL, lo);
+                    list_append(Ls + cap, cap, nH[i], inH, hi);
+                    list_append(Ls + 2 * cap, cap, nF[i], inL && lo == hi, lo);
                 }
             }
-            __syncthreads();
-            continue;
-        }
-        if (threadIdx.x < 32) select_candidates(A, A.logits + (size_t)rank * kMlpOut, blo, bhi, C);
-        if (threadIdx.x < 2 * kMaxCand) s_cnt[threadIdx.x] = 0;
-        __syncthreads();
-        const int nc = C.n + C.has_ref;
-        // exact below / above counts of every candidate over this chunk
-        const uint32_t r0 = info.x + ck.y * kChunk, r1 = min(info.x + info.y, r0 + kChunk);
-        uint32_t nb[kMaxCand], na[kMaxCand];
-#pragma unroll
-        for (int i = 0; i < kMaxCand; i++) nb[i] = na[i] = 0;
-        constexpr int kPer = kChunk / 256;
-        uint32_t tris[kPer];
-        float4 tlos[kPer], this_[kPer];
-#pragma unroll
-        for (int k = 0; k < kPer; k++) {
-            const uint32_t r = r0 + threadIdx.x + 256u * k;
-            tris[k] = r < r1 ? A.refs[r] : 0xffffffffu;
-        }
-#pragma unroll
-        for (int k = 0; k < kPer; k++)
-            if (tris[k] != 0xffffffffu) {
-                tlos[k] = A.tb_lo[tris[k]];
-                this_[k] = A.tb_hi[tris[k]];
-            }
-#pragma unroll
-        for (int k = 0; k < kPer; k++) {
-            if (tris[k] == 0xffffffffu) continue;
-            const float4 tlo = tlos[k], thi = this_[k];
-#pragma unroll
-            for (int i = 0; i < kMaxCand; i++) {
-                if (i >= nc) break;
-                const uint32_t a = (uint32_t)C.axis[i];
-                const float l = c3(blo, a), h = c3(bhi, a), p = C.plane[i];
-                const float lo = mxf(c3(tlo, a), l), hi = mnf(c3(thi, a), h);
-                const bool flat_on = (lo == hi) && lo == p;
-                nb[i] += (lo < p || flat_on) ? 1u : 0u;
-                na[i] += (hi > p || flat_on) ? 1u : 0u;
-            }
-        }
-#pragma unroll
-        for (int i = 0; i < kMaxCand; i++) {
-            if (i >= nc) break;
-            uint32_t b = nb[i], a = na[i];
-            for (int o = 16; o; o >>= 1) {
-                b += __shfl_xor_sync(0xffffffffu, b, o);
-                a += __shfl_xor_sync(0xffffffffu, a, o);
-            }
-            if ((threadIdx.x & 31u) == 0) {
-                atomicAdd(&s_cnt[2 * i], b);
-                atomicAdd(&s_cnt[2 * i + 1], a);
-            }
-        }
-        __syncthreads();
-        uint32_t *G = A.hist + (size_t)rank * kHist;   // 2 x 9 counters of the row
-        if (threadIdx.x < 2 * (uint32_t)nc && s_cnt[threadIdx.x]) atomicAdd(&G[threadIdx.x], s_cnt[threadIdx.x]);
-        __threadfence();
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            const uint32_t nchunks = (info.y + kChunk - 1) / kChunk;
-            s_last = (atomicAdd(&A.done[rank], 1u) == nchunks - 1) ? 1 : 0;
-        }
-        __syncthreads();
-        if (!s_last) continue;
-        __threadfence();
-        if (threadIdx.x == 0) {
-            uint32_t cb[kMaxCand], ca[kMaxCand];
-            for (int i = 0; i < nc; i++) {
-                cb[i] = __ldcg(G + 2 * i);
-                ca[i] = __ldcg(G + 2 * i + 1);
-                G[2 * i] = G[2 * i + 1] = 0;   // clean for the next level
-            }
-            A.done[rank] = 0;
+            __syncwarp();
+            // 3. exact costs of the listed candidates
             const float Anode = surf(blo, bhi);
-            auto cost = [&](int i) {
-                float4 bb = bhi, ba = blo;
-                s3(bb, (uint32_t)C.axis[i], C.plane[i]);
-                s3(ba, (uint32_t)C.axis[i], C.plane[i]);
-                float sb = surf(blo, bb), sa = surf(ba, bhi);
-                return __fadd_rn(A.ct, __fmul_rn(A.ci, __fdiv_rn(__fadd_rn(__fmul_rn(sb, (float)cb[i]),
-                                                                            __fmul_rn(sa, (float)ca[i])), Anode)));
-            };
-            int bi = -1;
-            float bc = INFINITY;
-            for (int i = 0; i < C.n; i++) {
-                float ci = cost(i);
-                if (ci < bc) {
-                    bc = ci;
-                    bi = i;
+            float mc = kInf, m_pk = 0.0f;
+            uint32_t m_ax = 3, m_nb = 0, m_na = 0;
+#pragma unroll
+            for (int i = 0; i < kLearnMaxK; i++) {
+                if ((uint32_t)i >= np) break;
+                uint32_t b0 = bl[i], a0 = ab[i];
+                for (int o = 16; o; o >>= 1) {
+                    b0 += __shfl_xor_sync(0xffffffffu, b0, o);
+                    a0 += __shfl_xor_sync(0xffffffffu, a0, o);
+                }
+                if (nL[i] > cap || nH[i] > cap || nF[i] > cap) continue;   // overflowed: not costed
+                const uint32_t a = pax[i];
+                const float l = c3(blo, a), h = c3(bhi, a);
+                const float *Ls = scratch + (size_t)i * 3 * cap, *Hs = Ls + cap, *Fs = Ls + 2 * cap;
+                const uint32_t nl = nL[i], nh = nH[i], nf = nF[i];
+                for (uint32_t q = lane; q < nl + nh; q += 32) {
+                    const float x = q < nl ? Ls[q] : Hs[q - nl];
+                    if (!(x > l && x < h)) continue;
+                    const float pk = __fadd_rn(x, 0.0f);
+                    uint32_t below = b0, above = a0, fon = 0;
+                    for (uint32_t k = 0; k < nl; k++) below += Ls[k] < pk ? 1u : 0u;
+                    for (uint32_t k = 0; k < nh; k++) above += Hs[k] > pk ? 1u : 0u;
+                    for (uint32_t k = 0; k < nf; k++) fon += Fs[k] == pk ? 1u : 0u;
+                    const uint32_t nb = below + fon, na = above + fon;
+                    float4 bb = bhi, ba = blo;
+                    s3(bb, a, pk);
+                    s3(ba, a, pk);
+                    const float sb = surf(blo, bb), sa = surf(ba, bhi);
+                    const float cost = __fadd_rn(
+                        A.ct, __fmul_rn(A.ci, __fdiv_rn(__fadd_rn(__fmul_rn(sb, (float)nb), __fmul_rn(sa, (float)na)),
+                                                        Anode)));
+                    if (cost < mc || (cost == mc && (a < m_ax || (a == m_ax && pk < m_pk)))) {
+                        mc = cost;
+                        m_ax = a;
+                        m_pk = pk;
+                        m_nb = nb;
+                        m_na = na;
+                    }
                 }
             }
-            bool fb = bi < 0 || (C.has_ref && bc > A.fallback_ratio * cost(C.n));
-            s_fallback = fb ? 1 : 0;
-            if (!fb) {
-                Decision d{C.axis[bi], C.plane[bi], cb[bi], ca[bi], bc, C.bin[bi]};
-                if (!(bc < __fmul_rn(A.ci, (float)info.y))) d.axis = -1;
-                write_decision(A, s, d);
-                tally.add(d, info.y);
-                atomicAdd(&A.ctr->learned_nodes, 1u);
+            float bc = mc, bp = m_pk;
+            uint32_t bax = m_ax, blane = lane;
+            for (int off = 16; off; off >>= 1) {
+                const float oc = __shfl_xor_sync(0xffffffffu, bc, off), op = __shfl_xor_sync(0xffffffffu, bp, off);
+                const uint32_t oax = __shfl_xor_sync(0xffffffffu, bax, off), ol = __shfl_xor_sync(0xffffffffu, blane, off);
+                if (oc < bc || (oc == bc && (oax < bax || (oax == bax && (op < bp || (op == bp && ol < blane)))))) {
+                    bc = oc;
+                    bp = op;
+                    bax = oax;
+                    blane = ol;
+                }
+            }
+            const uint32_t nb = __shfl_sync(0xffffffffu, m_nb, blane), na = __shfl_sync(0xffffffffu, m_na, blane);
+            // 4. the proposal's plane, or the binned optimum
+            const bool take = bc < kInf && bc <= __fmul_rn(A.fallback_ratio, lb.cost);
+            Decision d;
+            if (take) {
+                d = Decision{(int)bax, bp, nb, na, bc, 0};
+                if (!(bc < __fmul_rn(A.ci, (float)cnt))) d.axis = -1;
             } else {
-                atomicAdd(&A.ctr->fallback_nodes, 1u);
+                d = Decision{lb.axis, lb.plane, lb.nb, lb.na, lb.cost, 0};
             }
+            if (lane == 0) {
+                write_decision(A, s, d, blo, bhi);
+                tally.add(d, cnt);
+                if (take) n_learned++;
+                else n_fallback++;
+            }
+            __syncwarp();
         }
-        __syncthreads();
-        if (s_fallback) {
-            // the full binned SAH on this node
-            for (uint32_t i = threadIdx.x; i < kHist; i += blockDim.x) H[i] = 0;
-            __syncthreads();
-            const float4 inv3 = bin_scale(blo, bhi);
-            for (uint32_t r = info.x + threadIdx.x; r < info.x + info.y; r += blockDim.x) {
-                uint32_t tri = A.refs[r];
-                hist_ref(H, A.tb_lo[tri], A.tb_hi[tri], blo, bhi, inv3);
-            }
-            __syncthreads();
-            if (threadIdx.x < 32) {
-                Decision d = sah_warp(H, blo, bhi, info.y, A.ct, A.ci);
-                if (threadIdx.x == 0) {
-                    write_decision(A, s, d);
-                    tally.add(d, info.y);
-                }
-            }
-        }
-        __syncthreads();
+        __syncthreads();   // logits and lists are rewritten by the next tile
     }
+    if (threadIdx.x < 2) s_stat[threadIdx.x] = 0;
+    __syncthreads();
+    if (n_learned) atomicAdd(&s_stat[0], n_learned);
+    if (n_fallback) atomicAdd(&s_stat[1], n_fallback);
+    __syncthreads();
+    if (threadIdx.x == 0 && s_stat[0]) atomicAdd(&A.ctr->learned_nodes, s_stat[0]);
+    if (threadIdx.x == 1 && s_stat[1]) atomicAdd(&A.ctr->fallback_nodes, s_stat[1]);
     tally_flush(A, tally, s_tally);
 }
 
@@ -1344,7 +1318,6 @@ __device__ __forceinline__ bool level_over(const LevelArgs &A) {
 // their chunks (few per level, so plain atomics)
 __device__ void child_setup(const LevelArgs &A, uint32_t ns, uint32_t c) {
     const bool dec = c > A.leaf_size && A.level + 1 < A.max_depth;
-    if (A.learned) A.lrank[ns] = 0xffffffffu;
     if (dec && is_medium(A, c)) {
         const uint32_t m = atomicAdd(&A.nlc->n_medium, 1u);
         if (m < A.cap_medium) A.medium_slot[m] = ns;
@@ -1360,7 +1333,6 @@ __device__ void child_setup(const LevelArgs &A, uint32_t ns, uint32_t c) {
         return;
     }
     A.large_slot[rank] = ns;
-    if (A.learned && c > kChunk) A.lrank[ns] = rank;   // a proposer row (medium nodes: exact SAH)
     for (uint32_t k = 0; k < nch; k++) A.chunks[first + k] = make_uint2(rank, k);
 }
 
@@ -1739,11 +1711,12 @@ __global__ void __launch_bounds__(kScanThreads, 6) k_plan_refs(LevelArgs A, uint
 // (programmatic stream serialization); the kernel calls wait_prior_grid()
 // before it reads anything that kernel wrote
 template <class... KArgs, class... Args>
-static cudaError_t launch_pdl(void (*k)(KArgs...), unsigned grid, unsigned block, cudaStream_t st, Args... args) {
+static cudaError_t launch_pdl(void (*k)(KArgs...), unsigned grid, unsigned block, size_t smem, cudaStream_t st,
+                              Args... args) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(grid);
     cfg.blockDim = dim3(block);
-    cfg.dynamicSmemBytes = 0;
+    cfg.dynamicSmemBytes = smem;
     cfg.stream = st;
     cudaLaunchAttribute at[1];
     at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
@@ -1770,7 +1743,7 @@ void build_release(BuildState &S) {
         f(S.n_lo[k]); f(S.n_hi[k]); f(S.n_info[k]); f(S.refs[k]); f(S.ref_node[k]);
     }
     f(S.d_axis); f(S.d_plane); f(S.d_cnt); f(S.d_split); f(S.d_scat);
-    f(S.chunks); f(S.hist); f(S.done); f(S.medium_slot); f(S.lrank); f(S.feat); f(S.logits);
+    f(S.chunks); f(S.hist); f(S.done); f(S.medium_slot); f(S.learn_slot); f(S.learn_bin); f(S.feat); f(S.prop_log);
     f(S.plan_flags); f(S.ref_flags); f(S.plan_done); f(S.plan_agg); f(S.plan_incl); f(S.ref_agg); f(S.ref_incl); f(S.epoch);
     f(S.ctr); f(S.err);
     f(S.out_nodes); f(S.out_refs); f(S.out_ropes); f(S.out_cbox);
@@ -1792,7 +1765,10 @@ hk_status build_prepare(BuildState &S, const BuildParams &p, uint32_t nt, int sm
     uint32_t cap_nodes = (uint32_t)std::min<uint64_t>(std::max<uint64_t>(12ull * nt, 1024ull), kMaxIndex);
     S.p = p;
     S.sm_count = sm_count;
-    if (S.ctr && S.nt == nt && S.cap_refs == cap_refs && S.cap_nodes == cap_nodes) return HK_OK;
+    if (S.ctr && S.nt == nt && S.cap_refs == cap_refs && S.cap_nodes == cap_nodes) {
+        if (p.prop_log && !S.prop_log && dalloc(S.prop_log, (size_t)S.cap_nodes * 8) != cudaSuccess) return HK_E_ALLOC;
+        return HK_OK;
+    }
     build_release(S);
     S.nt = nt;
     S.cap_refs = cap_refs;
@@ -1801,6 +1777,7 @@ hk_status build_prepare(BuildState &S, const BuildParams &p, uint32_t nt, int sm
     S.cap_large = cap_refs / kSmall + 2;
     S.cap_chunks = cap_refs / kChunk + S.cap_large + 2;
     S.cap_medium = cap_refs / (kWarpExact + 1) + 2;
+    S.cap_learn = cap_refs / (kWarpExact + 1) + 2;
     S.plan_tiles = S.cap_level / kPlanTile + 2;
     S.ref_tiles = cap_refs / kTile + 2;
     bool bad = false;
@@ -1822,9 +1799,10 @@ hk_status build_prepare(BuildState &S, const BuildParams &p, uint32_t nt, int sm
     bad |= dalloc(S.hist, (size_t)S.cap_large * kHist) != cudaSuccess;
     bad |= dalloc(S.done, S.cap_large) != cudaSuccess;
     bad |= dalloc(S.medium_slot, S.cap_medium) != cudaSuccess;
-    bad |= dalloc(S.lrank, S.cap_level) != cudaSuccess;
-    bad |= dalloc(S.feat, (size_t)S.cap_large * 200) != cudaSuccess;
-    bad |= dalloc(S.logits, (size_t)S.cap_large * kMlpOut) != cudaSuccess;
+    bad |= dalloc(S.learn_slot, S.cap_learn) != cudaSuccess;
+    bad |= dalloc(S.learn_bin, S.cap_learn) != cudaSuccess;
+    bad |= dalloc(S.feat, (size_t)S.cap_learn * kMlpIn) != cudaSuccess;
+    if (p.prop_log) bad |= dalloc(S.prop_log, (size_t)cap_nodes * 8) != cudaSuccess;
     bad |= dalloc(S.plan_flags, S.plan_tiles) != cudaSuccess;
     bad |= dalloc(S.ref_flags, S.ref_tiles) != cudaSuccess;
     bad |= dalloc(S.plan_done, S.plan_tiles) != cudaSuccess;
@@ -1869,6 +1847,19 @@ hk_status build_ensure_outputs(BuildState &S, BuildOutputs *o) {
     return HK_OK;
 }
 
+cudaError_t build_learn_setup() {
+    static uint64_t attr_set = 0;   // the shared-memory opt-in is per device
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev >= 64 || !((attr_set >> dev) & 1u)) {
+        e = cudaFuncSetAttribute(k_learn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTileSmem);
+        if (e != cudaSuccess) return e;
+        if (dev < 64) attr_set |= 1ull << dev;
+    }
+    return cudaSuccess;
+}
+
 cudaError_t build_launch(BuildState &S, const float4 *verts, const uint4 *tris, uint32_t nt, const float *box,
                          cudaStream_t st) {
     const int G = S.sm_count * 4;
@@ -1903,12 +1894,16 @@ cudaError_t build_launch(BuildState &S, const float4 *verts, const uint4 *tris, 
     A.cap_chunks = S.cap_chunks;
     A.cap_medium = S.cap_medium;
     A.medium_slot = S.medium_slot;
-    A.exact_max = S.p.exact_max;
     A.learned = (S.p.mode == HK_BUILD_LEARNED) ? 1 : 0;
+    // learned mode: nodes up to 32 references take the warp's exact SAH,
+    // 33..1024 the proposer, larger ones the binned SAH (exact_max unused)
+    A.exact_max = A.learned ? 0u : S.p.exact_max;
     A.record = (S.p.mode == HK_BUILD_BINNED && S.p.record && S.learn && S.learn->rec_X) ? 1 : 0;
-    A.lrank = S.lrank;
+    A.learn_slot = S.learn_slot;
+    A.learn_bin = S.learn_bin;
     A.feat = S.feat;
-    A.logits = S.logits;
+    A.cap_learn = S.cap_learn;
+    A.prop_log = (A.learned && S.p.prop_log) ? S.prop_log : nullptr;
     A.fallback_ratio = S.p.fallback_ratio;
     A.topk = S.p.topk;
     if (S.learn) {
@@ -1917,8 +1912,14 @@ cudaError_t build_launch(BuildState &S, const float4 *verts, const uint4 *tris, 
         A.rec_rows = S.learn->rec_rows;
         A.rec_cap = S.learn->rec_cap;
     }
-    if (A.learned && !(S.learn && S.learn->have_mlp)) return cudaErrorInvalidValue;
+    if (A.learned) {
+        if (!(S.learn && S.learn->have_mlp)) return cudaErrorInvalidValue;
+        A.mlp = S.learn->mlp;
+        const cudaError_t e = build_learn_setup();
+        if (e != cudaSuccess) return e;
+    }
     cudaMemsetAsync(S.ctr, 0, sizeof(BuildCounters), st);
+    if (A.prop_log) cudaMemsetAsync(A.prop_log, 0xff, (size_t)S.cap_nodes * 8 * sizeof(int32_t), st);
     // per-rank histograms / done counters start at zero (the kernels clean
     // what they use; this also clears what an aborted build left)
     cudaMemsetAsync(S.hist, 0, (size_t)S.cap_large * kHist * sizeof(uint32_t), st);
@@ -1950,18 +1951,20 @@ cudaError_t build_launch(BuildState &S, const float4 *verts, const uint4 *tris, 
         // binned histograms, or the proposer's features, inference and costing
         cudaEventRecord(S.ev_fork, st);
         cudaStreamWaitEvent(S.aux, S.ev_fork, 0);
-        if (!A.learned) {
-            k_hist<<<G, 256, 0, S.aux>>>(A);
-        } else {
-            k_feat<<<G, 256, 0, S.aux>>>(A);
-            mlp_infer(S.learn->mlp, S.feat, &A.lc->n_large, S.cap_large, S.logits, S.sm_count, S.aux);
-            k_propose<<<G * 2, 256, 0, S.aux>>>(A);
-        }
+        k_hist<<<G, 256, 0, S.aux>>>(A);
         cudaEventRecord(S.ev_join, S.aux);
-        if (A.exact_max >= kWarpExact) launch_pdl(k_small<true>, G * 2, 256, st, A);
-        else launch_pdl(k_small<false>, G * 2, 256, st, A);
+        if (A.learned) {
+            // proposer rows from the small-node kernel, then the network and
+            // the restricted exact search, beside the large nodes' histograms
+            launch_pdl(k_small<true, true>, G * 2, 256, 0, st, A);
+            launch_pdl(k_learn, S.sm_count, 256, kTileSmem, st, A);
+        } else if (A.exact_max >= kWarpExact) {
+            launch_pdl(k_small<true, false>, G * 2, 256, 0, st, A);
+        } else {
+            launch_pdl(k_small<false, false>, G * 2, 256, 0, st, A);
+        }
         cudaStreamWaitEvent(st, S.ev_join, 0);
-        launch_pdl(k_plan_refs, S.sm_count * 6, kScanThreads, st, A, S.plan_flags, static_cast<U5 *>(S.plan_agg),
+        launch_pdl(k_plan_refs, S.sm_count * 6, kScanThreads, 0, st, A, S.plan_flags, static_cast<U5 *>(S.plan_agg),
                    static_cast<U5 *>(S.plan_incl), S.ref_flags, S.ref_agg, S.ref_incl, S.plan_done,
                    &A.lc->plan_ticket);
     }

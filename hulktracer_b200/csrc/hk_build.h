@@ -18,8 +18,10 @@ struct BuildParams {
     int mode = 0;               // hk_build_mode
     uint32_t topk = 4;
     float fallback_ratio = 1.02f;
-    int record = 0;             // binned mode: append (features, label) rows
+    int record = 0;             // binned mode with exact_max >= 33: append (features, label) rows of
+                                // the exactly searched nodes of 33..1024 references
     uint32_t exact_max = 0;     // nodes with at most this many refs (0, or 32..1024) take the exact SAH
+    int prop_log = 0;           // learned mode: log every proposer row's proposed bins by compact node
 };
 
 // learned-proposer buffers owned by the context (device pointers)
@@ -34,6 +36,14 @@ struct LearnBuffers {
 
 constexpr int kMaxLevels = 52;  // max_depth <= 48, plus the level after the last
 
+// the binned SAH's decision for a proposer row (axis -1: leaf, or no plane
+// when cost is infinite)
+struct LearnBin {
+    float cost, plane;
+    int32_t axis;
+    uint32_t nb, na, pad[3];
+};
+
 // counters of one tree level; level L's kernels read lvl[L] and the plan
 // scan that emits its children writes lvl[L + 1], so no bookkeeping launch
 // is needed
@@ -46,6 +56,7 @@ struct LevelCounters {
     uint32_t n_large;           // large nodes (chunked histograms)
     uint32_t n_chunks;          // histogram chunks
     uint32_t n_medium;          // exact-SAH nodes of 33..exact_max refs (one CTA each)
+    uint32_t n_learn;           // learned mode: proposer rows of the level (nodes of 33..1024 refs)
     // tallies of the level's decisions (the capacity guard's inputs)
     uint32_t t_leafrefs, t_leafnodes, t_splits, t_next, t_childrefs;
     // tile tickets of the single-pass scans
@@ -111,10 +122,13 @@ struct BuildState {
     uint32_t *out_refs = nullptr;
     uint32_t *out_ropes = nullptr;               // 6 per node: -x,+x,-y,+y,-z,+z (0xffffffff = none)
     float4 *out_cbox = nullptr;                  // 2 per node: cell min, max
-    // learned proposer: per-level rows (large nodes), their features and logits
-    uint32_t *lrank = nullptr;                   // node slot -> row (0xffffffff: none)
-    float *feat = nullptr;                       // [cap_large][200]
-    float *logits = nullptr;                     // [cap_large][96]
+    // learned proposer: per-level rows (nodes of 33..1024 references), their
+    // node slots, binned decisions and features
+    uint32_t cap_learn = 0;
+    uint32_t *learn_slot = nullptr;              // row -> node slot
+    LearnBin *learn_bin = nullptr;               // row -> the binned SAH's decision
+    float *feat = nullptr;                       // [cap_learn][200]
+    int32_t *prop_log = nullptr;                 // [cap_nodes][8] proposed bins (axis * 32 + bin, -1: none)
     LearnBuffers *learn = nullptr;               // context-owned (weights, recording)
 };
 
@@ -123,6 +137,9 @@ hk_status build_ensure_outputs(BuildState &S, BuildOutputs *o);
 cudaError_t build_launch(BuildState &S, const float4 *verts, const uint4 *tris, uint32_t nt, const float *box,
                          cudaStream_t s);
 hk_status build_read_stats(BuildState &S, cudaStream_t s, hk_tree_stats *st);
+// the learned level kernel's shared-memory opt-in on the current device
+// (done once per device; call before capturing a graph that builds)
+cudaError_t build_learn_setup();
 // device address of the built tree's node count (valid once build_launch ran)
 const uint32_t *build_nodes_total_ptr(const BuildState &S);
 void build_release(BuildState &S);

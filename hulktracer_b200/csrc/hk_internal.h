@@ -57,7 +57,32 @@ struct TraceLaunch {
     unsigned long long *start_ns;
 };
 
+// The trace kernel is compiled for at most kTraceMaxBlock threads per block
+// (its __launch_bounds__) and launched without opting in to more than the
+// default 48 KB of dynamic shared memory.
+constexpr uint32_t kTraceMaxBlock = 256;
+constexpr size_t kTraceMaxSmem = 48 * 1024;
+
+// Whether an instantiation shares its warp's leaf tests (coop_leaf, one
+// 8-byte slot per thread): the closest-hit single-scene kernels of every
+// variant but brute force. Counting launches of occlusion rays take the
+// closest-hit kernel. The kernel and the launcher both use this.
+__host__ __device__ constexpr bool trace_coop_slots(int variant, bool batch, bool any) {
+    return variant != HK_TRACE_BRUTE && !batch && !any;
+}
+
+// dynamic shared memory of one trace launch: the shared-memory ring of
+// SMEMSTACK (12 bytes per thread and ring entry) plus the coop_leaf slots
+__host__ __device__ constexpr size_t trace_smem_bytes(int variant, uint32_t block, uint32_t stack_depth, bool batch,
+                                                      bool occlusion, bool count) {
+    return (variant == HK_TRACE_SMEMSTACK ? (size_t)stack_depth * block * 12 : 0) +
+           (trace_coop_slots(variant, batch, occlusion && !count) ? (size_t)block * 8 : 0);
+}
+
 cudaError_t launch_trace(const TraceLaunch &L, cudaStream_t s);
+// load the closest-hit and occlusion kernels of one variant (single scene, not
+// counting) into the current device's context without launching them
+cudaError_t preload_trace_kernels(int variant);
 
 // hk_shade.cu
 cudaError_t launch_precompute(const float4 *verts, const uint4 *tris, uint32_t nt, TriRec *out,
@@ -78,6 +103,8 @@ cudaError_t launch_shade_cpu(const float4 *rays, const hk_hit *hits, const TriRe
                              const float *lights_dev, uint32_t nl, const uint32_t *slot, const hk_hit *shits,
                              uint32_t *rgba, cudaStream_t s, uint32_t w = 0, bool tiled = false);
 cudaError_t launch_hit4(const hk_hit *hits, const TriRec *tris, uint32_t n, float4 *hit4, cudaStream_t s);
+// load the kernels of the trace + shadow + CPU-shading pipeline's shading side
+cudaError_t preload_render_kernels();
 cudaError_t launch_shade_picture(const float4 *rays, const float4 *hit4, uint32_t n, const float *lights_dev,
                                  uint32_t nl, uint32_t *rgba, cudaStream_t s, uint32_t w = 0, bool tiled = false);
 

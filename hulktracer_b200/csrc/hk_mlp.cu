@@ -1,25 +1,21 @@
 // hk_mlp.cu -- the learned split proposer's network (no reference
 // counterpart): 200 -> 256 -> 256 -> 256 -> 96, ReLU between layers.
 //
-// * Inference: BF16 weights and activations on the tensor cores
-//   (mma.sync m16n8k16, FP32 accumulate). One CTA owns 128 rows (8 warps x
-//   16 rows); activations stay in shared memory between layers; weights are
-//   packed once into the per-lane B-fragment order so that a warp reads each
-//   fragment with one coalesced 8-byte load per lane.
+// * Inference: BF16 weights and activations on the tensor cores, FP32
+//   accumulate, 64-row tiles (hk_mlp_tile.cuh, shared with the builder);
+//   weights are packed once into the per-lane B-fragment order.
 // * Training: FP32 master weights; hand-written tiled SGEMM (with transposed
 //   operands), bias / ReLU epilogues, softmax cross-entropy, ReLU backward,
 //   column sums and Adam. Gradients are checked against a CPU FP32 reference.
 #include <cmath>
 #include <cstdint>
 #include <cuda_bf16.h>
-#include <cooperative_groups.h>
 #include <algorithm>
 
 #include "hk_mlp.h"
+#include "hk_mlp_tile.cuh"
 
 namespace hk {
-
-namespace cg = cooperative_groups;
 
 // ---------------------------------------------------------------------------
 // tiled FP32 GEMM: C[M x N] = op(A) op(B) (+ bias, ReLU); row-major storage
@@ -201,166 +197,33 @@ __device__ __forceinline__ void mma_bf16(float *c, const uint32_t *a, const uint
 }
 
 // ---------------------------------------------------------------------------
-// Inference kernel: a cluster of kClusterN CTAs shares every 64-row tile. CTA
-// r of the cluster owns the r-th quarter of each layer's output columns and
-// keeps the matching slices of all four layers' packed weights resident in
-// shared memory for the whole launch (staged once with 16-byte cp.async). A
-// layer's outputs are written, as BF16, into the activation buffer of every
-// CTA of the cluster (distributed shared memory), and a cluster barrier
-// separates the layers. The logits go straight to global memory.
-// Per tile a warp (row group rg of 16 rows, column half ch) runs m16n8k16
-// MMAs over its CTA's n-tiles; the arithmetic per output element is the same
-// MMA sequence as one CTA computing all columns.
+// Inference over host-visible batches (hk_mlp_forward): 64-row tiles, one CTA
+// each, the same tile_forward the builder's k_learn runs.
 // ---------------------------------------------------------------------------
-constexpr int kClusterN = 4;
-constexpr int kRowsCta = 64;      // 4 row groups of 16 x 2 column halves = 8 warps
-constexpr int kActStride = 264;   // bf16 elements per activation row (256 + 8: conflict-free fragment loads)
-constexpr int kKT1 = kMlpInPad / 16, kKT = kMlpHid / 16;
-constexpr int kNTcH = kMlpHid / 8 / kClusterN;   // hidden n-tiles per CTA (8)
-constexpr int kNTcO = kMlpOut / 8 / kClusterN;   // output n-tiles per CTA (3)
-constexpr size_t kW1Words = (size_t)kKT1 * kNTcH * 32 * 2, kWHWords = (size_t)kKT * kNTcH * 32 * 2,
-                 kW4Words = (size_t)kKT * kNTcO * 32 * 2;
-constexpr size_t kActBytes = 2 * (size_t)kRowsCta * kActStride * 2;
-constexpr size_t kInferSmem = kActBytes + 4 * (kW1Words + 2 * kWHWords + kW4Words);
-static_assert(kMlpHid % (8 * kClusterN) == 0 && kMlpOut % (8 * kClusterN) == 0, "column split");
-
-// this CTA's n-tile slice [r*NTc, (r+1)*NTc) of a packed layer (KT x NT tiles)
-__device__ __forceinline__ void stage_slice(uint32_t *dst, const uint32_t *__restrict__ Wp, int KT, int NT, int NTc,
-                                            int r) {
-    const int chunks = KT * NTc * 16;   // 16 x 16 bytes per (k-tile, n-tile)
-    const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(dst);
-    for (int i = threadIdx.x; i < chunks; i += blockDim.x) {
-        const int tile = i >> 4, part = i & 15;
-        const int kt = tile / NTc, nt = tile % NTc;
-        const uint32_t *src = Wp + ((size_t)(kt * NT + r * NTc + nt) * 32) * 2 + 4 * part;
-        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sbase + 16u * i), "l"(src) : "memory");
-    }
-}
-
-// one layer, this CTA's columns: warp (rg, ch) computes 16 rows x its n-tiles
-// of act(in[16 x K] W + b); hidden layers write BF16 into the act buffer of
-// every CTA of the cluster, the last layer writes FP32 logits
-template <bool LAST>
-__device__ __forceinline__ void cluster_layer(const __nv_bfloat16 *in, int KT, const uint32_t *Ws, int NTc, int r,
-                                              const float *__restrict__ bias, __nv_bfloat16 *const *out,
-                                              float *__restrict__ logits, int row0, int rows) {
-    const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
-    const int warp = threadIdx.x >> 5;
-    const int wrow = (warp & 3) * 16;
-    const int half = (NTc + 1) / 2;
-    const int nt0 = (warp >> 2) * half, nt1 = min(NTc, nt0 + half);
-    if (nt0 >= nt1) return;
-    const uint2 *Wf = reinterpret_cast<const uint2 *>(Ws);
-    float acc[4][4];
-#pragma unroll
-    for (int j = 0; j < 4; j++) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.0f;
-    const int nj = nt1 - nt0;
-    for (int kt = 0; kt < KT; kt++) {
-        const int c = kt * 16 + 2 * t;
-        uint32_t a[4];
-        a[0] = *reinterpret_cast<const uint32_t *>(in + (wrow + g) * kActStride + c);
-        a[1] = *reinterpret_cast<const uint32_t *>(in + (wrow + g + 8) * kActStride + c);
-        a[2] = *reinterpret_cast<const uint32_t *>(in + (wrow + g) * kActStride + c + 8);
-        a[3] = *reinterpret_cast<const uint32_t *>(in + (wrow + g + 8) * kActStride + c + 8);
-#pragma unroll
-        for (int j = 0; j < 4; j++) {
-            if (j >= nj) break;
-            const uint2 bf = Wf[(size_t)(kt * NTc + nt0 + j) * 32 + lane];
-            uint32_t b[2] = {bf.x, bf.y};
-            mma_bf16(acc[j], a, b);
-        }
-    }
-#pragma unroll
-    for (int j = 0; j < 4; j++) {
-        if (j >= nj) break;
-        const int col = (r * NTc + nt0 + j) * 8 + 2 * t;
-        float v0 = acc[j][0] + bias[col], v1 = acc[j][1] + bias[col + 1];
-        float v2 = acc[j][2] + bias[col], v3 = acc[j][3] + bias[col + 1];
-        if (LAST) {
-            const int rr = row0 + wrow + g;
-            if (rr < rows) {
-                logits[(size_t)rr * kMlpOut + col] = v0;
-                logits[(size_t)rr * kMlpOut + col + 1] = v1;
-            }
-            if (rr + 8 < rows) {
-                logits[(size_t)(rr + 8) * kMlpOut + col] = v2;
-                logits[(size_t)(rr + 8) * kMlpOut + col + 1] = v3;
-            }
-        } else {
-            const __nv_bfloat162 lo = __floats2bfloat162_rn(fmaxf(v0, 0.0f), fmaxf(v1, 0.0f));
-            const __nv_bfloat162 hi = __floats2bfloat162_rn(fmaxf(v2, 0.0f), fmaxf(v3, 0.0f));
-#pragma unroll
-            for (int q = 0; q < kClusterN; q++) {
-                *reinterpret_cast<__nv_bfloat162 *>(out[q] + (wrow + g) * kActStride + col) = lo;
-                *reinterpret_cast<__nv_bfloat162 *>(out[q] + (wrow + g + 8) * kActStride + col) = hi;
-            }
-        }
-    }
-}
-
-__global__ void __cluster_dims__(kClusterN, 1, 1) __launch_bounds__(256)
-    k_mlp_infer(MlpDevice M, const float *__restrict__ X, const uint32_t *rows_dev, uint32_t rows_host,
-                float *__restrict__ logits) {
-    extern __shared__ __align__(16) unsigned char sm_raw[];
-    cg::cluster_group cluster = cg::this_cluster();
-    const int r = (int)cluster.block_rank();
-    __nv_bfloat16 *act0 = reinterpret_cast<__nv_bfloat16 *>(sm_raw);
-    __nv_bfloat16 *act1 = act0 + kRowsCta * kActStride;
-    uint32_t *w1 = reinterpret_cast<uint32_t *>(sm_raw + kActBytes);
-    uint32_t *w2 = w1 + kW1Words, *w3 = w2 + kWHWords, *w4 = w3 + kWHWords;
-    // rows_dev (device count, e.g. written by the builder) is clamped to
-    // rows_host, the capacity of X and logits; the same for every CTA
-    const int rows = (int)(rows_dev ? min(*rows_dev, rows_host) : rows_host);
-    const int nclusters = (int)(gridDim.x / kClusterN);
-    const int cid = (int)(blockIdx.x / kClusterN);
-    if (cid * kRowsCta >= rows) return;   // no tile for this cluster (uniform across it)
-    // the activation buffers of every CTA of the cluster
-    __nv_bfloat16 *out0[kClusterN], *out1[kClusterN];
-#pragma unroll
-    for (int q = 0; q < kClusterN; q++) {
-        out0[q] = cluster.map_shared_rank(act0, q);
-        out1[q] = cluster.map_shared_rank(act1, q);
-    }
-    stage_slice(w1, M.w1p, kKT1, kMlpHid / 8, kNTcH, r);
-    stage_slice(w2, M.w2p, kKT, kMlpHid / 8, kNTcH, r);
-    stage_slice(w3, M.w3p, kKT, kMlpHid / 8, kNTcH, r);
-    stage_slice(w4, M.w4p, kKT, kMlpOut / 8, kNTcO, r);
-    asm volatile("cp.async.commit_group;\n" ::: "memory");
-    bool waited = false;
-    for (int row0 = cid * kRowsCta; row0 < rows; row0 += nclusters * kRowsCta) {
-        // the tile's rows as BF16 (features 200 -> padded 208 with zeros), in
-        // every CTA (each needs all input columns)
-        for (int i = threadIdx.x; i < kRowsCta * kMlpInPad; i += blockDim.x) {
-            const int rr = i / kMlpInPad, c = i % kMlpInPad;
-            const float v = (row0 + rr < rows && c < kMlpIn) ? X[(size_t)(row0 + rr) * kMlpIn + c] : 0.0f;
-            act0[rr * kActStride + c] = __float2bfloat16_rn(v);
-        }
-        if (!waited) {
-            asm volatile("cp.async.wait_group 0;\n" ::: "memory");
-            waited = true;
+__global__ void __launch_bounds__(256, 1)
+    k_mlp_fwd(MlpDevice M, const float *__restrict__ X, const uint32_t *rows_dev, uint32_t rows_host,
+              float *__restrict__ logits) {
+    extern __shared__ __align__(16) unsigned char fwd_smem[];
+    const TileSmem S = tile_smem(fwd_smem);
+    const uint32_t rows = rows_dev ? min(*rows_dev, rows_host) : rows_host;
+    for (uint32_t row0 = blockIdx.x * kTileRows; row0 < rows; row0 += gridDim.x * kTileRows) {
+        tile_forward(M, X, row0, rows, S);
+        for (uint32_t i = threadIdx.x; i < (uint32_t)kTileRows * kMlpOut; i += blockDim.x) {
+            const uint32_t r = row0 + i / kMlpOut;
+            if (r < rows) logits[(size_t)r * kMlpOut + i % kMlpOut] = S.logits[i];
         }
         __syncthreads();
-        cluster_layer<false>(act0, kKT1, w1, kNTcH, r, M.b1, out1, nullptr, row0, rows);
-        cluster.sync();
-        cluster_layer<false>(act1, kKT, w2, kNTcH, r, M.b2, out0, nullptr, row0, rows);
-        cluster.sync();
-        cluster_layer<false>(act0, kKT, w3, kNTcH, r, M.b3, out1, nullptr, row0, rows);
-        cluster.sync();
-        cluster_layer<true>(act1, kKT, w4, kNTcO, r, M.b4, nullptr, logits, row0, rows);
-        cluster.sync();   // act0 / act1 are rewritten by the next tile
     }
-    if (!waited) asm volatile("cp.async.wait_group 0;\n" ::: "memory");
 }
 
 cudaError_t mlp_setup() {
-    // the attribute is per device; set it once for each
+    // the shared-memory opt-in is per device; set it once for each
     static uint64_t attr_set = 0;
-    const size_t smem = kInferSmem;
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     if (dev >= 64 || !((attr_set >> dev) & 1u)) {
-        e = cudaFuncSetAttribute(k_mlp_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        e = cudaFuncSetAttribute(k_mlp_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTileSmem);
         if (e != cudaSuccess) return e;
         if (dev < 64) attr_set |= 1ull << dev;
     }
@@ -371,10 +234,9 @@ cudaError_t mlp_infer(const MlpDevice &M, const float *X, const uint32_t *rows_d
                       int grid, cudaStream_t s) {
     cudaError_t e = mlp_setup();
     if (e != cudaSuccess) return e;
-    // whole clusters; pass the SM count: one CTA per SM fits (the shared
-    // memory holds a quarter of the weights)
-    const int g = std::max(kClusterN, (grid / kClusterN) * kClusterN);
-    k_mlp_infer<<<g, 256, kInferSmem, s>>>(M, X, rows_dev, rows_host, logits);
+    const uint32_t tiles = (rows_host + kTileRows - 1) / kTileRows;
+    const int g = (int)std::max<uint32_t>(1u, std::min<uint32_t>(tiles, (uint32_t)grid));
+    k_mlp_fwd<<<g, 256, kTileSmem, s>>>(M, X, rows_dev, rows_host, logits);
     return cudaGetLastError();
 }
 

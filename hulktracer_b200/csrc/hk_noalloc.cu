@@ -18,9 +18,14 @@
 //
 // Host code cannot use the array's name as a device address (it is a host-side
 // stand-in), so the first call on each device looks the address up with
-// cudaGetSymbolAddress while that device is current and caches it; make that
-// first call before any stream capture begins. No cudaMalloc, cudaFree or
-// allocating library routine is called.
+// cudaGetSymbolAddress while that device is current and caches it. The same
+// first call also loads every kernel the entry point can launch (all accepted
+// traversal variants, closest-hit and occlusion, and the ray / shading
+// kernels): with lazy module loading the driver would otherwise allocate
+// module memory when a variant is first launched, possibly while another
+// component's stream capture is open. Make that first call before any stream
+// capture begins. No cudaMalloc, cudaFree or allocating library routine is
+// called.
 #include <cstring>
 #include <mutex>
 
@@ -72,6 +77,11 @@ hk_status device_scratch(unsigned char **out, int *sm) {
     if (!g_scratch_dev[dev]) {
         void *p = nullptr;
         if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return HK_E_CUDA;
+        const int variants[] = {HK_TRACE_FULLSTACK, HK_TRACE_SHORTSTACK, HK_TRACE_SMEMSTACK,
+                                HK_TRACE_RESTART,   HK_TRACE_RESTART_EARLY, HK_TRACE_BRUTE};
+        for (int v : variants)
+            if (hk::preload_trace_kernels(v) != cudaSuccess) return HK_E_CUDA;
+        if (hk::preload_render_kernels() != cudaSuccess) return HK_E_CUDA;
         int n = 0;
         if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return HK_E_CUDA;
         g_scratch_dev[dev] = static_cast<unsigned char *>(p);

@@ -363,6 +363,17 @@ cudaError_t launch_shade_cpu(const float4 *rays, const hk_hit *hits, const TriRe
     return cudaGetLastError();
 }
 
+// loads the camera-ray, shadow-ray and CPU-shading kernels into the current
+// device's context (the driver loads a kernel lazily, allocating module
+// memory, at its first launch otherwise)
+cudaError_t preload_render_kernels() {
+    cudaFuncAttributes fa;
+    cudaError_t e = cudaFuncGetAttributes(&fa, k_camera_rays);
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k_shadow_rays);
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k_shade_cpu);
+    return e;
+}
+
 // ---------------------------------------------------------------------------
 // ShadePicture (shadePicture.cl:7-55): float4(normal, t) per pixel, misses
 // t = FLT_MAX (SetInitialValues, GPU_setValues.cl:4-11)

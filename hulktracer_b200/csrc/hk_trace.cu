@@ -506,7 +506,8 @@ __device__ __forceinline__ uint32_t scene_of(const uint32_t *off, uint32_t nscen
 // traversal's, so "some hit closer than the light" is found exactly when the
 // closest-hit traversal's answer is closer than the light, in every variant.
 template <int VARIANT, bool COUNT, bool BATCH, bool ANY>
-__global__ void __launch_bounds__(256, BATCH ? 4 : ((VARIANT != HK_TRACE_BRUTE && !ANY) ? 5 : 6)) k_trace(TraceArgs A) {
+__global__ void __launch_bounds__(kTraceMaxBlock, BATCH ? 4 : ((VARIANT != HK_TRACE_BRUTE && !ANY) ? 5 : 6))
+    k_trace(TraceArgs A) {
     extern __shared__ float smem[];
     const bool smem_ring = (VARIANT == HK_TRACE_SMEMSTACK);
     float *s_s = smem;
@@ -522,9 +523,9 @@ __global__ void __launch_bounds__(256, BATCH ? 4 : ((VARIANT != HK_TRACE_BRUTE &
     // (coop_leaf), one 8-byte slot per lane in dynamic shared memory. Occlusion
     // rays keep the in-order test, which stops at the first hit closer than
     // the light.
-    constexpr bool COOP = VARIANT == HK_TRACE_ROPES && !BATCH && !ANY;
+    constexpr bool COOP = VARIANT == HK_TRACE_ROPES && trace_coop_slots(VARIANT, BATCH, ANY);
     // the stack variants defer their leaf test to the same warp-wide pass
-    constexpr bool COOP_LEG = VARIANT != HK_TRACE_ROPES && VARIANT != HK_TRACE_BRUTE && !BATCH && !ANY;
+    constexpr bool COOP_LEG = VARIANT != HK_TRACE_ROPES && trace_coop_slots(VARIANT, BATCH, ANY);
     unsigned long long *slot = reinterpret_cast<unsigned long long *>(
                                    smem + (smem_ring ? 3 * A.stack_depth * blockDim.x : 0u)) +
                                (threadIdx.x & ~31u);
@@ -750,6 +751,26 @@ static cudaError_t launch_v(const TraceArgs &a, bool count, bool occlusion, int 
     return cudaGetLastError();
 }
 
+template <int V>
+static cudaError_t preload_v() {
+    cudaFuncAttributes fa;
+    cudaError_t e = cudaFuncGetAttributes(&fa, k_trace<V, false, false, false>);
+    return e == cudaSuccess ? cudaFuncGetAttributes(&fa, k_trace<V, false, false, true>) : e;
+}
+
+cudaError_t preload_trace_kernels(int variant) {
+    switch (variant) {
+    case HK_TRACE_FULLSTACK: return preload_v<HK_TRACE_FULLSTACK>();
+    case HK_TRACE_SHORTSTACK: return preload_v<HK_TRACE_SHORTSTACK>();
+    case HK_TRACE_SMEMSTACK: return preload_v<HK_TRACE_SMEMSTACK>();
+    case HK_TRACE_RESTART: return preload_v<HK_TRACE_RESTART>();
+    case HK_TRACE_RESTART_EARLY: return preload_v<HK_TRACE_RESTART_EARLY>();
+    case HK_TRACE_ROPES: return preload_v<HK_TRACE_ROPES>();
+    case HK_TRACE_BRUTE: return preload_v<HK_TRACE_BRUTE>();
+    default: return cudaErrorInvalidValue;
+    }
+}
+
 cudaError_t launch_trace(const TraceLaunch &L, cudaStream_t s) {
     TraceArgs a;
     a.nodes = L.nodes;
@@ -782,10 +803,9 @@ cudaError_t launch_trace(const TraceLaunch &L, cudaStream_t s) {
     if (L.n == 0 && L.n_dev == nullptr) return cudaSuccess;
     int block = L.block;
     int grid = L.grid;
-    size_t smem = 0;
-    if (L.variant == HK_TRACE_SMEMSTACK) smem = (size_t)L.stack_depth * block * 12;
-    if (L.variant != HK_TRACE_BRUTE && !L.scenes && !(L.occlusion && !L.count))
-        smem += (size_t)block * 8;   // coop_leaf slots (the closest-hit single-scene kernels)
+    const size_t smem =
+        trace_smem_bytes(L.variant, (uint32_t)block, L.stack_depth, L.scenes != nullptr, L.occlusion, L.count);
+    if (block < 32 || (uint32_t)block > kTraceMaxBlock || smem > kTraceMaxSmem) return cudaErrorInvalidConfiguration;
     switch (L.variant) {
     case HK_TRACE_FULLSTACK: return launch_v<HK_TRACE_FULLSTACK>(a, L.count, L.occlusion, grid, block, smem, s);
     case HK_TRACE_SHORTSTACK: return launch_v<HK_TRACE_SHORTSTACK>(a, L.count, L.occlusion, grid, block, smem, s);

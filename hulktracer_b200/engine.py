@@ -171,6 +171,15 @@ class Context:
         self._check(self.L.hk_scene_get_counts(self.h, C.byref(nv), C.byref(nt)))
         self.nverts, self.ntris = nv.value, nt.value
 
+    def tree_cost(self, ct=None, ci=None):
+        """SAH cost of the current tree (full surface areas over the scene box;
+        the context's Ct / Ci unless given)."""
+        out = C.c_double()
+        ct = self.cfg.traverse_cost if ct is None else ct
+        ci = self.cfg.intersect_cost if ci is None else ci
+        self._check(self.L.hk_tree_cost(self.h, float(ct), float(ci), C.byref(out)))
+        return out.value
+
     def stats(self):
         st = _lib.TreeStats()
         self._check(self.L.hk_tree_stats_get(self.h, C.byref(st)))
@@ -240,6 +249,18 @@ class Context:
 
 
     # -- learned split proposer --
+    def set_proposal_log(self, on=True):
+        self._check(self.L.hk_set_proposal_log(self.h, 1 if on else 0))
+
+    def proposal_log(self):
+        """int32[nn, 8]: the bins proposed for each compact node of the last
+        learned build (axis * 32 + bin, -1 for none)."""
+        nn = C.c_uint32()
+        self._check(self.L.hk_get_proposal_log(self.h, None, 0, C.byref(nn)))
+        out = np.zeros((nn.value, 8), np.int32)
+        self._check(self.L.hk_get_proposal_log(self.h, ptr(out), nn.value, C.byref(nn)))
+        return out
+
     def mlp_init(self, seed=0):
         self._check(self.L.hk_mlp_init(self.h, seed))
 

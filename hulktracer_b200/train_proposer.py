@@ -3,13 +3,15 @@
     python -m hulktracer_b200.train_proposer [--scenes 160] [--epochs 24] \
         [--out hulktracer_b200/weights/proposer.bin]
 
-Data: every node with more than 256 references of exact binned-SAH builds
-(``HK_BUILD_BINNED`` with recording on) of seeded scenes from the two
-generators of the benchmark scenes -- rigid-part animations (``animated_parts``
-with other seeds, part counts and scales, at several frames) and clustered
-triangle soups (``cluster_soup``, the large static generator at other sizes).
-The label of a node is the (axis, plane) the exact search chose. The bench's
-animated scene (seed 3) is held out and used for validation only.
+Data: every node of 33..1024 references that the exact SAH splits in
+exact-SAH builds (``HK_BUILD_BINNED`` with ``exact_max`` 1024 and recording
+on) of seeded scenes from the two generators of the benchmark scenes --
+rigid-part animations (``animated_parts`` with other seeds, part counts and
+scales, at several frames) and clustered triangle soups (``cluster_soup``, the
+large static generator at other sizes). A row's features are the node's
+binned-SAH histogram (the features the learned build computes), its label the
+(axis, bin) holding the exact plane. The bench's animated scene (seed 3) is
+held out and used for validation only.
 
 Training runs entirely in libhulkcuda.so (``hk_mlp_train``: FP32 SGEMM
 forward/backward, softmax cross-entropy, Adam); the weights are written with
@@ -67,7 +69,7 @@ def validate(ctx, frames=(0, 20, 40, 59)):
 
     from hulktracer_b200 import scenes
     sc = scenes.animated_parts()
-    ctx.mlp_record(1 << 16)
+    ctx.mlp_record(1 << 20)
     ctx.upload(sc.verts, sc.tris)
     ctx.set_parts(sc.part_of_vertex, sc.part_center.shape[0])
     for f in frames:
@@ -89,18 +91,18 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--scenes", type=int, default=160)
     ap.add_argument("--frames", type=int, default=4)
-    ap.add_argument("--epochs", type=int, default=24)
+    ap.add_argument("--epochs", type=int, default=8)
     ap.add_argument("--batch", type=int, default=1024)
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--seed", type=int, default=2024)
-    ap.add_argument("--capacity", type=int, default=4_000_000)
+    ap.add_argument("--capacity", type=int, default=12_000_000)
     ap.add_argument("--out", default=os.path.join(ROOT, "hulktracer_b200", "weights", "proposer.bin"))
     a = ap.parse_args()
 
     def log(msg):
         print(msg, flush=True)
 
-    ctx = hk.Context()
+    ctx = hk.Context(exact_max=1024)
     ctx.mlp_init(a.seed)
     ctx.mlp_record(a.capacity)
     t0 = time.time()
@@ -110,7 +112,7 @@ def main():
     log("recorded %d rows from %d builds in %.1f s" % (rows, builds, t_data))
     # held-out agreement of the untrained network (its own context: validation
     # records into the recording buffer, which holds the training set here)
-    pre = hk.Context()
+    pre = hk.Context(exact_max=1024)
     pre.mlp_init(a.seed)
     before = validate(pre)
     pre.close()

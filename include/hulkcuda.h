@@ -69,7 +69,7 @@ typedef enum hk_variant {
 
 typedef enum hk_build_mode {
     HK_BUILD_BINNED = 0,   /* exact binned SAH, every (axis, bin) plane costed */
-    HK_BUILD_LEARNED = 1   /* MLP proposes top-k planes; binned fallback */
+    HK_BUILD_LEARNED = 1   /* MLP proposes top-k bins, searched exactly; binned fallback */
 } hk_build_mode;
 
 /* Shading semantics for hk_render */
@@ -95,13 +95,20 @@ typedef struct hk_config {
     uint32_t leaf_size;       /* a node with <= leaf_size refs becomes a leaf */
     uint32_t bins;            /* SAH bins per axis (32) */
     uint32_t short_stack;     /* ring depth of SHORTSTACK / SMEMSTACK (4..16) */
-    uint32_t block_size;      /* trace kernel block size (multiple of 32, <= 1024) */
+    uint32_t block_size;      /* trace kernel block size (multiple of 32, 32..256: the
+                                 kernel's launch bound). A trace whose shared memory
+                                 (SMEMSTACK: short_stack x block_size x 12 bytes, plus
+                                 block_size x 8 bytes for the warp-shared leaf test of
+                                 every closest-hit variant but BRUTE) exceeds 48 KB is
+                                 refused with HK_E_ILLEGAL_INPUT */
     uint32_t blocks_per_sm;   /* persistent trace grid = SMs * blocks_per_sm */
     uint32_t max_refs;        /* builder reference arena capacity (0 = 16 x tris) */
-    uint32_t topk;            /* learned builder: proposals costed per node (1..8, 4) */
-    float fallback_ratio;     /* learned builder: fall back to the full binned SAH
-                                 when the best proposal costs more than ratio x the
-                                 exactly costed reference plane (1.02; 0 = always) */
+    uint32_t topk;            /* learned builder: proposed bins refined per node (1..8, 4) */
+    float fallback_ratio;     /* learned builder: the binned SAH's plane splits a node
+                                 when the proposals' best costs more than ratio x the
+                                 binned optimum (default 1: the cheaper of the two;
+                                 1.02 lets a proposal up to 2% dearer stand; 0 = the
+                                 binned plane always) */
     uint32_t exact_max;       /* builder: nodes with at most this many references take
                                  the exact SAH over their references' bounds (the
                                  reference's candidate set) instead of 32 bins; 0 =
@@ -115,8 +122,8 @@ typedef struct hk_tree_stats {
     uint32_t depth;
     float build_ms;           /* device time of the last build */
     uint32_t capacity_hit;    /* 1 if a level stopped splitting for lack of arena */
-    uint32_t learned_nodes;   /* nodes split by a learned proposal */
-    uint32_t fallback_nodes;  /* nodes that fell back to the full binned search */
+    uint32_t learned_nodes;   /* proposer rows decided by a proposed bin's plane */
+    uint32_t fallback_nodes;  /* proposer rows decided by the binned SAH's plane */
 } hk_tree_stats;
 
 /* one hit: t (+inf on a miss) and the triangle index (-1 on a miss) */
@@ -186,6 +193,12 @@ hk_status hk_tree_export(hk_ctx *ctx, uint32_t *nodes4, uint32_t cap_nodes, uint
 hk_status hk_tree_export_compact(hk_ctx *ctx, uint32_t *cnodes2, uint32_t cap_nodes,
                                  uint32_t *refs, uint32_t cap_refs, uint32_t *cnn, uint32_t *nr);
 hk_status hk_tree_stats_get(hk_ctx *ctx, hk_tree_stats *stats);
+/* SAH cost of the current tree (no reference counterpart; the tree-quality
+ * measure of both builders): sum over junctions of ct * A(n) / A(root) plus
+ * over leaves of ci * |refs(n)| * A(n) / A(root), A the full surface area of the
+ * node's cell within the scene box, in double precision. An imported reference
+ * tree and a GPU-built one are costed by the same function. */
+hk_status hk_tree_cost(hk_ctx *ctx, double ct, double ci, double *cost);
 
 /* ---- tracing (KDTreeCPU::checkCollision, KDTreeCPU.cpp:230-253; gpu_trace,
  *      GPUTrace_stackless.cl:122-168) ---- */
@@ -270,17 +283,22 @@ hk_status hk_tree_save_file(hk_ctx *ctx, const char *path);
 hk_status hk_tree_load_file(hk_ctx *ctx, const char *path, int load_scene);
 
 /* ---- learned split proposer (no reference counterpart) ----
- * A 200 -> 256 -> 256 -> 256 -> 96 MLP (ReLU). Features of a node (sampled
- * from at most 64 of its references): per axis a 32-bin histogram of clipped
- * centroids and 16-bin histograms of clipped lower / upper bounds (fractions),
- * extents over the largest extent, depth / max_depth, 4 zeros. Output: one
- * logit per (axis, plane index 0..31). In HK_BUILD_LEARNED, nodes with more
- * than 256 references are handed to the proposer: the top-k valid planes
- * (hk_config.topk) and the middle plane of the longest axis are costed
- * exactly; the cheapest proposal is taken unless it costs more than
- * hk_config.fallback_ratio x the middle plane, in which case that node gets
- * the full binned SAH. Inference runs on the tensor cores in BF16 with FP32
- * accumulation; training uses FP32 master weights and Adam. */
+ * A 200 -> 256 -> 256 -> 256 -> 96 MLP (ReLU). Features of a node, from its
+ * 32-bin binned-SAH histogram: per axis the counts of the references' clipped
+ * lower bounds and upper bounds per bin as fractions of the node's references
+ * (192), extents over the largest extent (3), depth / max_depth, refs / 1024,
+ * 3 zeros. Output: one logit per (axis, bin 0..31) -- the bin expected
+ * to hold the node's exact-SAH plane. In HK_BUILD_LEARNED, nodes of up to 32
+ * references take the exact SAH in one warp, nodes of 33..1024 references are
+ * the proposer's rows and larger nodes take the binned SAH (exact_max is not
+ * used). A row gets the full binned SAH (every bin boundary costed exactly)
+ * and the network's top-k bins (hk_config.topk); every clipped reference
+ * bound inside a proposed bin -- the exact SAH's candidates there -- is
+ * costed exactly, and the cheapest of them splits the node unless it costs
+ * more than hk_config.fallback_ratio x the binned optimum, which is then the
+ * fallback (stats: learned_nodes / fallback_nodes). Inference runs on the
+ * tensor cores in BF16 with FP32 accumulation; training uses FP32 master
+ * weights and Adam. */
 hk_status hk_mlp_init(hk_ctx *ctx, uint64_t seed);
 hk_status hk_mlp_save(hk_ctx *ctx, const char *path);
 hk_status hk_mlp_load(hk_ctx *ctx, const char *path);
@@ -293,14 +311,22 @@ hk_status hk_mlp_forward(hk_ctx *ctx, const float *X, uint32_t n, float *logits)
 /* FP32 training kernels: mean softmax cross-entropy of labels y and its
  * gradient with respect to every parameter (flat layout above) */
 hk_status hk_mlp_grad(hk_ctx *ctx, const float *X, const int32_t *y, uint32_t n, float *grads, float *loss);
-/* record (features, label) rows during HK_BUILD_BINNED builds: label = axis *
- * 32 + plane index chosen by the exact binned SAH; capacity 0 stops recording.
- * Restarting recording empties the dataset. */
+/* record (features, label) rows during HK_BUILD_BINNED builds with
+ * exact_max >= 33: one row per node of 33..exact_max references the exact SAH
+ * splits, label = axis * 32 + the bin holding the exact plane; capacity 0
+ * stops recording. Restarting recording empties the dataset. */
 hk_status hk_mlp_record(hk_ctx *ctx, uint32_t capacity_rows);
 hk_status hk_mlp_dataset(hk_ctx *ctx, float *X, int32_t *y, uint32_t cap_rows, uint32_t *rows);
 /* train on the recorded rows (shuffled per epoch from seed); epoch_loss
  * (optional, host, epochs) receives the mean loss of every epoch */
 hk_status hk_mlp_train(hk_ctx *ctx, uint32_t epochs, uint32_t batch, float lr, uint64_t seed, float *epoch_loss);
+/* Verification aid: with the log on, every HK_BUILD_LEARNED build records
+ * the bins proposed for each proposer row, 8 int32 per compact node (axis * 32
+ * + bin in proposal order, -1 past the last proposal and for nodes that were
+ * not proposer rows); hk_get_proposal_log copies the log of the last build
+ * (nn = the tree's compact node count; pass bins8 = NULL for it). */
+hk_status hk_set_proposal_log(hk_ctx *ctx, int enable);
+hk_status hk_get_proposal_log(hk_ctx *ctx, int32_t *bins8, uint32_t cap_nodes, uint32_t *nn);
 
 /* ---- autotuner (no reference counterpart) ----
  * Times the persistent traversal on n device rays of the current scene for
@@ -357,11 +383,17 @@ hk_status hk_batch_trace_device(hk_batch *batch, const float *d_rays8, const uin
  * that every GPU loading the library holds until the process exits. A call
  * needing more scratch than that (roughly w*h*(40 + 44*point_lights +
  * 4*lights) bytes; 512x512 with one point light fits) returns HK_E_CAPACITY
- * before doing anything. The first call on a device looks up the array's
- * device address; make it before any stream capture starts. Calls share the
- * array and keep the last call's contents (counters are cleared per call);
- * calls whose GPU work overlaps race on it. The call synchronises
- * cuda_stream before returning (to read the device error word). */
+ * before doing anything. Traversal: FULLSTACK, SHORTSTACK, SMEMSTACK, RESTART,
+ * RESTART_EARLY or BRUTE at a fixed block of 128 threads and a ring of 6
+ * entries; ROPES needs per-node cells and ropes that this call does not take
+ * and is refused with HK_E_ILLEGAL_INPUT. The first call on a device looks up
+ * the array's device address and loads every kernel this call can launch
+ * (with lazy module loading the driver would otherwise allocate module memory
+ * at a variant's first launch); make that first call before any stream
+ * capture starts. Calls share the array and keep the last call's contents
+ * (counters are cleared per call); calls whose GPU work overlaps race on it.
+ * The call synchronises cuda_stream before returning (to read the device
+ * error word). */
 #define HK_NOALLOC_SCRATCH_BYTES (24u << 20)
 hk_status hk_render_noalloc(const uint32_t *d_nodes2, const uint32_t *d_refs, const float *d_records16,
                             uint32_t ntris, const float *box8, const float *cam16, const float *lights8,

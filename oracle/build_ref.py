@@ -28,8 +28,12 @@ Two libraries are produced:
   scenes (Ct 1, Ci 1.5, depth 24, leaf <= 4, no subsampling), for SAH-cost
   comparisons against the GPU builder.
 
-Usage: ``python oracle/build_ref.py [--reference /root/reference]``.
-The reference path defaults to ``$HK_REFERENCE_ROOT`` or ``/root/reference``.
+Usage: ``python oracle/build_ref.py [--reference DIR]``. Where the reference
+sources are is decided here and nowhere else (``reference_root()``): ``--reference``,
+else ``$HK_REFERENCE_ROOT``, else the directory the reference checkout is
+mounted at on the build machine (``DEFAULT_REFERENCE``). When none holds the
+sources, nothing is built and the checkers that need the compiled reference
+skip.
 """
 import argparse
 import os
@@ -40,6 +44,12 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "_ref")
+DEFAULT_REFERENCE = "/root/reference"
+
+
+def reference_root() -> str:
+    """The reference checkout this recipe compiles from (it may not exist)."""
+    return os.environ.get("HK_REFERENCE_ROOT", DEFAULT_REFERENCE)
 
 SOURCES = [
     "src/KDTreeSAH.cpp", "src/SPMatrix.cpp", "src/SseUtils.cpp", "src/Settings.cpp",
@@ -215,7 +225,7 @@ def build(ref, cfg):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default=os.environ.get("HK_REFERENCE_ROOT", "/root/reference"))
+    ap.add_argument("--reference", default=reference_root())
     a = ap.parse_args()
     if not os.path.isdir(os.path.join(a.reference, "HulkEngine")):
         print("reference sources not found at %s; nothing built" % a.reference)

@@ -1178,6 +1178,16 @@ static int search_ropes(const hko_tree *t, const float *o, const float *d, float
 /*    clipped bounds); ref order is kept;                                     */
 /*  - children are numbered as pairs (below, above) in the order their        */
 /*    parents appear in the level; an empty child is an empty leaf.           */
+/* Learned mode (the CUDA builder's k_learn, restated with the bins the GPU  */
+/* proposed, taken from its proposal log): nodes of at most 32 refs take the  */
+/* exact search; a node of 33..1024 refs takes the binned search and, for    */
+/* each proposed bin (axis a, bin b, closed interval [P0, P1] = [p_b,        */
+/* p_{b+1}], p_0 = node min, p_32 = node max), the exact search over the      */
+/* clipped bounds inside the interval (a bin whose in-interval lower bounds,  */
+/* upper bounds or flat refs exceed the list capacity (2048 / (3 topk))      */
+/* rounded down to a multiple of 8 is skipped); the best of those by          */
+/* (cost, axis, plane) replaces the binned plane unless it costs more than    */
+/* fallback_ratio x the binned optimum.                                       */
 /* ------------------------------------------------------------------------ */
 typedef struct {
     float box[8];
@@ -1235,7 +1245,7 @@ int hko_build_binned(const float *verts, const uint32_t *tris, uint32_t nt, cons
             float A = surf(n->box);
             float best = INFINITY;
             uint32_t bnb = 0, bna = 0;
-            if (n->count <= p->exact_max) {
+            if (n->count <= (p->learned ? 32u : p->exact_max)) {
                 /* small node: every clipped reference bound is a candidate
                  * (+0.0f makes a -0 bound the plane +0) */
                 for (uint32_t a = 0; a < 3; a++) {
@@ -1315,6 +1325,65 @@ int hko_build_binned(const float *verts, const uint32_t *tris, uint32_t nt, cons
                         bnb = nb;
                         bna = na;
                     }
+                }
+            }
+            if (p->learned && n->count > 32 && n->count <= 1024 && p->proposals) {
+                const int32_t *prop = p->proposals + 8 * (size_t)n->cidx;
+                uint32_t K = p->topk < 8 ? (p->topk ? p->topk : 1) : 8;
+                uint32_t cap = (2048u / (3u * K)) & ~7u;
+                float rbest = INFINITY, rpk = 0.0f;
+                int32_t rax = 3;
+                uint32_t rnb = 0, rna = 0;
+                for (uint32_t i = 0; i < 8 && prop[i] >= 0; i++) {
+                    uint32_t a = (uint32_t)prop[i] / 32u, b = (uint32_t)prop[i] % 32u;
+                    float lo_b = n->box[a], hi_b = n->box[4 + a];
+                    float P0 = b == 0 ? lo_b : bplane(n->box, a, b, 32);
+                    float P1 = b == 31 ? hi_b : bplane(n->box, a, b + 1, 32);
+                    uint32_t nl = 0, nh = 0, nf = 0;
+                    for (uint32_t r = 0; r < n->count; r++) {
+                        const float *t6 = tb + 6 * (size_t)refs[n->start + r];
+                        float lo = mx(t6[a], lo_b), hi = mn(t6[3 + a], hi_b);
+                        int inl = P0 <= lo && lo <= P1, inh = P0 <= hi && hi <= P1;
+                        nl += inl;
+                        nh += inh;
+                        nf += inl && lo == hi;
+                    }
+                    if (nl > cap || nh > cap || nf > cap) continue;
+                    for (uint32_t q = 0; q < 2 * n->count; q++) {
+                        const float *tq = tb + 6 * (size_t)refs[n->start + q / 2];
+                        float v = (q & 1) ? mn(tq[3 + a], hi_b) : mx(tq[a], lo_b);
+                        if (!(P0 <= v && v <= P1)) continue;
+                        if (!(v > lo_b && v < hi_b)) continue;
+                        float pk = v + 0.0f;
+                        uint32_t nb = 0, na = 0;
+                        for (uint32_t r = 0; r < n->count; r++) {
+                            const float *t6 = tb + 6 * (size_t)refs[n->start + r];
+                            float lo = mx(t6[a], lo_b), hi = mn(t6[3 + a], hi_b);
+                            int on = lo == hi && lo == pk;
+                            nb += (lo < pk || on) ? 1u : 0u;
+                            na += (hi > pk || on) ? 1u : 0u;
+                        }
+                        float bb[8], ba[8];
+                        memcpy(bb, n->box, 32);
+                        memcpy(ba, n->box, 32);
+                        bb[4 + a] = pk;
+                        ba[a] = pk;
+                        float cost = p->ct + p->ci * ((surf(bb) * (float)nb + surf(ba) * (float)na) / A);
+                        if (cost < rbest || (cost == rbest && ((int32_t)a < rax || ((int32_t)a == rax && pk < rpk)))) {
+                            rbest = cost;
+                            rax = (int32_t)a;
+                            rpk = pk;
+                            rnb = nb;
+                            rna = na;
+                        }
+                    }
+                }
+                if (rbest < INFINITY && rbest <= p->fallback_ratio * best) {
+                    best = rbest;
+                    axis[s] = rax;
+                    plane[s] = rpk;
+                    bnb = rnb;
+                    bna = rna;
                 }
             }
             if (axis[s] >= 0 && !(best < p->ci * (float)n->count)) axis[s] = -1;

@@ -146,6 +146,12 @@ typedef struct {
     uint32_t max_refs;      /* capacity of the reference arena (and of the leaf list) */
     uint32_t max_nodes;     /* capacity of the compact node array */
     uint32_t exact_max;     /* nodes with at most this many refs cost the event planes */
+    /* learned mode (exact_max is then 32): nodes of 33..1024 refs take the
+     * binned search plus the exact search restricted to their proposed bins */
+    uint32_t learned;
+    uint32_t topk;           /* proposals per node (list capacity depends on it) */
+    float fallback_ratio;
+    const int32_t *proposals; /* per compact node, 8 bins (axis * 32 + bin, -1: none) */
 } hko_binned_params;
 int hko_build_binned(const float *verts, const uint32_t *tris, uint32_t nt, const float *box,
                      const hko_binned_params *p, uint32_t **nodes_out, uint32_t *nn_out,

@@ -12,8 +12,9 @@ candidate plane. This file restates, in numpy, what the CUDA side computes:
 * ``forward_bf16``: the inference path -- inputs, weights and hidden
   activations rounded to BF16 (round to nearest even), products accumulated in
   FP32 (here in float64, then rounded), biases in FP32;
-* ``features``: the 200 node features the builder computes from the sampled
-  references of a node.
+* ``hist_features`` / ``exact_label``: the 200 node features the builder
+  computes from a node's binned histogram, and the training label of an
+  exactly searched node.
 """
 from __future__ import annotations
 
@@ -93,14 +94,15 @@ def forward_bf16(p, X):
     return (a @ bf16(P["W4"]).astype(np.float64)).astype(np.float32) + P["b4"]
 
 
-def features(node_lo, node_hi, tri_lo, tri_hi, depth, max_depth):
-    """The 200 features of one node from the bounds of its sampled triangles
-    (at most 64, taken by the caller at a fixed stride): per axis a 32-bin
-    histogram of clipped centroids, then per axis 16-bin histograms of the
-    clipped lower and upper bounds, each as a fraction of the sample; the node
-    extents over the largest extent; depth / max_depth; four zeros."""
+def hist_features(node_lo, node_hi, tri_lo, tri_hi, depth, max_depth):
+    """The 200 features of one node as the builder computes them from its
+    binned-SAH histogram (every reference of the node): per axis the counts
+    of the clipped lower bounds per bin b (p_b <= lo < p_{b+1}) and of the
+    clipped upper bounds per bin c (p_c < hi <= p_{c+1}), p_k = min + ext *
+    (k / 32), as fractions of the node's references; the node extents over the
+    largest extent; depth / max_depth; references / 1024; three zeros."""
     f = np.zeros(200, np.float32)
-    S = tri_lo.shape[0]
+    cnt = tri_lo.shape[0]
     lo_n = np.asarray(node_lo, np.float32)
     hi_n = np.asarray(node_hi, np.float32)
     for a in range(3):
@@ -108,19 +110,28 @@ def features(node_lo, node_hi, tri_lo, tri_hi, depth, max_depth):
         ext = np.float32(h - l)
         if not ext > 0:
             continue
+        k = np.arange(1, 32, dtype=np.float32) * np.float32(0.03125)
+        planes = (l + ext * k).astype(np.float32)          # p_1 .. p_31, non-decreasing
         lo = np.maximum(tri_lo[:, a].astype(np.float32), l)
         hi = np.minimum(tri_hi[:, a].astype(np.float32), h)
-        c = (lo + hi) * np.float32(0.5)
-        b32 = np.clip(((c - l) * (np.float32(32.0) / ext)).astype(np.int64), 0, 31)
-        b16l = np.clip(((lo - l) * (np.float32(16.0) / ext)).astype(np.int64), 0, 15)
-        b16h = np.clip(((hi - l) * (np.float32(16.0) / ext)).astype(np.int64), 0, 15)
-        np.add.at(f, a * 32 + b32, 1.0)
-        np.add.at(f, 96 + a * 32 + b16l, 1.0)
-        np.add.at(f, 96 + a * 32 + 16 + b16h, 1.0)
-    if S:
-        f[:192] *= np.float32(1.0) / np.float32(S)
+        b = np.searchsorted(planes, lo, side="right")       # planes <= lo
+        c = np.searchsorted(planes, hi, side="left")        # planes < hi
+        f[a * 64: a * 64 + 32] = np.bincount(b, minlength=32).astype(np.float32)
+        f[a * 64 + 32: a * 64 + 64] = np.bincount(c, minlength=32).astype(np.float32)
+    if cnt:
+        f[:192] *= np.float32(1.0) / np.float32(cnt)
     e = (hi_n[:3] - lo_n[:3]).astype(np.float32)
     m = e.max()
     f[192:195] = e * (np.float32(1.0) / m if m > 0 else np.float32(0.0))
     f[195] = np.float32(depth) / np.float32(max_depth)
+    f[196] = np.float32(cnt) * np.float32(1.0 / 1024.0)
     return f
+
+
+def exact_label(node_lo, node_hi, axis, plane):
+    """axis * 32 + the bin b holding the plane: p_b <= plane < p_{b+1}."""
+    l = np.float32(node_lo[axis])
+    ext = np.float32(np.float32(node_hi[axis]) - l)
+    k = np.arange(1, 32, dtype=np.float32) * np.float32(0.03125)
+    planes = (l + ext * k).astype(np.float32)
+    return int(axis) * 32 + int(np.searchsorted(planes, np.float32(plane), side="right"))

@@ -40,6 +40,25 @@ def test_null_arguments_rejected():
     assert L.hk_trace(None, None, 0, 0, None) == 4
 
 
+@pytest.mark.parametrize("block,ok", [(256, True), (288, False), (512, False), (1024, False), (48, False)])
+def test_block_size_beyond_the_launch_bound_rejected(block, ok):
+    """The trace kernel is compiled for at most 256 threads per block; a
+    larger block_size is refused when the context is created (HK_E_ILLEGAL_INPUT)
+    instead of failing every later launch. Validation runs before any CUDA call."""
+    L = _lib.load()
+    c = _lib.Config()
+    L.hk_config_default(C.byref(c))
+    c.block_size = block
+    h = C.c_void_p()
+    st = L.hk_create(C.byref(h), C.byref(c))
+    if ok:
+        assert st in (0, 16)   # 16: no GPU in this process
+        if st == 0:
+            L.hk_destroy(h)
+    else:
+        assert st == 4
+
+
 def test_create_without_gpu_fails_cleanly():
     import torch
     if torch.cuda.is_available():

@@ -1,8 +1,10 @@
 """The learned split proposer on the GPU: the network's tensor-core inference
 and FP32 training kernels against the CPU oracle (oracle/mlp.py), the
-recorded training rows against the oracle's features of the same (identical)
-binned tree, and learned builds (validity, the fallback's exactness, the
-trained network's cost and what it gains over an untrained one)."""
+recorded training rows (histogram features, exact-plane bins) against the
+oracle's exact tree, and learned builds: equal array for array to the
+oracle's restatement replaying the GPU's proposals, the fallback's
+exactness, valid trees, and the trained network's tree cost against the
+exact SAH with what it gains over an untrained network."""
 import os
 
 import numpy as np
@@ -15,7 +17,7 @@ pytestmark = pytest.mark.gpu
 
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
 WEIGHTS = os.path.join(os.path.dirname(os.path.dirname(__file__)), "hulktracer_b200", "weights", "proposer.bin")
-KPROPOSE = 1024         # nodes with more references than this go to the proposer
+LEARN_MIN, LEARN_MAX = 33, 1024     # proposer rows: nodes of 33..1024 references
 CT, CI = 1.0, 1.5
 
 
@@ -38,14 +40,14 @@ def features_like(n, seed):
 def test_forward_bf16_matches_oracle(ctx):
     ctx.mlp_init(7)
     p = ctx.mlp_params()
-    X = features_like(300, 1)                      # 3 CTAs, the last one partial
+    X = features_like(300, 1)                      # 5 tiles of 64 rows, the last one partial
     Z = ctx.mlp_forward(X)
     Zb = mlp.forward_bf16(p, X)
     Zf, _ = mlp.forward_fp32(p, X)
     scale = float(np.abs(Zb).max())
     err = np.abs(Z - Zb)
     assert err.max() <= 1e-2 * scale and err.mean() <= 1e-3 * scale
-    # BF16 against the FP32 network: close, and the same top plane on most rows
+    # BF16 against the FP32 network: close, and the same top bin on most rows
     assert np.abs(Z - Zf).max() <= 5e-2 * scale
     assert (Z.argmax(1) == Zf.argmax(1)).mean() >= 0.9
 
@@ -82,16 +84,20 @@ def test_params_save_load_roundtrip(ctx, hk, tmp_path):
         other.mlp_load(f)
 
 
-def oracle_rows(oracle, verts, tris, box, max_depth=24):
-    """(features, axis) of every node of the oracle's binned tree that has
-    more than KPROPOSE references and is split, from its references in
-    ascending triangle order (the builder's stable partition keeps that
-    order), sampled as the builder samples them."""
-    cn, cr = oracle.build_binned(verts, tris, box, ct=CT, ci=CI, max_depth=max_depth, leaf_size=4)
+def tri_bounds(verts, tris):
     v = verts[:, :3]
     t = tris[:, :3]
     tlo = np.minimum(np.minimum(v[t[:, 0]], v[t[:, 1]]), v[t[:, 2]]).astype(np.float32)
     thi = np.maximum(np.maximum(v[t[:, 0]], v[t[:, 1]]), v[t[:, 2]]).astype(np.float32)
+    return tlo, thi
+
+
+def oracle_rows(oracle, verts, tris, box, max_depth=24):
+    """(features, label) of every split node of 33..1024 references of the
+    oracle's exact tree (exact_max 1024, identical to the GPU's): the
+    node's binned histogram over all its references, the bin of its plane."""
+    cn, cr = oracle.build_binned(verts, tris, box, ct=CT, ci=CI, max_depth=max_depth, leaf_size=4, exact_max=1024)
+    tlo, thi = tri_bounds(verts, tris)
     rows = []
 
     def walk(i, lo, hi, level):
@@ -104,34 +110,34 @@ def oracle_rows(oracle, verts, tris, box, max_depth=24):
         lhi[axis] = plane
         rlo[axis] = plane
         refs = np.union1d(walk(pair, lo, lhi, level + 1), walk(pair + 1, rlo, hi, level + 1))
-        cnt = refs.shape[0]
-        if cnt > KPROPOSE:
-            S = min(cnt, 64)
-            pick = refs[(np.arange(S, dtype=np.int64) * cnt) // S]
-            rows.append((mlp.features(lo, hi, tlo[pick], thi[pick], level, max_depth), axis))
+        if LEARN_MIN <= refs.shape[0] <= LEARN_MAX:
+            rows.append((mlp.hist_features(lo, hi, tlo[refs], thi[refs], level, max_depth),
+                         mlp.exact_label(lo, hi, axis, plane)))
         return refs
 
     walk(0, np.asarray(box[:4], np.float32).copy(), np.asarray(box[4:], np.float32).copy(), 0)
     return rows
 
 
-def test_recorded_rows_match_oracle(ctx, oracle):
+def test_recorded_rows_match_oracle(hk, oracle):
     g = load("small24k.npz")
-    ctx.upload(g["verts"], g["tris"])
-    ctx.set_box(g["box"])
-    ctx.precompute()
-    ctx.mlp_record(100000)
+    c = hk.Context(exact_max=1024)
+    c.upload(g["verts"], g["tris"])
+    c.set_box(g["box"])
+    c.precompute()
+    c.mlp_record(100000)
     try:
-        ctx.build()
-        X, y = ctx.mlp_dataset()
+        c.build()
+        X, y = c.mlp_dataset()
     finally:
-        ctx.mlp_record(0)
+        c.mlp_record(0)
     rows = oracle_rows(oracle, g["verts"], g["tris"], g["box"])
     assert X.shape[0] == len(rows) > 0
     assert np.all((y >= 0) & (y < 96))
-    got = sorted((X[i].tobytes(), int(y[i]) // 32) for i in range(X.shape[0]))
-    want = sorted((f.tobytes(), a) for f, a in rows)
+    got = sorted((X[i].tobytes(), int(y[i])) for i in range(X.shape[0]))
+    want = sorted((f.tobytes(), lab) for f, lab in rows)
     assert got == want
+    c.close()
 
 
 def trace_equals_brute(ctx, hk, rays):
@@ -147,22 +153,59 @@ def trace_equals_brute(ctx, hk, rays):
         assert np.array_equal(h["t"][m], b["t"][m])
 
 
-def test_learned_build_valid_with_untrained_network(ctx, hk):
-    g = load("small24k.npz")
-    ctx.upload(g["verts"], g["tris"])
-    ctx.set_box(g["box"])
-    ctx.precompute()
-    ctx.mlp_init(3)
-    st = ctx.build(hk.BUILD_LEARNED)
-    assert st["learned_nodes"] + st["fallback_nodes"] > 0
-    trace_equals_brute(ctx, hk, g["rays"])
+def learned_case(hk, oracle, sc, frame, weights=None, seed=3, topk=4):
+    """A learned build (proposal log on) and the oracle's restatement of it
+    replaying the GPU's proposals; returns both trees and the stats."""
+    c = hk.Context(topk=topk)
+    if weights:
+        c.mlp_load(weights)
+    else:
+        c.mlp_init(seed)
+    c.upload(sc.verts, sc.tris)
+    c.set_parts(sc.part_of_vertex, sc.part_center.shape[0])
+    c.transform(scenes.part_matrices(sc, frame))
+    box = c.get_box()
+    c.set_proposal_log(True)
+    st = c.build(hk.BUILD_LEARNED)
+    gn, gr = c.export_compact()
+    log = c.proposal_log()
+    verts = c.get_vertices()
+    on, orf = oracle.build_binned(verts, sc.tris, box, ct=CT, ci=CI, max_depth=24, leaf_size=4,
+                                  proposals=log, topk=topk, fallback_ratio=1.0)
+    return c, (gn, gr), (on, orf), st, log
 
 
-def test_learned_fallback_zero_equals_binned(hk):
-    """fallback_ratio 0: every proposer node takes the full binned SAH, so
-    the learned build must equal the binned build bit for bit."""
-    c = hk.Context(fallback_ratio=0.0)
+@pytest.mark.parametrize("frame,topk", [(0, 4), (17, 4), (17, 2)])
+def test_learned_build_equals_oracle_replay(hk, oracle, frame, topk):
+    """The learned build (untrained network) equals, array for array, the
+    oracle's restatement fed the bins the GPU proposed: the histogram, the
+    restricted exact search, the list-capacity rule and the fallback are the
+    same; and the tree finds every closest hit."""
+    sc = scenes.animated_parts(seed=77, n_parts=16, width=96, height=64)
+    c, (gn, gr), (on, orf), st, log = learned_case(hk, oracle, sc, frame, topk=topk)
+    assert st["learned_nodes"] + st["fallback_nodes"] > 50
+    assert ((log >= 0).sum(1) == topk).sum() == st["learned_nodes"] + st["fallback_nodes"]
+    assert np.array_equal(gn, on) and np.array_equal(gr, orf)
+    rays = c.camera_rays(sc.camera, 96, 64)
+    trace_equals_brute(c, hk, rays)
+    c.close()
+
+
+@pytest.mark.skipif(not os.path.exists(WEIGHTS), reason="no trained proposer weights")
+def test_trained_learned_build_equals_oracle_replay(hk, oracle):
+    sc = scenes.animated_parts(seed=78, n_parts=24, width=96, height=64)
+    c, (gn, gr), (on, orf), st, _ = learned_case(hk, oracle, sc, 9, weights=WEIGHTS)
+    assert st["learned_nodes"] > st["fallback_nodes"]
+    assert np.array_equal(gn, on) and np.array_equal(gr, orf)
+    c.close()
+
+
+def test_learned_fallback_zero_equals_exact32(hk):
+    """fallback_ratio 0: every proposer row keeps the binned SAH's plane, so
+    the learned build (exact SAH up to 32 references, binned above) equals the
+    binned build with exact_max 32 bit for bit."""
     sc = scenes.animated_parts(n_parts=6, width=96, height=64)
+    c = hk.Context(fallback_ratio=0.0, exact_max=32)
     c.upload(sc.verts, sc.tris)
     c.set_box(sc.scene_box())
     c.precompute()
@@ -173,12 +216,26 @@ def test_learned_fallback_zero_equals_binned(hk):
     ln, lr = c.export_compact()
     assert st["learned_nodes"] == 0 and st["fallback_nodes"] > 0
     assert np.array_equal(bn, ln) and np.array_equal(br, lr)
+    c.close()
+
+
+def test_learned_build_valid_on_golden_scene(hk):
+    g = load("small24k.npz")
+    c = hk.Context()
+    c.upload(g["verts"], g["tris"])
+    c.set_box(g["box"])
+    c.precompute()
+    c.mlp_init(3)
+    st = c.build(hk.BUILD_LEARNED)
+    assert st["learned_nodes"] + st["fallback_nodes"] > 0
+    trace_equals_brute(c, hk, g["rays"])
+    c.close()
 
 
 def test_train_reduces_loss(hk):
-    c = hk.Context()
+    c = hk.Context(exact_max=1024)
     c.mlp_init(0)
-    c.mlp_record(200000)
+    c.mlp_record(400000)
     for seed in range(4):
         sc = scenes.animated_parts(seed=100 + seed, n_parts=12, width=64, height=64)
         c.upload(sc.verts, sc.tris)
@@ -192,74 +249,70 @@ def test_train_reduces_loss(hk):
     losses = c.mlp_train(epochs=8, batch=128, lr=1e-3, seed=1)
     assert np.all(np.isfinite(losses))
     assert losses[-1] < 0.8 * losses[0]
+    c.close()
 
 
-@pytest.mark.skipif(not os.path.exists(WEIGHTS), reason="no trained proposer weights")
-def test_trained_proposer_cost_and_gain(hk, oracle):
-    """On held-out frames of the animated 200k scene: the trained proposer's
-    tree costs within 2% of the exact binned tree (the fallback checks every
-    proposal), and it beats the untrained network on both the cost and the
-    share of proposer nodes that needed the fallback."""
-    sc = scenes.animated_parts()
-    res = {}
-    for name in ("trained", "untrained"):
-        c = hk.Context()
-        if name == "trained":
-            c.mlp_load(WEIGHTS)
-        else:
-            c.mlp_init(12345)
+def tree_costs_by_build(hk, sc, frames, weights=None, seed=12345):
+    """SAH costs (hk_tree_cost) of the learned, exact (exact_max 1024) and
+    binned trees per frame, and the learned build's fallback share."""
+    ex = hk.Context(exact_max=1024)
+    bi = hk.Context()
+    le = hk.Context()
+    if weights:
+        le.mlp_load(weights)
+    else:
+        le.mlp_init(seed)
+    out = []
+    fb = n = 0
+    for c in (ex, bi, le):
         c.upload(sc.verts, sc.tris)
         c.set_parts(sc.part_of_vertex, sc.part_center.shape[0])
-        costs, fb, n = [], 0, 0
-        for frame in (0, 17, 42):
-            c.transform(scenes.part_matrices(sc, frame))
-            box = c.get_box()
-            c.build(hk.BUILD_BINNED)
-            bn, _ = c.export_compact()
-            st = c.build(hk.BUILD_LEARNED)
-            ln, _ = c.export_compact()
-            cb = oracle.tree_cost(oracle.compact_to_ref(bn), box, CT, CI)
-            cl = oracle.tree_cost(oracle.compact_to_ref(ln), box, CT, CI)
-            costs.append(cl / cb)
-            fb += st["fallback_nodes"]
-            n += st["fallback_nodes"] + st["learned_nodes"]
-        res[name] = (max(costs), fb / max(n, 1))
+    for f in frames:
+        m = scenes.part_matrices(sc, f)
+        row = []
+        for c, mode in ((le, hk.BUILD_LEARNED), (ex, hk.BUILD_BINNED), (bi, hk.BUILD_BINNED)):
+            c.transform(m)
+            st = c.build(mode)
+            row.append(c.tree_cost(CT, CI))
+            if c is le:
+                fb += st["fallback_nodes"]
+                n += st["fallback_nodes"] + st["learned_nodes"]
+        out.append(row)
+    for c in (ex, bi, le):
         c.close()
-    print("proposer ablation (max cost ratio, fallback share):", res)
-    assert res["trained"][0] <= 1.02
-    assert res["trained"][1] < res["untrained"][1]
-    assert res["trained"][0] <= res["untrained"][0]
+    return np.array(out), fb / max(n, 1)
 
 
 @pytest.mark.skipif(not os.path.exists(WEIGHTS), reason="no trained proposer weights")
-def test_trained_proposer_heldout_2m(hk, oracle):
+def test_trained_proposer_cost_and_gain(hk):
+    """Held-out frames of the animated 200k scene (never trained on): the
+    trained proposer's tree costs within 2% of the exact SAH's tree, and it
+    beats the untrained network on the cost and on the share of rows the
+    binned plane decided (what the training buys)."""
+    sc = scenes.animated_parts()
+    frames = (5, 17, 42)
+    tr, fb_t = tree_costs_by_build(hk, sc, frames, weights=WEIGHTS)
+    un, fb_u = tree_costs_by_build(hk, sc, frames)
+    r_t = tr[:, 0] / tr[:, 1]
+    r_u = un[:, 0] / un[:, 1]
+    r_b = tr[:, 2] / tr[:, 1]
+    print("learned/exact cost trained", np.round(r_t, 4), "untrained", np.round(r_u, 4), "binned/exact",
+          np.round(r_b, 4), "fallback share trained %.3f untrained %.3f" % (fb_t, fb_u))
+    assert r_t.max() <= 1.02
+    assert r_t.mean() < r_u.mean()
+    assert fb_t < fb_u
+
+
+@pytest.mark.skipif(not os.path.exists(WEIGHTS), reason="no trained proposer weights")
+def test_trained_proposer_heldout_2m(hk):
     """The held-out 2M-triangle animated sequence (seed 9001, 640 parts, a
     density like the 200k scene's; neither it nor its seed was trained on):
-    over frames 0, 30 and 59 the learned tree costs within 2% of the binned
-    tree, and the device times of both builds are reported."""
+    over frames 0, 30 and 59 the learned tree costs within 2% of the exact
+    SAH's tree."""
     sc = scenes.animated_parts(seed=9001, n_parts=640, scale=2.15, width=64, height=64)
     assert sc.tris.shape[0] > 1_900_000
-    c = hk.Context()
-    c.mlp_load(WEIGHTS)
-    c.upload(sc.verts, sc.tris)
-    c.set_parts(sc.part_of_vertex, sc.part_center.shape[0])
-    ratios, fb, n, t_b, t_l = [], 0, 0, [], []
-    for frame in (0, 30, 59):
-        c.transform(scenes.part_matrices(sc, frame))
-        box = c.get_box()
-        c.build(hk.BUILD_BINNED)       # first build of a frame warms the arenas
-        sb = c.build(hk.BUILD_BINNED)
-        bn, _ = c.export_compact()
-        sl = c.build(hk.BUILD_LEARNED)
-        ln, _ = c.export_compact()
-        ratios.append(oracle.tree_cost(oracle.compact_to_ref(ln), box, CT, CI) /
-                      oracle.tree_cost(oracle.compact_to_ref(bn), box, CT, CI))
-        fb += sl["fallback_nodes"]
-        n += sl["fallback_nodes"] + sl["learned_nodes"]
-        t_b.append(sb["build_ms"])
-        t_l.append(sl["build_ms"])
-    c.close()
-    print("held-out 2M: learned/binned cost", [round(r, 4) for r in ratios], "fallback share %.3f" % (fb / max(n, 1)),
-          "build ms binned", [round(t, 3) for t in t_b], "learned", [round(t, 3) for t in t_l])
-    assert n > 0
-    assert max(ratios) <= 1.02
+    costs, fb = tree_costs_by_build(hk, sc, (0, 30, 59), weights=WEIGHTS)
+    r = costs[:, 0] / costs[:, 1]
+    print("held-out 2M: learned/exact cost", np.round(r, 4), "binned/exact", np.round(costs[:, 2] / costs[:, 1], 4),
+          "fallback share %.3f" % fb)
+    assert r.max() <= 1.02

@@ -240,3 +240,30 @@ def test_ropes_ties_and_signed_zero(hk):
         assert np.array_equal(h["tri"], b["tri"])
         assert np.array_equal(h["t"].view(np.uint32), b["t"].view(np.uint32))
     ctx.close()
+
+
+@pytest.mark.parametrize("stack,block,ok", [(16, 256, False), (8, 512, None), (15, 256, True), (8, 128, True)])
+def test_shared_memory_bound_of_the_shared_ring(hk, stack, block, ok):
+    """SMEMSTACK keeps its ring in shared memory (stack x block x 12 bytes) next
+    to the warp-shared leaf test's slots (block x 8 bytes). A configuration past
+    48 KB is refused with HK_E_ILLEGAL_INPUT before anything is launched; one
+    within it traces like the register ring. A block above the kernel's bound
+    of 256 threads is refused when the context is created (ok None)."""
+    g = load("soup3k.npz")
+    if ok is None:
+        with pytest.raises(hk.HkError) as e:
+            hk.Context(short_stack=stack, block_size=block)
+        assert e.value.status == 4
+        return
+    ctx = hk.Context(short_stack=stack, block_size=block)
+    setup_ref_tree(ctx, g)
+    rays = g["rays"]
+    if not ok:
+        with pytest.raises(hk.HkError) as e:
+            ctx.trace(rays, hk.SMEMSTACK)
+        assert e.value.status == 4 and "48 KB" in str(e.value)
+    else:
+        a = ctx.trace(rays, hk.SMEMSTACK)
+        b = ctx.trace(rays, hk.SHORTSTACK)
+        assert np.array_equal(a["tri"], b["tri"]) and np.array_equal(a["t"].view(np.uint32), b["t"].view(np.uint32))
+    ctx.close()

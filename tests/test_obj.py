@@ -10,7 +10,9 @@ from hulktracer_b200 import scenes
 from hulktracer_b200.engine import obj_parse
 from hulktracer_b200._lib import HkError
 
-TEAPOT = os.path.join(os.environ.get("HK_REFERENCE_ROOT", "/root/reference"), "OBJLoader/Models/teapot/teapot.obj")
+from oracle.build_ref import reference_root
+
+TEAPOT = os.path.join(reference_root(), "OBJLoader/Models/teapot/teapot.obj")
 
 
 def write_obj(path, verts, tris, quads=()):

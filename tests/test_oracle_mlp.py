@@ -47,16 +47,27 @@ def test_bf16_rounding_matches_torch():
     assert np.array_equal(mlp.bf16(x).view(np.uint32), t.view(np.uint32))
 
 
-def test_features_shape_and_sums():
+def test_hist_features_shape_sums_and_bins():
+    """Per axis the lower-bound and upper-bound bin counts each sum to the
+    node's references; a bound exactly on a bin plane goes to the bin above
+    it (lower bounds) or below it (upper bounds), as the builder's
+    corrections place them."""
     rng = np.random.default_rng(4)
-    lo = rng.uniform(-1, 0.5, size=(64, 3)).astype(np.float32)
-    hi = lo + rng.uniform(0, 0.5, size=(64, 3)).astype(np.float32)
-    f = mlp.features(np.float32([-1, -1, -1, 0]), np.float32([1, 2, 1, 0]), lo, hi, 3, 24)
+    lo = rng.uniform(-1, 0.5, size=(100, 3)).astype(np.float32)
+    hi = lo + rng.uniform(0, 0.5, size=(100, 3)).astype(np.float32)
+    nlo, nhi = np.float32([-1, -1, -1, 0]), np.float32([1, 2, 1, 0])
+    f = mlp.hist_features(nlo, nhi, lo, hi, 3, 24)
     assert f.shape == (200,)
     for a in range(3):
-        assert abs(f[a * 32:(a + 1) * 32].sum() - 1) < 1e-6
-        assert abs(f[96 + a * 32:96 + a * 32 + 16].sum() - 1) < 1e-6
-        assert abs(f[96 + a * 32 + 16:96 + (a + 1) * 32].sum() - 1) < 1e-6
+        assert abs(f[a * 64:a * 64 + 32].sum() - 1) < 1e-5
+        assert abs(f[a * 64 + 32:(a + 1) * 64].sum() - 1) < 1e-5
     third = np.float32(1) / np.float32(3)
     assert np.array_equal(f[192:195], np.float32([2 * third, 3 * third, 2 * third]))
     assert f[195] == np.float32(3) / np.float32(24)
+    assert f[196] == np.float32(100) / np.float32(1024)
+    # x in [-1, 1]: p_16 = 0 exactly; a bound on it
+    lo2 = np.zeros((1, 3), np.float32)
+    f2 = mlp.hist_features(nlo, nhi, lo2, lo2, 0, 24)
+    assert f2[16] == 1.0 and f2[32 + 15] == 1.0
+    assert mlp.exact_label(nlo, nhi, 0, np.float32(0.0)) == 16
+    assert mlp.exact_label(nlo, nhi, 1, np.float32(-0.99)) == 32
