@@ -66,6 +66,9 @@ def parse():
     ap.add_argument("--no-compare", action="store_true", help="skip the learned / exact comparison arms")
     ap.add_argument("--cost-frame", type=int, default=17, help="frame whose trees are costed in the comparison")
     ap.add_argument("--cpu-frames", type=int, default=2)
+    ap.add_argument("--split", default="frames", choices=["frames", "rays"],
+                    help="multi-GPU split: whole frames per rank (default), or row bands of every frame "
+                         "gathered over NCCL (the build replicated on every rank)")
     return ap.parse_args()
 
 
@@ -253,7 +256,7 @@ def run_ours(args):
     import torch
     import torch.distributed as dist
     import hulktracer_b200 as hk
-    from hulktracer_b200.shard import frames_for_rank, reduce_job
+    from hulktracer_b200.shard import frames_for_rank, gather_rows, reduce_job, rows_for_rank
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -281,7 +284,11 @@ def run_ours(args):
         ctx.set_frame_shading(hk.SHADE_MIRROR)
     rgba = torch.zeros(W * H, dtype=torch.int32, device="cuda")
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
-    frames = frames_for_rank(args.warmup, args.steps, rank, world)
+    rays_split = args.split == "rays"
+    # rays split: every rank takes part in every frame with its band of rows
+    frames = frames_for_rank(args.warmup, args.steps, 0 if rays_split else rank, 1 if rays_split else world)
+    y0, y1 = rows_for_rank(H, rank, world) if rays_split else (0, H)
+    band = torch.zeros(W * (y1 - y0), dtype=torch.int32, device="cuda")
     mats_all = {f: frame_mats(sc, f) for f in list(range(args.warmup)) + frames}
     # pinned host inputs / outputs for the e2e leg
     pin_mats = {f: (torch.from_numpy(m).pin_memory() if m is not None else None) for f, m in mats_all.items()}
@@ -289,8 +296,17 @@ def run_ours(args):
 
     def do_frame(f, use_graph=True):
         m = pin_mats[f]
-        ctx.frame(m.numpy() if m is not None else None, sc.camera, sc.lights, W, H, rgba.data_ptr(), mode, variant,
-                  use_graph)
+        if not rays_split:
+            ctx.frame(m.numpy() if m is not None else None, sc.camera, sc.lights, W, H, rgba.data_ptr(), mode,
+                      variant, use_graph)
+            return
+        # this rank's band of the frame on its own replica, then the gather
+        if m is not None:
+            ctx.transform(m.numpy())
+        ctx._check(ctx.L.hk_build(ctx.h, mode, None))
+        ctx.render_rows_device(sc.camera, sc.lights, W, H, y0, y1, band.data_ptr(), variant,
+                               hk.SHADE_MIRROR if "mirror" in sc.extra else hk.SHADE_CPU)
+        rgba.copy_(gather_rows(band, rank, world, W, H))
 
     with torch.cuda.stream(stream):
         for f in range(args.warmup):
@@ -357,12 +373,16 @@ def run_ours(args):
         line = {
             "metric": "Mrays/s (build+trace+shade per frame)", "value": total_rays / t_dev / 1e6, "unit": "Mrays/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": 1000.0 * t_dev / args.steps, "higher_is_better": True, "scaling": "weak",
+            "ms_per_step": 1000.0 * t_dev / args.steps, "higher_is_better": True,
+            "scaling": "strong" if rays_split else "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scene)",
             "config": {"workload": workload_name(sc), "build": "GPU %s SAH (32 bins/axis%s), per frame" % (
                            args.mode, ", exact on nodes <= %d refs" % args.exact_max if args.exact_max else ""),
-                       "traversal": args.variant, "graph": "one CUDA graph per frame",
-                       "l2": "flushed (256 MB write) between frames", "parallelism": "frames sharded over %d GPU(s)" % world},
+                       "traversal": args.variant,
+                       "graph": "stages launched per frame (row bands)" if rays_split else "one CUDA graph per frame",
+                       "l2": "flushed (256 MB write) between frames",
+                       "parallelism": ("row bands of every frame over %d GPU(s), framebuffer all_gather" % world)
+                       if rays_split else "frames sharded over %d GPU(s)" % world},
             "e2e": {"value": total_rays / t_e2e / 1e6, "unit": "Mrays/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": W * H * 4, "ms_per_step": 1000.0 * t_e2e / args.steps,
                     "timing": "host clock per frame (synchronise, call, image read-back, synchronise)"},

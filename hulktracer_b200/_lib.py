@@ -36,7 +36,7 @@ class Config(C.Structure):
                 ("max_depth", C.c_uint32), ("leaf_size", C.c_uint32), ("bins", C.c_uint32),
                 ("short_stack", C.c_uint32), ("block_size", C.c_uint32), ("blocks_per_sm", C.c_uint32),
                 ("max_refs", C.c_uint32), ("topk", C.c_uint32), ("fallback_ratio", C.c_float),
-                ("exact_max", C.c_uint32)]
+                ("exact_max", C.c_uint32), ("spin_limit", C.c_uint32), ("max_steps", C.c_uint32)]
 
 
 class TuneResult(C.Structure):
@@ -109,6 +109,7 @@ def load(path: str = LIB_PATH):
         "hk_camera_rays": [vp, f32p, u32, u32, f32p],
         "hk_render": [vp, f32p, f32p, u32, u32, u32, C.c_int, C.c_int, u32p],
         "hk_render_device": [vp, f32p, f32p, u32, u32, u32, C.c_int, C.c_int, vp],
+        "hk_render_rows_device": [vp, f32p, f32p, u32, u32, u32, u32, u32, C.c_int, C.c_int, vp],
         "hk_shade_picture": [vp, f32p, f32p, u32, f32p, u32, u32p],
         "hk_frame": [vp, f32p, f32p, f32p, u32, u32, u32, C.c_int, C.c_int, C.c_int, vp, C.POINTER(TreeStats)],
         "hk_get_ray_counts": [vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)],
@@ -126,6 +127,7 @@ def load(path: str = LIB_PATH):
         "hk_mlp_dataset": [vp, f32p, vp, u32, C.POINTER(C.c_uint32)],
         "hk_mlp_train": [vp, u32, u32, C.c_float, C.c_uint64, f32p],
         "hk_set_proposal_log": [vp, C.c_int],
+        "hk_set_debug_flags": [vp, u32],
         "hk_get_proposal_log": [vp, vp, u32, C.POINTER(C.c_uint32)],
         "hk_batch_create": [vp, C.POINTER(C.c_void_p)],
         "hk_batch_destroy": [vp],

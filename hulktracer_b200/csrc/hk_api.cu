@@ -118,6 +118,7 @@ struct hk_ctx {
     uint32_t rec_cap = 0;
     bool recording = false;
     bool prop_log = false;
+    uint32_t debug_flags = 0;
 };
 
 // current tree arrays (imported or built)
@@ -514,6 +515,10 @@ static hk_status sync_tree_sizes(hk_ctx *c) {
     if (c->tree_on_device_counts) {
         hk_status s = build_read_stats(c->build, c->stream, &c->stats);
         if (s != HK_OK) {
+            // the builder's output is not a tree: nothing may trace or export it
+            c->tree_valid = false;
+            c->tree_built = false;
+            c->tree_on_device_counts = false;
             char msg[96];
             snprintf(msg, sizeof msg, "build failed (error bits 0x%x)", c->build.last_err);
             return fail(c, s, msg);
@@ -584,6 +589,13 @@ hk_status hk_tree_stats_get(hk_ctx *c, hk_tree_stats *st) {
     hk_status s = sync_tree_sizes(c);
     if (s != HK_OK) return s;
     *st = c->stats;
+    return HK_OK;
+}
+
+hk_status hk_set_debug_flags(hk_ctx *c, uint32_t flags) {
+    if (!c || (flags & ~1u)) return HK_E_ILLEGAL_INPUT;
+    c->debug_flags = flags;
+    invalidate_graph(c);
     return HK_OK;
 }
 
@@ -681,6 +693,8 @@ static BuildParams build_params(hk_ctx *c, hk_build_mode mode) {
     p.exact_max = c->cfg.exact_max;
     p.record = c->recording ? 1 : 0;
     p.prop_log = c->prop_log ? 1 : 0;
+    p.spin_limit = c->cfg.spin_limit;
+    p.debug_flags = c->debug_flags;
     c->build.learn = &c->learn;
     return p;
 }
@@ -812,7 +826,7 @@ static hk_status trace_enqueue(hk_ctx *c, const float4 *d_rays, uint32_t n, cons
     L.counters = c->counters.p;
     L.err = c->errw.p;
     L.stack_depth = c->cfg.short_stack;
-    L.max_steps = 1u << 26;
+    L.max_steps = c->cfg.max_steps ? c->cfg.max_steps : (1u << 26);
     L.variant = (int)v;
     L.count = c->counting;
     L.occlusion = occlusion;
@@ -914,13 +928,15 @@ static hk_status render_buffers(hk_ctx *c, uint32_t npix, uint32_t nl) {
 }
 
 // camera + lights already in c->cam / c->lights
+// rows row0 .. row0 + h - 1 of a w x full_h frame (full_h 0: the frame is
+// w x h) into d_rgba, w x h pixels
 static hk_status render_enqueue(hk_ctx *c, uint32_t nl, uint32_t w, uint32_t h, hk_variant v, int shade,
-                                uint32_t *d_rgba) {
+                                uint32_t *d_rgba, uint32_t row0 = 0, uint32_t full_h = 0) {
     uint32_t npix = w * h;
     c->last_primary = npix;
     c->last_shade = shade;
     const bool tiled = (w % 8u == 0) && (h % 4u == 0);
-    HK_CUDA(c, launch_camera_rays(c->cam.p, w, h, c->rays.p, c->stream, tiled));
+    HK_CUDA(c, launch_camera_rays(c->cam.p, w, h, c->rays.p, c->stream, tiled, row0, full_h));
     // ropes: each pixel's last leaf, where its shadow rays may start
     const bool hint = v == HK_TRACE_ROPES && shade != HK_SHADE_PICTURE;
     hk_status s = trace_enqueue(c, c->rays.p, npix, nullptr, v, c->hits.p, false, hint ? c->hleaf.p : nullptr);
@@ -968,6 +984,25 @@ hk_status hk_render_device(hk_ctx *c, const float *cam16, const float *lights8, 
     HK_CUDA(c, cudaMemcpyAsync(c->cam.p, cam16, 64, cudaMemcpyHostToDevice, c->stream));
     if (nl) HK_CUDA(c, cudaMemcpyAsync(c->lights.p, lights8, (size_t)nl * 32, cudaMemcpyHostToDevice, c->stream));
     return render_enqueue(c, nl, w, h, v, shade, d_rgba);
+}
+
+hk_status hk_render_rows_device(hk_ctx *c, const float *cam16, const float *lights8, uint32_t nl, uint32_t w,
+                                uint32_t h, uint32_t y0, uint32_t y1, hk_variant v, int shade, uint32_t *d_rgba) {
+    if (!c || !cam16 || !d_rgba) return HK_E_ILLEGAL_INPUT;
+    if (y0 >= y1 || y1 > h) return fail(c, HK_E_ILLEGAL_INPUT, "row range");
+    if ((size_t)w * h == 0 || (size_t)w * h > (1u << 28)) return fail(c, HK_E_ILLEGAL_INPUT, "image size");
+    if (shade != HK_SHADE_CPU && shade != HK_SHADE_PICTURE && shade != HK_SHADE_MIRROR)
+        return fail(c, HK_E_ILLEGAL_INPUT, "shade mode");
+    if (shade == HK_SHADE_MIRROR && !c->has_mirrors) return fail(c, HK_E_STATE, "hk_scene_set_mirrors first");
+    hk_status s = validate_lights(c, lights8, nl);
+    if (s != HK_OK) return s;
+    cudaSetDevice(c->device);
+    const uint32_t rows = y1 - y0;
+    s = render_buffers(c, w * rows, nl);
+    if (s != HK_OK) return s;
+    HK_CUDA(c, cudaMemcpyAsync(c->cam.p, cam16, 64, cudaMemcpyHostToDevice, c->stream));
+    if (nl) HK_CUDA(c, cudaMemcpyAsync(c->lights.p, lights8, (size_t)nl * 32, cudaMemcpyHostToDevice, c->stream));
+    return render_enqueue(c, nl, w, rows, v, shade, d_rgba, y0, h);
 }
 
 hk_status hk_render(hk_ctx *c, const float *cam16, const float *lights8, uint32_t nl, uint32_t w, uint32_t h,
@@ -1255,7 +1290,7 @@ hk_status hk_batch_trace_device(hk_batch *b, const float *d_rays8, const uint32_
     L.counters = c->counters.p;
     L.err = c->errw.p;
     L.stack_depth = c->cfg.short_stack;
-    L.max_steps = 1u << 26;
+    L.max_steps = c->cfg.max_steps ? c->cfg.max_steps : (1u << 26);
     L.variant = (int)v;
     L.count = c->counting;
     L.block = (int)c->cfg.block_size;

@@ -135,10 +135,15 @@ __device__ __forceinline__ T block_excl(T v, T *sh_warp, T &total) {
 // already running and publishes its aggregate without waiting. A tile's flag
 // is (tag << 2) | status, status 1 = aggregate, 2 = inclusive prefix; the tag
 // (build epoch x 64 + level) makes flags of earlier levels and builds stale,
-// so the flag arrays are never cleared. Waits are bounded (kSpinLimit polls):
-// one that runs out sets error bit 4 and counts the tile as zero.
+// so the flag arrays are never cleared. Waits are bounded (the build's spin
+// limit, kSpinLimit polls by default): one that runs out sets error bit 4 and
+// counts the tile as zero; every later kernel of the build then returns at
+// once (level_aborted), so the inconsistent level is never read.
 // ---------------------------------------------------------------------------
 constexpr uint32_t kSpinLimit = 1u << 22;
+// error bits after which the build's data may be inconsistent: a wait ran
+// out (4), a partition / decision count mismatch (8), a plan bound (16)
+constexpr uint32_t kErrAbort = 4u | 8u | 16u;
 
 // Kernels launched as programmatic dependents (launch_pdl) start before their
 // predecessor in the stream has finished; this waits until it has, with its
@@ -147,7 +152,7 @@ __device__ __forceinline__ void wait_prior_grid() { asm volatile("griddepcontrol
 
 template <class T>
 __device__ T lookback(const uint32_t *flags, const T *aggs, const T *incls, uint32_t tile, uint32_t tag,
-                      uint32_t *err) {
+                      uint32_t *err, uint32_t spin_limit) {
     const int lane = threadIdx.x & 31;
     T excl = vzero<T>();
     int32_t p = (int32_t)tile - 1;
@@ -163,7 +168,7 @@ __device__ T lookback(const uint32_t *flags, const T *aggs, const T *incls, uint
                     st = f & 3u;
                     break;
                 }
-                if (spins >= kSpinLimit) {
+                if (spins >= spin_limit) {
                     atomicOr(err, 4u);
                     have = false;
                     st = 2;
@@ -217,7 +222,7 @@ __device__ __forceinline__ void scan_tile(const Op &op, uint32_t tile, uint32_t 
         *reinterpret_cast<volatile uint32_t *>(flags + tile) = (tag << 2) | (tile == 0 ? 2u : 1u);
     }
     if (threadIdx.x < 32) {
-        const T e = tile ? lookback(flags, aggs, incls, tile, tag, op.err()) : vzero<T>();
+        const T e = tile ? lookback(flags, aggs, incls, tile, tag, op.err(), op.A.spin_limit) : vzero<T>();
         if (threadIdx.x == 0) {
             if (tile) {
                 incls[tile] = vadd(e, tot);
@@ -457,7 +462,20 @@ struct LevelArgs {
     uint32_t *rec_rows, rec_cap;
     float fallback_ratio;
     uint32_t topk;
+    uint32_t spin_limit;       // polls before a bounded wait gives up
+    uint32_t withhold_level;   // test aid: at this level plan tile 0 never publishes its done flag
 };
+
+// true (on every thread of the CTA alike) when an earlier kernel of this build
+// hit an error after which its data may be inconsistent; the kernel then does
+// nothing. Called after wait_prior_grid by every thread.
+__device__ __forceinline__ bool level_aborted(const LevelArgs &A) {
+    __shared__ uint32_t s_abort;
+    __syncthreads();
+    if (threadIdx.x == 0) s_abort = __ldcg(A.err) & kErrAbort;
+    __syncthreads();
+    return s_abort != 0;
+}
 
 __global__ void k_tri_bounds(const float4 *__restrict__ V, const uint4 *__restrict__ T, uint32_t nt, float4 *lo,
                              float4 *hi) {
@@ -906,6 +924,7 @@ __global__ void __launch_bounds__(256, 3) k_hist(LevelArgs A) {
     __shared__ ExactCtaSmem XS;
     __shared__ int s_last;
     __shared__ uint32_t s_tally[5];
+    if (level_aborted(A)) return;
     Tally tally;
     const uint32_t wib = threadIdx.x >> 5, lane = threadIdx.x & 31u;
     const uint32_t nch = min(A.lc->n_chunks, A.cap_chunks);
@@ -1018,6 +1037,7 @@ __global__ void __launch_bounds__(256, 5) k_small(LevelArgs A) {
     __shared__ __align__(16) uint32_t HS[8][kHist];
     __shared__ uint32_t s_tally[5];
     wait_prior_grid();
+    if (level_aborted(A)) return;
     Tally tally;
     const uint32_t wib = threadIdx.x >> 5, lane = threadIdx.x & 31u;
     const uint32_t nodes = A.lc->nodes;
@@ -1123,6 +1143,7 @@ __global__ void __launch_bounds__(256, 1) k_learn(LevelArgs A) {
     __shared__ uint32_t s_tally[5];
     __shared__ uint32_t s_stat[2];
     wait_prior_grid();
+    if (level_aborted(A)) return;
     Tally tally;
     uint32_t n_learned = 0, n_fallback = 0;
     const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
@@ -1617,7 +1638,7 @@ __device__ void ref_tile(const RefOp &R, uint32_t rt, uint32_t nr, uint32_t tag,
     if (threadIdx.x < 32) {
         // the tile-0 rule is kept for the look-back: before tile 0 is zero
         const uint2 c = (rt && !__shfl_sync(0xffffffffu, starts ? 1u : 0u, 0))
-                            ? lookback(flags, aggs, incls, rt, tag, A.err)
+                            ? lookback(flags, aggs, incls, rt, tag, A.err, A.spin_limit)
                             : make_uint2(0, 0);
         if (threadIdx.x == 0) {
             if (!tot.h) {
@@ -1629,7 +1650,7 @@ __device__ void ref_tile(const RefOp &R, uint32_t rt, uint32_t nr, uint32_t tag,
         }
     }
     __syncthreads();
-    wait_plan();
+    if (!wait_plan()) return;   // uniform: the scatter needs the plan's destinations
     uint2 run = ex.h ? ex.v : vadd(ex.v, sh.carry);
 #pragma unroll
     for (int k = 0; k < kScanItems; k++) {
@@ -1657,7 +1678,9 @@ __global__ void __launch_bounds__(kScanThreads, 6) k_plan_refs(LevelArgs A, uint
     __shared__ U5 sxp;
     __shared__ RefTileSmem shr_seg;
     __shared__ uint32_t s_tile;
+    __shared__ uint32_t s_wait_ok;
     wait_prior_grid();
+    if (level_aborted(A)) return;
     const PlanOp P{A};
     const RefOp R{A};
     const uint32_t tag = level_tag(A);
@@ -1676,26 +1699,34 @@ __global__ void __launch_bounds__(kScanThreads, 6) k_plan_refs(LevelArgs A, uint
             scan_tile(P, t, nn, tag, pc, pflags, paggs, pincls, shp, sxp, [&] {
                 __threadfence();
                 __syncthreads();
-                if (threadIdx.x == 0) *reinterpret_cast<volatile uint32_t *>(pdone + t) = tag;
+                if (threadIdx.x == 0 && !(t == 0 && A.level == A.withhold_level))
+                    *reinterpret_cast<volatile uint32_t *>(pdone + t) = tag;
             });
         } else if (t < ntn + ntr) {
             const uint32_t rt = t - ntn;
-            auto wait_plan = [&] {
+            // true when every plan tile of this tile's nodes has published
+            // its reference destinations; a wait that runs out leaves the
+            // tile's scatter undone (error bit 4, the build reports failure)
+            auto wait_plan = [&]() -> bool {
                 if (threadIdx.x == 0) {
+                    uint32_t ok = 1;
                     const uint32_t r0 = rt * kTile, r1 = min(nr, r0 + kTile) - 1;
                     const uint32_t k0 = A.ref_node[r0] / kPlanTile, k1 = A.ref_node[r1] / kPlanTile;
-                    for (uint32_t k = k0; k <= k1 && k < ntn; k++) {
+                    for (uint32_t k = k0; k <= k1 && k < ntn && ok; k++) {
                         for (uint32_t spins = 0; __ldcv(pdone + k) != tag; spins++) {
-                            if (spins >= kSpinLimit) {
+                            if (spins >= A.spin_limit) {
                                 atomicOr(A.err, 4u);
+                                ok = 0;
                                 break;
                             }
                             __nanosleep(32);
                         }
                     }
                     __threadfence();
+                    s_wait_ok = ok;
                 }
                 __syncthreads();
+                return s_wait_ok != 0;
             };
             ref_tile(R, rt, nr, tag, stop, rflags, raggs, rincls, shr_seg, wait_plan);
         } else {
@@ -1906,6 +1937,8 @@ cudaError_t build_launch(BuildState &S, const float4 *verts, const uint4 *tris, 
     A.prop_log = (A.learned && S.p.prop_log) ? S.prop_log : nullptr;
     A.fallback_ratio = S.p.fallback_ratio;
     A.topk = S.p.topk;
+    A.spin_limit = S.p.spin_limit ? S.p.spin_limit : kSpinLimit;
+    A.withhold_level = (S.p.debug_flags & 1u) ? 1u : 0xffffffffu;
     if (S.learn) {
         A.rec_X = S.learn->rec_X;
         A.rec_y = S.learn->rec_y;

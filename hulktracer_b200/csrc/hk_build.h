@@ -22,6 +22,8 @@ struct BuildParams {
                                 // the exactly searched nodes of 33..1024 references
     uint32_t exact_max = 0;     // nodes with at most this many refs (0, or 32..1024) take the exact SAH
     int prop_log = 0;           // learned mode: log every proposer row's proposed bins by compact node
+    uint32_t spin_limit = 0;    // polls before a bounded wait gives up (0: the default, 4M)
+    uint32_t debug_flags = 0;   // test aid, bit 0: plan tile 0 of level 1 withholds its done flag
 };
 
 // learned-proposer buffers owned by the context (device pointers)

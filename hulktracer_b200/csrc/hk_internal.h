@@ -94,8 +94,9 @@ cudaError_t launch_transform(const float4 *rest, const uint32_t *part, uint32_t 
                              float4 *out, uint32_t *box_ord, cudaStream_t s);
 cudaError_t launch_box_finish(const uint32_t *box_ord, float *box, cudaStream_t s);
 cudaError_t launch_box(const float4 *verts, uint32_t nv, uint32_t *box_ord, float *box, cudaStream_t s);
+// rays of rows row0 .. row0 + h - 1 of a w x full_h image (full_h 0: h)
 cudaError_t launch_camera_rays(const float *cam16_dev, uint32_t w, uint32_t h, float4 *rays, cudaStream_t s,
-                               bool tiled = false);
+                               bool tiled = false, uint32_t row0 = 0, uint32_t full_h = 0);
 cudaError_t launch_shadow_rays(const float4 *rays, const hk_hit *hits, const TriRec *tris, uint32_t npix,
                                const float *lights_dev, uint32_t nl, const uint32_t *leaf_hint, float4 *srays,
                                uint32_t *slot, uint32_t *spix, uint32_t *scount, cudaStream_t s);

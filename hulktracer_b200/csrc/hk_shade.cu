@@ -193,13 +193,16 @@ __device__ __forceinline__ uint32_t pixel_of(uint32_t i, uint32_t w, bool tiled)
     return y * w + x;
 }
 
+// The rays of rows row0 .. row0 + h - 1 of a w x full_h image (the whole
+// image when row0 = 0 and full_h = h); ray i belongs to pixel pixel_of(i) of
+// that band.
 __global__ void k_camera_rays(const float *__restrict__ cam, uint32_t w, uint32_t h, float4 *__restrict__ rays,
-                              bool tiled) {
+                              bool tiled, uint32_t row0, uint32_t full_h) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= w * h) return;
     uint32_t pix = pixel_of(i, w, tiled);
-    uint32_t x = pix % w, y = pix / w;
-    float u = __fdiv_rn((float)x, (float)w), v = __fdiv_rn((float)y, (float)h);
+    uint32_t x = pix % w, y = pix / w + row0;
+    float u = __fdiv_rn((float)x, (float)w), v = __fdiv_rn((float)y, (float)full_h);
     float4 from = make_float4(cam[0], cam[1], cam[2], cam[3]);
     float d[4];
     for (int k = 0; k < 4; k++) {
@@ -213,9 +216,9 @@ __global__ void k_camera_rays(const float *__restrict__ cam, uint32_t w, uint32_
 }
 
 cudaError_t launch_camera_rays(const float *cam16_dev, uint32_t w, uint32_t h, float4 *rays, cudaStream_t s,
-                               bool tiled) {
+                               bool tiled, uint32_t row0, uint32_t full_h) {
     uint32_t n = w * h;
-    if (n) k_camera_rays<<<blocks_for(n, 256), 256, 0, s>>>(cam16_dev, w, h, rays, tiled);
+    if (n) k_camera_rays<<<blocks_for(n, 256), 256, 0, s>>>(cam16_dev, w, h, rays, tiled, row0, full_h ? full_h : h);
     return cudaGetLastError();
 }
 

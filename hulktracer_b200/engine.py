@@ -226,6 +226,13 @@ class Context:
         self._check(self.L.hk_render_device(self.h, ptr(_f32(cam).ravel()), ptr(lights), lights.shape[0], w, h,
                                             int(variant), int(shade), C.c_void_p(d_rgba)))
 
+    def render_rows_device(self, cam, lights, w, h, y0, y1, d_rgba: int, variant=_lib.SHORTSTACK,
+                           shade=_lib.SHADE_CPU):
+        """Rows y0 .. y1 - 1 of the w x h frame into d_rgba (w x (y1 - y0))."""
+        lights = _f32(lights).reshape(-1, 8)
+        self._check(self.L.hk_render_rows_device(self.h, ptr(_f32(cam).ravel()), ptr(lights), lights.shape[0], w, h,
+                                                 y0, y1, int(variant), int(shade), C.c_void_p(d_rgba)))
+
     def shade_picture(self, rays, hit4, lights):
         r = _f32(rays).reshape(-1, 8)
         lights = _f32(lights).reshape(-1, 8)
@@ -247,6 +254,11 @@ class Context:
                                     C.byref(st) if st is not None else None))
         return st.as_dict() if st is not None else None
 
+
+    def set_debug_flags(self, flags):
+        """Test aid (hk_set_debug_flags): bit 0 withholds one plan tile's done
+        flag so that the build's bounded waits run out."""
+        self._check(self.L.hk_set_debug_flags(self.h, int(flags)))
 
     # -- learned split proposer --
     def set_proposal_log(self, on=True):

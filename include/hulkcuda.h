@@ -113,6 +113,12 @@ typedef struct hk_config {
                                  the exact SAH over their references' bounds (the
                                  reference's candidate set) instead of 32 bins; 0 =
                                  binned everywhere (default), else 32..1024 */
+    uint32_t spin_limit;      /* builder: polls before a bounded device-side wait (a
+                                 scan look-back, a reference tile waiting for its
+                                 plan tile) gives up; the build then stops and
+                                 returns HK_E_DEVICE_TIMEOUT (0 = 4M polls) */
+    uint32_t max_steps;       /* traversal: node steps per ray before the trace stops
+                                 the ray and returns HK_E_BOUNDS (0 = 2^26) */
 } hk_config;
 
 typedef struct hk_tree_stats {
@@ -144,6 +150,11 @@ hk_status hk_destroy(hk_ctx *ctx);
 const char *hk_last_error(const hk_ctx *ctx);
 /* run subsequent work on this cudaStream_t (NULL = the context's own stream) */
 hk_status hk_set_stream(hk_ctx *ctx, void *cuda_stream);
+/* Test aid for failure detection: bit 0 makes every later build withhold the
+ * done flag of the first plan tile of tree level 1, so the reference tiles
+ * that wait for it run out of polls (hk_config.spin_limit) and the build
+ * returns HK_E_DEVICE_TIMEOUT without hanging; 0 restores normal builds. */
+hk_status hk_set_debug_flags(hk_ctx *ctx, uint32_t flags);
 hk_status hk_synchronize(hk_ctx *ctx);
 
 /* ---- scene (Scene::m_vertices / m_vertexIndices / m_sceneBox) ---- */
@@ -225,6 +236,15 @@ hk_status hk_render(hk_ctx *ctx, const float *cam16, const float *lights8, uint3
                     uint32_t h, hk_variant variant, int shade, uint32_t *rgba);
 hk_status hk_render_device(hk_ctx *ctx, const float *cam16, const float *lights8, uint32_t nl,
                            uint32_t w, uint32_t h, hk_variant variant, int shade, uint32_t *d_rgba);
+/* Rows y0 .. y1 - 1 of the w x h frame (ray-tile sharding of one frame over
+ * GPUs: every rank renders its band of rows of the same frame on its own
+ * replica of the scene and tree). d_rgba holds w x (y1 - y0) pixels, index
+ * (y - y0) * w + x; every pixel equals the one hk_render_device writes for
+ * the whole frame. No reference counterpart (the reference renders on one
+ * device). */
+hk_status hk_render_rows_device(hk_ctx *ctx, const float *cam16, const float *lights8, uint32_t nl, uint32_t w,
+                                uint32_t h, uint32_t y0, uint32_t y1, hk_variant variant, int shade,
+                                uint32_t *d_rgba);
 /* ShadePicture over caller hits: hit4 = float4(normal.xyz, t) per pixel as the
  * reference's pHitDataArray, t == FLT_MAX for a miss. */
 hk_status hk_shade_picture(hk_ctx *ctx, const float *rays8, const float *hit4, uint32_t n,

@@ -600,6 +600,75 @@ static int isect_acc(const float *o, const float *d, const float *p1, const floa
     return 0;
 }
 
+/* checkRayToPoly, SharedFunctions.hpp:47-103 -- the form the reference's
+ * OpenCL kernels call (GPU_common.cl:46-72, GPUTrace_bruteforce.cl:30-42):
+ * the normal recomputed per test, normalize(e0 x e1 + e1 x e2 + e2 x e0), and
+ * det, s1, s2 by fused multiply-add. Restated with IEEE single precision in
+ * the source's order (OpenCL lets an implementation relax division, sqrt and
+ * dot; this is the correctly rounded reading): dot over four lanes as
+ * ((x0 y0 + x1 y1) + x2 y2) + x3 y3, cross with w = 0, normalize as
+ * v * (1 / sqrt(v . v)), pow(e01, 2) as the rounded square. */
+static float dot4_seq(const float *a, const float *b) {
+    return ((a[0] * b[0] + a[1] * b[1]) + a[2] * b[2]) + a[3] * b[3];
+}
+
+static void cross_w0(const float *a, const float *b, float *o) {
+    o[0] = a[1] * b[2] - a[2] * b[1];
+    o[1] = a[2] * b[0] - a[0] * b[2];
+    o[2] = a[0] * b[1] - a[1] * b[0];
+    o[3] = 0.0f;
+}
+
+static int isect_poly(const float *o, const float *d, const float *p1, const float *p2, const float *p3,
+                      float *t_out, float *pos_out) {
+    float e0[4], e1[4], e2[4], c0[4], c1[4], c2[4], n[4];
+    sub4(p2, p1, e0);
+    sub4(p3, p1, e1);
+    sub4(p3, p2, e2);
+    cross_w0(e0, e1, c0);
+    cross_w0(e1, e2, c1);
+    cross_w0(e2, e0, c2);
+    for (int k = 0; k < 4; k++) n[k] = (c0[k] + c1[k]) + c2[k];
+    const float inv = 1.0f / sqrtf(dot4_seq(n, n));
+    for (int k = 0; k < 4; k++) n[k] = n[k] * inv;
+    float denum = dot4_seq(n, d);
+    if (fabsf(denum) < FLT_EPSILON) return 0;
+    denum = 1.0f / denum;
+    float v[4];
+    sub4(p1, o, v);
+    float time = dot4_seq(n, v) * denum;
+    if (time < 0) return 0;
+    float hp[4], hq[4];
+    for (int k = 0; k < 4; k++) hp[k] = o[k] + d[k] * time;
+    sub4(hp, p1, hq);
+    float q0 = dot4_seq(e0, hq), q1 = dot4_seq(e1, hq);
+    float e00 = dot4_seq(e0, e0), e01 = dot4_seq(e0, e1), e11 = dot4_seq(e1, e1);
+    float det = fmaf(e00, e11, -(e01 * e01));
+    float s1 = fmaf(e11, q0, -(e01 * q1));
+    float s2 = fmaf(e00, q1, -(e01 * q0));
+    if (s1 >= 0 && s2 >= 0 && (s1 + s2) <= det) {
+        *t_out = time;
+        memcpy(pos_out, hp, 16);
+        return 1;
+    }
+    return 0;
+}
+
+/* which intersection form the traversals use: 0 checkRayToPolyACC over the
+ * tree's cache (the CPU path), 1 checkRayToPoly from the vertices */
+static int g_isect_form = 0;
+void hko_set_isect_form(int form) { g_isect_form = form; }
+
+static int isect_tri_form(const hko_tree *t, uint32_t poly, const float *o, const float *d, float *tt, float *pos) {
+    const float *p1 = t->verts + 4 * (size_t)t->tris[4 * poly];
+    if (g_isect_form == 1) {
+        const float *p2 = t->verts + 4 * (size_t)t->tris[4 * poly + 1];
+        const float *p3 = t->verts + 4 * (size_t)t->tris[4 * poly + 2];
+        return isect_poly(o, d, p1, p2, p3, tt, pos);
+    }
+    return isect_acc(o, d, p1, t->cache + 16 * (size_t)poly, tt, pos);
+}
+
 /* KDTreeCPU::testNodePolygons, KDTreeCPU.cpp:255-283 */
 static int test_leaf(const hko_tree *t, const uint32_t *node, const float *o, const float *d, hit_t *hit,
                      hko_counters *cnt) {
@@ -609,9 +678,8 @@ static int test_leaf(const hko_tree *t, const uint32_t *node, const float *o, co
         uint32_t poly = t->refs[i];
         cnt->refs++;
         cnt->tests++;
-        const float *p1 = t->verts + 4 * (size_t)t->tris[4 * poly];
         float tt, pos[4];
-        if (isect_acc(o, d, p1, t->cache + 16 * (size_t)poly, &tt, pos)) {
+        if (isect_tri_form(t, poly, o, d, &tt, pos)) {
             if (tt < hit->t) {
                 ret = 1;
                 hit->t = tt;
@@ -805,10 +873,9 @@ int hko_trace_one(const hko_tree *t, int variant, int D, const float *ray, float
     if (variant == HKO_BRUTE) {
         /* GPUTrace_bruteforce.cl:30-42 over the cached intersection form */
         for (uint32_t i = 0; i < t->nt; i++) {
-            const float *p1 = t->verts + 4 * (size_t)t->tris[4 * i];
             float tt, pos[4];
             cnt->tests++;
-            if (isect_acc(o, d, p1, t->cache + 16 * (size_t)i, &tt, pos)) {
+            if (isect_tri_form(t, i, o, d, &tt, pos)) {
                 r = 1;
                 if (tt < hit.t) {
                     hit.t = tt;

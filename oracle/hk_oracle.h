@@ -70,6 +70,12 @@ typedef struct {
     uint32_t reduction;    /* c_reductionFactor (every k-th triangle sampled) */
 } hko_sah_params;
 
+/* intersection form of every traversal: 0 checkRayToPolyACC over the tree's
+ * cache (SharedFunctions.hpp:105-150, the CPU path; default), 1
+ * checkRayToPoly from the vertices (SharedFunctions.hpp:47-103, the form the
+ * reference's OpenCL kernels call) */
+void hko_set_isect_form(int form);
+
 /* ---- vector helpers (exposed for tests) ---- */
 float hko_dot4(const float *a, const float *b);
 void hko_normalize(float *v, int mode);

@@ -16,6 +16,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 
 SHORTSTACK, FULLSTACK, RESTART, RESTART_EARLY, ROPES, BRUTE = range(6)
 NORM_SSE, NORM_IEEE = 0, 1
+ISECT_ACC, ISECT_POLY = 0, 1
 
 _f32p = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
 _u32p = np.ctypeslib.ndpointer(dtype=np.uint32, flags="C_CONTIGUOUS")
@@ -102,6 +103,7 @@ class Oracle:
         L.hko_build_binned.argtypes = [_f32p, _u32p, C.c_uint32, _f32p, C.POINTER(_BinnedParams), pp,
                                        C.POINTER(C.c_uint32), pp, C.POINTER(C.c_uint32)]
         L.hko_free.argtypes = [C.c_void_p]
+        L.hko_set_isect_form.argtypes = [C.c_int]
         L.hko_tree_cost.restype = C.c_double
         L.hko_tree_cost.argtypes = [_u32p, C.c_uint32, _f32p, C.c_double, C.c_double]
         L.hko_node_boxes.argtypes = [_u32p, C.c_uint32, _f32p, _f32p]
@@ -119,6 +121,11 @@ class Oracle:
                                         C.c_int, _u32p, C.c_int]
 
     # -- helpers --
+    def set_isect_form(self, form):
+        """0: checkRayToPolyACC over the cache (default); 1: checkRayToPoly from
+        the vertices (the reference's OpenCL form)."""
+        self.lib.hko_set_isect_form(int(form))
+
     def dot4(self, a, b):
         return self.lib.hko_dot4(_c(a, np.float32), _c(b, np.float32))
 
