@@ -111,6 +111,7 @@ struct hk_ctx {
     LearnBuffers learn;
     DevBuf<float> mlp_params, mlp_grads, mlp_m, mlp_v;
     DevBuf<uint32_t> mlp_w1p, mlp_w2p, mlp_w3p, mlp_w4p;
+    DevBuf<unsigned char> mlp_tcw;   // tcgen05 weight chunks
     int mlp_step = 0;
     DevBuf<float> rec_X;
     DevBuf<int32_t> rec_y;
@@ -235,7 +236,7 @@ hk_status hk_destroy(hk_ctx *c) {
     c->mslot.release(); c->mcount.release();
     build_release(c->build);
     c->mlp_params.release(); c->mlp_grads.release(); c->mlp_m.release(); c->mlp_v.release();
-    c->mlp_w1p.release(); c->mlp_w2p.release(); c->mlp_w3p.release(); c->mlp_w4p.release();
+    c->mlp_w1p.release(); c->mlp_w2p.release(); c->mlp_w3p.release(); c->mlp_w4p.release(); c->mlp_tcw.release();
     c->rec_X.release(); c->rec_y.release(); c->rec_rows.release();
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
@@ -1436,6 +1437,7 @@ static hk_status mlp_alloc(hk_ctx *c) {
     HK_CUDA(c, c->mlp_w2p.ensure(packed_words(kMlpHid, kMlpHid)));
     HK_CUDA(c, c->mlp_w3p.ensure(packed_words(kMlpHid, kMlpHid)));
     HK_CUDA(c, c->mlp_w4p.ensure(packed_words(kMlpHid, kMlpOut)));
+    HK_CUDA(c, c->mlp_tcw.ensure(tc_packed_bytes()));
     return HK_OK;
 }
 
@@ -1448,7 +1450,9 @@ static hk_status mlp_pack(hk_ctx *c) {
     HK_CUDA(c, pack_b(P + kOffW2, kMlpHid, kMlpHid, c->mlp_w2p.p, c->stream));
     HK_CUDA(c, pack_b(P + kOffW3, kMlpHid, kMlpHid, c->mlp_w3p.p, c->stream));
     HK_CUDA(c, pack_b(P + kOffW4, kMlpHid, kMlpOut, c->mlp_w4p.p, c->stream));
+    HK_CUDA(c, pack_umma(P, c->mlp_tcw.p, c->stream));
     MlpDevice &M = c->learn.mlp;
+    M.tcw = c->mlp_tcw.p;
     M.w1p = c->mlp_w1p.p;
     M.w2p = c->mlp_w2p.p;
     M.w3p = c->mlp_w3p.p;
@@ -1548,11 +1552,17 @@ hk_status hk_mlp_forward(hk_ctx *c, const float *X, uint32_t n, float *logits) {
     HK_CUDA(c, dx.ensure((size_t)n * kMlpIn));
     HK_CUDA(c, dl.ensure((size_t)n * kMlpOut));
     HK_CUDA(c, cudaMemcpyAsync(dx.p, X, (size_t)n * kMlpIn * 4, cudaMemcpyHostToDevice, c->stream));
-    HK_CUDA(c, mlp_infer(c->learn.mlp, dx.p, nullptr, n, dl.p, c->sm_count, c->stream));
+    HK_CUDA(c, mlp_infer(c->learn.mlp, dx.p, nullptr, n, dl.p, c->sm_count, c->stream, c->errw.p));
     HK_CUDA(c, cudaMemcpyAsync(logits, dl.p, (size_t)n * kMlpOut * 4, cudaMemcpyDeviceToHost, c->stream));
     HK_CUDA(c, cudaStreamSynchronize(c->stream));
     dx.release();
     dl.release();
+    uint32_t w = 0;
+    HK_CUDA(c, cudaMemcpy(&w, c->errw.p, 4, cudaMemcpyDeviceToHost));
+    if (w) {
+        HK_CUDA(c, cudaMemset(c->errw.p, 0, 4));
+        return fail(c, HK_E_DEVICE_TIMEOUT, "tensor-core pipeline wait ran out");
+    }
     return HK_OK;
 }
 

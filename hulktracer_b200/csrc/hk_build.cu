@@ -43,6 +43,7 @@
 #include "hk_build.h"
 #include "hk_common.cuh"
 #include "hk_internal.h"
+#include "hk_mlp_tc.cuh"
 #include "hk_mlp_tile.cuh"
 
 namespace hk {
@@ -143,7 +144,7 @@ __device__ __forceinline__ T block_excl(T v, T *sh_warp, T &total) {
 constexpr uint32_t kSpinLimit = 1u << 22;
 // error bits after which the build's data may be inconsistent: a wait ran
 // out (4), a partition / decision count mismatch (8), a plan bound (16)
-constexpr uint32_t kErrAbort = 4u | 8u | 16u;
+constexpr uint32_t kErrAbort = 4u | 8u | 16u | kErrTensorWait;
 
 // Kernels launched as programmatic dependents (launch_pdl) start before their
 // predecessor in the stream has finished; this waits until it has, with its
@@ -1138,30 +1139,46 @@ __device__ __forceinline__ void list_append(float *list, uint32_t cap, uint32_t 
     n += __popc(m);
 }
 
+// TC: the network on the 5th-generation tensor cores (hk_mlp_tc.cuh, 128-row
+// tiles, TMEM accumulators), else mma.sync (hk_mlp_tile.cuh, 64-row tiles)
+template <bool TC>
 __global__ void __launch_bounds__(256, 1) k_learn(LevelArgs A) {
-    extern __shared__ __align__(16) unsigned char learn_smem[];
+    extern __shared__ __align__(1024) unsigned char learn_smem[];
     __shared__ uint32_t s_tally[5];
     __shared__ uint32_t s_stat[2];
+    constexpr uint32_t kRows = TC ? (uint32_t)kTcRows : (uint32_t)kTileRows;
     wait_prior_grid();
     if (level_aborted(A)) return;
+    const uint32_t rows = min(A.lc->n_learn, A.cap_learn);
+    if (TC && blockIdx.x * kRows >= rows) return;   // no tile: no TMEM taken (the CTA takes part in no barrier)
     Tally tally;
     uint32_t n_learned = 0, n_fallback = 0;
     const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
-    const uint32_t rows = min(A.lc->n_learn, A.cap_learn);
     const TileSmem S = tile_smem(learn_smem);
+    const TcSmem T = tc_smem(learn_smem);
+    uint32_t tmem = 0, g = 0;
+    if (TC) tmem = tc_setup(T);
     const uint32_t K = A.topk < (uint32_t)kLearnMaxK ? (A.topk ? A.topk : 1u) : (uint32_t)kLearnMaxK;
     const uint32_t cap = (kLearnScratch / (3u * K)) & ~7u;
-    float *scratch = reinterpret_cast<float *>(S.stage[0]) + (size_t)wib * kLearnScratch;
-    for (uint32_t row0 = blockIdx.x * kTileRows; row0 < rows; row0 += gridDim.x * kTileRows) {
-        tile_forward(A.mlp, A.feat, row0, rows, S);
-        for (uint32_t rr = wib; rr < (uint32_t)kTileRows && row0 + rr < rows; rr += 8) {
+    // list space: the weight stage buffers (mma.sync) or the activation
+    // operand (tcgen05), both free once the tile's logits exist
+    float *scratch = (TC ? reinterpret_cast<float *>(T.A) : reinterpret_cast<float *>(S.stage[0])) +
+                     (size_t)wib * kLearnScratch;
+    const float *logits = TC ? T.logits : S.logits;
+    for (uint32_t row0 = blockIdx.x * kRows; row0 < rows; row0 += gridDim.x * kRows) {
+        if constexpr (TC) {
+            if (!tc_tile_forward(A.mlp, A.feat, row0, rows, T, tmem, g, A.err)) break;
+        } else {
+            tile_forward(A.mlp, A.feat, row0, rows, S);
+        }
+        for (uint32_t rr = wib; rr < kRows && row0 + rr < rows; rr += 8) {
             const uint32_t row = row0 + rr;
             const uint32_t s = A.learn_slot[row];
             const uint4 info = A.n_info[s];
             const float4 blo = A.n_lo[s], bhi = A.n_hi[s];
             const uint32_t cnt = info.y;
             const LearnBin lb = A.learn_bin[row];
-            const float *Lg = S.logits + rr * kMlpOut;
+            const float *Lg = logits + rr * kMlpOut;
             // 1. top-k valid bins
             float v[3];
 #pragma unroll
@@ -1306,6 +1323,7 @@ __global__ void __launch_bounds__(256, 1) k_learn(LevelArgs A) {
         }
         __syncthreads();   // logits and lists are rewritten by the next tile
     }
+    if (TC) tc_teardown(tmem);
     if (threadIdx.x < 2) s_stat[threadIdx.x] = 0;
     __syncthreads();
     if (n_learned) atomicAdd(&s_stat[0], n_learned);
@@ -1884,7 +1902,9 @@ cudaError_t build_learn_setup() {
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     if (dev >= 64 || !((attr_set >> dev) & 1u)) {
-        e = cudaFuncSetAttribute(k_learn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTileSmem);
+        e = cudaFuncSetAttribute(k_learn<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTileSmem);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(k_learn<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem);
         if (e != cudaSuccess) return e;
         if (dev < 64) attr_set |= 1ull << dev;
     }
@@ -1990,7 +2010,8 @@ cudaError_t build_launch(BuildState &S, const float4 *verts, const uint4 *tris, 
             // proposer rows from the small-node kernel, then the network and
             // the restricted exact search, beside the large nodes' histograms
             launch_pdl(k_small<true, true>, G * 2, 256, 0, st, A);
-            launch_pdl(k_learn, S.sm_count, 256, kTileSmem, st, A);
+            if (mlp_use_tcgen05() && A.mlp.tcw) launch_pdl(k_learn<true>, S.sm_count, 256, kTcSmem, st, A);
+            else launch_pdl(k_learn<false>, S.sm_count, 256, kTileSmem, st, A);
         } else if (A.exact_max >= kWarpExact) {
             launch_pdl(k_small<true, false>, G * 2, 256, 0, st, A);
         } else {
@@ -2019,7 +2040,7 @@ hk_status build_read_stats(BuildState &S, cudaStream_t st, hk_tree_stats *out) {
     S.last_err = err;
     if (err) {
         cudaMemsetAsync(S.err, 0, 4, st);
-        if (err & 4u) return HK_E_DEVICE_TIMEOUT;      // a bounded wait ran out
+        if (err & (4u | kErrTensorWait)) return HK_E_DEVICE_TIMEOUT;   // a bounded wait ran out
         if (err & (8u | 16u)) return HK_E_BOUNDS;       // a partition / plan check fired
         return HK_E_CAPACITY;                           // an arena or list was too small
     }

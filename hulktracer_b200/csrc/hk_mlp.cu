@@ -12,7 +12,11 @@
 #include <cuda_bf16.h>
 #include <algorithm>
 
+#include <cstdlib>
+#include <cstring>
+
 #include "hk_mlp.h"
+#include "hk_mlp_tc.cuh"
 #include "hk_mlp_tile.cuh"
 
 namespace hk {
@@ -188,6 +192,41 @@ cudaError_t pack_b(const float *W, int K, int N, uint32_t *out, cudaStream_t s) 
     return cudaGetLastError();
 }
 
+// the tcgen05 chunk layout (hk_mlp_tc.cuh): element (k, n) of layer l's W
+// (K x N, row-major FP32; K padded with zeros to 256) at chunk kc = k / 64,
+// byte (n / 8) * 1024 + ((k % 64) / 8) * 128 + (n % 8) * 16 + (k % 8) * 2
+__global__ void k_pack_umma(const float *__restrict__ W, int K, int N, unsigned char *__restrict__ out, int layer) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;   // over 256 x N
+    if (i >= kTcAK * N) return;
+    const int k = i / N, n = i % N;
+    const float v = k < K ? W[(size_t)k * N + n] : 0.0f;
+    const int kc = k / kTcChunkK, kk = k % kTcChunkK;
+    const size_t off = tc_chunk_off(layer, kc) + (size_t)(n / 8) * kTcBSbo + (size_t)(kk / 8) * 128 + (n % 8) * 16 +
+                       (kk % 8) * 2;
+    *reinterpret_cast<__nv_bfloat16 *>(out + off) = __float2bfloat16_rn(v);
+}
+
+size_t tc_packed_bytes() { return kTcPackedBytes; }
+
+cudaError_t pack_umma(const float *P, unsigned char *out, cudaStream_t s) {
+    const size_t offs[4] = {kOffW1, kOffW2, kOffW3, kOffW4};
+    const int Ks[4] = {kMlpIn, kMlpHid, kMlpHid, kMlpHid};
+    for (int l = 0; l < 4; l++) {
+        const int N = (int)tc_layer_n(l);
+        k_pack_umma<<<(kTcAK * N + 255) / 256, 256, 0, s>>>(P + offs[l], Ks[l], N, out, l);
+    }
+    return cudaGetLastError();
+}
+
+bool mlp_use_tcgen05() {
+    static int v = -1;
+    if (v < 0) {
+        const char *e = getenv("HK_MLP_PATH");
+        v = (e && strcmp(e, "mma") == 0) ? 0 : 1;
+    }
+    return v == 1;
+}
+
 __device__ __forceinline__ void mma_bf16(float *c, const uint32_t *a, const uint32_t *b) {
     asm volatile(
         "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
@@ -216,6 +255,28 @@ __global__ void __launch_bounds__(256, 1)
     }
 }
 
+// The same on the 5th-generation tensor cores: 128-row tiles (hk_mlp_tc.cuh);
+// a pipeline wait that runs out sets *err and the CTA stops.
+__global__ void __launch_bounds__(256, 1)
+    k_mlp_fwd_tc(MlpDevice M, const float *__restrict__ X, const uint32_t *rows_dev, uint32_t rows_host,
+                 float *__restrict__ logits, uint32_t *err) {
+    extern __shared__ __align__(1024) unsigned char fwd_tc_smem[];
+    const TcSmem S = tc_smem(fwd_tc_smem);
+    const uint32_t rows = rows_dev ? min(*rows_dev, rows_host) : rows_host;
+    if (blockIdx.x * kTcRows >= rows) return;   // no tile for this CTA: no TMEM taken
+    const uint32_t tmem = tc_setup(S);
+    uint32_t g = 0;
+    for (uint32_t row0 = blockIdx.x * kTcRows; row0 < rows; row0 += gridDim.x * kTcRows) {
+        if (!tc_tile_forward(M, X, row0, rows, S, tmem, g, err)) break;
+        for (uint32_t i = threadIdx.x; i < (uint32_t)kTcRows * kMlpOut; i += blockDim.x) {
+            const uint32_t r = row0 + i / kMlpOut;
+            if (r < rows) logits[(size_t)r * kMlpOut + i % kMlpOut] = S.logits[i];
+        }
+        __syncthreads();
+    }
+    tc_teardown(tmem);
+}
+
 cudaError_t mlp_setup() {
     // the shared-memory opt-in is per device; set it once for each
     static uint64_t attr_set = 0;
@@ -224,6 +285,8 @@ cudaError_t mlp_setup() {
     if (e != cudaSuccess) return e;
     if (dev >= 64 || !((attr_set >> dev) & 1u)) {
         e = cudaFuncSetAttribute(k_mlp_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTileSmem);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(k_mlp_fwd_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem);
         if (e != cudaSuccess) return e;
         if (dev < 64) attr_set |= 1ull << dev;
     }
@@ -231,12 +294,18 @@ cudaError_t mlp_setup() {
 }
 
 cudaError_t mlp_infer(const MlpDevice &M, const float *X, const uint32_t *rows_dev, uint32_t rows_host, float *logits,
-                      int grid, cudaStream_t s) {
+                      int grid, cudaStream_t s, uint32_t *err) {
     cudaError_t e = mlp_setup();
     if (e != cudaSuccess) return e;
-    const uint32_t tiles = (rows_host + kTileRows - 1) / kTileRows;
-    const int g = (int)std::max<uint32_t>(1u, std::min<uint32_t>(tiles, (uint32_t)grid));
-    k_mlp_fwd<<<g, 256, kTileSmem, s>>>(M, X, rows_dev, rows_host, logits);
+    if (mlp_use_tcgen05() && M.tcw && err) {
+        const uint32_t tiles = (rows_host + kTcRows - 1) / kTcRows;
+        const int g = (int)std::max<uint32_t>(1u, std::min<uint32_t>(tiles, (uint32_t)grid));
+        k_mlp_fwd_tc<<<g, 256, kTcSmem, s>>>(M, X, rows_dev, rows_host, logits, err);
+    } else {
+        const uint32_t tiles = (rows_host + kTileRows - 1) / kTileRows;
+        const int g = (int)std::max<uint32_t>(1u, std::min<uint32_t>(tiles, (uint32_t)grid));
+        k_mlp_fwd<<<g, 256, kTileSmem, s>>>(M, X, rows_dev, rows_host, logits);
+    }
     return cudaGetLastError();
 }
 

@@ -1,0 +1,304 @@
+// hk_mlp_tc.cuh -- the split proposer's network on the 5th-generation tensor
+// cores (tcgen05), one tile of 128 rows per CTA of 256 threads.
+//
+// 200 -> 256 -> 256 -> 256 -> 96, ReLU between layers, BF16 operands, FP32
+// accumulation in tensor memory (TMEM, 128 lanes = rows x 256 columns).
+//   * Weights: packed once (pack_umma) into the canonical K-major layout of
+//     the UMMA shared-memory descriptor without swizzle, in chunks of 64 K
+//     values: chunk (layer, kc) holds the layer's N output rows x K values
+//     kc*64 .. kc*64+63, 8 x 8 core matrices of 128 bytes,
+//       byte(n, k) = (n / 8) * 1024 + (k / 8) * 128 + (n % 8) * 16 + (k % 8) * 2.
+//     Each chunk (32 KB, 12 KB for the last layer) is one bulk copy
+//     (cp.async.bulk, completion counted on an mbarrier) from global memory
+//     (L2-resident) into one of two shared-memory buffers, the next chunk's
+//     copy in flight while the current chunk is multiplied.
+//   * Activations: the tile's 128 rows x 256 K values in the same canonical
+//     layout (byte(m, k) = (m / 8) * 4096 + (k / 8) * 128 + (m % 8) * 16 +
+//     (k % 8) * 2), rewritten in place by each layer's epilogue.
+//   * One thread issues tcgen05.mma (kind::f16, M = 128, N = 256 or 96, K =
+//     16 per instruction) and tcgen05.commit to an mbarrier; all 8 warps then
+//     read the accumulators with tcgen05.ld (warp w: lanes 32 (w % 4) ..,
+//     columns of half w / 4), add the bias, apply ReLU and store BF16 back as
+//     the next layer's A operand (fence.proxy.async before the next MMA).
+// Every mbarrier wait is bounded; one that runs out sets *err and the tile is
+// abandoned (the caller reports the error) after the copies in flight land.
+#pragma once
+#include <cuda_bf16.h>
+
+#include "hk_mlp.h"
+
+namespace hk {
+
+constexpr int kTcRows = 128;
+constexpr int kTcAK = 256;                                   // K extent of the activation operand
+constexpr uint32_t kTcASbo = kTcAK / 8 * 128;                // 4096: next 8-row group
+constexpr uint32_t kTcABytes = (uint32_t)kTcRows * kTcAK * 2;   // 65536
+constexpr int kTcChunkK = 64;
+constexpr uint32_t kTcBSbo = kTcChunkK / 8 * 128;            // 1024: next 8 output rows
+constexpr uint32_t kTcBBytes = 256u * kTcChunkK * 2;         // 32768, the largest chunk
+constexpr int kTcChunks = 16;                                // 4 layers x 4 chunks of 64 K values
+constexpr uint32_t kTcTmemCols = 256;
+constexpr uint32_t kTcBarOff = kTcABytes + 2 * kTcBBytes;    // 131072: 4 mbarriers + the TMEM address
+constexpr size_t kTcSmem = kTcBarOff + 64;
+constexpr uint32_t kTcSpin = 1u << 20;                       // try_wait attempts before giving up
+constexpr uint32_t kErrTensorWait = 32u;                     // *err bit: a tensor-core pipeline wait ran out
+static_assert((size_t)kTcRows * kMlpOut * 4 <= 2 * kTcBBytes, "logits overlay the weight buffers");
+
+__host__ __device__ constexpr uint32_t tc_layer_n(int l) { return l == 3 ? (uint32_t)kMlpOut : (uint32_t)kMlpHid; }
+__host__ __device__ constexpr uint32_t tc_chunk_bytes(int l) { return tc_layer_n(l) * kTcChunkK * 2; }
+// byte offset of chunk (l, kc) in the packed weights
+__host__ __device__ constexpr size_t tc_chunk_off(int l, int kc) {
+    return (size_t)(l < 3 ? l : 3) * 4 * ((size_t)kMlpHid * kTcChunkK * 2) + (size_t)kc * tc_chunk_bytes(l);
+}
+constexpr size_t kTcPackedBytes = tc_chunk_off(3, 4);       // 3 x 128 KB + 48 KB
+
+// UMMA shared-memory descriptor: canonical K-major, no swizzle (layout type
+// 0), start address / leading byte offset (next core matrix along K) /
+// stride byte offset (next 8 rows) in 16-byte units, version 1 (bit 46)
+__device__ __forceinline__ uint64_t tc_sdesc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+// instruction descriptor, kind::f16: D F32 (bit 4), A and B BF16 (bits 7, 10),
+// both K-major, N >> 3 at bit 17, M >> 4 at bit 24
+__host__ __device__ constexpr uint32_t tc_idesc(uint32_t M, uint32_t N) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((N >> 3) << 17) | ((M >> 4) << 24);
+}
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void tc_mbar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ bool tc_mbar_wait(uint32_t bar, uint32_t parity) {
+    for (uint32_t i = 0; i < kTcSpin; i++) {
+        uint32_t ok;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(ok)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (ok) return true;
+    }
+    return false;
+}
+
+// one bulk copy of `bytes` (a multiple of 16, both addresses 16-byte aligned)
+// from global memory into shared memory, counted on the mbarrier
+__device__ __forceinline__ void tc_bulk_load(uint32_t dst, const void *src, uint32_t bytes, uint32_t bar) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+                 "l"(src), "r"(bytes), "r"(bar)
+                 : "memory");
+}
+
+__device__ __forceinline__ void tc_mma(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+        "l"(da), "l"(db), "r"(idesc), "r"(acc)
+        : "memory");
+}
+
+__device__ __forceinline__ void tc_commit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+
+__device__ __forceinline__ void tc_ld16(uint32_t taddr, uint32_t *r) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+struct TcSmem {
+    unsigned char *A;     // activations (canonical layout)
+    unsigned char *B[2];  // weight chunks
+    float *logits;        // kTcRows x 96, over the weight buffers after the last layer
+    uint32_t bar_load[2], bar_mma[2];
+    uint32_t *tmem_addr;
+};
+
+__device__ __forceinline__ TcSmem tc_smem(unsigned char *base) {
+    TcSmem S;
+    S.A = base;
+    S.B[0] = base + kTcABytes;
+    S.B[1] = base + kTcABytes + kTcBBytes;
+    S.logits = reinterpret_cast<float *>(base + kTcABytes);
+    const uint32_t bars = smem_u32(base + kTcBarOff);
+    S.bar_load[0] = bars;
+    S.bar_load[1] = bars + 8;
+    S.bar_mma[0] = bars + 16;
+    S.bar_mma[1] = bars + 24;
+    S.tmem_addr = reinterpret_cast<uint32_t *>(base + kTcBarOff + 32);
+    return S;
+}
+
+// Kernel prologue (all threads): barriers initialised by thread 0, 256 TMEM
+// columns allocated by warp 0. Pair with tc_teardown.
+__device__ __forceinline__ uint32_t tc_setup(const TcSmem &S) {
+    if (threadIdx.x == 0) {
+        tc_mbar_init(S.bar_load[0], 1);
+        tc_mbar_init(S.bar_load[1], 1);
+        tc_mbar_init(S.bar_mma[0], 1);
+        tc_mbar_init(S.bar_mma[1], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (threadIdx.x < 32) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(S.tmem_addr)),
+                     "r"(kTcTmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    return *S.tmem_addr;
+}
+
+__device__ __forceinline__ void tc_teardown(uint32_t tmem) {
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (threadIdx.x < 32)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTcTmemCols) : "memory");
+}
+
+// byte offset of (row m, column k) in the activation operand
+__device__ __forceinline__ uint32_t tc_a_off(uint32_t m, uint32_t k) {
+    return (m >> 3) * kTcASbo + (k >> 3) * 128u + (m & 7u) * 16u + (k & 7u) * 2u;
+}
+
+// The network on rows row0 .. row0 + 127 of X (rows at or past `rows` are
+// zero); logits in S.logits[r][96] on return. `g` counts the chunks every
+// earlier call of this CTA consumed (mbarrier phases); it advances by
+// kTcChunks. All 256 threads call it. Returns false (on every thread) when a
+// wait ran out; *err then holds kErrTensorWait.
+__device__ __forceinline__ bool tc_tile_forward(const MlpDevice &M, const float *__restrict__ X, uint32_t row0,
+                                                uint32_t rows, const TcSmem &S, uint32_t tmem, uint32_t &g,
+                                                uint32_t *err) {
+    __shared__ uint32_t s_ok;
+    const unsigned char *__restrict__ Wp = M.tcw;
+    const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
+    if (tid == 0) {
+        s_ok = 1;
+        // the buffers were last read by generic loads (the previous tile's logits)
+        tc_fence_async_smem();
+        tc_bulk_load(smem_u32(S.B[g & 1u]), Wp + tc_chunk_off(0, 0), tc_chunk_bytes(0), S.bar_load[g & 1u]);
+    }
+    // the tile's features as BF16 in the canonical layout, K 200 .. 255 zero
+    for (uint32_t i = tid; i < (uint32_t)kTcRows * (kTcAK / 8); i += blockDim.x) {
+        const uint32_t m = i / (kTcAK / 8), k0 = (i % (kTcAK / 8)) * 8;
+        const uint32_t r = row0 + m;
+        uint32_t w[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const uint32_t k = k0 + 2 * j;
+            const float a = (r < rows && k < (uint32_t)kMlpIn) ? X[(size_t)r * kMlpIn + k] : 0.0f;
+            const float b = (r < rows && k + 1 < (uint32_t)kMlpIn) ? X[(size_t)r * kMlpIn + k + 1] : 0.0f;
+            const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+            w[j] = *reinterpret_cast<const uint32_t *>(&h);
+        }
+        *reinterpret_cast<uint4 *>(S.A + tc_a_off(m, k0)) = make_uint4(w[0], w[1], w[2], w[3]);
+    }
+    tc_fence_async_smem();
+    tc_fence_before();
+    __syncthreads();
+    const uint32_t abase = smem_u32(S.A);
+    for (int l = 0; l < 4; l++) {
+        const uint32_t N = tc_layer_n(l);
+        const uint32_t idesc = tc_idesc(kTcRows, N);
+        if (tid == 0 && s_ok) {
+            tc_fence_after();
+            for (int kc = 0; kc < 4 && s_ok; kc++) {
+                const uint32_t q = (uint32_t)(l * 4 + kc), gq = g + q, b = gq & 1u;
+                // the next chunk into the other buffer, once the MMAs that read it are done
+                if (q + 1 < (uint32_t)kTcChunks) {
+                    if (q >= 1 && !tc_mbar_wait(S.bar_mma[b ^ 1u], ((gq - 1) >> 1) & 1u)) s_ok = 0;
+                    const int l1 = (int)(q + 1) / 4, kc1 = (int)(q + 1) % 4;
+                    if (s_ok)
+                        tc_bulk_load(smem_u32(S.B[b ^ 1u]), Wp + tc_chunk_off(l1, kc1), tc_chunk_bytes(l1),
+                                     S.bar_load[b ^ 1u]);
+                }
+                if (!s_ok || !tc_mbar_wait(S.bar_load[b], (gq >> 1) & 1u)) {
+                    s_ok = 0;
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t bbase = smem_u32(S.B[b]);
+                // layer 0 has K = 200: its last chunk has one step of real data (192 .. 207)
+                const int steps = (l == 0 && kc == 3) ? 1 : 4;
+                for (int s = 0; s < steps; s++) {
+                    const uint64_t da = tc_sdesc(abase + (uint32_t)(kc * 8 + s * 2) * 128u, 128u, kTcASbo);
+                    const uint64_t db = tc_sdesc(bbase + (uint32_t)s * 256u, 128u, kTcBSbo);
+                    tc_mma(tmem, da, db, idesc, (kc > 0 || s > 0) ? 1u : 0u);
+                }
+                tc_commit(S.bar_mma[b]);
+            }
+        }
+        __syncthreads();
+        // every thread waits for the layer's last chunk (its commit covers all
+        // MMAs issued before it)
+        const uint32_t glast = g + (uint32_t)(l * 4 + 3);
+        bool ok = s_ok != 0;
+        if (ok && !tc_mbar_wait(S.bar_mma[glast & 1u], (glast >> 1) & 1u)) ok = false;
+        if (!ok) s_ok = 0;
+        __syncthreads();
+        if (!s_ok) break;
+        tc_fence_after();
+        // epilogue: warp w reads lanes 32 (w % 4) .. + 31 (rows), columns of half w / 4
+        const uint32_t m = 32u * (warp & 3u) + lane;
+        const uint32_t half = N / 2, c0 = (warp >> 2) * half;
+        const float *bl = l == 0 ? M.b1 : (l == 1 ? M.b2 : (l == 2 ? M.b3 : M.b4));
+        for (uint32_t c = c0; c < c0 + half; c += 16) {
+            uint32_t r[16];
+            tc_ld16(tmem + ((32u * (warp & 3u)) << 16) + c, r);
+            if (l < 3) {
+                uint32_t w[8];
+#pragma unroll
+                for (int j = 0; j < 8; j++) {
+                    const float a = fmaxf(__uint_as_float(r[2 * j]) + bl[c + 2 * j], 0.0f);
+                    const float b = fmaxf(__uint_as_float(r[2 * j + 1]) + bl[c + 2 * j + 1], 0.0f);
+                    const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+                    w[j] = *reinterpret_cast<const uint32_t *>(&h);
+                }
+                *reinterpret_cast<uint4 *>(S.A + tc_a_off(m, c)) = make_uint4(w[0], w[1], w[2], w[3]);
+                *reinterpret_cast<uint4 *>(S.A + tc_a_off(m, c + 8)) = make_uint4(w[4], w[5], w[6], w[7]);
+            } else {
+#pragma unroll
+                for (int j = 0; j < 16; j++) S.logits[m * kMlpOut + c + j] = __uint_as_float(r[j]) + bl[c + j];
+            }
+        }
+        tc_fence_async_smem();
+        tc_fence_before();
+        __syncthreads();
+    }
+    g += kTcChunks;
+    if (!s_ok) {
+        // let every copy this tile started land before the CTA moves on
+        if (tid == 0) {
+            atomicOr(err, kErrTensorWait);
+            for (uint32_t k = 0; k < 2; k++) {
+                // the last load into each buffer was chunk kTcChunks - 2 + k (or earlier on a break)
+                const uint32_t gq = g - 2 + k;
+                tc_mbar_wait(S.bar_load[gq & 1u], (gq >> 1) & 1u);
+            }
+        }
+        __syncthreads();
+        return false;
+    }
+    return true;
+}
+
+}  // namespace hk

@@ -52,6 +52,42 @@ def test_forward_bf16_matches_oracle(ctx):
     assert (Z.argmax(1) == Zf.argmax(1)).mean() >= 0.9
 
 
+def test_forward_many_tiles_per_cta(ctx):
+    """40,000 rows: more 128-row tiles than SMs, so each CTA of the tcgen05
+    kernel runs several tiles through its mbarrier phases and TMEM."""
+    ctx.mlp_init(9)
+    p = ctx.mlp_params()
+    X = features_like(40000, 5)
+    Z = ctx.mlp_forward(X)
+    Zb = mlp.forward_bf16(p, X)
+    scale = float(np.abs(Zb).max())
+    err = np.abs(Z - Zb)
+    assert err.max() <= 1e-2 * scale and err.mean() <= 1e-3 * scale
+
+
+def test_forward_paths_agree():
+    """The mma.sync network (HK_MLP_PATH=mma, in a child process) and the
+    tcgen05 one give the same logits within BF16 rounding of the hidden
+    activations."""
+    import subprocess
+    import sys
+    import tempfile
+    code = ("import sys, numpy as np; sys.path.insert(0, %r); import hulktracer_b200 as hk; "
+            "c = hk.Context(); c.mlp_init(21); X = np.load(sys.argv[1]); np.save(sys.argv[2], c.mlp_forward(X))"
+            % os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    X = features_like(1000, 6)
+    with tempfile.TemporaryDirectory() as d:
+        np.save(os.path.join(d, "x.npy"), X)
+        out = {}
+        for path in ("mma", "tcgen05"):
+            env = dict(os.environ, HK_MLP_PATH=path)
+            subprocess.check_call([sys.executable, "-c", code, os.path.join(d, "x.npy"), os.path.join(d, path + ".npy")],
+                                  env=env, timeout=300)
+            out[path] = np.load(os.path.join(d, path + ".npy"))
+    scale = float(np.abs(out["mma"]).max())
+    assert np.abs(out["mma"] - out["tcgen05"]).max() <= 1e-2 * scale
+
+
 def test_grad_matches_oracle(ctx):
     ctx.mlp_init(11)
     p = ctx.mlp_params()
