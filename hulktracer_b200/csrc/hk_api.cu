@@ -43,6 +43,8 @@ struct DevBuf {
 
 }  // namespace
 
+static void batch_detach(hk_batch *b);
+
 struct hk_ctx {
     hk_config cfg;
     int device = 0;
@@ -119,6 +121,7 @@ struct hk_ctx {
     uint32_t rec_cap = 0;
     bool recording = false;
     bool prop_log = false;
+    std::vector<hk_batch *> batches;     // live batches (detached when the context goes first)
     uint32_t debug_flags = 0;
 };
 
@@ -223,6 +226,10 @@ hk_status hk_destroy(hk_ctx *c) {
     if (!c) return HK_E_ILLEGAL_INPUT;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
+    // batches still alive lose their device memory and their context; a
+    // later hk_batch_destroy only frees the host side
+    for (hk_batch *b : c->batches) batch_detach(b);
+    c->batches.clear();
     if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
     if (c->graph) cudaGraphDestroy(c->graph);
     c->verts.release(); c->rest.release(); c->tris.release(); c->part.release(); c->mats.release();
@@ -1193,19 +1200,39 @@ hk_status hk_batch_create(hk_ctx *c, hk_batch **out) {
     if (!c || !out) return HK_E_ILLEGAL_INPUT;
     hk_batch *b = new hk_batch();
     b->ctx = c;
+    c->batches.push_back(b);
     *out = b;
     return HK_OK;
 }
 
-hk_status hk_batch_destroy(hk_batch *b) {
-    if (!b) return HK_E_ILLEGAL_INPUT;
-    cudaSetDevice(b->ctx->device);
-    cudaStreamSynchronize(b->ctx->stream);
+}  // extern "C"
+
+// frees the batch's device memory (its context's device current, its stream
+// idle) and cuts it from the context
+static void batch_detach(hk_batch *b) {
     for (auto *s : b->scenes) {
         s->rec.release(); s->nodes.release(); s->refs.release(); s->ropes.release(); s->cbox.release();
         delete s;
     }
+    b->scenes.clear();
     b->table.release(); b->offsets.release(); b->remaining.release(); b->times.release();
+    b->ctx = nullptr;
+}
+
+extern "C" {
+
+hk_status hk_batch_destroy(hk_batch *b) {
+    if (!b) return HK_E_ILLEGAL_INPUT;
+    if (hk_ctx *c = b->ctx) {
+        cudaSetDevice(c->device);
+        cudaStreamSynchronize(c->stream);
+        for (size_t i = 0; i < c->batches.size(); i++)
+            if (c->batches[i] == b) {
+                c->batches.erase(c->batches.begin() + (long)i);
+                break;
+            }
+        batch_detach(b);
+    }
     delete b;
     return HK_OK;
 }
@@ -1213,6 +1240,7 @@ hk_status hk_batch_destroy(hk_batch *b) {
 hk_status hk_batch_add_scene(hk_batch *b, const float *verts4, uint32_t nv, const uint32_t *tris4, uint32_t nt,
                              uint32_t *scene_id) {
     if (!b || nt == 0) return HK_E_ILLEGAL_INPUT;
+    if (!b->ctx) return HK_E_STATE;   // its context was destroyed
     hk_ctx *c = b->ctx;
     hk_status st = hk_scene_upload(c, verts4, nv, tris4, nt);
     if (st != HK_OK) return st;
@@ -1246,6 +1274,7 @@ hk_status hk_batch_add_scene(hk_batch *b, const float *verts4, uint32_t nv, cons
 hk_status hk_batch_trace_device(hk_batch *b, const float *d_rays8, const uint32_t *ray_offsets, uint32_t nscenes,
                                 hk_variant v, hk_hit *d_hits, float *scene_ms) {
     if (!b || !ray_offsets || !d_rays8 || !d_hits) return HK_E_ILLEGAL_INPUT;
+    if (!b->ctx) return HK_E_STATE;   // its context was destroyed
     hk_ctx *c = b->ctx;
     if (nscenes == 0 || nscenes != b->scenes.size()) return fail(c, HK_E_ILLEGAL_INPUT, "nscenes != scenes in batch");
     if ((int)v < HK_TRACE_FULLSTACK || (int)v > HK_TRACE_BRUTE) return fail(c, HK_E_ILLEGAL_INPUT, "variant");

@@ -454,6 +454,7 @@ struct LevelArgs {
     int learned, record;
     uint32_t *learn_slot;   // proposer row -> node slot
     LearnBin *learn_bin;    // proposer row -> binned decision
+    uint2 *learn_prop;      // proposer row -> proposed bins, one byte each (0xff: none)
     float *feat;            // proposer row -> features
     int32_t *prop_log;      // optional: compact node -> its 8 proposed bins
     uint32_t cap_learn;
@@ -1102,31 +1103,18 @@ __global__ void __launch_bounds__(256, 5) k_small(LevelArgs A) {
     tally_flush(A, tally, s_tally);
 }
 
-// ---------------------------------------------------------------------------
-// learned split search (no reference counterpart). For a tile of 64 proposer
-// rows the network (tile_forward) gives 96 logits per row, one per (axis,
-// bin); warp w then takes rows w, w + 8, ... and per row
-//   1. the top-k bins by logit (ties to the lower index; an axis of zero
-//      extent has no valid bin);
-//   2. one pass over the node's references: per proposal (axis a, bin b, the
-//      closed interval [P0, P1] = [p_b, p_{b+1}] with p_0 the node's minimum
-//      and p_32 its maximum) the references whose clipped lower bound lies
-//      below P0 and those whose clipped upper bound lies above P1 are
-//      counted, and the lower bounds, upper bounds and flat references inside
-//      [P0, P1] are listed in shared memory;
-//   3. every listed bound p strictly inside the node is a candidate -- the
-//      exact SAH's candidates that fall in the bin -- with
-//        below = #(lo < P0) + #(listed lo < p) + #(listed flat at p),
-//        above = #(hi > P1) + #(listed hi > p) + #(listed flat at p),
-//      the exact SAH's own counts; the cheapest by (cost, axis, plane) wins;
-//   4. that plane is taken unless it costs more than fallback_ratio x the
-//      binned optimum that k_small found for the node (then the binned
-//      plane); the usual leaf test follows.
-// A proposal whose lists overflow their share of shared memory is not costed.
-// ---------------------------------------------------------------------------
 constexpr int kLearnMaxK = 8;
-constexpr uint32_t kLearnScratch = 2048;   // floats of list space per warp (8 warps: the two stage buffers)
-static_assert(8 * kLearnScratch * 4 <= 2 * kStageWords * 4, "list space overlays the weight stage buffers");
+constexpr uint32_t kLearnScratch = 2048;   // floats of list space per warp
+constexpr uint32_t kRefineWarps = 8;
+constexpr size_t kRefineSmem = (size_t)kRefineWarps * kLearnScratch * 4;   // 64 KB
+
+// list capacity per (proposal, list): the largest power of two with 3 k of
+// them in one warp's space (128 for k = 4), so a list sorts in place
+__host__ __device__ constexpr uint32_t learn_list_cap(uint32_t K) {
+    uint32_t c = 1;
+    while (2 * c * 3 * K <= kLearnScratch) c *= 2;
+    return c;
+}
 
 // warp-aggregated append of val (where pred) to list[n ..); n counts past cap
 __device__ __forceinline__ void list_append(float *list, uint32_t cap, uint32_t &n, bool pred, float val) {
@@ -1139,31 +1127,54 @@ __device__ __forceinline__ void list_append(float *list, uint32_t cap, uint32_t 
     n += __popc(m);
 }
 
-// TC: the network on the 5th-generation tensor cores (hk_mlp_tc.cuh, 128-row
-// tiles, TMEM accumulators), else mma.sync (hk_mlp_tile.cuh, 64-row tiles)
+// ascending bitonic sort of v[0, n) in shared memory by one warp; the list's
+// capacity is a power of two >= n, the padding up to the next power of two
+// is filled with +inf
+__device__ __forceinline__ void warp_sort_smem(float *v, uint32_t n) {
+    const uint32_t lane = threadIdx.x & 31u;
+    uint32_t n2 = 1;
+    while (n2 < n) n2 <<= 1;
+    for (uint32_t i = n + lane; i < n2; i += 32) v[i] = kInf;
+    __syncwarp();
+    for (uint32_t k = 2; k <= n2; k <<= 1)
+        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+            for (uint32_t i = lane; i < n2; i += 32) {
+                const uint32_t ixj = i ^ j;
+                if (ixj > i) {
+                    const bool up = (i & k) == 0;
+                    const float x = v[i], y = v[ixj];
+                    if ((x > y) == up) {
+                        v[i] = y;
+                        v[ixj] = x;
+                    }
+                }
+            }
+            __syncwarp();
+        }
+}
+
+// ---------------------------------------------------------------------------
+// learned split search (no reference counterpart), two launches per level.
+// k_learn: the network on the level's proposer rows (tcgen05: 128-row tiles,
+// hk_mlp_tc.cuh; else mma.sync: 64-row tiles, hk_mlp_tile.cuh), then per row
+// the top-k valid bins by logit (ties to the lower index; an axis of zero
+// extent has no valid bin), one byte each (axis * 32 + bin, 0xff: none) in
+// learn_prop.
+// ---------------------------------------------------------------------------
 template <bool TC>
 __global__ void __launch_bounds__(256, 1) k_learn(LevelArgs A) {
     extern __shared__ __align__(1024) unsigned char learn_smem[];
-    __shared__ uint32_t s_tally[5];
-    __shared__ uint32_t s_stat[2];
     constexpr uint32_t kRows = TC ? (uint32_t)kTcRows : (uint32_t)kTileRows;
     wait_prior_grid();
     if (level_aborted(A)) return;
     const uint32_t rows = min(A.lc->n_learn, A.cap_learn);
-    if (TC && blockIdx.x * kRows >= rows) return;   // no tile: no TMEM taken (the CTA takes part in no barrier)
-    Tally tally;
-    uint32_t n_learned = 0, n_fallback = 0;
+    if (blockIdx.x * kRows >= rows) return;   // no tile: no TMEM taken (the CTA takes part in no barrier)
     const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
     const TileSmem S = tile_smem(learn_smem);
     const TcSmem T = tc_smem(learn_smem);
     uint32_t tmem = 0, g = 0;
     if (TC) tmem = tc_setup(T);
     const uint32_t K = A.topk < (uint32_t)kLearnMaxK ? (A.topk ? A.topk : 1u) : (uint32_t)kLearnMaxK;
-    const uint32_t cap = (kLearnScratch / (3u * K)) & ~7u;
-    // list space: the weight stage buffers (mma.sync) or the activation
-    // operand (tcgen05), both free once the tile's logits exist
-    float *scratch = (TC ? reinterpret_cast<float *>(T.A) : reinterpret_cast<float *>(S.stage[0])) +
-                     (size_t)wib * kLearnScratch;
     const float *logits = TC ? T.logits : S.logits;
     for (uint32_t row0 = blockIdx.x * kRows; row0 < rows; row0 += gridDim.x * kRows) {
         if constexpr (TC) {
@@ -1174,24 +1185,16 @@ __global__ void __launch_bounds__(256, 1) k_learn(LevelArgs A) {
         for (uint32_t rr = wib; rr < kRows && row0 + rr < rows; rr += 8) {
             const uint32_t row = row0 + rr;
             const uint32_t s = A.learn_slot[row];
-            const uint4 info = A.n_info[s];
             const float4 blo = A.n_lo[s], bhi = A.n_hi[s];
-            const uint32_t cnt = info.y;
-            const LearnBin lb = A.learn_bin[row];
             const float *Lg = logits + rr * kMlpOut;
-            // 1. top-k valid bins
             float v[3];
 #pragma unroll
             for (int j = 0; j < 3; j++) {
                 const float x = Lg[32 * j + lane];
                 v[j] = __fsub_rn(c3(bhi, j), c3(blo, j)) > 0.0f ? (x == x ? x : -INFINITY) : NAN;
             }
-            uint32_t pax[kLearnMaxK];
-            float p0[kLearnMaxK], p1[kLearnMaxK];
-            uint32_t np = 0;
-#pragma unroll
-            for (int r = 0; r < kLearnMaxK; r++) {
-                if ((uint32_t)r >= K) break;
+            uint32_t packed[2] = {0xffffffffu, 0xffffffffu};
+            for (uint32_t r = 0; r < K; r++) {
                 float bv = NAN;
                 int bc = 1 << 30;
 #pragma unroll
@@ -1212,118 +1215,179 @@ __global__ void __launch_bounds__(256, 1) k_learn(LevelArgs A) {
 #pragma unroll
                 for (int j = 0; j < 3; j++)
                     if (bc == (int)lane + 32 * j) v[j] = NAN;
-                const uint32_t a = (uint32_t)bc >> 5, b = (uint32_t)bc & 31u;
-                const float l = c3(blo, a), h = c3(bhi, a), ext = __fsub_rn(h, l);
-                pax[r] = a;
-                p0[r] = b == 0 ? l : plane_k(l, ext, b);
-                p1[r] = b == kBins - 1 ? h : plane_k(l, ext, b + 1);
-                if (A.prop_log && lane == 0 && info.z < A.cap_nodes) A.prop_log[(size_t)info.z * 8 + r] = bc;
-                np++;
+                const uint32_t sh = 8u * (r & 3u);
+                packed[r >> 2] = (packed[r >> 2] & ~(0xffu << sh)) | ((uint32_t)bc << sh);
             }
-            // 2. counts and lists over the node's references
-            uint32_t bl[kLearnMaxK], ab[kLearnMaxK], nL[kLearnMaxK], nH[kLearnMaxK], nF[kLearnMaxK];
-#pragma unroll
-            for (int i = 0; i < kLearnMaxK; i++) bl[i] = ab[i] = nL[i] = nH[i] = nF[i] = 0;
-            for (uint32_t base = 0; base < cnt; base += 32) {
-                const bool have = base + lane < cnt;
-                float4 tlo = make_float4(0, 0, 0, 0), thi = tlo;
-                if (have) {
-                    const uint32_t tri = A.refs[info.x + base + lane];
-                    tlo = A.tb_lo[tri];
-                    thi = A.tb_hi[tri];
-                }
-#pragma unroll
-                for (int i = 0; i < kLearnMaxK; i++) {
-                    if ((uint32_t)i >= np) break;
-                    const uint32_t a = pax[i];
-                    const float l = c3(blo, a), h = c3(bhi, a);
-                    const float lo = mxf(c3(tlo, a), l), hi = mnf(c3(thi, a), h);
-                    bl[i] += (have && lo < p0[i]) ? 1u : 0u;
-                    ab[i] += (have && hi > p1[i]) ? 1u : 0u;
-                    const bool inL = have && p0[i] <= lo && lo <= p1[i];
-                    const bool inH = have && p0[i] <= hi && hi <= p1[i];
-                    float *Ls = scratch + (size_t)i * 3 * cap;
-                    list_append(Ls, cap, nL[i], inL, lo);
-                    list_append(Ls + cap, cap, nH[i], inH, hi);
-                    list_append(Ls + 2 * cap, cap, nF[i], inL && lo == hi, lo);
-                }
+            if (lane == 0) {
+                A.learn_prop[row] = make_uint2(packed[0], packed[1]);
+                const uint32_t cidx = A.n_info[s].z;
+                if (A.prop_log && cidx < A.cap_nodes)
+                    for (uint32_t r = 0; r < 8; r++) {
+                        const uint32_t b = (packed[r >> 2] >> (8u * (r & 3u))) & 0xffu;
+                        A.prop_log[(size_t)cidx * 8 + r] = b == 0xffu ? -1 : (int32_t)b;
+                    }
             }
-            __syncwarp();
-            // 3. exact costs of the listed candidates
-            const float Anode = surf(blo, bhi);
-            float mc = kInf, m_pk = 0.0f;
-            uint32_t m_ax = 3, m_nb = 0, m_na = 0;
+        }
+        __syncthreads();   // the logits are rewritten by the next tile
+    }
+    if (TC) tc_teardown(tmem);
+}
+
+// ---------------------------------------------------------------------------
+// k_refine: one warp per proposer row over the whole GPU.
+//   1. one pass over the node's references: per proposed bin (axis a, bin b,
+//      the closed interval [P0, P1] = [p_b, p_{b+1}] with p_0 the node's
+//      minimum and p_32 its maximum) the references whose clipped lower bound
+//      lies below P0 and those whose clipped upper bound lies above P1 are
+//      counted, and the lower bounds, upper bounds and flat references inside
+//      [P0, P1] are listed in shared memory (then sorted);
+//   2. every listed bound p strictly inside the node is a candidate -- the
+//      exact SAH's candidates that fall in the bin -- with
+//        below = #(lo < P0) + #(listed lo < p) + #(listed flat at p),
+//        above = #(hi > P1) + #(listed hi > p) + #(listed flat at p)
+//      (binary searches in the sorted lists), the exact SAH's own counts; the
+//      cheapest by (cost, axis, plane) wins;
+//   3. that plane is taken unless it costs more than fallback_ratio x the
+//      binned optimum k_small found for the node (then the binned plane); the
+//      usual leaf test follows.
+// A bin whose lists overflow their capacity (learn_list_cap) is not costed.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_refine(LevelArgs A) {
+    extern __shared__ __align__(16) float refine_smem[];
+    __shared__ uint32_t s_tally[5];
+    __shared__ uint32_t s_stat[2];
+    wait_prior_grid();
+    if (level_aborted(A)) return;
+    Tally tally;
+    uint32_t n_learned = 0, n_fallback = 0;
+    const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
+    const uint32_t rows = min(A.lc->n_learn, A.cap_learn);
+    const uint32_t K = A.topk < (uint32_t)kLearnMaxK ? (A.topk ? A.topk : 1u) : (uint32_t)kLearnMaxK;
+    const uint32_t cap = learn_list_cap(K);
+    float *scratch = refine_smem + (size_t)wib * kLearnScratch;
+    for (uint32_t row = blockIdx.x * kRefineWarps + wib; row < rows; row += gridDim.x * kRefineWarps) {
+        const uint32_t s = A.learn_slot[row];
+        const uint4 info = A.n_info[s];
+        const float4 blo = A.n_lo[s], bhi = A.n_hi[s];
+        const uint32_t cnt = info.y;
+        const LearnBin lb = A.learn_bin[row];
+        const uint2 pp = A.learn_prop[row];
+        uint32_t pax[kLearnMaxK];
+        float p0[kLearnMaxK], p1[kLearnMaxK];
+        uint32_t np = 0;
+#pragma unroll
+        for (int r = 0; r < kLearnMaxK; r++) {
+            const uint32_t b8 = ((r < 4 ? pp.x : pp.y) >> (8 * (r & 3))) & 0xffu;
+            if (b8 == 0xffu || (uint32_t)r >= K) break;
+            const uint32_t a = b8 >> 5, b = b8 & 31u;
+            const float l = c3(blo, a), h = c3(bhi, a), ext = __fsub_rn(h, l);
+            pax[r] = a;
+            p0[r] = b == 0 ? l : plane_k(l, ext, b);
+            p1[r] = b == kBins - 1 ? h : plane_k(l, ext, b + 1);
+            np++;
+        }
+        // 1. counts and lists over the node's references
+        uint32_t bl[kLearnMaxK], ab[kLearnMaxK], nL[kLearnMaxK], nH[kLearnMaxK], nF[kLearnMaxK];
+#pragma unroll
+        for (int i = 0; i < kLearnMaxK; i++) bl[i] = ab[i] = nL[i] = nH[i] = nF[i] = 0;
+        for (uint32_t base = 0; base < cnt; base += 32) {
+            const bool have = base + lane < cnt;
+            float4 tlo = make_float4(0, 0, 0, 0), thi = tlo;
+            if (have) {
+                const uint32_t tri = A.refs[info.x + base + lane];
+                tlo = A.tb_lo[tri];
+                thi = A.tb_hi[tri];
+            }
 #pragma unroll
             for (int i = 0; i < kLearnMaxK; i++) {
                 if ((uint32_t)i >= np) break;
-                uint32_t b0 = bl[i], a0 = ab[i];
-                for (int o = 16; o; o >>= 1) {
-                    b0 += __shfl_xor_sync(0xffffffffu, b0, o);
-                    a0 += __shfl_xor_sync(0xffffffffu, a0, o);
-                }
-                if (nL[i] > cap || nH[i] > cap || nF[i] > cap) continue;   // overflowed: not costed
                 const uint32_t a = pax[i];
                 const float l = c3(blo, a), h = c3(bhi, a);
-                const float *Ls = scratch + (size_t)i * 3 * cap, *Hs = Ls + cap, *Fs = Ls + 2 * cap;
-                const uint32_t nl = nL[i], nh = nH[i], nf = nF[i];
-                for (uint32_t q = lane; q < nl + nh; q += 32) {
-                    const float x = q < nl ? Ls[q] : Hs[q - nl];
-                    if (!(x > l && x < h)) continue;
-                    const float pk = __fadd_rn(x, 0.0f);
-                    uint32_t below = b0, above = a0, fon = 0;
-                    for (uint32_t k = 0; k < nl; k++) below += Ls[k] < pk ? 1u : 0u;
-                    for (uint32_t k = 0; k < nh; k++) above += Hs[k] > pk ? 1u : 0u;
-                    for (uint32_t k = 0; k < nf; k++) fon += Fs[k] == pk ? 1u : 0u;
-                    const uint32_t nb = below + fon, na = above + fon;
-                    float4 bb = bhi, ba = blo;
-                    s3(bb, a, pk);
-                    s3(ba, a, pk);
-                    const float sb = surf(blo, bb), sa = surf(ba, bhi);
-                    const float cost = __fadd_rn(
-                        A.ct, __fmul_rn(A.ci, __fdiv_rn(__fadd_rn(__fmul_rn(sb, (float)nb), __fmul_rn(sa, (float)na)),
-                                                        Anode)));
-                    if (cost < mc || (cost == mc && (a < m_ax || (a == m_ax && pk < m_pk)))) {
-                        mc = cost;
-                        m_ax = a;
-                        m_pk = pk;
-                        m_nb = nb;
-                        m_na = na;
-                    }
-                }
+                const float lo = mxf(c3(tlo, a), l), hi = mnf(c3(thi, a), h);
+                bl[i] += (have && lo < p0[i]) ? 1u : 0u;
+                ab[i] += (have && hi > p1[i]) ? 1u : 0u;
+                const bool inL = have && p0[i] <= lo && lo <= p1[i];
+                const bool inH = have && p0[i] <= hi && hi <= p1[i];
+                float *Ls = scratch + (size_t)i * 3 * cap;
+                list_append(Ls, cap, nL[i], inL, lo);
+                list_append(Ls + cap, cap, nH[i], inH, hi);
+                list_append(Ls + 2 * cap, cap, nF[i], inL && lo == hi, lo);
             }
-            float bc = mc, bp = m_pk;
-            uint32_t bax = m_ax, blane = lane;
-            for (int off = 16; off; off >>= 1) {
-                const float oc = __shfl_xor_sync(0xffffffffu, bc, off), op = __shfl_xor_sync(0xffffffffu, bp, off);
-                const uint32_t oax = __shfl_xor_sync(0xffffffffu, bax, off), ol = __shfl_xor_sync(0xffffffffu, blane, off);
-                if (oc < bc || (oc == bc && (oax < bax || (oax == bax && (op < bp || (op == bp && ol < blane)))))) {
-                    bc = oc;
-                    bp = op;
-                    bax = oax;
-                    blane = ol;
-                }
-            }
-            const uint32_t nb = __shfl_sync(0xffffffffu, m_nb, blane), na = __shfl_sync(0xffffffffu, m_na, blane);
-            // 4. the proposal's plane, or the binned optimum
-            const bool take = bc < kInf && bc <= __fmul_rn(A.fallback_ratio, lb.cost);
-            Decision d;
-            if (take) {
-                d = Decision{(int)bax, bp, nb, na, bc, 0};
-                if (!(bc < __fmul_rn(A.ci, (float)cnt))) d.axis = -1;
-            } else {
-                d = Decision{lb.axis, lb.plane, lb.nb, lb.na, lb.cost, 0};
-            }
-            if (lane == 0) {
-                write_decision(A, s, d, blo, bhi);
-                tally.add(d, cnt);
-                if (take) n_learned++;
-                else n_fallback++;
-            }
-            __syncwarp();
         }
-        __syncthreads();   // logits and lists are rewritten by the next tile
+        __syncwarp();
+        // 2. exact costs of the listed candidates
+        const float Anode = surf(blo, bhi);
+        float mc = kInf, m_pk = 0.0f;
+        uint32_t m_ax = 3, m_nb = 0, m_na = 0;
+#pragma unroll
+        for (int i = 0; i < kLearnMaxK; i++) {
+            if ((uint32_t)i >= np) break;
+            uint32_t b0 = bl[i], a0 = ab[i];
+            for (int o = 16; o; o >>= 1) {
+                b0 += __shfl_xor_sync(0xffffffffu, b0, o);
+                a0 += __shfl_xor_sync(0xffffffffu, a0, o);
+            }
+            if (nL[i] > cap || nH[i] > cap || nF[i] > cap) continue;   // overflowed: not costed
+            const uint32_t a = pax[i];
+            const float l = c3(blo, a), h = c3(bhi, a);
+            float *Ls = scratch + (size_t)i * 3 * cap, *Hs = Ls + cap, *Fs = Ls + 2 * cap;
+            const uint32_t nl = nL[i], nh = nH[i], nf = nF[i];
+            warp_sort_smem(Ls, nl);
+            warp_sort_smem(Hs, nh);
+            if (nf) warp_sort_smem(Fs, nf);
+            for (uint32_t q = lane; q < nl + nh; q += 32) {
+                const float x = q < nl ? Ls[q] : Hs[q - nl];
+                if (!(x > l && x < h)) continue;
+                const float pk = __fadd_rn(x, 0.0f);
+                const uint32_t fon = nf ? upper_bound_f(Fs, nf, pk) - lower_bound_f(Fs, nf, pk) : 0u;
+                const uint32_t nb = b0 + lower_bound_f(Ls, nl, pk) + fon;
+                const uint32_t na = a0 + (nh - upper_bound_f(Hs, nh, pk)) + fon;
+                float4 bb = bhi, ba = blo;
+                s3(bb, a, pk);
+                s3(ba, a, pk);
+                const float sb = surf(blo, bb), sa = surf(ba, bhi);
+                const float cost = __fadd_rn(
+                    A.ct,
+                    __fmul_rn(A.ci, __fdiv_rn(__fadd_rn(__fmul_rn(sb, (float)nb), __fmul_rn(sa, (float)na)), Anode)));
+                if (cost < mc || (cost == mc && (a < m_ax || (a == m_ax && pk < m_pk)))) {
+                    mc = cost;
+                    m_ax = a;
+                    m_pk = pk;
+                    m_nb = nb;
+                    m_na = na;
+                }
+            }
+        }
+        float bc = mc, bp = m_pk;
+        uint32_t bax = m_ax, blane = lane;
+        for (int off = 16; off; off >>= 1) {
+            const float oc = __shfl_xor_sync(0xffffffffu, bc, off), op = __shfl_xor_sync(0xffffffffu, bp, off);
+            const uint32_t oax = __shfl_xor_sync(0xffffffffu, bax, off), ol = __shfl_xor_sync(0xffffffffu, blane, off);
+            if (oc < bc || (oc == bc && (oax < bax || (oax == bax && (op < bp || (op == bp && ol < blane)))))) {
+                bc = oc;
+                bp = op;
+                bax = oax;
+                blane = ol;
+            }
+        }
+        const uint32_t nb = __shfl_sync(0xffffffffu, m_nb, blane), na = __shfl_sync(0xffffffffu, m_na, blane);
+        // 3. the proposal's plane, or the binned optimum
+        const bool take = bc < kInf && bc <= __fmul_rn(A.fallback_ratio, lb.cost);
+        Decision d;
+        if (take) {
+            d = Decision{(int)bax, bp, nb, na, bc, 0};
+            if (!(bc < __fmul_rn(A.ci, (float)cnt))) d.axis = -1;
+        } else {
+            d = Decision{lb.axis, lb.plane, lb.nb, lb.na, lb.cost, 0};
+        }
+        if (lane == 0) {
+            write_decision(A, s, d, blo, bhi);
+            tally.add(d, cnt);
+            if (take) n_learned++;
+            else n_fallback++;
+        }
+        __syncwarp();
     }
-    if (TC) tc_teardown(tmem);
     if (threadIdx.x < 2) s_stat[threadIdx.x] = 0;
     __syncthreads();
     if (n_learned) atomicAdd(&s_stat[0], n_learned);
@@ -1792,7 +1856,7 @@ void build_release(BuildState &S) {
         f(S.n_lo[k]); f(S.n_hi[k]); f(S.n_info[k]); f(S.refs[k]); f(S.ref_node[k]);
     }
     f(S.d_axis); f(S.d_plane); f(S.d_cnt); f(S.d_split); f(S.d_scat);
-    f(S.chunks); f(S.hist); f(S.done); f(S.medium_slot); f(S.learn_slot); f(S.learn_bin); f(S.feat); f(S.prop_log);
+    f(S.chunks); f(S.hist); f(S.done); f(S.medium_slot); f(S.learn_slot); f(S.learn_bin); f(S.learn_prop); f(S.feat); f(S.prop_log);
     f(S.plan_flags); f(S.ref_flags); f(S.plan_done); f(S.plan_agg); f(S.plan_incl); f(S.ref_agg); f(S.ref_incl); f(S.epoch);
     f(S.ctr); f(S.err);
     f(S.out_nodes); f(S.out_refs); f(S.out_ropes); f(S.out_cbox);
@@ -1850,6 +1914,7 @@ hk_status build_prepare(BuildState &S, const BuildParams &p, uint32_t nt, int sm
     bad |= dalloc(S.medium_slot, S.cap_medium) != cudaSuccess;
     bad |= dalloc(S.learn_slot, S.cap_learn) != cudaSuccess;
     bad |= dalloc(S.learn_bin, S.cap_learn) != cudaSuccess;
+    bad |= dalloc(S.learn_prop, S.cap_learn) != cudaSuccess;
     bad |= dalloc(S.feat, (size_t)S.cap_learn * kMlpIn) != cudaSuccess;
     if (p.prop_log) bad |= dalloc(S.prop_log, (size_t)cap_nodes * 8) != cudaSuccess;
     bad |= dalloc(S.plan_flags, S.plan_tiles) != cudaSuccess;
@@ -1905,6 +1970,8 @@ cudaError_t build_learn_setup() {
         e = cudaFuncSetAttribute(k_learn<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTileSmem);
         if (e == cudaSuccess)
             e = cudaFuncSetAttribute(k_learn<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(k_refine, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kRefineSmem);
         if (e != cudaSuccess) return e;
         if (dev < 64) attr_set |= 1ull << dev;
     }
@@ -1952,6 +2019,7 @@ cudaError_t build_launch(BuildState &S, const float4 *verts, const uint4 *tris, 
     A.record = (S.p.mode == HK_BUILD_BINNED && S.p.record && S.learn && S.learn->rec_X) ? 1 : 0;
     A.learn_slot = S.learn_slot;
     A.learn_bin = S.learn_bin;
+    A.learn_prop = S.learn_prop;
     A.feat = S.feat;
     A.cap_learn = S.cap_learn;
     A.prop_log = (A.learned && S.p.prop_log) ? S.prop_log : nullptr;
@@ -2012,6 +2080,7 @@ cudaError_t build_launch(BuildState &S, const float4 *verts, const uint4 *tris, 
             launch_pdl(k_small<true, true>, G * 2, 256, 0, st, A);
             if (mlp_use_tcgen05() && A.mlp.tcw) launch_pdl(k_learn<true>, S.sm_count, 256, kTcSmem, st, A);
             else launch_pdl(k_learn<false>, S.sm_count, 256, kTileSmem, st, A);
+            launch_pdl(k_refine, S.sm_count * 3, 256, kRefineSmem, st, A);
         } else if (A.exact_max >= kWarpExact) {
             launch_pdl(k_small<true, false>, G * 2, 256, 0, st, A);
         } else {

@@ -129,6 +129,7 @@ struct BuildState {
     uint32_t cap_learn = 0;
     uint32_t *learn_slot = nullptr;              // row -> node slot
     LearnBin *learn_bin = nullptr;               // row -> the binned SAH's decision
+    uint2 *learn_prop = nullptr;                 // row -> proposed bins (bytes, 0xff: none)
     float *feat = nullptr;                       // [cap_learn][200]
     int32_t *prop_log = nullptr;                 // [cap_nodes][8] proposed bins (axis * 32 + bin, -1: none)
     LearnBuffers *learn = nullptr;               // context-owned (weights, recording)

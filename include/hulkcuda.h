@@ -378,6 +378,9 @@ hk_status hk_autotune(hk_ctx *ctx, const float *d_rays8, uint32_t n, const char 
  * finished (device %globaltimer). */
 typedef struct hk_batch hk_batch;
 hk_status hk_batch_create(hk_ctx *ctx, hk_batch **batch);
+/* A batch may outlive its context: hk_destroy frees the device memory of the
+ * context's batches, later calls on them return HK_E_STATE, and
+ * hk_batch_destroy then frees only the host side. */
 hk_status hk_batch_destroy(hk_batch *batch);
 /* upload + triangle records + GPU build (the context's settings), then keep a
  * copy; uses the context's scene slot as working space */

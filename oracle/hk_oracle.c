@@ -1251,8 +1251,8 @@ static int search_ropes(const hko_tree *t, const float *o, const float *d, float
 /* each proposed bin (axis a, bin b, closed interval [P0, P1] = [p_b,        */
 /* p_{b+1}], p_0 = node min, p_32 = node max), the exact search over the      */
 /* clipped bounds inside the interval (a bin whose in-interval lower bounds,  */
-/* upper bounds or flat refs exceed the list capacity (2048 / (3 topk))      */
-/* rounded down to a multiple of 8 is skipped); the best of those by          */
+/* upper bounds or flat refs exceed the list capacity (the largest power of  */
+/* two c with 3 topk c <= 2048) is skipped); the best of those by          */
 /* (cost, axis, plane) replaces the binned plane unless it costs more than    */
 /* fallback_ratio x the binned optimum.                                       */
 /* ------------------------------------------------------------------------ */
@@ -1397,7 +1397,8 @@ int hko_build_binned(const float *verts, const uint32_t *tris, uint32_t nt, cons
             if (p->learned && n->count > 32 && n->count <= 1024 && p->proposals) {
                 const int32_t *prop = p->proposals + 8 * (size_t)n->cidx;
                 uint32_t K = p->topk < 8 ? (p->topk ? p->topk : 1) : 8;
-                uint32_t cap = (2048u / (3u * K)) & ~7u;
+                uint32_t cap = 1;
+                while (2u * cap * 3u * K <= 2048u) cap *= 2u;
                 float rbest = INFINITY, rpk = 0.0f;
                 int32_t rax = 3;
                 uint32_t rnb = 0, rna = 0;

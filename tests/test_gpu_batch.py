@@ -38,3 +38,27 @@ def test_batch_equals_per_scene(hk, variant):
         assert np.array_equal(h["t"], e["t"])
     assert ms.shape == (5,) and np.all(ms > 0)
     batch.close()
+
+
+def test_batch_outliving_its_context(hk):
+    """hk_destroy with a batch still alive frees the batch's device memory;
+    later batch calls return HK_E_STATE, hk_batch_destroy frees the rest, and
+    the process's CUDA state stays sound for the next context."""
+    import ctypes as C
+    from hulktracer_b200 import scenes
+    sc = scenes.cluster_soup(5000, seed=3)
+    ctx = hk.Context()
+    batch = hk.engine.Batch(ctx)
+    batch.add_scene(sc.verts, sc.tris)
+    ctx.close()
+    L = hk._lib.load()
+    sid = C.c_uint32()
+    assert L.hk_batch_add_scene(batch.h, hk._lib.ptr(np.ascontiguousarray(sc.verts, np.float32)), sc.verts.shape[0],
+                                hk._lib.ptr(np.ascontiguousarray(sc.tris, np.uint32)), sc.tris.shape[0],
+                                C.byref(sid)) == 20
+    batch.close()
+    c2 = hk.Context()
+    c2.upload(sc.verts, sc.tris)
+    c2.precompute()
+    assert c2.build()["nodes"] > 0
+    c2.close()

@@ -219,6 +219,7 @@ def test_batch_incoherent_rays_equal_oracle(hk, oracle):
                                     with_ropes=(ov == O_ROPES))
             oh, oid = oracle.trace(tree, rays[i], ov, 6)
             hits_equal(h[offsets[i]:offsets[i + 1]], oid, oh[:, 0])
+    batch.close()
     ctx.close()
 
 
