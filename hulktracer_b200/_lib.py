@@ -56,6 +56,22 @@ class TreeStats(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class AffInfo(C.Structure):
+    _fields_ = [("nv", C.c_uint32), ("nt", C.c_uint32), ("nmeshes", C.c_uint32), ("ndynamic", C.c_uint32),
+                ("ntransforms", C.c_uint32), ("nanimations", C.c_uint32), ("nlights", C.c_uint32),
+                ("has_view", C.c_int32), ("from_", C.c_float * 3), ("at", C.c_float * 3), ("up", C.c_float * 3),
+                ("fov_deg", C.c_float), ("hither", C.c_float), ("resx", C.c_int32), ("resy", C.c_int32),
+                ("has_anim_params", C.c_int32), ("anim_start", C.c_float), ("anim_end", C.c_float),
+                ("anim_frames", C.c_int32), ("has_camera_anim", C.c_int32)]
+
+    def as_dict(self):
+        out = {}
+        for k, _ in self._fields_:
+            v = getattr(self, k)
+            out[k.rstrip("_")] = list(v) if hasattr(v, "__len__") else v
+        return out
+
+
 NOALLOC_SCRATCH_BYTES = 24 << 20
 MLP_IN, MLP_HID, MLP_OUT = 200, 256, 96
 MLP_PARAMS = 200 * 256 + 256 + 2 * (256 * 256 + 256) + 256 * 96 + 96
@@ -133,6 +149,15 @@ def load(path: str = LIB_PATH):
         "hk_batch_destroy": [vp],
         "hk_batch_add_scene": [vp, f32p, u32, u32p, u32, C.POINTER(C.c_uint32)],
         "hk_batch_trace_device": [vp, vp, u32p, u32, C.c_int, vp, f32p],
+        "hk_aff_open": [C.c_char_p, C.POINTER(C.c_void_p)],
+        "hk_aff_close": [vp],
+        "hk_aff_get_info": [vp, C.POINTER(AffInfo)],
+        "hk_aff_geometry": [vp, f32p, u32p, u32p],
+        "hk_aff_part_matrices": [vp, C.c_float, f32p],
+        "hk_aff_lights": [vp, f32p],
+        "hk_aff_camera": [vp, C.c_float, f32p],
+        "hk_scene_load_aff": [vp, vp, C.c_float],
+        "hk_scene_animate_aff": [vp, vp, C.c_float],
     }
     for name, args in sig.items():
         fn = getattr(L, name)
@@ -140,6 +165,8 @@ def load(path: str = LIB_PATH):
         fn.restype = C.c_int
     L.hk_last_error.argtypes = [vp]
     L.hk_last_error.restype = C.c_char_p
+    L.hk_aff_last_error.argtypes = []
+    L.hk_aff_last_error.restype = C.c_char_p
     _lib = L
     return L
 

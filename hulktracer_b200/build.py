@@ -21,7 +21,10 @@ LIB = os.path.join(PKG, "libhulkcuda.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 # -fmad=false: the traversal, shading and build arithmetic must round after
 # every operation in source order to reproduce the reference bit for bit.
+# -Xcompiler -ffp-contract=off does the same for host code (the AFF splines and
+# matrices reproduce the reference's x86 arithmetic).
 NVFLAGS = ["-O3", "-lineinfo", "-std=c++17", "-fmad=false", "-Xcompiler", "-fPIC",
+           "-Xcompiler", "-ffp-contract=off",
            "-Xptxas", "-warn-spills", "-I" + os.path.join(ROOT, "include")]
 # files whose arithmetic has no parity constraint may contract (none: the
 # network's tile code is shared by the builder and hk_mlp_forward, which must

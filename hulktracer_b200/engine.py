@@ -47,6 +47,73 @@ def obj_parse(path: str):
     return v, t
 
 
+def fixed_tick_time(frame: int) -> float:
+    """Scene time of frame `frame` under the reference's --fixedTic=1 clock
+    (GLWindow::display, HulkEngine/src/GLWindow.cpp:115-123): tick / 10 as a
+    float, with ticks 59 and 421 skipped."""
+    tick = 0
+    for _ in range(frame):
+        tick += 1
+        if tick in (59, 421):
+            tick += 1
+    return float(np.float32(tick) / np.float32(10))
+
+
+class Aff:
+    """An AFF (BART) scene parsed by the library (hk_aff_*): rest-pose meshes,
+    transforms and keyframe animations. Host-side; no GPU needed."""
+
+    def __init__(self, path: str):
+        self.L = _lib.load()
+        self.h = C.c_void_p()
+        st = self.L.hk_aff_open(path.encode(), C.byref(self.h))
+        if st != 0:
+            raise HkError(st, "hk_aff_open(%s): %s" % (path, self.L.hk_aff_last_error().decode()))
+        info = _lib.AffInfo()
+        self._check(self.L.hk_aff_get_info(self.h, C.byref(info)))
+        self.info = info.as_dict()
+
+    def _check(self, st):
+        if st != 0:
+            raise HkError(st, self.L.hk_aff_last_error().decode())
+
+    def close(self):
+        if self.h:
+            self.L.hk_aff_close(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def geometry(self):
+        """(verts float32[V, 4], tris uint32[T, 4], part uint32[V])"""
+        i = self.info
+        v = np.zeros((i["nv"], 4), np.float32)
+        t = np.zeros((i["nt"], 4), np.uint32)
+        p = np.zeros(i["nv"], np.uint32)
+        self._check(self.L.hk_aff_geometry(self.h, ptr(v), ptr(t), ptr(p)))
+        return v, t, p
+
+    def part_matrices(self, time: float):
+        m = np.zeros((self.info["nmeshes"], 12), np.float32)
+        self._check(self.L.hk_aff_part_matrices(self.h, float(time), ptr(m)))
+        return m
+
+    def lights(self):
+        out = np.zeros((self.info["nlights"], 8), np.float32)
+        if out.size:
+            self._check(self.L.hk_aff_lights(self.h, ptr(out)))
+        return out
+
+    def camera(self, time: float):
+        cam = np.zeros(16, np.float32)
+        self._check(self.L.hk_aff_camera(self.h, float(time), ptr(cam)))
+        return cam
+
+
 class Context:
     def __init__(self, device: int = 0, **cfg):
         self.L = _lib.load()
@@ -93,6 +160,14 @@ class Context:
         nv, nt = C.c_uint32(), C.c_uint32()
         self._check(self.L.hk_scene_load_obj(self.h, path.encode(), C.byref(nv), C.byref(nt)))
         self.nverts, self.ntris = nv.value, nt.value
+
+    def load_aff(self, aff: "Aff", time: float = 0.0):
+        """Upload an AFF scene (one part per mesh) transformed to `time`."""
+        self._check(self.L.hk_scene_load_aff(self.h, aff.h, float(time)))
+        self.nverts, self.ntris = aff.info["nv"], aff.info["nt"]
+
+    def animate_aff(self, aff: "Aff", time: float):
+        self._check(self.L.hk_scene_animate_aff(self.h, aff.h, float(time)))
 
     def set_box(self, box):
         self._check(self.L.hk_scene_set_box(self.h, ptr(_f32(box))))

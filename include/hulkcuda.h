@@ -278,6 +278,67 @@ hk_status hk_obj_parse(const char *path, float *verts4, uint32_t cap_verts, uint
                        uint32_t *nv, uint32_t *nt);
 hk_status hk_scene_load_obj(hk_ctx *ctx, const char *path, uint32_t *nv, uint32_t *nt);
 
+/* ---- AFF (BART animated scene) ingest ----
+ * The reference's AFFParser (BartLoader/src/AFFParser.cpp; the interface is
+ * LoaderInterface, HulkEngine/public/LoaderInterface.hpp:18-27, and
+ * BartLoader/public/AFFParser.hpp:37-84) with its keyframe animation
+ * (BartLoader/src/animation.cpp, kbsplpos.cpp, kbsplrot.cpp, quat.cpp) and
+ * per-frame transform (AFFTransformVisitor::preAct, BartLoader/src/
+ * AFFTransformVisitor.cpp:25-88). Host-side calls, no GPU needed except for
+ * hk_scene_load_aff / hk_scene_animate_aff.
+ *
+ * Geometry comes from the triangle meshes ("m"), concatenated in file order
+ * (includes "i" expanded in place, relative to the top file's directory, and
+ * skipped above the "d" detail level, which starts at 0 on every open). Each
+ * mesh is one part; its matrix is the product of the enclosing static ("xs":
+ * T*R*S) and keyframed ("x" + "k": Kochanek-Bartels splines for translation
+ * and scale, squad for rotation, clamped outside the keys) transforms. Lights
+ * ("l", "la") keep the reference's Light layout; the viewpoint ("v") gives the
+ * field of view and resolution; the "camera" animation places the camera
+ * (GLVisitorCPUTrace::updateCamera, HulkEngine/src/GLVisitorCPUTrace.cpp:
+ * 105-146). Materials, spheres, cones, polygons and textured triangles are
+ * parsed and dropped, as by the reference. Results are bit-identical to the
+ * reference's Scene::m_vertices at the same time. A syntax error returns
+ * HK_E_ILLEGAL_INPUT, a missing file HK_E_FILE_OPEN; hk_aff_last_error (per
+ * thread) names the cause. */
+typedef struct hk_aff hk_aff;
+typedef struct hk_aff_info {
+    uint32_t nv, nt;          /* vertices and triangles of all meshes */
+    uint32_t nmeshes;         /* parts: one per mesh */
+    uint32_t ndynamic;        /* meshes under at least one keyframed transform */
+    uint32_t ntransforms;     /* "xs" and "x" blocks */
+    uint32_t nanimations;     /* "k" blocks */
+    uint32_t nlights;
+    int32_t has_view;         /* a "v" block was read (else the reference's defaults) */
+    float from[3], at[3], up[3];
+    float fov_deg, hither;    /* fov 45 without "v" */
+    int32_t resx, resy;       /* 800 x 600 without "v" */
+    int32_t has_anim_params;  /* an "a start end frames" line was read */
+    float anim_start, anim_end;
+    int32_t anim_frames;
+    int32_t has_camera_anim;  /* a "k camera" block exists */
+} hk_aff_info;
+
+hk_status hk_aff_open(const char *path, hk_aff **out);
+hk_status hk_aff_close(hk_aff *aff);
+const char *hk_aff_last_error(void);
+hk_status hk_aff_get_info(const hk_aff *aff, hk_aff_info *info);
+/* Rest-pose vertices (float4, w = 1), triangles (uint4, global vertex indices)
+ * and the mesh index of every vertex; each array may be null. Sizes from
+ * hk_aff_get_info: nv x 4 floats, nt x 4 uints, nv uints. */
+hk_status hk_aff_geometry(const hk_aff *aff, float *verts4, uint32_t *tris4, uint32_t *part_of_vertex);
+/* nmeshes x 3x4 row-major matrices at `time` (the reference's Scene::m_time),
+ * in the layout of hk_scene_transform. */
+hk_status hk_aff_part_matrices(const hk_aff *aff, float time, float *mats12);
+/* nlights x float[8] (Light layout: color.xyz, 1 = point light, position.xyzw). */
+hk_status hk_aff_lights(const hk_aff *aff, float *lights8);
+/* CameraPos (float[16], the hk_camera_rays layout) at `time`. */
+hk_status hk_aff_camera(const hk_aff *aff, float time, float *cam16);
+/* Upload the rest pose, one part per mesh, and transform it to `time`. */
+hk_status hk_scene_load_aff(hk_ctx *ctx, const hk_aff *aff, float time);
+/* Re-transform the loaded AFF scene to `time` (hk_scene_transform). */
+hk_status hk_scene_animate_aff(hk_ctx *ctx, const hk_aff *aff, float time);
+
 /* ---- tree interchange file ----
  * The reference's dataset dump (GLVisitorGPUTrace::saveDataSetToFile,
  * HulkEngine/src/GLVisitorGPUTrace.cpp:638-674, read back by

@@ -1,5 +1,5 @@
 #!/usr/bin/env python3
-"""Compile the reference HulkEngine CPU KD-tree path into ``oracle/_ref``.
+"""Compile the reference HulkEngine CPU KD-tree path and BART loader into ``oracle/_ref``.
 
 Test infrastructure only: the product never links or loads what this builds.
 
@@ -19,6 +19,12 @@ and a few MSVC-only constructs are patched in *generated copies* that live in
 * ``HulkEngine/src/KDTreeCPU.cpp``: instrumented copy that records the winning
   polygon index in ``testNodePolygons`` (the reference has no hit ID) and counts
   node visits / triangle tests in ``searchKDTreeStackless``.
+
+The BART loader (``BartLoader/src``: AFFParser, AFFTransformVisitor and the
+keyframe code) is compiled into both libraries unchanged except for two
+process-wide statics that the driver re-arms per scene: the detail level
+(``AFFParser.cpp:23``) and the first-traversal flag of the transform visitor
+(``AFFTransformVisitor.cpp:134-140``).
 
 Two libraries are produced:
 
@@ -159,6 +165,29 @@ def _patch_cfg_sah(src):
     return t
 
 
+BART_SOURCES = ["animation.cpp", "kbsplpos.cpp", "kbsplrot.cpp", "quat.cpp"]
+
+
+def _patch_aff_parser(src):
+    # gDetailLevel is a file static that outlives one load; the driver loads
+    # many scenes in one process, so every top-level parse starts at level 0
+    # as a fresh process does (AFFParser.cpp:23,1462-1467)
+    t = _read(src)
+    return _replace(t, "\tm_relPath = relPath;\n", "\tgDetailLevel = 0;\n\tm_relPath = relPath;\n",
+                    what="AFFParser detail level")
+
+
+def _patch_aff_visitor(src):
+    # traverseBegin transforms static meshes on the first traversal of the
+    # process only (a function static, AFFTransformVisitor.cpp:134-140); the
+    # driver re-arms it for every new visitor it creates
+    t = _read(src)
+    t = "extern int hkref_aff_rearm;\n" + t
+    return _replace(t, "\tstatic int count = 0;\n",
+                    "\tstatic int count = 0;\n\tif (hkref_aff_rearm) { count = 0; hkref_aff_rearm = 0; }\n",
+                    what="AFFTransformVisitor static count")
+
+
 def _make_gen(ref, gen, cfg):
     if os.path.isdir(gen):
         shutil.rmtree(gen)
@@ -195,6 +224,9 @@ def _make_gen(ref, gen, cfg):
     }
     if cfg:
         srcs["KDTreeSAH.cpp"] = _patch_cfg_sah(os.path.join(he, "src", "KDTreeSAH.cpp"))
+    bart = os.path.join(ref, "BartLoader", "src")
+    srcs["AFFParser.cpp"] = _patch_aff_parser(os.path.join(bart, "AFFParser.cpp"))
+    srcs["AFFTransformVisitor.cpp"] = _patch_aff_visitor(os.path.join(bart, "AFFTransformVisitor.cpp"))
     for name, text in srcs.items():
         _write(os.path.join(gen, name), text)
     return srcs
@@ -207,10 +239,13 @@ def build(ref, cfg):
     os.makedirs(objdir, exist_ok=True)
     gen_srcs = _make_gen(ref, gen, cfg)
     he = os.path.join(ref, "HulkEngine")
-    incs = ["-I" + gen, "-I" + os.path.join(he, "public"), "-I" + os.path.join(he, "src")]
+    bl = os.path.join(ref, "BartLoader")
+    incs = ["-I" + gen, "-I" + os.path.join(he, "public"), "-I" + os.path.join(he, "src"),
+            "-I" + os.path.join(bl, "public"), "-I" + os.path.join(bl, "src")]
     pre = ["-include", os.path.join(gen, "windows.h")]
     units = [os.path.join(gen, n) for n in gen_srcs]
     units += [os.path.join(he, s) for s in SOURCES if os.path.basename(s) not in gen_srcs]
+    units += [os.path.join(bl, "src", s) for s in BART_SOURCES]
     units.append(os.path.join(HERE, "ref_driver.cpp"))
     objs = []
     for u in units:

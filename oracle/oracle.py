@@ -360,3 +360,68 @@ class Reference:
                 self.lib.hkref_destroy(self.h)
         except Exception:
             pass
+
+
+class ReferenceAff:
+    """An AFF scene loaded by the reference's own AFFParser and animated by its
+    AFFTransformVisitor (compiled from BartLoader/src into oracle/_ref)."""
+
+    def __init__(self, path: str):
+        lib_path = os.path.join(HERE, "_ref", "libhulkref.so")
+        if not os.path.exists(lib_path):
+            raise FileNotFoundError(lib_path)
+        L = self.lib = C.CDLL(lib_path)
+        L.hkref_aff_open.restype = C.c_void_p
+        L.hkref_aff_open.argtypes = [C.c_char_p]
+        L.hkref_aff_close.argtypes = [C.c_void_p]
+        L.hkref_aff_counts.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.hkref_aff_view.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.hkref_aff_tris.argtypes = [C.c_void_p, _u32p]
+        L.hkref_aff_lights.argtypes = [C.c_void_p, _f32p]
+        L.hkref_aff_frame.argtypes = [C.c_void_p, C.c_float, _f32p, _f32p]
+        L.hkref_aff_camera.argtypes = [C.c_void_p, C.c_float, _f32p]
+        if not os.path.exists(path):
+            raise FileNotFoundError(path)
+        self.h = L.hkref_aff_open(path.encode())
+        if not self.h:
+            raise FileNotFoundError(path)
+        nv, nt, nl = C.c_uint(), C.c_uint(), C.c_uint()
+        L.hkref_aff_counts(self.h, C.byref(nv), C.byref(nt), C.byref(nl))
+        self.nv, self.nt, self.nl = nv.value, nt.value, nl.value
+        fov, res, asp = C.c_float(), (C.c_int * 2)(), C.c_float()
+        L.hkref_aff_view(self.h, C.byref(fov), res, C.byref(asp))
+        self.fov, self.res, self.aspect = fov.value, (res[0], res[1]), asp.value
+
+    def tris(self):
+        t = np.zeros((self.nt, 4), np.uint32)
+        self.lib.hkref_aff_tris(self.h, t)
+        return t
+
+    def lights(self):
+        out = np.zeros((self.nl, 8), np.float32)
+        if self.nl:
+            self.lib.hkref_aff_lights(self.h, out)
+        return out
+
+    def frame(self, time: float):
+        """Scene::m_vertices and the scene box after the frame at `time`."""
+        v = np.zeros((self.nv, 4), np.float32)
+        box = np.zeros(8, np.float32)
+        self.lib.hkref_aff_frame(self.h, float(time), v, box)
+        return v, box
+
+    def camera(self, time: float):
+        cam = np.zeros(16, np.float32)
+        self.lib.hkref_aff_camera(self.h, float(time), cam)
+        return cam
+
+    def close(self):
+        if self.h:
+            self.lib.hkref_aff_close(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

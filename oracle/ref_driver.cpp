@@ -1,7 +1,8 @@
 // C entry points over the compiled reference HulkEngine CPU path.
 //
 // Test infrastructure only (built by oracle/build_ref.py into oracle/_ref).
-// It fills a reference Scene directly (no loader), runs the reference's own
+// It fills a reference Scene directly (or through the reference's own AFF
+// loader, at the end of this file), runs the reference's own
 // KDTreeCPU::buildKDTree / checkCollision, and restates the per-pixel shading
 // loop of GLVisitorCPUTrace::traceScene (HulkEngine/src/GLVisitorCPUTrace.cpp:
 // 149-200) on top of the reference's checkCollision and
@@ -13,10 +14,14 @@
 #include "Scene.hpp"
 #include "Settings.hpp"
 #include "SharedFunctions.hpp"
+#include "AFFParser.hpp"
+#include "BoundingBoxVisitor.hpp"
+#include "util.hpp"
 
 thread_local unsigned hkref_last_poly = 0;
 thread_local unsigned long long hkref_nodes = 0;
 thread_local unsigned long long hkref_tests = 0;
+int hkref_aff_rearm = 0;
 
 namespace {
 struct RefCtx {
@@ -227,6 +232,120 @@ float hkref_box_volume(const float *box) {
     b.m_min = SPVector(box[0], box[1], box[2], box[3]);
     b.m_max = SPVector(box[4], box[5], box[6], box[7]);
     return getBoxVolume(b);
+}
+
+// ---- AFF (BART) scenes through the reference's own loader ----
+// AFFParser::viParseFile (BartLoader/src/AFFParser.cpp:1462-1539) fills a
+// Scene; AFFTransformVisitor (BartLoader/src/AFFTransformVisitor.cpp) and
+// BoundingBoxVisitor run per frame as GLWindow::display does
+// (HulkEngine/src/GLWindow.cpp:111-133).
+struct RefAff {
+    Scene scene;
+    AFFParser parser;
+    Visitor *xf = nullptr;
+    RefAff() : scene("hkaff") {}
+    ~RefAff() {
+        if (xf) parser.freeTransformVisitor(xf);
+    }
+};
+
+void *hkref_aff_open(const char *path) {
+    FILE *f = fopen(path, "r");
+    if (!f) return nullptr;
+    std::string p(path);
+    RefAff *a = new RefAff();
+    a->parser.viParseFile(f, p.substr(0, p.rfind('/') + 1), a->scene);
+    fclose(f);
+    a->xf = a->parser.getTransformVisitor(a->scene);
+    hkref_aff_rearm = 1;
+    return a;
+}
+
+void hkref_aff_close(void *h) { delete (RefAff *)h; }
+
+// vertices, triangles, lights; fov, resolution, aspect
+void hkref_aff_counts(void *h, unsigned *nv, unsigned *nt, unsigned *nl) {
+    RefAff *a = (RefAff *)h;
+    *nv = a->scene.m_vertices.size();
+    *nt = a->scene.m_vertexIndices.size();
+    *nl = a->scene.m_lights.size();
+}
+
+void hkref_aff_view(void *h, float *fov, int *res, float *aspect) {
+    RefAff *a = (RefAff *)h;
+    *fov = a->scene.m_fov;
+    res[0] = a->scene.m_resx;
+    res[1] = a->scene.m_resy;
+    *aspect = a->scene.m_aspect;
+}
+
+void hkref_aff_tris(void *h, unsigned *tris4) {
+    RefAff *a = (RefAff *)h;
+    for (unsigned i = 0; i < a->scene.m_vertexIndices.size(); i++)
+        for (int k = 0; k < 3; k++) tris4[4 * i + k] = a->scene.m_vertexIndices[i].indices[k];
+    for (unsigned i = 0; i < a->scene.m_vertexIndices.size(); i++) tris4[4 * i + 3] = 0;
+}
+
+void hkref_aff_lights(void *h, float *l8) {
+    RefAff *a = (RefAff *)h;
+    for (unsigned i = 0; i < a->scene.m_lights.size(); i++) {
+        Light &L = a->scene.m_lights[i];
+        SPVector pos(L.data.pos);
+        for (int k = 0; k < 4; k++) {
+            l8[8 * i + k] = L.color.vector[k];
+            l8[8 * i + 4 + k] = pos.vector[k];
+        }
+    }
+}
+
+// one frame at `time`: transformed vertices (float4) and the scene box
+void hkref_aff_frame(void *h, float time, float *verts4, float *box8) {
+    RefAff *a = (RefAff *)h;
+    a->scene.setTime(time);
+    a->xf->traverse(a->scene.m_pRoot);
+    BoundingBoxVisitor bb(a->scene);
+    bb.traverse(a->scene.m_pRoot);
+    for (unsigned i = 0; i < a->scene.m_vertices.size(); i++)
+        for (int k = 0; k < 4; k++) verts4[4 * i + k] = a->scene.m_vertices[i].vector[k];
+    for (int k = 0; k < 4; k++) {
+        box8[k] = a->scene.m_sceneBox.m_min.vector[k];
+        box8[4 + k] = a->scene.m_sceneBox.m_max.vector[k];
+    }
+}
+
+// GLVisitorCPUTrace::updateCamera (HulkEngine/src/GLVisitorCPUTrace.cpp:
+// 105-146), which needs GL headers to compile, restated over the reference's
+// SPVector / SPMatrix and its loader's getTransformation.
+void hkref_aff_camera(void *h, float time, float *cam16) {
+    RefAff *a = (RefAff *)h;
+    a->scene.setTime(time);
+    SPMatrix rotMat, transMat;
+    double trans[3] = {0}, rot[4] = {0};
+    a->parser.getTransformation(a->scene, "camera", rot, trans);
+    transMat.TranslateMatrix((float)trans[0], (float)trans[1], (float)trans[2]);
+    rotMat.rotateMatrix((float)rot[0], (float)rot[1], (float)rot[2], -(float)rot[3]);
+    SPVector from(0, 0, 0), down(0, -1, 0), left(-1, 0, 0), to(0, 0, -1);
+    SPVector f = from * transMat;
+    down = down * rotMat;
+    left = left * rotMat;
+    to = to * rotMat;
+    down.w = 0;
+    left.w = 0;
+    to.w = 0;
+    f.w = 0;
+    float verticalFactor = tan(DEG_TO_RAD(a->scene.m_fov) / 2);
+    float horizontalFactor = verticalFactor * a->scene.m_aspect;
+    down = down * verticalFactor;
+    left = left * horizontalFactor;
+    SPVector lowerLeft = f + to + down + left;
+    SPVector vert = left * -2.0;
+    SPVector horiz = down * -2.0;
+    for (int k = 0; k < 4; k++) {
+        cam16[k] = f.vector[k];
+        cam16[4 + k] = vert.vector[k];
+        cam16[8 + k] = horiz.vector[k];
+        cam16[12 + k] = lowerLeft.vector[k];
+    }
 }
 
 }  // extern "C"
