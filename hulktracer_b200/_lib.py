@@ -21,7 +21,7 @@ STATUS_NAMES = {0: "HK_OK", 1: "HK_E_ALLOC", 2: "HK_E_FILE_OPEN", 3: "HK_E_FILE_
 FULLSTACK, SHORTSTACK, SMEMSTACK, RESTART, RESTART_EARLY, ROPES, BRUTE = range(7)
 VARIANTS = {"fullstack": FULLSTACK, "shortstack": SHORTSTACK, "smemstack": SMEMSTACK,
             "restart": RESTART, "restart_early": RESTART_EARLY, "ropes": ROPES, "brute": BRUTE}
-BUILD_BINNED, BUILD_LEARNED = 0, 1
+BUILD_BINNED, BUILD_LEARNED, BUILD_SAH_RESORT = 0, 1, 2
 SHADE_CPU, SHADE_PICTURE, SHADE_MIRROR = 0, 1, 2
 
 
@@ -36,7 +36,8 @@ class Config(C.Structure):
                 ("max_depth", C.c_uint32), ("leaf_size", C.c_uint32), ("bins", C.c_uint32),
                 ("short_stack", C.c_uint32), ("block_size", C.c_uint32), ("blocks_per_sm", C.c_uint32),
                 ("max_refs", C.c_uint32), ("topk", C.c_uint32), ("fallback_ratio", C.c_float),
-                ("exact_max", C.c_uint32), ("spin_limit", C.c_uint32), ("max_steps", C.c_uint32)]
+                ("exact_max", C.c_uint32), ("spin_limit", C.c_uint32), ("max_steps", C.c_uint32),
+                ("sah_sample", C.c_uint32)]
 
 
 class TuneResult(C.Structure):

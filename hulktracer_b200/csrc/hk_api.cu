@@ -10,6 +10,7 @@
 #include <vector>
 
 #include "hk_build.h"
+#include "hk_resort.h"
 #include "hk_common.cuh"
 #include "hk_internal.h"
 #include "hk_mlp.h"
@@ -75,6 +76,7 @@ struct hk_ctx {
     bool tree_on_device_counts = false;  // its sizes still live in device memory
     hk_tree_stats stats{};
     BuildState build;
+    ResortState resort;   // HK_BUILD_SAH_RESORT
     // ropes of an imported tree (computed on the host when first needed)
     std::vector<uint2> host_nodes;
     DevBuf<uint32_t> imp_ropes;
@@ -173,6 +175,7 @@ hk_status hk_config_default(hk_config *cfg) {
     cfg->topk = 4;
     cfg->fallback_ratio = 1.0f;
     cfg->exact_max = 0;
+    cfg->sah_sample = 5;
     return HK_OK;
 }
 
@@ -242,6 +245,7 @@ hk_status hk_destroy(hk_ctx *c) {
     c->mirror.release(); c->mrays.release(); c->prays.release(); c->mhits.release(); c->phits.release();
     c->mslot.release(); c->mcount.release();
     build_release(c->build);
+    c->resort.release();
     c->mlp_params.release(); c->mlp_grads.release(); c->mlp_m.release(); c->mlp_v.release();
     c->mlp_w1p.release(); c->mlp_w2p.release(); c->mlp_w3p.release(); c->mlp_w4p.release(); c->mlp_tcw.release();
     c->rec_X.release(); c->rec_y.release(); c->rec_rows.release();
@@ -732,9 +736,58 @@ static hk_status build_enqueue(hk_ctx *c, hk_build_mode mode) {
 
 extern "C" {
 
+// HK_BUILD_SAH_RESORT: the reference's --treeType=SAH builder on the GPU
+// (hk_build_resort.cu); its tree takes the place of an imported one
+static hk_status build_resort(hk_ctx *c, hk_tree_stats *stats) {
+    const ResortParams p{c->cfg.traverse_cost, c->cfg.intersect_cost, c->cfg.max_depth, c->cfg.leaf_size,
+                         c->cfg.sah_sample ? c->cfg.sah_sample : 5u};
+    float hb[8];
+    HK_CUDA(c, cudaMemcpyAsync(hb, c->box.p, 32, cudaMemcpyDeviceToHost, c->stream));
+    HK_CUDA(c, cudaStreamSynchronize(c->stream));
+    invalidate_graph(c);
+    c->tree_valid = false;
+    c->tree_built = false;
+    HK_CUDA(c, cudaEventRecord(c->ev0, c->stream));
+    std::string err;
+    hk_status s = resort_build(c->resort, p, c->verts.p, c->tris.p, c->nt, hb, c->stream, &err);
+    if (s != HK_OK) return fail(c, s, err.c_str());
+    HK_CUDA(c, cudaEventRecord(c->ev1, c->stream));
+    const ResortState &R = c->resort;
+    HK_CUDA(c, c->nodes.ensure(R.nn));
+    HK_CUDA(c, c->refs.ensure(std::max<uint32_t>(R.nr, 1)));
+    HK_CUDA(c, c->imp_ropes.ensure(6 * (size_t)R.nn));
+    HK_CUDA(c, c->imp_cbox.ensure(2 * (size_t)R.nn));
+    HK_CUDA(c, cudaMemcpyAsync(c->nodes.p, R.nodes.p, (size_t)R.nn * 8, cudaMemcpyDeviceToDevice, c->stream));
+    if (R.nr)
+        HK_CUDA(c, cudaMemcpyAsync(c->refs.p, R.out_refs.p, (size_t)R.nr * 4, cudaMemcpyDeviceToDevice, c->stream));
+    HK_CUDA(c, cudaMemcpyAsync(c->imp_ropes.p, R.out_ropes.p, (size_t)R.nn * 24, cudaMemcpyDeviceToDevice, c->stream));
+    HK_CUDA(c, cudaMemcpyAsync(c->imp_cbox.p, R.out_cbox.p, (size_t)R.nn * 32, cudaMemcpyDeviceToDevice, c->stream));
+    HK_CUDA(c, cudaStreamSynchronize(c->stream));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+    c->nn = R.nn;
+    c->nr = R.nr;
+    c->tree_valid = true;
+    c->tree_built = false;
+    c->tree_on_device_counts = false;
+    c->imp_ropes_valid = true;
+    c->host_nodes.clear();
+    memset(&c->stats, 0, sizeof(c->stats));
+    c->stats.nodes = R.nn;
+    c->stats.refs = R.nr;
+    c->stats.depth = R.depth;
+    c->stats.build_ms = ms;
+    if (stats) *stats = c->stats;
+    return HK_OK;
+}
+
 hk_status hk_build(hk_ctx *c, hk_build_mode mode, hk_tree_stats *stats) {
     if (!c) return HK_E_ILLEGAL_INPUT;
     if (c->nt == 0) return fail(c, HK_E_STATE, "no scene");
+    if (mode == HK_BUILD_SAH_RESORT) {
+        cudaSetDevice(c->device);
+        return build_resort(c, stats);
+    }
     if (mode != HK_BUILD_BINNED && mode != HK_BUILD_LEARNED) return fail(c, HK_E_ILLEGAL_INPUT, "mode");
     cudaSetDevice(c->device);
     HK_CUDA(c, cudaEventRecord(c->ev0, c->stream));

@@ -3,10 +3,13 @@
     python -m hulktracer_b200.profile_case --case trace --variant shortstack
     python -m hulktracer_b200.profile_case --case build
     python -m hulktracer_b200.profile_case --case frame
+    python -m hulktracer_b200.profile_case --case aff --aff scene.aff --frames 60
 
 Each case sets up the animated 64-part scene (~200k triangles, 1280x720), does
 its warm-up work first and then launches the kernel of interest a few times, so
-an ncu command can select it with -k / -s / -c.
+an ncu command can select it with -k / -s / -c. The aff case instead renders an
+AFF (BART) scene frame by frame on the reference's fixed-tick clock and prints
+device times per frame.
 """
 from __future__ import annotations
 
@@ -27,7 +30,10 @@ def main():
     from hulktracer_b200 import scenes
 
     ap = argparse.ArgumentParser()
-    ap.add_argument("--case", default="trace", choices=["trace", "build", "frame", "breakdown", "batch"])
+    ap.add_argument("--case", default="trace", choices=["trace", "build", "frame", "breakdown", "batch", "aff"])
+    ap.add_argument("--aff", help="aff case: the scene file")
+    ap.add_argument("--frames", type=int, default=60, help="aff case: frames timed")
+    ap.add_argument("--size", type=int, nargs=2, help="aff case: image size (default: the file's resolution)")
     ap.add_argument("--scenes", type=int, default=64, help="batch case: number of scenes")
     ap.add_argument("--rays", type=int, nargs=2, default=[65_536, 4_194_304], help="batch case: ray batch range")
     ap.add_argument("--tris", type=int, nargs=2, default=[10_000, 2_000_000], help="batch case: triangle range")
@@ -39,6 +45,9 @@ def main():
     a = ap.parse_args()
     if a.case == "batch":
         batch_case(a)
+        return
+    if a.case == "aff":
+        aff_case(a)
         return
     sc = scenes.animated_parts()
     W, H = sc.width, sc.height
@@ -104,6 +113,57 @@ def main():
                       hk.VARIANTS[a.variant], True)
         ctx.synchronize()
     print("case %s done: tree %s" % (a.case, {k: st[k] for k in ("nodes", "refs", "depth")}))
+
+
+def aff_case(a):
+    """Frames of an AFF scene through hk_frame (transform, build, trace,
+    shadows, shading in one CUDA graph), timed with CUDA events."""
+    import json
+
+    import numpy as np
+    import torch
+
+    import hulktracer_b200 as hk
+    from hulktracer_b200.engine import Aff, fixed_tick_time
+
+    aff = Aff(a.aff)
+    info = aff.info
+    W, H = a.size if a.size else (info["resx"], info["resy"])
+    W, H = W // 8 * 8, H // 4 * 4
+    lights = aff.lights()
+    if lights.shape[0] == 0:
+        lights = np.array([[1, 1, 1, 1, 0, 100, 0, 1]], np.float32)
+    ctx = hk.Context(exact_max=a.exact_max)
+    mode = hk.BUILD_LEARNED if a.mode == "learned" else hk.BUILD_BINNED
+    if a.mode == "learned":
+        ctx.mlp_load(a.weights)
+    ctx.load_aff(aff, 0.0)
+    out = torch.zeros(W * H, dtype=torch.int32, device="cuda")
+    stream = torch.cuda.Stream()
+    ctx.set_stream(stream.cuda_stream)
+    v = hk.VARIANTS[a.variant]
+    times = [fixed_tick_time(f) for f in range(a.frames)]
+    with torch.cuda.stream(stream):
+        for t in times[:3]:      # warm-up, graph capture
+            ctx.frame(aff.part_matrices(t), aff.camera(t), lights, W, H, out.data_ptr(), mode, v, True)
+        ms, stats = [], []
+        for t in times:
+            mats, cam = aff.part_matrices(t), aff.camera(t)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            ctx.frame(mats, cam, lights, W, H, out.data_ptr(), mode, v, True)
+            e1.record(stream)
+            stream.synchronize()
+            ms.append(e0.elapsed_time(e1))
+    p_, s_ = ctx.ray_counts()
+    st = ctx.stats()
+    res = {"scene": os.path.basename(a.aff), "tris": info["nt"], "meshes": info["nmeshes"],
+           "dynamic_meshes": info["ndynamic"], "size": [W, H], "frames": a.frames, "build": a.mode,
+           "ms_per_frame_median": float(np.median(ms)), "ms_per_frame_mean": float(np.mean(ms)),
+           "rays_last_frame": {"primary": p_, "shadow": s_},
+           "mrays_s": (p_ + s_) / (float(np.median(ms)) * 1e3),
+           "tree_last_frame": {k: st[k] for k in ("nodes", "refs", "depth", "build_ms")}}
+    print(json.dumps(res))
 
 
 def batch_case(a):

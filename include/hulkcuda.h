@@ -69,7 +69,16 @@ typedef enum hk_variant {
 
 typedef enum hk_build_mode {
     HK_BUILD_BINNED = 0,   /* exact binned SAH, every (axis, bin) plane costed */
-    HK_BUILD_LEARNED = 1   /* MLP proposes top-k bins, searched exactly; binned fallback */
+    HK_BUILD_LEARNED = 1,  /* MLP proposes top-k bins, searched exactly; binned fallback */
+    HK_BUILD_SAH_RESORT = 2 /* the reference's --treeType=SAH builder (KDTreeCPU::
+                               buildKDTreeSAH / buildNodeSAH, HulkEngine/src/
+                               KDTreeSAH.cpp:9-244): every node re-samples every
+                               sah_sample-th polygon of its list and sweeps the
+                               sorted candidates; leaf at max_depth or at most
+                               leaf_size polygons. Ct, Ci, max_depth, leaf_size and
+                               sah_sample come from hk_config (the reference's own
+                               constants: 1, 5, 20, 9, 5). The tree equals the
+                               reference's in the compact layout of hk_tree_import */
 } hk_build_mode;
 
 /* Shading semantics for hk_render */
@@ -119,6 +128,9 @@ typedef struct hk_config {
                                  returns HK_E_DEVICE_TIMEOUT (0 = 4M polls) */
     uint32_t max_steps;       /* traversal: node steps per ray before the trace stops
                                  the ray and returns HK_E_BOUNDS (0 = 2^26) */
+    uint32_t sah_sample;      /* HK_BUILD_SAH_RESORT: every sah_sample-th polygon of a
+                                 node makes candidates (c_reductionFactor,
+                                 KDTreeCPU.hpp; 0 = 5) */
 } hk_config;
 
 typedef struct hk_tree_stats {

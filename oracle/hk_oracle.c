@@ -459,6 +459,180 @@ int hko_build_sah_nlogn(const float *verts, const uint32_t *tris, uint32_t nt, c
 }
 
 /* ------------------------------------------------------------------------ */
+/* SAH with per-node re-sampling (--treeType=SAH): KDTreeCPU::buildKDTreeSAH  */
+/* + buildNodeSAH, KDTreeSAH.cpp:9-244                                        */
+/* ------------------------------------------------------------------------ */
+/* KDTreeCPU::buildNodeSAH, KDTreeSAH.cpp:35-244. Every node re-samples its
+ * own polygon list (every reduction-th entry, in list order), clips each
+ * sampled triangle's bounds to the node box, makes a co-planar candidate
+ * where the clipped extent is at most FLT_EPSILON and begin / end candidates
+ * otherwise, sorts by value and sweeps with the same counters as the NlogN
+ * build; the counts start from list size / reduction (integer division) and
+ * run in unsigned 32-bit arithmetic, as there. */
+static void build_node_resort(sah_ctx *c, split_iter *it) {
+    const float Ct = c->p.ct, Ci = c->p.ci;
+    if (it->depth >= c->p.max_depth || it->polys.n < c->p.leaf_below) { /* :38-43 */
+        make_leaf(c, it);
+        return;
+    }
+    for (size_t i = 0; i < it->polys.n; i += c->p.reduction) { /* :51-82 */
+        uint32_t poly = it->polys.a[i];
+        const float *p1 = c->verts + 4 * (size_t)c->tris[4 * poly];
+        const float *p2 = c->verts + 4 * (size_t)c->tris[4 * poly + 1];
+        const float *p3 = c->verts + 4 * (size_t)c->tris[4 * poly + 2];
+        for (uint32_t j = 0; j < 3; j++) {
+            float lo = mn(mn(p1[j], p2[j]), p3[j]);
+            float hi = mx(mx(p1[j], p2[j]), p3[j]);
+            lo = mx(lo, it->box[j]);
+            hi = mn(hi, it->box[4 + j]);
+            cand_t e;
+            e.poly = poly;
+            if (fabsf(lo - hi) <= FLT_EPSILON) {
+                e.marker = EV_COPLANAR;
+                e.value = lo;
+                cv_push(&it->cands[j], e);
+            } else {
+                e.marker = EV_BEGIN;
+                e.value = lo;
+                cv_push(&it->cands[j], e);
+                e.marker = EV_END;
+                e.value = hi;
+                cv_push(&it->cands[j], e);
+            }
+        }
+    }
+    const uint32_t sampled_count = (uint32_t)(it->polys.n / c->p.reduction);
+    float bestScore = FLT_MAX, bestUpper = 0, bestLower = 0, bestValue = 0;
+    uint32_t bestDim = 0;
+    float dim[4];
+    sub4(it->box + 4, it->box, dim);
+    float invBoxSurface = 1.0f / it->surface;
+    for (uint32_t j = 0; j < 3; j++) { /* :96-183 */
+        cvec *cv = &it->cands[j];
+        if (cv->n) qsort(cv->a, cv->n, sizeof(cand_t), cmp_cand);
+        uint32_t below = 0, coplanar = 0, above = 0;
+        uint32_t counters[3] = {0, 0, 0};
+        uint32_t plusPrev = 0, copPrev = 0;
+        float x = dim[(j + 1) % 3], y = dim[(j + 2) % 3];
+        float XplusY = x + y;
+        float planeArea = x * y;
+        size_t i = 0;
+        int first = 1;
+        while (i < cv->n) {
+            float cur = cv->a[i].value;
+            while (i < cv->n && cv->a[i].value == cur) {
+                counters[cv->a[i].marker]++;
+                i++;
+            }
+            below = below + copPrev + plusPrev;
+            coplanar = copPrev;
+            above = above - counters[EV_COPLANAR] - counters[EV_END];
+            if (first) {
+                below = 0;
+                coplanar = counters[EV_COPLANAR];
+                above = sampled_count - counters[EV_COPLANAR];
+                first = 0;
+            }
+            plusPrev = counters[EV_BEGIN];
+            copPrev = counters[EV_COPLANAR];
+            counters[0] = counters[1] = counters[2] = 0;
+            float upper = planeArea + (it->box[4 + j] - cur) * (XplusY);
+            float lower = planeArea + (cur - it->box[j]) * (XplusY);
+            float costBelow = lower * (float)below;
+            float costAbove = upper * (float)above;
+            float costIntersect = planeArea * (float)coplanar;
+            float score = Ct + Ci * ((costIntersect + costBelow + costAbove) * invBoxSurface);
+            if (score < bestScore) {
+                bestScore = score;
+                bestValue = cur;
+                bestDim = j;
+                bestUpper = upper;
+                bestLower = lower;
+            }
+        }
+    }
+    for (int j = 0; j < 3; j++) {
+        free(it->cands[j].a);
+        memset(&it->cands[j], 0, sizeof it->cands[j]);
+    }
+    float leafcost = Ci * (float)sampled_count; /* :186-191 */
+    if (bestScore >= leafcost) {
+        make_leaf(c, it);
+        return;
+    }
+    uint32_t *nd = c->nodes.a + 4 * (size_t)it->node;
+    memcpy(&nd[3], &bestValue, 4);
+    nd[0] = bestDim | HKO_JUNCTION;
+    split_iter A, B; /* above, below */
+    memset(&A, 0, sizeof A);
+    memset(&B, 0, sizeof B);
+    for (size_t i = 0; i < it->polys.n; i++) { /* :203-222 */
+        uint32_t poly = it->polys.a[i];
+        int r = poly_to_plane(c, bestDim, bestValue, poly);
+        if (r == REL_ABOVE) uv_push(&A.polys, poly);
+        else if (r == REL_BELOW) uv_push(&B.polys, poly);
+        else {
+            uv_push(&A.polys, poly);
+            uv_push(&B.polys, poly);
+        }
+    }
+    uint32_t depth = it->depth, node = it->node;
+    float box[8];
+    memcpy(box, it->box, sizeof box);
+    free_iter(it);
+    if (A.polys.n > 0) { /* :226-238 */
+        A.depth = depth + 1;
+        memcpy(A.box, box, sizeof box);
+        A.surface = bestUpper;
+        A.box[bestDim] = bestValue;
+        uint32_t idx = new_node(c);
+        A.node = idx;
+        c->nodes.a[4 * (size_t)node + 1] = idx;
+        build_node_resort(c, &A);
+    }
+    free_iter(&A);
+    if (B.polys.n > 0) { /* :239-251 */
+        B.depth = depth + 1;
+        memcpy(B.box, box, sizeof box);
+        B.surface = bestLower;
+        B.box[4 + bestDim] = bestValue;
+        uint32_t idx = new_node(c);
+        B.node = idx;
+        c->nodes.a[4 * (size_t)node + 2] = idx;
+        build_node_resort(c, &B);
+    }
+    free_iter(&B);
+}
+
+/* KDTreeCPU::buildKDTree + buildKDTreeSAH, KDTreeCPU.cpp:61-94,
+ * KDTreeSAH.cpp:9-32. buildKDTree has pushed the root and buildKDTreeSAH
+ * pushes a second default node that nothing links to (index 1); the root's
+ * box surface is the half surface here (getHalfBoxSurface). */
+int hko_build_sah_resort(const float *verts, const uint32_t *tris, uint32_t nt, const float *box,
+                         const hko_sah_params *p, uint32_t **nodes_out, uint32_t *nn_out,
+                         uint32_t **refs_out, uint32_t *nr_out) {
+    sah_ctx c;
+    memset(&c, 0, sizeof c);
+    c.verts = verts;
+    c.tris = tris;
+    c.p = *p;
+    new_node(&c);
+    new_node(&c);
+    split_iter root;
+    memset(&root, 0, sizeof root);
+    for (uint32_t i = 0; i < nt; i++) uv_push(&root.polys, i);
+    memcpy(root.box, box, 8 * sizeof(float));
+    root.surface = hko_box_half_surface(box);
+    build_node_resort(&c, &root);
+    free_iter(&root);
+    *nodes_out = c.nodes.a;
+    *nn_out = (uint32_t)(c.nodes.n / 4);
+    *refs_out = c.leafpolys.a ? c.leafpolys.a : (uint32_t *)malloc(4);
+    *nr_out = (uint32_t)c.leafpolys.n;
+    return 0;
+}
+
+/* ------------------------------------------------------------------------ */
 /* tree cost and node boxes                                                  */
 /* ------------------------------------------------------------------------ */
 void hko_node_boxes(const uint32_t *nodes, uint32_t nn, const float *box, float *out) {

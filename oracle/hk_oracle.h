@@ -100,6 +100,12 @@ void hko_camera_rays(const float *cam16, uint32_t w, uint32_t h, int norm_mode, 
 int hko_build_sah_nlogn(const float *verts, const uint32_t *tris, uint32_t nt, const float *box,
                         const hko_sah_params *p, uint32_t **nodes_out, uint32_t *nn_out,
                         uint32_t **refs_out, uint32_t *nr_out);
+/* KDTreeCPU::buildKDTreeSAH / buildNodeSAH (KDTreeSAH.cpp:9-244, the
+ * --treeType=SAH builder): the same outputs; node 1 is the unlinked default
+ * node the reference leaves there */
+int hko_build_sah_resort(const float *verts, const uint32_t *tris, uint32_t nt, const float *box,
+                         const hko_sah_params *p, uint32_t **nodes_out, uint32_t *nn_out,
+                         uint32_t **refs_out, uint32_t *nr_out);
 void hko_free(void *p);
 
 /* ---- tree SAH cost with full surface areas ----

@@ -100,6 +100,8 @@ class Oracle:
         pp = C.POINTER(C.POINTER(C.c_uint32))
         L.hko_build_sah_nlogn.argtypes = [_f32p, _u32p, C.c_uint32, _f32p, C.POINTER(_SahParams), pp,
                                           C.POINTER(C.c_uint32), pp, C.POINTER(C.c_uint32)]
+        L.hko_build_sah_resort.argtypes = [_f32p, _u32p, C.c_uint32, _f32p, C.POINTER(_SahParams), pp,
+                                          C.POINTER(C.c_uint32), pp, C.POINTER(C.c_uint32)]
         L.hko_build_binned.argtypes = [_f32p, _u32p, C.c_uint32, _f32p, C.POINTER(_BinnedParams), pp,
                                        C.POINTER(C.c_uint32), pp, C.POINTER(C.c_uint32)]
         L.hko_free.argtypes = [C.c_void_p]
@@ -179,6 +181,18 @@ class Oracle:
         tris = _c(tris, np.uint32)
         self.lib.hko_build_sah_nlogn(_c(verts, np.float32), tris, tris.shape[0], _c(box, np.float32),
                                      C.byref(prm), C.byref(pn), C.byref(nn), C.byref(pr), C.byref(nr))
+        return self._take(pn, nn.value, pr, nr.value, 4)
+
+    def build_sah_resort(self, verts, tris, box, **kw):
+        """buildKDTreeSAH / buildNodeSAH (the --treeType=SAH builder)."""
+        p = dict(REF_SAH)
+        p.update(kw)
+        prm = _SahParams(p["ct"], p["ci"], p["max_depth"], p["leaf_below"], p["reduction"])
+        pn, pr = C.POINTER(C.c_uint32)(), C.POINTER(C.c_uint32)()
+        nn, nr = C.c_uint32(), C.c_uint32()
+        tris = _c(tris, np.uint32)
+        self.lib.hko_build_sah_resort(_c(verts, np.float32), tris, tris.shape[0], _c(box, np.float32),
+                                      C.byref(prm), C.byref(pn), C.byref(nn), C.byref(pr), C.byref(nr))
         return self._take(pn, nn.value, pr, nr.value, 4)
 
     def build_binned(self, verts, tris, box, ct=1.0, ci=1.5, max_depth=24, leaf_size=4, bins=32,
@@ -282,6 +296,7 @@ class Reference:
         L.hkref_create.argtypes = [_f32p, C.c_uint, _u32p, C.c_uint, _f32p]
         L.hkref_destroy.argtypes = [C.c_void_p]
         L.hkref_build.argtypes = [C.c_void_p]
+        L.hkref_set_tree_type.argtypes = [C.c_int]
         L.hkref_set_vertices.argtypes = [C.c_void_p, _f32p, _f32p]
         L.hkref_node_count.restype = C.c_uint
         L.hkref_node_count.argtypes = [C.c_void_p]
@@ -315,7 +330,9 @@ class Reference:
         self._v = _c(verts, np.float32)
         self.lib.hkref_set_vertices(self.h, self._v, _c(box, np.float32))
 
-    def build(self):
+    def build(self, tree_type: str = "SAHNlogN"):
+        """KDTreeCPU::buildKDTree with --treeType (SAHNlogN, the default, or SAH)."""
+        self.lib.hkref_set_tree_type(1 if tree_type == "SAH" else 0)
         self.lib.hkref_build(self.h)
         nn = self.lib.hkref_node_count(self.h)
         nr = self.lib.hkref_ref_count(self.h)

@@ -65,6 +65,15 @@ void *hkref_create(const float *verts, unsigned nv, const unsigned *tris, unsign
 
 void hkref_destroy(void *h) { delete (RefCtx *)h; }
 
+// --treeType: 1 selects buildKDTreeSAH (KDTreeSAH.cpp:9-244), 0 the default
+// buildKDTreeSAH_NlogN (Settings::parseStrings, HulkEngine/src/Settings.cpp:8-23)
+void hkref_set_tree_type(int sah) {
+    set_settings();
+    wchar_t a0[] = L"hk", a1[] = L"scene", a2[] = L"--treeType=SAH", a3[] = L"--treeType=SAHNlogN";
+    wchar_t *argv[] = {a0, a1, sah ? a2 : a3};
+    Settings::getInstance().parseStrings(3, argv);
+}
+
 int hkref_build(void *h) {
     RefCtx *c = (RefCtx *)h;
     return (int)c->tree.buildKDTree(c->scene);
