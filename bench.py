@@ -389,6 +389,7 @@ def run_ours(args):
             "gpu_launches": int(kern_nodes) * args.steps,
             "clocks": cl,
             "roofline": roof,
+            "build_roofline": build_roofline(compare, args.mode),
             "cpu_baseline": base,
             "compare": compare,
         }
@@ -397,6 +398,20 @@ def run_ours(args):
         dist.barrier()
         dist.destroy_process_group()
     ctx.close()
+
+
+def build_roofline(compare, mode):
+    """The builder against HBM: its algorithmic bytes (per level, every
+    reference's index and clipped box read and its next-level slot written,
+    plus the tree written) over its measured time, for the headline's build."""
+    arm = (compare or {}).get("learned" if mode == "learned" else "binned") or {}
+    if "build_gbs" not in arm:
+        return None
+    peak, src = measured_peak()
+    return {"bound": "hbm", "achieved": arm["build_gbs"], "peak": peak, "unit": "GB/s",
+            "frac": arm["build_gbs"] / peak, "peak_source": src, "bytes_per_build": arm["build_bytes"],
+            "build_ms": arm["build_ms"],
+            "bytes": "sum over levels of references x 36 B + nodes x 8 B + leaf references x 4 B"}
 
 
 def reference_tree_cost(hk, rt, device):
@@ -480,11 +495,18 @@ def compare_arms(args, sc, device, ref_cost):
             st = ctx.build(mode)
             cost = ctx.tree_cost(1.0, 1.5)
             learned_nodes, fallback_nodes = st["learned_nodes"], st["fallback_nodes"]
+            # algorithmic bytes of the build: per level, each reference's index
+            # (4 B) and clipped box (24 B) read and its next-level slot (8 B)
+            # written; the tree's nodes (8 B) and leaf references (4 B) written
+            _, lrefs = ctx.level_counts()
+            build_bytes = int(lrefs.astype(np.int64).sum()) * 36 + st["nodes"] * 8 + st["refs"] * 4
         ms = t_frame / len(frames)
         out[name] = {"build": "%s%s" % (mode_s, ", exact SAH on nodes <= %d refs" % exact_max if exact_max else ""),
                      "ms_per_frame": ms, "mrays_s": rays / (t_frame / 1000.0) / 1e6,
                      "build_ms": float(np.median(t_build)), "trace_shade_ms": float(np.median(t_trace)),
-                     "sah_cost": cost, "sah_cost_vs_reference": (cost / ref_cost) if ref_cost else None}
+                     "sah_cost": cost, "sah_cost_vs_reference": (cost / ref_cost) if ref_cost else None,
+                     "build_bytes": build_bytes,
+                     "build_gbs": build_bytes / (float(np.median(t_build)) * 1e-3) / 1e9}
         if mode == hk.BUILD_LEARNED:
             out[name].update({"learned_nodes": learned_nodes, "fallback_nodes": fallback_nodes})
         ctx.close()

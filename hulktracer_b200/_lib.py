@@ -119,6 +119,7 @@ def load(path: str = LIB_PATH):
         "hk_tree_export_compact": [vp, u32p, u32, u32p, u32, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)],
         "hk_tree_stats_get": [vp, C.POINTER(TreeStats)],
         "hk_tree_cost": [vp, C.c_double, C.c_double, C.POINTER(C.c_double)],
+        "hk_build_level_counts": [vp, u32p, u32p, u32, C.POINTER(C.c_uint32)],
         "hk_trace": [vp, f32p, u32, C.c_int, vp],
         "hk_trace_device": [vp, vp, u32, C.c_int, vp],
         "hk_set_counting": [vp, C.c_int],

@@ -604,6 +604,25 @@ hk_status hk_tree_stats_get(hk_ctx *c, hk_tree_stats *st) {
     return HK_OK;
 }
 
+hk_status hk_build_level_counts(hk_ctx *c, uint32_t *nodes, uint32_t *refs, uint32_t cap, uint32_t *nlevels) {
+    if (!c || !nlevels) return HK_E_ILLEGAL_INPUT;
+    if (!c->tree_valid || !c->tree_built) return fail(c, HK_E_STATE, "no tree from hk_build's level-synchronous builder");
+    cudaSetDevice(c->device);
+    hk_status s = sync_tree_sizes(c);
+    if (s != HK_OK) return s;
+    BuildCounters bc;
+    HK_CUDA(c, cudaMemcpyAsync(&bc, c->build.ctr, sizeof bc, cudaMemcpyDeviceToHost, c->stream));
+    HK_CUDA(c, cudaStreamSynchronize(c->stream));
+    uint32_t n = 0;
+    while (n < (uint32_t)kMaxLevels && bc.lvl[n].nodes) n++;
+    *nlevels = n;
+    for (uint32_t l = 0; l < n && l < cap; l++) {
+        if (nodes) nodes[l] = bc.lvl[l].nodes;
+        if (refs) refs[l] = bc.lvl[l].refs;
+    }
+    return HK_OK;
+}
+
 hk_status hk_set_debug_flags(hk_ctx *c, uint32_t flags) {
     if (!c || (flags & ~1u)) return HK_E_ILLEGAL_INPUT;
     c->debug_flags = flags;

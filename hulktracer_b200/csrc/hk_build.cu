@@ -1115,6 +1115,9 @@ __host__ __device__ constexpr uint32_t learn_list_cap(uint32_t K) {
     while (2 * c * 3 * K <= kLearnScratch) c *= 2;
     return c;
 }
+// lists of up to 32 x kLearnSortRegs values sort in registers (every list
+// with k >= 4 proposals); longer ones in shared memory
+constexpr int kLearnSortRegs = 4;
 
 // warp-aggregated append of val (where pred) to list[n ..); n counts past cap
 __device__ __forceinline__ void list_append(float *list, uint32_t cap, uint32_t &n, bool pred, float val) {
@@ -1151,6 +1154,64 @@ __device__ __forceinline__ void warp_sort_smem(float *v, uint32_t n) {
             }
             __syncwarp();
         }
+}
+
+// ascending bitonic sort of v[0, n) by one warp, done in registers: element
+// r * 32 + lane of the list padded with +inf to the next power of two in x[r]
+// of that lane (R registers, up to 32 R elements), every compare-exchange a
+// shuffle (partner in another lane) or a swap between two of the lane's
+// registers; the sorted list is written back to v[0, n)
+template <int R>
+__device__ __forceinline__ void warp_sort_regs(float *v, uint32_t n) {
+    const uint32_t lane = threadIdx.x & 31u;
+    uint32_t n2 = 1;
+    while (n2 < n) n2 <<= 1;
+    const uint32_t nr = (n2 + 31u) >> 5;
+    float x[R];
+#pragma unroll
+    for (int r = 0; r < R; r++) {
+        const uint32_t i = (uint32_t)r * 32u + lane;
+        x[r] = i < n ? v[i] : kInf;
+    }
+    for (uint32_t k = 2; k <= n2; k <<= 1)
+        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+            if (j >= 32) {
+                const uint32_t rj = j >> 5;
+#pragma unroll
+                for (int r = 0; r < R; r++) {
+                    if ((uint32_t)r >= nr || ((uint32_t)r & rj)) continue;
+                    const int r2 = r | (int)rj;
+                    const bool up = (((uint32_t)r * 32u + lane) & k) == 0;
+                    const float a = x[r], b = x[r2];
+                    if ((a > b) == up) {
+                        x[r] = b;
+                        x[r2] = a;
+                    }
+                }
+            } else {
+                const bool lower = (lane & j) == 0;
+#pragma unroll
+                for (int r = 0; r < R; r++) {
+                    if ((uint32_t)r >= nr) continue;
+                    const float p = __shfl_xor_sync(0xffffffffu, x[r], (int)j);
+                    const bool up = (((uint32_t)r * 32u + lane) & k) == 0;
+                    const float mn = x[r] < p ? x[r] : p, mx = x[r] < p ? p : x[r];
+                    x[r] = (lower == up) ? mn : mx;
+                }
+            }
+        }
+    __syncwarp();
+#pragma unroll
+    for (int r = 0; r < R; r++) {
+        const uint32_t i = (uint32_t)r * 32u + lane;
+        if (i < n) v[i] = x[r];
+    }
+    __syncwarp();
+}
+
+__device__ __forceinline__ void warp_sort_list(float *v, uint32_t n) {
+    if (n <= 32u * kLearnSortRegs) warp_sort_regs<kLearnSortRegs>(v, n);
+    else warp_sort_smem(v, n);
 }
 
 // ---------------------------------------------------------------------------
@@ -1290,28 +1351,39 @@ __global__ void __launch_bounds__(256) k_refine(LevelArgs A) {
         uint32_t bl[kLearnMaxK], ab[kLearnMaxK], nL[kLearnMaxK], nH[kLearnMaxK], nF[kLearnMaxK];
 #pragma unroll
         for (int i = 0; i < kLearnMaxK; i++) bl[i] = ab[i] = nL[i] = nH[i] = nF[i] = 0;
-        for (uint32_t base = 0; base < cnt; base += 32) {
-            const bool have = base + lane < cnt;
-            float4 tlo = make_float4(0, 0, 0, 0), thi = tlo;
-            if (have) {
-                const uint32_t tri = A.refs[info.x + base + lane];
-                tlo = A.tb_lo[tri];
-                thi = A.tb_hi[tri];
+        // four references per lane per pass: their loads are issued together
+        for (uint32_t base = 0; base < cnt; base += 128) {
+            float4 tlo[4], thi[4];
+            bool have[4];
+            uint32_t tri[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                have[u] = base + 32u * u + lane < cnt;
+                tri[u] = have[u] ? A.refs[info.x + base + 32u * u + lane] : 0u;
             }
 #pragma unroll
-            for (int i = 0; i < kLearnMaxK; i++) {
-                if ((uint32_t)i >= np) break;
-                const uint32_t a = pax[i];
-                const float l = c3(blo, a), h = c3(bhi, a);
-                const float lo = mxf(c3(tlo, a), l), hi = mnf(c3(thi, a), h);
-                bl[i] += (have && lo < p0[i]) ? 1u : 0u;
-                ab[i] += (have && hi > p1[i]) ? 1u : 0u;
-                const bool inL = have && p0[i] <= lo && lo <= p1[i];
-                const bool inH = have && p0[i] <= hi && hi <= p1[i];
-                float *Ls = scratch + (size_t)i * 3 * cap;
-                list_append(Ls, cap, nL[i], inL, lo);
-                list_append(Ls + cap, cap, nH[i], inH, hi);
-                list_append(Ls + 2 * cap, cap, nF[i], inL && lo == hi, lo);
+            for (int u = 0; u < 4; u++) {
+                tlo[u] = have[u] ? A.tb_lo[tri[u]] : make_float4(0, 0, 0, 0);
+                thi[u] = have[u] ? A.tb_hi[tri[u]] : make_float4(0, 0, 0, 0);
+            }
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                if (base + 32u * u >= cnt) break;   // uniform across the warp
+#pragma unroll
+                for (int i = 0; i < kLearnMaxK; i++) {
+                    if ((uint32_t)i >= np) break;
+                    const uint32_t a = pax[i];
+                    const float l = c3(blo, a), h = c3(bhi, a);
+                    const float lo = mxf(c3(tlo[u], a), l), hi = mnf(c3(thi[u], a), h);
+                    bl[i] += (have[u] && lo < p0[i]) ? 1u : 0u;
+                    ab[i] += (have[u] && hi > p1[i]) ? 1u : 0u;
+                    const bool inL = have[u] && p0[i] <= lo && lo <= p1[i];
+                    const bool inH = have[u] && p0[i] <= hi && hi <= p1[i];
+                    float *Ls = scratch + (size_t)i * 3 * cap;
+                    list_append(Ls, cap, nL[i], inL, lo);
+                    list_append(Ls + cap, cap, nH[i], inH, hi);
+                    list_append(Ls + 2 * cap, cap, nF[i], inL && lo == hi, lo);
+                }
             }
         }
         __syncwarp();
@@ -1332,9 +1404,9 @@ __global__ void __launch_bounds__(256) k_refine(LevelArgs A) {
             const float l = c3(blo, a), h = c3(bhi, a);
             float *Ls = scratch + (size_t)i * 3 * cap, *Hs = Ls + cap, *Fs = Ls + 2 * cap;
             const uint32_t nl = nL[i], nh = nH[i], nf = nF[i];
-            warp_sort_smem(Ls, nl);
-            warp_sort_smem(Hs, nh);
-            if (nf) warp_sort_smem(Fs, nf);
+            warp_sort_list(Ls, nl);
+            warp_sort_list(Hs, nh);
+            if (nf) warp_sort_list(Fs, nf);
             for (uint32_t q = lane; q < nl + nh; q += 32) {
                 const float x = q < nl ? Ls[q] : Hs[q - nl];
                 if (!(x > l && x < h)) continue;

@@ -10,8 +10,10 @@
 //       byte(n, k) = (n / 8) * 1024 + (k / 8) * 128 + (n % 8) * 16 + (k % 8) * 2.
 //     Each chunk (32 KB, 12 KB for the last layer) is one bulk copy
 //     (cp.async.bulk, completion counted on an mbarrier) from global memory
-//     (L2-resident) into one of two shared-memory buffers, the next chunk's
-//     copy in flight while the current chunk is multiplied.
+//     (L2-resident) into a ring of four shared-memory buffers: three chunks
+//     are in flight ahead of the one being multiplied, so a tile pays the
+//     copy latency about once instead of once per chunk, and the next
+//     layer's first chunks arrive during the epilogue.
 //   * Activations: the tile's 128 rows x 256 K values in the same canonical
 //     layout (byte(m, k) = (m / 8) * 4096 + (k / 8) * 128 + (m % 8) * 16 +
 //     (k % 8) * 2), rewritten in place by each layer's epilogue.
@@ -38,11 +40,14 @@ constexpr uint32_t kTcBSbo = kTcChunkK / 8 * 128;            // 1024: next 8 out
 constexpr uint32_t kTcBBytes = 256u * kTcChunkK * 2;         // 32768, the largest chunk
 constexpr int kTcChunks = 16;                                // 4 layers x 4 chunks of 64 K values
 constexpr uint32_t kTcTmemCols = 256;
-constexpr uint32_t kTcBarOff = kTcABytes + 2 * kTcBBytes;    // 131072: 4 mbarriers + the TMEM address
-constexpr size_t kTcSmem = kTcBarOff + 64;
+constexpr int kTcNBuf = 4;                                   // weight-chunk ring
+constexpr uint32_t kTcAhead = kTcNBuf - 1;                   // chunks in flight ahead of the multiplied one
+constexpr uint32_t kTcBarOff = kTcABytes + kTcNBuf * kTcBBytes;   // 196608: 8 mbarriers + the TMEM address
+constexpr size_t kTcSmem = kTcBarOff + 128;
 constexpr uint32_t kTcSpin = 1u << 20;                       // try_wait attempts before giving up
 constexpr uint32_t kErrTensorWait = 32u;                     // *err bit: a tensor-core pipeline wait ran out
-static_assert((size_t)kTcRows * kMlpOut * 4 <= 2 * kTcBBytes, "logits overlay the weight buffers");
+static_assert((size_t)kTcRows * kMlpOut * 4 <= kTcNBuf * kTcBBytes, "logits overlay the weight buffers");
+static_assert(kTcSmem <= 227 * 1024, "shared memory of one CTA");
 
 __host__ __device__ constexpr uint32_t tc_layer_n(int l) { return l == 3 ? (uint32_t)kMlpOut : (uint32_t)kMlpHid; }
 __host__ __device__ constexpr uint32_t tc_chunk_bytes(int l) { return tc_layer_n(l) * kTcChunkK * 2; }
@@ -123,25 +128,23 @@ __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::
 __device__ __forceinline__ void tc_fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
 struct TcSmem {
-    unsigned char *A;     // activations (canonical layout)
-    unsigned char *B[2];  // weight chunks
-    float *logits;        // kTcRows x 96, over the weight buffers after the last layer
-    uint32_t bar_load[2], bar_mma[2];
+    unsigned char *A;      // activations (canonical layout)
+    unsigned char *B0;     // weight chunk ring: buffer b at B0 + b * kTcBBytes
+    float *logits;         // kTcRows x 96, over the weight buffers after the last layer
+    uint32_t bars;         // copy mbarriers (8 bytes each), then the MMA mbarriers
     uint32_t *tmem_addr;
+    __device__ __forceinline__ uint32_t buf(uint32_t b) const { return smem_u32(B0) + b * kTcBBytes; }
+    __device__ __forceinline__ uint32_t bar_load(uint32_t b) const { return bars + 8u * b; }
+    __device__ __forceinline__ uint32_t bar_mma(uint32_t b) const { return bars + 8u * (kTcNBuf + b); }
 };
 
 __device__ __forceinline__ TcSmem tc_smem(unsigned char *base) {
     TcSmem S;
     S.A = base;
-    S.B[0] = base + kTcABytes;
-    S.B[1] = base + kTcABytes + kTcBBytes;
+    S.B0 = base + kTcABytes;
+    S.bars = smem_u32(base + kTcBarOff);
     S.logits = reinterpret_cast<float *>(base + kTcABytes);
-    const uint32_t bars = smem_u32(base + kTcBarOff);
-    S.bar_load[0] = bars;
-    S.bar_load[1] = bars + 8;
-    S.bar_mma[0] = bars + 16;
-    S.bar_mma[1] = bars + 24;
-    S.tmem_addr = reinterpret_cast<uint32_t *>(base + kTcBarOff + 32);
+    S.tmem_addr = reinterpret_cast<uint32_t *>(base + kTcBarOff + 16 * kTcNBuf);
     return S;
 }
 
@@ -149,10 +152,10 @@ __device__ __forceinline__ TcSmem tc_smem(unsigned char *base) {
 // columns allocated by warp 0. Pair with tc_teardown.
 __device__ __forceinline__ uint32_t tc_setup(const TcSmem &S) {
     if (threadIdx.x == 0) {
-        tc_mbar_init(S.bar_load[0], 1);
-        tc_mbar_init(S.bar_load[1], 1);
-        tc_mbar_init(S.bar_mma[0], 1);
-        tc_mbar_init(S.bar_mma[1], 1);
+        for (uint32_t b = 0; b < (uint32_t)kTcNBuf; b++) {
+            tc_mbar_init(S.bar_load(b), 1);
+            tc_mbar_init(S.bar_mma(b), 1);
+        }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (threadIdx.x < 32) {
@@ -182,20 +185,33 @@ __device__ __forceinline__ uint32_t tc_a_off(uint32_t m, uint32_t k) {
 
 // The network on rows row0 .. row0 + 127 of X (rows at or past `rows` are
 // zero); logits in S.logits[r][96] on return. `g` counts the chunks every
-// earlier call of this CTA consumed (mbarrier phases); it advances by
-// kTcChunks. All 256 threads call it. Returns false (on every thread) when a
-// wait ran out; *err then holds kErrTensorWait.
+// earlier call of this CTA consumed: chunk g + q of the CTA goes to buffer
+// (g + q) % 4 and is that buffer's use (g + q) / 4 (the mbarrier phase
+// parity); it advances by kTcChunks. All 256 threads call it. Returns false
+// (on every thread) when a wait ran out; *err then holds kErrTensorWait.
 __device__ __forceinline__ bool tc_tile_forward(const MlpDevice &M, const float *__restrict__ X, uint32_t row0,
                                                 uint32_t rows, const TcSmem &S, uint32_t tmem, uint32_t &g,
                                                 uint32_t *err) {
-    __shared__ uint32_t s_ok;
+    __shared__ uint32_t s_ok, s_issued;
     const unsigned char *__restrict__ Wp = M.tcw;
     const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
+    // thread 0: copy chunk q of this tile into its buffer once the MMAs of the
+    // buffer's previous chunk (kTcNBuf chunks earlier) are done
+    auto issue = [&](uint32_t q) -> bool {
+        const uint32_t gq = g + q, b = gq % kTcNBuf, u = gq / kTcNBuf;
+        if (u >= 1 && !tc_mbar_wait(S.bar_mma(b), (u - 1) & 1u)) return false;
+        const int l = (int)q / 4, kc = (int)q % 4;
+        tc_bulk_load(S.buf(b), Wp + tc_chunk_off(l, kc), tc_chunk_bytes(l), S.bar_load(b));
+        s_issued = q + 1;
+        return true;
+    };
     if (tid == 0) {
         s_ok = 1;
+        s_issued = 0;
         // the buffers were last read by generic loads (the previous tile's logits)
         tc_fence_async_smem();
-        tc_bulk_load(smem_u32(S.B[g & 1u]), Wp + tc_chunk_off(0, 0), tc_chunk_bytes(0), S.bar_load[g & 1u]);
+        for (uint32_t q = 0; q < kTcAhead && s_ok; q++)
+            if (!issue(q)) s_ok = 0;
     }
     // the tile's features as BF16 in the canonical layout, K 200 .. 255 zero
     for (uint32_t i = tid; i < (uint32_t)kTcRows * (kTcAK / 8); i += blockDim.x) {
@@ -216,27 +232,21 @@ __device__ __forceinline__ bool tc_tile_forward(const MlpDevice &M, const float 
     tc_fence_before();
     __syncthreads();
     const uint32_t abase = smem_u32(S.A);
+    uint32_t consumed = 0;   // chunks whose copy thread 0 has waited for
     for (int l = 0; l < 4; l++) {
         const uint32_t N = tc_layer_n(l);
         const uint32_t idesc = tc_idesc(kTcRows, N);
         if (tid == 0 && s_ok) {
             tc_fence_after();
             for (int kc = 0; kc < 4 && s_ok; kc++) {
-                const uint32_t q = (uint32_t)(l * 4 + kc), gq = g + q, b = gq & 1u;
-                // the next chunk into the other buffer, once the MMAs that read it are done
-                if (q + 1 < (uint32_t)kTcChunks) {
-                    if (q >= 1 && !tc_mbar_wait(S.bar_mma[b ^ 1u], ((gq - 1) >> 1) & 1u)) s_ok = 0;
-                    const int l1 = (int)(q + 1) / 4, kc1 = (int)(q + 1) % 4;
-                    if (s_ok)
-                        tc_bulk_load(smem_u32(S.B[b ^ 1u]), Wp + tc_chunk_off(l1, kc1), tc_chunk_bytes(l1),
-                                     S.bar_load[b ^ 1u]);
-                }
-                if (!s_ok || !tc_mbar_wait(S.bar_load[b], (gq >> 1) & 1u)) {
+                const uint32_t q = (uint32_t)(l * 4 + kc), gq = g + q, b = gq % kTcNBuf;
+                if (!tc_mbar_wait(S.bar_load(b), (gq / kTcNBuf) & 1u)) {
                     s_ok = 0;
                     break;
                 }
+                consumed = q + 1;
                 tc_fence_after();
-                const uint32_t bbase = smem_u32(S.B[b]);
+                const uint32_t bbase = S.buf(b);
                 // layer 0 has K = 200: its last chunk has one step of real data (192 .. 207)
                 const int steps = (l == 0 && kc == 3) ? 1 : 4;
                 for (int s = 0; s < steps; s++) {
@@ -244,7 +254,9 @@ __device__ __forceinline__ bool tc_tile_forward(const MlpDevice &M, const float 
                     const uint64_t db = tc_sdesc(bbase + (uint32_t)s * 256u, 128u, kTcBSbo);
                     tc_mma(tmem, da, db, idesc, (kc > 0 || s > 0) ? 1u : 0u);
                 }
-                tc_commit(S.bar_mma[b]);
+                tc_commit(S.bar_mma(b));
+                // refill the ring: the buffer of chunk q - 1, whose MMAs precede these
+                if (q + kTcAhead < (uint32_t)kTcChunks && !issue(q + kTcAhead)) s_ok = 0;
             }
         }
         __syncthreads();
@@ -252,7 +264,7 @@ __device__ __forceinline__ bool tc_tile_forward(const MlpDevice &M, const float 
         // MMAs issued before it)
         const uint32_t glast = g + (uint32_t)(l * 4 + 3);
         bool ok = s_ok != 0;
-        if (ok && !tc_mbar_wait(S.bar_mma[glast & 1u], (glast >> 1) & 1u)) ok = false;
+        if (ok && !tc_mbar_wait(S.bar_mma(glast % kTcNBuf), (glast / kTcNBuf) & 1u)) ok = false;
         if (!ok) s_ok = 0;
         __syncthreads();
         if (!s_ok) break;
@@ -284,20 +296,20 @@ __device__ __forceinline__ bool tc_tile_forward(const MlpDevice &M, const float 
         tc_fence_before();
         __syncthreads();
     }
-    g += kTcChunks;
     if (!s_ok) {
         // let every copy this tile started land before the CTA moves on
         if (tid == 0) {
             atomicOr(err, kErrTensorWait);
-            for (uint32_t k = 0; k < 2; k++) {
-                // the last load into each buffer was chunk kTcChunks - 2 + k (or earlier on a break)
-                const uint32_t gq = g - 2 + k;
-                tc_mbar_wait(S.bar_load[gq & 1u], (gq >> 1) & 1u);
+            for (uint32_t q = consumed; q < s_issued; q++) {
+                const uint32_t gq = g + q;
+                tc_mbar_wait(S.bar_load(gq % kTcNBuf), (gq / kTcNBuf) & 1u);
             }
         }
         __syncthreads();
+        g += kTcChunks;
         return false;
     }
+    g += kTcChunks;
     return true;
 }
 

@@ -216,6 +216,16 @@ class Context:
         n, r = _u32(nodes).reshape(-1, 4), _u32(refs)
         self._check(self.L.hk_tree_import(self.h, ptr(n), n.shape[0], ptr(r), r.shape[0]))
 
+    def level_counts(self):
+        """(nodes, refs) per level of the last level-synchronous build."""
+        n = C.c_uint32()
+        cap = 64
+        nodes = np.zeros(cap, np.uint32)
+        refs = np.zeros(cap, np.uint32)
+        self._check(self.L.hk_build_level_counts(self.h, ptr(nodes), ptr(refs), cap, C.byref(n)))
+        k = min(n.value, cap)
+        return nodes[:k].copy(), refs[:k].copy()
+
     def export_tree(self):
         nn, nr = C.c_uint32(), C.c_uint32()
         self._check(self.L.hk_tree_export(self.h, None, 0, None, 0, C.byref(nn), C.byref(nr)))

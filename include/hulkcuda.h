@@ -216,6 +216,10 @@ hk_status hk_tree_export(hk_ctx *ctx, uint32_t *nodes4, uint32_t cap_nodes, uint
 hk_status hk_tree_export_compact(hk_ctx *ctx, uint32_t *cnodes2, uint32_t cap_nodes,
                                  uint32_t *refs, uint32_t cap_refs, uint32_t *cnn, uint32_t *nr);
 hk_status hk_tree_stats_get(hk_ctx *ctx, hk_tree_stats *stats);
+/* Per level of the last HK_BUILD_BINNED / HK_BUILD_LEARNED build: the level's
+ * nodes and the references they hold (what the builder reads and writes per
+ * level); *nlevels levels, the first min(cap, *nlevels) written. */
+hk_status hk_build_level_counts(hk_ctx *ctx, uint32_t *nodes, uint32_t *refs, uint32_t cap, uint32_t *nlevels);
 /* SAH cost of the current tree (no reference counterpart; the tree-quality
  * measure of both builders): sum over junctions of ct * A(n) / A(root) plus
  * over leaves of ci * |refs(n)| * A(n) / A(root), A the full surface area of the

@@ -64,7 +64,7 @@ def test_frame_on_reference_tree(hk, oracle, golden, k):
     h = c.trace(rays, hk.SHORTSTACK)
     assert np.array_equal(h["tri"], rid)
     m = rid >= 0
-    assert m.mean() > 0.1
+    assert m.sum() > 500   # the animated camera sees part of the scene
     assert np.array_equal(bits(h["t"][m]), bits(rh[m, 0]))
     c.close()
     aff.close()
