@@ -54,7 +54,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="animated", choices=["animated", "static_small", "static_large"])
+    ap.add_argument("--workload", default="animated", choices=["animated", "static_small", "static_large", "aff"])
+    ap.add_argument("--aff", help="aff workload: an AFF (BART) scene file, animated on the reference's fixed-tick clock")
     ap.add_argument("--mode", default="binned", choices=["binned", "learned"])
     ap.add_argument("--variant", default="ropes")
     ap.add_argument("--exact-max", type=int, default=0,
@@ -72,8 +73,12 @@ def parse():
     return ap.parse_args()
 
 
-def make_scene(name):
+def make_scene(name, aff_path=None):
     from hulktracer_b200 import scenes
+    if name == "aff":
+        if not aff_path:
+            raise SystemExit("--workload aff needs --aff <scene file>")
+        return scenes.from_aff(aff_path)
     if name == "animated":
         return scenes.animated_parts()
     if name == "static_small":
@@ -95,6 +100,17 @@ def frame_mats(sc, f):
     if sc.part_center is None:
         return None
     return scenes.part_matrices(sc, f)
+
+
+def frame_cam(sc, f):
+    from hulktracer_b200 import scenes
+    return scenes.frame_camera(sc, f)
+
+
+def data_desc(sc):
+    if "aff" in sc.extra:
+        return "AFF scene file %s (keyframes on the fixed-tick clock)" % sc.name[4:]
+    return "synthetic (seeded procedural scene)"
 
 
 # ---------------------------------------------------------------------------
@@ -152,6 +168,9 @@ def reference_frame(R, O, sc, f, prim, nthreads):
     rigid transform of the vertices, KDTreeCPU::buildKDTree, traceScene.
     Returns (seconds, rays)."""
     t0 = time.perf_counter()
+    if prim is None:   # a moving camera
+        from oracle.oracle import NORM_IEEE
+        prim = O.camera_rays(frame_cam(sc, f), sc.width, sc.height, NORM_IEEE)
     mats = frame_mats(sc, f)
     if mats is not None:
         verts = O.transform(sc.rest_verts, sc.part_of_vertex, mats)
@@ -192,7 +211,7 @@ def cpu_baseline(sc, frames, nthreads):
         kind = "reference"
     else:
         return None
-    prim = O.camera_rays(sc.camera, sc.width, sc.height, NORM_IEEE)
+    prim = None if "aff" in sc.extra else O.camera_rays(sc.camera, sc.width, sc.height, NORM_IEEE)
     R.load(sc.verts, sc.tris, sc.scene_box())
     reference_frame(R, O, sc, 0, prim, nthreads)   # warm-up (page-in, OpenMP pool)
     tot_t, tot_r = 0.0, 0
@@ -209,7 +228,7 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    sc = make_scene(args.workload)
+    sc = make_scene(args.workload, args.aff)
     nthreads = os.cpu_count() or 1
     from oracle.oracle import NORM_IEEE, Oracle, Reference
     if not Reference.available():
@@ -217,7 +236,7 @@ def run_reference(args):
         return
     O = Oracle()
     R = Reference()
-    prim = O.camera_rays(sc.camera, sc.width, sc.height, NORM_IEEE)
+    prim = None if "aff" in sc.extra else O.camera_rays(sc.camera, sc.width, sc.height, NORM_IEEE)
     R.load(sc.verts, sc.tris, sc.scene_box())
     for f in range(args.warmup):
         reference_frame(R, O, sc, f, prim, nthreads)
@@ -230,7 +249,7 @@ def run_reference(args):
     line = {"metric": "Mrays/s (build+trace+shade per frame)", "value": v, "unit": "Mrays/s",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1000.0 * tot_t / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scene)",
+            "vs_baseline": None, "dtype": "f32", "data": data_desc(sc),
             "config": {"workload": workload_name(sc), "build": "reference SAH-NlogN (CPU)",
                        "parallelism": "OpenMP rows, %d threads" % nthreads},
             "impl": "reference",
@@ -265,7 +284,7 @@ def run_ours(args):
     if world > 1:
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
-    sc = make_scene(args.workload)
+    sc = make_scene(args.workload, args.aff)
     W, H = sc.width, sc.height
     variant = hk.VARIANTS[args.variant]
     mode = hk.BUILD_LEARNED if args.mode == "learned" else hk.BUILD_BINNED
@@ -297,14 +316,14 @@ def run_ours(args):
     def do_frame(f, use_graph=True):
         m = pin_mats[f]
         if not rays_split:
-            ctx.frame(m.numpy() if m is not None else None, sc.camera, sc.lights, W, H, rgba.data_ptr(), mode,
+            ctx.frame(m.numpy() if m is not None else None, frame_cam(sc, f), sc.lights, W, H, rgba.data_ptr(), mode,
                       variant, use_graph)
             return
         # this rank's band of the frame on its own replica, then the gather
         if m is not None:
             ctx.transform(m.numpy())
         ctx._check(ctx.L.hk_build(ctx.h, mode, None))
-        ctx.render_rows_device(sc.camera, sc.lights, W, H, y0, y1, band.data_ptr(), variant,
+        ctx.render_rows_device(frame_cam(sc, f), sc.lights, W, H, y0, y1, band.data_ptr(), variant,
                                hk.SHADE_MIRROR if "mirror" in sc.extra else hk.SHADE_CPU)
         rgba.copy_(gather_rows(band, rank, world, W, H))
 
@@ -358,13 +377,13 @@ def run_ours(args):
     ref_cost = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         base = cpu_baseline(sc, args.cpu_frames, os.cpu_count() or 1)
-        if animated and not args.no_compare:
+        if args.workload == "animated" and not args.no_compare:
             rt = reference_tree(sc, args.cost_frame)
             if rt is not None:
                 ref_cost = reference_tree_cost(hk, rt, local)
 
     compare = None
-    if rank == 0 and not args.no_compare and animated:
+    if rank == 0 and not args.no_compare and args.workload == "animated":
         compare = compare_arms(args, sc, local, ref_cost)
 
     if rank == 0:
@@ -375,7 +394,7 @@ def run_ours(args):
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1000.0 * t_dev / args.steps, "higher_is_better": True,
             "scaling": "strong" if rays_split else "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scene)",
+            "vs_baseline": None, "dtype": "f32", "data": data_desc(sc),
             "config": {"workload": workload_name(sc), "build": "GPU %s SAH (32 bins/axis%s), per frame" % (
                            args.mode, ", exact on nodes <= %d refs" % args.exact_max if args.exact_max else ""),
                        "traversal": args.variant,

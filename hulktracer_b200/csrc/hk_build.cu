@@ -500,9 +500,10 @@ __device__ __forceinline__ bool is_medium(const LevelArgs &A, uint32_t c) {
     return A.exact_max >= kWarpExact && c > kWarpExact && c <= A.exact_max;
 }
 __device__ __forceinline__ bool is_large(const LevelArgs &A, uint32_t c) {
-    return c > (A.learned ? kLearnMax : kSmall) && !is_medium(A, c);
+    return c > kSmall && !is_medium(A, c);
 }
-// learned mode: a proposer row (one warp each in k_small, then k_learn)
+// learned mode: a proposer row (its histogram and binned decision from
+// k_small up to 256 references, from k_hist's chunk path above; then k_learn)
 __device__ __forceinline__ bool is_learn(const LevelArgs &A, uint32_t c) {
     return A.learned && c > kWarpExact && c <= kLearnMax;
 }
@@ -1013,7 +1014,23 @@ __global__ void __launch_bounds__(256, 3) k_hist(LevelArgs A) {
         if (s_last && wib == 0) {
             __threadfence();
             const Decision d = sah_warp(GHist{G}, blo, bhi, info.y, A.ct, A.ci);
-            if (lane == 0) {
+            bool row_taken = false;
+            if (is_learn(A, info.y)) {
+                // a proposer row: the binned decision and the features stay
+                // with the row; k_refine_cta / k_refine_warp decide the node
+                uint32_t row = 0;
+                if (lane == 0) row = atomicAdd(&A.lc->n_learn, 1u);
+                row = __shfl_sync(0xffffffffu, row, 0);
+                if (row < A.cap_learn) {
+                    if (lane == 0) {
+                        A.learn_slot[row] = s;
+                        A.learn_bin[row] = LearnBin{d.cost, d.plane, d.axis, d.nb, d.na, {info.y, 0, 0}};
+                    }
+                    hist_features(GHist{G}, info.y, blo, bhi, A.level, A.max_depth, A.feat + (size_t)row * 200);
+                    row_taken = true;
+                }
+            }
+            if (!row_taken && lane == 0) {
                 write_decision(A, s, d);
                 tally.add(d, info.y);
             }
@@ -1087,7 +1104,7 @@ __global__ void __launch_bounds__(256, 5) k_small(LevelArgs A) {
                 if (row < A.cap_learn) {
                     if (lane == 0) {
                         A.learn_slot[row] = s;
-                        A.learn_bin[row] = LearnBin{d.cost, d.plane, d.axis, d.nb, d.na, {0, 0, 0}};
+                        A.learn_bin[row] = LearnBin{d.cost, d.plane, d.axis, d.nb, d.na, {info.y, 0, 0}};
                     }
                     hist_features(Hw, cnt, blo, bhi, A.level, A.max_depth, A.feat + (size_t)row * 200);
                     continue;   // decided and tallied by k_learn
@@ -1105,8 +1122,7 @@ __global__ void __launch_bounds__(256, 5) k_small(LevelArgs A) {
 
 constexpr int kLearnMaxK = 8;
 constexpr uint32_t kLearnScratch = 2048;   // floats of list space per warp
-constexpr uint32_t kRefineWarps = 8;
-constexpr size_t kRefineSmem = (size_t)kRefineWarps * kLearnScratch * 4;   // 64 KB
+constexpr size_t kRefineSmem = (size_t)kLearnScratch * 4;   // the lists of one row, 8 KB
 
 // list capacity per (proposal, list): the largest power of two with 3 k of
 // them in one warp's space (128 for k = 4), so a list sorts in place
@@ -1243,16 +1259,30 @@ __global__ void __launch_bounds__(256, 1) k_learn(LevelArgs A) {
         } else {
             tile_forward(A.mlp, A.feat, row0, rows, S);
         }
+        // the warp's rows are rr = wib + 8 q: lane q looks up row q's node
+        // first (the axes of zero extent have no valid bin), all at once
+        uint32_t my_slot = 0, my_axes = 0, my_cidx = 0;
+        {
+            const uint32_t rr = wib + 8u * lane;
+            if (lane < kRows / 8 && row0 + rr < rows) {
+                my_slot = A.learn_slot[row0 + rr];
+                const float4 blo = A.n_lo[my_slot], bhi = A.n_hi[my_slot];
+#pragma unroll
+                for (int j = 0; j < 3; j++)
+                    if (__fsub_rn(c3(bhi, j), c3(blo, j)) > 0.0f) my_axes |= 1u << j;
+                if (A.prop_log) my_cidx = A.n_info[my_slot].z;
+            }
+        }
         for (uint32_t rr = wib; rr < kRows && row0 + rr < rows; rr += 8) {
-            const uint32_t row = row0 + rr;
-            const uint32_t s = A.learn_slot[row];
-            const float4 blo = A.n_lo[s], bhi = A.n_hi[s];
+            const uint32_t row = row0 + rr, q = rr >> 3;
+            const uint32_t axes = __shfl_sync(0xffffffffu, my_axes, (int)q);
+            const uint32_t cidx = __shfl_sync(0xffffffffu, my_cidx, (int)q);
             const float *Lg = logits + rr * kMlpOut;
             float v[3];
 #pragma unroll
             for (int j = 0; j < 3; j++) {
                 const float x = Lg[32 * j + lane];
-                v[j] = __fsub_rn(c3(bhi, j), c3(blo, j)) > 0.0f ? (x == x ? x : -INFINITY) : NAN;
+                v[j] = ((axes >> j) & 1u) ? (x == x ? x : -INFINITY) : NAN;
             }
             uint32_t packed[2] = {0xffffffffu, 0xffffffffu};
             for (uint32_t r = 0; r < K; r++) {
@@ -1281,7 +1311,6 @@ __global__ void __launch_bounds__(256, 1) k_learn(LevelArgs A) {
             }
             if (lane == 0) {
                 A.learn_prop[row] = make_uint2(packed[0], packed[1]);
-                const uint32_t cidx = A.n_info[s].z;
                 if (A.prop_log && cidx < A.cap_nodes)
                     for (uint32_t r = 0; r < 8; r++) {
                         const uint32_t b = (packed[r >> 2] >> (8u * (r & 3u))) & 0xffu;
@@ -1295,25 +1324,235 @@ __global__ void __launch_bounds__(256, 1) k_learn(LevelArgs A) {
 }
 
 // ---------------------------------------------------------------------------
-// k_refine: one warp per proposer row over the whole GPU.
-//   1. one pass over the node's references: per proposed bin (axis a, bin b,
-//      the closed interval [P0, P1] = [p_b, p_{b+1}] with p_0 the node's
-//      minimum and p_32 its maximum) the references whose clipped lower bound
-//      lies below P0 and those whose clipped upper bound lies above P1 are
-//      counted, and the lower bounds, upper bounds and flat references inside
-//      [P0, P1] are listed in shared memory (then sorted);
-//   2. every listed bound p strictly inside the node is a candidate -- the
+// k_refine_cta: one CTA per proposer row of more than kRefineWarpMax
+// references, grid-striding over the level's rows (k_refine_warp takes the
+// others).
+//   1. the 256 threads pass over the node's references once: per proposed bin
+//      (axis a, bin b, the closed interval [P0, P1] = [p_b, p_{b+1}] with p_0
+//      the node's minimum and p_32 its maximum) the references whose clipped
+//      lower bound lies below P0 and those whose clipped upper bound lies
+//      above P1 are counted, and the lower bounds, upper bounds and flat
+//      references inside [P0, P1] are listed in shared memory (slots taken
+//      per warp with one shared atomic: the order of a list is arbitrary, its
+//      contents are not);
+//   2. each warp sorts some of the lists (in registers);
+//   3. every listed bound p strictly inside the node is a candidate -- the
 //      exact SAH's candidates that fall in the bin -- with
 //        below = #(lo < P0) + #(listed lo < p) + #(listed flat at p),
 //        above = #(hi > P1) + #(listed hi > p) + #(listed flat at p)
 //      (binary searches in the sorted lists), the exact SAH's own counts; the
-//      cheapest by (cost, axis, plane) wins;
-//   3. that plane is taken unless it costs more than fallback_ratio x the
+//      threads share the candidates and the cheapest by (cost, axis, plane)
+//      wins (equal keys are the same plane with the same counts);
+//   4. that plane is taken unless it costs more than fallback_ratio x the
 //      binned optimum k_small found for the node (then the binned plane); the
 //      usual leaf test follows.
 // A bin whose lists overflow their capacity (learn_list_cap) is not costed.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_refine(LevelArgs A) {
+constexpr uint32_t kRefineThreads = 256;
+constexpr uint32_t kRefineWarpMax = 128;   // rows up to this many references: one warp each
+constexpr uint32_t kRefineRowWarps = 8;
+constexpr size_t kRefineWarpSmem = (size_t)kRefineRowWarps * kLearnScratch * 4;   // 64 KB
+
+__device__ __forceinline__ bool refine_better(float c, uint32_t a, float p, float bc, uint32_t ba, float bp) {
+    return c < bc || (c == bc && (a < ba || (a == ba && p < bp)));
+}
+
+__global__ void __launch_bounds__(kRefineThreads) k_refine_cta(LevelArgs A) {
+    extern __shared__ __align__(16) float refine_smem[];
+    __shared__ uint32_t s_tally[5];
+    __shared__ uint32_t s_stat[2];
+    __shared__ uint32_t s_n[3 * kLearnMaxK], s_bl[kLearnMaxK], s_ab[kLearnMaxK];
+    __shared__ float s_wc[kRefineThreads / 32], s_wp[kRefineThreads / 32];
+    __shared__ uint32_t s_wa[kRefineThreads / 32], s_wnb[kRefineThreads / 32], s_wna[kRefineThreads / 32];
+    wait_prior_grid();
+    if (level_aborted(A)) return;
+    Tally tally;
+    uint32_t n_learned = 0, n_fallback = 0;
+    const uint32_t tid = threadIdx.x, lane = tid & 31u, wib = tid >> 5;
+    constexpr uint32_t kWarps = kRefineThreads / 32;
+    const uint32_t rows = min(A.lc->n_learn, A.cap_learn);
+    const uint32_t K = A.topk < (uint32_t)kLearnMaxK ? (A.topk ? A.topk : 1u) : (uint32_t)kLearnMaxK;
+    const uint32_t cap = learn_list_cap(K);
+    for (uint32_t row = blockIdx.x; row < rows; row += gridDim.x) {
+        const LearnBin lb = A.learn_bin[row];
+        if (lb.pad[0] <= kRefineWarpMax) continue;   // k_refine_warp's row (uniform over the CTA)
+        const uint32_t s = A.learn_slot[row];
+        const uint4 info = A.n_info[s];
+        const float4 blo = A.n_lo[s], bhi = A.n_hi[s];
+        const uint32_t cnt = info.y;
+        const uint2 pp = A.learn_prop[row];
+        uint32_t pax[kLearnMaxK];
+        float p0[kLearnMaxK], p1[kLearnMaxK];
+        uint32_t np = 0;
+#pragma unroll
+        for (int r = 0; r < kLearnMaxK; r++) {
+            const uint32_t b8 = ((r < 4 ? pp.x : pp.y) >> (8 * (r & 3))) & 0xffu;
+            if (b8 == 0xffu || (uint32_t)r >= K) break;
+            const uint32_t a = b8 >> 5, b = b8 & 31u;
+            const float l = c3(blo, a), h = c3(bhi, a), ext = __fsub_rn(h, l);
+            pax[r] = a;
+            p0[r] = b == 0 ? l : plane_k(l, ext, b);
+            p1[r] = b == kBins - 1 ? h : plane_k(l, ext, b + 1);
+            np++;
+        }
+        if (tid < 3 * kLearnMaxK) s_n[tid] = 0;
+        if (tid < kLearnMaxK) s_bl[tid] = s_ab[tid] = 0;
+        __syncthreads();
+        // 1. counts and lists over the node's references
+        uint32_t bl[kLearnMaxK], ab[kLearnMaxK];
+#pragma unroll
+        for (int i = 0; i < kLearnMaxK; i++) bl[i] = ab[i] = 0;
+        for (uint32_t base = 0; base < cnt; base += kRefineThreads) {
+            const bool have = base + tid < cnt;
+            float4 tlo = make_float4(0, 0, 0, 0), thi = tlo;
+            if (have) {
+                const uint32_t tri = A.refs[info.x + base + tid];
+                tlo = A.tb_lo[tri];
+                thi = A.tb_hi[tri];
+            }
+#pragma unroll
+            for (int i = 0; i < kLearnMaxK; i++) {
+                if ((uint32_t)i >= np) break;
+                const uint32_t a = pax[i];
+                const float l = c3(blo, a), h = c3(bhi, a);
+                const float lo = mxf(c3(tlo, a), l), hi = mnf(c3(thi, a), h);
+                bl[i] += (have && lo < p0[i]) ? 1u : 0u;
+                ab[i] += (have && hi > p1[i]) ? 1u : 0u;
+                const bool inL = have && p0[i] <= lo && lo <= p1[i];
+                const bool inH = have && p0[i] <= hi && hi <= p1[i];
+                const bool inF = inL && lo == hi;
+                float *Ls = refine_smem + (size_t)i * 3 * cap;
+#pragma unroll
+                for (int q = 0; q < 3; q++) {
+                    const bool pred = q == 0 ? inL : (q == 1 ? inH : inF);
+                    const uint32_t m = __ballot_sync(0xffffffffu, pred);
+                    if (!m) continue;
+                    uint32_t pos0 = 0;
+                    if (lane == (uint32_t)(__ffs(m) - 1)) pos0 = atomicAdd(&s_n[3 * i + q], (uint32_t)__popc(m));
+                    pos0 = __shfl_sync(0xffffffffu, pos0, __ffs(m) - 1);
+                    if (pred) {
+                        const uint32_t pos = pos0 + __popc(m & ((1u << lane) - 1u));
+                        if (pos < cap) Ls[(size_t)q * cap + pos] = q == 1 ? hi : lo;
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < kLearnMaxK; i++) {
+            if ((uint32_t)i >= np) break;
+            uint32_t b0 = bl[i], a0 = ab[i];
+            for (int o = 16; o; o >>= 1) {
+                b0 += __shfl_xor_sync(0xffffffffu, b0, o);
+                a0 += __shfl_xor_sync(0xffffffffu, a0, o);
+            }
+            if (lane == 0) {
+                if (b0) atomicAdd(&s_bl[i], b0);
+                if (a0) atomicAdd(&s_ab[i], a0);
+            }
+        }
+        __syncthreads();
+        // 2. sort the lists of the bins that did not overflow
+        for (uint32_t j = wib; j < 3 * np; j += kWarps) {
+            const uint32_t i = j / 3;
+            if (s_n[3 * i] > cap || s_n[3 * i + 1] > cap || s_n[3 * i + 2] > cap) continue;
+            const uint32_t n = s_n[j];
+            if (n > 1) warp_sort_list(refine_smem + (size_t)j * cap, n);
+        }
+        __syncthreads();
+        // 3. exact costs of the listed candidates
+        const float Anode = surf(blo, bhi);
+        float mc = kInf, m_pk = 0.0f;
+        uint32_t m_ax = 3, m_nb = 0, m_na = 0;
+        for (uint32_t i = 0; i < np; i++) {
+            const uint32_t nl = s_n[3 * i], nh = s_n[3 * i + 1], nf = s_n[3 * i + 2];
+            if (nl > cap || nh > cap || nf > cap) continue;   // overflowed: not costed
+            const uint32_t a = pax[i], b0 = s_bl[i], a0 = s_ab[i];
+            const float l = c3(blo, a), h = c3(bhi, a);
+            const float *Ls = refine_smem + (size_t)i * 3 * cap, *Hs = Ls + cap, *Fs = Ls + 2 * cap;
+            for (uint32_t q = tid; q < nl + nh; q += kRefineThreads) {
+                const float x = q < nl ? Ls[q] : Hs[q - nl];
+                if (!(x > l && x < h)) continue;
+                const float pk = __fadd_rn(x, 0.0f);
+                const uint32_t fon = nf ? upper_bound_f(Fs, nf, pk) - lower_bound_f(Fs, nf, pk) : 0u;
+                const uint32_t nb = b0 + lower_bound_f(Ls, nl, pk) + fon;
+                const uint32_t na = a0 + (nh - upper_bound_f(Hs, nh, pk)) + fon;
+                float4 bb = bhi, ba = blo;
+                s3(bb, a, pk);
+                s3(ba, a, pk);
+                const float sb = surf(blo, bb), sa = surf(ba, bhi);
+                const float cost = __fadd_rn(
+                    A.ct,
+                    __fmul_rn(A.ci, __fdiv_rn(__fadd_rn(__fmul_rn(sb, (float)nb), __fmul_rn(sa, (float)na)), Anode)));
+                if (refine_better(cost, a, pk, mc, m_ax, m_pk)) {
+                    mc = cost;
+                    m_ax = a;
+                    m_pk = pk;
+                    m_nb = nb;
+                    m_na = na;
+                }
+            }
+        }
+        // 4. the cheapest over the CTA
+        for (int off = 16; off; off >>= 1) {
+            const float oc = __shfl_xor_sync(0xffffffffu, mc, off), op = __shfl_xor_sync(0xffffffffu, m_pk, off);
+            const uint32_t oa = __shfl_xor_sync(0xffffffffu, m_ax, off);
+            const uint32_t onb = __shfl_xor_sync(0xffffffffu, m_nb, off), ona = __shfl_xor_sync(0xffffffffu, m_na, off);
+            if (refine_better(oc, oa, op, mc, m_ax, m_pk)) {
+                mc = oc;
+                m_pk = op;
+                m_ax = oa;
+                m_nb = onb;
+                m_na = ona;
+            }
+        }
+        if (lane == 0) {
+            s_wc[wib] = mc;
+            s_wp[wib] = m_pk;
+            s_wa[wib] = m_ax;
+            s_wnb[wib] = m_nb;
+            s_wna[wib] = m_na;
+        }
+        __syncthreads();
+        if (tid == 0) {
+            float bc = s_wc[0], bp = s_wp[0];
+            uint32_t bax = s_wa[0], nb = s_wnb[0], na = s_wna[0];
+            for (uint32_t w = 1; w < kWarps; w++)
+                if (refine_better(s_wc[w], s_wa[w], s_wp[w], bc, bax, bp)) {
+                    bc = s_wc[w];
+                    bp = s_wp[w];
+                    bax = s_wa[w];
+                    nb = s_wnb[w];
+                    na = s_wna[w];
+                }
+            // 5. the proposal's plane, or the binned optimum
+            const bool take = bc < kInf && bc <= __fmul_rn(A.fallback_ratio, lb.cost);
+            Decision d;
+            if (take) {
+                d = Decision{(int)bax, bp, nb, na, bc, 0};
+                if (!(bc < __fmul_rn(A.ci, (float)cnt))) d.axis = -1;
+            } else {
+                d = Decision{lb.axis, lb.plane, lb.nb, lb.na, lb.cost, 0};
+            }
+            write_decision(A, s, d, blo, bhi);
+            tally.add(d, cnt);
+            if (take) n_learned++;
+            else n_fallback++;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x < 2) s_stat[threadIdx.x] = 0;
+    __syncthreads();
+    if (n_learned) atomicAdd(&s_stat[0], n_learned);
+    if (n_fallback) atomicAdd(&s_stat[1], n_fallback);
+    __syncthreads();
+    if (threadIdx.x == 0 && s_stat[0]) atomicAdd(&A.ctr->learned_nodes, s_stat[0]);
+    if (threadIdx.x == 1 && s_stat[1]) atomicAdd(&A.ctr->fallback_nodes, s_stat[1]);
+    tally_flush(A, tally, s_tally);
+}
+
+// rows of at most kRefineWarpMax references: one warp per row, eight rows per
+// CTA, the same three steps with the lists in the warp's own shared memory
+__global__ void __launch_bounds__(256) k_refine_warp(LevelArgs A) {
     extern __shared__ __align__(16) float refine_smem[];
     __shared__ uint32_t s_tally[5];
     __shared__ uint32_t s_stat[2];
@@ -1326,12 +1565,13 @@ __global__ void __launch_bounds__(256) k_refine(LevelArgs A) {
     const uint32_t K = A.topk < (uint32_t)kLearnMaxK ? (A.topk ? A.topk : 1u) : (uint32_t)kLearnMaxK;
     const uint32_t cap = learn_list_cap(K);
     float *scratch = refine_smem + (size_t)wib * kLearnScratch;
-    for (uint32_t row = blockIdx.x * kRefineWarps + wib; row < rows; row += gridDim.x * kRefineWarps) {
+    for (uint32_t row = blockIdx.x * kRefineRowWarps + wib; row < rows; row += gridDim.x * kRefineRowWarps) {
+        const LearnBin lb = A.learn_bin[row];
+        if (lb.pad[0] > kRefineWarpMax) continue;   // k_refine_cta's row
         const uint32_t s = A.learn_slot[row];
         const uint4 info = A.n_info[s];
         const float4 blo = A.n_lo[s], bhi = A.n_hi[s];
         const uint32_t cnt = info.y;
-        const LearnBin lb = A.learn_bin[row];
         const uint2 pp = A.learn_prop[row];
         uint32_t pax[kLearnMaxK];
         float p0[kLearnMaxK], p1[kLearnMaxK];
@@ -2043,7 +2283,9 @@ cudaError_t build_learn_setup() {
         if (e == cudaSuccess)
             e = cudaFuncSetAttribute(k_learn<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem);
         if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(k_refine, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kRefineSmem);
+            e = cudaFuncSetAttribute(k_refine_cta, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kRefineSmem);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(k_refine_warp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kRefineWarpSmem);
         if (e != cudaSuccess) return e;
         if (dev < 64) attr_set |= 1ull << dev;
     }
@@ -2147,12 +2389,14 @@ cudaError_t build_launch(BuildState &S, const float4 *verts, const uint4 *tris, 
         k_hist<<<G, 256, 0, S.aux>>>(A);
         cudaEventRecord(S.ev_join, S.aux);
         if (A.learned) {
-            // proposer rows from the small-node kernel, then the network and
-            // the restricted exact search, beside the large nodes' histograms
+            // proposer rows from both node kernels (so the join comes first),
+            // then the network and the restricted exact search
             launch_pdl(k_small<true, true>, G * 2, 256, 0, st, A);
+            cudaStreamWaitEvent(st, S.ev_join, 0);
             if (mlp_use_tcgen05() && A.mlp.tcw) launch_pdl(k_learn<true>, S.sm_count, 256, kTcSmem, st, A);
             else launch_pdl(k_learn<false>, S.sm_count, 256, kTileSmem, st, A);
-            launch_pdl(k_refine, S.sm_count * 3, 256, kRefineSmem, st, A);
+            launch_pdl(k_refine_cta, S.sm_count * 8, kRefineThreads, kRefineSmem, st, A);
+            launch_pdl(k_refine_warp, S.sm_count * 3, 256, kRefineWarpSmem, st, A);
         } else if (A.exact_max >= kWarpExact) {
             launch_pdl(k_small<true, false>, G * 2, 256, 0, st, A);
         } else {

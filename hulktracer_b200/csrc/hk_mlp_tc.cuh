@@ -43,7 +43,9 @@ constexpr uint32_t kTcTmemCols = 256;
 constexpr int kTcNBuf = 4;                                   // weight-chunk ring
 constexpr uint32_t kTcAhead = kTcNBuf - 1;                   // chunks in flight ahead of the multiplied one
 constexpr uint32_t kTcBarOff = kTcABytes + kTcNBuf * kTcBBytes;   // 196608: 8 mbarriers + the TMEM address
-constexpr size_t kTcSmem = kTcBarOff + 128;
+constexpr uint32_t kTcBiasOff = kTcBarOff + 128;                 // the four bias vectors (864 floats)
+constexpr uint32_t kTcBiasN = 3 * kMlpHid + kMlpOut;
+constexpr size_t kTcSmem = kTcBiasOff + kTcBiasN * 4;
 constexpr uint32_t kTcSpin = 1u << 20;                       // try_wait attempts before giving up
 constexpr uint32_t kErrTensorWait = 32u;                     // *err bit: a tensor-core pipeline wait ran out
 static_assert((size_t)kTcRows * kMlpOut * 4 <= kTcNBuf * kTcBBytes, "logits overlay the weight buffers");
@@ -133,6 +135,7 @@ struct TcSmem {
     float *logits;         // kTcRows x 96, over the weight buffers after the last layer
     uint32_t bars;         // copy mbarriers (8 bytes each), then the MMA mbarriers
     uint32_t *tmem_addr;
+    float *bias;           // b1 | b2 | b3 | b4, copied at the start of every tile
     __device__ __forceinline__ uint32_t buf(uint32_t b) const { return smem_u32(B0) + b * kTcBBytes; }
     __device__ __forceinline__ uint32_t bar_load(uint32_t b) const { return bars + 8u * b; }
     __device__ __forceinline__ uint32_t bar_mma(uint32_t b) const { return bars + 8u * (kTcNBuf + b); }
@@ -145,6 +148,7 @@ __device__ __forceinline__ TcSmem tc_smem(unsigned char *base) {
     S.bars = smem_u32(base + kTcBarOff);
     S.logits = reinterpret_cast<float *>(base + kTcABytes);
     S.tmem_addr = reinterpret_cast<uint32_t *>(base + kTcBarOff + 16 * kTcNBuf);
+    S.bias = reinterpret_cast<float *>(base + kTcBiasOff);
     return S;
 }
 
@@ -213,20 +217,43 @@ __device__ __forceinline__ bool tc_tile_forward(const MlpDevice &M, const float 
         for (uint32_t q = 0; q < kTcAhead && s_ok; q++)
             if (!issue(q)) s_ok = 0;
     }
+    // the biases, read by every epilogue
+    for (uint32_t i = tid; i < kTcBiasN; i += blockDim.x) {
+        const uint32_t l = i / kMlpHid, j = i % kMlpHid;
+        S.bias[i] = l == 0 ? M.b1[j] : (l == 1 ? M.b2[j] : (l == 2 ? M.b3[j] : M.b4[j]));
+    }
     // the tile's features as BF16 in the canonical layout, K 200 .. 255 zero
-    for (uint32_t i = tid; i < (uint32_t)kTcRows * (kTcAK / 8); i += blockDim.x) {
-        const uint32_t m = i / (kTcAK / 8), k0 = (i % (kTcAK / 8)) * 8;
-        const uint32_t r = row0 + m;
-        uint32_t w[4];
+    // (a row of 200 floats starts 800-byte aligned: 8 values are two float4)
+    // (four rows' loads in flight per thread before any is converted)
+    constexpr uint32_t kStage = 4;
+    for (uint32_t i0 = tid; i0 < (uint32_t)kTcRows * (kTcAK / 8); i0 += kStage * blockDim.x) {
+        float4 x0[kStage], x1[kStage];
 #pragma unroll
-        for (int j = 0; j < 4; j++) {
-            const uint32_t k = k0 + 2 * j;
-            const float a = (r < rows && k < (uint32_t)kMlpIn) ? X[(size_t)r * kMlpIn + k] : 0.0f;
-            const float b = (r < rows && k + 1 < (uint32_t)kMlpIn) ? X[(size_t)r * kMlpIn + k + 1] : 0.0f;
-            const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
-            w[j] = *reinterpret_cast<const uint32_t *>(&h);
+        for (uint32_t u = 0; u < kStage; u++) {
+            const uint32_t i = i0 + u * blockDim.x;
+            const uint32_t m = i / (kTcAK / 8), k0 = (i % (kTcAK / 8)) * 8;
+            const uint32_t r = row0 + m;
+            x0[u] = x1[u] = make_float4(0, 0, 0, 0);
+            if (i < (uint32_t)kTcRows * (kTcAK / 8) && r < rows && k0 < (uint32_t)kMlpIn) {
+                const float4 *src = reinterpret_cast<const float4 *>(X + (size_t)r * kMlpIn + k0);
+                x0[u] = src[0];
+                x1[u] = src[1];
+            }
         }
-        *reinterpret_cast<uint4 *>(S.A + tc_a_off(m, k0)) = make_uint4(w[0], w[1], w[2], w[3]);
+#pragma unroll
+        for (uint32_t u = 0; u < kStage; u++) {
+            const uint32_t i = i0 + u * blockDim.x;
+            if (i >= (uint32_t)kTcRows * (kTcAK / 8)) break;
+            const uint32_t m = i / (kTcAK / 8), k0 = (i % (kTcAK / 8)) * 8;
+            const float v[8] = {x0[u].x, x0[u].y, x0[u].z, x0[u].w, x1[u].x, x1[u].y, x1[u].z, x1[u].w};
+            uint32_t w[4];
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const __nv_bfloat162 h = __floats2bfloat162_rn(v[2 * j], v[2 * j + 1]);
+                w[j] = *reinterpret_cast<const uint32_t *>(&h);
+            }
+            *reinterpret_cast<uint4 *>(S.A + tc_a_off(m, k0)) = make_uint4(w[0], w[1], w[2], w[3]);
+        }
     }
     tc_fence_async_smem();
     tc_fence_before();
@@ -272,7 +299,7 @@ __device__ __forceinline__ bool tc_tile_forward(const MlpDevice &M, const float 
         // epilogue: warp w reads lanes 32 (w % 4) .. + 31 (rows), columns of half w / 4
         const uint32_t m = 32u * (warp & 3u) + lane;
         const uint32_t half = N / 2, c0 = (warp >> 2) * half;
-        const float *bl = l == 0 ? M.b1 : (l == 1 ? M.b2 : (l == 2 ? M.b3 : M.b4));
+        const float *bl = S.bias + (uint32_t)l * kMlpHid;
         for (uint32_t c = c0; c < c0 + half; c += 16) {
             uint32_t r[16];
             tc_ld16(tmem + ((32u * (warp & 3u)) << 16) + c, r);

@@ -338,9 +338,44 @@ def animated_parts(seed: int = 3, width: int = 1280, height: int = 720, n_parts:
     return sc
 
 
+def from_aff(path: str) -> Scene:
+    """An AFF (BART) scene file as an animated scene: one part per mesh, the
+    rest pose as vertices, the file's lights (one white point light above the
+    scene when it has none), resolution and camera. Frame f is the reference's
+    fixed-tick time f / 10 (engine.fixed_tick_time); its part matrices and
+    camera come from the file's keyframes (``part_matrices``, ``frame_camera``)."""
+    import os
+
+    from .engine import Aff
+    aff = Aff(path)
+    i = aff.info
+    verts, tris, part = aff.geometry()
+    lights = aff.lights()
+    if lights.shape[0] == 0:
+        box = scene_box(verts)
+        lights = np.array([[1, 1, 1, E_POINT, (box[0] + box[4]) / 2, box[5] + (box[5] - box[1]), (box[2] + box[6]) / 2,
+                            1]], np.float32)
+    w, h = max(8, i["resx"] // 8 * 8), max(4, i["resy"] // 4 * 4)
+    return Scene(verts=verts, tris=tris, lights=lights, camera=aff.camera(0.0).reshape(4, 4), width=w, height=h,
+                 name="aff_" + os.path.splitext(os.path.basename(path))[0], part_of_vertex=part, rest_verts=verts,
+                 part_center=np.zeros((i["nmeshes"], 3)), extra={"aff": aff})
+
+
+def frame_camera(sc: Scene, frame: int) -> np.ndarray:
+    """The camera of ``frame``: an AFF scene's "camera" animation, else fixed."""
+    if "aff" in sc.extra:
+        from .engine import fixed_tick_time
+        return sc.extra["aff"].camera(fixed_tick_time(frame)).reshape(4, 4)
+    return sc.camera
+
+
 def part_matrices(sc: Scene, frame: int) -> np.ndarray:
     """Per-part 3x4 row-major rigid transforms (float32[P, 12]) for ``frame``:
-    rotate about the part centre by omega*frame around its axis, then drift."""
+    rotate about the part centre by omega*frame around its axis, then drift
+    (an AFF scene: its keyframed transforms at the frame's time)."""
+    if "aff" in sc.extra:
+        from .engine import fixed_tick_time
+        return sc.extra["aff"].part_matrices(fixed_tick_time(frame))
     P = sc.part_center.shape[0]
     out = np.zeros((P, 12), dtype=np.float32)
     for p in range(P):

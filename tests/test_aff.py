@@ -185,3 +185,16 @@ def test_bart_museum_missing_blob():
     with pytest.raises(HkError) as e:
         Aff(os.path.join(BART, "museum", "museum7.aff"))
     assert e.value.status == HK_E_FILE_OPEN and "animart7.aff" in str(e.value)
+
+
+def test_scene_from_aff(aff, oracle):
+    """The bench's AFF workload: one part per mesh, the file's lights and
+    resolution, matrices and camera on the fixed-tick clock."""
+    from hulktracer_b200 import scenes
+    sc = scenes.from_aff(SCENE)
+    assert sc.ntris == 812 and (sc.width, sc.height) == (320, 200)
+    assert sc.part_center.shape[0] == aff.info["nmeshes"] and sc.lights.shape == (3, 8)
+    t = fixed_tick_time(7)
+    assert np.array_equal(scenes.part_matrices(sc, 7), aff.part_matrices(t))
+    assert np.array_equal(scenes.frame_camera(sc, 7).ravel(), aff.camera(t))
+    assert not np.array_equal(scenes.frame_camera(sc, 0), scenes.frame_camera(sc, 30))
