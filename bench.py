@@ -57,7 +57,8 @@ def parse():
     ap.add_argument("--workload", default="animated", choices=["animated", "static_small", "static_large", "aff"])
     ap.add_argument("--aff", help="aff workload: an AFF (BART) scene file, animated on the reference's fixed-tick clock")
     ap.add_argument("--mode", default="binned", choices=["binned", "learned"])
-    ap.add_argument("--variant", default="ropes")
+    ap.add_argument("--variant", default="auto",
+                    help="traversal variant, or auto: hk_autotune picks variant, block size and stack depth")
     ap.add_argument("--exact-max", type=int, default=0,
                     help="exact SAH on nodes of at most this many references (0: 32-bin binned SAH everywhere)")
     ap.add_argument("--weights", default=os.path.join(os.path.dirname(os.path.abspath(__file__)), "hulktracer_b200",
@@ -286,7 +287,7 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
     sc = make_scene(args.workload, args.aff)
     W, H = sc.width, sc.height
-    variant = hk.VARIANTS[args.variant]
+    variant = hk.VARIANTS.get(args.variant, hk.ROPES)
     mode = hk.BUILD_LEARNED if args.mode == "learned" else hk.BUILD_BINNED
     stream = torch.cuda.Stream()
     ctx = hk.Context(device=local, exact_max=args.exact_max)
@@ -301,6 +302,20 @@ def run_ours(args):
         # the large static scene: one mirror bounce on 30% of the triangles
         ctx.set_mirrors(sc.extra["mirror"])
         ctx.set_frame_shading(hk.SHADE_MIRROR)
+    tuned = None
+    if args.variant == "auto":
+        # hk_autotune (untimed setup): traversal layout, block size and stack
+        # depth timed on the first frame's primary rays of this scene and tree
+        m0 = frame_mats(sc, 0)
+        if m0 is not None:
+            ctx.transform(m0)
+        else:
+            ctx.precompute()
+        ctx.build(mode)
+        d_rays = torch.from_numpy(ctx.camera_rays(frame_cam(sc, 0), W, H)).cuda()
+        tuned = ctx.autotune(d_rays.data_ptr(), W * H)
+        variant = tuned["variant"]
+        del d_rays
     rgba = torch.zeros(W * H, dtype=torch.int32, device="cuda")
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     rays_split = args.split == "rays"
@@ -384,7 +399,7 @@ def run_ours(args):
 
     compare = None
     if rank == 0 and not args.no_compare and args.workload == "animated":
-        compare = compare_arms(args, sc, local, ref_cost)
+        compare = compare_arms(args, sc, local, ref_cost, variant, tuned)
 
     if rank == 0:
         nl = sc.lights.shape[0]
@@ -397,7 +412,8 @@ def run_ours(args):
             "vs_baseline": None, "dtype": "f32", "data": data_desc(sc),
             "config": {"workload": workload_name(sc), "build": "GPU %s SAH (32 bins/axis%s), per frame" % (
                            args.mode, ", exact on nodes <= %d refs" % args.exact_max if args.exact_max else ""),
-                       "traversal": args.variant,
+                       "traversal": {v: k for k, v in hk.VARIANTS.items()}[variant],
+                       "autotune": tuned,
                        "graph": "stages launched per frame (row bands)" if rays_split else "one CUDA graph per frame",
                        "l2": "flushed (256 MB write) between frames",
                        "parallelism": ("row bands of every frame over %d GPU(s), framebuffer all_gather" % world)
@@ -451,7 +467,7 @@ def reference_tree_cost(hk, rt, device):
 ARMS = (("binned", "binned", 0), ("learned", "learned", 0), ("exact", "binned", 1024))
 
 
-def compare_arms(args, sc, device, ref_cost):
+def compare_arms(args, sc, device, ref_cost, variant, tuned):
     """The metric's comparison on this GPU: the same frames through the same
     engine with each build (binned 32-bin SAH, learned proposer, exact SAH on
     nodes of up to 1024 references). Per arm: ms per frame (one CUDA graph per
@@ -462,14 +478,14 @@ def compare_arms(args, sc, device, ref_cost):
 
     import hulktracer_b200 as hk
     W, H = sc.width, sc.height
-    variant = hk.VARIANTS[args.variant]
+    cfg = {"block_size": tuned["block_size"], "short_stack": tuned["short_stack"]} if tuned else {}
     out = {}
     frames = list(range(args.warmup, args.warmup + args.steps))
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     for name, mode_s, exact_max in ARMS:
         mode = hk.BUILD_LEARNED if mode_s == "learned" else hk.BUILD_BINNED
         stream = torch.cuda.Stream()
-        ctx = hk.Context(device=device, exact_max=exact_max)
+        ctx = hk.Context(device=device, exact_max=exact_max, **cfg)
         ctx.set_stream(stream.cuda_stream)
         if mode == hk.BUILD_LEARNED:
             if not os.path.exists(args.weights):

@@ -499,13 +499,14 @@ __device__ __forceinline__ bool decidable(const LevelArgs &A, uint32_t cnt) {
 __device__ __forceinline__ bool is_medium(const LevelArgs &A, uint32_t c) {
     return A.exact_max >= kWarpExact && c > kWarpExact && c <= A.exact_max;
 }
-__device__ __forceinline__ bool is_large(const LevelArgs &A, uint32_t c) {
-    return c > kSmall && !is_medium(A, c);
-}
-// learned mode: a proposer row (its histogram and binned decision from
-// k_small up to 256 references, from k_hist's chunk path above; then k_learn)
+// learned mode: a proposer row (33..1024 references)
 __device__ __forceinline__ bool is_learn(const LevelArgs &A, uint32_t c) {
     return A.learned && c > kWarpExact && c <= kLearnMax;
+}
+// large: k_hist's chunked histograms (in learned mode the proposer rows too, so
+// that the proposer's chain needs nothing from k_small)
+__device__ __forceinline__ bool is_large(const LevelArgs &A, uint32_t c) {
+    return (c > kSmall || is_learn(A, c)) && !is_medium(A, c);
 }
 
 // root node + references of level 0 (the counters were zeroed by a memset);
@@ -922,6 +923,33 @@ __device__ Decision sah_exact_cta(const LevelArgs &A, uint4 info, float4 blo, fl
 // Large nodes, binned mode: one CTA per chunk of 1024 references builds the
 // chunk's histograms in shared memory and adds them to the node's global
 // histogram; the CTA that finishes the node's last chunk evaluates the SAH.
+// the binned SAH of a large node from its complete histogram (one warp): a
+// proposer row keeps the binned decision and the features for k_refine_cta /
+// k_refine_warp, every other node is decided here
+template <class HistPtr>
+__device__ __forceinline__ void finish_large(const LevelArgs &A, uint32_t s, const uint4 &info, float4 blo,
+                                             float4 bhi, HistPtr H, Tally &tally) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const Decision d = sah_warp(H, blo, bhi, info.y, A.ct, A.ci);
+    if (is_learn(A, info.y)) {
+        uint32_t row = 0;
+        if (lane == 0) row = atomicAdd(&A.lc->n_learn, 1u);
+        row = __shfl_sync(0xffffffffu, row, 0);
+        if (row < A.cap_learn) {
+            if (lane == 0) {
+                A.learn_slot[row] = s;
+                A.learn_bin[row] = LearnBin{d.cost, d.plane, d.axis, d.nb, d.na, {info.y, 0, 0}};
+            }
+            hist_features(H, info.y, blo, bhi, A.level, A.max_depth, A.feat + (size_t)row * 200);
+            return;
+        }
+    }
+    if (lane == 0) {
+        write_decision(A, s, d);
+        tally.add(d, info.y);
+    }
+}
+
 __global__ void __launch_bounds__(256, 3) k_hist(LevelArgs A) {
     __shared__ uint32_t H[kHist];
     __shared__ ExactCtaSmem XS;
@@ -1001,6 +1029,12 @@ __global__ void __launch_bounds__(256, 3) k_hist(LevelArgs A) {
                 if (tri[k] != 0xffffffffu) hist_ref(H, tlo[k], thi[k], blo, bhi, inv3);
         }
         __syncthreads();
+        if (info.y <= kChunk) {
+            // the node's only chunk: its histogram is complete in shared memory
+            if (wib == 0) finish_large(A, s, info, blo, bhi, H, tally);
+            __syncthreads();
+            continue;
+        }
         uint32_t *G = A.hist + (size_t)rank * kHist;
         for (uint32_t i = threadIdx.x; i < kHist; i += blockDim.x)
             if (H[i]) atomicAdd(&G[i], H[i]);
@@ -1013,27 +1047,7 @@ __global__ void __launch_bounds__(256, 3) k_hist(LevelArgs A) {
         __syncthreads();
         if (s_last && wib == 0) {
             __threadfence();
-            const Decision d = sah_warp(GHist{G}, blo, bhi, info.y, A.ct, A.ci);
-            bool row_taken = false;
-            if (is_learn(A, info.y)) {
-                // a proposer row: the binned decision and the features stay
-                // with the row; k_refine_cta / k_refine_warp decide the node
-                uint32_t row = 0;
-                if (lane == 0) row = atomicAdd(&A.lc->n_learn, 1u);
-                row = __shfl_sync(0xffffffffu, row, 0);
-                if (row < A.cap_learn) {
-                    if (lane == 0) {
-                        A.learn_slot[row] = s;
-                        A.learn_bin[row] = LearnBin{d.cost, d.plane, d.axis, d.nb, d.na, {info.y, 0, 0}};
-                    }
-                    hist_features(GHist{G}, info.y, blo, bhi, A.level, A.max_depth, A.feat + (size_t)row * 200);
-                    row_taken = true;
-                }
-            }
-            if (!row_taken && lane == 0) {
-                write_decision(A, s, d);
-                tally.add(d, info.y);
-            }
+            finish_large(A, s, info, blo, bhi, GHist{G}, tally);
             // clean the histogram and the done counter for the next level
             __syncwarp();
             for (uint32_t i = lane; i < kHist; i += 32) G[i] = 0;
@@ -2199,7 +2213,7 @@ hk_status build_prepare(BuildState &S, const BuildParams &p, uint32_t nt, int sm
     S.cap_refs = cap_refs;
     S.cap_nodes = cap_nodes;
     S.cap_level = std::min(cap_refs, cap_nodes) + 1;
-    S.cap_large = cap_refs / kSmall + 2;
+    S.cap_large = cap_refs / (kWarpExact + 1) + 2;   // learned mode: every node above 32 references
     S.cap_chunks = cap_refs / kChunk + S.cap_large + 2;
     S.cap_medium = cap_refs / (kWarpExact + 1) + 2;
     S.cap_learn = cap_refs / (kWarpExact + 1) + 2;
@@ -2257,10 +2271,15 @@ hk_status build_prepare(BuildState &S, const BuildParams &p, uint32_t nt, int sm
     }
     cudaMemset(S.err, 0, 4);
     cudaMemset(S.epoch, 0, 4);
+    cudaMemset(S.hist, 0, (size_t)S.cap_large * kHist * sizeof(uint32_t));
+    cudaMemset(S.done, 0, (size_t)S.cap_large * sizeof(uint32_t));
     cudaMemset(S.plan_flags, 0, (size_t)S.plan_tiles * 4);
     cudaMemset(S.ref_flags, 0, (size_t)S.ref_tiles * 4);
     cudaMemset(S.plan_done, 0, (size_t)S.plan_tiles * 4);
     cudaMemset(S.ctr, 0, sizeof(BuildCounters));
+    // these run on the legacy stream, which does not order against the
+    // context's own stream: every one is finished before a build may start
+    if (cudaDeviceSynchronize() != cudaSuccess) return HK_E_ALLOC;
     return HK_OK;
 }
 
@@ -2355,10 +2374,9 @@ cudaError_t build_launch(BuildState &S, const float4 *verts, const uint4 *tris, 
     }
     cudaMemsetAsync(S.ctr, 0, sizeof(BuildCounters), st);
     if (A.prop_log) cudaMemsetAsync(A.prop_log, 0xff, (size_t)S.cap_nodes * 8 * sizeof(int32_t), st);
-    // per-rank histograms / done counters start at zero (the kernels clean
-    // what they use; this also clears what an aborted build left)
-    cudaMemsetAsync(S.hist, 0, (size_t)S.cap_large * kHist * sizeof(uint32_t), st);
-    cudaMemsetAsync(S.done, 0, (size_t)S.cap_large * sizeof(uint32_t), st);
+    // the per-rank histograms and done counters are zero here: zeroed at
+    // allocation, cleaned by the kernel that used them, and zeroed again by
+    // build_read_stats after a build that stopped on an error
     if (nt) k_tri_bounds<<<(nt + 255) / 256, 256, 0, st>>>(verts, tris, nt, S.tb_lo, S.tb_hi);
     A.nx_lo = S.n_lo[0];
     A.nx_hi = S.n_hi[0];
@@ -2387,16 +2405,17 @@ cudaError_t build_launch(BuildState &S, const float4 *verts, const uint4 *tris, 
         cudaEventRecord(S.ev_fork, st);
         cudaStreamWaitEvent(S.aux, S.ev_fork, 0);
         k_hist<<<G, 256, 0, S.aux>>>(A);
+        if (A.learned) {
+            // the proposer's chain on the second stream after the histograms
+            // (every proposer row comes from k_hist), beside the small nodes
+            if (mlp_use_tcgen05() && A.mlp.tcw) launch_pdl(k_learn<true>, S.sm_count, 256, kTcSmem, S.aux, A);
+            else launch_pdl(k_learn<false>, S.sm_count, 256, kTileSmem, S.aux, A);
+            launch_pdl(k_refine_cta, S.sm_count * 8, kRefineThreads, kRefineSmem, S.aux, A);
+            launch_pdl(k_refine_warp, S.sm_count * 3, 256, kRefineWarpSmem, S.aux, A);
+        }
         cudaEventRecord(S.ev_join, S.aux);
         if (A.learned) {
-            // proposer rows from both node kernels (so the join comes first),
-            // then the network and the restricted exact search
             launch_pdl(k_small<true, true>, G * 2, 256, 0, st, A);
-            cudaStreamWaitEvent(st, S.ev_join, 0);
-            if (mlp_use_tcgen05() && A.mlp.tcw) launch_pdl(k_learn<true>, S.sm_count, 256, kTcSmem, st, A);
-            else launch_pdl(k_learn<false>, S.sm_count, 256, kTileSmem, st, A);
-            launch_pdl(k_refine_cta, S.sm_count * 8, kRefineThreads, kRefineSmem, st, A);
-            launch_pdl(k_refine_warp, S.sm_count * 3, 256, kRefineWarpSmem, st, A);
         } else if (A.exact_max >= kWarpExact) {
             launch_pdl(k_small<true, false>, G * 2, 256, 0, st, A);
         } else {
@@ -2425,6 +2444,9 @@ hk_status build_read_stats(BuildState &S, cudaStream_t st, hk_tree_stats *out) {
     S.last_err = err;
     if (err) {
         cudaMemsetAsync(S.err, 0, 4, st);
+        // a stopped build may leave partial histograms behind
+        cudaMemsetAsync(S.hist, 0, (size_t)S.cap_large * kHist * sizeof(uint32_t), st);
+        cudaMemsetAsync(S.done, 0, (size_t)S.cap_large * sizeof(uint32_t), st);
         if (err & (4u | kErrTensorWait)) return HK_E_DEVICE_TIMEOUT;   // a bounded wait ran out
         if (err & (8u | 16u)) return HK_E_BOUNDS;       // a partition / plan check fired
         return HK_E_CAPACITY;                           // an arena or list was too small

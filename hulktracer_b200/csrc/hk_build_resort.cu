@@ -31,6 +31,7 @@
 // breadth-first order: below, above; an absent child is an empty leaf cell),
 // with the ropes and cell boxes of every cell. It is the tree of the
 // reference's builder in the layout hk_tree_import makes of it.
+#include <algorithm>
 #include <cfloat>
 #include <string>
 
@@ -276,6 +277,7 @@ struct LevelPtrs {
     uint32_t *nkeys, *koff, *jflag, *jrank, *leafcnt, *loff, *efirst, *decision, *gfirst;
     float *plane, *surf_lo, *surf_hi;
     u64 *best, *keys, *f1, *f2, *rflag, *rscan;
+    uint32_t *maxseg;   // longest candidate segment of the level
     // next level
     float4 *nlo, *nhi;
     float *nsurf;
@@ -299,6 +301,7 @@ __global__ void k_r_init(LevelPtrs L) {
     const uint32_t c = L.cnt[i];
     const uint32_t s = forced_leaf(L, c) ? 0u : (c + L.p.sample - 1) / L.p.sample;
     L.nkeys[i] = 6u * s;
+    if (s) atomicMax(L.maxseg, 2u * s);
     L.best[i] = ~0ull;
     L.efirst[3 * i] = L.efirst[3 * i + 1] = L.efirst[3 * i + 2] = 0;
 }
@@ -346,6 +349,99 @@ __device__ __forceinline__ void seg_range(const LevelPtrs &L, uint32_t seg, uint
     s1 = s0 + 2 * s;
 }
 
+// Levels whose candidate segments are all short sort each segment on its own
+// instead of the whole level: a warp in registers up to kSegWarpMax keys
+// (8 per lane), a CTA in shared memory up to kSegCtaMax. Segments hold their
+// keys in fixed ranges, so either way every segment ends up sorted in place.
+constexpr uint32_t kSegWarpMax = 256, kSegCtaMax = 4096;
+
+template <int RJ>
+__device__ __forceinline__ void reg_exchange(u64 (&x)[kSegWarpMax / 32], uint32_t nr, uint32_t lane, uint32_t k) {
+#pragma unroll
+    for (int r = 0; r < (int)(kSegWarpMax / 32); r++) {
+        if ((r & RJ) || (uint32_t)r >= nr) continue;
+        const bool up = (((uint32_t)r * 32u + lane) & k) == 0;
+        const u64 a = x[r], b = x[r | RJ];
+        if ((a > b) == up) {
+            x[r] = b;
+            x[r | RJ] = a;
+        }
+    }
+}
+
+__global__ void k_seg_sort_warp(LevelPtrs L, uint32_t nseg) {
+    const uint32_t lane = threadIdx.x & 31u, seg = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (seg >= nseg) return;   // uniform over the warp
+    uint32_t i, ax, s0, s1;
+    seg_range(L, seg, i, ax, s0, s1);
+    const uint32_t n = s1 - s0;
+    if (n <= 1 || n > kSegWarpMax) return;
+    uint32_t n2 = 1;
+    while (n2 < n) n2 <<= 1;
+    const uint32_t nr = (n2 + 31u) >> 5;
+    u64 x[kSegWarpMax / 32];
+#pragma unroll
+    for (int r = 0; r < (int)(kSegWarpMax / 32); r++) {
+        const uint32_t e = (uint32_t)r * 32u + lane;
+        x[r] = e < n ? L.keys[s0 + e] : ~0ull;
+    }
+    for (uint32_t k = 2; k <= n2; k <<= 1)
+        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+            if (j >= 32) {
+                // partners in the lane's own registers (compile-time indices)
+                if (j == 32) reg_exchange<1>(x, nr, lane, k);
+                else if (j == 64) reg_exchange<2>(x, nr, lane, k);
+                else reg_exchange<4>(x, nr, lane, k);
+            } else {
+                const bool lower = (lane & j) == 0;
+#pragma unroll
+                for (int r = 0; r < (int)(kSegWarpMax / 32); r++) {
+                    if ((uint32_t)r >= nr) continue;
+                    const u64 o = __shfl_xor_sync(0xffffffffu, x[r], (int)j);
+                    const bool up = (((uint32_t)r * 32u + lane) & k) == 0;
+                    const u64 mn = x[r] < o ? x[r] : o, mx = x[r] < o ? o : x[r];
+                    x[r] = (lower == up) ? mn : mx;
+                }
+            }
+        }
+#pragma unroll
+    for (int r = 0; r < (int)(kSegWarpMax / 32); r++) {
+        const uint32_t e = (uint32_t)r * 32u + lane;
+        if (e < n) L.keys[s0 + e] = x[r];
+    }
+}
+
+__global__ void __launch_bounds__(256) k_seg_sort_cta(LevelPtrs L, uint32_t nseg) {
+    __shared__ u64 sk[kSegCtaMax];
+    for (uint32_t seg = blockIdx.x; seg < nseg; seg += gridDim.x) {
+        uint32_t i, ax, s0, s1;
+        seg_range(L, seg, i, ax, s0, s1);
+        const uint32_t n = s1 - s0;
+        if (n <= kSegWarpMax || n > kSegCtaMax) continue;   // uniform over the CTA
+        uint32_t n2 = 1;
+        while (n2 < n) n2 <<= 1;
+        for (uint32_t e = threadIdx.x; e < n2; e += blockDim.x) sk[e] = e < n ? L.keys[s0 + e] : ~0ull;
+        __syncthreads();
+        for (uint32_t k = 2; k <= n2; k <<= 1)
+            for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+                for (uint32_t e = threadIdx.x; e < n2; e += blockDim.x) {
+                    const uint32_t p = e ^ j;
+                    if (p > e) {
+                        const bool up = (e & k) == 0;
+                        const u64 a = sk[e], b = sk[p];
+                        if ((a > b) == up) {
+                            sk[e] = b;
+                            sk[p] = a;
+                        }
+                    }
+                }
+                __syncthreads();
+            }
+        for (uint32_t e = threadIdx.x; e < n; e += blockDim.x) L.keys[s0 + e] = sk[e];
+        __syncthreads();
+    }
+}
+
 // group heads and the counters the sweep accumulates:
 //   f1 = [begin or co-planar] | [co-planar] << 32, f2 = [end] | [head] << 32
 __global__ void k_r_heads(LevelPtrs L, uint32_t K) {
@@ -375,12 +471,11 @@ __global__ void k_r_gfirst(LevelPtrs L, uint32_t K) {
     if (hi32(b) != hi32(a)) L.gfirst[hi32(a)] = p;
 }
 
-// the SAH of every group (KDTreeSAH.cpp:147-175)
-__global__ void k_r_cost(LevelPtrs L, uint32_t K) {
-    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= K) return;
+// (cost, key position) of the group that starts at key p, or ~0 when p
+// starts no group or its cost is not below FLT_MAX
+__device__ u64 r_group_cost(const LevelPtrs &L, uint32_t p) {
     const u64 g2 = L.f2[p], g2n = L.f2[p + 1];
-    if (hi32(g2n) == hi32(g2)) return;   // not a group head
+    if (hi32(g2n) == hi32(g2)) return ~0ull;   // not a group head
     const uint32_t g = hi32(g2);
     const u64 k = L.keys[p];
     const uint32_t seg = (uint32_t)(k >> 34);
@@ -406,8 +501,33 @@ __global__ void k_r_cost(LevelPtrs L, uint32_t K) {
     const float inv = __fdiv_rn(1.0f, L.surf[i]);
     const float score =
         __fadd_rn(L.p.ct, __fmul_rn(L.p.ci, __fmul_rn(__fadd_rn(__fadd_rn(ci, cb), ca), inv)));
-    if (score < FLT_MAX) atomicMin(&L.best[i], ((u64)f2o(score) << 32) | p);
+    return score < FLT_MAX ? ((u64)f2o(score) << 32) | p : ~0ull;
 }
+
+// the SAH of every group (KDTreeSAH.cpp:147-175); the node's minimum of
+// (cost, position) is taken over the warp first (keys are sorted by node, so
+// a warp's lanes span few nodes), then with one atomicMin per node and warp
+__global__ void k_r_cost(LevelPtrs L, uint32_t K) {
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t lane = threadIdx.x & 31u;
+    u64 packed = ~0ull;
+    uint32_t node = 0xffffffffu;
+    if (p < K) {
+        node = (uint32_t)(L.keys[p] >> 34) / 3u;
+        packed = r_group_cost(L, p);
+    }
+    // segmented minimum over runs of equal node in lane order
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const u64 o = __shfl_down_sync(0xffffffffu, packed, off);
+        const uint32_t on = __shfl_down_sync(0xffffffffu, node, off);
+        if (lane + off < 32 && on == node && o < packed) packed = o;
+    }
+    const uint32_t prev = __shfl_up_sync(0xffffffffu, node, 1);
+    const bool first = lane == 0 || prev != node;
+    if (p < K && first && packed != ~0ull) atomicMin(&L.best[node], packed);
+}
+
 
 // leaf test (KDTreeSAH.cpp:186-191) and the split's child surfaces
 __global__ void k_r_decide(LevelPtrs L) {
@@ -694,10 +814,13 @@ hk_status resort_build(ResortState &S, const ResortParams &p, const float4 *vert
         L.nbase = level == 0 ? 2u : cbase + n;   // the next level's first cell
         L.rbase = rbase;
         // 1. candidates
+        L.maxseg = S.dev_u32.p + 3;
+        RS_CHECK(cudaMemsetAsync(L.maxseg, 0, 4, st));
         k_r_init<<<blocks(n), 256, 0, st>>>(L);
         RS_CHECK(scan_excl<uint32_t>(S.nkeys.p, S.koff.p, n, S.scan_part, st));
-        uint32_t K = 0;
+        uint32_t K = 0, maxseg = 0;
         RS_CHECK(cudaMemcpyAsync(&K, S.koff.p + n, 4, cudaMemcpyDeviceToHost, st));
+        RS_CHECK(cudaMemcpyAsync(&maxseg, L.maxseg, 4, cudaMemcpyDeviceToHost, st));
         RS_CHECK(cudaStreamSynchronize(st));
         RS_CHECK(S.keys[0].ensure(K ? K : 1));
         RS_CHECK(S.keys[1].ensure(K ? K : 1));
@@ -711,16 +834,23 @@ hk_status resort_build(ResortState &S, const ResortParams &p, const float4 *vert
         if (K) {
             k_r_emit<<<blocks(K / 6), 256, 0, st>>>(L, K / 6, verts, tris);
             // 2. sort by (segment, value, marker)
-            uint32_t segbits = 1;
-            while (segbits < 30 && (1ull << segbits) < 3ull * n) segbits++;
-            const int nbits = 34 + (int)segbits;
-            const uint32_t ntiles = (K + kTile - 1) / kTile;
-            RS_CHECK(S.hist.ensure(256 * (size_t)ntiles + 1));
-            for (int shift = 0; shift < nbits; shift += 8) {
-                k_rs_hist<<<ntiles, kRT, 0, st>>>(S.keys[kc].p, K, shift, ntiles, S.hist.p);
-                RS_CHECK(scan_excl<uint32_t>(S.hist.p, S.hist.p, 256 * ntiles, S.scan_part, st));
-                k_rs_scatter<<<ntiles, kRT, 0, st>>>(S.keys[kc].p, S.keys[kc ^ 1].p, K, shift, ntiles, S.hist.p);
-                kc ^= 1;
+            if (maxseg <= kSegCtaMax) {
+                const uint32_t nseg = 3 * n;
+                k_seg_sort_warp<<<(unsigned)(((size_t)nseg * 32 + 255) / 256), 256, 0, st>>>(L, nseg);
+                if (maxseg > kSegWarpMax) k_seg_sort_cta<<<std::min<uint32_t>(nseg, 148u * 8u), 256, 0, st>>>(L, nseg);
+            } else {
+                uint32_t segbits = 1;
+                while (segbits < 30 && (1ull << segbits) < 3ull * n) segbits++;
+                const int nbits = 34 + (int)segbits;
+                const uint32_t ntiles = (K + kTile - 1) / kTile;
+                RS_CHECK(S.hist.ensure(256 * (size_t)ntiles + 1));
+                for (int shift = 0; shift < nbits; shift += 8) {
+                    k_rs_hist<<<ntiles, kRT, 0, st>>>(S.keys[kc].p, K, shift, ntiles, S.hist.p);
+                    RS_CHECK(scan_excl<uint32_t>(S.hist.p, S.hist.p, 256 * ntiles, S.scan_part, st));
+                    k_rs_scatter<<<ntiles, kRT, 0, st>>>(S.keys[kc].p, S.keys[kc ^ 1].p, K, shift, ntiles,
+                                                         S.hist.p);
+                    kc ^= 1;
+                }
             }
             L.keys = S.keys[kc].p;
             // 3. sweep

@@ -38,7 +38,9 @@ def main():
     ap.add_argument("--rays", type=int, nargs=2, default=[65_536, 4_194_304], help="batch case: ray batch range")
     ap.add_argument("--tris", type=int, nargs=2, default=[10_000, 2_000_000], help="batch case: triangle range")
     ap.add_argument("--variant", default="shortstack")
-    ap.add_argument("--mode", default="binned", choices=["binned", "learned"])
+    ap.add_argument("--mode", default="binned", choices=["binned", "learned", "resort"],
+                    help="resort: the reference's --treeType=SAH builder with its own constants "
+                         "(Ct 1, Ci 5, depth 20, leaves below 10, every 5th polygon sampled)")
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--weights", default=os.path.join(ROOT, "hulktracer_b200", "weights", "proposer.bin"))
     ap.add_argument("--exact-max", type=int, default=0, help="exact SAH on nodes of at most this many refs")
@@ -51,13 +53,14 @@ def main():
         return
     sc = scenes.animated_parts()
     W, H = sc.width, sc.height
-    ctx = hk.Context(exact_max=a.exact_max)
+    resort = dict(traverse_cost=1.0, intersect_cost=5.0, max_depth=20, leaf_size=9, sah_sample=5)
+    ctx = hk.Context(exact_max=a.exact_max, **(resort if a.mode == "resort" else {}))
     if a.mode == "learned":
         ctx.mlp_load(a.weights)
     ctx.upload(sc.verts, sc.tris)
     ctx.set_parts(sc.part_of_vertex, sc.part_center.shape[0])
     ctx.transform(scenes.part_matrices(sc, 1))
-    mode = hk.BUILD_LEARNED if a.mode == "learned" else hk.BUILD_BINNED
+    mode = {"learned": hk.BUILD_LEARNED, "resort": hk.BUILD_SAH_RESORT}.get(a.mode, hk.BUILD_BINNED)
     st = ctx.build(mode)
     if a.case == "trace":
         # primary rays in the frame's 8x4-pixel tile order
@@ -69,8 +72,11 @@ def main():
             ctx.trace_device(rays.data_ptr(), W * H, hits.data_ptr(), hk.VARIANTS[a.variant])
         ctx.synchronize()
     elif a.case == "build":
+        ms = []
         for _ in range(a.reps):
             st = ctx.build(mode)
+            ms.append(st["build_ms"])
+        print("build_ms per build: %s" % ", ".join("%.3f" % m for m in ms))
     elif a.case == "breakdown":
         # device time per stage (CUDA events, no graph), median of reps
         import json

@@ -30,7 +30,7 @@ def ratio(oracle, verts, tris, box, exact_max=1024):
 
 
 @pytest.mark.parametrize("which", ["C1", "C2_100k", "C3_frame5", "C3_frame17", "C3_frame42"])
-def test_binned_cost_within_1pct_on_benchmark_scenes(oracle, which):
+def test_exact_cost_within_1pct_on_benchmark_scenes(oracle, which):
     if which == "C1":
         sc = scenes.static_small()
         v = sc.verts
@@ -46,7 +46,7 @@ def test_binned_cost_within_1pct_on_benchmark_scenes(oracle, which):
 
 
 @pytest.mark.parametrize("which", ["cluster4", "cluster5", "random20k"])
-def test_binned_cost_on_soups(oracle, which):
+def test_exact_cost_on_soups(oracle, which):
     if which == "random20k":
         sc = scenes.random_soup(20000, seed=4)
         bound = 1.05
@@ -57,10 +57,10 @@ def test_binned_cost_on_soups(oracle, which):
 
 
 def test_binned_only_cost_recorded(oracle):
-    """Binned everywhere (the default, 32 bins): the rest pose is far cheaper
-    than the reference's tree, a rotated frame about 17% dearer -- the
-    reason exact_max exists."""
+    """Binned everywhere (the default, 32 bins, the headline arm): a rotated
+    frame costs 1.17x the reference's tree -- it does not meet the 1% bar,
+    which is why the exact (exact_max = 1024) and learned arms exist."""
     sc = scenes.animated_parts()
     v = oracle.transform(sc.rest_verts, sc.part_of_vertex, scenes.part_matrices(sc, 5))
     r = ratio(oracle, v, sc.tris, oracle.scene_box(v), exact_max=0)
-    assert 1.0 < r <= 1.25
+    assert 1.15 < r < 1.19, r
