@@ -57,6 +57,14 @@ class TreeStats(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class StreamStats(C.Structure):
+    _fields_ = [("launches", C.c_uint32), ("leaves_loaded", C.c_uint32), ("leaves_evicted", C.c_uint32),
+                ("resident", C.c_uint32), ("bytes_paged", C.c_uint64), ("ms", C.c_float)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class AffInfo(C.Structure):
     _fields_ = [("nv", C.c_uint32), ("nt", C.c_uint32), ("nmeshes", C.c_uint32), ("ndynamic", C.c_uint32),
                 ("ntransforms", C.c_uint32), ("nanimations", C.c_uint32), ("nlights", C.c_uint32),
@@ -151,6 +159,8 @@ def load(path: str = LIB_PATH):
         "hk_batch_destroy": [vp],
         "hk_batch_add_scene": [vp, f32p, u32, u32p, u32, C.POINTER(C.c_uint32)],
         "hk_batch_trace_device": [vp, vp, u32p, u32, C.c_int, vp, f32p],
+        "hk_stream_setup": [vp, u32],
+        "hk_trace_streamed": [vp, f32p, u32, vp, C.POINTER(StreamStats)],
         "hk_aff_open": [C.c_char_p, C.POINTER(C.c_void_p)],
         "hk_aff_close": [vp],
         "hk_aff_get_info": [vp, C.POINTER(AffInfo)],

@@ -11,6 +11,7 @@
 
 #include "hk_build.h"
 #include "hk_resort.h"
+#include "hk_stream.h"
 #include "hk_common.cuh"
 #include "hk_internal.h"
 #include "hk_mlp.h"
@@ -77,6 +78,8 @@ struct hk_ctx {
     hk_tree_stats stats{};
     BuildState build;
     ResortState resort;   // HK_BUILD_SAH_RESORT
+    StreamState ooc;      // out-of-core leaf geometry
+    uint64_t tree_epoch = 0, rec_epoch = 0;   // bumped whenever the tree / the records change
     // ropes of an imported tree (computed on the host when first needed)
     std::vector<uint2> host_nodes;
     DevBuf<uint32_t> imp_ropes;
@@ -246,6 +249,7 @@ hk_status hk_destroy(hk_ctx *c) {
     c->mslot.release(); c->mcount.release();
     build_release(c->build);
     c->resort.release();
+    c->ooc.release();
     c->mlp_params.release(); c->mlp_grads.release(); c->mlp_m.release(); c->mlp_v.release();
     c->mlp_w1p.release(); c->mlp_w2p.release(); c->mlp_w3p.release(); c->mlp_w4p.release(); c->mlp_tcw.release();
     c->rec_X.release(); c->rec_y.release(); c->rec_rows.release();
@@ -370,6 +374,7 @@ static hk_status transform_device(hk_ctx *c) {
     if (!c->box_user) HK_CUDA(c, launch_box_finish(c->box_ord.p, c->box.p, c->stream));
     HK_CUDA(c, launch_precompute(c->verts.p, c->tris.p, c->nt, c->rec.p, c->stream));
     c->rec_valid = true;
+    c->rec_epoch++;
     return HK_OK;
 }
 
@@ -422,6 +427,7 @@ hk_status hk_precompute(hk_ctx *c) {
     HK_CUDA(c, launch_precompute(c->verts.p, c->tris.p, c->nt, c->rec.p, c->stream));
     HK_CUDA(c, cudaStreamSynchronize(c->stream));
     c->rec_valid = true;
+    c->rec_epoch++;
     return HK_OK;
 }
 
@@ -442,6 +448,7 @@ hk_status hk_cache_import(hk_ctx *c, const float *cache16, uint32_t nt) {
     HK_CUDA(c, launch_cache_to_rec(c->cache_tmp.p, c->verts.p, c->tris.p, nt, c->rec.p, c->stream));
     HK_CUDA(c, cudaStreamSynchronize(c->stream));
     c->rec_valid = true;
+    c->rec_epoch++;
     return HK_OK;
 }
 
@@ -513,6 +520,7 @@ hk_status hk_tree_import(hk_ctx *c, const uint32_t *nodes4, uint32_t nn, const u
     c->nn = (uint32_t)out.size();
     c->nr = nr;
     c->tree_valid = true;
+    c->tree_epoch++;
     c->tree_built = false;
     c->host_nodes.swap(out);
     c->imp_ropes_valid = false;
@@ -745,6 +753,7 @@ static hk_status build_enqueue(hk_ctx *c, hk_build_mode mode) {
     }
     // the device tree lives in the builder's output buffers
     c->tree_valid = true;
+    c->tree_epoch++;
     c->tree_built = true;
     c->tree_on_device_counts = true;
     return HK_OK;
@@ -787,6 +796,7 @@ static hk_status build_resort(hk_ctx *c, hk_tree_stats *stats) {
     c->nn = R.nn;
     c->nr = R.nr;
     c->tree_valid = true;
+    c->tree_epoch++;
     c->tree_built = false;
     c->tree_on_device_counts = false;
     c->imp_ropes_valid = true;
@@ -941,6 +951,49 @@ hk_status hk_trace(hk_ctx *c, const float *rays8, uint32_t n, hk_variant v, hk_h
     HK_CUDA(c, cudaMemcpyAsync(c->rays.p, rays8, (size_t)n * 32, cudaMemcpyHostToDevice, c->stream));
     hk_status s = trace_enqueue(c, c->rays.p, n, nullptr, v, c->hits.p);
     if (s != HK_OK) return s;
+    HK_CUDA(c, cudaMemcpyAsync(hits, c->hits.p, (size_t)n * 8, cudaMemcpyDeviceToHost, c->stream));
+    HK_CUDA(c, cudaStreamSynchronize(c->stream));
+    return check_err_word(c);
+}
+
+hk_status hk_stream_setup(hk_ctx *c, uint32_t pool_tris) {
+    if (!c || pool_tris == 0) return HK_E_ILLEGAL_INPUT;
+    if (!c->tree_valid || !c->rec_valid) return fail(c, HK_E_STATE, "streaming needs a tree and triangle records");
+    cudaSetDevice(c->device);
+    hk_status s = sync_tree_sizes(c);
+    if (s != HK_OK) return s;
+    std::string err;
+    s = stream_setup(c->ooc, tree_nodes(c), c->nn, tree_refs(c), c->nr, c->rec.p, pool_tris, c->stream, &err);
+    if (s != HK_OK) return fail(c, s, err.c_str());
+    c->ooc.tree_epoch = c->tree_epoch;
+    c->ooc.rec_epoch = c->rec_epoch;
+    return HK_OK;
+}
+
+hk_status hk_trace_streamed(hk_ctx *c, const float *rays8, uint32_t n, hk_hit *hits, hk_stream_stats *stats) {
+    if (!c || (n && (!rays8 || !hits))) return HK_E_ILLEGAL_INPUT;
+    if (!c->ooc.ready) return fail(c, HK_E_STATE, "hk_stream_setup first");
+    if (c->ooc.tree_epoch != c->tree_epoch || c->ooc.rec_epoch != c->rec_epoch)
+        return fail(c, HK_E_STATE, "the tree or the records changed since hk_stream_setup");
+    for (size_t i = 0; i < n; i++)
+        if (rays8[8 * i + 3] != 0.0f || rays8[8 * i + 7] != 0.0f)
+            return fail(c, HK_E_ILLEGAL_INPUT, "ray w lanes must be 0");
+    cudaSetDevice(c->device);
+    HK_CUDA(c, c->rays.ensure(2 * (size_t)std::max<uint32_t>(n, 1)));
+    HK_CUDA(c, c->hits.ensure(std::max<uint32_t>(n, 1)));
+    HK_CUDA(c, cudaMemcpyAsync(c->rays.p, rays8, (size_t)n * 32, cudaMemcpyHostToDevice, c->stream));
+    StreamTraceArgs a;
+    a.nodes = tree_nodes(c);
+    a.refs = tree_refs(c);
+    a.rays = c->rays.p;
+    a.hits = c->hits.p;
+    a.n = n;
+    a.box = c->box.p;
+    a.max_steps = c->cfg.max_steps ? c->cfg.max_steps : (1u << 26);
+    a.err = c->errw.p;
+    std::string err;
+    hk_status s = stream_trace(c->ooc, a, c->stream, stats, &err);
+    if (s != HK_OK) return fail(c, s, err.c_str());
     HK_CUDA(c, cudaMemcpyAsync(hits, c->hits.p, (size_t)n * 8, cudaMemcpyDeviceToHost, c->stream));
     HK_CUDA(c, cudaStreamSynchronize(c->stream));
     return check_err_word(c);
@@ -1130,6 +1183,7 @@ static hk_status frame_enqueue(hk_ctx *c, bool animated, uint32_t nl, uint32_t w
     } else if (!c->rec_valid) {
         HK_CUDA(c, launch_precompute(c->verts.p, c->tris.p, c->nt, c->rec.p, c->stream));
         c->rec_valid = true;
+    c->rec_epoch++;
     }
     s = build_enqueue(c, mode);
     if (s != HK_OK) return s;
@@ -1197,6 +1251,7 @@ hk_status hk_frame(hk_ctx *c, const float *mats12, const float *cam16, const flo
         }
         HK_CUDA(c, cudaGraphLaunch(c->graph_exec, c->stream));
         c->tree_valid = true;
+    c->tree_epoch++;
         c->tree_built = true;
         c->tree_on_device_counts = true;
     }

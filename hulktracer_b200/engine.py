@@ -277,6 +277,19 @@ class Context:
         self._check(self.L.hk_trace(self.h, ptr(r), r.shape[0], int(variant), ptr(hits)))
         return hits
 
+    def stream_setup(self, pool_tris: int):
+        """Out-of-core leaf geometry: snapshot the tree's leaf records into pinned
+        host memory and empty a device pool of pool_tris triangle records."""
+        self._check(self.L.hk_stream_setup(self.h, int(pool_tris)))
+
+    def trace_streamed(self, rays):
+        """kd-restart with leaves paged into the pool on demand: (hits, stats)."""
+        r = _f32(rays).reshape(-1, 8)
+        hits = np.zeros(r.shape[0], _lib.HIT_DTYPE)
+        st = _lib.StreamStats()
+        self._check(self.L.hk_trace_streamed(self.h, ptr(r), r.shape[0], ptr(hits), C.byref(st)))
+        return hits, st.as_dict()
+
     def trace_device(self, d_rays: int, n: int, d_hits: int, variant=_lib.SHORTSTACK):
         self._check(self.L.hk_trace_device(self.h, C.c_void_p(d_rays), n, int(variant), C.c_void_p(d_hits)))
 

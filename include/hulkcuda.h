@@ -425,6 +425,32 @@ hk_status hk_mlp_train(hk_ctx *ctx, uint32_t epochs, uint32_t batch, float lr, u
 hk_status hk_set_proposal_log(hk_ctx *ctx, int enable);
 hk_status hk_get_proposal_log(hk_ctx *ctx, int32_t *bins8, uint32_t cap_nodes, uint32_t *nn);
 
+/* ---- out-of-core leaf geometry ----
+ * The reference's leaf residency (GPUTrace_stackless.cl:6-120 with
+ * GLVisitorGPUTrace::launchTraceIterations, GLVisitorGPUTrace.cpp:412-502):
+ * a kd-restart traversal that tests a leaf only when its triangles are
+ * resident in a device pool; otherwise it requests the leaf, keeps its resume
+ * point and stops; the leaves requested by a launch are paged in (the oldest
+ * resident leaves evicted first, at most half the pool per round except for
+ * the round's first leaf) and the traversal relaunched until no ray waits.
+ * The leaves' records stay in pinned host memory and the device copies them
+ * itself. Hits equal HK_TRACE_RESTART's for any pool size that holds the
+ * largest leaf. hk_stream_setup snapshots the current tree and triangle
+ * records (call it again after a rebuild or hk_precompute; hk_trace_streamed
+ * returns HK_E_STATE until then) and empties the pool; the pool stays warm
+ * across hk_trace_streamed calls. A pool smaller than a requested leaf, or
+ * rounds that stop making progress, give HK_E_CAPACITY. */
+typedef struct hk_stream_stats {
+    uint32_t launches;        /* traversal launches (rounds) */
+    uint32_t leaves_loaded;   /* page-ins */
+    uint32_t leaves_evicted;
+    uint32_t resident;        /* leaves resident at the end */
+    uint64_t bytes_paged;     /* triangle-record bytes copied from host memory */
+    float ms;                 /* device time of the whole call */
+} hk_stream_stats;
+hk_status hk_stream_setup(hk_ctx *ctx, uint32_t pool_tris);
+hk_status hk_trace_streamed(hk_ctx *ctx, const float *rays8, uint32_t n, hk_hit *hits, hk_stream_stats *stats);
+
 /* ---- autotuner (no reference counterpart) ----
  * Times the persistent traversal on n device rays of the current scene for
  * every candidate: traversal layout (ropes: compact nodes + per-node cells and
