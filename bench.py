@@ -446,7 +446,8 @@ def build_roofline(compare, mode):
     return {"bound": "hbm", "achieved": arm["build_gbs"], "peak": peak, "unit": "GB/s",
             "frac": arm["build_gbs"] / peak, "peak_source": src, "bytes_per_build": arm["build_bytes"],
             "build_ms": arm["build_ms"],
-            "bytes": "sum over levels of references x 36 B + nodes x 8 B + leaf references x 4 B"}
+            "bytes": "sum over levels of references x 36 B + deferred-subtree root references x 28 B + "
+                     "nodes x 8 B + leaf references x 4 B"}
 
 
 def reference_tree_cost(hk, rt, device):
@@ -534,7 +535,11 @@ def compare_arms(args, sc, device, ref_cost, variant, tuned):
             # (4 B) and clipped box (24 B) read and its next-level slot (8 B)
             # written; the tree's nodes (8 B) and leaf references (4 B) written
             _, lrefs = ctx.level_counts()
-            build_bytes = int(lrefs.astype(np.int64).sum()) * 36 + st["nodes"] * 8 + st["refs"] * 4
+            # deferred subtrees: each root's references read once (index and
+            # box, 28 B) by the warp that builds the subtree in registers
+            sub = ctx.subtree_counts()
+            build_bytes = (int(lrefs.astype(np.int64).sum()) * 36 + sub["root_refs"] * 28 + st["nodes"] * 8 +
+                           st["refs"] * 4)
         ms = t_frame / len(frames)
         out[name] = {"build": "%s%s" % (mode_s, ", exact SAH on nodes <= %d refs" % exact_max if exact_max else ""),
                      "ms_per_frame": ms, "mrays_s": rays / (t_frame / 1000.0) / 1e6,

@@ -37,7 +37,7 @@ class Config(C.Structure):
                 ("short_stack", C.c_uint32), ("block_size", C.c_uint32), ("blocks_per_sm", C.c_uint32),
                 ("max_refs", C.c_uint32), ("topk", C.c_uint32), ("fallback_ratio", C.c_float),
                 ("exact_max", C.c_uint32), ("spin_limit", C.c_uint32), ("max_steps", C.c_uint32),
-                ("sah_sample", C.c_uint32)]
+                ("sah_sample", C.c_uint32), ("subtree_max", C.c_uint32)]
 
 
 class TuneResult(C.Structure):
@@ -128,6 +128,8 @@ def load(path: str = LIB_PATH):
         "hk_tree_stats_get": [vp, C.POINTER(TreeStats)],
         "hk_tree_cost": [vp, C.c_double, C.c_double, C.POINTER(C.c_double)],
         "hk_build_level_counts": [vp, u32p, u32p, u32, C.POINTER(C.c_uint32)],
+        "hk_build_subtree_counts": [vp, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32),
+                                    C.POINTER(C.c_uint32)],
         "hk_trace": [vp, f32p, u32, C.c_int, vp],
         "hk_trace_device": [vp, vp, u32, C.c_int, vp],
         "hk_set_counting": [vp, C.c_int],

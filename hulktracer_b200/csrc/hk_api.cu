@@ -179,6 +179,7 @@ hk_status hk_config_default(hk_config *cfg) {
     cfg->fallback_ratio = 1.0f;
     cfg->exact_max = 0;
     cfg->sah_sample = 5;
+    cfg->subtree_max = 32;
     return HK_OK;
 }
 
@@ -190,6 +191,7 @@ static hk_status validate_config(const hk_config *c) {
     if (!(c->intersect_cost > 0) || !(c->traverse_cost >= 0)) return HK_E_ILLEGAL_INPUT;
     if (c->topk < 1 || c->topk > 8 || !(c->fallback_ratio >= 0)) return HK_E_ILLEGAL_INPUT;
     if (c->exact_max != 0 && (c->exact_max < 32 || c->exact_max > 1024)) return HK_E_ILLEGAL_INPUT;
+    if (c->subtree_max > 32) return HK_E_ILLEGAL_INPUT;
     return HK_OK;
 }
 
@@ -631,6 +633,24 @@ hk_status hk_build_level_counts(hk_ctx *c, uint32_t *nodes, uint32_t *refs, uint
     return HK_OK;
 }
 
+hk_status hk_build_subtree_counts(hk_ctx *c, uint32_t *roots, uint32_t *root_refs, uint32_t *nodes,
+                                  uint32_t *leaf_refs) {
+    if (!c) return HK_E_ILLEGAL_INPUT;
+    if (!c->tree_valid || !c->tree_built) return fail(c, HK_E_STATE, "no tree from hk_build's level-synchronous builder");
+    cudaSetDevice(c->device);
+    hk_status s = sync_tree_sizes(c);
+    if (s != HK_OK) return s;
+    BuildCounters bc;
+    HK_CUDA(c, cudaMemcpyAsync(&bc, c->build.ctr, sizeof bc, cudaMemcpyDeviceToHost, c->stream));
+    HK_CUDA(c, cudaStreamSynchronize(c->stream));
+    const LevelCounters &fin = bc.lvl[c->build.last_level];
+    if (roots) *roots = fin.defer_nodes_total;
+    if (root_refs) *root_refs = fin.defer_refs_total;
+    if (nodes) *nodes = bc.sub_fits ? bc.sub_nodes : 0u;
+    if (leaf_refs) *leaf_refs = bc.sub_fits ? bc.sub_refs : 0u;
+    return HK_OK;
+}
+
 hk_status hk_set_debug_flags(hk_ctx *c, uint32_t flags) {
     if (!c || (flags & ~1u)) return HK_E_ILLEGAL_INPUT;
     c->debug_flags = flags;
@@ -734,6 +754,7 @@ static BuildParams build_params(hk_ctx *c, hk_build_mode mode) {
     p.prop_log = c->prop_log ? 1 : 0;
     p.spin_limit = c->cfg.spin_limit;
     p.debug_flags = c->debug_flags;
+    p.defer = c->cfg.subtree_max;
     c->build.learn = &c->learn;
     return p;
 }

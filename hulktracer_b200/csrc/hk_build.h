@@ -24,6 +24,7 @@ struct BuildParams {
     int prop_log = 0;           // learned mode: log every proposer row's proposed bins by compact node
     uint32_t spin_limit = 0;    // polls before a bounded wait gives up (0: the default, 4M)
     uint32_t debug_flags = 0;   // test aid, bit 0: plan tile 0 of level 1 withholds its done flag
+    uint32_t defer = 32;        // nodes of 2..defer references: subtrees built after the levels (0: none)
 };
 
 // learned-proposer buffers owned by the context (device pointers)
@@ -54,15 +55,18 @@ struct LevelCounters {
     uint32_t refs;              // their references
     uint32_t nodes_total;       // compact nodes written before this level
     uint32_t leafrefs_total;    // leaf references written before this level
+    uint32_t defer_refs_total;  // references of the deferred subtree roots recorded before this level
+    uint32_t defer_nodes_total; // deferred subtree roots recorded before this level
     uint32_t stop;              // the level stops splitting (capacity)
     uint32_t n_large;           // large nodes (chunked histograms)
     uint32_t n_chunks;          // histogram chunks
     uint32_t n_medium;          // exact-SAH nodes of 33..exact_max refs (one CTA each)
     uint32_t n_learn;           // learned mode: proposer rows of the level (nodes of 33..1024 refs)
     // tallies of the level's decisions (the capacity guard's inputs)
-    uint32_t t_leafrefs, t_leafnodes, t_splits, t_next, t_childrefs;
-    // tile tickets of the single-pass scans
-    uint32_t plan_ticket, ref_ticket;
+    uint32_t t_leafrefs, t_leafnodes, t_splits, t_next, t_childrefs, t_deferrefs, t_defernodes;
+    // tile tickets of the single-pass scans; level 0's sub_ticket: the
+    // subtree tickets of the deferred roots
+    uint32_t plan_ticket, ref_ticket, sub_ticket;
 };
 
 // device scalars of one build (one struct in device memory)
@@ -72,6 +76,15 @@ struct BuildCounters {
     uint32_t capacity_hit;
     uint32_t learned_nodes;
     uint32_t fallback_nodes;
+    // deferred subtrees (built after the levels, one warp each)
+    uint32_t sub_leaves;        // leaves of the subtrees (empty cells excluded)
+    uint32_t sub_depth;         // deepest subtree node
+    uint32_t sub_overflow;      // a scratch arena ran out (the roots then stay leaves)
+    uint32_t sc_node_ctr, sc_ref_ctr;   // scratch slots handed out (in chunks)
+    uint32_t sub_ticket;        // tile tickets of the subtree-size scan
+    uint32_t sub_fits;          // 1: the subtrees are placed; 0: the roots stay leaves
+    uint32_t sub_n0, sub_r0;    // nodes / leaf references of the levels (where the subtrees start)
+    uint32_t sub_nodes, sub_refs;   // the subtrees' nodes and leaf references
     uint32_t pad[3];
     LevelCounters lvl[kMaxLevels];
 };
@@ -84,6 +97,7 @@ struct BuildOutputs {
 struct BuildState {
     BuildParams p{};
     uint32_t nt = 0, cap_refs = 0, cap_nodes = 0, cap_level = 0, cap_large = 0, cap_chunks = 0, cap_medium = 0;
+    uint32_t alloc_depth = 0;   // max_depth the subtree scratch was sized for
     int sm_count = 148;
     bool active = false;        // a built tree is the current tree
     uint32_t last_level = 0;    // lvl[] index holding the final totals
@@ -117,6 +131,7 @@ struct BuildState {
     // second stream: large-node histograms run beside the small-node work
     cudaStream_t aux = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+
     BuildCounters *ctr = nullptr;
     uint32_t *err = nullptr;
     // output
@@ -124,6 +139,24 @@ struct BuildState {
     uint32_t *out_refs = nullptr;
     uint32_t *out_ropes = nullptr;               // 6 per node: -x,+x,-y,+y,-z,+z (0xffffffff = none)
     float4 *out_cbox = nullptr;                  // 2 per node: cell min, max
+    // deferred subtree roots (nodes of at most 32 references): their records
+    // (compact index, reference offset, count, depth), cells and references
+    uint32_t cap_defer = 0;
+    uint4 *d_root = nullptr;
+    float4 *d_lo = nullptr, *d_hi = nullptr;
+    uint32_t *defer_refs = nullptr;
+    // subtree scratch: node slots (subtree, local index), their entries, cells
+    // and ropes; reference slots (subtree, local index, triangle); per subtree
+    // its sizes, root entry and place
+    uint32_t cap_sc_nodes = 0, cap_sc_refs = 0;
+    uint2 *sc_key = nullptr, *sc_node = nullptr;
+    float4 *sc_cbox = nullptr;
+    uint32_t *sc_rope = nullptr;
+    uint4 *sc_ref = nullptr;
+    uint2 *st_cnt = nullptr, *st_root = nullptr, *st_base = nullptr;
+    uint32_t sub_tiles = 0;
+    uint32_t *sub_flags = nullptr;
+    uint2 *sub_agg = nullptr, *sub_incl = nullptr;
     // learned proposer: per-level rows (nodes of 33..1024 references), their
     // node slots, binned decisions and features
     uint32_t cap_learn = 0;

@@ -226,6 +226,13 @@ class Context:
         k = min(n.value, cap)
         return nodes[:k].copy(), refs[:k].copy()
 
+    def subtree_counts(self):
+        """The last build's deferred subtrees: roots, the references they hold,
+        and the nodes and leaf references the subtrees added."""
+        v = [C.c_uint32() for _ in range(4)]
+        self._check(self.L.hk_build_subtree_counts(self.h, *[C.byref(x) for x in v]))
+        return dict(zip(("roots", "root_refs", "nodes", "leaf_refs"), (x.value for x in v)))
+
     def export_tree(self):
         nn, nr = C.c_uint32(), C.c_uint32()
         self._check(self.L.hk_tree_export(self.h, None, 0, None, 0, C.byref(nn), C.byref(nr)))

@@ -4,12 +4,15 @@
     python -m hulktracer_b200.profile_case --case build
     python -m hulktracer_b200.profile_case --case frame
     python -m hulktracer_b200.profile_case --case aff --aff scene.aff --frames 60
+    python -m hulktracer_b200.profile_case --case stream --pools 1 0.25 0.05 0.01
 
 Each case sets up the animated 64-part scene (~200k triangles, 1280x720), does
 its warm-up work first and then launches the kernel of interest a few times, so
 an ncu command can select it with -k / -s / -c. The aff case instead renders an
 AFF (BART) scene frame by frame on the reference's fixed-tick clock and prints
-device times per frame.
+device times per frame. The stream case traces the frame's primary rays with
+leaves paged in from host memory (hk_trace_streamed) for pools of the given
+fractions of the tree's leaf records, beside the resident kd-restart traversal.
 """
 from __future__ import annotations
 
@@ -30,7 +33,10 @@ def main():
     from hulktracer_b200 import scenes
 
     ap = argparse.ArgumentParser()
-    ap.add_argument("--case", default="trace", choices=["trace", "build", "frame", "breakdown", "batch", "aff"])
+    ap.add_argument("--case", default="trace", choices=["trace", "build", "frame", "breakdown", "batch", "aff",
+                                                         "stream"])
+    ap.add_argument("--pools", type=float, nargs="+", default=[1.0, 0.25, 0.05, 0.01],
+                    help="stream case: pool sizes as fractions of the leaf records")
     ap.add_argument("--aff", help="aff case: the scene file")
     ap.add_argument("--frames", type=int, default=60, help="aff case: frames timed")
     ap.add_argument("--size", type=int, nargs=2, help="aff case: image size (default: the file's resolution)")
@@ -111,6 +117,40 @@ def main():
         p_, s_ = ctx.ray_counts()
         res["rays"] = {"primary": p_, "shadow": s_}
         res["tree"] = ctx.stats()
+        print(json.dumps(res))
+    elif a.case == "stream":
+        import json
+        rays_h = ctx.camera_rays(sc.camera, W, H)
+        rays = torch.from_numpy(rays_h).cuda()
+        hits = torch.zeros(2 * W * H, dtype=torch.int32, device="cuda")
+        res = {"rays": W * H}
+        stream = torch.cuda.Stream()
+        ctx.set_stream(stream.cuda_stream)
+        for name in ("restart", "restart_early"):
+            ts = []
+            for _ in range(a.reps + 1):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                ctx.trace_device(rays.data_ptr(), W * H, hits.data_ptr(), hk.VARIANTS[name])
+                e1.record(stream)
+                stream.synchronize()
+                ts.append(e0.elapsed_time(e1))
+            res[name + "_ms"] = sorted(ts[1:])[len(ts[1:]) // 2]
+        ctx.set_stream(None)
+        cn = ctx.export_compact()[0]
+        leaves = cn[(cn[:, 0] & 3) == 3]
+        total = int(leaves[:, 1].sum())
+        res["leaf_records"] = total
+        ref = ctx.trace(rays_h, hk.RESTART)
+        for frac in a.pools:
+            pool = max(int(leaves[:, 1].max()), int(total * frac))
+            ctx.stream_setup(pool)
+            h1, cold = ctx.trace_streamed(rays_h)
+            _, warm = ctx.trace_streamed(rays_h)
+            assert np.array_equal(h1["tri"], ref["tri"])
+            cold["pool_records"] = pool
+            cold["paged_gbs"] = cold["bytes_paged"] / (cold["ms"] * 1e6) if cold["ms"] > 0 else 0.0
+            res["pool_%g" % frac] = {"cold": cold, "warm": warm}
         print(json.dumps(res))
     else:
         out = torch.zeros(W * H, dtype=torch.int32, device="cuda")

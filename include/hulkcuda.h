@@ -131,6 +131,11 @@ typedef struct hk_config {
     uint32_t sah_sample;      /* HK_BUILD_SAH_RESORT: every sah_sample-th polygon of a
                                  node makes candidates (c_reductionFactor,
                                  KDTreeCPU.hpp; 0 = 5) */
+    uint32_t subtree_max;     /* HK_BUILD_BINNED / LEARNED: a node of 2..subtree_max
+                                 references is not split by the level-synchronous
+                                 passes; one warp builds its whole subtree after the
+                                 last level (same splits, nodes numbered after the
+                                 levels'). 0 = none, at most 32; default 32 */
 } hk_config;
 
 typedef struct hk_tree_stats {
@@ -220,6 +225,13 @@ hk_status hk_tree_stats_get(hk_ctx *ctx, hk_tree_stats *stats);
  * nodes and the references they hold (what the builder reads and writes per
  * level); *nlevels levels, the first min(cap, *nlevels) written. */
 hk_status hk_build_level_counts(hk_ctx *ctx, uint32_t *nodes, uint32_t *refs, uint32_t cap, uint32_t *nlevels);
+/* The same build's deferred subtrees (nodes of 2..32 references whose
+ * subtrees one warp each builds after the levels, numbered after the levels'
+ * nodes): their roots and the references the roots hold, and the nodes and
+ * leaf references the subtrees added (0, 0 when they did not fit and the
+ * roots stayed leaves). Any pointer may be null. */
+hk_status hk_build_subtree_counts(hk_ctx *ctx, uint32_t *roots, uint32_t *root_refs, uint32_t *nodes,
+                                  uint32_t *leaf_refs);
 /* SAH cost of the current tree (no reference counterpart; the tree-quality
  * measure of both builders): sum over junctions of ct * A(n) / A(root) plus
  * over leaves of ci * |refs(n)| * A(n) / A(root), A the full surface area of the

@@ -1445,6 +1445,268 @@ static float surf(const float *b) {
     return 2.0f * (sx * sy + sz * sy + sx * sz);
 }
 
+typedef struct {
+    const hko_binned_params *p;
+    const float *tb;            /* per triangle: min xyz, max xyz */
+    uint32_t *hlo, *hhi, *hon;  /* bins counters */
+    float *pl;                  /* bins + 1 planes */
+} bin_ctx;
+
+/* the split of one decidable node whose references are refs[n->start ..
+ * n->start + n->count): the axis (-1: leaf), its plane and the below / above
+ * counts of the chosen plane */
+static int32_t decide_binned(bin_ctx *c, const bnode_t *n, const uint32_t *refs, float *plane_out,
+                             uint32_t *nb_out, uint32_t *na_out) {
+    const hko_binned_params *p = c->p;
+    const float *tb = c->tb;
+    const uint32_t B = p->bins;
+    uint32_t *hlo = c->hlo, *hhi = c->hhi, *hon = c->hon;
+    float *pl = c->pl;
+    int32_t axis = -1;
+    float plane = 0.0f;
+    float A = surf(n->box);
+    float best = INFINITY;
+    uint32_t bnb = 0, bna = 0;
+    if (n->count <= (p->learned ? 32u : p->exact_max)) {
+        /* small node: every clipped reference bound is a candidate
+         * (+0.0f makes a -0 bound the plane +0) */
+        for (uint32_t a = 0; a < 3; a++) {
+            float lo_b = n->box[a], hi_b = n->box[4 + a];
+            if (!(hi_b - lo_b > 0)) continue;
+            for (uint32_t q = 0; q < 2 * n->count; q++) {
+                const float *tq = tb + 6 * (size_t)refs[n->start + q / 2];
+                float pk = ((q & 1) ? mn(tq[3 + a], hi_b) : mx(tq[a], lo_b)) + 0.0f;
+                if (!(pk > lo_b && pk < hi_b)) continue;
+                uint32_t nb = 0, na = 0;
+                for (uint32_t r = 0; r < n->count; r++) {
+                    const float *t6 = tb + 6 * (size_t)refs[n->start + r];
+                    float lo = mx(t6[a], lo_b), hi = mn(t6[3 + a], hi_b);
+                    int on = lo == hi && lo == pk;
+                    nb += (lo < pk || on) ? 1u : 0u;
+                    na += (hi > pk || on) ? 1u : 0u;
+                }
+                float bb[8], ba[8];
+                memcpy(bb, n->box, 32);
+                memcpy(ba, n->box, 32);
+                bb[4 + a] = pk;
+                ba[a] = pk;
+                float cost = p->ct + p->ci * ((surf(bb) * (float)nb + surf(ba) * (float)na) / A);
+                /* first minimum in (axis, plane) order */
+                if (cost < best || (cost == best && (int32_t)a == axis && pk < plane)) {
+                    best = cost;
+                    axis = (int32_t)a;
+                    plane = pk;
+                    bnb = nb;
+                    bna = na;
+                }
+            }
+        }
+    } else
+    for (uint32_t a = 0; a < 3; a++) {
+        float lo_b = n->box[a], hi_b = n->box[4 + a];
+        float ext = hi_b - lo_b;
+        if (!(ext > 0)) continue;
+        float inv = (float)B / ext;
+        for (uint32_t k = 1; k < B; k++) pl[k] = bplane(n->box, a, k, B);
+        memset(hlo, 0, B * 4);
+        memset(hhi, 0, B * 4);
+        memset(hon, 0, B * 4);
+        for (uint32_t r = 0; r < n->count; r++) {
+            const float *t6 = tb + 6 * (size_t)refs[n->start + r];
+            float lo = mx(t6[a], lo_b), hi = mn(t6[3 + a], hi_b);
+            int b = (int)((lo - lo_b) * inv);
+            b = b < 0 ? 0 : (b > (int)B - 1 ? (int)B - 1 : b);
+            while (b > 0 && lo < pl[b]) b--;
+            while (b < (int)B - 1 && lo >= pl[b + 1]) b++;
+            int c2 = (int)((hi - lo_b) * inv);
+            c2 = c2 < 0 ? 0 : (c2 > (int)B - 1 ? (int)B - 1 : c2);
+            while (c2 > 0 && hi <= pl[c2]) c2--;
+            while (c2 < (int)B - 1 && hi > pl[c2 + 1]) c2++;
+            hlo[b]++;
+            hhi[c2]++;
+            if (lo == hi && b >= 1 && lo == pl[b]) hon[b]++;
+        }
+        uint32_t below = 0, above = n->count;
+        for (uint32_t k = 1; k < B; k++) {
+            below += hlo[k - 1];
+            above -= hhi[k - 1];
+            float pk = pl[k];
+            if (!(pk > lo_b && pk < hi_b)) continue;
+            if (k < B - 1 && !(pk < pl[k + 1])) continue;
+            uint32_t nb = below + hon[k], na = above + hon[k];
+            float bb[8], ba[8];
+            memcpy(bb, n->box, 32);
+            memcpy(ba, n->box, 32);
+            bb[4 + a] = pk;
+            ba[a] = pk;
+            float cost = p->ct + p->ci * ((surf(bb) * (float)nb + surf(ba) * (float)na) / A);
+            if (cost < best) {
+                best = cost;
+                axis = (int32_t)a;
+                plane = pk;
+                bnb = nb;
+                bna = na;
+            }
+        }
+    }
+    if (p->learned && n->count > 32 && n->count <= 1024 && p->proposals) {
+        const int32_t *prop = p->proposals + 8 * (size_t)n->cidx;
+        uint32_t K = p->topk < 8 ? (p->topk ? p->topk : 1) : 8;
+        uint32_t cap = 1;
+        while (2u * cap * 3u * K <= 2048u) cap *= 2u;
+        float rbest = INFINITY, rpk = 0.0f;
+        int32_t rax = 3;
+        uint32_t rnb = 0, rna = 0;
+        for (uint32_t i = 0; i < 8 && prop[i] >= 0; i++) {
+            uint32_t a = (uint32_t)prop[i] / 32u, b = (uint32_t)prop[i] % 32u;
+            float lo_b = n->box[a], hi_b = n->box[4 + a];
+            float P0 = b == 0 ? lo_b : bplane(n->box, a, b, 32);
+            float P1 = b == 31 ? hi_b : bplane(n->box, a, b + 1, 32);
+            uint32_t nl = 0, nh = 0, nf = 0;
+            for (uint32_t r = 0; r < n->count; r++) {
+                const float *t6 = tb + 6 * (size_t)refs[n->start + r];
+                float lo = mx(t6[a], lo_b), hi = mn(t6[3 + a], hi_b);
+                int inl = P0 <= lo && lo <= P1, inh = P0 <= hi && hi <= P1;
+                nl += inl;
+                nh += inh;
+                nf += inl && lo == hi;
+            }
+            if (nl > cap || nh > cap || nf > cap) continue;
+            for (uint32_t q = 0; q < 2 * n->count; q++) {
+                const float *tq = tb + 6 * (size_t)refs[n->start + q / 2];
+                float v = (q & 1) ? mn(tq[3 + a], hi_b) : mx(tq[a], lo_b);
+                if (!(P0 <= v && v <= P1)) continue;
+                if (!(v > lo_b && v < hi_b)) continue;
+                float pk = v + 0.0f;
+                uint32_t nb = 0, na = 0;
+                for (uint32_t r = 0; r < n->count; r++) {
+                    const float *t6 = tb + 6 * (size_t)refs[n->start + r];
+                    float lo = mx(t6[a], lo_b), hi = mn(t6[3 + a], hi_b);
+                    int on = lo == hi && lo == pk;
+                    nb += (lo < pk || on) ? 1u : 0u;
+                    na += (hi > pk || on) ? 1u : 0u;
+                }
+                float bb[8], ba[8];
+                memcpy(bb, n->box, 32);
+                memcpy(ba, n->box, 32);
+                bb[4 + a] = pk;
+                ba[a] = pk;
+                float cost = p->ct + p->ci * ((surf(bb) * (float)nb + surf(ba) * (float)na) / A);
+                if (cost < rbest || (cost == rbest && ((int32_t)a < rax || ((int32_t)a == rax && pk < rpk)))) {
+                    rbest = cost;
+                    rax = (int32_t)a;
+                    rpk = pk;
+                    rnb = nb;
+                    rna = na;
+                }
+            }
+        }
+        if (rbest < INFINITY && rbest <= p->fallback_ratio * best) {
+            best = rbest;
+            axis = rax;
+            plane = rpk;
+            bnb = rnb;
+            bna = rna;
+        }
+    }
+    if (axis >= 0 && !(best < p->ci * (float)n->count)) axis = -1;
+    *plane_out = plane;
+    *nb_out = bnb;
+    *na_out = bna;
+    return axis;
+}
+
+/* the stable partition of a split node's references: below ones to
+ * out[0 .. *nb), above ones after them (*na) */
+static void partition_refs(const float *tb, const bnode_t *n, const uint32_t *refs, uint32_t a, float pk,
+                           uint32_t *out, uint32_t *nb, uint32_t *na) {
+    uint32_t k = 0;
+    for (uint32_t r = 0; r < n->count; r++) {
+        uint32_t tri = refs[n->start + r];
+        const float *t6 = tb + 6 * (size_t)tri;
+        float lo = mx(t6[a], n->box[a]), hi = mn(t6[3 + a], n->box[4 + a]);
+        if (lo < pk || (lo == hi && lo == pk)) out[k++] = tri;
+    }
+    *nb = k;
+    for (uint32_t r = 0; r < n->count; r++) {
+        uint32_t tri = refs[n->start + r];
+        const float *t6 = tb + 6 * (size_t)tri;
+        float lo = mx(t6[a], n->box[a]), hi = mn(t6[3 + a], n->box[4 + a]);
+        if (hi > pk || (lo == hi && lo == pk)) out[k++] = tri;
+    }
+    *na = k - *nb;
+}
+
+/* One deferred subtree, depth first (the CUDA builder's k_subtree): the node
+ * on top of the stack is decided; a leaf appends its references; a split
+ * takes the next pair of node indices (below, above), pushes the above child
+ * and then the below child (so the below child is taken next); an empty
+ * child is an empty leaf. Returns 0, or -1 when out of memory. */
+typedef struct {
+    bnode_t n;
+    uint32_t *refs;   /* the node's references (n.start = 0) */
+} snode_t;
+
+static int expand_subtree(bin_ctx *c, uvec *cn, uvec *leafrefs, const bnode_t *root, const uint32_t *root_refs) {
+    const hko_binned_params *p = c->p;
+    size_t cap = 2u * (p->max_depth + 2u), sp = 0;
+    snode_t *st = (snode_t *)malloc(cap * sizeof(snode_t));
+    if (!st) return -1;
+    st[0].n = *root;
+    st[0].n.start = 0;
+    st[0].refs = (uint32_t *)malloc((root->count ? root->count : 1) * sizeof(uint32_t));
+    memcpy(st[0].refs, root_refs, root->count * sizeof(uint32_t));
+    sp = 1;
+    while (sp > 0) {
+        snode_t e = st[--sp];
+        bnode_t *n = &e.n;
+        float pk = 0.0f;
+        uint32_t nb = 0, na = 0;
+        int32_t a = -1;
+        if (n->count > p->leaf_size && n->depth < p->max_depth) a = decide_binned(c, n, e.refs, &pk, &nb, &na);
+        if (a < 0) {
+            cn->a[2 * n->cidx] = ((uint32_t)leafrefs->n << 2) | CLEAF;
+            cn->a[2 * n->cidx + 1] = n->count;
+            for (uint32_t r = 0; r < n->count; r++) uv_push(leafrefs, e.refs[r]);
+            free(e.refs);
+            continue;
+        }
+        uint32_t pair = (uint32_t)(cn->n / 2);
+        for (int k = 0; k < 4; k++) uv_push(cn, 0);
+        cn->a[2 * n->cidx] = (pair << 2) | (uint32_t)a;
+        memcpy(&cn->a[2 * n->cidx + 1], &pk, 4);
+        uint32_t *part = (uint32_t *)malloc((n->count ? 2 * n->count : 1) * sizeof(uint32_t));
+        uint32_t cb = 0, ca = 0;
+        partition_refs(c->tb, n, e.refs, (uint32_t)a, pk, part, &cb, &ca);
+        for (int ch = 1; ch >= 0; ch--) {
+            uint32_t cnt2 = ch ? ca : cb;
+            uint32_t idx = pair + (uint32_t)ch;
+            if (cnt2 == 0) {
+                cn->a[2 * idx] = CLEAF;
+                cn->a[2 * idx + 1] = 0;
+                continue;
+            }
+            if (sp == cap) {
+                cap *= 2;
+                st = (snode_t *)realloc(st, cap * sizeof(snode_t));
+            }
+            snode_t *d = &st[sp++];
+            memcpy(d->n.box, n->box, 32);
+            if (ch == 0) d->n.box[4 + a] = pk; else d->n.box[a] = pk;
+            d->n.start = 0;
+            d->n.count = cnt2;
+            d->n.depth = n->depth + 1;
+            d->n.cidx = idx;
+            d->refs = (uint32_t *)malloc(cnt2 * sizeof(uint32_t));
+            memcpy(d->refs, part + (ch ? cb : 0), cnt2 * sizeof(uint32_t));
+        }
+        free(part);
+        free(e.refs);
+    }
+    free(st);
+    return 0;
+}
+
 int hko_build_binned(const float *verts, const uint32_t *tris, uint32_t nt, const float *box,
                      const hko_binned_params *p, uint32_t **nodes_out, uint32_t *nn_out,
                      uint32_t **refs_out, uint32_t *nr_out) {
@@ -1459,6 +1721,13 @@ int hko_build_binned(const float *verts, const uint32_t *tris, uint32_t nt, cons
             tb[6 * i + 3 + a] = mx(mx(p1[a], p2[a]), p3[a]);
         }
     }
+    bin_ctx bc;
+    bc.p = p;
+    bc.tb = tb;
+    bc.hlo = (uint32_t *)malloc(B * sizeof(uint32_t));
+    bc.hhi = (uint32_t *)malloc(B * sizeof(uint32_t));
+    bc.hon = (uint32_t *)malloc(B * sizeof(uint32_t));
+    bc.pl = (float *)malloc((B + 1) * sizeof(float));
     uvec cn = {0, 0, 0}, leafrefs = {0, 0, 0};
     for (int k = 0; k < 4; k++) uv_push(&cn, 0);
     cn.a[2] = CLEAF; /* padding node */
@@ -1471,169 +1740,32 @@ int hko_build_binned(const float *verts, const uint32_t *tris, uint32_t nt, cons
     cur[0].cidx = 0;
     uint32_t *refs = (uint32_t *)malloc((size_t)(nt ? nt : 1) * sizeof(uint32_t));
     for (uint32_t i = 0; i < nt; i++) refs[i] = i;
-    uint32_t *hlo = (uint32_t *)malloc(B * sizeof(uint32_t)), *hhi = (uint32_t *)malloc(B * sizeof(uint32_t));
-    uint32_t *hon = (uint32_t *)malloc(B * sizeof(uint32_t));
-    float *pl = (float *)malloc((B + 1) * sizeof(float));
+    /* deferred subtree roots, in the order the levels meet them */
+    bnode_t *droot = NULL;
+    uvec drefs = {0, 0, 0};
+    uint32_t nd = 0, dcap = 0;
     while (ncur > 0) {
-        /* 1) decisions */
+        /* 1) decisions; -2: a deferred subtree root */
         int32_t *axis = (int32_t *)malloc(ncur * sizeof(int32_t));
         float *plane = (float *)malloc(ncur * sizeof(float));
         uint64_t child_refs = 0;
         for (uint32_t s = 0; s < ncur; s++) {
             bnode_t *n = &cur[s];
             axis[s] = -1;
+            plane[s] = 0.0f;
             if (n->count <= p->leaf_size || n->depth >= p->max_depth) continue;
-            float A = surf(n->box);
-            float best = INFINITY;
+            if (n->count >= 2u && n->count <= p->defer) {
+                axis[s] = -2;
+                continue;
+            }
             uint32_t bnb = 0, bna = 0;
-            if (n->count <= (p->learned ? 32u : p->exact_max)) {
-                /* small node: every clipped reference bound is a candidate
-                 * (+0.0f makes a -0 bound the plane +0) */
-                for (uint32_t a = 0; a < 3; a++) {
-                    float lo_b = n->box[a], hi_b = n->box[4 + a];
-                    if (!(hi_b - lo_b > 0)) continue;
-                    for (uint32_t q = 0; q < 2 * n->count; q++) {
-                        const float *tq = tb + 6 * (size_t)refs[n->start + q / 2];
-                        float pk = ((q & 1) ? mn(tq[3 + a], hi_b) : mx(tq[a], lo_b)) + 0.0f;
-                        if (!(pk > lo_b && pk < hi_b)) continue;
-                        uint32_t nb = 0, na = 0;
-                        for (uint32_t r = 0; r < n->count; r++) {
-                            const float *t6 = tb + 6 * (size_t)refs[n->start + r];
-                            float lo = mx(t6[a], lo_b), hi = mn(t6[3 + a], hi_b);
-                            int on = lo == hi && lo == pk;
-                            nb += (lo < pk || on) ? 1u : 0u;
-                            na += (hi > pk || on) ? 1u : 0u;
-                        }
-                        float bb[8], ba[8];
-                        memcpy(bb, n->box, 32);
-                        memcpy(ba, n->box, 32);
-                        bb[4 + a] = pk;
-                        ba[a] = pk;
-                        float cost = p->ct + p->ci * ((surf(bb) * (float)nb + surf(ba) * (float)na) / A);
-                        /* first minimum in (axis, plane) order */
-                        if (cost < best || (cost == best && (int32_t)a == axis[s] && pk < plane[s])) {
-                            best = cost;
-                            axis[s] = (int32_t)a;
-                            plane[s] = pk;
-                            bnb = nb;
-                            bna = na;
-                        }
-                    }
-                }
-            } else
-            for (uint32_t a = 0; a < 3; a++) {
-                float lo_b = n->box[a], hi_b = n->box[4 + a];
-                float ext = hi_b - lo_b;
-                if (!(ext > 0)) continue;
-                float inv = (float)B / ext;
-                for (uint32_t k = 1; k < B; k++) pl[k] = bplane(n->box, a, k, B);
-                memset(hlo, 0, B * 4);
-                memset(hhi, 0, B * 4);
-                memset(hon, 0, B * 4);
-                for (uint32_t r = 0; r < n->count; r++) {
-                    const float *t6 = tb + 6 * (size_t)refs[n->start + r];
-                    float lo = mx(t6[a], lo_b), hi = mn(t6[3 + a], hi_b);
-                    int b = (int)((lo - lo_b) * inv);
-                    b = b < 0 ? 0 : (b > (int)B - 1 ? (int)B - 1 : b);
-                    while (b > 0 && lo < pl[b]) b--;
-                    while (b < (int)B - 1 && lo >= pl[b + 1]) b++;
-                    int c = (int)((hi - lo_b) * inv);
-                    c = c < 0 ? 0 : (c > (int)B - 1 ? (int)B - 1 : c);
-                    while (c > 0 && hi <= pl[c]) c--;
-                    while (c < (int)B - 1 && hi > pl[c + 1]) c++;
-                    hlo[b]++;
-                    hhi[c]++;
-                    if (lo == hi && b >= 1 && lo == pl[b]) hon[b]++;
-                }
-                uint32_t below = 0, above = n->count;
-                for (uint32_t k = 1; k < B; k++) {
-                    below += hlo[k - 1];
-                    above -= hhi[k - 1];
-                    float pk = pl[k];
-                    if (!(pk > lo_b && pk < hi_b)) continue;
-                    if (k < B - 1 && !(pk < pl[k + 1])) continue;
-                    uint32_t nb = below + hon[k], na = above + hon[k];
-                    float bb[8], ba[8];
-                    memcpy(bb, n->box, 32);
-                    memcpy(ba, n->box, 32);
-                    bb[4 + a] = pk;
-                    ba[a] = pk;
-                    float cost = p->ct + p->ci * ((surf(bb) * (float)nb + surf(ba) * (float)na) / A);
-                    if (cost < best) {
-                        best = cost;
-                        axis[s] = (int32_t)a;
-                        plane[s] = pk;
-                        bnb = nb;
-                        bna = na;
-                    }
-                }
-            }
-            if (p->learned && n->count > 32 && n->count <= 1024 && p->proposals) {
-                const int32_t *prop = p->proposals + 8 * (size_t)n->cidx;
-                uint32_t K = p->topk < 8 ? (p->topk ? p->topk : 1) : 8;
-                uint32_t cap = 1;
-                while (2u * cap * 3u * K <= 2048u) cap *= 2u;
-                float rbest = INFINITY, rpk = 0.0f;
-                int32_t rax = 3;
-                uint32_t rnb = 0, rna = 0;
-                for (uint32_t i = 0; i < 8 && prop[i] >= 0; i++) {
-                    uint32_t a = (uint32_t)prop[i] / 32u, b = (uint32_t)prop[i] % 32u;
-                    float lo_b = n->box[a], hi_b = n->box[4 + a];
-                    float P0 = b == 0 ? lo_b : bplane(n->box, a, b, 32);
-                    float P1 = b == 31 ? hi_b : bplane(n->box, a, b + 1, 32);
-                    uint32_t nl = 0, nh = 0, nf = 0;
-                    for (uint32_t r = 0; r < n->count; r++) {
-                        const float *t6 = tb + 6 * (size_t)refs[n->start + r];
-                        float lo = mx(t6[a], lo_b), hi = mn(t6[3 + a], hi_b);
-                        int inl = P0 <= lo && lo <= P1, inh = P0 <= hi && hi <= P1;
-                        nl += inl;
-                        nh += inh;
-                        nf += inl && lo == hi;
-                    }
-                    if (nl > cap || nh > cap || nf > cap) continue;
-                    for (uint32_t q = 0; q < 2 * n->count; q++) {
-                        const float *tq = tb + 6 * (size_t)refs[n->start + q / 2];
-                        float v = (q & 1) ? mn(tq[3 + a], hi_b) : mx(tq[a], lo_b);
-                        if (!(P0 <= v && v <= P1)) continue;
-                        if (!(v > lo_b && v < hi_b)) continue;
-                        float pk = v + 0.0f;
-                        uint32_t nb = 0, na = 0;
-                        for (uint32_t r = 0; r < n->count; r++) {
-                            const float *t6 = tb + 6 * (size_t)refs[n->start + r];
-                            float lo = mx(t6[a], lo_b), hi = mn(t6[3 + a], hi_b);
-                            int on = lo == hi && lo == pk;
-                            nb += (lo < pk || on) ? 1u : 0u;
-                            na += (hi > pk || on) ? 1u : 0u;
-                        }
-                        float bb[8], ba[8];
-                        memcpy(bb, n->box, 32);
-                        memcpy(ba, n->box, 32);
-                        bb[4 + a] = pk;
-                        ba[a] = pk;
-                        float cost = p->ct + p->ci * ((surf(bb) * (float)nb + surf(ba) * (float)na) / A);
-                        if (cost < rbest || (cost == rbest && ((int32_t)a < rax || ((int32_t)a == rax && pk < rpk)))) {
-                            rbest = cost;
-                            rax = (int32_t)a;
-                            rpk = pk;
-                            rnb = nb;
-                            rna = na;
-                        }
-                    }
-                }
-                if (rbest < INFINITY && rbest <= p->fallback_ratio * best) {
-                    best = rbest;
-                    axis[s] = rax;
-                    plane[s] = rpk;
-                    bnb = rnb;
-                    bna = rna;
-                }
-            }
-            if (axis[s] >= 0 && !(best < p->ci * (float)n->count)) axis[s] = -1;
+            axis[s] = decide_binned(&bc, n, refs, &plane[s], &bnb, &bna);
             if (axis[s] >= 0) child_refs += (uint64_t)bnb + bna;
         }
         /* capacity guard: a level whose children would overflow the reference
-         * arena, the leaf-reference array or the node array stops splitting
-         * (every node of the level becomes a leaf) */
+         * arena, the leaf-reference array (deferred references count as leaf
+         * references) or the node array stops splitting (every node of the
+         * level becomes a leaf) */
         {
             uint64_t leaf_refs_level = 0, splits = 0;
             for (uint32_t s = 0; s < ncur; s++) {
@@ -1641,17 +1773,28 @@ int hko_build_binned(const float *verts, const uint32_t *tris, uint32_t nt, cons
                 else leaf_refs_level += cur[s].count;
             }
             if (child_refs > p->max_refs ||
-                (uint64_t)leafrefs.n + leaf_refs_level + child_refs > p->max_refs ||
+                (uint64_t)leafrefs.n + drefs.n + leaf_refs_level + child_refs > p->max_refs ||
                 (uint64_t)(cn.n / 2) + 2 * splits > p->max_nodes)
                 for (uint32_t s = 0; s < ncur; s++) axis[s] = -1;
         }
-        /* 2) emit leaves and partition */
+        /* 2) emit leaves, deferred roots and partition */
         bnode_t *nxt = (bnode_t *)malloc((size_t)2 * ncur * sizeof(bnode_t) + sizeof(bnode_t));
         uint32_t nnxt = 0;
         uint32_t *nrefs = (uint32_t *)malloc((size_t)(child_refs ? child_refs : 1) * sizeof(uint32_t));
         uint32_t nr = 0;
         for (uint32_t s = 0; s < ncur; s++) {
             bnode_t *n = &cur[s];
+            if (axis[s] == -2) {
+                if (nd == dcap) {
+                    dcap = dcap ? 2 * dcap : 64;
+                    droot = (bnode_t *)realloc(droot, dcap * sizeof(bnode_t));
+                }
+                droot[nd] = *n;
+                droot[nd].start = (uint32_t)drefs.n;
+                nd++;
+                for (uint32_t r = 0; r < n->count; r++) uv_push(&drefs, refs[n->start + r]);
+                continue;
+            }
             if (axis[s] < 0) {
                 cn.a[2 * n->cidx] = ((uint32_t)leafrefs.n << 2) | CLEAF;
                 cn.a[2 * n->cidx + 1] = n->count;
@@ -1664,22 +1807,9 @@ int hko_build_binned(const float *verts, const uint32_t *tris, uint32_t nt, cons
             for (int k = 0; k < 4; k++) uv_push(&cn, 0);
             cn.a[2 * n->cidx] = (pair << 2) | a;
             memcpy(&cn.a[2 * n->cidx + 1], &pk, 4);
-            uint32_t bstart = nr;
-            for (uint32_t r = 0; r < n->count; r++) {
-                uint32_t tri = refs[n->start + r];
-                const float *t6 = tb + 6 * (size_t)tri;
-                float lo = mx(t6[a], n->box[a]), hi = mn(t6[3 + a], n->box[4 + a]);
-                if (lo < pk || (lo == hi && lo == pk)) nrefs[nr++] = tri;
-            }
-            uint32_t bcount = nr - bstart;
-            uint32_t astart = nr;
-            for (uint32_t r = 0; r < n->count; r++) {
-                uint32_t tri = refs[n->start + r];
-                const float *t6 = tb + 6 * (size_t)tri;
-                float lo = mx(t6[a], n->box[a]), hi = mn(t6[3 + a], n->box[4 + a]);
-                if (hi > pk || (lo == hi && lo == pk)) nrefs[nr++] = tri;
-            }
-            uint32_t acount = nr - astart;
+            uint32_t bcount = 0, acount = 0, bstart = nr;
+            partition_refs(tb, n, refs, a, pk, nrefs + nr, &bcount, &acount);
+            nr += bcount + acount;
             for (uint32_t ch = 0; ch < 2; ch++) {
                 uint32_t cnt2 = ch ? acount : bcount;
                 uint32_t idx = pair + ch;
@@ -1691,7 +1821,7 @@ int hko_build_binned(const float *verts, const uint32_t *tris, uint32_t nt, cons
                 bnode_t *c2 = &nxt[nnxt++];
                 memcpy(c2->box, n->box, 32);
                 if (ch == 0) c2->box[4 + a] = pk; else c2->box[a] = pk;
-                c2->start = ch ? astart : bstart;
+                c2->start = ch ? bstart + bcount : bstart;
                 c2->count = cnt2;
                 c2->depth = n->depth + 1;
                 c2->cidx = idx;
@@ -1705,12 +1835,30 @@ int hko_build_binned(const float *verts, const uint32_t *tris, uint32_t nt, cons
         ncur = nnxt;
         refs = nrefs;
     }
+    /* 3) the deferred subtrees, in order, after every level's nodes and leaf
+     * references; when they do not all fit the node and reference capacities
+     * every deferred root stays a leaf instead */
+    {
+        size_t n0 = cn.n, r0 = leafrefs.n;
+        for (uint32_t i = 0; i < nd; i++) expand_subtree(&bc, &cn, &leafrefs, &droot[i], drefs.a + droot[i].start);
+        if ((uint64_t)(cn.n / 2) > p->max_nodes || (uint64_t)leafrefs.n > p->max_refs) {
+            cn.n = n0;
+            leafrefs.n = r0;
+            for (uint32_t i = 0; i < nd; i++) {
+                cn.a[2 * droot[i].cidx] = ((uint32_t)leafrefs.n << 2) | CLEAF;
+                cn.a[2 * droot[i].cidx + 1] = droot[i].count;
+                for (uint32_t r = 0; r < droot[i].count; r++) uv_push(&leafrefs, drefs.a[droot[i].start + r]);
+            }
+        }
+    }
+    free(droot);
+    free(drefs.a);
     free(cur);
     free(refs);
-    free(hlo);
-    free(hhi);
-    free(hon);
-    free(pl);
+    free(bc.hlo);
+    free(bc.hhi);
+    free(bc.hon);
+    free(bc.pl);
     free(tb);
     *nodes_out = cn.a;
     *nn_out = (uint32_t)(cn.n / 2);

@@ -164,6 +164,11 @@ typedef struct {
     uint32_t topk;           /* proposals per node (list capacity depends on it) */
     float fallback_ratio;
     const int32_t *proposals; /* per compact node, 8 bins (axis * 32 + bin, -1: none) */
+    /* T > 0: a decidable node of 2..T refs (T <= 32) is a deferred subtree
+     * root: its subtree is built depth first after the levels and numbered
+     * after every level's nodes (the CUDA builder's layout, hk_config
+     * subtree_max); 0: every node level by level */
+    uint32_t defer;
 } hko_binned_params;
 int hko_build_binned(const float *verts, const uint32_t *tris, uint32_t nt, const float *box,
                      const hko_binned_params *p, uint32_t **nodes_out, uint32_t *nn_out,

@@ -51,6 +51,27 @@ def test_build_identical_to_oracle(hk, oracle, which, exact_max):
     assert st["nodes"] == on.shape[0] and st["refs"] == orf.shape[0]
 
 
+@pytest.mark.parametrize("subtree_max", [0, 16])
+def test_subtree_threshold_identical_to_oracle(hk, oracle, subtree_max):
+    """hk_config.subtree_max: no deferred subtrees (every node level by
+    level), and subtrees of nodes of at most 16 references; the GPU tree
+    equals the oracle's with the same threshold."""
+    sc = small_animated()
+    verts, tris, box = sc.verts, sc.tris, sc.scene_box()
+    ctx = hk.Context(subtree_max=subtree_max)
+    ctx.upload(verts, tris)
+    ctx.set_box(box)
+    ctx.precompute()
+    st = ctx.build()
+    cn, cr = ctx.export_compact()
+    on, orf = oracle.build_binned(verts, tris, box, ct=1.0, ci=1.5, max_depth=24, leaf_size=4, defer=subtree_max)
+    assert np.array_equal(cn, on) and np.array_equal(cr, orf)
+    sub = ctx.subtree_counts()
+    assert (sub["roots"] == 0) == (subtree_max == 0)
+    assert st["nodes"] == on.shape[0]
+    ctx.close()
+
+
 def test_trace_on_built_tree(ctx, hk, oracle):
     g = load("small24k.npz")
     ctx.upload(g["verts"], g["tris"])
