@@ -435,10 +435,11 @@ __device__ Decision sah_warp(HistPtr H, float4 blo, float4 bhi, uint32_t cnt, fl
 // ---------------------------------------------------------------------------
 struct LevelArgs {
     const float4 *tb_lo, *tb_hi;
-    const float4 *n_lo, *n_hi;
-    const uint4 *n_info;
-    float4 *nx_lo, *nx_hi;
-    uint4 *nx_info;
+    // the level's nodes and references, ping-pong by level parity: level L
+    // reads buffer L & 1 and writes the other (the accessors below)
+    float4 *lo_buf[2], *hi_buf[2];
+    uint4 *info_buf[2];
+    uint32_t *refs_buf[2], *ref_node_buf[2];
     int32_t *axis;
     float *plane;
     uint2 *cnt;
@@ -449,9 +450,6 @@ struct LevelArgs {
     uint32_t *medium_slot;
     uint32_t *hist;
     uint32_t *done;
-    const uint32_t *refs;
-    const uint32_t *ref_node;
-    uint32_t *nx_refs, *nx_ref_node;
     uint2 *out_nodes;
     uint32_t *out_refs;
     uint32_t *out_ropes;
@@ -496,6 +494,20 @@ struct LevelArgs {
     uint4 *sc_ref;             // subtree scratch reference slots: (subtree, local index, triangle, -)
     uint32_t cap_sc_nodes, cap_sc_refs;
     uint2 *st_cnt, *st_root, *st_base;   // per subtree: (nodes, refs), root entry, place
+
+    // (selects rather than indexing: a copy of the struct whose level changes
+    // stays in registers)
+    __device__ __forceinline__ bool odd() const { return (level & 1u) != 0; }
+    __device__ __forceinline__ float4 *n_lo() const { return odd() ? lo_buf[1] : lo_buf[0]; }
+    __device__ __forceinline__ float4 *n_hi() const { return odd() ? hi_buf[1] : hi_buf[0]; }
+    __device__ __forceinline__ uint4 *n_info() const { return odd() ? info_buf[1] : info_buf[0]; }
+    __device__ __forceinline__ uint32_t *refs() const { return odd() ? refs_buf[1] : refs_buf[0]; }
+    __device__ __forceinline__ uint32_t *ref_node() const { return odd() ? ref_node_buf[1] : ref_node_buf[0]; }
+    __device__ __forceinline__ float4 *nx_lo() const { return odd() ? lo_buf[0] : lo_buf[1]; }
+    __device__ __forceinline__ float4 *nx_hi() const { return odd() ? hi_buf[0] : hi_buf[1]; }
+    __device__ __forceinline__ uint4 *nx_info() const { return odd() ? info_buf[0] : info_buf[1]; }
+    __device__ __forceinline__ uint32_t *nx_refs() const { return odd() ? refs_buf[0] : refs_buf[1]; }
+    __device__ __forceinline__ uint32_t *nx_ref_node() const { return odd() ? ref_node_buf[0] : ref_node_buf[1]; }
 };
 
 // true (on every thread of the CTA alike) when an earlier kernel of this build
@@ -562,19 +574,20 @@ __global__ void k_root(LevelArgs A, const float *box, uint32_t nt) {
         l0->n_medium = medium ? 1u : 0u;
         if (large) A.large_slot[0] = 0;
         if (medium) A.medium_slot[0] = 0;
-        A.nx_lo[0] = make_float4(box[0], box[1], box[2], 0.0f);
-        A.nx_hi[0] = make_float4(box[4], box[5], box[6], 0.0f);
-        A.nx_info[0] = make_uint4(0, nt, 0, 0);
+        // level 0's node buffers (A.level is 0)
+        A.n_lo()[0] = make_float4(box[0], box[1], box[2], 0.0f);
+        A.n_hi()[0] = make_float4(box[4], box[5], box[6], 0.0f);
+        A.n_info()[0] = make_uint4(0, nt, 0, 0);
         A.out_nodes[1] = make_uint2(kLeafTag, 0);
         A.out_nodes[0] = make_uint2(kLeafTag, 0);
         // root cell = scene box, no ropes (every face is the scene boundary)
-        A.out_cbox[0] = A.nx_lo[0];
-        A.out_cbox[1] = A.nx_hi[0];
+        A.out_cbox[0] = make_float4(box[0], box[1], box[2], 0.0f);
+        A.out_cbox[1] = make_float4(box[4], box[5], box[6], 0.0f);
         for (int f = 0; f < 6; f++) A.out_ropes[f] = 0xffffffffu;
     }
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nt; i += gridDim.x * blockDim.x) {
-        const_cast<uint32_t *>(A.refs)[i] = i;
-        const_cast<uint32_t *>(A.ref_node)[i] = 0;
+        A.refs()[i] = i;
+        A.ref_node()[i] = 0;
     }
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < nch; k += gridDim.x * blockDim.x)
         A.chunks[k] = make_uint2(0, k);
@@ -634,7 +647,7 @@ __device__ __forceinline__ void write_decision(const LevelArgs &A, uint32_t s, c
 }
 
 __device__ __forceinline__ void write_decision(const LevelArgs &A, uint32_t s, const Decision &d) {
-    if (d.axis >= 0) write_decision(A, s, d, A.n_lo[s], A.n_hi[s]);
+    if (d.axis >= 0) write_decision(A, s, d, A.n_lo()[s], A.n_hi()[s]);
     else write_decision(A, s, d, make_float4(0, 0, 0, 0), make_float4(0, 0, 0, 0));
 }
 
@@ -796,7 +809,7 @@ __device__ Decision sah_exact_warp32(const LevelArgs &A, uint4 info, float4 blo,
     const bool have = lane < info.y;
     float4 tlo = make_float4(0, 0, 0, 0), thi = tlo;
     if (have) {
-        const uint32_t tri = A.refs[info.x + lane];
+        const uint32_t tri = A.refs()[info.x + lane];
         tlo = A.tb_lo[tri];
         thi = A.tb_hi[tri];
     }
@@ -850,7 +863,7 @@ __device__ Decision sah_exact_cta(const LevelArgs &A, uint4 info, float4 blo, fl
         for (uint32_t i = tid; i < n2; i += blockDim.x) {
             float lo = kInf, hi = kInf;
             if (i < cnt) {
-                const uint32_t tri = A.refs[info.x + i];
+                const uint32_t tri = A.refs()[info.x + i];
                 lo = mxf(c3(A.tb_lo[tri], a), l);
                 hi = mnf(c3(A.tb_hi[tri], a), h);
                 if (lo == hi) S.fl[atomicAdd(&S.nflat, 1u)] = lo;   // flat references, any order
@@ -997,25 +1010,30 @@ __device__ __forceinline__ void finish_large(const LevelArgs &A, uint32_t s, con
     }
 }
 
-__global__ void __launch_bounds__(256, 3) k_hist(LevelArgs A) {
-    __shared__ uint32_t H[kHist];
-    __shared__ ExactCtaSmem XS;
-    __shared__ int s_last;
-    __shared__ uint32_t s_tally[kTallies];
-    if (level_aborted(A)) return;
-    Tally tally;
+// shared memory of a CTA's large-node work
+struct HistSmem {
+    uint32_t H[kHist];
+    int last;
+};
+
+// k_hist's work for one level (every CTA of the grid calls it): the chunks of
+// the large nodes and, with MEDIUM, the medium nodes (exact SAH, XS)
+template <bool MEDIUM>
+__device__ __forceinline__ void hist_body(const LevelArgs &A, HistSmem &SH, ExactCtaSmem *XSp, Tally &tally) {
+    uint32_t *H = SH.H;
+    int &s_last = SH.last;
     const uint32_t wib = threadIdx.x >> 5, lane = threadIdx.x & 31u;
     const uint32_t nch = min(A.lc->n_chunks, A.cap_chunks);
-    const uint32_t nmed = min(A.lc->n_medium, A.cap_medium);
+    const uint32_t nmed = MEDIUM ? min(A.lc->n_medium, A.cap_medium) : 0u;
     const uint32_t nodes = A.lc->nodes;
     for (uint32_t item = blockIdx.x; item < nch + nmed; item += gridDim.x) {
-        if (item >= nch) {
+        if (MEDIUM && item >= nch) {
             // a medium node: the exact SAH in this CTA
             const uint32_t s = A.medium_slot[item - nch];
             if (s >= nodes) continue;
-            const uint4 info = A.n_info[s];
-            const float4 blo = A.n_lo[s], bhi = A.n_hi[s];
-            const Decision d = sah_exact_cta(A, info, blo, bhi, A.ct, A.ci, XS);
+            const uint4 info = A.n_info()[s];
+            const float4 blo = A.n_lo()[s], bhi = A.n_hi()[s];
+            const Decision d = sah_exact_cta(A, info, blo, bhi, A.ct, A.ci, *XSp);
             if (threadIdx.x == 0) {
                 write_decision(A, s, d);
                 tally.add(d, info.y);
@@ -1027,7 +1045,7 @@ __global__ void __launch_bounds__(256, 3) k_hist(LevelArgs A) {
                 __syncthreads();
                 const float4 inv3 = bin_scale(blo, bhi);
                 for (uint32_t r = info.x + threadIdx.x; r < info.x + info.y; r += blockDim.x) {
-                    const uint32_t tri = A.refs[r];
+                    const uint32_t tri = A.refs()[r];
                     hist_ref(H, A.tb_lo[tri], A.tb_hi[tri], blo, bhi, inv3);
                 }
                 __syncthreads();
@@ -1049,8 +1067,8 @@ __global__ void __launch_bounds__(256, 3) k_hist(LevelArgs A) {
         if (rank >= A.cap_large) continue;  // uniform per CTA
         const uint32_t s = A.large_slot[rank];
         if (s >= nodes) continue;
-        const uint4 info = A.n_info[s];
-        const float4 blo = A.n_lo[s], bhi = A.n_hi[s];
+        const uint4 info = A.n_info()[s];
+        const float4 blo = A.n_lo()[s], bhi = A.n_hi()[s];
         const uint32_t r0 = info.x + ck.y * kChunk, r1 = min(info.x + info.y, r0 + kChunk);
         for (uint32_t i = threadIdx.x; i < kHist; i += blockDim.x) H[i] = 0;
         __syncthreads();
@@ -1063,7 +1081,7 @@ __global__ void __launch_bounds__(256, 3) k_hist(LevelArgs A) {
 #pragma unroll
             for (int k = 0; k < kPer; k++) {
                 const uint32_t r = r0 + threadIdx.x + 256u * k;
-                tri[k] = r < r1 ? A.refs[r] : 0xffffffffu;
+                tri[k] = r < r1 ? A.refs()[r] : 0xffffffffu;
             }
 #pragma unroll
             for (int k = 0; k < kPer; k++)
@@ -1102,6 +1120,15 @@ __global__ void __launch_bounds__(256, 3) k_hist(LevelArgs A) {
         }
         __syncthreads();
     }
+}
+
+__global__ void __launch_bounds__(256, 3) k_hist(LevelArgs A) {
+    __shared__ HistSmem SH;
+    __shared__ ExactCtaSmem XS;
+    __shared__ uint32_t s_tally[kTallies];
+    if (level_aborted(A)) return;
+    Tally tally;
+    hist_body<true>(A, SH, &XS, tally);
     tally_flush(A, tally, s_tally);
 }
 
@@ -1113,19 +1140,14 @@ __global__ void __launch_bounds__(256, 3) k_hist(LevelArgs A) {
 // binned decision and histogram features are stored for k_learn, which
 // decides it (a node past the row capacity keeps the binned decision).
 template <bool WARP_EXACT, bool LEARNED>
-__global__ void __launch_bounds__(256, 5) k_small(LevelArgs A) {
-    __shared__ __align__(16) uint32_t HS[8][kHist];
-    __shared__ uint32_t s_tally[kTallies];
-    wait_prior_grid();
-    if (level_aborted(A)) return;
-    Tally tally;
+__device__ __forceinline__ void small_body(const LevelArgs &A, uint32_t (*HS)[kHist], Tally &tally) {
     const uint32_t wib = threadIdx.x >> 5, lane = threadIdx.x & 31u;
     const uint32_t nodes = A.lc->nodes;
     const uint32_t ngroups = (nodes + 7) / 8;
     for (uint32_t g = blockIdx.x; g < ngroups; g += gridDim.x) {
         const uint32_t s = g * 8 + wib;
         if (s >= nodes) continue;
-        const uint4 info = A.n_info[s];
+        const uint4 info = A.n_info()[s];
         const uint32_t cnt = info.y;
         const bool dec = decidable(A, cnt);
         if (dec && (is_large(A, cnt) || is_medium(A, cnt))) continue;   // k_hist
@@ -1138,7 +1160,7 @@ __global__ void __launch_bounds__(256, 5) k_small(LevelArgs A) {
             }
             continue;
         }
-        const float4 blo = A.n_lo[s], bhi = A.n_hi[s];
+        const float4 blo = A.n_lo()[s], bhi = A.n_hi()[s];
         Decision d;
         if (WARP_EXACT && cnt <= kWarpExact) {
             d = sah_exact_warp32(A, info, blo, bhi, A.ct, A.ci);
@@ -1154,7 +1176,7 @@ __global__ void __launch_bounds__(256, 5) k_small(LevelArgs A) {
             __syncwarp();
             const float4 inv3 = bin_scale(blo, bhi);
             for (uint32_t r = info.x + lane; r < info.x + cnt; r += 32) {
-                const uint32_t tri = A.refs[r];
+                const uint32_t tri = A.refs()[r];
                 hist_ref(Hw, A.tb_lo[tri], A.tb_hi[tri], blo, bhi, inv3);
             }
             __syncwarp();
@@ -1179,6 +1201,36 @@ __global__ void __launch_bounds__(256, 5) k_small(LevelArgs A) {
         }
         __syncwarp();
     }
+}
+
+template <bool WARP_EXACT, bool LEARNED>
+__global__ void __launch_bounds__(256, 5) k_small(LevelArgs A) {
+    __shared__ __align__(16) uint32_t HS[8][kHist];
+    __shared__ uint32_t s_tally[kTallies];
+    wait_prior_grid();
+    if (level_aborted(A)) return;
+    Tally tally;
+    small_body<WARP_EXACT, LEARNED>(A, HS, tally);
+    tally_flush(A, tally, s_tally);
+}
+
+// Binned mode (no medium nodes, no proposer): a level's large-node chunks and
+// small nodes in one launch on the build's stream, PDL-chained to the plan
+// (no second stream, no fork and join per level)
+union DecideSmem {
+    HistSmem hist;
+    uint32_t HS[8][kHist];
+};
+
+__global__ void __launch_bounds__(256, 4) k_decide(LevelArgs A) {
+    __shared__ __align__(16) DecideSmem sm;
+    __shared__ uint32_t s_tally[kTallies];
+    wait_prior_grid();
+    if (level_aborted(A)) return;
+    Tally tally;
+    hist_body<false>(A, sm.hist, nullptr, tally);
+    __syncthreads();
+    small_body<false, false>(A, sm.HS, tally);
     tally_flush(A, tally, s_tally);
 }
 
@@ -1328,11 +1380,11 @@ __global__ void __launch_bounds__(256, 1) k_learn(LevelArgs A) {
             const uint32_t rr = wib + 8u * lane;
             if (lane < kRows / 8 && row0 + rr < rows) {
                 my_slot = A.learn_slot[row0 + rr];
-                const float4 blo = A.n_lo[my_slot], bhi = A.n_hi[my_slot];
+                const float4 blo = A.n_lo()[my_slot], bhi = A.n_hi()[my_slot];
 #pragma unroll
                 for (int j = 0; j < 3; j++)
                     if (__fsub_rn(c3(bhi, j), c3(blo, j)) > 0.0f) my_axes |= 1u << j;
-                if (A.prop_log) my_cidx = A.n_info[my_slot].z;
+                if (A.prop_log) my_cidx = A.n_info()[my_slot].z;
             }
         }
         for (uint32_t rr = wib; rr < kRows && row0 + rr < rows; rr += 8) {
@@ -1439,8 +1491,8 @@ __global__ void __launch_bounds__(kRefineThreads) k_refine_cta(LevelArgs A) {
         const LearnBin lb = A.learn_bin[row];
         if (lb.pad[0] <= kRefineWarpMax) continue;   // k_refine_warp's row (uniform over the CTA)
         const uint32_t s = A.learn_slot[row];
-        const uint4 info = A.n_info[s];
-        const float4 blo = A.n_lo[s], bhi = A.n_hi[s];
+        const uint4 info = A.n_info()[s];
+        const float4 blo = A.n_lo()[s], bhi = A.n_hi()[s];
         const uint32_t cnt = info.y;
         const uint2 pp = A.learn_prop[row];
         uint32_t pax[kLearnMaxK];
@@ -1468,7 +1520,7 @@ __global__ void __launch_bounds__(kRefineThreads) k_refine_cta(LevelArgs A) {
             const bool have = base + tid < cnt;
             float4 tlo = make_float4(0, 0, 0, 0), thi = tlo;
             if (have) {
-                const uint32_t tri = A.refs[info.x + base + tid];
+                const uint32_t tri = A.refs()[info.x + base + tid];
                 tlo = A.tb_lo[tri];
                 thi = A.tb_hi[tri];
             }
@@ -1631,8 +1683,8 @@ __global__ void __launch_bounds__(256) k_refine_warp(LevelArgs A) {
         const LearnBin lb = A.learn_bin[row];
         if (lb.pad[0] > kRefineWarpMax) continue;   // k_refine_cta's row
         const uint32_t s = A.learn_slot[row];
-        const uint4 info = A.n_info[s];
-        const float4 blo = A.n_lo[s], bhi = A.n_hi[s];
+        const uint4 info = A.n_info()[s];
+        const float4 blo = A.n_lo()[s], bhi = A.n_hi()[s];
         const uint32_t cnt = info.y;
         const uint2 pp = A.learn_prop[row];
         uint32_t pax[kLearnMaxK];
@@ -1661,7 +1713,7 @@ __global__ void __launch_bounds__(256) k_refine_warp(LevelArgs A) {
 #pragma unroll
             for (int u = 0; u < 4; u++) {
                 have[u] = base + 32u * u + lane < cnt;
-                tri[u] = have[u] ? A.refs[info.x + base + 32u * u + lane] : 0u;
+                tri[u] = have[u] ? A.refs()[info.x + base + 32u * u + lane] : 0u;
             }
 #pragma unroll
             for (int u = 0; u < 4; u++) {
@@ -1855,7 +1907,7 @@ struct PlanOp {
     }
     __device__ Item load(uint32_t s, const Ctx &) const {
         if (s == 0xffffffffu) return Item{make_uint4(0, 0, 0, 0), make_uint2(0, 0), -1};
-        return Item{A.n_info[s], A.cnt[s], A.axis[s]};
+        return Item{A.n_info()[s], A.cnt[s], A.axis[s]};
     }
     __device__ T value(const Item &it) const {
         if (it.axis == kDeferAxis) return U7{0, 0, 0, 0, 0, it.info.y, 1};
@@ -1898,8 +1950,8 @@ struct PlanOp {
             const uint32_t did = cx.defer_nodes_total + pl.e;
             if (did < A.cap_defer) {
                 A.d_root[did] = make_uint4(info.z, cx.defer_refs_total + pl.d, info.y, A.level);
-                A.d_lo[did] = A.n_lo[s];
-                A.d_hi[did] = A.n_hi[s];
+                A.d_lo[did] = A.n_lo()[s];
+                A.d_hi[did] = A.n_hi()[s];
             } else {
                 atomicOr(A.err, 2u);
             }
@@ -1920,7 +1972,7 @@ struct PlanOp {
             return;
         }
         const float p = A.plane[s];
-        const float4 lo = A.n_lo[s], hi = A.n_hi[s];
+        const float4 lo = A.n_lo()[s], hi = A.n_hi()[s];
         uint32_t r[6];
         {
             // the parent's ropes: 6 words at a 24-byte stride (8-byte aligned)
@@ -1957,9 +2009,9 @@ struct PlanOp {
         if (ct.x) {
             float4 h2 = hi;
             s3(h2, ax, p);
-            A.nx_lo[ns] = lo;
-            A.nx_hi[ns] = h2;
-            A.nx_info[ns] = make_uint4(co, ct.x, pair, 0);
+            A.nx_lo()[ns] = lo;
+            A.nx_hi()[ns] = h2;
+            A.nx_info()[ns] = make_uint4(co, ct.x, pair, 0);
             child_setup(A, ns, ct.x);
             ns++;
         } else {
@@ -1968,9 +2020,9 @@ struct PlanOp {
         if (ct.y) {
             float4 l2 = lo;
             s3(l2, ax, p);
-            A.nx_lo[ns] = l2;
-            A.nx_hi[ns] = hi;
-            A.nx_info[ns] = make_uint4(co + ct.x, ct.y, pair + 1, 0);
+            A.nx_lo()[ns] = l2;
+            A.nx_hi()[ns] = hi;
+            A.nx_info()[ns] = make_uint4(co + ct.x, ct.y, pair + 1, 0);
             child_setup(A, ns, ct.y);
         } else {
             A.out_nodes[pair + 1] = make_uint2(kLeafTag, 0);
@@ -2000,8 +2052,8 @@ struct RefOp {
     __device__ Ctx ctx() const { return A.lc->stop; }
     __device__ Item load(uint32_t r, const Ctx &stop) const {
         if (r == 0xffffffffu) return Item{make_uint2(0, 0), 0, 0};
-        const uint32_t s = A.ref_node[r];
-        const uint32_t tri = A.refs[r];
+        const uint32_t s = A.ref_node()[r];
+        const uint32_t tri = A.refs()[r];
         const float4 sp = A.split[s];
         const int ax = stop ? -1 : __float_as_int(sp.x);
         if (ax < 0) return Item{make_uint2(0, 0), s, tri};
@@ -2023,8 +2075,8 @@ struct RefOp {
         if (it.f.x) {
             const uint32_t pos = sc.x + R.x;
             if (pos < A.cap_refs && R.x < sc.y - sc.x) {
-                A.nx_refs[pos] = it.tri;
-                A.nx_ref_node[pos] = sc.z;
+                A.nx_refs()[pos] = it.tri;
+                A.nx_ref_node()[pos] = sc.z;
             } else {
                 atomicOr(A.err, 8u);
             }
@@ -2032,8 +2084,8 @@ struct RefOp {
         if (it.f.y) {
             const uint32_t pos = sc.y + R.y;
             if (pos < A.cap_refs && R.y < (sc.w >> 2)) {
-                A.nx_refs[pos] = it.tri;
-                A.nx_ref_node[pos] = sc.z + ((sc.w & 2u) ? 1u : 0u);
+                A.nx_refs()[pos] = it.tri;
+                A.nx_ref_node()[pos] = sc.z + ((sc.w & 2u) ? 1u : 0u);
             } else {
                 atomicOr(A.err, 8u);
             }
@@ -2081,7 +2133,7 @@ __device__ void ref_tile(const RefOp &R, uint32_t rt, uint32_t nr, uint32_t tag,
     // node of the reference before this thread's first one
     uint32_t prev = __shfl_up_sync(0xffffffffu, it[kScanItems - 1].s, 1);
     if (lane == 31) sh.w_last[wid] = it[kScanItems - 1].s;
-    const uint32_t first_prev = (threadIdx.x == 0 && r0 > 0) ? A.ref_node[r0 - 1] : 0xffffffffu;
+    const uint32_t first_prev = (threadIdx.x == 0 && r0 > 0) ? A.ref_node()[r0 - 1] : 0xffffffffu;
     __syncthreads();
     if (lane == 0) prev = wid ? sh.w_last[wid - 1] : first_prev;
     SegV t{make_uint2(0, 0), 0u};
@@ -2151,16 +2203,21 @@ __device__ void ref_tile(const RefOp &R, uint32_t rt, uint32_t nr, uint32_t tag,
 // their tickets before any reference tile and wait for nothing but earlier
 // plan tiles, so every wait ends.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kScanThreads, 6) k_plan_refs(LevelArgs A, uint32_t *pflags, U7 *paggs, U7 *pincls,
-                                                            uint32_t *rflags, uint2 *raggs, uint2 *rincls,
-                                                            uint32_t *pdone, uint32_t *ticket) {
-    __shared__ U7 shp[kScanThreads / 32 + 1];
-    __shared__ U7 sxp;
-    __shared__ RefTileSmem shr_seg;
-    __shared__ uint32_t s_tile;
-    __shared__ uint32_t s_wait_ok;
-    wait_prior_grid();
-    if (level_aborted(A)) return;
+struct PlanSmem {
+    U7 shp[kScanThreads / 32 + 1];
+    U7 sxp;
+    RefTileSmem shr_seg;
+    uint32_t tile, wait_ok;
+};
+
+__device__ __forceinline__ void plan_refs_body(const LevelArgs &A, PlanSmem &SM, uint32_t *pflags, U7 *paggs,
+                                               U7 *pincls, uint32_t *rflags, uint2 *raggs, uint2 *rincls,
+                                               uint32_t *pdone, uint32_t *ticket) {
+    U7 *shp = SM.shp;
+    U7 &sxp = SM.sxp;
+    RefTileSmem &shr_seg = SM.shr_seg;
+    uint32_t &s_tile = SM.tile;
+    uint32_t &s_wait_ok = SM.wait_ok;
     const PlanOp P{A};
     const RefOp R{A};
     const uint32_t tag = level_tag(A);
@@ -2191,7 +2248,7 @@ __global__ void __launch_bounds__(kScanThreads, 6) k_plan_refs(LevelArgs A, uint
                 if (threadIdx.x == 0) {
                     uint32_t ok = 1;
                     const uint32_t r0 = rt * kTile, r1 = min(nr, r0 + kTile) - 1;
-                    const uint32_t k0 = A.ref_node[r0] / kPlanTile, k1 = A.ref_node[r1] / kPlanTile;
+                    const uint32_t k0 = A.ref_node()[r0] / kPlanTile, k1 = A.ref_node()[r1] / kPlanTile;
                     for (uint32_t k = k0; k <= k1 && k < ntn && ok; k++) {
                         for (uint32_t spins = 0; __ldcv(pdone + k) != tag; spins++) {
                             if (spins >= A.spin_limit) {
@@ -2213,6 +2270,15 @@ __global__ void __launch_bounds__(kScanThreads, 6) k_plan_refs(LevelArgs A, uint
             break;
         }
     }
+}
+
+__global__ void __launch_bounds__(kScanThreads, 6) k_plan_refs(LevelArgs A, uint32_t *pflags, U7 *paggs, U7 *pincls,
+                                                            uint32_t *rflags, uint2 *raggs, uint2 *rincls,
+                                                            uint32_t *pdone, uint32_t *ticket) {
+    __shared__ PlanSmem SM;
+    wait_prior_grid();
+    if (level_aborted(A)) return;
+    plan_refs_body(A, SM, pflags, paggs, pincls, rflags, raggs, rincls, pdone, ticket);
 }
 
 // ---------------------------------------------------------------------------
@@ -2750,6 +2816,7 @@ hk_status build_prepare(BuildState &S, const BuildParams &p, uint32_t nt, int sm
     cudaMemset(S.ref_flags, 0, (size_t)S.ref_tiles * 4);
     cudaMemset(S.plan_done, 0, (size_t)S.plan_tiles * 4);
     cudaMemset(S.sub_flags, 0, (size_t)S.sub_tiles * 4);
+
     cudaMemset(S.ctr, 0, sizeof(BuildCounters));
     // these run on the legacy stream, which does not order against the
     // context's own stream: every one is finished before a build may start
@@ -2868,30 +2935,30 @@ cudaError_t build_launch(BuildState &S, const float4 *verts, const uint4 *tris, 
     // allocation, cleaned by the kernel that used them, and zeroed again by
     // build_read_stats after a build that stopped on an error
     if (nt) k_tri_bounds<<<(nt + 255) / 256, 256, 0, st>>>(verts, tris, nt, S.tb_lo, S.tb_hi);
-    A.nx_lo = S.n_lo[0];
-    A.nx_hi = S.n_hi[0];
-    A.nx_info = S.n_info[0];
-    A.refs = S.refs[0];
-    A.ref_node = S.ref_node[0];
+    for (int k = 0; k < 2; k++) {
+        A.lo_buf[k] = S.n_lo[k];
+        A.hi_buf[k] = S.n_hi[k];
+        A.info_buf[k] = S.n_info[k];
+        A.refs_buf[k] = S.refs[k];
+        A.ref_node_buf[k] = S.ref_node[k];
+    }
+    A.level = 0;
     k_root<<<G, 256, 0, st>>>(A, box, nt);
     const bool exact_small = A.learned || A.exact_max >= kWarpExact;
     const uint32_t sub_E = sub_stack_entries(S.p.max_depth);
     const size_t sub_smem = kSubWarps * sub_warp_smem(sub_E);
+    const bool binned_only = !A.learned && A.exact_max == 0;
     for (uint32_t L = 0; L <= S.p.max_depth; L++) {
-        int cur = L & 1, nxt = cur ^ 1;
         A.level = L;
         A.lc = &S.ctr->lvl[L];
         A.nlc = &S.ctr->lvl[L + 1];
-        A.n_lo = S.n_lo[cur];
-        A.n_hi = S.n_hi[cur];
-        A.n_info = S.n_info[cur];
-        A.nx_lo = S.n_lo[nxt];
-        A.nx_hi = S.n_hi[nxt];
-        A.nx_info = S.n_info[nxt];
-        A.refs = S.refs[cur];
-        A.ref_node = S.ref_node[cur];
-        A.nx_refs = S.refs[nxt];
-        A.nx_ref_node = S.ref_node[nxt];
+        if (binned_only) {
+            launch_pdl(k_decide, G * 2, 256, 0, st, A);
+            launch_pdl(k_plan_refs, S.sm_count * 6, kScanThreads, 0, st, A, S.plan_flags,
+                       static_cast<U7 *>(S.plan_agg), static_cast<U7 *>(S.plan_incl), S.ref_flags, S.ref_agg,
+                       S.ref_incl, S.plan_done, &A.lc->plan_ticket);
+            continue;
+        }
         // large (and medium) nodes on the second stream, beside the small
         // nodes (independent nodes; both only add to the level tallies):
         // binned histograms, or the proposer's features, inference and costing

@@ -98,6 +98,7 @@ struct BuildState {
     BuildParams p{};
     uint32_t nt = 0, cap_refs = 0, cap_nodes = 0, cap_level = 0, cap_large = 0, cap_chunks = 0, cap_medium = 0;
     uint32_t alloc_depth = 0;   // max_depth the subtree scratch was sized for
+
     int sm_count = 148;
     bool active = false;        // a built tree is the current tree
     uint32_t last_level = 0;    // lvl[] index holding the final totals
