@@ -334,6 +334,60 @@ __device__ __forceinline__ void hist_ref(uint32_t *H, float4 tlo, float4 thi, fl
     }
 }
 
+// The node's planes p_k (k = 0..31) of each axis in P[a * 32 + k], so the bin
+// corrections read them instead of recomputing them (the same values): one
+// warp (lane k writes plane k of the three axes) or threads 0..95 of a CTA;
+// the caller syncs before reading.
+constexpr uint32_t kPlanes = 3 * kBins;
+__device__ __forceinline__ void node_planes_warp(float *P, float4 blo, float4 bhi) {
+    const uint32_t lane = threadIdx.x & 31u;
+#pragma unroll
+    for (uint32_t a = 0; a < 3; a++) {
+        const float l = c3(blo, a);
+        P[a * 32 + lane] = plane_k(l, __fsub_rn(c3(bhi, a), l), lane);
+    }
+}
+__device__ __forceinline__ void node_planes_cta(float *P, float4 blo, float4 bhi) {
+    if (threadIdx.x < kPlanes) {
+        const uint32_t a = threadIdx.x >> 5, k = threadIdx.x & 31u;
+        const float l = c3(blo, a);
+        P[threadIdx.x] = plane_k(l, __fsub_rn(c3(bhi, a), l), k);
+    }
+}
+
+// bin_interval with the planes of the axis read from Pa
+__device__ __forceinline__ void bin_interval_tab(float lo, float hi, float blo, float inv, const float *Pa, int &b,
+                                                 int &c, bool &on) {
+    b = __float2int_rz(__fmul_rn(__fsub_rn(lo, blo), inv));
+    b = b < 0 ? 0 : (b > (int)kBins - 1 ? (int)kBins - 1 : b);
+    while (b > 0 && lo < Pa[b]) b--;
+    while (b < (int)kBins - 1 && lo >= Pa[b + 1]) b++;
+    c = __float2int_rz(__fmul_rn(__fsub_rn(hi, blo), inv));
+    c = c < 0 ? 0 : (c > (int)kBins - 1 ? (int)kBins - 1 : c);
+    while (c > 0 && hi <= Pa[c]) c--;
+    while (c < (int)kBins - 1 && hi > Pa[c + 1]) c++;
+    on = (lo == hi) && b >= 1 && lo == Pa[b];
+}
+
+// hist_ref with the node's plane table P (node_planes_*)
+__device__ __forceinline__ void hist_ref_tab(uint32_t *H, float4 tlo, float4 thi, float4 blo, float4 bhi, float4 inv3,
+                                             const float *P) {
+#pragma unroll
+    for (uint32_t a = 0; a < 3; a++) {
+        float l = c3(blo, a), h = c3(bhi, a);
+        float ext = __fsub_rn(h, l);
+        if (!(ext > 0.0f)) continue;
+        float inv = c3(inv3, a);
+        float lo = mxf(c3(tlo, a), l), hi = mnf(c3(thi, a), h);
+        int b, c;
+        bool on;
+        bin_interval_tab(lo, hi, l, inv, P + a * 32, b, c, on);
+        atomicAdd(&H[a * 96 + b], 1u);
+        atomicAdd(&H[a * 96 + 32 + c], 1u);
+        if (on) atomicAdd(&H[a * 96 + 64 + b], 1u);
+    }
+}
+
 struct Decision {
     int axis;
     float plane;
@@ -403,17 +457,13 @@ __device__ Decision sah_warp(HistPtr H, float4 blo, float4 bhi, uint32_t cnt, fl
             m_pk = pk;
         }
     }
-    // argmin over (cost, axis, plane)
-    float bc = mc;
-    uint32_t bk = mkey;
-    for (int off = 16; off; off >>= 1) {
-        const float oc = __shfl_xor_sync(0xffffffffu, bc, off);
-        const uint32_t ok = __shfl_xor_sync(0xffffffffu, bk, off);
-        if (oc < bc || (oc == bc && ok < bk)) {
-            bc = oc;
-            bk = ok;
-        }
-    }
+    // argmin over (cost, axis, plane): costs are +0 .. +inf (ct >= 0, ci > 0,
+    // surfaces and counts >= 0; NaN never replaced kInf), so their bit
+    // patterns order as the values do: the least cost, then the least key
+    const uint32_t cbits = __float_as_uint(mc);
+    const uint32_t mbits = __reduce_min_sync(0xffffffffu, cbits);
+    const uint32_t bk = __reduce_min_sync(0xffffffffu, cbits == mbits ? mkey : 0xffffffffu);
+    const float bc = __uint_as_float(mbits);
     Decision best{-1, 0.0f, 0, 0, kInf, 0};
     const uint32_t src = bk & 31u;
     const float pk = __shfl_sync(0xffffffffu, m_pk, src);
@@ -1013,6 +1063,7 @@ __device__ __forceinline__ void finish_large(const LevelArgs &A, uint32_t s, con
 // shared memory of a CTA's large-node work
 struct HistSmem {
     uint32_t H[kHist];
+    float P[kPlanes];
     int last;
 };
 
@@ -1071,6 +1122,7 @@ __device__ __forceinline__ void hist_body(const LevelArgs &A, HistSmem &SH, Exac
         const float4 blo = A.n_lo()[s], bhi = A.n_hi()[s];
         const uint32_t r0 = info.x + ck.y * kChunk, r1 = min(info.x + info.y, r0 + kChunk);
         for (uint32_t i = threadIdx.x; i < kHist; i += blockDim.x) H[i] = 0;
+        node_planes_cta(SH.P, blo, bhi);
         __syncthreads();
         {
             // all of the thread's references and bounds loaded first
@@ -1091,7 +1143,7 @@ __device__ __forceinline__ void hist_body(const LevelArgs &A, HistSmem &SH, Exac
                 }
 #pragma unroll
             for (int k = 0; k < kPer; k++)
-                if (tri[k] != 0xffffffffu) hist_ref(H, tlo[k], thi[k], blo, bhi, inv3);
+                if (tri[k] != 0xffffffffu) hist_ref_tab(H, tlo[k], thi[k], blo, bhi, inv3, SH.P);
         }
         __syncthreads();
         if (info.y <= kChunk) {
@@ -1140,7 +1192,8 @@ __global__ void __launch_bounds__(256, 3) k_hist(LevelArgs A) {
 // binned decision and histogram features are stored for k_learn, which
 // decides it (a node past the row capacity keeps the binned decision).
 template <bool WARP_EXACT, bool LEARNED>
-__device__ __forceinline__ void small_body(const LevelArgs &A, uint32_t (*HS)[kHist], Tally &tally) {
+__device__ __forceinline__ void small_body(const LevelArgs &A, uint32_t (*HS)[kHist], float (*PS)[kPlanes],
+                                           Tally &tally) {
     const uint32_t wib = threadIdx.x >> 5, lane = threadIdx.x & 31u;
     const uint32_t nodes = A.lc->nodes;
     const uint32_t ngroups = (nodes + 7) / 8;
@@ -1166,6 +1219,8 @@ __device__ __forceinline__ void small_body(const LevelArgs &A, uint32_t (*HS)[kH
             d = sah_exact_warp32(A, info, blo, bhi, A.ct, A.ci);
         } else {
             uint32_t *Hw = HS[wib];
+            float *Pw = PS[wib];
+            __syncwarp();   // the previous node's readers are done
             {
                 // 288 counters = 72 16-byte stores
                 uint4 *H4 = reinterpret_cast<uint4 *>(Hw);
@@ -1173,11 +1228,12 @@ __device__ __forceinline__ void small_body(const LevelArgs &A, uint32_t (*HS)[kH
                 H4[lane + 32] = make_uint4(0, 0, 0, 0);
                 if (lane < kHist / 4 - 64) H4[lane + 64] = make_uint4(0, 0, 0, 0);
             }
+            node_planes_warp(Pw, blo, bhi);
             __syncwarp();
             const float4 inv3 = bin_scale(blo, bhi);
             for (uint32_t r = info.x + lane; r < info.x + cnt; r += 32) {
                 const uint32_t tri = A.refs()[r];
-                hist_ref(Hw, A.tb_lo[tri], A.tb_hi[tri], blo, bhi, inv3);
+                hist_ref_tab(Hw, A.tb_lo[tri], A.tb_hi[tri], blo, bhi, inv3, Pw);
             }
             __syncwarp();
             d = sah_warp(Hw, blo, bhi, cnt, A.ct, A.ci);
@@ -1206,11 +1262,12 @@ __device__ __forceinline__ void small_body(const LevelArgs &A, uint32_t (*HS)[kH
 template <bool WARP_EXACT, bool LEARNED>
 __global__ void __launch_bounds__(256, 5) k_small(LevelArgs A) {
     __shared__ __align__(16) uint32_t HS[8][kHist];
+    __shared__ float PS[8][kPlanes];
     __shared__ uint32_t s_tally[kTallies];
     wait_prior_grid();
     if (level_aborted(A)) return;
     Tally tally;
-    small_body<WARP_EXACT, LEARNED>(A, HS, tally);
+    small_body<WARP_EXACT, LEARNED>(A, HS, PS, tally);
     tally_flush(A, tally, s_tally);
 }
 
@@ -1219,7 +1276,10 @@ __global__ void __launch_bounds__(256, 5) k_small(LevelArgs A) {
 // (no second stream, no fork and join per level)
 union DecideSmem {
     HistSmem hist;
-    uint32_t HS[8][kHist];
+    struct {
+        uint32_t HS[8][kHist];
+        float PS[8][kPlanes];
+    } small;
 };
 
 __global__ void __launch_bounds__(256, 4) k_decide(LevelArgs A) {
@@ -1230,7 +1290,7 @@ __global__ void __launch_bounds__(256, 4) k_decide(LevelArgs A) {
     Tally tally;
     hist_body<false>(A, sm.hist, nullptr, tally);
     __syncthreads();
-    small_body<false, false>(A, sm.HS, tally);
+    small_body<false, false>(A, sm.small.HS, sm.small.PS, tally);
     tally_flush(A, tally, s_tally);
 }
 
@@ -2308,9 +2368,11 @@ constexpr int kSubWarps = 8;
 // the root, an even count (the per-warp shared-memory regions stay 16-byte
 // aligned)
 __host__ __device__ constexpr uint32_t sub_stack_entries(uint32_t max_depth) { return (max_depth + 3u) & ~1u; }
-// per warp: the binned histograms, then the stack (cells lo, hi; meta: lane
-// mask, depth, scratch slot; 6 rope words per entry)
-__host__ __device__ constexpr size_t sub_warp_smem(uint32_t entries) { return kHist * 4 + (size_t)72 * entries; }
+// per warp: the binned histograms, the plane table, then the stack (cells lo,
+// hi; meta: lane mask, depth, scratch slot; 6 rope words per entry)
+__host__ __device__ constexpr size_t sub_warp_smem(uint32_t entries) {
+    return kHist * 4 + kPlanes * 4 + (size_t)72 * entries;
+}
 
 // a scratch entry moved to its place: child pairs and leaf starts shifted by
 // the subtree's first node / reference; an empty cell keeps start 0
@@ -2361,7 +2423,8 @@ __global__ void __launch_bounds__(kSubWarps * 32, 4) k_subtree(LevelArgs A, uint
     const uint32_t wib = threadIdx.x >> 5, lane = threadIdx.x & 31u;
     unsigned char *wbase = sub_smem + (size_t)wib * sub_warp_smem(E);
     uint32_t *Hw = reinterpret_cast<uint32_t *>(wbase);
-    float4 *s_lo = reinterpret_cast<float4 *>(wbase + kHist * 4);
+    float *Pw = reinterpret_cast<float *>(wbase + kHist * 4);
+    float4 *s_lo = reinterpret_cast<float4 *>(wbase + kHist * 4 + kPlanes * 4);
     float4 *s_hi = s_lo + E;
     uint4 *s_meta = reinterpret_cast<uint4 *>(s_hi + E);
     uint32_t *s_rope = reinterpret_cast<uint32_t *>(s_meta + E);
@@ -2407,8 +2470,9 @@ __global__ void __launch_bounds__(kSubWarps * 32, 4) k_subtree(LevelArgs A, uint
                     H4[lane] = make_uint4(0, 0, 0, 0);
                     H4[lane + 32] = make_uint4(0, 0, 0, 0);
                     if (lane < kHist / 4 - 64) H4[lane + 64] = make_uint4(0, 0, 0, 0);
+                    node_planes_warp(Pw, lo, hi);
                     __syncwarp();
-                    if (in) hist_ref(Hw, tlo, thi, lo, hi, bin_scale(lo, hi));
+                    if (in) hist_ref_tab(Hw, tlo, thi, lo, hi, bin_scale(lo, hi), Pw);
                     __syncwarp();
                     d = sah_warp(Hw, lo, hi, c, A.ct, A.ci);
                 }
