@@ -316,6 +316,13 @@ def run_ours(args):
         tuned = ctx.autotune(d_rays.data_ptr(), W * H)
         variant = tuned["variant"]
         del d_rays
+    # hk_autotune_build (untimed setup): the builder layout on this scene
+    m0 = frame_mats(sc, 0)
+    if m0 is not None:
+        ctx.transform(m0)
+    else:
+        ctx.precompute()
+    build_tuned = ctx.autotune_build(mode)
     rgba = torch.zeros(W * H, dtype=torch.int32, device="cuda")
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     rays_split = args.split == "rays"
@@ -414,6 +421,7 @@ def run_ours(args):
                            args.mode, ", exact on nodes <= %d refs" % args.exact_max if args.exact_max else ""),
                        "traversal": {v: k for k, v in hk.VARIANTS.items()}[variant],
                        "autotune": tuned,
+                       "build_layout": build_tuned,
                        "graph": "stages launched per frame (row bands)" if rays_split else "one CUDA graph per frame",
                        "l2": "flushed (256 MB write) between frames",
                        "parallelism": ("row bands of every frame over %d GPU(s), framebuffer all_gather" % world)
@@ -498,6 +506,9 @@ def compare_arms(args, sc, device, ref_cost, variant, tuned):
         ctx.set_parts(sc.part_of_vertex, sc.part_center.shape[0])
         rgba = torch.zeros(W * H, dtype=torch.int32, device="cuda")
         with torch.cuda.stream(stream):
+            # the arm's builder layout (hk_autotune_build, untimed setup)
+            ctx.transform(frame_mats(sc, 0))
+            layout = ctx.autotune_build(mode, 3)
             for f in range(args.warmup):
                 ctx.frame(frame_mats(sc, f), sc.camera, sc.lights, W, H, rgba.data_ptr(), mode, variant, True)
             stream.synchronize()
@@ -546,7 +557,9 @@ def compare_arms(args, sc, device, ref_cost, variant, tuned):
                      "build_ms": float(np.median(t_build)), "trace_shade_ms": float(np.median(t_trace)),
                      "sah_cost": cost, "sah_cost_vs_reference": (cost / ref_cost) if ref_cost else None,
                      "build_bytes": build_bytes,
-                     "build_gbs": build_bytes / (float(np.median(t_build)) * 1e-3) / 1e9}
+                     "build_gbs": build_bytes / (float(np.median(t_build)) * 1e-3) / 1e9,
+                     "layout": None if layout is None else {k: layout[k] for k in ("subtree_max", "subtree_depth",
+                                                                                   "level_streams")}}
         if mode == hk.BUILD_LEARNED:
             out[name].update({"learned_nodes": learned_nodes, "fallback_nodes": fallback_nodes})
         ctx.close()

@@ -37,12 +37,22 @@ class Config(C.Structure):
                 ("short_stack", C.c_uint32), ("block_size", C.c_uint32), ("blocks_per_sm", C.c_uint32),
                 ("max_refs", C.c_uint32), ("topk", C.c_uint32), ("fallback_ratio", C.c_float),
                 ("exact_max", C.c_uint32), ("spin_limit", C.c_uint32), ("max_steps", C.c_uint32),
-                ("sah_sample", C.c_uint32), ("subtree_max", C.c_uint32)]
+                ("sah_sample", C.c_uint32), ("subtree_max", C.c_uint32),
+                ("subtree_depth", C.c_uint32), ("level_streams", C.c_uint32)]
 
 
 class TuneResult(C.Structure):
     _fields_ = [("variant", C.c_int), ("block_size", C.c_uint32), ("short_stack", C.c_uint32),
                 ("best_ms", C.c_float), ("default_ms", C.c_float), ("tried", C.c_uint32)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class BuildTuneResult(C.Structure):
+    _fields_ = [("subtree_max", C.c_uint32), ("subtree_depth", C.c_uint32), ("level_streams", C.c_uint32),
+                ("best_ms", C.c_float),
+                ("default_ms", C.c_float), ("tried", C.c_uint32)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -144,6 +154,7 @@ def load(path: str = LIB_PATH):
         "hk_frame_graph_info": [vp, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)],
         "hk_render_noalloc": [vp, vp, vp, u32, f32p, f32p, f32p, u32, u32, u32, C.c_int, vp, vp],
         "hk_autotune": [vp, vp, u32, C.c_char_p, C.POINTER(TuneResult)],
+        "hk_autotune_build": [vp, C.c_int, u32, C.POINTER(BuildTuneResult)],
         "hk_mlp_init": [vp, C.c_uint64],
         "hk_mlp_save": [vp, C.c_char_p],
         "hk_mlp_load": [vp, C.c_char_p],

@@ -180,6 +180,8 @@ hk_status hk_config_default(hk_config *cfg) {
     cfg->exact_max = 0;
     cfg->sah_sample = 5;
     cfg->subtree_max = 32;
+    cfg->subtree_depth = 8;
+    cfg->level_streams = 1;
     return HK_OK;
 }
 
@@ -191,7 +193,7 @@ static hk_status validate_config(const hk_config *c) {
     if (!(c->intersect_cost > 0) || !(c->traverse_cost >= 0)) return HK_E_ILLEGAL_INPUT;
     if (c->topk < 1 || c->topk > 8 || !(c->fallback_ratio >= 0)) return HK_E_ILLEGAL_INPUT;
     if (c->exact_max != 0 && (c->exact_max < 32 || c->exact_max > 1024)) return HK_E_ILLEGAL_INPUT;
-    if (c->subtree_max > 32) return HK_E_ILLEGAL_INPUT;
+    if (c->subtree_max > 32 || c->level_streams > 2) return HK_E_ILLEGAL_INPUT;
     return HK_OK;
 }
 
@@ -755,6 +757,8 @@ static BuildParams build_params(hk_ctx *c, hk_build_mode mode) {
     p.spin_limit = c->cfg.spin_limit;
     p.debug_flags = c->debug_flags;
     p.defer = c->cfg.subtree_max;
+    p.defer_margin = c->cfg.subtree_depth;
+    p.level_streams = c->cfg.level_streams;
     c->build.learn = &c->learn;
     return p;
 }
@@ -1519,6 +1523,58 @@ static std::string tune_key(hk_ctx *c) {
     char buf[256];
     snprintf(buf, sizeof buf, "%s|sm%d|tris2^%u", prop.name, c->sm_count, cls);
     return buf;
+}
+
+// median device time of reps builds after one warm-up build (-1: a build failed)
+static float time_build(hk_ctx *c, hk_build_mode mode, uint32_t reps) {
+    std::vector<float> ts;
+    for (uint32_t r = 0; r < reps + 1; r++) {
+        hk_tree_stats st;
+        if (hk_build(c, mode, &st) != HK_OK) return -1.0f;
+        if (r >= 1) ts.push_back(st.build_ms);
+    }
+    std::sort(ts.begin(), ts.end());
+    return ts[ts.size() / 2];
+}
+
+hk_status hk_autotune_build(hk_ctx *c, hk_build_mode mode, uint32_t reps, hk_build_tune_result *res) {
+    if (!c) return HK_E_ILLEGAL_INPUT;
+    if (mode != HK_BUILD_BINNED && mode != HK_BUILD_LEARNED) return fail(c, HK_E_ILLEGAL_INPUT, "mode");
+    if (c->nt == 0) return fail(c, HK_E_STATE, "no scene");
+    if (reps == 0) reps = 5;
+    cudaSetDevice(c->device);
+    hk_build_tune_result r;
+    memset(&r, 0, sizeof r);
+    r.default_ms = time_build(c, mode, reps);
+    if (r.default_ms < 0) return HK_E_CUDA;
+    r.subtree_max = c->cfg.subtree_max;
+    r.subtree_depth = c->cfg.subtree_depth;
+    r.level_streams = c->cfg.level_streams ? c->cfg.level_streams : 1u;
+    r.best_ms = r.default_ms;
+    const uint32_t cand[][2] = {{0, 0}, {32, 0}, {32, 10}, {32, 8}, {32, 6}};
+    for (const auto &k : cand) {
+        for (uint32_t ls = 1; ls <= 2; ls++) {
+            c->cfg.subtree_max = k[0];
+            c->cfg.subtree_depth = k[1];
+            c->cfg.level_streams = ls;
+            invalidate_graph(c);
+            const float ms = time_build(c, mode, reps);
+            r.tried++;
+            if (ms < 0) return HK_E_CUDA;
+            if (ms < r.best_ms) {
+                r.best_ms = ms;
+                r.subtree_max = k[0];
+                r.subtree_depth = k[1];
+                r.level_streams = ls;
+            }
+        }
+    }
+    c->cfg.subtree_max = r.subtree_max;
+    c->cfg.subtree_depth = r.subtree_depth;
+    c->cfg.level_streams = r.level_streams;
+    invalidate_graph(c);
+    if (res) *res = r;
+    return HK_OK;
 }
 
 hk_status hk_autotune(hk_ctx *c, const float *d_rays8, uint32_t n, const char *cache_path, hk_tune_result *res) {

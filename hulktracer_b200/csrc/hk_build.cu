@@ -534,6 +534,7 @@ struct LevelArgs {
     // depth; d_lo / d_hi: its cell; defer_refs: its references) and built
     // after the levels; 0: none
     uint32_t defer;
+    uint32_t defer_level;      // the first level whose nodes may be deferred
     uint4 *d_root;
     float4 *d_lo, *d_hi;
     uint32_t *defer_refs;
@@ -603,7 +604,9 @@ __device__ __forceinline__ bool is_large(const LevelArgs &A, uint32_t c) {
 // a decidable node of 2..A.defer references roots a deferred subtree
 constexpr uint32_t kDeferMax = 32;   // one reference per lane
 constexpr int kDeferAxis = -2;       // the decision that records a deferred root
-__device__ __forceinline__ bool is_deferred(const LevelArgs &A, uint32_t c) { return c >= 2 && c <= A.defer; }
+__device__ __forceinline__ bool is_deferred(const LevelArgs &A, uint32_t c) {
+    return c >= 2 && c <= A.defer && A.level >= A.defer_level;
+}
 
 // root node + references of level 0 (the counters were zeroed by a memset);
 // a root with more than 256 references is the first large node
@@ -2966,6 +2969,7 @@ cudaError_t build_launch(BuildState &S, const float4 *verts, const uint4 *tris, 
     A.spin_limit = S.p.spin_limit ? S.p.spin_limit : kSpinLimit;
     A.withhold_level = (S.p.debug_flags & 1u) ? 1u : 0xffffffffu;
     A.defer = std::min<uint32_t>(S.p.defer, kDeferMax);
+    A.defer_level = (S.p.defer_margin && S.p.defer_margin < S.p.max_depth) ? S.p.max_depth - S.p.defer_margin : 0u;
     A.d_root = S.d_root;
     A.d_lo = S.d_lo;
     A.d_hi = S.d_hi;
@@ -3011,7 +3015,7 @@ cudaError_t build_launch(BuildState &S, const float4 *verts, const uint4 *tris, 
     const bool exact_small = A.learned || A.exact_max >= kWarpExact;
     const uint32_t sub_E = sub_stack_entries(S.p.max_depth);
     const size_t sub_smem = kSubWarps * sub_warp_smem(sub_E);
-    const bool binned_only = !A.learned && A.exact_max == 0;
+    const bool binned_only = !A.learned && A.exact_max == 0 && S.p.level_streams != 2;
     for (uint32_t L = 0; L <= S.p.max_depth; L++) {
         A.level = L;
         A.lc = &S.ctr->lvl[L];

@@ -25,6 +25,8 @@ struct BuildParams {
     uint32_t spin_limit = 0;    // polls before a bounded wait gives up (0: the default, 4M)
     uint32_t debug_flags = 0;   // test aid, bit 0: plan tile 0 of level 1 withholds its done flag
     uint32_t defer = 32;        // nodes of 2..defer references: subtrees built after the levels (0: none)
+    uint32_t defer_margin = 8;  // ... when within defer_margin levels of max_depth (0: any level)
+    uint32_t level_streams = 1; // binned: 1 = k_decide per level, 2 = k_hist on a second stream beside k_small
 };
 
 // learned-proposer buffers owned by the context (device pointers)

@@ -434,6 +434,13 @@ class Context:
                                        cache_path.encode() if cache_path else None, C.byref(r)))
         return r.as_dict()
 
+    def autotune_build(self, mode=_lib.BUILD_BINNED, reps: int = 5):
+        """hk_autotune_build: the builder layout (subtree_max, subtree_depth)
+        with the fastest builds on the current scene, set in the context."""
+        r = _lib.BuildTuneResult()
+        self._check(self.L.hk_autotune_build(self.h, int(mode), int(reps), C.byref(r)))
+        return r.as_dict()
+
     def ray_counts(self):
         p, sh = C.c_uint64(), C.c_uint64()
         self._check(self.L.hk_get_ray_counts(self.h, C.byref(p), C.byref(sh)))

@@ -136,6 +136,14 @@ typedef struct hk_config {
                                  passes; one warp builds its whole subtree after the
                                  last level (same splits, nodes numbered after the
                                  levels'). 0 = none, at most 32; default 32 */
+    uint32_t subtree_depth;   /* only nodes within subtree_depth levels of max_depth are
+                                 deferred that way (a deferred subtree is one warp's
+                                 serial work, so its depth is bounded); 0 = any depth;
+                                 default 8 */
+    uint32_t level_streams;   /* HK_BUILD_BINNED without exact_max: 1 = one launch per
+                                 level decides the large and the small nodes; 2 = the
+                                 large nodes on a second stream beside the small ones
+                                 (0 = 1) */
 } hk_config;
 
 typedef struct hk_tree_stats {
@@ -481,6 +489,26 @@ typedef struct hk_tune_result {
 } hk_tune_result;
 hk_status hk_autotune(hk_ctx *ctx, const float *d_rays8, uint32_t n, const char *cache_path,
                       hk_tune_result *result);
+/* The builder's layout for the current scene: times builds of `mode`
+ * (HK_BUILD_BINNED or HK_BUILD_LEARNED) with each candidate (subtree_max,
+ * subtree_depth): (0, 0) every node level by level; (32, 0), (32, 10),
+ * (32, 8), (32, 6) deferred subtrees; each with level_streams 1 and 2; takes
+ * the fastest (median of `reps`
+ * builds after one warm-up build; 0 = 5) and writes it into the context's
+ * configuration. The candidates' trees differ only in node numbering: deferred
+ * subtrees pay off on scenes whose small nodes would otherwise add tree
+ * levels, and cost a serial chain on scenes whose small nodes sit in deep
+ * regions. The current tree afterwards is a valid tree of the last
+ * candidate. */
+typedef struct hk_build_tune_result {
+    uint32_t subtree_max;
+    uint32_t subtree_depth;
+    uint32_t level_streams;
+    float best_ms;          /* median build time of the winner */
+    float default_ms;       /* the configuration the context had */
+    uint32_t tried;
+} hk_build_tune_result;
+hk_status hk_autotune_build(hk_ctx *ctx, hk_build_mode mode, uint32_t reps, hk_build_tune_result *result);
 
 /* ---- batching: many scenes, uneven ray batches, one persistent launch ----
  * No reference counterpart (the reference renders one scene per frame). A

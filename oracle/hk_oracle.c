@@ -1754,7 +1754,8 @@ int hko_build_binned(const float *verts, const uint32_t *tris, uint32_t nt, cons
             axis[s] = -1;
             plane[s] = 0.0f;
             if (n->count <= p->leaf_size || n->depth >= p->max_depth) continue;
-            if (n->count >= 2u && n->count <= p->defer) {
+            if (n->count >= 2u && n->count <= p->defer &&
+                (p->defer_margin == 0 || p->defer_margin >= p->max_depth || n->depth >= p->max_depth - p->defer_margin)) {
                 axis[s] = -2;
                 continue;
             }

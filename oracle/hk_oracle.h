@@ -169,6 +169,9 @@ typedef struct {
      * after every level's nodes (the CUDA builder's layout, hk_config
      * subtree_max); 0: every node level by level */
     uint32_t defer;
+    /* M > 0: only nodes at depth >= max_depth - M are deferred (hk_config
+     * subtree_depth); 0: any depth */
+    uint32_t defer_margin;
 } hko_binned_params;
 int hko_build_binned(const float *verts, const uint32_t *tris, uint32_t nt, const float *box,
                      const hko_binned_params *p, uint32_t **nodes_out, uint32_t *nn_out,

@@ -45,7 +45,7 @@ class _BinnedParams(C.Structure):
                 ("leaf_size", C.c_uint32), ("bins", C.c_uint32), ("max_refs", C.c_uint32),
                 ("max_nodes", C.c_uint32), ("exact_max", C.c_uint32), ("learned", C.c_uint32),
                 ("topk", C.c_uint32), ("fallback_ratio", C.c_float), ("proposals", C.c_void_p),
-                ("defer", C.c_uint32)]
+                ("defer", C.c_uint32), ("defer_margin", C.c_uint32)]
 
 
 # reference constants (KDTreeCPU.cpp:17-18, SharedStructs.hpp:16, KDTreeSAH.cpp:317,
@@ -198,13 +198,14 @@ class Oracle:
 
     def build_binned(self, verts, tris, box, ct=1.0, ci=1.5, max_depth=24, leaf_size=4, bins=32,
                      max_refs=None, max_nodes=None, exact_max=0, proposals=None, topk=4, fallback_ratio=1.0,
-                     defer=32):
+                     defer=32, defer_margin=8):
         """The CUDA builder restated. With ``proposals`` (int32[nodes, 8], the
         GPU's proposal log of a learned build) it restates the learned build.
         ``defer`` (hk_config.subtree_max, the CUDA builder's layout) builds the
         subtrees of nodes of 2..defer references depth first after the levels;
         0 numbers every node level by level (the same tree, other node and
-        reference order)."""
+        reference order). ``defer_margin`` (hk_config.subtree_depth): only nodes
+        at depth >= max_depth - defer_margin are deferred (0: any depth)."""
         nt = int(np.asarray(tris).shape[0])
         if max_refs is None:
             max_refs = max(16 * nt, 1024)
@@ -213,7 +214,7 @@ class Oracle:
         prop = None if proposals is None else _c(proposals, np.int32)
         prm = _BinnedParams(ct, ci, max_depth, leaf_size, bins, max_refs, max_nodes, exact_max,
                             0 if prop is None else 1, topk, fallback_ratio,
-                            None if prop is None else prop.ctypes.data, min(int(defer), 32))
+                            None if prop is None else prop.ctypes.data, min(int(defer), 32), int(defer_margin))
         pn, pr = C.POINTER(C.c_uint32)(), C.POINTER(C.c_uint32)()
         nn, nr = C.c_uint32(), C.c_uint32()
         tris = _c(tris, np.uint32)

@@ -51,20 +51,24 @@ def test_build_identical_to_oracle(hk, oracle, which, exact_max):
     assert st["nodes"] == on.shape[0] and st["refs"] == orf.shape[0]
 
 
-@pytest.mark.parametrize("subtree_max", [0, 16])
-def test_subtree_threshold_identical_to_oracle(hk, oracle, subtree_max):
-    """hk_config.subtree_max: no deferred subtrees (every node level by
-    level), and subtrees of nodes of at most 16 references; the GPU tree
-    equals the oracle's with the same threshold."""
+@pytest.mark.parametrize("subtree_max,subtree_depth,streams", [(0, 8, 1), (16, 8, 1), (32, 0, 1), (32, 4, 1),
+                                                                (0, 0, 2), (32, 8, 2)])
+def test_subtree_threshold_identical_to_oracle(hk, oracle, subtree_max, subtree_depth, streams):
+    """hk_config.subtree_max / subtree_depth / level_streams: no deferred
+    subtrees (every node level by level), subtrees of nodes of at most 16
+    references, deferral at any depth, and only in the last 4 levels; the
+    large nodes decided in the small nodes' launch or on a second stream; the
+    GPU tree equals the oracle's with the same rule."""
     sc = small_animated()
     verts, tris, box = sc.verts, sc.tris, sc.scene_box()
-    ctx = hk.Context(subtree_max=subtree_max)
+    ctx = hk.Context(subtree_max=subtree_max, subtree_depth=subtree_depth, level_streams=streams)
     ctx.upload(verts, tris)
     ctx.set_box(box)
     ctx.precompute()
     st = ctx.build()
     cn, cr = ctx.export_compact()
-    on, orf = oracle.build_binned(verts, tris, box, ct=1.0, ci=1.5, max_depth=24, leaf_size=4, defer=subtree_max)
+    on, orf = oracle.build_binned(verts, tris, box, ct=1.0, ci=1.5, max_depth=24, leaf_size=4, defer=subtree_max,
+                                  defer_margin=subtree_depth)
     assert np.array_equal(cn, on) and np.array_equal(cr, orf)
     sub = ctx.subtree_counts()
     assert (sub["roots"] == 0) == (subtree_max == 0)
