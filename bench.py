@@ -64,6 +64,9 @@ def parse():
     ap.add_argument("--weights", default=os.path.join(os.path.dirname(os.path.abspath(__file__)), "hulktracer_b200",
                                                       "weights", "proposer.bin"),
                     help="trained proposer weights (learned mode)")
+    ap.add_argument("--layout", type=int, nargs=3, metavar=("SUBTREE_MAX", "SUBTREE_DEPTH", "LEVEL_STREAMS"),
+                    help="builder layout (hk_config subtree_max, subtree_depth, level_streams) instead of "
+                         "hk_autotune_build")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-compare", action="store_true", help="skip the learned / exact comparison arms")
     ap.add_argument("--cost-frame", type=int, default=17, help="frame whose trees are costed in the comparison")
@@ -322,7 +325,11 @@ def run_ours(args):
         ctx.transform(m0)
     else:
         ctx.precompute()
-    build_tuned = ctx.autotune_build(mode)
+    if args.layout:
+        ctx.set_build_layout(*args.layout)
+        build_tuned = dict(zip(("subtree_max", "subtree_depth", "level_streams"), args.layout), tried=0)
+    else:
+        build_tuned = ctx.autotune_build(mode)
     rgba = torch.zeros(W * H, dtype=torch.int32, device="cuda")
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     rays_split = args.split == "rays"
@@ -508,7 +515,11 @@ def compare_arms(args, sc, device, ref_cost, variant, tuned):
         with torch.cuda.stream(stream):
             # the arm's builder layout (hk_autotune_build, untimed setup)
             ctx.transform(frame_mats(sc, 0))
-            layout = ctx.autotune_build(mode, 3)
+            if args.layout:
+                ctx.set_build_layout(*args.layout)
+                layout = dict(zip(("subtree_max", "subtree_depth", "level_streams"), args.layout))
+            else:
+                layout = ctx.autotune_build(mode, 3)
             for f in range(args.warmup):
                 ctx.frame(frame_mats(sc, f), sc.camera, sc.lights, W, H, rgba.data_ptr(), mode, variant, True)
             stream.synchronize()

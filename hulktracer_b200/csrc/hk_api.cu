@@ -653,6 +653,15 @@ hk_status hk_build_subtree_counts(hk_ctx *c, uint32_t *roots, uint32_t *root_ref
     return HK_OK;
 }
 
+hk_status hk_set_build_layout(hk_ctx *c, uint32_t subtree_max, uint32_t subtree_depth, uint32_t level_streams) {
+    if (!c || subtree_max > 32 || level_streams > 2) return HK_E_ILLEGAL_INPUT;
+    c->cfg.subtree_max = subtree_max;
+    c->cfg.subtree_depth = subtree_depth;
+    c->cfg.level_streams = level_streams;
+    invalidate_graph(c);
+    return HK_OK;
+}
+
 hk_status hk_set_debug_flags(hk_ctx *c, uint32_t flags) {
     if (!c || (flags & ~1u)) return HK_E_ILLEGAL_INPUT;
     c->debug_flags = flags;

@@ -441,6 +441,9 @@ class Context:
         self._check(self.L.hk_autotune_build(self.h, int(mode), int(reps), C.byref(r)))
         return r.as_dict()
 
+    def set_build_layout(self, subtree_max: int, subtree_depth: int, level_streams: int = 1):
+        self._check(self.L.hk_set_build_layout(self.h, int(subtree_max), int(subtree_depth), int(level_streams)))
+
     def ray_counts(self):
         p, sh = C.c_uint64(), C.c_uint64()
         self._check(self.L.hk_get_ray_counts(self.h, C.byref(p), C.byref(sh)))

@@ -180,6 +180,9 @@ hk_status hk_set_stream(hk_ctx *ctx, void *cuda_stream);
  * that wait for it run out of polls (hk_config.spin_limit) and the build
  * returns HK_E_DEVICE_TIMEOUT without hanging; 0 restores normal builds. */
 hk_status hk_set_debug_flags(hk_ctx *ctx, uint32_t flags);
+/* The builder layout of the next builds (hk_config subtree_max <= 32,
+ * subtree_depth, level_streams 0..2), as hk_autotune_build sets it. */
+hk_status hk_set_build_layout(hk_ctx *ctx, uint32_t subtree_max, uint32_t subtree_depth, uint32_t level_streams);
 hk_status hk_synchronize(hk_ctx *ctx);
 
 /* ---- scene (Scene::m_vertices / m_vertexIndices / m_sceneBox) ---- */
