@@ -3021,7 +3021,8 @@ cudaError_t build_launch(BuildState &S, const float4 *verts, const uint4 *tris, 
         A.lc = &S.ctr->lvl[L];
         A.nlc = &S.ctr->lvl[L + 1];
         if (binned_only) {
-            launch_pdl(k_decide, G * 2, 256, 0, st, A);
+            // one wave (four CTAs per SM resident), grid-stride over the work
+            launch_pdl(k_decide, S.sm_count * 4, 256, 0, st, A);
             launch_pdl(k_plan_refs, S.sm_count * 6, kScanThreads, 0, st, A, S.plan_flags,
                        static_cast<U7 *>(S.plan_agg), static_cast<U7 *>(S.plan_incl), S.ref_flags, S.ref_agg,
                        S.ref_incl, S.plan_done, &A.lc->plan_ticket);
@@ -3032,7 +3033,7 @@ cudaError_t build_launch(BuildState &S, const float4 *verts, const uint4 *tris, 
         // binned histograms, or the proposer's features, inference and costing
         cudaEventRecord(S.ev_fork, st);
         cudaStreamWaitEvent(S.aux, S.ev_fork, 0);
-        k_hist<<<G, 256, 0, S.aux>>>(A);
+        k_hist<<<S.sm_count * 3, 256, 0, S.aux>>>(A);   // one wave: three CTAs per SM resident
         if (A.learned) {
             // the proposer's chain on the second stream after the histograms
             // (every proposer row comes from k_hist), beside the small nodes
@@ -3043,11 +3044,11 @@ cudaError_t build_launch(BuildState &S, const float4 *verts, const uint4 *tris, 
         }
         cudaEventRecord(S.ev_join, S.aux);
         if (A.learned) {
-            launch_pdl(k_small<true, true>, G * 2, 256, 0, st, A);
+            launch_pdl(k_small<true, true>, S.sm_count * 5, 256, 0, st, A);
         } else if (A.exact_max >= kWarpExact) {
-            launch_pdl(k_small<true, false>, G * 2, 256, 0, st, A);
+            launch_pdl(k_small<true, false>, S.sm_count * 5, 256, 0, st, A);
         } else {
-            launch_pdl(k_small<false, false>, G * 2, 256, 0, st, A);
+            launch_pdl(k_small<false, false>, S.sm_count * 5, 256, 0, st, A);
         }
         cudaStreamWaitEvent(st, S.ev_join, 0);
         launch_pdl(k_plan_refs, S.sm_count * 6, kScanThreads, 0, st, A, S.plan_flags, static_cast<U7 *>(S.plan_agg),
