@@ -156,6 +156,7 @@ def load(path: str = LIB_PATH):
         "hk_autotune": [vp, vp, u32, C.c_char_p, C.POINTER(TuneResult)],
         "hk_autotune_build": [vp, C.c_int, u32, C.POINTER(BuildTuneResult)],
         "hk_set_build_layout": [vp, u32, u32, u32],
+        "hk_set_trace_config": [vp, u32, u32],
         "hk_mlp_init": [vp, C.c_uint64],
         "hk_mlp_save": [vp, C.c_char_p],
         "hk_mlp_load": [vp, C.c_char_p],

@@ -662,6 +662,16 @@ hk_status hk_set_build_layout(hk_ctx *c, uint32_t subtree_max, uint32_t subtree_
     return HK_OK;
 }
 
+hk_status hk_set_trace_config(hk_ctx *c, uint32_t block_size, uint32_t short_stack) {
+    if (!c || block_size < 32 || block_size > kTraceMaxBlock || (block_size % 32) || short_stack < 1 ||
+        short_stack > 16)
+        return HK_E_ILLEGAL_INPUT;
+    c->cfg.block_size = block_size;
+    c->cfg.short_stack = short_stack;
+    invalidate_graph(c);
+    return HK_OK;
+}
+
 hk_status hk_set_debug_flags(hk_ctx *c, uint32_t flags) {
     if (!c || (flags & ~1u)) return HK_E_ILLEGAL_INPUT;
     c->debug_flags = flags;

@@ -444,6 +444,9 @@ class Context:
     def set_build_layout(self, subtree_max: int, subtree_depth: int, level_streams: int = 1):
         self._check(self.L.hk_set_build_layout(self.h, int(subtree_max), int(subtree_depth), int(level_streams)))
 
+    def set_trace_config(self, block_size: int, short_stack: int):
+        self._check(self.L.hk_set_trace_config(self.h, int(block_size), int(short_stack)))
+
     def ray_counts(self):
         p, sh = C.c_uint64(), C.c_uint64()
         self._check(self.L.hk_get_ray_counts(self.h, C.byref(p), C.byref(sh)))

@@ -229,19 +229,45 @@ def batch_case(a):
     from hulktracer_b200 import scenes
     t0 = time.time()
     sets = scenes.batch_scenes(n_scenes=a.scenes, tris=tuple(a.tris), rays=tuple(a.rays))
+    rays = [scenes.incoherent_rays(sc, nr, seed=1000 + i) for i, (sc, nr) in enumerate(sets)]
     ctx = hk.Context()
     batch = hk.engine.Batch(ctx)
-    rays, offsets = [], [0]
+    offsets = [0]
     for i, (sc, nr) in enumerate(sets):
         batch.add_scene(sc.verts, sc.tris)
-        rays.append(scenes.incoherent_rays(sc, nr, seed=1000 + i))
         offsets.append(offsets[-1] + nr)
     allr = np.concatenate(rays)
     n = allr.shape[0]
     d_rays = torch.from_numpy(allr).cuda()
     d_hits = torch.zeros(2 * n, dtype=torch.int32, device="cuda")
     setup_s = time.time() - t0
-    v = hk.VARIANTS[a.variant]
+    tuned, cfg = None, {}
+    if a.variant == "auto":
+        # the batch launch itself timed for each candidate (a configuration
+        # tuned on one scene does not carry over to the whole batch): variant,
+        # block size, short-stack depth; the fastest is kept
+        t1 = time.time()
+        cands = [(vn, bs, ss) for vn in ("ropes", "shortstack", "fullstack", "restart_early")
+                 for bs in (64, 128, 256) for ss in ((4, 6, 8) if vn == "shortstack" else (6,))]
+        best = None
+        for vn, bs, ss in cands:
+            ctx.set_trace_config(bs, ss)
+            batch.trace_device(d_rays.data_ptr(), offsets, d_hits.data_ptr(), hk.VARIANTS[vn])
+            ts = []
+            for _ in range(2):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                batch.trace_device(d_rays.data_ptr(), offsets, d_hits.data_ptr(), hk.VARIANTS[vn])
+                e1.record()
+                torch.cuda.synchronize()
+                ts.append(e0.elapsed_time(e1))
+            if best is None or min(ts) < best[0]:
+                best = (min(ts), vn, bs, ss)
+        tuned = {"variant": best[1], "block_size": best[2], "short_stack": best[3], "best_ms": best[0],
+                 "tried": len(cands), "tune_s": round(time.time() - t1, 1)}
+        cfg = {"block_size": best[2], "short_stack": best[3]}
+        ctx.set_trace_config(best[2], best[3])
+    v = hk.VARIANTS[tuned["variant"]] if tuned else hk.VARIANTS[a.variant]
     for _ in range(2):
         batch.trace_device(d_rays.data_ptr(), offsets, d_hits.data_ptr(), v)
     torch.cuda.synchronize()
@@ -259,7 +285,7 @@ def batch_case(a):
     # one launch per scene, same rays (each scene's own context and tree)
     single = []
     for i, (sc, nr) in enumerate(sets):
-        c = hk.Context()
+        c = hk.Context(**cfg)
         c.upload(sc.verts, sc.tris)
         c.precompute()
         c.build()
@@ -278,7 +304,7 @@ def batch_case(a):
         run_single()
         ts.append((time.perf_counter() - t1) * 1000.0)
     out = {"scenes": len(sets), "tris_total": int(sum(sc.ntris for sc, _ in sets)), "rays": int(n),
-           "variant": a.variant, "batched_ms": t, "batched_mrays_s": n / t / 1e3,
+           "variant": {x: k for k, x in hk.VARIANTS.items()}[v], "autotune": tuned, "batched_ms": t, "batched_mrays_s": n / t / 1e3,
            "scene_done_ms_p50": float(np.percentile(per, 50)), "scene_done_ms_p99": float(np.percentile(per, 99)),
            "per_scene_launches_ms": float(np.median(ts)), "per_scene_mrays_s": n / float(np.median(ts)) / 1e3,
            "setup_s": round(setup_s, 1)}

@@ -183,6 +183,10 @@ hk_status hk_set_debug_flags(hk_ctx *ctx, uint32_t flags);
 /* The builder layout of the next builds (hk_config subtree_max <= 32,
  * subtree_depth, level_streams 0..2), as hk_autotune_build sets it. */
 hk_status hk_set_build_layout(hk_ctx *ctx, uint32_t subtree_max, uint32_t subtree_depth, uint32_t level_streams);
+/* The traversal launch configuration of the next traces (hk_config
+ * block_size, a multiple of 32 up to 256, and short_stack 1..16), as
+ * hk_autotune sets it; batches of the context take it too. */
+hk_status hk_set_trace_config(hk_ctx *ctx, uint32_t block_size, uint32_t short_stack);
 hk_status hk_synchronize(hk_ctx *ctx);
 
 /* ---- scene (Scene::m_vertices / m_vertexIndices / m_sceneBox) ---- */

@@ -55,3 +55,30 @@ def test_autotune_build_layout(hk, oracle):
     assert abs(ctx.tree_cost(1.0, 1.5) - cost0) <= 1e-6 * cost0
     assert st["nodes"] == on.shape[0]
     ctx.close()
+
+
+def test_set_trace_and_build_config(hk):
+    """hk_set_trace_config / hk_set_build_layout: invalid values are refused
+    with HK_E_ILLEGAL_INPUT; valid ones change the launches, not the hits."""
+    from hulktracer_b200._lib import HkError
+    sc = scenes.animated_parts(n_parts=6, width=96, height=64)
+    ctx = hk.Context()
+    ctx.upload(sc.verts, sc.tris)
+    ctx.precompute()
+    ctx.build()
+    rays = ctx.camera_rays(sc.camera, 96, 64)
+    ref = ctx.trace(rays, hk.SHORTSTACK)
+    for bad in ((48, 6), (512, 6), (128, 0), (128, 17)):
+        with pytest.raises(HkError) as e:
+            ctx.set_trace_config(*bad)
+        assert e.value.status == 4
+    with pytest.raises(HkError):
+        ctx.set_build_layout(33, 0, 1)
+    ctx.set_trace_config(64, 4)
+    h = ctx.trace(rays, hk.SHORTSTACK)
+    assert np.array_equal(h["tri"], ref["tri"]) and np.array_equal(h["t"], ref["t"])
+    ctx.set_build_layout(0, 0, 2)
+    ctx.build()
+    h = ctx.trace(rays, hk.SHORTSTACK)
+    assert np.array_equal(h["tri"], ref["tri"]) and np.array_equal(h["t"], ref["t"])
+    ctx.close()
