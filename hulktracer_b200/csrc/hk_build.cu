@@ -1,9 +1,14 @@
 // hk_build.cu -- GPU KD-tree builder: exact binned SAH (sm_100a).
 //
-// Breadth-first and level-synchronous; three launches per level (four with
-// the learned proposer). Splits are searched over 32 bins per axis, or, with
-// exact_max (32..1024), over every clipped reference bound for nodes of at
-// most exact_max references (one warp in registers up to 32, one CTA above):
+// Breadth-first and level-synchronous for nodes of more than 32 references:
+// two launches per level in the binned mode (k_decide, k_plan_refs), three
+// with exact_max or the proposer (k_hist on a second stream beside k_small,
+// then k_plan_refs; the proposer adds its chain after k_hist); smaller nodes
+// are deferred subtrees (below; hk_config subtree_max / subtree_depth /
+// level_streams choose the layout). Splits are searched over 32 bins per
+// axis, or, with exact_max (32..1024), over every clipped reference bound for
+// nodes of at most exact_max references (one warp in registers up to 32, one
+// CTA above):
 //   work      large nodes (> 256 references): one CTA per chunk of 1024
 //             references builds shared-memory histograms (3 axes x {lo bin,
 //             hi bin, flat-on-plane}) of the clipped reference bounds and
