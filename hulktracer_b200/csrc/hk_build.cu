@@ -41,7 +41,8 @@
 //             node's references a lane mask, the same SAH), a scan over the
 //             subtrees' sizes places them after the levels' nodes and leaf
 //             references, and a last pass moves them there. On the 200k-triangle
-//             animated frame 94% of the split decisions are taken this way.
+//             animated frame, deferring at any depth, 94% of the split
+//             decisions are taken this way.
 // Every kernel reads its work size from device memory, so the whole build is
 // a fixed launch sequence (graph-capturable, no host round trips). Look-back
 // waits are bounded: a wait that runs out sets an error bit and the build
