@@ -51,14 +51,17 @@ def frame_verts(hk, sc, frame):
     return v, box
 
 
-def check_tree(hk, oracle, verts, tris, box, exact_max):
-    c = hk.Context(exact_max=exact_max)
+def check_tree(hk, oracle, verts, tris, box, exact_max, layout=(32, 8, 1)):
+    """The GPU tree with builder layout (subtree_max, subtree_depth,
+    level_streams) equals the oracle's with the same layout."""
+    c = hk.Context(exact_max=exact_max, subtree_max=layout[0], subtree_depth=layout[1], level_streams=layout[2])
     c.upload(verts, tris)
     c.set_box(box)
     c.precompute()
     st = c.build()
     gn, gr = c.export_compact()
-    on, orf = oracle.build_binned(verts, tris, box, ct=CT, ci=CI, max_depth=24, leaf_size=4, exact_max=exact_max)
+    on, orf = oracle.build_binned(verts, tris, box, ct=CT, ci=CI, max_depth=24, leaf_size=4, exact_max=exact_max,
+                                  defer=layout[0], defer_margin=layout[1])
     assert st["capacity_hit"] == 0
     assert gn.shape == on.shape and gr.shape == orf.shape
     assert np.array_equal(gn, on) and np.array_equal(gr, orf)
@@ -76,6 +79,15 @@ def hits_equal(h, ids, t):
 def test_animated_full_size_tree_equals_oracle(hk, oracle, animated, frame, exact_max):
     v, box = frame_verts(hk, animated, frame)
     check_tree(hk, oracle, v, animated.tris, box, exact_max).close()
+
+
+@pytest.mark.parametrize("layout", [(32, 0, 1), (0, 0, 2)])
+def test_animated_full_size_tree_layouts(hk, oracle, animated, layout):
+    """The layouts the builder autotuner picks for this scene (deferred
+    subtrees at any depth) and for the BART scenes (level by level, large
+    nodes on a second stream), at full size."""
+    v, box = frame_verts(hk, animated, 17)
+    check_tree(hk, oracle, v, animated.tris, box, 0, layout).close()
 
 
 @pytest.mark.skipif(not HAVE_REF, reason="compiled reference not built")
