@@ -634,7 +634,8 @@ def trace_roofline(ctx, sc, stream, variant):
     out = {"kernel": "k_trace primary rays", "bound": "hbm", "achieved": achieved, "peak": peak,
            "peak_source": src, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
            "traffic_source": (prof_rel + " (dram__bytes_read.sum + dram__bytes_write.sum of one ncu capture of "
-                              "the same kernel, workload and tree)") if traffic is not None else None,
+                              "the same kernel and workload; the file names the tree's layout)")
+           if traffic is not None else None,
            "launch_ms": t * 1000.0, "rays_per_launch": n, "bytes_per_ray": b_ray,
            "l2": "flushed (256 MB write) before every timed launch",
            "per_ray": {"nodes": n_node, "refs": n_ref, "tris": n_tri}, "mrays_per_s": n / t / 1e6}

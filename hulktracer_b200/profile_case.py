@@ -50,6 +50,8 @@ def main():
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--weights", default=os.path.join(ROOT, "hulktracer_b200", "weights", "proposer.bin"))
     ap.add_argument("--exact-max", type=int, default=0, help="exact SAH on nodes of at most this many refs")
+    ap.add_argument("--layout", type=int, nargs=3, metavar=("SUBTREE_MAX", "SUBTREE_DEPTH", "LEVEL_STREAMS"),
+                    help="builder layout (hk_set_build_layout) instead of the library default")
     a = ap.parse_args()
     if a.case == "batch":
         batch_case(a)
@@ -63,6 +65,8 @@ def main():
     ctx = hk.Context(exact_max=a.exact_max, **(resort if a.mode == "resort" else {}))
     if a.mode == "learned":
         ctx.mlp_load(a.weights)
+    if a.layout:
+        ctx.set_build_layout(*a.layout)
     ctx.upload(sc.verts, sc.tris)
     ctx.set_parts(sc.part_of_vertex, sc.part_center.shape[0])
     ctx.transform(scenes.part_matrices(sc, 1))
