@@ -618,8 +618,9 @@ def trace_roofline(ctx, sc, stream, variant):
     del flush
     peak, src = measured_peak()
     achieved = n * b_ray / t / 1e9
-    # DRAM bytes of one launch from the committed ncu summary of the same
-    # kernel, workload and tree (dram__bytes_read.sum + dram__bytes_write.sum)
+    # DRAM and L2 bytes of one launch from the committed ncu summary of the
+    # same kernel and workload (dram__bytes_read.sum + dram__bytes_write.sum,
+    # lts__t_sectors.sum x 32); the summary names its tree's builder layout
     traffic = l2_bytes = None
     vname = {v: k for k, v in hk.VARIANTS.items()}.get(variant, "")
     prof_rel = os.path.join("profiles", "k_trace_%s_%s_primary.md" % (vname, traffic_tag(sc)))
