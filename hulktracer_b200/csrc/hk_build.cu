@@ -1429,7 +1429,6 @@ __global__ void __launch_bounds__(256, 1) k_learn(LevelArgs A) {
     if (level_aborted(A)) return;
     const uint32_t rows = min(A.lc->n_learn, A.cap_learn);
     if (blockIdx.x * kRows >= rows) return;   // no tile: no TMEM taken (the CTA takes part in no barrier)
-    const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
     const TileSmem S = tile_smem(learn_smem);
     const TcSmem T = tc_smem(learn_smem);
     uint32_t tmem = 0, g = 0;
@@ -1442,62 +1441,59 @@ __global__ void __launch_bounds__(256, 1) k_learn(LevelArgs A) {
         } else {
             tile_forward(A.mlp, A.feat, row0, rows, S);
         }
-        // the warp's rows are rr = wib + 8 q: lane q looks up row q's node
-        // first (the axes of zero extent have no valid bin), all at once
-        uint32_t my_slot = 0, my_axes = 0, my_cidx = 0;
-        {
-            const uint32_t rr = wib + 8u * lane;
-            if (lane < kRows / 8 && row0 + rr < rows) {
-                my_slot = A.learn_slot[row0 + rr];
-                const float4 blo = A.n_lo()[my_slot], bhi = A.n_hi()[my_slot];
+        // one thread per row (rr = threadIdx.x): the row's candidates are the
+        // bins of its node's axes of nonzero extent, a NaN logit counting as
+        // -inf; the k best by (logit, then the lower index) are kept in a
+        // sorted list of keys, key = (the logit's bits in an order-preserving
+        // unsigned form) << 32 | (95 - index), so that a larger key is the
+        // better candidate and no two keys are equal; an empty slot holds 0,
+        // below every candidate's key (-inf maps to 0x007fffff)
+        constexpr uint32_t kStride = TC ? kTcLogitStride : (uint32_t)kMlpOut;
+        const uint32_t rr = threadIdx.x;
+        if (rr < kRows && row0 + rr < rows) {
+            const uint32_t row = row0 + rr;
+            const uint32_t slot = A.learn_slot[row];
+            const float4 blo = A.n_lo()[slot], bhi = A.n_hi()[slot];
+            const float *Lg = logits + rr * kStride;
+            uint64_t top[kLearnMaxK];
 #pragma unroll
-                for (int j = 0; j < 3; j++)
-                    if (__fsub_rn(c3(bhi, j), c3(blo, j)) > 0.0f) my_axes |= 1u << j;
-                if (A.prop_log) my_cidx = A.n_info()[my_slot].z;
-            }
-        }
-        for (uint32_t rr = wib; rr < kRows && row0 + rr < rows; rr += 8) {
-            const uint32_t row = row0 + rr, q = rr >> 3;
-            const uint32_t axes = __shfl_sync(0xffffffffu, my_axes, (int)q);
-            const uint32_t cidx = __shfl_sync(0xffffffffu, my_cidx, (int)q);
-            const float *Lg = logits + rr * kMlpOut;
-            float v[3];
+            for (int i = 0; i < kLearnMaxK; i++) top[i] = 0;
 #pragma unroll
-            for (int j = 0; j < 3; j++) {
-                const float x = Lg[32 * j + lane];
-                v[j] = ((axes >> j) & 1u) ? (x == x ? x : -INFINITY) : NAN;
+            for (uint32_t j = 0; j < 3; j++) {
+                if (!(__fsub_rn(c3(bhi, j), c3(blo, j)) > 0.0f)) continue;
+#pragma unroll 8
+                for (uint32_t k = 0; k < 32; k++) {
+                    const uint32_t c = 32u * j + k;
+                    float x = Lg[c];
+                    if (x != x) x = -INFINITY;
+                    if (x == 0.0f) x = 0.0f;   // -0 ties with +0, as the values compare
+                    const uint32_t u = __float_as_uint(x);
+                    const uint32_t ord = (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+                    uint64_t key = ((uint64_t)ord << 32) | (uint64_t)(95u - c);
+                    if (key <= top[kLearnMaxK - 1]) continue;
+#pragma unroll
+                    for (int i = 0; i < kLearnMaxK; i++)
+                        if (key > top[i]) {
+                            const uint64_t t = top[i];
+                            top[i] = key;
+                            key = t;
+                        }
+                }
             }
             uint32_t packed[2] = {0xffffffffu, 0xffffffffu};
-            for (uint32_t r = 0; r < K; r++) {
-                float bv = NAN;
-                int bc = 1 << 30;
 #pragma unroll
-                for (int j = 0; j < 3; j++)
-                    if (v[j] == v[j] && (bv != bv || v[j] > bv)) {
-                        bv = v[j];
-                        bc = (int)lane + 32 * j;
-                    }
-                for (int o = 16; o; o >>= 1) {
-                    const float ov = __shfl_xor_sync(0xffffffffu, bv, o);
-                    const int oc = __shfl_xor_sync(0xffffffffu, bc, o);
-                    if ((ov == ov) && (bv != bv || ov > bv || (ov == bv && oc < bc))) {
-                        bv = ov;
-                        bc = oc;
-                    }
+            for (uint32_t r = 0; r < (uint32_t)kLearnMaxK; r++)
+                if (r < K && top[r] != 0) {
+                    const uint32_t bc = 95u - (uint32_t)(top[r] & 0xffffffffu), sh = 8u * (r & 3u);
+                    packed[r >> 2] = (packed[r >> 2] & ~(0xffu << sh)) | (bc << sh);
                 }
-                if (bv != bv) break;   // no valid bin left (uniform across the warp)
-#pragma unroll
-                for (int j = 0; j < 3; j++)
-                    if (bc == (int)lane + 32 * j) v[j] = NAN;
-                const uint32_t sh = 8u * (r & 3u);
-                packed[r >> 2] = (packed[r >> 2] & ~(0xffu << sh)) | ((uint32_t)bc << sh);
-            }
-            if (lane == 0) {
-                A.learn_prop[row] = make_uint2(packed[0], packed[1]);
-                if (A.prop_log && cidx < A.cap_nodes)
+            A.learn_prop[row] = make_uint2(packed[0], packed[1]);
+            if (A.prop_log) {
+                const uint32_t cidx = A.n_info()[slot].z;
+                if (cidx < A.cap_nodes)
                     for (uint32_t r = 0; r < 8; r++) {
-                        const uint32_t b = (packed[r >> 2] >> (8u * (r & 3u))) & 0xffu;
-                        A.prop_log[(size_t)cidx * 8 + r] = b == 0xffu ? -1 : (int32_t)b;
+                        const uint32_t bb = (packed[r >> 2] >> (8u * (r & 3u))) & 0xffu;
+                        A.prop_log[(size_t)cidx * 8 + r] = bb == 0xffu ? -1 : (int32_t)bb;
                     }
             }
         }
@@ -2772,9 +2768,12 @@ void build_release(BuildState &S) {
     S.cap_defer = S.cap_sc_nodes = S.cap_sc_refs = S.sub_tiles = 0;
     if (S.ev_fork) cudaEventDestroy(S.ev_fork);
     if (S.ev_join) cudaEventDestroy(S.ev_join);
+    if (S.ev_learn) cudaEventDestroy(S.ev_learn);
+    if (S.ev_join2) cudaEventDestroy(S.ev_join2);
     if (S.aux) cudaStreamDestroy(S.aux);
-    S.ev_fork = S.ev_join = nullptr;
-    S.aux = nullptr;
+    if (S.aux2) cudaStreamDestroy(S.aux2);
+    S.ev_fork = S.ev_join = S.ev_learn = S.ev_join2 = nullptr;
+    S.aux = S.aux2 = nullptr;
     S.nt = S.cap_refs = S.cap_nodes = S.cap_level = 0;
     S.plan_tiles = S.ref_tiles = 0;
     S.active = false;
@@ -2877,6 +2876,9 @@ hk_status build_prepare(BuildState &S, const BuildParams &p, uint32_t nt, int sm
     bad |= cudaStreamCreateWithFlags(&S.aux, cudaStreamNonBlocking) != cudaSuccess;
     bad |= cudaEventCreateWithFlags(&S.ev_fork, cudaEventDisableTiming) != cudaSuccess;
     bad |= cudaEventCreateWithFlags(&S.ev_join, cudaEventDisableTiming) != cudaSuccess;
+    bad |= cudaStreamCreateWithFlags(&S.aux2, cudaStreamNonBlocking) != cudaSuccess;
+    bad |= cudaEventCreateWithFlags(&S.ev_learn, cudaEventDisableTiming) != cudaSuccess;
+    bad |= cudaEventCreateWithFlags(&S.ev_join2, cudaEventDisableTiming) != cudaSuccess;
     if (bad) {
         build_release(S);
         return HK_E_ALLOC;
@@ -3045,8 +3047,14 @@ cudaError_t build_launch(BuildState &S, const float4 *verts, const uint4 *tris, 
             // (every proposer row comes from k_hist), beside the small nodes
             if (mlp_use_tcgen05() && A.mlp.tcw) launch_pdl(k_learn<true>, S.sm_count, 256, kTcSmem, S.aux, A);
             else launch_pdl(k_learn<false>, S.sm_count, 256, kTileSmem, S.aux, A);
+            // the two costing kernels take disjoint rows (by reference count)
+            // and only add to the tallies: the warp-costed rows on a third
+            // stream, beside the CTA-costed ones
+            cudaEventRecord(S.ev_learn, S.aux);
+            cudaStreamWaitEvent(S.aux2, S.ev_learn, 0);
+            k_refine_warp<<<S.sm_count * 3, 256, kRefineWarpSmem, S.aux2>>>(A);
+            cudaEventRecord(S.ev_join2, S.aux2);
             launch_pdl(k_refine_cta, S.sm_count * 8, kRefineThreads, kRefineSmem, S.aux, A);
-            launch_pdl(k_refine_warp, S.sm_count * 3, 256, kRefineWarpSmem, S.aux, A);
         }
         cudaEventRecord(S.ev_join, S.aux);
         if (A.learned) {
@@ -3057,6 +3065,7 @@ cudaError_t build_launch(BuildState &S, const float4 *verts, const uint4 *tris, 
             launch_pdl(k_small<false, false>, S.sm_count * 5, 256, 0, st, A);
         }
         cudaStreamWaitEvent(st, S.ev_join, 0);
+        if (A.learned) cudaStreamWaitEvent(st, S.ev_join2, 0);
         launch_pdl(k_plan_refs, S.sm_count * 6, kScanThreads, 0, st, A, S.plan_flags, static_cast<U7 *>(S.plan_agg),
                    static_cast<U7 *>(S.plan_incl), S.ref_flags, S.ref_agg, S.ref_incl, S.plan_done,
                    &A.lc->plan_ticket);

@@ -131,9 +131,10 @@ struct BuildState {
     uint2 *ref_agg = nullptr, *ref_incl = nullptr;
     uint32_t plan_tiles = 0, ref_tiles = 0;
     uint32_t *epoch = nullptr;                   // build counter (scan flag tags)
-    // second stream: large-node histograms run beside the small-node work
-    cudaStream_t aux = nullptr;
-    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    // second stream: large-node histograms run beside the small-node work;
+    // third stream: the proposer's warp-costed rows beside its CTA-costed ones
+    cudaStream_t aux = nullptr, aux2 = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_learn = nullptr, ev_join2 = nullptr;
 
     BuildCounters *ctr = nullptr;
     uint32_t *err = nullptr;

@@ -269,8 +269,8 @@ __global__ void __launch_bounds__(256, 1)
     for (uint32_t row0 = blockIdx.x * kTcRows; row0 < rows; row0 += gridDim.x * kTcRows) {
         if (!tc_tile_forward(M, X, row0, rows, S, tmem, g, err)) break;
         for (uint32_t i = threadIdx.x; i < (uint32_t)kTcRows * kMlpOut; i += blockDim.x) {
-            const uint32_t r = row0 + i / kMlpOut;
-            if (r < rows) logits[(size_t)r * kMlpOut + i % kMlpOut] = S.logits[i];
+            const uint32_t m = i / kMlpOut, j = i % kMlpOut, r = row0 + m;
+            if (r < rows) logits[(size_t)r * kMlpOut + j] = S.logits[m * kTcLogitStride + j];
         }
         __syncthreads();
     }

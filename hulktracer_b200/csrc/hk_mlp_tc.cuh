@@ -48,7 +48,10 @@ constexpr uint32_t kTcBiasN = 3 * kMlpHid + kMlpOut;
 constexpr size_t kTcSmem = kTcBiasOff + kTcBiasN * 4;
 constexpr uint32_t kTcSpin = 1u << 20;                       // try_wait attempts before giving up
 constexpr uint32_t kErrTensorWait = 32u;                     // *err bit: a tensor-core pipeline wait ran out
-static_assert((size_t)kTcRows * kMlpOut * 4 <= kTcNBuf * kTcBBytes, "logits overlay the weight buffers");
+// row stride of the tile's logits in shared memory: one float more than a row,
+// so that lanes holding consecutive rows touch different banks
+constexpr uint32_t kTcLogitStride = (uint32_t)kMlpOut + 1u;
+static_assert((size_t)kTcRows * kTcLogitStride * 4 <= kTcNBuf * kTcBBytes, "logits overlay the weight buffers");
 static_assert(kTcSmem <= 227 * 1024, "shared memory of one CTA");
 
 __host__ __device__ constexpr uint32_t tc_layer_n(int l) { return l == 3 ? (uint32_t)kMlpOut : (uint32_t)kMlpHid; }
@@ -132,7 +135,7 @@ __device__ __forceinline__ void tc_fence_async_smem() { asm volatile("fence.prox
 struct TcSmem {
     unsigned char *A;      // activations (canonical layout)
     unsigned char *B0;     // weight chunk ring: buffer b at B0 + b * kTcBBytes
-    float *logits;         // kTcRows x 96, over the weight buffers after the last layer
+    float *logits;         // kTcRows rows of kTcLogitStride, over the weight buffers after the last layer
     uint32_t bars;         // copy mbarriers (8 bytes each), then the MMA mbarriers
     uint32_t *tmem_addr;
     float *bias;           // b1 | b2 | b3 | b4, copied at the start of every tile
@@ -188,10 +191,10 @@ __device__ __forceinline__ uint32_t tc_a_off(uint32_t m, uint32_t k) {
 }
 
 // The network on rows row0 .. row0 + 127 of X (rows at or past `rows` are
-// zero); logits in S.logits[r][96] on return. `g` counts the chunks every
-// earlier call of this CTA consumed: chunk g + q of the CTA goes to buffer
-// (g + q) % 4 and is that buffer's use (g + q) / 4 (the mbarrier phase
-// parity); it advances by kTcChunks. All 256 threads call it. Returns false
+// zero); logits in S.logits[r * kTcLogitStride + j] on return. `g` counts
+// the chunks every earlier call of this CTA consumed: chunk g + q of the CTA
+// goes to buffer (g + q) % 4 and is that buffer's use (g + q) / 4 (the
+// mbarrier phase parity); it advances by kTcChunks. All 256 threads call it. Returns false
 // (on every thread) when a wait ran out; *err then holds kErrTensorWait.
 __device__ __forceinline__ bool tc_tile_forward(const MlpDevice &M, const float *__restrict__ X, uint32_t row0,
                                                 uint32_t rows, const TcSmem &S, uint32_t tmem, uint32_t &g,
@@ -316,7 +319,7 @@ __device__ __forceinline__ bool tc_tile_forward(const MlpDevice &M, const float 
                 *reinterpret_cast<uint4 *>(S.A + tc_a_off(m, c + 8)) = make_uint4(w[4], w[5], w[6], w[7]);
             } else {
 #pragma unroll
-                for (int j = 0; j < 16; j++) S.logits[m * kMlpOut + c + j] = __uint_as_float(r[j]) + bl[c + j];
+                for (int j = 0; j < 16; j++) S.logits[m * kTcLogitStride + c + j] = __uint_as_float(r[j]) + bl[c + j];
             }
         }
         tc_fence_async_smem();
