@@ -53,6 +53,7 @@
 // written with explicit IEEE round-to-nearest intrinsics for that reason.
 #include <algorithm>
 #include <cstdio>
+#include <type_traits>
 
 #include "hk_build.h"
 #include "hk_common.cuh"
@@ -1441,13 +1442,13 @@ __global__ void __launch_bounds__(256, 1) k_learn(LevelArgs A) {
         } else {
             tile_forward(A.mlp, A.feat, row0, rows, S);
         }
-        // one thread per row (rr = threadIdx.x): the row's candidates are the
+        // one thread per row (rr = threadIdx.x): a row's candidates are the
         // bins of its node's axes of nonzero extent, a NaN logit counting as
-        // -inf; the k best by (logit, then the lower index) are kept in a
-        // sorted list of keys, key = (the logit's bits in an order-preserving
-        // unsigned form) << 32 | (95 - index), so that a larger key is the
-        // better candidate and no two keys are equal; an empty slot holds 0,
-        // below every candidate's key (-inf maps to 0x007fffff)
+        // -inf, taken as the logits' bits in an order-preserving unsigned form
+        // (-inf maps to 0x007fffff; an empty slot holds 0, below every
+        // candidate). The candidates pass in index order through a sorted
+        // list of NS slots, a candidate moving ahead of a slot only when its
+        // key is strictly greater: the k best by (logit, then the lower index).
         constexpr uint32_t kStride = TC ? kTcLogitStride : (uint32_t)kMlpOut;
         const uint32_t rr = threadIdx.x;
         if (rr < kRows && row0 + rr < rows) {
@@ -1455,42 +1456,47 @@ __global__ void __launch_bounds__(256, 1) k_learn(LevelArgs A) {
             const uint32_t slot = A.learn_slot[row];
             const float4 blo = A.n_lo()[slot], bhi = A.n_hi()[slot];
             const float *Lg = logits + rr * kStride;
-            uint64_t top[kLearnMaxK];
+            uint32_t tk[kLearnMaxK], tix[kLearnMaxK];
 #pragma unroll
-            for (int i = 0; i < kLearnMaxK; i++) top[i] = 0;
+            for (int i = 0; i < kLearnMaxK; i++) tk[i] = 0u, tix[i] = 0xffu;
+            auto select = [&](auto ns_tag) {
+                constexpr int NS = decltype(ns_tag)::value;
 #pragma unroll
-            for (uint32_t j = 0; j < 3; j++) {
-                if (!(__fsub_rn(c3(bhi, j), c3(blo, j)) > 0.0f)) continue;
-#pragma unroll 8
-                for (uint32_t k = 0; k < 32; k++) {
-                    const uint32_t c = 32u * j + k;
-                    float x = Lg[c];
-                    if (x != x) x = -INFINITY;
-                    if (x == 0.0f) x = 0.0f;   // -0 ties with +0, as the values compare
-                    const uint32_t u = __float_as_uint(x);
-                    const uint32_t ord = (u & 0x80000000u) ? ~u : (u | 0x80000000u);
-                    uint64_t key = ((uint64_t)ord << 32) | (uint64_t)(95u - c);
-                    if (key <= top[kLearnMaxK - 1]) continue;
+                for (uint32_t j = 0; j < 3; j++) {
+                    if (!(__fsub_rn(c3(bhi, j), c3(blo, j)) > 0.0f)) continue;
+#pragma unroll 4
+                    for (uint32_t k = 0; k < 32; k++) {
+                        float x = Lg[32u * j + k];
+                        if (x != x) x = -INFINITY;
+                        if (x == 0.0f) x = 0.0f;   // -0 ties with +0, as the values compare
+                        const uint32_t u = __float_as_uint(x);
+                        uint32_t key = (u & 0x80000000u) ? ~u : (u | 0x80000000u), c = 32u * j + k;
 #pragma unroll
-                    for (int i = 0; i < kLearnMaxK; i++)
-                        if (key > top[i]) {
-                            const uint64_t t = top[i];
-                            top[i] = key;
-                            key = t;
+                        for (int i = 0; i < NS; i++) {
+                            const bool sw = key > tk[i];
+                            const uint32_t k2 = sw ? tk[i] : key, c2 = sw ? tix[i] : c;
+                            tk[i] = sw ? key : tk[i];
+                            tix[i] = sw ? c : tix[i];
+                            key = k2;
+                            c = c2;
                         }
+                    }
                 }
-            }
+            };
+            if (K <= 4) select(std::integral_constant<int, 4>{});
+            else select(std::integral_constant<int, kLearnMaxK>{});
             uint32_t packed[2] = {0xffffffffu, 0xffffffffu};
 #pragma unroll
             for (uint32_t r = 0; r < (uint32_t)kLearnMaxK; r++)
-                if (r < K && top[r] != 0) {
-                    const uint32_t bc = 95u - (uint32_t)(top[r] & 0xffffffffu), sh = 8u * (r & 3u);
-                    packed[r >> 2] = (packed[r >> 2] & ~(0xffu << sh)) | (bc << sh);
+                if (r < K && tk[r] != 0u) {
+                    const uint32_t sh = 8u * (r & 3u);
+                    packed[r >> 2] = (packed[r >> 2] & ~(0xffu << sh)) | (tix[r] << sh);
                 }
             A.learn_prop[row] = make_uint2(packed[0], packed[1]);
             if (A.prop_log) {
                 const uint32_t cidx = A.n_info()[slot].z;
                 if (cidx < A.cap_nodes)
+#pragma unroll
                     for (uint32_t r = 0; r < 8; r++) {
                         const uint32_t bb = (packed[r >> 2] >> (8u * (r & 3u))) & 0xffu;
                         A.prop_log[(size_t)cidx * 8 + r] = bb == 0xffu ? -1 : (int32_t)bb;

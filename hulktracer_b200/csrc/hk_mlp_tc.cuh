@@ -119,13 +119,29 @@ __device__ __forceinline__ void tc_commit(uint32_t bar) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
 }
 
+// 16 or 32 consecutive accumulator columns of the warp's 32 lanes; the load
+// and its wait are one asm statement, so no use of the registers can be
+// scheduled before the wait
 __device__ __forceinline__ void tc_ld16(uint32_t taddr, uint32_t *r) {
     asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n\t"
+        "tcgen05.wait::ld.sync.aligned;"
         : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
           "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-        : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        : "r"(taddr)
+        : "memory");
+}
+__device__ __forceinline__ void tc_ld32(uint32_t taddr, uint32_t *r) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n\t"
+        "tcgen05.wait::ld.sync.aligned;"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr)
+        : "memory");
 }
 
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
@@ -220,15 +236,20 @@ __device__ __forceinline__ bool tc_tile_forward(const MlpDevice &M, const float 
         for (uint32_t q = 0; q < kTcAhead && s_ok; q++)
             if (!issue(q)) s_ok = 0;
     }
-    // the biases, read by every epilogue
-    for (uint32_t i = tid; i < kTcBiasN; i += blockDim.x) {
-        const uint32_t l = i / kMlpHid, j = i % kMlpHid;
-        S.bias[i] = l == 0 ? M.b1[j] : (l == 1 ? M.b2[j] : (l == 2 ? M.b3[j] : M.b4[j]));
+    // the biases, read by every epilogue: loaded now, stored to shared memory
+    // after the features (all of a thread's loads in flight at once)
+    constexpr uint32_t kBiasPer = (kTcBiasN + 255u) / 256u;
+    float bias_v[kBiasPer];
+#pragma unroll
+    for (uint32_t u = 0; u < kBiasPer; u++) {
+        const uint32_t i = tid + u * blockDim.x, l = i / kMlpHid, j = i % kMlpHid;
+        const float *bp = l == 0 ? M.b1 : (l == 1 ? M.b2 : (l == 2 ? M.b3 : M.b4));
+        bias_v[u] = i < kTcBiasN ? bp[j] : 0.0f;
     }
     // the tile's features as BF16 in the canonical layout, K 200 .. 255 zero
     // (a row of 200 floats starts 800-byte aligned: 8 values are two float4)
-    // (four rows' loads in flight per thread before any is converted)
-    constexpr uint32_t kStage = 4;
+    // (eight rows' loads in flight per thread before any is converted)
+    constexpr uint32_t kStage = 8;
     for (uint32_t i0 = tid; i0 < (uint32_t)kTcRows * (kTcAK / 8); i0 += kStage * blockDim.x) {
         float4 x0[kStage], x1[kStage];
 #pragma unroll
@@ -258,6 +279,9 @@ __device__ __forceinline__ bool tc_tile_forward(const MlpDevice &M, const float 
             *reinterpret_cast<uint4 *>(S.A + tc_a_off(m, k0)) = make_uint4(w[0], w[1], w[2], w[3]);
         }
     }
+#pragma unroll
+    for (uint32_t u = 0; u < kBiasPer; u++)
+        if (tid + u * blockDim.x < kTcBiasN) S.bias[tid + u * blockDim.x] = bias_v[u];
     tc_fence_async_smem();
     tc_fence_before();
     __syncthreads();
@@ -303,9 +327,10 @@ __device__ __forceinline__ bool tc_tile_forward(const MlpDevice &M, const float 
         const uint32_t m = 32u * (warp & 3u) + lane;
         const uint32_t half = N / 2, c0 = (warp >> 2) * half;
         const float *bl = S.bias + (uint32_t)l * kMlpHid;
-        for (uint32_t c = c0; c < c0 + half; c += 16) {
-            uint32_t r[16];
-            tc_ld16(tmem + ((32u * (warp & 3u)) << 16) + c, r);
+        const uint32_t trow = tmem + ((32u * (warp & 3u)) << 16);
+        // columns c .. c + 15 from r: bias, ReLU and BF16 into the next
+        // layer's operand, or bias into the logits after the last layer
+        auto epi16 = [&](const uint32_t *r, uint32_t c) {
             if (l < 3) {
                 uint32_t w[8];
 #pragma unroll
@@ -321,6 +346,19 @@ __device__ __forceinline__ bool tc_tile_forward(const MlpDevice &M, const float 
 #pragma unroll
                 for (int j = 0; j < 16; j++) S.logits[m * kTcLogitStride + c + j] = __uint_as_float(r[j]) + bl[c + j];
             }
+        };
+        // 32 columns per TMEM load while they last (half is 128 or 48)
+        uint32_t c = c0;
+        for (; c + 32 <= c0 + half; c += 32) {
+            uint32_t r[32];
+            tc_ld32(trow + c, r);
+            epi16(r, c);
+            epi16(r + 16, c + 16);
+        }
+        if (c < c0 + half) {
+            uint32_t r[16];
+            tc_ld16(trow + c, r);
+            epi16(r, c);
         }
         tc_fence_async_smem();
         tc_fence_before();
