@@ -247,15 +247,18 @@ __device__ __forceinline__ bool tc_tile_forward(const MlpDevice &M, const float 
         bias_v[u] = i < kTcBiasN ? bp[j] : 0.0f;
     }
     // the tile's features as BF16 in the canonical layout, K 200 .. 255 zero
-    // (a row of 200 floats starts 800-byte aligned: 8 values are two float4)
-    // (eight rows' loads in flight per thread before any is converted)
+    // (a row of 200 floats starts 800-byte aligned: 8 values are two float4;
+    // eight loads in flight per thread before any is converted). Item i is
+    // row m = (i / 256) * 8 + i % 8, values k0 = ((i / 8) % 32) * 8 .. + 7,
+    // whose 16 bytes sit at tc_a_off(m, k0) = 16 i: a warp stores 512
+    // consecutive bytes, and reads 8 rows x 128 bytes.
     constexpr uint32_t kStage = 8;
     for (uint32_t i0 = tid; i0 < (uint32_t)kTcRows * (kTcAK / 8); i0 += kStage * blockDim.x) {
         float4 x0[kStage], x1[kStage];
 #pragma unroll
         for (uint32_t u = 0; u < kStage; u++) {
             const uint32_t i = i0 + u * blockDim.x;
-            const uint32_t m = i / (kTcAK / 8), k0 = (i % (kTcAK / 8)) * 8;
+            const uint32_t m = (i >> 8) * 8u + (i & 7u), k0 = ((i >> 3) & 31u) * 8u;
             const uint32_t r = row0 + m;
             x0[u] = x1[u] = make_float4(0, 0, 0, 0);
             if (i < (uint32_t)kTcRows * (kTcAK / 8) && r < rows && k0 < (uint32_t)kMlpIn) {
@@ -268,7 +271,6 @@ __device__ __forceinline__ bool tc_tile_forward(const MlpDevice &M, const float 
         for (uint32_t u = 0; u < kStage; u++) {
             const uint32_t i = i0 + u * blockDim.x;
             if (i >= (uint32_t)kTcRows * (kTcAK / 8)) break;
-            const uint32_t m = i / (kTcAK / 8), k0 = (i % (kTcAK / 8)) * 8;
             const float v[8] = {x0[u].x, x0[u].y, x0[u].z, x0[u].w, x1[u].x, x1[u].y, x1[u].z, x1[u].w};
             uint32_t w[4];
 #pragma unroll
@@ -276,7 +278,7 @@ __device__ __forceinline__ bool tc_tile_forward(const MlpDevice &M, const float 
                 const __nv_bfloat162 h = __floats2bfloat162_rn(v[2 * j], v[2 * j + 1]);
                 w[j] = *reinterpret_cast<const uint32_t *>(&h);
             }
-            *reinterpret_cast<uint4 *>(S.A + tc_a_off(m, k0)) = make_uint4(w[0], w[1], w[2], w[3]);
+            *reinterpret_cast<uint4 *>(S.A + 16u * i) = make_uint4(w[0], w[1], w[2], w[3]);
         }
     }
 #pragma unroll
@@ -309,8 +311,9 @@ __device__ __forceinline__ bool tc_tile_forward(const MlpDevice &M, const float 
                     tc_mma(tmem, da, db, idesc, (kc > 0 || s > 0) ? 1u : 0u);
                 }
                 tc_commit(S.bar_mma(b));
-                // refill the ring: the buffer of chunk q - 1, whose MMAs precede these
-                if (q + kTcAhead < (uint32_t)kTcChunks && !issue(q + kTcAhead)) s_ok = 0;
+                // refill the ring: the buffer of chunk q - 1, whose MMAs precede
+                // these (a layer's last chunk was issued before the epilogue)
+                if (q + kTcAhead < (uint32_t)kTcChunks && (kc != 0 || l == 0) && !issue(q + kTcAhead)) s_ok = 0;
             }
         }
         __syncthreads();
@@ -322,6 +325,9 @@ __device__ __forceinline__ bool tc_tile_forward(const MlpDevice &M, const float 
         if (!ok) s_ok = 0;
         __syncthreads();
         if (!s_ok) break;
+        // the next layer's last chunk into the buffer this layer's last chunk
+        // has just freed, so that its copy runs during the epilogue
+        if (tid == 0 && l < 3 && !issue((uint32_t)(l * 4 + 4 + kTcAhead))) s_ok = 0;
         tc_fence_after();
         // epilogue: warp w reads lanes 32 (w % 4) .. + 31 (rows), columns of half w / 4
         const uint32_t m = 32u * (warp & 3u) + lane;
