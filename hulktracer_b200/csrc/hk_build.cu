@@ -1537,6 +1537,9 @@ constexpr uint32_t kRefineThreads = 256;
 constexpr uint32_t kRefineWarpMax = 128;   // rows up to this many references: one warp each
 constexpr uint32_t kRefineRowWarps = 8;
 constexpr size_t kRefineWarpSmem = (size_t)kRefineRowWarps * kLearnScratch * 4;   // 64 KB
+// k_refine_warp's grid in CTAs per SM: more than are resident (two, by its
+// registers), so that CTAs finishing early are replaced by new ones
+constexpr int kRefineWarpGrid = 3;
 
 __device__ __forceinline__ bool refine_better(float c, uint32_t a, float p, float bc, uint32_t ba, float bp) {
     return c < bc || (c == bc && (a < ba || (a == ba && p < bp)));
@@ -3058,7 +3061,7 @@ cudaError_t build_launch(BuildState &S, const float4 *verts, const uint4 *tris, 
             // stream, beside the CTA-costed ones
             cudaEventRecord(S.ev_learn, S.aux);
             cudaStreamWaitEvent(S.aux2, S.ev_learn, 0);
-            k_refine_warp<<<S.sm_count * 3, 256, kRefineWarpSmem, S.aux2>>>(A);
+            k_refine_warp<<<S.sm_count * kRefineWarpGrid, 256, kRefineWarpSmem, S.aux2>>>(A);
             cudaEventRecord(S.ev_join2, S.aux2);
             launch_pdl(k_refine_cta, S.sm_count * 8, kRefineThreads, kRefineSmem, S.aux, A);
         }
